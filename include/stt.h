@@ -1,0 +1,185 @@
+/* include/stt.h -- C ABI of libstt.so, the B200 (sm_100a) implementation of
+ * SpaceTimeTomography's reconstruction hot path.
+ *
+ * Conventions
+ *   - Every entry point returns stt_status; STT_OK is 0.  Nothing throws across
+ *     the ABI.  stt_last_error() returns the message of the last failure on a
+ *     context (a pointer valid until the next call on that context).
+ *   - All array arguments are DEVICE pointers owned by the caller, except where
+ *     a comment says "host".  Layouts follow the reference: volumes x-fastest
+ *     (idx = x + y*nx + z*nx*ny, CImg (x,y,z) order), detector images
+ *     m-fastest (idx = m + n*W), multi-channel volumes planar (CImg (x,y,z,c)),
+ *     projection stacks view-major (idx = m + n*W + v*W*H).
+ *   - `stream` is a cudaStream_t passed as void*; NULL is the legacy default
+ *     stream.  Calls only enqueue work; nothing synchronises unless stated.
+ *   - A context is used by one host thread at a time; different contexts may
+ *     be used concurrently.  A context owns its geometry tables and the scratch
+ *     accumulators of the ray-driven backprojector.
+ *
+ * Reference interfaces replaced (paths relative to the reference project root
+ * gmzang/SpaceTimeTomography, S/ = SpaceTimeTomography/):
+ *   forward projector  GenerateImage_GetCorrections  S/ImageFormationModel/TypicalRayProducer.core.h:230
+ *                      + SingleScalarVolumePrepare    S/ImageFormationModel/SingleScalarVolume.core.h:195
+ *                      + RayCasterPrepare             S/ImageFormationModel/RayCaster.core.h:191
+ *   geometry           TypicalRayProducer ctor / SetVolSize / SetViewMatrix / SetProjectionMatrix
+ *                      S/ImageFormationModel/TypicalRayProducer.h:11-24, Scene::_calculateMatrix Scene.cpp:181,
+ *                      ST_Tomography::InitViews S/ST_Tomo/ST_Tomography.cpp:887
+ *   SART               ST_Tomography::SART        S/ST_Tomo/ST_Tomography.cpp:616-808
+ *   primal-dual steps  ST_Tomography::Render      S/ST_Tomo/ST_Tomography.cpp:492-607
+ *   warp               warping::warp              S/ST_Tomo/warping.h:116-145
+ */
+#ifndef STT_H
+#define STT_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum stt_status {
+    STT_OK = 0,
+    STT_ERR_INVALID = 1,      /* bad argument (null pointer, size, geometry) */
+    STT_ERR_CUDA = 2,         /* a CUDA runtime call or kernel launch failed */
+    STT_ERR_NOMEM = 3,        /* device allocation failed */
+    STT_ERR_STATE = 4,        /* call out of order (e.g. no geometry set) */
+    STT_ERR_UNSUPPORTED = 5,  /* option not available in this build */
+    STT_ERR_TIMEOUT = 6       /* a bounded device-side wait gave up */
+} stt_status;
+
+typedef struct stt_ctx stt_ctx;
+
+/* Scan geometry.  Replaces the TypicalRayProducer constructor arguments
+ * (TypicalRayProducer.h:11), VolumeData::SetSpacings, the Scene members set by
+ * the ST_Tomography constructor (ST_Tomography.cpp:200-246) and the per-view
+ * quaternions of InitViews (:887-934).  The per-view ray and voxel projections
+ * are built on the host in FP64.
+ *   angles_rad: HOST array of n_views rotation angles about +y (radians);
+ *   stt_views_from_rounds() builds the reference's "rounds x 10 views 36 deg
+ *   apart" lists. */
+typedef struct stt_geometry {
+    int nx, ny, nz;        /* volume dimensions (voxels)             -f        */
+    double sx, sy, sz;     /* voxel spacing (mm)                      -c        */
+    int W, H;              /* detector size (pixels)                  -u        */
+    double ds;             /* detector pixel spacing (mm)             -d        */
+    double sid, sdd;       /* source-isocentre, source-detector (mm)  -g, -j    */
+    double off[3];         /* volume-centre offset (mm)               --oxyz    */
+    int n_views;
+    const double *angles_rad;
+} stt_geometry;
+
+/* Context lifetime.  device: CUDA ordinal. */
+stt_status stt_create(stt_ctx **ctx, int device);
+stt_status stt_destroy(stt_ctx *ctx);
+const char *stt_last_error(const stt_ctx *ctx);
+/* Library version string, e.g. "stt 0.1.0 sm_100a". */
+const char *stt_version(void);
+
+/* Host helper: angles (radians) of the reference's view list.  Round r of
+ * `rounds` starts at start_deg[r] (host); views k = 0..views_per_round-1 sit
+ * step_deg apart; angles_out (host) receives rounds*views_per_round values.
+ * The start angle is rounded through float and pi is 3.1415926 as in
+ * ST_Tomography.cpp:264-268, 871, 899. */
+stt_status stt_views_from_rounds(int rounds, const double *start_deg, int views_per_round,
+                                 double step_deg, double *angles_out);
+
+/* Low-discrepancy start angles (degrees) of the acquisition scripts
+ * (low discrepancy sequence/Low_discrepency_squence.m:38-67): van der Corput in
+ * base p, Ns segments, a reference angle 0 every Nz entries.  out (host) gets n values. */
+stt_status stt_lds_angles(int n, int Ns, int p, int Nz, double *out);
+
+/* Set (or replace) the geometry and view list. Allocates the context's device tables. */
+stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g);
+
+/* ---- forward projector (TypicalRayProducer.core.h:123-268) ---------------
+ * Projects views [view0, view0+nviews) of `vol`.
+ *   proj   : nviews*W*H line integrals (sum of f*sd, entry sample counted twice)
+ *   raylen : optional W*H*nviews ray lengths (tfar - tnear, mm); written only
+ *            where the ray hits the volume, as the reference does
+ *   weight : optional W*H*nviews sample counts */
+stt_status stt_fp(stt_ctx *ctx, const float *vol, float *proj, float *raylen, float *weight,
+                  int view0, int nviews, void *stream);
+
+/* Forward projection of one view fused with the SART correction
+ * (ST_Tomography.cpp:667-676): corr = (b - Ax) / (L + 1), where L is the
+ * sticky ray-length state (W*H, updated where the ray hits). */
+stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, float *raylen_state,
+                             float *corr, int view, void *stream);
+
+/* Exact adjoint of stt_fp: vol_bar += A^T proj_bar over views [view0, view0+nviews).
+ * Scatter with float atomics (order-nondeterministic). */
+stt_status stt_fp_vjp(stt_ctx *ctx, const float *proj_bar, float *vol_bar, int view0, int nviews,
+                      void *stream);
+
+/* ---- backprojectors ------------------------------------------------------
+ * Voxel-driven (ST_Tomography.cpp:690-730): vol = clamp(vol + alpha *
+ * bicubic(corr at the voxel's projection), 0, gmax); voxels projecting
+ * outside [2, W-2) x [2, H-2) are left unchanged.  Deterministic. */
+stt_status stt_bp_voxel(stt_ctx *ctx, const float *corr, float *vol, double alpha, float gmax,
+                        int view, void *stream);
+
+/* Ray-driven (ST_Tomography.cpp:733-764, SingleScalarVolume.core.h:73-84):
+ * scatters corr*w and w along every ray into the context's accumulators, then
+ * vol = clamp(vol + contrib/weight, 0, gmax) with 0/0 -> 0 and the
+ * accumulators reset.  Atomics: result is order-nondeterministic in the last bits. */
+stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, int view,
+                      void *stream);
+
+/* ---- SART (ST_Tomography.cpp:616-808) -------------------------------------
+ * One SART call for one frame: for i in 0..nperm-1, view = view_offset +
+ * perm[i] (perm is HOST): FP + correction, then backprojection (bp_mode 0
+ * voxel-based with alpha, 1 ray-based).  proj_stack holds the frame's
+ * projections indexed by perm values (W*H each).  raylen_state: W*H sticky
+ * ray lengths (zero it once at start; ray-based mode re-zeroes it after every
+ * view as TypicalRayProducer::Initial does).  If roi_cut (HOST, 8 ints) is not
+ * NULL the ROI mask of ST_Tomography.cpp:303-329 is applied at the end. */
+stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, const int *perm,
+                          int nperm, int view_offset, double alpha, float gmax, int bp_mode,
+                          float *raylen_state, const int *roi_cut, void *stream);
+
+/* Host helper: the seeded view permutation that replaces srand(time(0)) +
+ * random_shuffle (ST_Tomography.cpp:635-642): SplitMix64 + Fisher-Yates. */
+stt_status stt_permutation(unsigned long long seed, int n, int *perm_out);
+
+/* ---- primal-dual steps (ST_Tomography.cpp:492-604) -------------------------
+ * Parameters as the reference uses them: sigma = CP_sigma, tau = CP_tau,
+ * tv_w = TV_w, tp_w = TP_w, bc_w = BC_w, huber_factor = m_huberfactor,
+ * gmax = G_Max; cut = the ROI cut[8] (ST_Tomography.cpp:114). */
+typedef struct stt_pd_params {
+    float sigma, tau, tv_w, tp_w, bc_w, huber_factor, gmax;
+    int cut[8];
+} stt_pd_params;
+
+/* Dual step of frame f (:504-534).  bw = warp(flow[f], xbar[f+1], -1).
+ * ytv: 3 planar channels.  All arrays nx*ny*nz (dims from the geometry). */
+stt_status stt_pd_dual(stt_ctx *ctx, const stt_pd_params *p, const float *xbar_f,
+                       const float *xbar_f1, const float *bw, float *ytv, float *ytp, float *ybc,
+                       void *stream);
+/* Primal step of frame f (:536-578).  first_frame != 0 uses ytp/ybc only;
+ * otherwise fw = warp(flow[f-1], ybc[f-1], +1) and ytp_prev = ytp[f-1].
+ * Writes xprev = vol (before the update). */
+stt_status stt_pd_primal(stt_ctx *ctx, const stt_pd_params *p, int first_frame,
+                         const float *ytp_prev, const float *ytp, const float *fw,
+                         const float *ybc, const float *ytv, float *vol, float *xprev,
+                         void *stream);
+/* Over-relaxation (:586-604): xbar = 2*vol - xprev inside the ROI box. */
+stt_status stt_pd_extrapolate(stt_ctx *ctx, const int *cut, const float *vol, const float *xprev,
+                              float *xbar, void *stream);
+/* ROI mask (:303-329): roi = 0/1 per voxel; cut is HOST int[8]. */
+stt_status stt_roi_mask(stt_ctx *ctx, const int *cut, float *roi, void *stream);
+
+/* ---- warp (ST_Tomo/warping.h:49-145) ---------------------------------------
+ * Semi-Lagrangian warp on the cell-centred grid with aabb = [0, dim]:
+ * out(x) = clamped-Catmull-Rom(src, trace(x, -dt)), nc planar channels.
+ * vel: 3 planar channels.  dim (HOST) is independent of the geometry. */
+stt_status stt_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
+                    float *out, void *stream);
+/* Vector-Jacobian product of stt_warp: src_bar += J_src^T out_bar and
+ * vel_bar += J_vel^T out_bar (either may be NULL; both accumulate with atomics). */
+stt_status stt_warp_vjp(const int *dim, const float *vel, const float *src, int nc, float dt,
+                        const float *out_bar, float *src_bar, float *vel_bar, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STT_H */

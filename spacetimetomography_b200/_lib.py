@@ -1,0 +1,85 @@
+"""ctypes binding of libstt.so (the C ABI declared in include/stt.h).
+
+The CUDA library is the only implementation: importing this module without a
+built ``libstt.so`` raises, and there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libstt.so"
+
+
+class STTError(RuntimeError):
+    """A libstt call returned a non-zero stt_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"stt status {status}: {message}")
+        self.status = status
+
+
+STATUS = {0: "STT_OK", 1: "STT_ERR_INVALID", 2: "STT_ERR_CUDA", 3: "STT_ERR_NOMEM",
+          4: "STT_ERR_STATE", 5: "STT_ERR_UNSUPPORTED", 6: "STT_ERR_TIMEOUT"}
+
+
+class Geometry(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("sx", C.c_double), ("sy", C.c_double), ("sz", C.c_double),
+                ("W", C.c_int), ("H", C.c_int), ("ds", C.c_double),
+                ("sid", C.c_double), ("sdd", C.c_double), ("off", C.c_double * 3),
+                ("n_views", C.c_int), ("angles_rad", C.POINTER(C.c_double))]
+
+
+class PdParams(C.Structure):
+    _fields_ = [("sigma", C.c_float), ("tau", C.c_float), ("tv_w", C.c_float),
+                ("tp_w", C.c_float), ("bc_w", C.c_float), ("huber_factor", C.c_float),
+                ("gmax", C.c_float), ("cut", C.c_int * 8)]
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is not built; run `python -m spacetimetomography_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    vp, i, d, f = C.c_void_p, C.c_int, C.c_double, C.c_float
+    sigs = {
+        "stt_create": [C.POINTER(vp), i],
+        "stt_destroy": [vp],
+        "stt_set_geometry": [vp, C.POINTER(Geometry)],
+        "stt_views_from_rounds": [i, vp, i, d, vp],
+        "stt_lds_angles": [i, i, i, i, vp],
+        "stt_permutation": [C.c_ulonglong, i, vp],
+        "stt_fp": [vp, vp, vp, vp, vp, i, i, vp],
+        "stt_fp_correction": [vp, vp, vp, vp, vp, i, vp],
+        "stt_fp_vjp": [vp, vp, vp, i, i, vp],
+        "stt_bp_voxel": [vp, vp, vp, d, f, i, vp],
+        "stt_bp_ray": [vp, vp, vp, f, i, vp],
+        "stt_sart_sweep": [vp, vp, vp, vp, i, i, d, f, i, vp, vp, vp],
+        "stt_pd_dual": [vp, C.POINTER(PdParams), vp, vp, vp, vp, vp, vp, vp],
+        "stt_pd_primal": [vp, C.POINTER(PdParams), i, vp, vp, vp, vp, vp, vp, vp, vp],
+        "stt_pd_extrapolate": [vp, vp, vp, vp, vp, vp],
+        "stt_roi_mask": [vp, vp, vp, vp],
+        "stt_warp": [vp, vp, vp, i, f, vp, vp],
+        "stt_warp_vjp": [vp, vp, vp, i, f, vp, vp, vp, vp],
+    }
+    for name, argtypes in sigs.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = C.c_int
+    lib.stt_last_error.argtypes = [vp]
+    lib.stt_last_error.restype = C.c_char_p
+    lib.stt_version.argtypes = []
+    lib.stt_version.restype = C.c_char_p
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int, ctx=None) -> None:
+    if status != 0:
+        msg = lib.stt_last_error(ctx)
+        raise STTError(status, (msg or b"").decode(errors="replace"))

@@ -1,0 +1,207 @@
+"""Python side of the libstt C ABI (include/stt.h), on torch CUDA tensors.
+
+Shapes (C order, x fastest as in the reference's CImg layout):
+  volume            (nz, ny, nx)        float32
+  projection stack  (nviews, H, W)      float32
+  flow / velocity   (3, nz, ny, nx)     float32, planar channels
+  dual TV variable  (3, nz, ny, nx)     float32
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+from ._lib import Geometry, check, lib
+from ._lib import PdParams as _PdParams
+
+# ROI cut of the reference (ST_Tomography.cpp:114)
+REFERENCE_CUT = (8, 8, 8, 45, 8, 8, 30, 20)
+
+
+def _ptr(t) -> C.c_void_p | None:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("libstt works on CUDA tensors")
+    if not t.is_contiguous():
+        raise ValueError("tensor must be contiguous")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream) -> C.c_void_p | None:
+    if stream is None:
+        import torch
+
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream) if stream.cuda_stream else None
+
+
+def views_from_rounds(start_deg: Sequence[float], views_per_round: int = 10,
+                      step_deg: float = 36.0) -> np.ndarray:
+    """Angles (rad) of the reference's view list (InitViews, ST_Tomography.cpp:887-934)."""
+    s = np.ascontiguousarray(start_deg, dtype=np.float64)
+    out = np.zeros(len(s) * views_per_round, dtype=np.float64)
+    check(lib.stt_views_from_rounds(len(s), s.ctypes.data_as(C.c_void_p), views_per_round,
+                                    float(step_deg), out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+def lds_angles(n: int, segments: int = 10, base: int = 2, zero_every: int = 10000) -> np.ndarray:
+    """Low_discrepency_squence.m:38-67 (degrees)."""
+    out = np.zeros(n, dtype=np.float64)
+    check(lib.stt_lds_angles(n, segments, base, zero_every, out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+def permutation(seed: int, n: int) -> np.ndarray:
+    """Seeded view order (SplitMix64 + Fisher-Yates) used in place of time(0)."""
+    out = np.zeros(n, dtype=np.int32)
+    check(lib.stt_permutation(C.c_ulonglong(seed), n, out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+@dataclass
+class PdParams:
+    """Primal-dual parameters as ST_Tomography uses them (ST_Tomography.cpp:99-120, 215-219)."""
+
+    sigma: float = 0.9 / 8.0
+    tau: float = 1.0
+    tv_w: float = 0.1
+    tp_w: float = 0.5
+    bc_w: float = 0.5
+    huber_factor: float = 1.0
+    gmax: float = 10.0
+    cut: tuple = field(default=REFERENCE_CUT)
+
+    def c(self) -> _PdParams:
+        p = _PdParams(self.sigma, self.tau, self.tv_w, self.tp_w, self.bc_w, self.huber_factor,
+                      self.gmax)
+        for k in range(8):
+            p.cut[k] = int(self.cut[k])
+        return p
+
+
+class Context:
+    """One libstt context (stt_create/stt_destroy) on one device."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib.stt_create(C.byref(h), int(device)))
+        self._h = h
+        self.device = device
+        self.dims = None
+        self.det = None
+        self.n_views = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.stt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st: int) -> None:
+        check(st, self._h)
+
+    def set_geometry(self, dims, spacing, det, ds, sid, sdd, angles, offset=(0.0, 0.0, 0.0)):
+        """dims=(nx,ny,nz), spacing=(sx,sy,sz) mm, det=(W,H), angles in radians."""
+        ang = np.ascontiguousarray(angles, dtype=np.float64)
+        self._angles = ang  # keep alive for the call
+        g = Geometry(int(dims[0]), int(dims[1]), int(dims[2]), float(spacing[0]), float(spacing[1]),
+                     float(spacing[2]), int(det[0]), int(det[1]), float(ds), float(sid), float(sdd),
+                     (C.c_double * 3)(*map(float, offset)), len(ang),
+                     ang.ctypes.data_as(C.POINTER(C.c_double)))
+        self._chk(lib.stt_set_geometry(self._h, C.byref(g)))
+        self.dims = tuple(int(x) for x in dims)
+        self.det = (int(det[0]), int(det[1]))
+        self.n_views = len(ang)
+
+    # ---- projector ---------------------------------------------------------
+    def fp(self, vol, proj, view0=0, nviews=None, raylen=None, weight=None, stream=None):
+        nviews = self.n_views - view0 if nviews is None else nviews
+        self._chk(lib.stt_fp(self._h, _ptr(vol), _ptr(proj), _ptr(raylen), _ptr(weight), view0,
+                             nviews, _stream(stream)))
+        return proj
+
+    def fp_correction(self, vol, b, raylen_state, corr, view, stream=None):
+        self._chk(lib.stt_fp_correction(self._h, _ptr(vol), _ptr(b), _ptr(raylen_state), _ptr(corr),
+                                        view, _stream(stream)))
+        return corr
+
+    def fp_vjp(self, proj_bar, vol_bar, view0=0, nviews=None, stream=None):
+        nviews = self.n_views - view0 if nviews is None else nviews
+        self._chk(lib.stt_fp_vjp(self._h, _ptr(proj_bar), _ptr(vol_bar), view0, nviews,
+                                 _stream(stream)))
+        return vol_bar
+
+    def bp_voxel(self, corr, vol, alpha, gmax, view, stream=None):
+        self._chk(lib.stt_bp_voxel(self._h, _ptr(corr), _ptr(vol), float(alpha), float(gmax), view,
+                                   _stream(stream)))
+        return vol
+
+    def bp_ray(self, corr, vol, gmax, view, stream=None):
+        self._chk(lib.stt_bp_ray(self._h, _ptr(corr), _ptr(vol), float(gmax), view, _stream(stream)))
+        return vol
+
+    def sart_sweep(self, vol, proj_stack, perm, alpha, gmax, bp_mode, raylen_state,
+                   view_offset=0, roi_cut=None, stream=None):
+        perm = np.ascontiguousarray(perm, dtype=np.int32)
+        cut = None if roi_cut is None else (C.c_int * 8)(*map(int, roi_cut))
+        self._chk(lib.stt_sart_sweep(self._h, _ptr(vol), _ptr(proj_stack),
+                                     perm.ctypes.data_as(C.c_void_p), len(perm), view_offset,
+                                     float(alpha), float(gmax), int(bp_mode), _ptr(raylen_state),
+                                     cut, _stream(stream)))
+        return vol
+
+    # ---- primal-dual -------------------------------------------------------
+    def pd_dual(self, p: PdParams, xbar_f, xbar_f1, bw, ytv, ytp, ybc, stream=None):
+        pc = p.c()
+        self._chk(lib.stt_pd_dual(self._h, C.byref(pc), _ptr(xbar_f), _ptr(xbar_f1), _ptr(bw),
+                                  _ptr(ytv), _ptr(ytp), _ptr(ybc), _stream(stream)))
+
+    def pd_primal(self, p: PdParams, first_frame, ytp_prev, ytp, fw, ybc, ytv, vol, xprev,
+                  stream=None):
+        pc = p.c()
+        self._chk(lib.stt_pd_primal(self._h, C.byref(pc), int(bool(first_frame)), _ptr(ytp_prev),
+                                    _ptr(ytp), _ptr(fw), _ptr(ybc), _ptr(ytv), _ptr(vol),
+                                    _ptr(xprev), _stream(stream)))
+
+    def pd_extrapolate(self, cut, vol, xprev, xbar, stream=None):
+        c = (C.c_int * 8)(*map(int, cut))
+        self._chk(lib.stt_pd_extrapolate(self._h, c, _ptr(vol), _ptr(xprev), _ptr(xbar),
+                                         _stream(stream)))
+
+    def roi_mask(self, cut, roi, stream=None):
+        c = (C.c_int * 8)(*map(int, cut))
+        self._chk(lib.stt_roi_mask(self._h, c, _ptr(roi), _stream(stream)))
+        return roi
+
+
+def warp(flow, src, dt, out=None, stream=None):
+    """warping::warp (warping.h:116-145) with aabb = [0, dim]; src (nc, nz, ny, nx) or (nz, ny, nx)."""
+    import torch
+
+    nc = 1 if src.dim() == 3 else src.shape[0]
+    nz, ny, nx = src.shape[-3:]
+    dim = (C.c_int * 3)(nx, ny, nz)
+    if out is None:
+        out = torch.empty_like(src)
+    check(lib.stt_warp(dim, _ptr(flow), _ptr(src), nc, float(dt), _ptr(out), _stream(stream)))
+    return out
+
+
+def warp_vjp(flow, src, dt, out_bar, src_bar=None, flow_bar=None, stream=None):
+    """Accumulates J_src^T out_bar into src_bar and J_flow^T out_bar into flow_bar."""
+    nc = 1 if src.dim() == 3 else src.shape[0]
+    nz, ny, nx = src.shape[-3:]
+    dim = (C.c_int * 3)(nx, ny, nz)
+    check(lib.stt_warp_vjp(dim, _ptr(flow), _ptr(src), nc, float(dt), _ptr(out_bar), _ptr(src_bar),
+                           _ptr(flow_bar), _stream(stream)))
+    return src_bar, flow_bar

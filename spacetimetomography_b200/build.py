@@ -1,0 +1,80 @@
+"""In-tree build of libstt.so (CUDA, sm_100a) and the C++ drop-in layer.
+
+``python -m spacetimetomography_b200.build`` compiles
+
+* ``spacetimetomography_b200/libstt.so``  -- kernels + the C ABI of include/stt.h
+* ``spacetimetomography_b200/libstt_facade.so`` and ``bin/st_tomography`` -- the
+  C++ classes and command line that keep the reference's names (built only when
+  their sources exist)
+
+with nvcc for ``arch=compute_100a,code=sm_100a``.  Outputs stay inside the
+package directory so they travel with the repository snapshot.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+LIB = PKG / "libstt.so"
+
+GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
+
+KERNEL_SOURCES = ["stt_capi.cu", "k_project.cu", "k_voxel.cu", "k_warp.cu"]
+
+
+def _nvcc() -> str:
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    cand = Path(cuda) / "bin" / "nvcc"
+    if cand.exists():
+        return str(cand)
+    found = shutil.which("nvcc")
+    if not found:
+        raise RuntimeError("nvcc not found: libstt.so cannot be built")
+    return found
+
+
+def _host_compiler() -> list[str]:
+    # The image exports CXX=/opt/gcc/bin/g++; nvcc is pinned to the system g++.
+    gxx = "/usr/bin/g++"
+    return ["-ccbin", gxx] if Path(gxx).exists() else []
+
+
+def _stale(out: Path, deps: list[Path]) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build_libstt(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
+    srcs = [CSRC / s for s in KERNEL_SOURCES]
+    deps = srcs + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [INCLUDE / "stt.h"]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    cmd = [_nvcc(), *GENCODE, *NVCC_FLAGS, *_host_compiler(), "-shared",
+           f"-I{INCLUDE}", f"-I{CSRC}", "-o", str(LIB), *map(str, srcs), *(extra or [])]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+def build_all(force: bool = False, verbose: bool = False) -> None:
+    build_libstt(force=force, verbose=verbose)
+    facade = CSRC / "facade"
+    if facade.exists():
+        from . import build_facade  # noqa: WPS433  (optional second stage)
+
+        build_facade.build(force=force, verbose=verbose)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv, verbose=True)

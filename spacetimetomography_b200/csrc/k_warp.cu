@@ -1,0 +1,302 @@
+// k_warp.cu -- semi-Lagrangian tricubic warp (S/ST_Tomo/warping.h:49-145) and
+// its vector-Jacobian product.
+//
+// One thread per output voxel, x fastest.  Per voxel: the velocity at the
+// cell centre (an exact grid read: the Catmull-Rom sampler interpolates, and
+// the centre lands on a node), one clamped tricubic velocity sample at the
+// half-traced point (3 channels sharing one 64-tap stencil) and one clamped
+// tricubic sample of every source channel at the traced point.  Taps come from
+// L1/L2 through the read-only path.
+#include "stt_internal.cuh"
+#include "stt_kernels.h"
+
+namespace stt {
+
+namespace {
+
+struct Dim3i {
+    int x, y, z;
+};
+
+// world (aabb = [0,dim]) -> cell grid, clamped to [1, dim-2] (warping.h:54-62).
+__device__ __forceinline__ float to_grid(float p, int dim, bool *clamped) {
+    float gw = __fdiv_rn(__fmul_rn((float)dim, p), (float)dim);
+    float gq = gw - 0.5f;
+    const float hi = (float)(dim - 2), lo = 1.0f;
+    bool c = !(gq >= lo && gq <= hi);
+    gq = (gq < hi) ? gq : hi;  // std::min(hi, g)
+    gq = (lo < gq) ? gq : lo;  // std::max(lo, g)
+    if (clamped) *clamped = c;
+    return gq;
+}
+
+// Stencil of CImg::_cubic_atXYZ (CImg.h:13429-13438) for an already clamped
+// coordinate: taps x-1, x, x+1 (only when the fraction is non-zero), x+2,
+// clamped to the image.
+struct Stencil {
+    int xo[4], yo[4], zo[4];  // element offsets per axis
+    float wx[4], wy[4], wz[4];
+    float dx, dy, dz;
+    long long c0;            // linear index of the integer corner (ix,iy,iz)
+    int sx1, sy1, sz1;       // offsets to the +1 corner (for the 8-corner min/max)
+};
+
+__device__ __forceinline__ void axis_taps(float g, int dim, int stride, int o[4], float &d, int &ix) {
+    int x = (int)g;
+    d = g - (float)x;
+    const int p = x - 1 < 0 ? 0 : x - 1;
+    const int n = d > 0.0f ? x + 1 : x;
+    const int a = x + 2 >= dim ? dim - 1 : x + 2;
+    o[0] = p * stride;
+    o[1] = x * stride;
+    o[2] = n * stride;
+    o[3] = a * stride;
+    ix = x;
+}
+
+__device__ __forceinline__ void make_stencil(const Dim3i d, const float gq[3], Stencil &s) {
+    int ix, iy, iz;
+    axis_taps(gq[0], d.x, 1, s.xo, s.dx, ix);
+    axis_taps(gq[1], d.y, d.x, s.yo, s.dy, iy);
+    axis_taps(gq[2], d.z, d.x * d.y, s.zo, s.dz, iz);
+    cr_weights(s.dx, s.wx);
+    cr_weights(s.dy, s.wy);
+    cr_weights(s.dz, s.wz);
+    s.c0 = ix + (long long)iy * d.x + (long long)iz * d.x * d.y;
+    s.sx1 = 1;
+    s.sy1 = d.x;
+    s.sz1 = d.x * d.y;
+}
+
+// sample_image (warping.h:49-88): Catmull-Rom value clamped to the min/max of
+// the 8 corners of the cell.
+__device__ __forceinline__ float sample_clamped(const float *__restrict__ img, const Stencil &s) {
+    float val = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float yv = 0.0f;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const float *row = img + s.yo[b] + s.zo[c];
+            float xv = s.wx[0] * __ldg(row + s.xo[0]) + s.wx[1] * __ldg(row + s.xo[1]) +
+                       s.wx[2] * __ldg(row + s.xo[2]) + s.wx[3] * __ldg(row + s.xo[3]);
+            yv += s.wy[b] * xv;
+        }
+        val += s.wz[c] * yv;
+    }
+    const float *c0 = img + s.c0;
+    float mn = __ldg(c0), mx = mn;
+    const int off[7] = {s.sx1, s.sx1 + s.sy1, s.sy1, s.sz1, s.sx1 + s.sz1, s.sx1 + s.sy1 + s.sz1,
+                        s.sy1 + s.sz1};
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        float v = __ldg(c0 + off[k]);
+        mn = (v < mn) ? v : mn;
+        mx = (mx < v) ? v : mx;
+    }
+    float inner = (val < mx) ? val : mx;
+    return (mn < inner) ? inner : mn;
+}
+
+__device__ __forceinline__ void trace(const Dim3i d, const float *__restrict__ vel, size_t n, int i,
+                                      int j, int k, float h, float q[3], float p2[3], float v1[3],
+                                      float v2[3]) {
+    // cell centre (warping.h:25-29) and the velocity there (an exact node read)
+    const float p[3] = {(float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f};
+    const int ci = min(max(i, 1), d.x - 2), cj = min(max(j, 1), d.y - 2), ck = min(max(k, 1), d.z - 2);
+    const size_t c = ci + (size_t)cj * d.x + (size_t)ck * d.x * d.y;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) v1[a] = __ldg(vel + a * n + c);
+    // trace (warping.h:100-114): p2 = p + h v(p); p0 = p2 - h v(p2); q = p2 + (p - p0)/2
+#pragma unroll
+    for (int a = 0; a < 3; ++a) p2[a] = __fadd_rn(p[a], __fmul_rn(h, v1[a]));
+    float g2[3] = {to_grid(p2[0], d.x, nullptr), to_grid(p2[1], d.y, nullptr), to_grid(p2[2], d.z, nullptr)};
+    Stencil s2;
+    make_stencil(d, g2, s2);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) v2[a] = sample_clamped(vel + a * n, s2);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float p0 = __fsub_rn(p2[a], __fmul_rn(h, v2[a]));
+        q[a] = __fadd_rn(p2[a], __fmul_rn(0.5f, __fsub_rn(p[a], p0)));
+    }
+}
+
+__global__ void __launch_bounds__(128) k_warp(const Dim3i d, const float *__restrict__ vel,
+                                              const float *__restrict__ src, int nc, float dt,
+                                              float *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= d.x) return;
+    const size_t n = (size_t)d.x * d.y * d.z;
+    float q[3], p2[3], v1[3], v2[3];
+    trace(d, vel, n, i, j, k, -dt, q, p2, v1, v2);
+    float gq[3] = {to_grid(q[0], d.x, nullptr), to_grid(q[1], d.y, nullptr), to_grid(q[2], d.z, nullptr)};
+    Stencil s;
+    make_stencil(d, gq, s);
+    const size_t o = i + (size_t)j * d.x + (size_t)k * d.x * d.y;
+    for (int c = 0; c < nc; ++c) out[o + c * n] = sample_clamped(src + c * n, s);
+}
+
+// ---- VJP ---------------------------------------------------------------
+// For one clamped sample: which branch the clamp took and, when unclamped,
+// the spatial gradient of the Catmull-Rom value (zero along an axis whose
+// grid coordinate was clamped to [1, dim-2]).
+struct SampleD {
+    float value;
+    int branch;        // 0 interior, 1 clamped to max corner, 2 clamped to min corner
+    long long corner;  // arg-max / arg-min corner index when branch != 0
+    float grad[3];
+};
+
+__device__ __forceinline__ void cr_dweights(float d, float w[4]) {
+    float d2 = d * d;
+    w[0] = 0.5f * (-1.0f + 4.0f * d - 3.0f * d2);
+    w[1] = 0.5f * (-10.0f * d + 9.0f * d2);
+    w[2] = 0.5f * (1.0f + 8.0f * d - 9.0f * d2);
+    w[3] = 0.5f * (-2.0f * d + 3.0f * d2);
+}
+
+__device__ __forceinline__ void sample_d(const float *__restrict__ img, const Stencil &s,
+                                         const bool clamped[3], SampleD &r) {
+    float dwx[4], dwy[4], dwz[4];
+    cr_dweights(s.dx, dwx);
+    cr_dweights(s.dy, dwy);
+    cr_dweights(s.dz, dwz);
+    float val = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const float *row = img + s.yo[b] + s.zo[c];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                float v = __ldg(row + s.xo[a]);
+                val += s.wx[a] * s.wy[b] * s.wz[c] * v;
+                gx += dwx[a] * s.wy[b] * s.wz[c] * v;
+                gy += s.wx[a] * dwy[b] * s.wz[c] * v;
+                gz += s.wx[a] * s.wy[b] * dwz[c] * v;
+            }
+        }
+    long long imn = s.c0, imx = s.c0;
+    float mn = __ldg(img + s.c0), mx = mn;
+    const int off[7] = {s.sx1, s.sx1 + s.sy1, s.sy1, s.sz1, s.sx1 + s.sz1, s.sx1 + s.sy1 + s.sz1,
+                        s.sy1 + s.sz1};
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        float v = __ldg(img + s.c0 + off[k]);
+        if (v < mn) { mn = v; imn = s.c0 + off[k]; }
+        if (mx < v) { mx = v; imx = s.c0 + off[k]; }
+    }
+    r.grad[0] = r.grad[1] = r.grad[2] = 0.0f;
+    if (val > mx) {
+        r.value = mx; r.branch = 1; r.corner = imx;
+    } else if (val < mn) {
+        r.value = mn; r.branch = 2; r.corner = imn;
+    } else {
+        r.value = val; r.branch = 0; r.corner = -1;
+        r.grad[0] = clamped[0] ? 0.0f : gx;
+        r.grad[1] = clamped[1] ? 0.0f : gy;
+        r.grad[2] = clamped[2] ? 0.0f : gz;
+    }
+}
+
+__device__ __forceinline__ void scatter_sample(float *__restrict__ bar, const Stencil &s,
+                                               const SampleD &r, float g) {
+    if (g == 0.0f) return;
+    if (r.branch != 0) {
+        atomicAdd(bar + r.corner, g);
+        return;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            float wbc = g * s.wy[b] * s.wz[c];
+            float *row = bar + s.yo[b] + s.zo[c];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                float w = s.wx[a] * wbc;
+                if (w != 0.0f) atomicAdd(row + s.xo[a], w);
+            }
+        }
+}
+
+// q = p + (h/2) v(p) + (h/2) v(p2), p2 = p + h v(p).  Reverse mode:
+//   out_c = S(src_c, q)        -> src_bar, q_bar
+//   q_bar -> v2_bar = (h/2) q_bar;  p2_bar = q_bar/2 + J_v(p2)^T v2_bar
+//   v1_bar = (h/2) q_bar' ... folded: v1_bar = h * p2_bar (p2 = p + h v1)
+// The centre read v(p) is an exact node value, so its adjoint is a single add.
+__global__ void __launch_bounds__(128) k_warp_vjp(const Dim3i d, const float *__restrict__ vel,
+                                                  const float *__restrict__ src, int nc, float dt,
+                                                  const float *__restrict__ out_bar,
+                                                  float *__restrict__ src_bar,
+                                                  float *__restrict__ vel_bar) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= d.x) return;
+    const size_t n = (size_t)d.x * d.y * d.z;
+    const float h = -dt;
+    float q[3], p2[3], v1[3], v2[3];
+    trace(d, vel, n, i, j, k, h, q, p2, v1, v2);
+    bool cq[3];
+    float gq[3] = {to_grid(q[0], d.x, &cq[0]), to_grid(q[1], d.y, &cq[1]), to_grid(q[2], d.z, &cq[2])};
+    Stencil sq;
+    make_stencil(d, gq, sq);
+    const size_t o = i + (size_t)j * d.x + (size_t)k * d.x * d.y;
+    float qbar[3] = {0.0f, 0.0f, 0.0f};
+    for (int c = 0; c < nc; ++c) {
+        const float ob = __ldg(out_bar + o + c * n);
+        if (ob == 0.0f) continue;
+        SampleD r;
+        sample_d(src + c * n, sq, cq, r);
+        if (src_bar) scatter_sample(src_bar + c * n, sq, r, ob);
+        qbar[0] += ob * r.grad[0];
+        qbar[1] += ob * r.grad[1];
+        qbar[2] += ob * r.grad[2];
+    }
+    if (!vel_bar) return;
+    if (qbar[0] == 0.0f && qbar[1] == 0.0f && qbar[2] == 0.0f) return;
+    bool c2[3];
+    float g2[3] = {to_grid(p2[0], d.x, &c2[0]), to_grid(p2[1], d.y, &c2[1]), to_grid(p2[2], d.z, &c2[2])};
+    Stencil s2;
+    make_stencil(d, g2, s2);
+    float v2bar[3], p2bar[3] = {0.5f * qbar[0], 0.5f * qbar[1], 0.5f * qbar[2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) v2bar[a] = 0.5f * h * qbar[a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        SampleD r;
+        sample_d(vel + a * n, s2, c2, r);
+        scatter_sample(vel_bar + a * n, s2, r, v2bar[a]);
+        p2bar[0] += v2bar[a] * r.grad[0];
+        p2bar[1] += v2bar[a] * r.grad[1];
+        p2bar[2] += v2bar[a] * r.grad[2];
+    }
+    const int ci = min(max(i, 1), d.x - 2), cj = min(max(j, 1), d.y - 2), ck = min(max(k, 1), d.z - 2);
+    const size_t cc = ci + (size_t)cj * d.x + (size_t)ck * d.x * d.y;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float g = h * p2bar[a];
+        if (g != 0.0f) atomicAdd(vel_bar + a * n + cc, g);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
+                        float *out, cudaStream_t s) {
+    Dim3i d{dim[0], dim[1], dim[2]};
+    k_warp<<<dim3((d.x + 127) / 128, d.y, d.z), 128, 0, s>>>(d, vel, src, nc, dt, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_warp_vjp(const int *dim, const float *vel, const float *src, int nc, float dt,
+                            const float *out_bar, float *src_bar, float *vel_bar, cudaStream_t s) {
+    Dim3i d{dim[0], dim[1], dim[2]};
+    k_warp_vjp<<<dim3((d.x + 127) / 128, d.y, d.z), 128, 0, s>>>(d, vel, src, nc, dt, out_bar,
+                                                                  src_bar, vel_bar);
+    return cudaGetLastError();
+}
+
+}  // namespace stt

@@ -1,0 +1,468 @@
+// stt_capi.cu -- the C ABI of libstt.so (declared in include/stt.h): context,
+// FP64 view geometry, argument checking and kernel dispatch.
+//
+// Reference paths are relative to gmzang/SpaceTimeTomography (S/ = SpaceTimeTomography/).
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "stt.h"
+#include "stt_internal.cuh"
+#include "stt_kernels.h"
+
+struct stt_ctx {
+    int device = 0;
+    std::string err;
+    bool has_geom = false;
+    stt::GeomDev g{};
+    double sp[3] = {1, 1, 1};
+    std::vector<stt::ViewRec> views_h;
+    stt::ViewRec *views_d = nullptr;
+    size_t views_cap = 0;
+    float2 *acc = nullptr;  // ray-BP accumulators (contrib, weight) per voxel
+    size_t acc_n = 0;
+    float *corr = nullptr;  // W*H correction image used by stt_sart_sweep
+    size_t corr_n = 0;
+};
+
+namespace {
+
+thread_local std::string g_thread_err;
+
+stt_status fail(stt_ctx *ctx, stt_status st, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    else g_thread_err = msg;
+    return st;
+}
+
+stt_status cuda_fail(stt_ctx *ctx, cudaError_t e, const char *where) {
+    return fail(ctx, STT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define STT_CUDA(ctx, call, where)                          \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+    } while (0)
+
+cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+long long nvox(const stt_ctx *c) { return (long long)c->g.nx * c->g.ny * c->g.nz; }
+
+stt_status need_geom(stt_ctx *ctx) {
+    if (!ctx) return fail(nullptr, STT_ERR_INVALID, "null context");
+    if (!ctx->has_geom) return fail(ctx, STT_ERR_STATE, "no geometry set (call stt_set_geometry)");
+    return STT_OK;
+}
+
+stt_status set_device(stt_ctx *ctx) {
+    STT_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    return STT_OK;
+}
+
+// Per-view FP64 geometry.  Camera = T(-ox, -oz, oy - sid) * R_y(theta) applied
+// to model coordinates centred at (dims-1)*spacing/2 (Scene::_calculateMatrix
+// Scene.cpp:187-188, TypicalRayProducer::_calculateMatrix
+// TypicalRayProducer.cpp:146-147, ST_Tomography ctor :244-246).  Detector
+// pixel (i,j) lies on the near plane z = -sdd at ((i-(W-1)/2)ds, (j-(H-1)/2)ds)
+// (ViewToPixels and the frustum of Scene.cpp:194-206, TypicalRayProducer.cpp:174-194).
+void build_view(const stt_geometry &g, double theta, stt::ViewRec &v) {
+    const double c = std::cos(theta), s = std::sin(theta);
+    const double R[3][3] = {{c, 0, s}, {0, 1, 0}, {-s, 0, c}};
+    const double t[3] = {-g.off[0], -g.off[2], -g.sid + g.off[1]};
+    const double sp[3] = {g.sx, g.sy, g.sz};
+    const int dims[3] = {g.nx, g.ny, g.nz};
+    double ctr[3];
+    for (int k = 0; k < 3; ++k) ctr[k] = (dims[k] - 1) * sp[k] * 0.5;
+    auto to_model = [&](const double cam[3], double out[3]) {
+        const double d[3] = {cam[0] - t[0], cam[1] - t[1], cam[2] - t[2]};
+        for (int r = 0; r < 3; ++r) out[r] = ctr[r] + R[0][r] * d[0] + R[1][r] * d[1] + R[2][r] * d[2];
+    };
+    const double zero[3] = {0, 0, 0};
+    to_model(zero, v.src);
+    const double p0[3] = {-(g.W - 1) * 0.5 * g.ds, -(g.H - 1) * 0.5 * g.ds, -g.sdd};
+    to_model(p0, v.det0);
+    for (int r = 0; r < 3; ++r) {
+        v.du[r] = R[0][r] * g.ds;
+        v.dv[r] = R[1][r] * g.ds;
+    }
+    // voxel (x,y,z) -> camera: R * (diag(sp) * x - ctr) + t
+    for (int r = 0; r < 3; ++r) {
+        double b = t[r];
+        for (int q = 0; q < 3; ++q) {
+            v.A[r * 3 + q] = (float)(R[r][q] * sp[q]);
+            b -= R[r][q] * ctr[q];
+        }
+        v.b[r] = (float)b;
+    }
+    for (int k = 0; k < 4; ++k) v.pad[k] = 0.0f;
+}
+
+template <typename T>
+stt_status ensure(stt_ctx *ctx, T *&ptr, size_t &cap, size_t n, const char *what) {
+    if (cap >= n && ptr) return STT_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc((void **)&ptr, n * sizeof(T));
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return fail(ctx, STT_ERR_NOMEM, std::string("cudaMalloc(") + what + "): " + cudaGetErrorString(e));
+    }
+    cap = n;
+    return STT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *stt_version(void) { return "stt 0.1.0 sm_100a"; }
+
+stt_status stt_create(stt_ctx **out, int device) {
+    if (!out) return fail(nullptr, STT_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceCount");
+    if (device < 0 || device >= n) return fail(nullptr, STT_ERR_INVALID, "device ordinal out of range");
+    stt_ctx *ctx = new stt_ctx();
+    ctx->device = device;
+    *out = ctx;
+    return STT_OK;
+}
+
+stt_status stt_destroy(stt_ctx *ctx) {
+    if (!ctx) return STT_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->views_d) cudaFree(ctx->views_d);
+    if (ctx->acc) cudaFree(ctx->acc);
+    if (ctx->corr) cudaFree(ctx->corr);
+    delete ctx;
+    return STT_OK;
+}
+
+const char *stt_last_error(const stt_ctx *ctx) {
+    return ctx ? ctx->err.c_str() : g_thread_err.c_str();
+}
+
+stt_status stt_views_from_rounds(int rounds, const double *start_deg, int views_per_round,
+                                 double step_deg, double *angles_out) {
+    if (rounds < 0 || views_per_round < 0 || (rounds > 0 && (!start_deg || !angles_out)))
+        return fail(nullptr, STT_ERR_INVALID, "bad arguments to stt_views_from_rounds");
+    // InitViews / RotateVolume (ST_Tomography.cpp:887-934): start angle read as
+    // float, pi = 3.1415926, each following view 36 degrees further.
+    const double step = step_deg * 3.1415926 / 180;
+    for (int r = 0; r < rounds; ++r) {
+        const double a0 = (double)(float)start_deg[r] * 3.1415926 / 180;
+        for (int k = 0; k < views_per_round; ++k) angles_out[r * views_per_round + k] = a0 + k * step;
+    }
+    return STT_OK;
+}
+
+stt_status stt_lds_angles(int n, int Ns, int p, int Nz, double *out) {
+    if (n < 0 || Ns <= 0 || p < 2 || Nz <= 0 || (n > 0 && !out))
+        return fail(nullptr, STT_ERR_INVALID, "bad arguments to stt_lds_angles");
+    // Low_discrepency_squence.m:38-67: van der Corput radical inverse of i in
+    // base p, scaled to one segment of 360/Ns degrees, repeated over the Ns
+    // segments; an extra 0 every Nz entries.
+    int len = 0;
+    long long i = 0;
+    while (len < n) {
+        if (len > 0 && len % Nz == 0) out[len++] = 0.0;
+        if (len >= n) break;
+        long long b = i++;
+        double r = 0.0, q = 1.0 / p;
+        while (b != 0) {
+            r += (double)(b % p) * q;
+            q /= p;
+            b /= p;
+        }
+        r = 360.0 * r / Ns;
+        for (int k = 0; len < n && k < Ns; ++k) out[len++] = r + k * 360.0 / Ns;
+    }
+    return STT_OK;
+}
+
+stt_status stt_permutation(unsigned long long seed, int n, int *perm) {
+    if (n < 0 || (n > 0 && !perm)) return fail(nullptr, STT_ERR_INVALID, "bad arguments to stt_permutation");
+    // SplitMix64 (Steele, Lea, Flood 2014) driving a Fisher-Yates shuffle.
+    uint64_t s = seed;
+    auto next = [&s]() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    for (int i = n - 1; i > 0; --i) {
+        int j = (int)(next() % (uint64_t)(i + 1));
+        int tmp = perm[i];
+        perm[i] = perm[j];
+        perm[j] = tmp;
+    }
+    return STT_OK;
+}
+
+stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g) {
+    if (!ctx || !g) return fail(ctx, STT_ERR_INVALID, "null argument");
+    if (g->nx < 2 || g->ny < 2 || g->nz < 2) return fail(ctx, STT_ERR_INVALID, "volume dims must be >= 2");
+    if (g->W < 5 || g->H < 5) return fail(ctx, STT_ERR_INVALID, "detector must be at least 5x5");
+    if (!(g->sx > 0 && g->sy > 0 && g->sz > 0 && g->ds > 0))
+        return fail(ctx, STT_ERR_INVALID, "spacings must be positive");
+    if (!(g->sdd > 0 && g->sid > 0 && std::isfinite(g->sid) && std::isfinite(g->sdd)))
+        return fail(ctx, STT_ERR_INVALID, "sid and sdd must be positive and finite");
+    if ((long long)g->nx * g->ny * g->nz > (1LL << 34))
+        return fail(ctx, STT_ERR_INVALID, "volume too large");
+    if (g->n_views < 0 || (g->n_views > 0 && !g->angles_rad))
+        return fail(ctx, STT_ERR_INVALID, "n_views > 0 needs angles_rad");
+    // The source must lie outside the volume so that every voxel projects in
+    // front of it (cam.z < 0 in the voxel-driven backprojector).
+    const double hx = (g->nx - 1) * g->sx * 0.5, hy = (g->ny - 1) * g->sy * 0.5, hz = (g->nz - 1) * g->sz * 0.5;
+    const double off = std::sqrt(g->off[0] * g->off[0] + g->off[1] * g->off[1] + g->off[2] * g->off[2]);
+    if (g->sid <= std::sqrt(hx * hx + hy * hy + hz * hz) + off)
+        return fail(ctx, STT_ERR_INVALID, "sid must exceed the volume half-diagonal plus the offset");
+    stt_status st = set_device(ctx);
+    if (st) return st;
+    ctx->views_h.resize(g->n_views);
+    for (int v = 0; v < g->n_views; ++v) build_view(*g, g->angles_rad[v], ctx->views_h[v]);
+    if (g->n_views > 0) {
+        st = ensure(ctx, ctx->views_d, ctx->views_cap, (size_t)g->n_views, "view table");
+        if (st) return st;
+        STT_CUDA(ctx, cudaMemcpy(ctx->views_d, ctx->views_h.data(), sizeof(stt::ViewRec) * g->n_views,
+                                 cudaMemcpyHostToDevice),
+                 "cudaMemcpy(view table)");
+    }
+    stt::GeomDev &d = ctx->g;
+    d.nx = g->nx;
+    d.ny = g->ny;
+    d.nz = g->nz;
+    d.W = g->W;
+    d.H = g->H;
+    d.n_views = g->n_views;
+    d.inv_sp[0] = 1.0 / g->sx;
+    d.inv_sp[1] = 1.0 / g->sy;
+    d.inv_sp[2] = 1.0 / g->sz;
+    // ST_Tomography.cpp:300: sqrt of the float spacings, stored as float
+    const float fx = (float)g->sx, fy = (float)g->sy, fz = (float)g->sz;
+    d.sd = std::sqrt(fx * fx + fy * fy + fz * fz);
+    d.cx = (float)((g->W - 1) * 0.5);
+    d.cy = (float)((g->H - 1) * 0.5);
+    d.sdd_ds = (float)(g->sdd / g->ds);
+    ctx->sp[0] = g->sx;
+    ctx->sp[1] = g->sy;
+    ctx->sp[2] = g->sz;
+    ctx->has_geom = true;
+    return STT_OK;
+}
+
+static stt_status check_views(stt_ctx *ctx, int view0, int nviews) {
+    if (view0 < 0 || nviews < 0 || view0 + nviews > ctx->g.n_views)
+        return fail(ctx, STT_ERR_INVALID, "view range outside the geometry's view list");
+    return STT_OK;
+}
+
+stt_status stt_fp(stt_ctx *ctx, const float *vol, float *proj, float *raylen, float *weight,
+                  int view0, int nviews, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!vol || !proj) return fail(ctx, STT_ERR_INVALID, "null vol or proj");
+    if ((st = check_views(ctx, view0, nviews))) return st;
+    if (nviews == 0) return STT_OK;
+    if ((st = set_device(ctx))) return st;
+    STT_CUDA(ctx, stt::launch_fp(ctx->g, ctx->views_d, vol, view0, nviews, proj, raylen, weight, S(stream)),
+             "k_fp launch");
+    return STT_OK;
+}
+
+stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, float *raylen_state,
+                             float *corr, int view, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!vol || !b || !corr) return fail(ctx, STT_ERR_INVALID, "null vol, b or corr");
+    if ((st = check_views(ctx, view, 1))) return st;
+    if ((st = set_device(ctx))) return st;
+    STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, view, b, raylen_state, corr, S(stream)),
+             "k_fp_corr launch");
+    return STT_OK;
+}
+
+stt_status stt_fp_vjp(stt_ctx *ctx, const float *proj_bar, float *vol_bar, int view0, int nviews,
+                      void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!proj_bar || !vol_bar) return fail(ctx, STT_ERR_INVALID, "null proj_bar or vol_bar");
+    if ((st = check_views(ctx, view0, nviews))) return st;
+    if (nviews == 0) return STT_OK;
+    if ((st = set_device(ctx))) return st;
+    STT_CUDA(ctx, stt::launch_fp_adjoint(ctx->g, ctx->views_d, view0, nviews, proj_bar, vol_bar, S(stream)),
+             "k_fp_adjoint launch");
+    return STT_OK;
+}
+
+stt_status stt_bp_voxel(stt_ctx *ctx, const float *corr, float *vol, double alpha, float gmax,
+                        int view, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!corr || !vol) return fail(ctx, STT_ERR_INVALID, "null corr or vol");
+    if ((st = check_views(ctx, view, 1))) return st;
+    if ((st = set_device(ctx))) return st;
+    STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, view, corr, vol, (float)alpha, gmax, S(stream)),
+             "k_bp_voxel launch");
+    return STT_OK;
+}
+
+static stt_status ensure_acc(stt_ctx *ctx, cudaStream_t s) {
+    const size_t n = (size_t)nvox(ctx);
+    if (ctx->acc && ctx->acc_n >= n) return STT_OK;
+    stt_status st = ensure(ctx, ctx->acc, ctx->acc_n, n, "ray-BP accumulators");
+    if (st) return st;
+    STT_CUDA(ctx, cudaMemsetAsync(ctx->acc, 0, n * sizeof(float2), s), "cudaMemsetAsync(accumulators)");
+    return STT_OK;
+}
+
+stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, int view, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!corr || !vol) return fail(ctx, STT_ERR_INVALID, "null corr or vol");
+    if ((st = check_views(ctx, view, 1))) return st;
+    if ((st = set_device(ctx))) return st;
+    if ((st = ensure_acc(ctx, S(stream)))) return st;
+    STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, view, corr, ctx->acc, vol, gmax, S(stream)),
+             "k_bp_ray launch");
+    return STT_OK;
+}
+
+stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, const int *perm,
+                          int nperm, int view_offset, double alpha, float gmax, int bp_mode,
+                          float *raylen_state, const int *roi_cut, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!vol || !proj_stack || (nperm > 0 && !perm)) return fail(ctx, STT_ERR_INVALID, "null argument");
+    if (bp_mode != 0 && bp_mode != 1) return fail(ctx, STT_ERR_INVALID, "bp_mode must be 0 or 1");
+    if (bp_mode == 0 && !raylen_state)
+        return fail(ctx, STT_ERR_INVALID, "voxel-based SART needs the sticky ray-length state");
+    for (int i = 0; i < nperm; ++i)
+        if (perm[i] < 0 || view_offset + perm[i] >= ctx->g.n_views || view_offset + perm[i] < 0)
+            return fail(ctx, STT_ERR_INVALID, "perm entry outside the view list");
+    if ((st = set_device(ctx))) return st;
+    cudaStream_t s = S(stream);
+    const size_t npix = (size_t)ctx->g.W * ctx->g.H;
+    if ((st = ensure(ctx, ctx->corr, ctx->corr_n, npix, "correction image"))) return st;
+    if (bp_mode == 1 && (st = ensure_acc(ctx, s))) return st;
+    for (int i = 0; i < nperm; ++i) {
+        const int v = view_offset + perm[i];
+        const float *b = proj_stack + (size_t)perm[i] * npix;
+        // ray-based mode: TypicalRayProducer::Initial zeroes the ray lengths
+        // after every view, so missed rays see L = 0 (no sticky state)
+        STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, v, b, bp_mode == 0 ? raylen_state : nullptr,
+                                          ctx->corr, s),
+                 "k_fp_corr launch");
+        if (bp_mode == 0)
+            STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, v, ctx->corr, vol, (float)alpha, gmax, s),
+                     "k_bp_voxel launch");
+        else
+            STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, v, ctx->corr, ctx->acc, vol, gmax, s),
+                     "k_bp_ray launch");
+    }
+    if (bp_mode == 1 && raylen_state)
+        STT_CUDA(ctx, cudaMemsetAsync(raylen_state, 0, npix * sizeof(float), s), "cudaMemsetAsync(raylen)");
+    if (roi_cut) {
+        const int d[3] = {ctx->g.nx, ctx->g.ny, ctx->g.nz};
+        STT_CUDA(ctx, stt::launch_roi_apply(d, roi_cut, nullptr, vol, nullptr, nullptr, s), "k_roi_apply launch");
+    }
+    return STT_OK;
+}
+
+static stt::PdParams to_pd(const stt_pd_params *p) {
+    stt::PdParams q;
+    q.sigma = p->sigma;
+    q.tau = p->tau;
+    q.tv_w = p->tv_w;
+    q.tp_w = p->tp_w;
+    q.bc_w = p->bc_w;
+    q.hf = p->huber_factor;
+    q.gmax = p->gmax;
+    for (int i = 0; i < 8; ++i) q.cut[i] = p->cut[i];
+    return q;
+}
+
+stt_status stt_pd_dual(stt_ctx *ctx, const stt_pd_params *p, const float *xbar_f, const float *xbar_f1,
+                       const float *bw, float *ytv, float *ytp, float *ybc, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!p || !xbar_f || !xbar_f1 || !bw || !ytv || !ytp || !ybc) return fail(ctx, STT_ERR_INVALID, "null argument");
+    if ((st = set_device(ctx))) return st;
+    const int d[3] = {ctx->g.nx, ctx->g.ny, ctx->g.nz};
+    STT_CUDA(ctx, stt::launch_pd_dual(d, to_pd(p), xbar_f, xbar_f1, bw, ytv, ytp, ybc, S(stream)), "k_pd_dual launch");
+    return STT_OK;
+}
+
+stt_status stt_pd_primal(stt_ctx *ctx, const stt_pd_params *p, int first_frame, const float *ytp_prev,
+                         const float *ytp, const float *fw, const float *ybc, const float *ytv, float *vol,
+                         float *xprev, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!p || !ytp || !ybc || !ytv || !vol || !xprev) return fail(ctx, STT_ERR_INVALID, "null argument");
+    if (!first_frame && (!ytp_prev || !fw)) return fail(ctx, STT_ERR_INVALID, "ytp_prev and fw needed after frame 0");
+    if ((st = set_device(ctx))) return st;
+    const int d[3] = {ctx->g.nx, ctx->g.ny, ctx->g.nz};
+    STT_CUDA(ctx, stt::launch_pd_primal(d, to_pd(p), first_frame ? 1 : 0, ytp_prev, ytp, fw, ybc, ytv, vol, xprev,
+                                        S(stream)),
+             "k_pd_primal launch");
+    return STT_OK;
+}
+
+stt_status stt_pd_extrapolate(stt_ctx *ctx, const int *cut, const float *vol, const float *xprev, float *xbar,
+                              void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!cut || !vol || !xprev || !xbar) return fail(ctx, STT_ERR_INVALID, "null argument");
+    if ((st = set_device(ctx))) return st;
+    const int d[3] = {ctx->g.nx, ctx->g.ny, ctx->g.nz};
+    STT_CUDA(ctx, stt::launch_pd_extrapolate(d, cut, vol, xprev, xbar, S(stream)), "k_pd_extrapolate launch");
+    return STT_OK;
+}
+
+stt_status stt_roi_mask(stt_ctx *ctx, const int *cut, float *roi, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!cut || !roi) return fail(ctx, STT_ERR_INVALID, "null argument");
+    if ((st = set_device(ctx))) return st;
+    const int d[3] = {ctx->g.nx, ctx->g.ny, ctx->g.nz};
+    STT_CUDA(ctx, stt::launch_roi_mask(d, cut, roi, S(stream)), "k_roi_mask launch");
+    return STT_OK;
+}
+
+static stt_status check_warp_args(const int *dim, const float *vel, const float *src, int nc) {
+    if (!dim || !vel || !src) return fail(nullptr, STT_ERR_INVALID, "null argument");
+    if (dim[0] < 4 || dim[1] < 4 || dim[2] < 4)
+        return fail(nullptr, STT_ERR_INVALID, "warp needs every dimension >= 4");
+    if (nc < 1) return fail(nullptr, STT_ERR_INVALID, "nc must be >= 1");
+    if ((long long)dim[0] * dim[1] * dim[2] * (nc > 3 ? nc : 3) >= (1LL << 31))
+        return fail(nullptr, STT_ERR_INVALID, "warp volume too large for 32-bit tap offsets");
+    return STT_OK;
+}
+
+stt_status stt_warp(const int *dim, const float *vel, const float *src, int nc, float dt, float *out,
+                    void *stream) {
+    stt_status st = check_warp_args(dim, vel, src, nc);
+    if (st) return st;
+    if (!out) return fail(nullptr, STT_ERR_INVALID, "null out");
+    STT_CUDA(nullptr, stt::launch_warp(dim, vel, src, nc, dt, out, S(stream)), "k_warp launch");
+    return STT_OK;
+}
+
+stt_status stt_warp_vjp(const int *dim, const float *vel, const float *src, int nc, float dt,
+                        const float *out_bar, float *src_bar, float *vel_bar, void *stream) {
+    stt_status st = check_warp_args(dim, vel, src, nc);
+    if (st) return st;
+    if (!out_bar) return fail(nullptr, STT_ERR_INVALID, "null out_bar");
+    STT_CUDA(nullptr, stt::launch_warp_vjp(dim, vel, src, nc, dt, out_bar, src_bar, vel_bar, S(stream)),
+             "k_warp_vjp launch");
+    return STT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,300 @@
+"""ctypes bindings of the checkers: oracle/liboracle.so (CPU restatement) and,
+when it was built, oracle/_ref/libstt_ref.so (the reference's own code).
+
+Test infrastructure only: the product never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE_SO = ROOT / "oracle" / "liboracle.so"
+REF_SO = ROOT / "oracle" / "_ref" / "libstt_ref.so"
+
+P = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+
+
+class OGeom(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("sx", C.c_double),
+                ("sy", C.c_double), ("sz", C.c_double), ("W", C.c_int), ("H", C.c_int),
+                ("ds", C.c_double), ("sid", C.c_double), ("sdd", C.c_double),
+                ("off", C.c_double * 3)]
+
+
+class OView(C.Structure):
+    _fields_ = [("angle", C.c_double), ("quat", C.c_float * 4)]
+
+
+class OPd(C.Structure):
+    _fields_ = [("sigma", C.c_float), ("tau", C.c_float), ("tv_w", C.c_float), ("tp_w", C.c_float),
+                ("bc_w", C.c_float), ("huber_factor", C.c_float), ("gmax", C.c_float),
+                ("cut", C.c_int * 8)]
+
+
+def _ensure_built():
+    if not ORACLE_SO.exists():
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "all"], check=True)
+
+
+_ensure_built()
+O = C.CDLL(str(ORACLE_SO))
+_vp, _i, _d, _f = C.c_void_p, C.c_int, C.c_double, C.c_float
+O.orc_view_from_round.argtypes = [_d, _i, C.POINTER(OView)]
+O.orc_view_from_angle.argtypes = [_d, C.POINTER(OView)]
+O.orc_fp_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp, _vp, _vp, _i]
+O.orc_fp_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp, _vp, _vp, _i]
+O.orc_bp_ray_scatter_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp, _vp]
+O.orc_fp_adjoint_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp]
+O.orc_bp_voxel_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _f, _f, _vp, _i]
+O.orc_bp_voxel_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _d, _d, _vp, _i]
+O.orc_correction_f32.argtypes = [_i, _vp, _vp, _vp, _vp]
+O.orc_bp_ray_update_f32.argtypes = [C.c_long, _vp, _vp, _f, _vp]
+O.orc_sart_f32.argtypes = [C.POINTER(OGeom), _i, _vp, _vp, _i, _vp, _f, _f, _i, _vp, _vp, _vp, _i]
+O.orc_sart_f64.argtypes = [C.POINTER(OGeom), _vp, _vp, _i, _vp, _d, _d, _i, _vp, _vp, _vp, _i]
+O.orc_roi_mask_f32.argtypes = [_vp, _vp, _vp]
+O.orc_permutation.argtypes = [C.c_ulonglong, _i, _vp]
+O.orc_pd_dual_f32.argtypes = [_vp, C.POINTER(OPd), _vp, _vp, _vp, _vp, _vp, _vp]
+O.orc_pd_primal_f32.argtypes = [_vp, C.POINTER(OPd), _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+O.orc_pd_extrapolate_f32.argtypes = [_vp, _vp, _vp, _vp, _vp]
+O.orc_pd_dual_f64.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+O.orc_pd_primal_f64.argtypes = [_vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+O.orc_pd_extrapolate_f64.argtypes = [_vp, _vp, _vp, _vp, _vp]
+O.orc_warp_f32.argtypes = [_vp, _vp, _vp, _i, _f, _vp, _i]
+O.orc_warp_f64.argtypes = [_vp, _vp, _vp, _i, _d, _vp, _i]
+O.orc_warp_vjp_f64.argtypes = [_vp, _vp, _vp, _i, _d, _vp, _vp, _vp]
+O.orc_cubic_at_f32.argtypes = [_vp, _vp, _f, _f, _f]
+O.orc_cubic_at_f32.restype = _f
+
+REF = None
+if REF_SO.exists():
+    REF = C.CDLL(str(REF_SO))
+    REF.ref_fp_view.argtypes = [_vp, _vp, _i, _i, _d, _d, _d, _vp, _d, _i, _vp, _vp, _vp, _vp, _vp, _i]
+    REF.ref_bp_ray_view.argtypes = [_vp, _vp, _i, _i, _d, _d, _d, _vp, _d, _i, _vp, _vp, _vp, _vp]
+    REF.ref_warp.argtypes = [_vp, _vp, _vp, _i, _f, _vp]
+    REF.ref_cubic_at.argtypes = [_vp, _vp, _i, _vp, _vp, _vp, _vp]
+
+
+class Scan:
+    """One scan geometry, as both checkers and libstt take it."""
+
+    def __init__(self, n, det, sid=600.0, sdd=1000.0, spacing=1.0, ds=1.0, off=(0.0, 0.0, 0.0)):
+        self.dims = tuple(n) if hasattr(n, "__len__") else (n, n, n)
+        self.det = tuple(det) if hasattr(det, "__len__") else (det, det)
+        self.sp = tuple(spacing) if hasattr(spacing, "__len__") else (spacing,) * 3
+        self.ds, self.sid, self.sdd, self.off = ds, sid, sdd, tuple(off)
+
+    def ogeom(self) -> OGeom:
+        nx, ny, nz = self.dims
+        W, H = self.det
+        return OGeom(nx, ny, nz, *map(float, self.sp), W, H, float(self.ds), float(self.sid),
+                     float(self.sdd), (C.c_double * 3)(*self.off))
+
+
+def view_round(start_deg: float, k: int) -> OView:
+    v = OView()
+    O.orc_view_from_round(float(start_deg), int(k), C.byref(v))
+    return v
+
+
+def view_angle(angle: float) -> OView:
+    v = OView()
+    O.orc_view_from_angle(float(angle), C.byref(v))
+    return v
+
+
+def views_array(views):
+    arr = (OView * len(views))()
+    for i, v in enumerate(views):
+        arr[i] = v
+    return arr
+
+
+def fp32(scan: Scan, view: OView, vol: np.ndarray, gmode: int = 0, threads: int = 0):
+    W, H = scan.det
+    img = np.zeros((H, W), np.float32)
+    rl = np.zeros_like(img)
+    wt = np.zeros_like(img)
+    g = scan.ogeom()
+    O.orc_fp_f32(C.byref(g), gmode, C.byref(view), P(np.ascontiguousarray(vol, np.float32)), P(img),
+                 P(rl), P(wt), threads)
+    return img, rl, wt
+
+
+def fp64(scan: Scan, view: OView, vol: np.ndarray, threads: int = 0):
+    W, H = scan.det
+    img = np.zeros((H, W), np.float64)
+    rl = np.zeros_like(img)
+    wt = np.zeros_like(img)
+    g = scan.ogeom()
+    O.orc_fp_f64(C.byref(g), C.byref(view), P(np.ascontiguousarray(vol, np.float64)), P(img), P(rl),
+                 P(wt), threads)
+    return img, rl, wt
+
+
+def ref_fp(scan: Scan, start_deg: float, k: int, vol: np.ndarray, threads: int = 0):
+    W, H = scan.det
+    img = np.zeros((H, W), np.float32)
+    rl = np.zeros_like(img)
+    wt = np.zeros_like(img)
+    dims = np.array(scan.dims, np.int32)
+    sp = np.array(scan.sp, np.float32)
+    off = np.array(scan.off, np.float64)
+    REF.ref_fp_view(P(dims), P(sp), W, H, scan.ds, scan.sid, scan.sdd, P(off), float(start_deg), int(k),
+                    P(np.ascontiguousarray(vol, np.float32)), P(img), P(rl), P(wt), None, threads)
+    return img, rl, wt
+
+
+def ref_bp_ray(scan: Scan, start_deg: float, k: int, corr: np.ndarray):
+    nx, ny, nz = scan.dims
+    W, H = scan.det
+    c = np.zeros((nz, ny, nx), np.float32)
+    w = np.zeros_like(c)
+    dims = np.array(scan.dims, np.int32)
+    sp = np.array(scan.sp, np.float32)
+    off = np.array(scan.off, np.float64)
+    REF.ref_bp_ray_view(P(dims), P(sp), W, H, scan.ds, scan.sid, scan.sdd, P(off), float(start_deg),
+                        int(k), P(np.ascontiguousarray(corr, np.float32)), P(c), P(w), None)
+    return c, w
+
+
+def bp_ray_scatter32(scan: Scan, view: OView, corr: np.ndarray, gmode: int = 0):
+    nx, ny, nz = scan.dims
+    c = np.zeros((nz, ny, nx), np.float32)
+    w = np.zeros_like(c)
+    g = scan.ogeom()
+    O.orc_bp_ray_scatter_f32(C.byref(g), gmode, C.byref(view), P(np.ascontiguousarray(corr, np.float32)),
+                             P(c), P(w))
+    return c, w
+
+
+def fp_adjoint64(scan: Scan, view: OView, proj_bar: np.ndarray):
+    nx, ny, nz = scan.dims
+    out = np.zeros((nz, ny, nx), np.float64)
+    g = scan.ogeom()
+    O.orc_fp_adjoint_f64(C.byref(g), C.byref(view), P(np.ascontiguousarray(proj_bar, np.float64)), P(out))
+    return out
+
+
+def bp_voxel32(scan, view, corr, alpha, gmax, vol, gmode=0):
+    v = np.array(vol, np.float32, copy=True)
+    g = scan.ogeom()
+    O.orc_bp_voxel_f32(C.byref(g), gmode, C.byref(view), P(np.ascontiguousarray(corr, np.float32)),
+                       float(alpha), float(gmax), P(v), 0)
+    return v
+
+
+def bp_voxel64(scan, view, corr, alpha, gmax, vol):
+    v = np.array(vol, np.float64, copy=True)
+    g = scan.ogeom()
+    O.orc_bp_voxel_f64(C.byref(g), C.byref(view), P(np.ascontiguousarray(corr, np.float64)),
+                       float(alpha), float(gmax), P(v), 0)
+    return v
+
+
+def sart64(scan, views, perm, proj, alpha, gmax, bp_mode, vol, raylen=None, roi=None, threads=0):
+    v = np.array(vol, np.float64, copy=True)
+    W, H = scan.det
+    rl = np.zeros((H, W), np.float64) if raylen is None else raylen
+    g = scan.ogeom()
+    va = views_array(views)
+    pm = np.ascontiguousarray(perm, np.int32)
+    O.orc_sart_f64(C.byref(g), va, P(pm), len(pm), P(np.ascontiguousarray(proj, np.float64)), float(alpha),
+                   float(gmax), int(bp_mode), P(v), P(rl),
+                   None if roi is None else P(np.ascontiguousarray(roi, np.float64)), threads)
+    return v, rl
+
+
+def sart32(scan, views, perm, proj, alpha, gmax, bp_mode, vol, raylen=None, roi=None, gmode=1,
+           threads=0):
+    v = np.array(vol, np.float32, copy=True)
+    W, H = scan.det
+    rl = np.zeros((H, W), np.float32) if raylen is None else raylen
+    g = scan.ogeom()
+    va = views_array(views)
+    pm = np.ascontiguousarray(perm, np.int32)
+    O.orc_sart_f32(C.byref(g), gmode, va, P(pm), len(pm), P(np.ascontiguousarray(proj, np.float32)),
+                   float(alpha), float(gmax), int(bp_mode), P(v), P(rl),
+                   None if roi is None else P(np.ascontiguousarray(roi, np.float32)), threads)
+    return v, rl
+
+
+def roi_mask(dims, cut):
+    nx, ny, nz = dims
+    r = np.zeros((nz, ny, nx), np.float32)
+    O.orc_roi_mask_f32(P(np.array(dims, np.int32)), P(np.array(cut, np.int32)), P(r))
+    return r
+
+
+def permutation(seed, n):
+    out = np.zeros(n, np.int32)
+    O.orc_permutation(C.c_ulonglong(seed), n, P(out))
+    return out
+
+
+def warp32(vel, src, dt, threads=0):
+    nc = 1 if src.ndim == 3 else src.shape[0]
+    nz, ny, nx = src.shape[-3:]
+    out = np.zeros_like(src, dtype=np.float32)
+    O.orc_warp_f32(P(np.array([nx, ny, nz], np.int32)), P(np.ascontiguousarray(vel, np.float32)),
+                   P(np.ascontiguousarray(src, np.float32)), nc, float(dt), P(out), threads)
+    return out
+
+
+def warp64(vel, src, dt, threads=0):
+    nc = 1 if src.ndim == 3 else src.shape[0]
+    nz, ny, nx = src.shape[-3:]
+    out = np.zeros(src.shape, np.float64)
+    O.orc_warp_f64(P(np.array([nx, ny, nz], np.int32)), P(np.ascontiguousarray(vel, np.float64)),
+                   P(np.ascontiguousarray(src, np.float64)), nc, float(dt), P(out), threads)
+    return out
+
+
+def warp_vjp64(vel, src, dt, out_bar):
+    nc = 1 if src.ndim == 3 else src.shape[0]
+    nz, ny, nx = src.shape[-3:]
+    sb = np.zeros(src.shape, np.float64)
+    vb = np.zeros(vel.shape, np.float64)
+    O.orc_warp_vjp_f64(P(np.array([nx, ny, nz], np.int32)), P(np.ascontiguousarray(vel, np.float64)),
+                       P(np.ascontiguousarray(src, np.float64)), nc, float(dt),
+                       P(np.ascontiguousarray(out_bar, np.float64)), P(sb), P(vb))
+    return sb, vb
+
+
+def ref_warp(vel, src, dt):
+    nc = 1 if src.ndim == 3 else src.shape[0]
+    nz, ny, nx = src.shape[-3:]
+    out = np.zeros_like(src, dtype=np.float32)
+    REF.ref_warp(P(np.array([nx, ny, nz], np.int32)), P(np.ascontiguousarray(vel, np.float32)),
+                 P(np.ascontiguousarray(src, np.float32)), nc, float(dt), P(out))
+    return out
+
+
+def pd_dual32(dims, p: OPd, xf, xf1, bw, ytv, ytp, ybc):
+    ytv, ytp, ybc = (np.array(a, np.float32, copy=True) for a in (ytv, ytp, ybc))
+    O.orc_pd_dual_f32(P(np.array(dims, np.int32)), C.byref(p), P(xf), P(xf1), P(bw), P(ytv), P(ytp), P(ybc))
+    return ytv, ytp, ybc
+
+
+def pd_primal32(dims, p: OPd, first, ytp_prev, ytp, fw, ybc, ytv, vol):
+    v = np.array(vol, np.float32, copy=True)
+    xprev = np.zeros_like(v)
+    O.orc_pd_primal_f32(P(np.array(dims, np.int32)), C.byref(p), int(first), P(ytp_prev), P(ytp), P(fw),
+                        P(ybc), P(ytv), P(v), P(xprev))
+    return v, xprev
+
+
+def pd_extrapolate32(dims, cut, vol, xprev, xbar):
+    xb = np.array(xbar, np.float32, copy=True)
+    O.orc_pd_extrapolate_f32(P(np.array(dims, np.int32)), P(np.array(cut, np.int32)), P(vol), P(xprev), P(xb))
+    return xb
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    n = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (n if n > 0 else 1.0))

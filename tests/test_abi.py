@@ -1,0 +1,94 @@
+"""The C ABI: libstt.so loads, exports every entry point of include/stt.h, and
+its host-only helpers and argument checks behave (no GPU needed)."""
+import ctypes as C
+import math
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle_bind as ob
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from spacetimetomography_b200 import build
+
+    build.build_libstt()
+    from spacetimetomography_b200._lib import lib as L
+
+    return L
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        names |= set(re.findall(r"^\s*(?:stt_status|const char \*|void|int)\s*\*?\s*(stt_\w+)\s*\(", text, re.M))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    for must in ("stt_create", "stt_fp", "stt_fp_vjp", "stt_bp_voxel", "stt_bp_ray", "stt_sart_sweep",
+                 "stt_pd_dual", "stt_pd_primal", "stt_warp", "stt_warp_vjp"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, f"libstt.so lacks {missing}"
+
+
+def test_views_from_rounds_matches_reference_composition(lib):
+    from spacetimetomography_b200 import views_from_rounds
+
+    starts = [0.0, 17.3, 200.5]
+    ang = views_from_rounds(starts, 10)
+    assert ang.shape == (30,)
+    for r, s in enumerate(starts):
+        for k in range(10):
+            v = ob.view_round(s, k)
+            # the reference composes float quaternions; the FP64 angle is the exact sum
+            assert abs(ang[r * 10 + k] - v.angle) < 1e-12
+            half = ang[r * 10 + k] / 2
+            assert abs(math.cos(half) - v.quat[3]) < 2e-6 and abs(math.sin(half) - v.quat[1]) < 2e-6
+
+
+def test_permutation_matches_oracle(lib):
+    from spacetimetomography_b200 import permutation
+
+    for seed, n in [(0, 1), (1, 10), (1234, 360), (2**63 + 5, 97)]:
+        p = permutation(seed, n)
+        np.testing.assert_array_equal(p, ob.permutation(seed, n))
+        assert sorted(p.tolist()) == list(range(n))
+
+
+def test_lds_angles_known_values(lib):
+    from spacetimetomography_b200 import lds_angles
+
+    # van der Corput base 2: 0, 1/2, 1/4, 3/4, 1/8 -> scaled to one 36-degree segment
+    a = lds_angles(50, segments=10, base=2)
+    starts = a[::10]
+    np.testing.assert_allclose(starts, [0.0, 18.0, 9.0, 27.0, 4.5])
+    np.testing.assert_allclose(a[:10], np.arange(10) * 36.0)
+    z = lds_angles(25, segments=10, base=2, zero_every=10)
+    # the reference angle is inserted only when the length is a multiple of Nz
+    # at the top of an outer iteration (Low_discrepency_squence.m:44-46)
+    assert z[10] == 0.0 and z[11] == 18.0 and z[21] == 9.0
+
+
+def test_argument_errors_without_gpu(lib):
+    from spacetimetomography_b200._lib import Geometry
+
+    assert lib.stt_fp(None, None, None, None, None, 0, 1, None) != 0
+    assert lib.stt_set_geometry(None, None) != 0
+    assert lib.stt_views_from_rounds(-1, None, 10, 36.0, None) == 1
+    assert lib.stt_warp(None, None, None, 1, 1.0, None, None) == 1
+    msg = lib.stt_last_error(None)
+    assert msg and b"null" in msg
+    assert lib.stt_version().startswith(b"stt ")
+    assert C.sizeof(Geometry) == 112  # LP64 layout of stt_geometry
