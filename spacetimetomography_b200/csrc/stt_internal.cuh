@@ -4,7 +4,9 @@
 // S/ = SpaceTimeTomography/.
 #pragma once
 
+#ifndef cuda_runtime_h
 #include <cuda_runtime.h>
+#endif
 #include <stdint.h>
 
 namespace stt {
@@ -152,9 +154,12 @@ __device__ __forceinline__ long long tap_index(const Taps &t, int k) {
 // 0.5 on an axis it travels down; each segment restarts at
 // ceil((t1-tnear)/sd)*sd + tnear with pos recomputed, then steps t += sd,
 // pos += vu*sd.  The entry sample is visited once before the loop and again
-// as the first sample of the first segment.  `visit(pos)` is called per
-// sample.  Loops are bounded: at most 8 segments and ceil(len/sd)+4 samples
-// per segment (the reference's own bounds are 4 and ceil(len/sd)+1).
+// as the first sample of the first segment.  A split point can lie before
+// tnear (entry coordinate in [0, 0.5) on a descending axis); the reference then
+// restarts at ceil of a negative count and re-walks clamped samples outside the
+// box up to the split's far end, and so does this march.  `visit(pos)` is
+// called per sample.  Loops are bounded by the segment's own extent
+// ((tb - t)/sd + 2 samples), at most 16 segments, and 2^22 samples per ray.
 template <typename Visit>
 __device__ __forceinline__ void march(const GeomDev &g, const Ray &r, Visit &&visit) {
     const float sd = g.sd;
@@ -183,14 +188,18 @@ __device__ __forceinline__ void march(const GeomDev &g, const Ray &r, Visit &&vi
             tdelta[k] = __fdiv_rn((float)b, r.vu[k]);
         }
     }
-    const int cap = (int)ceilf(__fdiv_rn(tfar - tnear, sd)) + 4;
-    for (int seg = 0; seg < 8 && t1 < tfar; ++seg) {
+    constexpr int kMaxSamples = 1 << 22;
+    int budget = kMaxSamples;
+    for (int seg = 0; seg < 16 && t1 < tfar && budget > 0; ++seg) {
         float tb = rmin(rmin(tmax[0], tmax[1]), tmax[2]);
         if (tb > tfar) tb = tfar;
         float t = __fadd_rn(__fmul_rn(ceilf(__fdiv_rn(__fsub_rn(t1, tnear), sd)), sd), tnear);
         float pos[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(r.vz[k], __fmul_rn(r.vu[k], t));
+        // fminf drops a NaN extent; the t < tb test then ends the segment
+        const int cap = (int)fminf(ceilf(__fdiv_rn(tb - t, sd)) + 2.0f, (float)budget);
+        budget -= cap > 0 ? cap : 0;
         for (int n = 0; n < cap && t < tb; ++n) {
             visit(pos);
             t = __fadd_rn(t, sd);

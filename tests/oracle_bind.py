@@ -49,6 +49,7 @@ O.orc_fp_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp, _vp, 
 O.orc_fp_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp, _vp, _vp, _i]
 O.orc_bp_ray_scatter_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp, _vp]
 O.orc_fp_adjoint_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp]
+O.orc_fp_adjoint_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp]
 O.orc_bp_voxel_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _f, _f, _vp, _i]
 O.orc_bp_voxel_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _d, _d, _vp, _i]
 O.orc_correction_f32.argtypes = [_i, _vp, _vp, _vp, _vp]
@@ -176,6 +177,14 @@ def fp_adjoint64(scan: Scan, view: OView, proj_bar: np.ndarray):
     out = np.zeros((nz, ny, nx), np.float64)
     g = scan.ogeom()
     O.orc_fp_adjoint_f64(C.byref(g), C.byref(view), P(np.ascontiguousarray(proj_bar, np.float64)), P(out))
+    return out
+
+
+def fp_adjoint32(scan: Scan, view: OView, proj_bar: np.ndarray, gmode: int = 1):
+    nx, ny, nz = scan.dims
+    out = np.zeros((nz, ny, nx), np.float32)
+    g = scan.ogeom()
+    O.orc_fp_adjoint_f32(C.byref(g), gmode, C.byref(view), P(np.ascontiguousarray(proj_bar, np.float32)), P(out))
     return out
 
 

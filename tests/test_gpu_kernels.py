@@ -32,11 +32,23 @@ def _np(t):
     return t.detach().cpu().numpy()
 
 
-def phantom(dims, seed, n=8, semi=None):
+def phantom(dims, seed, n=8, semi=None, zero_boundary=True):
+    """Ellipsoid phantom; by default its outer voxel shell is zeroed.
+
+    The reference's march restarts before the entry point when the entry
+    coordinate of a descending axis lies in [0, 0.5) (RayCaster.core.h:70-76,
+    137), re-walking clamped boundary samples.  Whether a ray takes that branch
+    can differ between FP32 and FP64 evaluation for rays right at the 0.5
+    threshold; with a zero boundary shell the branch adds nothing, so the FP64
+    comparison is well-posed.  test_fp_nonzero_boundary covers the other case.
+    """
     from spacetimetomography_b200 import phantom as ph
 
     s = semi or (0.06 * min(dims), 0.3 * min(dims))
-    return ph.ellipsoid_phantom(dims, n, seed, semi=s).numpy()
+    v = ph.ellipsoid_phantom(dims, n, seed, semi=s).numpy()
+    if zero_boundary:
+        v[0], v[-1], v[:, 0], v[:, -1], v[:, :, 0], v[:, :, -1] = 0, 0, 0, 0, 0, 0
+    return v
 
 
 SCANS = [
@@ -81,12 +93,36 @@ def test_fp_parity(cuda, si):
         assert ob.rel_l2(proj[v], ref32) < TOL
         assert np.mean(wt[v] == w64) > 0.999
         assert np.mean(wt[v] == w32) > 0.999
-        hit = w64 > 0
-        assert ob.rel_l2(rl[v][hit], rl64[hit]) < 1e-6
+        hit = (w64 > 0) & (wt[v] > 0)
+        # tfar - tnear of two ~600 mm floats: ~1e-4 mm absolute rounding, as in the reference
+        assert np.max(np.abs(rl[v][hit] - rl64[hit])) < 2e-4
         if ob.REF is not None:
             r_img, r_rl, r_w = ob.ref_fp(scan, sd, k, vol)
             np.testing.assert_array_equal(r_img, ref32)
             assert ob.rel_l2(proj[v], r_img) < TOL
+
+
+def test_fp_nonzero_boundary(cuda):
+    """Non-zero boundary voxels: the kernel takes the reference's FP32 branch decisions."""
+    import torch
+
+    stt = _stt()
+    scan = ob.Scan(30, (64, 64), spacing=1.3)
+    vol = phantom(scan.dims, seed=2, zero_boundary=False) + 0.25
+    angles = stt.views_from_rounds([s for s, _ in ROUND_VIEWS], 10)
+    idx = [r * 10 + k for r, (_, k) in enumerate(ROUND_VIEWS)]
+    ctx = make_ctx(scan, angles[idx])
+    proj = torch.zeros((len(idx), 64, 64), device=cuda)
+    wt = torch.zeros_like(proj)
+    ctx.fp(_t(vol, cuda), proj, weight=wt)
+    proj, wt = _np(proj), _np(wt)
+    for v, (sd, k) in enumerate(ROUND_VIEWS):
+        ref32, _, w32 = ob.fp32(scan, ob.view_round(sd, k), vol, gmode=0)
+        d64, _, w64 = ob.fp64(scan, ob.view_round(sd, k), vol)
+        assert ob.rel_l2(proj[v], ref32) < TOL
+        flip = wt[v] != w64
+        assert np.mean(flip) < 2e-3
+        assert ob.rel_l2(proj[v][~flip], d64[~flip]) < TOL
 
 
 def test_fp_axis_aligned_and_odd_detector(cuda):
@@ -126,7 +162,7 @@ def test_fp_correction_sticky_raylength(cuda):
         st_ref = np.where(w64 > 0, rl64, st_ref)
         c_ref = (b[v] - d64) / (st_ref + 1.0)
         assert ob.rel_l2(_np(corr), c_ref) < TOL
-        assert ob.rel_l2(_np(state), st_ref) < 1e-6
+        assert np.max(np.abs(_np(state) - st_ref)) < 2e-4
 
 
 def test_fp_adjoint_dot_product(cuda):
@@ -147,8 +183,13 @@ def test_fp_adjoint_dot_product(cuda):
     lhs = float(np.sum(_np(ax).astype(np.float64) * y))
     rhs = float(np.sum(x.astype(np.float64) * _np(aty)))
     assert abs(lhs - rhs) / abs(lhs) < 1e-5
-    ref = sum(ob.fp_adjoint64(scan, ob.view_angle(a), y[v]) for v, a in enumerate(angles))
-    assert ob.rel_l2(_np(aty), ref) < 1e-5
+    ref64 = sum(ob.fp_adjoint64(scan, ob.view_angle(a), y[v]) for v, a in enumerate(angles))
+    ref32 = sum(ob.fp_adjoint32(scan, ob.view_angle(a), y[v]).astype(np.float64) for v, a in enumerate(angles))
+    # same FP32 march as the kernel: only the atomic summation order differs
+    assert ob.rel_l2(_np(aty), ref32) < 1e-5
+    # against the FP64 march: sample positions differ by float rounding, and
+    # a random y gives each voxel few, sign-mixed contributions
+    assert ob.rel_l2(_np(aty), ref64) < TOL
 
 
 @pytest.mark.parametrize("alpha", [0.3, 1.0])
@@ -214,7 +255,7 @@ def test_sart_sweep(cuda, bp_mode):
     ref, rl = ob.sart64(scan, views, perm, proj, 0.3, gmax, bp_mode, vol0, roi=roi)
     ref, rl = ob.sart64(scan, views, perm[::-1].copy(), proj, 0.3, gmax, bp_mode, ref, raylen=rl, roi=roi)
     assert ob.rel_l2(_np(g), ref) < TOL
-    assert ob.rel_l2(_np(state), rl) < 1e-6
+    assert np.max(np.abs(_np(state) - rl)) < 2e-4
 
 
 def test_pd_steps(cuda):
