@@ -179,6 +179,56 @@ stt_status stt_warp(const int *dim, const float *vel, const float *src, int nc, 
 stt_status stt_warp_vjp(const int *dim, const float *vel, const float *src, int nc, float dt,
                         const float *out_bar, float *src_bar, float *vel_bar, void *stream);
 
+/* ---- space-time primal-dual solver (ST_Tomography::Render, ST_Tomography.cpp:492-607) ----
+ * One call to stt_solver_iterate runs one primal-dual iteration over all
+ * frames: for every frame the backward warp + dual step, the forward warp +
+ * primal step, SART(f) over its views, the ROI mask and the over-relaxation.
+ * Frame f uses views [f*V, (f+1)*V) of the context's geometry and its V
+ * projections at proj + f*V*W*H.  The view order of each SART call is a
+ * seeded permutation (stt_solver_frame_order gives it on the host).
+ * State arrays are caller-owned device memory, nx*ny*nz floats per volume:
+ *   vol   (F+1) volumes, vol[F] the duplicated last frame (VolumeData.cpp:124-126)
+ *   xbar  (F+1)  over-relaxed volumes X_bar (initialise to vol)
+ *   xprev  F     previous primal iterate X_prev
+ *   ytv   F*3    TV dual (planar channels), ytp F, ybc F
+ *   flow  F*3    flow[f]: motion from frame f to f+1 (planar channels)
+ *   proj  F*V*H*W measured projections */
+typedef enum stt_solve_mode {
+    STT_SOLVE_PLAIN = 0,    /* per-view launches from a host loop, sync per view */
+    STT_SOLVE_STREAMS = 1,  /* batched: fused launches, one stream per frame */
+    STT_SOLVE_GRAPH = 2     /* batched, captured once into a CUDA graph and replayed */
+} stt_solve_mode;
+
+typedef struct stt_solve_cfg {
+    int n_frames, views_per_frame;
+    int bp_mode;               /* 0 voxel-based (alpha), 1 ray-based */
+    double alpha;              /* SART step of the voxel-based BP (-a) */
+    stt_pd_params pd;          /* sigma, tau, weights, gmax, PD region cut */
+    int roi_cut[8];            /* cut of the ROI mask applied after each SART call */
+    unsigned long long seed;   /* view-order seed */
+    int mode;                  /* stt_solve_mode */
+} stt_solve_cfg;
+
+typedef struct stt_pd_state {
+    float *vol, *xbar, *xprev, *ytv, *ytp, *ybc;
+    const float *flow, *proj;
+} stt_pd_state;
+
+typedef struct stt_solver stt_solver;
+
+stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_pd_state *state,
+                             stt_solver **out);
+/* Enqueue n_iters iterations on `stream` (the plain mode synchronises it). */
+stt_status stt_solver_iterate(stt_solver *s, int n_iters, void *stream);
+/* Kernel launches per iteration and iterations run so far. */
+stt_status stt_solver_stats(const stt_solver *s, long long *launches_per_iter,
+                            unsigned long long *iterations);
+const char *stt_solver_last_error(const stt_solver *s);
+stt_status stt_solver_destroy(stt_solver *s);
+/* Host copy of the view order frame `frame` uses in iteration `iter` (HOST perm_out). */
+stt_status stt_solver_frame_order(unsigned long long seed, unsigned long long iter, int n_frames,
+                                  int frame, int views, int *perm_out);
+
 #ifdef __cplusplus
 }
 #endif

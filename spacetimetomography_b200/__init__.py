@@ -7,8 +7,13 @@ streams only); every operation is a call into libstt.
 """
 from ._lib import STTError, lib  # noqa: F401  (loads libstt.so or raises)
 from .api import (  # noqa: F401
+    SOLVE_GRAPH,
+    SOLVE_PLAIN,
+    SOLVE_STREAMS,
     Context,
     PdParams,
+    Solver,
+    frame_order,
     lds_angles,
     permutation,
     views_from_rounds,

@@ -38,6 +38,18 @@ class PdParams(C.Structure):
                 ("gmax", C.c_float), ("cut", C.c_int * 8)]
 
 
+class SolveCfg(C.Structure):
+    _fields_ = [("n_frames", C.c_int), ("views_per_frame", C.c_int), ("bp_mode", C.c_int),
+                ("alpha", C.c_double), ("pd", PdParams), ("roi_cut", C.c_int * 8),
+                ("seed", C.c_ulonglong), ("mode", C.c_int)]
+
+
+class PdState(C.Structure):
+    _fields_ = [("vol", C.c_void_p), ("xbar", C.c_void_p), ("xprev", C.c_void_p),
+                ("ytv", C.c_void_p), ("ytp", C.c_void_p), ("ybc", C.c_void_p),
+                ("flow", C.c_void_p), ("proj", C.c_void_p)]
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
@@ -64,6 +76,11 @@ def _load() -> C.CDLL:
         "stt_roi_mask": [vp, vp, vp, vp],
         "stt_warp": [vp, vp, vp, i, f, vp, vp],
         "stt_warp_vjp": [vp, vp, vp, i, f, vp, vp, vp, vp],
+        "stt_solver_create": [vp, C.POINTER(SolveCfg), C.POINTER(PdState), C.POINTER(vp)],
+        "stt_solver_iterate": [vp, i, vp],
+        "stt_solver_stats": [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_ulonglong)],
+        "stt_solver_destroy": [vp],
+        "stt_solver_frame_order": [C.c_ulonglong, C.c_ulonglong, i, i, i, vp],
     }
     for name, argtypes in sigs.items():
         fn = getattr(lib, name)
@@ -71,6 +88,8 @@ def _load() -> C.CDLL:
         fn.restype = C.c_int
     lib.stt_last_error.argtypes = [vp]
     lib.stt_last_error.restype = C.c_char_p
+    lib.stt_solver_last_error.argtypes = [vp]
+    lib.stt_solver_last_error.restype = C.c_char_p
     lib.stt_version.argtypes = []
     lib.stt_version.restype = C.c_char_p
     return lib

@@ -14,7 +14,7 @@ from typing import Sequence
 
 import numpy as np
 
-from ._lib import Geometry, check, lib
+from ._lib import Geometry, PdState, SolveCfg, STTError, check, lib
 from ._lib import PdParams as _PdParams
 
 # ROI cut of the reference (ST_Tomography.cpp:114)
@@ -205,3 +205,58 @@ def warp_vjp(flow, src, dt, out_bar, src_bar=None, flow_bar=None, stream=None):
     check(lib.stt_warp_vjp(dim, _ptr(flow), _ptr(src), nc, float(dt), _ptr(out_bar), _ptr(src_bar),
                            _ptr(flow_bar), _stream(stream)))
     return src_bar, flow_bar
+
+
+SOLVE_PLAIN, SOLVE_STREAMS, SOLVE_GRAPH = 0, 1, 2
+
+
+def frame_order(seed: int, iteration: int, n_frames: int, frame: int, views: int) -> np.ndarray:
+    """View order of SART(frame) in PD iteration `iteration` (matches the device draw)."""
+    out = np.zeros(views, dtype=np.int32)
+    check(lib.stt_solver_frame_order(C.c_ulonglong(seed), C.c_ulonglong(iteration), n_frames, frame,
+                                     views, out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+class Solver:
+    """stt_solver: the space-time primal-dual iteration of ST_Tomography::Render.
+
+    `state` holds torch CUDA tensors: vol (F+1,nz,ny,nx), xbar (F+1,...), xprev
+    (F,...), ytv (F,3,...), ytp (F,...), ybc (F,...), flow (F,3,...), proj (F,V,H,W).
+    """
+
+    def __init__(self, ctx: Context, state: dict, n_frames: int, views_per_frame: int,
+                 pd: PdParams, alpha: float = 0.3, bp_mode: int = 0, roi_cut=REFERENCE_CUT,
+                 seed: int = 0, mode: int = SOLVE_GRAPH):
+        self.ctx = ctx
+        self.state = state  # keeps the tensors alive
+        cfg = SolveCfg(n_frames, views_per_frame, bp_mode, float(alpha), pd.c(),
+                       (C.c_int * 8)(*map(int, roi_cut)), C.c_ulonglong(seed), mode)
+        st = PdState(*[state[k].data_ptr() for k in ("vol", "xbar", "xprev", "ytv", "ytp", "ybc",
+                                                     "flow", "proj")])
+        h = C.c_void_p()
+        rc = lib.stt_solver_create(ctx._h, C.byref(cfg), C.byref(st), C.byref(h))
+        if rc != 0:
+            raise STTError(rc, (lib.stt_last_error(ctx._h) or b"solver create failed").decode())
+        self._h = h
+
+    def iterate(self, n: int = 1, stream=None):
+        rc = lib.stt_solver_iterate(self._h, int(n), _stream(stream))
+        if rc != 0:
+            raise STTError(rc, lib.stt_solver_last_error(self._h).decode())
+
+    def stats(self):
+        nl, it = C.c_longlong(), C.c_ulonglong()
+        check(lib.stt_solver_stats(self._h, C.byref(nl), C.byref(it)))
+        return nl.value, it.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.stt_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -56,12 +56,15 @@ __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__re
 // updated where the ray hits, kept where it misses; with no state buffer
 // (ray-based SART, whose producer is reset after every view) a miss gives L = 0.
 __global__ void __launch_bounds__(128) k_fp_corr(const GeomDev g, const ViewRec *__restrict__ views,
-                                                 const float *__restrict__ vol, int view,
-                                                 const float *__restrict__ b,
+                                                 const float *__restrict__ vol, const ViewSel sel,
+                                                 const float *__restrict__ b_stack,
                                                  float *__restrict__ raylen_state,
                                                  float *__restrict__ corr) {
     int i, j;
     if (!tile_pixel(g, i, j)) return;
+    int local;
+    const int view = sel_view(sel, local);
+    const float *b = b_stack + (size_t)local * g.W * g.H;
     Ray r;
     make_ray(g, views[view], i, j, r);
     Kahan acc{0.0f, 0.0f};
@@ -85,11 +88,14 @@ __global__ void __launch_bounds__(128) k_fp_corr(const GeomDev g, const ViewRec 
 // :73-84): every sample scatters (c*w_k, w_k) into the interleaved
 // accumulator of its 8 clamped corners with one vector atomic each.
 __global__ void __launch_bounds__(128) k_bp_ray_scatter(const GeomDev g,
-                                                        const ViewRec *__restrict__ views, int view,
+                                                        const ViewRec *__restrict__ views,
+                                                        const ViewSel sel,
                                                         const float *__restrict__ corr,
                                                         float2 *__restrict__ acc) {
     int i, j;
     if (!tile_pixel(g, i, j)) return;
+    int local;
+    const int view = sel_view(sel, local);
     Ray r;
     make_ray(g, views[view], i, j, r);
     if (!(r.tnear < r.tfar)) return;
@@ -142,6 +148,15 @@ __global__ void k_bp_ray_update(long long n, float2 *__restrict__ acc, float *__
     }
 }
 
+// Stand-alone SART correction (ST_Tomography.cpp:667-676) for the unfused
+// per-view form: the ray lengths are the sticky state k_fp updated on hits.
+__global__ void k_correction(long long n, const float *__restrict__ b, const float *__restrict__ ax,
+                             const float *__restrict__ raylen, float *__restrict__ corr) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x)
+        corr[k] = __fdiv_rn(__fsub_rn(b[k], ax[k]), __fadd_rn(raylen ? raylen[k] : 0.0f, 1.0f));
+}
+
 __global__ void k_fill_zero(long long n, float *__restrict__ p) {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x)
@@ -166,15 +181,21 @@ cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, int view,
-                           const float *b, float *raylen_state, float *corr, cudaStream_t s) {
-    k_fp_corr<<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, view, b, raylen_state, corr);
+cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const ViewSel &sel,
+                           const float *b_stack, float *raylen_state, float *corr, cudaStream_t s) {
+    k_fp_corr<<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, sel, b_stack, raylen_state, corr);
     return cudaGetLastError();
 }
 
-cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, int view, const float *corr,
+cudaError_t launch_correction(long long n, const float *b, const float *ax, const float *raylen,
+                              float *corr, cudaStream_t s) {
+    k_correction<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, b, ax, raylen, corr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                           float2 *acc, float *vol, float gmax, cudaStream_t s) {
-    k_bp_ray_scatter<<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, corr, acc);
+    k_bp_ray_scatter<<<ray_grid(g, 1), 128, 0, s>>>(g, views, sel, corr, acc);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const long long n = (long long)g.nx * g.ny * g.nz;

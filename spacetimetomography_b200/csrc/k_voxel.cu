@@ -38,12 +38,13 @@ struct Cut8 {
 // vol += alpha*val, clamp to [0, gmax]; voxels whose footprint leaves
 // [2, W-2) x [2, H-2) are untouched.
 __global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec *__restrict__ views,
-                                                  int view, const float *__restrict__ corr,
+                                                  const ViewSel sel, const float *__restrict__ corr,
                                                   float *__restrict__ vol, float alpha, float gmax) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y, z = blockIdx.z;
     if (x >= g.nx) return;
-    const ViewRec &v = views[view];
+    int local;
+    const ViewRec &v = views[sel_view(sel, local)];
     const float fx = (float)x, fy = (float)y, fz = (float)z;
     const float cxm = v.A[0] * fx + v.A[1] * fy + v.A[2] * fz + v.b[0];
     const float cym = v.A[3] * fx + v.A[4] * fy + v.A[5] * fz + v.b[1];
@@ -186,9 +187,9 @@ Cut8 to_cut(const int *c) {
 
 }  // namespace
 
-cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, int view, const float *corr,
+cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                             float *vol, float alpha, float gmax, cudaStream_t s) {
-    k_bp_voxel<<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, view, corr, vol, alpha, gmax);
+    k_bp_voxel<<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, sel, corr, vol, alpha, gmax);
     return cudaGetLastError();
 }
 

@@ -9,118 +9,13 @@
 // L1/L2 through the read-only path.
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
+#include "warp_dev.cuh"
 
 namespace stt {
 
 namespace {
 
-struct Dim3i {
-    int x, y, z;
-};
-
-// world (aabb = [0,dim]) -> cell grid, clamped to [1, dim-2] (warping.h:54-62).
-__device__ __forceinline__ float to_grid(float p, int dim, bool *clamped) {
-    float gw = __fdiv_rn(__fmul_rn((float)dim, p), (float)dim);
-    float gq = gw - 0.5f;
-    const float hi = (float)(dim - 2), lo = 1.0f;
-    bool c = !(gq >= lo && gq <= hi);
-    gq = (gq < hi) ? gq : hi;  // std::min(hi, g)
-    gq = (lo < gq) ? gq : lo;  // std::max(lo, g)
-    if (clamped) *clamped = c;
-    return gq;
-}
-
-// Stencil of CImg::_cubic_atXYZ (CImg.h:13429-13438) for an already clamped
-// coordinate: taps x-1, x, x+1 (only when the fraction is non-zero), x+2,
-// clamped to the image.
-struct Stencil {
-    int xo[4], yo[4], zo[4];  // element offsets per axis
-    float wx[4], wy[4], wz[4];
-    float dx, dy, dz;
-    long long c0;            // linear index of the integer corner (ix,iy,iz)
-    int sx1, sy1, sz1;       // offsets to the +1 corner (for the 8-corner min/max)
-};
-
-__device__ __forceinline__ void axis_taps(float g, int dim, int stride, int o[4], float &d, int &ix) {
-    int x = (int)g;
-    d = g - (float)x;
-    const int p = x - 1 < 0 ? 0 : x - 1;
-    const int n = d > 0.0f ? x + 1 : x;
-    const int a = x + 2 >= dim ? dim - 1 : x + 2;
-    o[0] = p * stride;
-    o[1] = x * stride;
-    o[2] = n * stride;
-    o[3] = a * stride;
-    ix = x;
-}
-
-__device__ __forceinline__ void make_stencil(const Dim3i d, const float gq[3], Stencil &s) {
-    int ix, iy, iz;
-    axis_taps(gq[0], d.x, 1, s.xo, s.dx, ix);
-    axis_taps(gq[1], d.y, d.x, s.yo, s.dy, iy);
-    axis_taps(gq[2], d.z, d.x * d.y, s.zo, s.dz, iz);
-    cr_weights(s.dx, s.wx);
-    cr_weights(s.dy, s.wy);
-    cr_weights(s.dz, s.wz);
-    s.c0 = ix + (long long)iy * d.x + (long long)iz * d.x * d.y;
-    s.sx1 = 1;
-    s.sy1 = d.x;
-    s.sz1 = d.x * d.y;
-}
-
-// sample_image (warping.h:49-88): Catmull-Rom value clamped to the min/max of
-// the 8 corners of the cell.
-__device__ __forceinline__ float sample_clamped(const float *__restrict__ img, const Stencil &s) {
-    float val = 0.0f;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        float yv = 0.0f;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const float *row = img + s.yo[b] + s.zo[c];
-            float xv = s.wx[0] * __ldg(row + s.xo[0]) + s.wx[1] * __ldg(row + s.xo[1]) +
-                       s.wx[2] * __ldg(row + s.xo[2]) + s.wx[3] * __ldg(row + s.xo[3]);
-            yv += s.wy[b] * xv;
-        }
-        val += s.wz[c] * yv;
-    }
-    const float *c0 = img + s.c0;
-    float mn = __ldg(c0), mx = mn;
-    const int off[7] = {s.sx1, s.sx1 + s.sy1, s.sy1, s.sz1, s.sx1 + s.sz1, s.sx1 + s.sy1 + s.sz1,
-                        s.sy1 + s.sz1};
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        float v = __ldg(c0 + off[k]);
-        mn = (v < mn) ? v : mn;
-        mx = (mx < v) ? v : mx;
-    }
-    float inner = (val < mx) ? val : mx;
-    return (mn < inner) ? inner : mn;
-}
-
-__device__ __forceinline__ void trace(const Dim3i d, const float *__restrict__ vel, size_t n, int i,
-                                      int j, int k, float h, float q[3], float p2[3], float v1[3],
-                                      float v2[3]) {
-    // cell centre (warping.h:25-29) and the velocity there (an exact node read)
-    const float p[3] = {(float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f};
-    const int ci = min(max(i, 1), d.x - 2), cj = min(max(j, 1), d.y - 2), ck = min(max(k, 1), d.z - 2);
-    const size_t c = ci + (size_t)cj * d.x + (size_t)ck * d.x * d.y;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) v1[a] = __ldg(vel + a * n + c);
-    // trace (warping.h:100-114): p2 = p + h v(p); p0 = p2 - h v(p2); q = p2 + (p - p0)/2
-#pragma unroll
-    for (int a = 0; a < 3; ++a) p2[a] = __fadd_rn(p[a], __fmul_rn(h, v1[a]));
-    float g2[3] = {to_grid(p2[0], d.x, nullptr), to_grid(p2[1], d.y, nullptr), to_grid(p2[2], d.z, nullptr)};
-    Stencil s2;
-    make_stencil(d, g2, s2);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) v2[a] = sample_clamped(vel + a * n, s2);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        float p0 = __fsub_rn(p2[a], __fmul_rn(h, v2[a]));
-        q[a] = __fadd_rn(p2[a], __fmul_rn(0.5f, __fsub_rn(p[a], p0)));
-    }
-}
+using namespace warpdev;
 
 __global__ void __launch_bounds__(128) k_warp(const Dim3i d, const float *__restrict__ vel,
                                               const float *__restrict__ src, int nc, float dt,

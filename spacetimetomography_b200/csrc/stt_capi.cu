@@ -284,7 +284,8 @@ stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, flo
     if (!vol || !b || !corr) return fail(ctx, STT_ERR_INVALID, "null vol, b or corr");
     if ((st = check_views(ctx, view, 1))) return st;
     if ((st = set_device(ctx))) return st;
-    STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, view, b, raylen_state, corr, S(stream)),
+    const stt::ViewSel sel{view, nullptr, 0, view};
+    STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, sel, b, raylen_state, corr, S(stream)),
              "k_fp_corr launch");
     return STT_OK;
 }
@@ -309,7 +310,8 @@ stt_status stt_bp_voxel(stt_ctx *ctx, const float *corr, float *vol, double alph
     if (!corr || !vol) return fail(ctx, STT_ERR_INVALID, "null corr or vol");
     if ((st = check_views(ctx, view, 1))) return st;
     if ((st = set_device(ctx))) return st;
-    STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, view, corr, vol, (float)alpha, gmax, S(stream)),
+    const stt::ViewSel sel{view, nullptr, 0, view};
+    STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, sel, corr, vol, (float)alpha, gmax, S(stream)),
              "k_bp_voxel launch");
     return STT_OK;
 }
@@ -330,7 +332,8 @@ stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, i
     if ((st = check_views(ctx, view, 1))) return st;
     if ((st = set_device(ctx))) return st;
     if ((st = ensure_acc(ctx, S(stream)))) return st;
-    STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, view, corr, ctx->acc, vol, gmax, S(stream)),
+    const stt::ViewSel sel{view, nullptr, 0, view};
+    STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, sel, corr, ctx->acc, vol, gmax, S(stream)),
              "k_bp_ray launch");
     return STT_OK;
 }
@@ -353,18 +356,17 @@ stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, con
     if ((st = ensure(ctx, ctx->corr, ctx->corr_n, npix, "correction image"))) return st;
     if (bp_mode == 1 && (st = ensure_acc(ctx, s))) return st;
     for (int i = 0; i < nperm; ++i) {
-        const int v = view_offset + perm[i];
-        const float *b = proj_stack + (size_t)perm[i] * npix;
+        const stt::ViewSel sel{view_offset + perm[i], nullptr, 0, view_offset};
         // ray-based mode: TypicalRayProducer::Initial zeroes the ray lengths
         // after every view, so missed rays see L = 0 (no sticky state)
-        STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, v, b, bp_mode == 0 ? raylen_state : nullptr,
-                                          ctx->corr, s),
+        STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, sel, proj_stack,
+                                          bp_mode == 0 ? raylen_state : nullptr, ctx->corr, s),
                  "k_fp_corr launch");
         if (bp_mode == 0)
-            STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, v, ctx->corr, vol, (float)alpha, gmax, s),
+            STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, sel, ctx->corr, vol, (float)alpha, gmax, s),
                      "k_bp_voxel launch");
         else
-            STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, v, ctx->corr, ctx->acc, vol, gmax, s),
+            STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, sel, ctx->corr, ctx->acc, vol, gmax, s),
                      "k_bp_ray launch");
     }
     if (bp_mode == 1 && raylen_state)
@@ -443,6 +445,16 @@ static stt_status check_warp_args(const int *dim, const float *vel, const float 
     if (nc < 1) return fail(nullptr, STT_ERR_INVALID, "nc must be >= 1");
     if ((long long)dim[0] * dim[1] * dim[2] * (nc > 3 ? nc : 3) >= (1LL << 31))
         return fail(nullptr, STT_ERR_INVALID, "warp volume too large for 32-bit tap offsets");
+    return STT_OK;
+}
+
+// Solver access to the context's geometry (not part of the public header).
+stt_status stt_internal_geom(stt_ctx *ctx, const void **geom, const void **views) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if ((st = set_device(ctx))) return st;
+    *geom = &ctx->g;
+    *views = ctx->views_d;
     return STT_OK;
 }
 

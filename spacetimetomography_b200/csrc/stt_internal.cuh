@@ -46,6 +46,22 @@ __device__ __forceinline__ T rmax(T a, T b) { return (a > b) ? a : b; }
 template <typename T>
 __device__ __forceinline__ T rmin(T a, T b) { return (a < b) ? a : b; }
 
+// Which view a launch works on: a fixed index, or base + perm[slot] read from
+// device memory (the solver's per-iteration view order, drawn on the device so
+// that a captured CUDA graph replays with a fresh order each time).  `local`
+// is the view's index within its frame (its slot in the projection stack).
+struct ViewSel {
+    int view;
+    const int *perm;
+    int slot;
+    int base;
+};
+
+__device__ __forceinline__ int sel_view(const ViewSel &s, int &local) {
+    local = s.perm ? __ldg(s.perm + s.slot) : s.view - s.base;
+    return s.base + local;
+}
+
 // Compensated (Kahan) accumulator for ray sums.
 struct Kahan {
     float s, c;

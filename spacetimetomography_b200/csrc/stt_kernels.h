@@ -7,6 +7,7 @@ namespace stt {
 
 struct ViewRec;
 struct GeomDev;
+struct ViewSel;
 
 struct PdParams {
     float sigma, tau, tv_w, tp_w, bc_w, hf, gmax;
@@ -17,16 +18,20 @@ int grid_stride_blocks(long long n, int threads);
 
 cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, int view0,
                       int nviews, float *proj, float *raylen, float *weight, cudaStream_t s);
-cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, int view,
-                           const float *b, float *raylen_state, float *corr, cudaStream_t s);
-cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, int view, const float *corr,
+cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const ViewSel &sel,
+                           const float *b_stack, float *raylen_state, float *corr, cudaStream_t s);
+cudaError_t launch_correction(long long n, const float *b, const float *ax, const float *raylen,
+                              float *corr, cudaStream_t s);
+cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                           float2 *acc, float *vol, float gmax, cudaStream_t s);
 cudaError_t launch_fp_adjoint(const GeomDev &g, const ViewRec *views, int view0, int nviews,
                               const float *proj_bar, float *vol_bar, cudaStream_t s);
 cudaError_t launch_fill_zero(float *p, long long n, cudaStream_t s);
 
-cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, int view, const float *corr,
+cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                             float *vol, float alpha, float gmax, cudaStream_t s);
+cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counter, int frames,
+                             int views, int *perm, cudaStream_t s);
 cudaError_t launch_pd_dual(const int *dims, const PdParams &p, const float *xf, const float *xf1,
                            const float *bw, float *ytv, float *ytp, float *ybc, cudaStream_t s);
 cudaError_t launch_pd_primal(const int *dims, const PdParams &p, int first, const float *ytp_prev,

@@ -1,0 +1,429 @@
+// stt_solver.cu -- one space-time primal-dual iteration of ST_Tomography::Render
+// (S/ST_Tomo/ST_Tomography.cpp:492-607) over all frames, enqueued three ways:
+//
+//   STT_SOLVE_PLAIN    the per-view GPU form: frames in order, every view's
+//                      forward projection, correction and backprojection as
+//                      separate launches from a host loop, host sync per view;
+//   STT_SOLVE_STREAMS  the batched form enqueued directly: all duals first,
+//                      then the per-frame primal + SART + over-relaxation
+//                      chains on one stream per frame, FP fused with the
+//                      correction;
+//   STT_SOLVE_GRAPH    the batched form captured once into a CUDA graph and
+//                      replayed (the view order is drawn on the device from a
+//                      counter, so every replay gets a fresh seeded order).
+//
+// Reordering "all duals, then every frame's primal chain" is exact: frame f's
+// dual reads X_bar[f], X_bar[f+1] and flow[f] only, and X_bar[f] is rewritten
+// only by frame f's own over-relaxation (ST_Tomography.cpp:503-534 vs :598),
+// which the graph orders after the duals of frames f-1 and f.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "stt.h"
+#include "stt_internal.cuh"
+#include "stt_kernels.h"
+
+namespace stt {
+namespace {
+
+__device__ __host__ __forceinline__ unsigned long long splitmix(unsigned long long &s) {
+    unsigned long long z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Seed of frame f's view order in PD iteration `iter` (the reference reseeds
+// with time(0) in every SART call, ST_Tomography.cpp:635).
+__device__ __host__ __forceinline__ unsigned long long frame_seed(unsigned long long seed,
+                                                                 unsigned long long iter, int frames,
+                                                                 int f) {
+    return seed + 0x9E3779B97F4A7C15ull * (iter * (unsigned long long)frames + (unsigned long long)f + 1ull);
+}
+
+// One thread per frame: Fisher-Yates with SplitMix64 (the same stream as
+// stt_permutation), then thread 0 advances the iteration counter.
+__global__ void k_make_perm(unsigned long long seed, unsigned long long *counter, int frames, int views,
+                            int *perm) {
+    const int f = threadIdx.x + blockIdx.x * blockDim.x;
+    const unsigned long long iter = *counter;
+    if (f < frames) {
+        int *p = perm + (size_t)f * views;
+        for (int i = 0; i < views; ++i) p[i] = i;
+        unsigned long long s = frame_seed(seed, iter, frames, f);
+        for (int i = views - 1; i > 0; --i) {
+            const int j = (int)(splitmix(s) % (unsigned long long)(i + 1));
+            const int t = p[i];
+            p[i] = p[j];
+            p[j] = t;
+        }
+    }
+    __syncthreads();
+    if (f == 0) *counter = iter + 1;
+}
+
+}  // namespace
+
+cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counter, int frames, int views,
+                             int *perm, cudaStream_t s) {
+    k_make_perm<<<1, ((frames + 31) / 32) * 32, 0, s>>>(seed, counter, frames, views, perm);
+    return cudaGetLastError();
+}
+
+void host_perm(unsigned long long seed, unsigned long long iter, int frames, int f, int views, int *p) {
+    for (int i = 0; i < views; ++i) p[i] = i;
+    unsigned long long s = frame_seed(seed, iter, frames, f);
+    for (int i = views - 1; i > 0; --i) {
+        const int j = (int)(splitmix(s) % (unsigned long long)(i + 1));
+        const int t = p[i];
+        p[i] = p[j];
+        p[j] = t;
+    }
+}
+
+}  // namespace stt
+
+// The context internals the solver needs (defined in stt_capi.cu).
+extern "C" stt_status stt_internal_geom(stt_ctx *ctx, const void **geom, const void **views);
+
+struct stt_solver {
+    stt_ctx *ctx = nullptr;
+    stt_solve_cfg cfg{};
+    stt_pd_state st{};
+    const stt::GeomDev *g = nullptr;
+    const stt::ViewRec *views = nullptr;
+    int F = 0, V = 0;
+    size_t n = 0, npix = 0;
+    float *warpbuf = nullptr;  // F volumes: backward-warped X_bar[f+1], then forward-warped Y_bc[f-1]
+    float *corr = nullptr;     // F correction images
+    float *ax = nullptr;       // plain form: forward projection image
+    float *raylen = nullptr;   // F sticky ray-length images
+    float2 *acc = nullptr;     // ray-based BP accumulators, F volumes
+    int *perm = nullptr;       // F x V device view order
+    unsigned long long *counter = nullptr;
+    unsigned long long host_iter = 0;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> ev_dual, ev_done;
+    cudaEvent_t ev_fork = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long launches_per_iter = 0;
+    std::string err;
+};
+
+namespace {
+
+stt_status sfail(stt_solver *s, stt_status st, const std::string &m) {
+    if (s) s->err = m;
+    return st;
+}
+
+#define SCUDA(s, call, where)                                                                         \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) return sfail(s, STT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+stt::PdParams pdp(const stt_pd_params &p) {
+    stt::PdParams q;
+    q.sigma = p.sigma;
+    q.tau = p.tau;
+    q.tv_w = p.tv_w;
+    q.tp_w = p.tp_w;
+    q.bc_w = p.bc_w;
+    q.hf = p.huber_factor;
+    q.gmax = p.gmax;
+    for (int i = 0; i < 8; ++i) q.cut[i] = p.cut[i];
+    return q;
+}
+
+// Frame f's dual step: backward warp of X_bar[f+1] along flow[f]
+// (ST_Tomography.cpp:502-503) then the fused dual kernel (:504-534).
+stt_status enqueue_dual(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
+    const int d[3] = {s->g->nx, s->g->ny, s->g->nz};
+    const size_t n = s->n;
+    float *bw = s->warpbuf + f * n;
+    SCUDA(s, stt::launch_warp(d, s->st.flow + (size_t)f * 3 * n, s->st.xbar + (f + 1) * n, 1, -1.0f, bw, cs),
+          "warp (dual)");
+    SCUDA(s, stt::launch_pd_dual(d, pdp(s->cfg.pd), s->st.xbar + f * n, s->st.xbar + (f + 1) * n, bw,
+                                 s->st.ytv + (size_t)f * 3 * n, s->st.ytp + f * n, s->st.ybc + f * n, cs),
+          "pd_dual");
+    nl += 2;
+    return STT_OK;
+}
+
+// Frame f's primal step (ST_Tomography.cpp:536-578): forward warp of
+// Y_bc[f-1] along flow[f-1] for f > 0, then the fused primal kernel.
+stt_status enqueue_primal(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
+    const int d[3] = {s->g->nx, s->g->ny, s->g->nz};
+    const size_t n = s->n;
+    float *fw = s->warpbuf + f * n;
+    if (f > 0) {
+        SCUDA(s, stt::launch_warp(d, s->st.flow + (size_t)(f - 1) * 3 * n, s->st.ybc + (f - 1) * n, 1, 1.0f, fw, cs),
+              "warp (primal)");
+        ++nl;
+    }
+    SCUDA(s, stt::launch_pd_primal(d, pdp(s->cfg.pd), f == 0, f > 0 ? s->st.ytp + (f - 1) * n : nullptr,
+                                   s->st.ytp + f * n, f > 0 ? fw : nullptr, s->st.ybc + f * n,
+                                   s->st.ytv + (size_t)f * 3 * n, s->st.vol + f * n, s->st.xprev + f * n, cs),
+          "pd_primal");
+    ++nl;
+    return STT_OK;
+}
+
+// SART(f) (ST_Tomography.cpp:616-808) as fused launches, views read from the
+// device-side order, then the ROI mask (:793-804) fused with the
+// over-relaxation X_bar[f] = 2V - X_prev (:586-604).
+stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
+    const stt::GeomDev &g = *s->g;
+    const int V = s->V;
+    float *vol = s->st.vol + f * s->n;
+    float *corr = s->corr + f * s->npix;
+    const float *stack = s->st.proj + (size_t)f * V * s->npix;
+    const int voxel = s->cfg.bp_mode == 0;
+    for (int i = 0; i < V; ++i) {
+        const stt::ViewSel sel{0, s->perm + (size_t)f * V, i, f * V};
+        SCUDA(s, stt::launch_fp_corr(g, s->views, vol, sel, stack, voxel ? s->raylen + f * s->npix : nullptr, corr, cs),
+              "fp_corr");
+        if (voxel)
+            SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs),
+                  "bp_voxel");
+        else
+            SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs),
+                  "bp_ray");
+        nl += voxel ? 2 : 3;
+    }
+    const int d[3] = {g.nx, g.ny, g.nz};
+    SCUDA(s, stt::launch_roi_apply(d, s->cfg.roi_cut, s->cfg.pd.cut, vol, s->st.xprev + f * s->n,
+                                   s->st.xbar + f * s->n, cs),
+          "roi_apply");
+    ++nl;
+    return STT_OK;
+}
+
+stt_status enqueue_batched(stt_solver *s, cudaStream_t main, long long &nl) {
+    const int F = s->F;
+    SCUDA(s, stt::launch_make_perm(s->cfg.seed, s->counter, F, s->V, s->perm, main), "make_perm");
+    ++nl;
+    SCUDA(s, cudaEventRecord(s->ev_fork, main), "event record");
+    for (int f = 0; f < F; ++f) SCUDA(s, cudaStreamWaitEvent(s->streams[f], s->ev_fork, 0), "stream wait");
+    for (int f = 0; f < F; ++f) {
+        stt_status st = enqueue_dual(s, f, s->streams[f], nl);
+        if (st) return st;
+        SCUDA(s, cudaEventRecord(s->ev_dual[f], s->streams[f]), "event record");
+    }
+    for (int f = 0; f < F; ++f) {
+        cudaStream_t cs = s->streams[f];
+        if (f > 0) SCUDA(s, cudaStreamWaitEvent(cs, s->ev_dual[f - 1], 0), "stream wait");
+        stt_status st = enqueue_primal(s, f, cs, nl);
+        if (st) return st;
+        if ((st = enqueue_sart_batched(s, f, cs, nl))) return st;
+        SCUDA(s, cudaEventRecord(s->ev_done[f], cs), "event record");
+        SCUDA(s, cudaStreamWaitEvent(main, s->ev_done[f], 0), "stream wait");
+    }
+    return STT_OK;
+}
+
+// The per-view form: frame by frame as the reference loops, each view's
+// forward projection, correction and backprojection as separate launches,
+// and a host synchronisation after every view.
+stt_status run_plain(stt_solver *s, cudaStream_t cs, long long &nl) {
+    const stt::GeomDev &g = *s->g;
+    const int F = s->F, V = s->V;
+    const int d[3] = {g.nx, g.ny, g.nz};
+    std::vector<int> perm(V);
+    const int voxel = s->cfg.bp_mode == 0;
+    for (int f = 0; f < F; ++f) {
+        stt_status st = enqueue_dual(s, f, cs, nl);
+        if (st) return st;
+        if ((st = enqueue_primal(s, f, cs, nl))) return st;
+        stt::host_perm(s->cfg.seed, s->host_iter, F, f, V, perm.data());
+        float *vol = s->st.vol + f * s->n;
+        float *corr = s->corr + f * s->npix;
+        float *rl = s->raylen + f * s->npix;
+        for (int i = 0; i < V; ++i) {
+            const int view = f * V + perm[i];
+            const float *b = s->st.proj + ((size_t)f * V + perm[i]) * s->npix;
+            const stt::ViewSel sel{view, nullptr, 0, view};
+            if (voxel) {
+                SCUDA(s, stt::launch_fp(g, s->views, vol, view, 1, s->ax, rl, nullptr, cs), "fp");
+                SCUDA(s, stt::launch_correction((long long)s->npix, b, s->ax, rl, corr, cs), "correction");
+                SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs),
+                      "bp_voxel");
+                nl += 3;
+            } else {
+                // ray-based: the producer is reset after every view (L = 0 on a miss)
+                SCUDA(s, stt::launch_fill_zero(rl, (long long)s->npix, cs), "fill");
+                SCUDA(s, stt::launch_fp(g, s->views, vol, view, 1, s->ax, rl, nullptr, cs), "fp");
+                SCUDA(s, stt::launch_correction((long long)s->npix, b, s->ax, rl, corr, cs), "correction");
+                SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs),
+                      "bp_ray");
+                nl += 5;
+            }
+            SCUDA(s, cudaStreamSynchronize(cs), "per-view synchronize");
+        }
+        SCUDA(s, stt::launch_roi_apply(d, s->cfg.roi_cut, s->cfg.pd.cut, vol, s->st.xprev + f * s->n,
+                                       s->st.xbar + f * s->n, cs),
+              "roi_apply");
+        ++nl;
+    }
+    ++s->host_iter;
+    // keep the device counter in step so that the modes can be mixed
+    SCUDA(s, cudaMemcpyAsync(s->counter, &s->host_iter, sizeof(unsigned long long), cudaMemcpyHostToDevice, cs),
+          "counter update");
+    SCUDA(s, cudaStreamSynchronize(cs), "synchronize");
+    return STT_OK;
+}
+
+template <typename T>
+stt_status alloc(stt_solver *s, T *&p, size_t count, const char *what) {
+    cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return sfail(s, STT_ERR_NOMEM, std::string("cudaMalloc(") + what + "): " + cudaGetErrorString(e));
+    }
+    return STT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_pd_state *state,
+                             stt_solver **out) {
+    if (!ctx || !cfg || !state || !out) return STT_ERR_INVALID;
+    *out = nullptr;
+    const void *gp = nullptr, *vp = nullptr;
+    stt_status st = stt_internal_geom(ctx, &gp, &vp);
+    if (st) return st;
+    const stt::GeomDev *g = (const stt::GeomDev *)gp;
+    if (cfg->n_frames < 1 || cfg->views_per_frame < 1 || (long long)cfg->n_frames * cfg->views_per_frame > g->n_views)
+        return STT_ERR_INVALID;
+    if (cfg->bp_mode != 0 && cfg->bp_mode != 1) return STT_ERR_INVALID;
+    if (cfg->mode < STT_SOLVE_PLAIN || cfg->mode > STT_SOLVE_GRAPH) return STT_ERR_INVALID;
+    if (!state->vol || !state->xbar || !state->xprev || !state->ytv || !state->ytp || !state->ybc ||
+        !state->flow || !state->proj)
+        return STT_ERR_INVALID;
+    stt_solver *s = new stt_solver();
+    s->ctx = ctx;
+    s->cfg = *cfg;
+    s->st = *state;
+    s->g = g;
+    s->views = (const stt::ViewRec *)vp;
+    s->F = cfg->n_frames;
+    s->V = cfg->views_per_frame;
+    s->n = (size_t)g->nx * g->ny * g->nz;
+    s->npix = (size_t)g->W * g->H;
+    const int F = s->F;
+    stt_status e = STT_OK;
+    if (!e) e = alloc(s, s->warpbuf, (size_t)F * s->n, "warp buffers");
+    if (!e) e = alloc(s, s->corr, (size_t)F * s->npix, "corrections");
+    if (!e) e = alloc(s, s->ax, s->npix, "projection");
+    if (!e) e = alloc(s, s->raylen, (size_t)F * s->npix, "ray lengths");
+    if (!e) e = alloc(s, s->perm, (size_t)F * s->V, "view order");
+    if (!e) e = alloc(s, s->counter, 1, "iteration counter");
+    if (!e && cfg->bp_mode == 1) e = alloc(s, s->acc, (size_t)F * s->n, "ray-BP accumulators");
+    if (e) {
+        stt_solver_destroy(s);
+        return e;
+    }
+    cudaError_t ce = cudaMemset(s->raylen, 0, (size_t)F * s->npix * sizeof(float));
+    if (ce == cudaSuccess) ce = cudaMemset(s->counter, 0, sizeof(unsigned long long));
+    if (ce == cudaSuccess && s->acc) ce = cudaMemset(s->acc, 0, (size_t)F * s->n * sizeof(float2));
+    s->streams.resize(F);
+    s->ev_dual.resize(F);
+    s->ev_done.resize(F);
+    for (int f = 0; f < F && ce == cudaSuccess; ++f) {
+        ce = cudaStreamCreateWithFlags(&s->streams[f], cudaStreamNonBlocking);
+        if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&s->ev_dual[f], cudaEventDisableTiming);
+        if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&s->ev_done[f], cudaEventDisableTiming);
+    }
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
+    if (ce != cudaSuccess) {
+        stt_solver_destroy(s);
+        return STT_ERR_CUDA;
+    }
+    *out = s;
+    return STT_OK;
+}
+
+stt_status stt_solver_iterate(stt_solver *s, int n_iters, void *stream) {
+    if (!s || n_iters < 0) return STT_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+    for (int it = 0; it < n_iters; ++it) {
+        long long nl = 0;
+        stt_status st = STT_OK;
+        if (s->cfg.mode == STT_SOLVE_PLAIN) {
+            st = run_plain(s, cs, nl);
+        } else if (s->cfg.mode == STT_SOLVE_STREAMS) {
+            st = enqueue_batched(s, cs, nl);
+            ++s->host_iter;
+        } else {
+            if (!s->exec) {
+                cudaStream_t cap;
+                SCUDA(s, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "capture stream");
+                SCUDA(s, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+                st = enqueue_batched(s, cap, nl);
+                cudaGraph_t graph = nullptr;
+                cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+                cudaStreamDestroy(cap);
+                if (st) {
+                    if (graph) cudaGraphDestroy(graph);
+                    return st;
+                }
+                if (ce != cudaSuccess) return sfail(s, STT_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ce));
+                s->graph = graph;
+                SCUDA(s, cudaGraphInstantiate(&s->exec, graph, 0), "graph instantiate");
+                s->launches_per_iter = nl;
+            }
+            SCUDA(s, cudaGraphLaunch(s->exec, cs), "graph launch");
+            nl = s->launches_per_iter;
+            ++s->host_iter;
+        }
+        if (st) return st;
+        s->launches_per_iter = nl;
+    }
+    return STT_OK;
+}
+
+stt_status stt_solver_stats(const stt_solver *s, long long *launches_per_iter, unsigned long long *iterations) {
+    if (!s) return STT_ERR_INVALID;
+    if (launches_per_iter) *launches_per_iter = s->launches_per_iter;
+    if (iterations) *iterations = s->host_iter;
+    return STT_OK;
+}
+
+const char *stt_solver_last_error(const stt_solver *s) { return s ? s->err.c_str() : ""; }
+
+stt_status stt_solver_destroy(stt_solver *s) {
+    if (!s) return STT_OK;
+    if (s->exec) cudaGraphExecDestroy(s->exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    for (auto st : s->streams)
+        if (st) cudaStreamDestroy(st);
+    for (auto e : s->ev_dual)
+        if (e) cudaEventDestroy(e);
+    for (auto e : s->ev_done)
+        if (e) cudaEventDestroy(e);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    cudaFree(s->warpbuf);
+    cudaFree(s->corr);
+    cudaFree(s->ax);
+    cudaFree(s->raylen);
+    cudaFree(s->acc);
+    cudaFree(s->perm);
+    cudaFree(s->counter);
+    delete s;
+    return STT_OK;
+}
+
+stt_status stt_solver_frame_order(unsigned long long seed, unsigned long long iter, int n_frames, int frame,
+                                  int views, int *perm_out) {
+    if (n_frames < 1 || frame < 0 || frame >= n_frames || views < 1 || !perm_out) return STT_ERR_INVALID;
+    stt::host_perm(seed, iter, n_frames, frame, views, perm_out);
+    return STT_OK;
+}
+
+}  // extern "C"

@@ -121,6 +121,11 @@ def deformation_flow(dims, t0: float, t1: float, period: float, amplitude: float
     fx = torch.sin(k * torch.arange(nx, device=device, dtype=torch.float32)) * s
     fy = torch.sin(k * torch.arange(ny, device=device, dtype=torch.float32)) * s
     fz = torch.sin(k * torch.arange(nz, device=device, dtype=torch.float32)) * s
+    # sin(k x) vanishes exactly at the nodes x = 0, pi/k, ...; float rounding
+    # leaves ~1e-16 there, which the semi-Lagrangian trace would resolve
+    # differently in FP32 and FP64 (the clamped tricubic sampler is
+    # discontinuous across cell boundaries), so the exact zeros are restored.
+    fx, fy, fz = (torch.where(v.abs() < 1e-6 * max(abs(s), 1e-30), torch.zeros_like(v), v) for v in (fx, fy, fz))
     flow = torch.empty((3, nz, ny, nx), dtype=torch.float32, device=device)
     flow[0] = fx.view(1, 1, nx).expand(nz, ny, nx)
     flow[1] = fy.view(1, ny, 1).expand(nz, ny, nx)

@@ -307,3 +307,71 @@ def rel_l2(a, b) -> float:
     b = np.asarray(b, np.float64)
     n = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (n if n > 0 else 1.0))
+
+
+def pd_dual64(dims, pp, cut, xf, xf1, bw, ytv, ytp, ybc):
+    ytv, ytp, ybc = (np.array(a, np.float64, copy=True) for a in (ytv, ytp, ybc))
+    O.orc_pd_dual_f64(P(np.array(dims, np.int32)), P(np.array(pp, np.float64)), P(np.array(cut, np.int32)),
+                      P(np.ascontiguousarray(xf, np.float64)), P(np.ascontiguousarray(xf1, np.float64)),
+                      P(np.ascontiguousarray(bw, np.float64)), P(ytv), P(ytp), P(ybc))
+    return ytv, ytp, ybc
+
+
+def pd_primal64(dims, pp, cut, first, ytp_prev, ytp, fw, ybc, ytv, vol):
+    v = np.array(vol, np.float64, copy=True)
+    xprev = np.zeros_like(v)
+    z = np.zeros_like(v)
+    O.orc_pd_primal_f64(P(np.array(dims, np.int32)), P(np.array(pp, np.float64)), P(np.array(cut, np.int32)),
+                        int(first), P(np.ascontiguousarray(z if ytp_prev is None else ytp_prev, np.float64)),
+                        P(np.ascontiguousarray(ytp, np.float64)),
+                        P(np.ascontiguousarray(z if fw is None else fw, np.float64)),
+                        P(np.ascontiguousarray(ybc, np.float64)), P(np.ascontiguousarray(ytv, np.float64)),
+                        P(v), P(xprev))
+    return v, xprev
+
+
+def pd_extrapolate64(dims, cut, vol, xprev, xbar):
+    xb = np.array(xbar, np.float64, copy=True)
+    O.orc_pd_extrapolate_f64(P(np.array(dims, np.int32)), P(np.array(cut, np.int32)),
+                             P(np.ascontiguousarray(vol, np.float64)), P(np.ascontiguousarray(xprev, np.float64)),
+                             P(xb))
+    return xb
+
+
+def pd_iteration(scan, angles, st, F, V, pp, pd_cut, roi_cut, alpha, bp_mode, orders, raylen, fp64=True):
+    """One primal-dual iteration of ST_Tomography::Render (ST_Tomography.cpp:492-607)
+    in the reference's sequential frame order.  fp64=True: the FP64 oracle;
+    fp64=False: the reference's FP32 arithmetic (float march on FP64 ray setup).
+    st: dict of arrays (vol (F+1), xbar (F+1), xprev F, ytv F x 3, ytp F, ybc F,
+    flow F x 3, proj F x V); orders[f] is frame f's view order; raylen[f] the
+    sticky ray-length state.  pp = (sigma, tau, tv_w, tp_w, bc_w, huber_factor, gmax)."""
+    dims = scan.dims
+    dt = np.float64 if fp64 else np.float32
+    st = {k: np.array(v, dt, copy=True) for k, v in st.items()}
+    roi = roi_mask(dims, roi_cut).astype(dt)
+    views = [view_angle(a) for a in angles]
+    opd = OPd(*pp, (C.c_int * 8)(*pd_cut))
+    for f in range(F):
+        if fp64:
+            bw = warp64(st["flow"][f], st["xbar"][f + 1], -1.0)
+            st["ytv"][f], st["ytp"][f], st["ybc"][f] = pd_dual64(dims, pp, pd_cut, st["xbar"][f], st["xbar"][f + 1],
+                                                                 bw, st["ytv"][f], st["ytp"][f], st["ybc"][f])
+            fw = None if f == 0 else warp64(st["flow"][f - 1], st["ybc"][f - 1], 1.0)
+            st["vol"][f], st["xprev"][f] = pd_primal64(dims, pp, pd_cut, f == 0,
+                                                       None if f == 0 else st["ytp"][f - 1], st["ytp"][f], fw,
+                                                       st["ybc"][f], st["ytv"][f], st["vol"][f])
+            st["vol"][f], raylen[f] = sart64(scan, views[f * V:(f + 1) * V], orders[f], st["proj"][f], alpha, pp[6],
+                                             bp_mode, st["vol"][f], raylen=raylen[f], roi=roi)
+            st["xbar"][f] = pd_extrapolate64(dims, pd_cut, st["vol"][f], st["xprev"][f], st["xbar"][f])
+        else:
+            bw = warp32(st["flow"][f], st["xbar"][f + 1], -1.0)
+            st["ytv"][f], st["ytp"][f], st["ybc"][f] = pd_dual32(dims, opd, st["xbar"][f], st["xbar"][f + 1], bw,
+                                                                 st["ytv"][f], st["ytp"][f], st["ybc"][f])
+            z = np.zeros_like(st["vol"][f])
+            fw = z if f == 0 else warp32(st["flow"][f - 1], st["ybc"][f - 1], 1.0)
+            st["vol"][f], st["xprev"][f] = pd_primal32(dims, opd, f == 0, z if f == 0 else st["ytp"][f - 1],
+                                                       st["ytp"][f], fw, st["ybc"][f], st["ytv"][f], st["vol"][f])
+            st["vol"][f], raylen[f] = sart32(scan, views[f * V:(f + 1) * V], orders[f], st["proj"][f], alpha, pp[6],
+                                             bp_mode, st["vol"][f], raylen=raylen[f], roi=roi, gmode=1)
+            st["xbar"][f] = pd_extrapolate32(dims, pd_cut, st["vol"][f], st["xprev"][f], st["xbar"][f])
+    return st
