@@ -1,0 +1,518 @@
+#!/usr/bin/env python
+"""Benchmark: one space-time primal-dual iteration of the 4D reconstruction.
+
+Workload (the 4D configuration the "s per 4D primal-dual iteration" metric is
+quoted on): 10 frames of a 256^3 FP32 deforming ellipsoid phantom (30
+ellipsoids displaced by u(x,t) = 4 sin(2 pi t/T + phi)(sin kx, sin ky, sin kz),
+k = 2 pi/256), 36 views per frame on golden-angle low-discrepancy angles, a
+512x512 detector, sid 600 mm, sdd 1000 mm, voxel-based SART (alpha 0.3),
+TV weight 0.01 (Huber 0.01), temporal weight 0.1, brightness-constancy weight
+0.05, the reference's ROI cut.  Synthetic, seeded data stand in for the
+reference's external scans.  A step is one full primal-dual iteration over all
+frames: backward warp + dual, forward warp + primal, SART over every view,
+ROI mask, over-relaxation.
+
+metric: projector GUPS over the 4D primal-dual iteration
+        = frames * N^3 * views_per_frame / seconds_per_iteration / 1e9
+        (each voxel-view update is one forward projection + one backprojection).
+
+`python bench.py [--gpus N --steps K --warmup W]`; for N > 1 launch with
+torch.distributed.run: each rank solves its own 10 frames (weak scaling) and
+exchanges the neighbouring frames' boundary volumes with NCCL.
+`--impl reference` times the reference's CPU implementation of the same step
+(the reference's own projector and warp compiled from its sources, the SART and
+primal-dual loop bodies restated in FP32) on the host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC_FILE = ROOT / "profiles" / "fp_corr_traffic.json"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["stt", "reference"], default="stt")
+    ap.add_argument("--n", type=int, default=256, help="volume edge (voxels)")
+    ap.add_argument("--frames", type=int, default=10)
+    ap.add_argument("--views", type=int, default=36, help="views per frame")
+    ap.add_argument("--det", type=int, default=512, help="detector edge (pixels)")
+    ap.add_argument("--bp", choices=["voxel", "ray"], default="voxel")
+    ap.add_argument("--no-plain", action="store_true", help="skip the per-view (plain) comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def workload(args) -> dict:
+    return {"workload": f"4D primal-dual iteration, {args.frames} frames x {args.n}^3 FP32, "
+                        f"{args.views} views/frame, {args.det}^2 detector",
+            "frames": args.frames, "volume": [args.n] * 3, "views_per_frame": args.views,
+            "detector": [args.det, args.det], "sid_mm": 600.0, "sdd_mm": 1000.0,
+            "backprojector": "voxel-based" if args.bp == "voxel" else "ray-based",
+            "alpha": 0.3, "tv_weight": 0.01, "huber": 0.01, "tp_weight": 0.1, "bc_weight": 0.05,
+            "angles": "golden-angle low-discrepancy, consecutive across frames",
+            "l2": "inputs larger than L2 (solver state ~8 GB per GPU), no flush needed"}
+
+
+def pd_params(gmax: float):
+    import spacetimetomography_b200 as stt
+
+    sigma = 0.9 / 8.0  # CP_sigma = 0.9/(L*CP_tau), L = 8, CP_tau = 1 (ST_Tomography.cpp:99-102)
+    lam, huber = 0.01, 0.01
+    return stt.PdParams(sigma=sigma, tau=1.0, tv_w=lam, tp_w=0.1, bc_w=0.05,
+                        huber_factor=1.0 / (1.0 + sigma * huber / lam), gmax=gmax)
+
+
+def angles_for(args, rank: int) -> np.ndarray:
+    golden = math.pi * (3.0 - math.sqrt(5.0))
+    first = rank * args.frames * args.views
+    return (np.arange(first, first + args.frames * args.views) * golden) % (2 * math.pi)
+
+
+def build_problem(args, dev, rank: int):
+    """Device state of one rank's frames plus the pinned host copy of its inputs."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200 import phantom as ph
+
+    N, F, V, D = args.n, args.frames, args.views, args.det
+    dims = (N, N, N)
+    ang = angles_for(args, rank)
+    ctx = stt.Context(dev.index or 0)
+    ctx.set_geometry(dims, (1.0, 1.0, 1.0), (D, D), 1.0, 600.0, 1000.0, ang)
+    params = ph.ellipsoid_params(30, dims, seed=2024, semi=(5.0 * N / 256, 40.0 * N / 256))
+    T = F * max(1, int(os.environ.get("WORLD_SIZE", "1")))
+    phase = 0.7
+    proj = torch.empty((F, V, D, D), device=dev)
+    flow = torch.empty((F, 3, N, N, N), device=dev)
+    for f in range(F):
+        t = rank * F + f
+        truth = ph.rasterize(ph.displaced_params(params, t, T, 4.0, 2 * math.pi / N, phase), dims, dev)
+        ctx.fp(truth, proj[f], view0=f * V, nviews=V)
+        flow[f] = ph.deformation_flow(dims, t, t + 1, T, 4.0, 2 * math.pi / N, phase, device=dev)
+    proj = ph.add_noise(proj, 0.01, seed=7 + rank)
+    torch.cuda.synchronize()
+    gmax = float(proj[0].max().item() / 4.0)
+    st = dict(vol=torch.zeros((F + 1, N, N, N), device=dev), xbar=torch.zeros((F + 1, N, N, N), device=dev),
+              xprev=torch.zeros((F, N, N, N), device=dev), ytv=torch.zeros((F, 3, N, N, N), device=dev),
+              ytp=torch.zeros((F, N, N, N), device=dev), ybc=torch.zeros((F, N, N, N), device=dev),
+              flow=flow, proj=proj)
+    return ctx, st, gmax, ang
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms in the background."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    if PEAKS_FILE.exists():
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(args):
+    """DRAM bytes per k_fp_corr launch from the committed ncu capture summary, if any."""
+    if TRAFFIC_FILE.exists():
+        d = json.loads(TRAFFIC_FILE.read_text())
+        key = f"{args.n}x{args.det}"
+        if key in d:
+            return d[key]
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_sample(args, threads: int, gpu_check=None) -> dict:
+    """Times the reference's CPU implementation of one frame's share of a PD
+    iteration on a bounded sample and scales it to the full iteration:
+    2 warps + dual + primal of one frame, and `k` views of forward projection +
+    correction + voxel backprojection.  The projector and warp are the
+    reference's own code compiled from its sources (oracle/_ref) when present;
+    the loop bodies of ST_Tomography.cpp (correction, voxel BP, PD steps) are
+    the FP32 restatement (oracle/liboracle.so), run with the reference's
+    OpenMP loops."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_bind as ob
+    from spacetimetomography_b200 import phantom as ph
+    import torch
+
+    N, D, V, F = args.n, args.det, args.views, args.frames
+    dims = (N, N, N)
+    scan = ob.Scan(N, (D, D))
+    vol = ph.ellipsoid_phantom(dims, 30, seed=2024, semi=(5.0 * N / 256, 40.0 * N / 256)).numpy()
+    flow = ph.deformation_flow(dims, 0, 1, F, 4.0, 2 * math.pi / N, 0.7).numpy()
+    k = 2
+    use_ref = ob.REF is not None
+    t0 = time.perf_counter()
+    fps = []
+    for i in range(k):
+        if use_ref:
+            img, rl, _ = ob.ref_fp(scan, 13.0 * i, i, vol, threads=threads)
+        else:
+            img, rl, _ = ob.fp32(scan, ob.view_round(13.0 * i, i), vol, gmode=0, threads=threads)
+        fps.append((img, rl))
+    t_fp = (time.perf_counter() - t0) / k
+    c = np.zeros((D, D), np.float32)
+    t0 = time.perf_counter()
+    for img, rl in fps:
+        ob.O.orc_correction_f32(D * D, ob.P(img), ob.P(img), ob.P(rl), ob.P(c))
+    t_corr = (time.perf_counter() - t0) / k
+    t0 = time.perf_counter()
+    v2 = vol.copy()
+    g = scan.ogeom()
+    for i in range(k):
+        ob.O.orc_bp_voxel_f32(ob.C.byref(g), 0, ob.C.byref(ob.view_round(13.0 * i, i)), ob.P(fps[i][0]), 0.3, 10.0,
+                              ob.P(v2), threads)
+    t_bp = (time.perf_counter() - t0) / k
+    t0 = time.perf_counter()
+    if use_ref:
+        bw = ob.ref_warp(flow, vol, -1.0)
+    else:
+        bw = ob.warp32(flow, vol, -1.0, threads=4)
+    t_warp = time.perf_counter() - t0
+    opd = ob.OPd(0.1125, 1.0, 0.01, 0.1, 0.05, 0.9, 10.0, (ob.C.c_int * 8)(8, 8, 8, 45, 8, 8, 30, 20))
+    z = np.zeros((3,) + vol.shape, np.float32)
+    t0 = time.perf_counter()
+    ytv, ytp, ybc = ob.pd_dual32(dims, opd, vol, vol, bw, z, z[0], z[1])
+    t_dual = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ob.pd_primal32(dims, opd, 0, ytp, ytp, bw, ybc, ytv, vol)
+    t_primal = time.perf_counter() - t0
+    t_frame = 2 * t_warp + t_dual + t_primal + V * (t_fp + t_corr + t_bp)
+    t_iter = F * t_frame
+    gups = F * N ** 3 * V / t_iter / 1e9
+    out = {"value": gups, "unit": "GUPS", "cores": threads,
+           "kind": "reference" if use_ref else "port",
+           "sample": (f"one frame at full size: {k} views of FP+correction+voxel BP, 2 warps, dual, primal; "
+                      f"scaled to {F} frames x {V} views; FP and warp are the reference's own code"
+                      + (" (oracle/_ref)" if use_ref else " (restated)") +
+                      f", warp on its hard-coded 4 threads, other loops on {threads} OpenMP threads"),
+           "s_per_iter": t_iter,
+           "per_op_s": {"fp_view": t_fp, "correction_view": t_corr, "bp_voxel_view": t_bp, "warp": t_warp,
+                        "dual": t_dual, "primal": t_primal}}
+    if gpu_check is not None:
+        out["fp64_check"] = gpu_check(ob)
+    return out
+
+
+def fp64_sart_check(ctx, st, args, gmax, n_views: int = 6):
+    """Relative L2 of the GPU SART sweep against the FP64 oracle at full size,
+    on one frame's first `n_views` views, from the current GPU state."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+
+    def run(ob):
+        N, D = args.n, args.det
+        scan = ob.Scan(N, (D, D))
+        vol0 = st["vol"][0].detach().clone()
+        order = stt.frame_order(99, 0, args.frames, 0, args.views)[:n_views]
+        g = vol0.clone()
+        state = torch.zeros((D, D), device=vol0.device)
+        ctx.sart_sweep(g, st["proj"][0].contiguous(), order, 0.3, gmax, 0, state, view_offset=0,
+                       roi_cut=(8, 8, 8, 45, 8, 8, 30, 20))
+        torch.cuda.synchronize()
+        ang = angles_for(args, 0)
+        views = [ob.view_angle(a) for a in ang[:args.views]]
+        roi = ob.roi_mask(scan.dims, (8, 8, 8, 45, 8, 8, 30, 20)).astype(np.float64)
+        ref, _ = ob.sart64(scan, views, order, st["proj"][0].cpu().numpy().astype(np.float64), 0.3, gmax, 0,
+                           vol0.cpu().numpy().astype(np.float64), roi=roi, threads=os.cpu_count() or 1)
+        return {"sart_rel_l2_vs_fp64": ob.rel_l2(g.cpu().numpy(), ref),
+                "sample": f"SART over {n_views} views of frame 0 at {N}^3/{D}^2 from the solver's current state"}
+
+    return run
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference_sample(args, threads)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_reference_sample(args, threads))
+    wall = time.perf_counter() - t0
+    v = statistics.median(r["value"] for r in vals)
+    last = vals[-1]
+    line = {"impl": "reference", "metric": "projector GUPS over a 4D primal-dual iteration", "value": v,
+            "unit": "GUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * F_iter_s(vals), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload(args),
+            "cpu_baseline": {"value": v, "unit": "GUPS", "cores": last["cores"], "kind": last["kind"],
+                             "sample": last["sample"]},
+            "e2e": {"value": v, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "s_per_4d_pd_iter": statistics.median(r["s_per_iter"] for r in vals),
+            "per_op_s": last["per_op_s"], "wall_s": wall}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def F_iter_s(vals):
+    return statistics.median(r["s_per_iter"] for r in vals)
+
+
+# ---------------------------------------------------------------------------
+def run_stt(args):
+    import torch
+
+    import spacetimetomography_b200 as stt
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        args.gpus = world if world > 1 else args.gpus
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    from spacetimetomography_b200.halo import HaloExchange
+
+    ctx, st, gmax, _ = build_problem(args, dev, rank)
+    if world > 1:
+        gmax_t = torch.tensor([gmax], device=dev)
+        dist.all_reduce(gmax_t, op=dist.ReduceOp.MAX)
+        gmax = float(gmax_t.item())
+    F, V, N = args.frames, args.views, args.n
+    pd = pd_params(gmax)
+    bp_mode = 0 if args.bp == "voxel" else 1
+    stream = torch.cuda.Stream(device=dev)
+    halo = HaloExchange(rank, world, st, dist) if world > 1 else None
+
+    def make_solver(mode):
+        return stt.Solver(ctx, st, F, V, pd, alpha=0.3, bp_mode=bp_mode, seed=99, mode=mode,
+                          halo=(halo is not None and rank > 0))
+
+    solver = make_solver(stt.SOLVE_GRAPH)
+
+    def step(s):
+        if halo is not None:
+            halo.exchange_xbar(stream)
+            s.iterate_phase(0, stream)
+            halo.exchange_duals(stream)
+            s.iterate_phase(1, stream)
+        else:
+            s.iterate(1, stream)
+
+    with torch.cuda.stream(stream):
+        st["xbar"].copy_(st["vol"])
+    for _ in range(args.warmup):
+        step(solver)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(solver)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t = e0.elapsed_time(e1) / 1000.0
+    if world > 1:
+        tt = torch.tensor([t], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+        dist.barrier()
+    t_iter = t / args.steps
+    launches_per_iter, _ = solver.stats()
+    value = world * F * N ** 3 * V / t_iter / 1e9
+
+    # ---- dominant kernel: forward projection fused with the correction ----
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    corr = torch.empty((args.det, args.det), device=dev)
+    rl = torch.zeros((args.det, args.det), device=dev)
+    vol0 = st["vol"][0]
+    with torch.cuda.stream(stream):
+        for v in range(3):
+            ctx.fp_correction(vol0, st["proj"][0, v], rl, corr, v, stream=stream)
+        e2.record(stream)
+        for v in range(V):
+            ctx.fp_correction(vol0, st["proj"][0, v], rl, corr, v, stream=stream)
+        e3.record(stream)
+    torch.cuda.synchronize()
+    t_fp = e2.elapsed_time(e3) / 1000.0 / V
+    fp_bytes = 4 * N ** 3 + 12 * args.det * args.det  # volume read + b read, corr write, ray length (per view)
+    peak, peak_kind = peaks()
+    achieved = fp_bytes / t_fp / 1e9
+
+    # ---- the per-view GPU form ----
+    plain = None
+    if not args.no_plain and world == 1:
+        sp = make_solver(stt.SOLVE_PLAIN)
+        sp.iterate(1, stream)  # warm-up
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        sp.iterate(1, stream)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain = p0.elapsed_time(p1) / 1000.0
+        sp.close()
+
+    # ---- end to end through the C ABI with host buffers ----
+    host = {k: st[k].detach().cpu().pin_memory() for k in ("vol", "flow", "proj")}
+    out_host = torch.empty_like(st["vol"][:F], device="cpu").pin_memory()
+    h2d = sum(v.numel() * 4 for v in host.values())
+    d2h = out_host.numel() * 4
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            for k_, v_ in host.items():
+                st[k_].copy_(v_, non_blocking=True)
+            st["xbar"].copy_(st["vol"])
+            for k_ in ("ytv", "ytp", "ybc"):
+                st[k_].zero_()
+        step(solver)
+        with torch.cuda.stream(stream):
+            out_host.copy_(st["vol"][:F], non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ksteps = max(1, min(args.steps, 3))
+    q0.record(stream)
+    for _ in range(ksteps):
+        e2e_step()
+    q1.record(stream)
+    torch.cuda.synchronize()
+    te = q0.elapsed_time(q1) / 1000.0
+    if world > 1:
+        tt = torch.tensor([te], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e_value = world * F * N ** 3 * V / (te / ksteps) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference_sample(args, os.cpu_count() or 1, gpu_check=fp64_sart_check(ctx, st, args, gmax))
+
+    if rank == 0:
+        line = {"metric": "projector GUPS over a 4D primal-dual iteration", "value": value, "unit": "GUPS",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_iter,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": workload(args),
+                "s_per_4d_pd_iter": t_iter,
+                "plain_s_per_iter": plain,
+                "batched_vs_plain": (plain / t_iter) if plain else None,
+                "roofline": {"bound": "hbm", "kernel": "k_fp_corr (forward projection + SART correction)",
+                             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                             "peak_source": peak_kind, "traffic": traffic_per_launch(args),
+                             "algorithmic_bytes_per_launch": fp_bytes, "launch_s": t_fp,
+                             "note": "volume is L2-resident; the kernel is bound by gather (L1/L2) throughput"},
+                "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "steps": ksteps},
+                "gpu_launches": launches_per_iter * args.steps,
+                "launches_per_iter": launches_per_iter,
+                "clocks": clk,
+                "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "cpu_s_per_iter": None if cpu is None else cpu["s_per_iter"],
+                "fp64_check": None if cpu is None else cpu.get("fp64_check")}
+        print(json.dumps(line), flush=True)
+    solver.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_stt(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

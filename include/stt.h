@@ -207,11 +207,17 @@ typedef struct stt_solve_cfg {
     int roi_cut[8];            /* cut of the ROI mask applied after each SART call */
     unsigned long long seed;   /* view-order seed */
     int mode;                  /* stt_solve_mode */
+    /* Frame sharding across GPUs: when `halo` is set, local frame 0 is not the
+     * sequence's first frame; its primal step uses ytp_halo/ybc_halo/flow_halo
+     * (the previous shard's last frame) and xbar[F] holds the next shard's
+     * X_bar[0].  The caller exchanges them between the two phases. */
+    int halo;
 } stt_solve_cfg;
 
 typedef struct stt_pd_state {
     float *vol, *xbar, *xprev, *ytv, *ytp, *ybc;
     const float *flow, *proj;
+    const float *ytp_halo, *ybc_halo, *flow_halo;  /* only read when cfg.halo is set */
 } stt_pd_state;
 
 typedef struct stt_solver stt_solver;
@@ -220,6 +226,11 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
                              stt_solver **out);
 /* Enqueue n_iters iterations on `stream` (the plain mode synchronises it). */
 stt_status stt_solver_iterate(stt_solver *s, int n_iters, void *stream);
+/* One phase of one iteration: phase 0 = view order + every frame's backward
+ * warp and dual step; phase 1 = every frame's forward warp, primal step,
+ * SART, ROI mask and over-relaxation.  Phase 0 then phase 1 equals one
+ * stt_solver_iterate step; sharded solves exchange halos in between. */
+stt_status stt_solver_iterate_phase(stt_solver *s, int phase, void *stream);
 /* Kernel launches per iteration and iterations run so far. */
 stt_status stt_solver_stats(const stt_solver *s, long long *launches_per_iter,
                             unsigned long long *iterations);

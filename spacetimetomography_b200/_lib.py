@@ -41,13 +41,14 @@ class PdParams(C.Structure):
 class SolveCfg(C.Structure):
     _fields_ = [("n_frames", C.c_int), ("views_per_frame", C.c_int), ("bp_mode", C.c_int),
                 ("alpha", C.c_double), ("pd", PdParams), ("roi_cut", C.c_int * 8),
-                ("seed", C.c_ulonglong), ("mode", C.c_int)]
+                ("seed", C.c_ulonglong), ("mode", C.c_int), ("halo", C.c_int)]
 
 
 class PdState(C.Structure):
     _fields_ = [("vol", C.c_void_p), ("xbar", C.c_void_p), ("xprev", C.c_void_p),
                 ("ytv", C.c_void_p), ("ytp", C.c_void_p), ("ybc", C.c_void_p),
-                ("flow", C.c_void_p), ("proj", C.c_void_p)]
+                ("flow", C.c_void_p), ("proj", C.c_void_p), ("ytp_halo", C.c_void_p),
+                ("ybc_halo", C.c_void_p), ("flow_halo", C.c_void_p)]
 
 
 def _load() -> C.CDLL:
@@ -78,6 +79,7 @@ def _load() -> C.CDLL:
         "stt_warp_vjp": [vp, vp, vp, i, f, vp, vp, vp, vp],
         "stt_solver_create": [vp, C.POINTER(SolveCfg), C.POINTER(PdState), C.POINTER(vp)],
         "stt_solver_iterate": [vp, i, vp],
+        "stt_solver_iterate_phase": [vp, i, vp],
         "stt_solver_stats": [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_ulonglong)],
         "stt_solver_destroy": [vp],
         "stt_solver_frame_order": [C.c_ulonglong, C.c_ulonglong, i, i, i, vp],

@@ -227,13 +227,16 @@ class Solver:
 
     def __init__(self, ctx: Context, state: dict, n_frames: int, views_per_frame: int,
                  pd: PdParams, alpha: float = 0.3, bp_mode: int = 0, roi_cut=REFERENCE_CUT,
-                 seed: int = 0, mode: int = SOLVE_GRAPH):
+                 seed: int = 0, mode: int = SOLVE_GRAPH, halo: bool = False):
+        """halo=True: local frame 0 continues a previous shard (state needs
+        ytp_halo, ybc_halo, flow_halo; see spacetimetomography_b200.halo)."""
         self.ctx = ctx
         self.state = state  # keeps the tensors alive
         cfg = SolveCfg(n_frames, views_per_frame, bp_mode, float(alpha), pd.c(),
-                       (C.c_int * 8)(*map(int, roi_cut)), C.c_ulonglong(seed), mode)
-        st = PdState(*[state[k].data_ptr() for k in ("vol", "xbar", "xprev", "ytv", "ytp", "ybc",
-                                                     "flow", "proj")])
+                       (C.c_int * 8)(*map(int, roi_cut)), C.c_ulonglong(seed), mode, int(bool(halo)))
+        keys = ("vol", "xbar", "xprev", "ytv", "ytp", "ybc", "flow", "proj", "ytp_halo", "ybc_halo",
+                "flow_halo")
+        st = PdState(*[state[k].data_ptr() if k in state else None for k in keys])
         h = C.c_void_p()
         rc = lib.stt_solver_create(ctx._h, C.byref(cfg), C.byref(st), C.byref(h))
         if rc != 0:
@@ -242,6 +245,11 @@ class Solver:
 
     def iterate(self, n: int = 1, stream=None):
         rc = lib.stt_solver_iterate(self._h, int(n), _stream(stream))
+        if rc != 0:
+            raise STTError(rc, lib.stt_solver_last_error(self._h).decode())
+
+    def iterate_phase(self, phase: int, stream=None):
+        rc = lib.stt_solver_iterate_phase(self._h, int(phase), _stream(stream))
         if rc != 0:
             raise STTError(rc, lib.stt_solver_last_error(self._h).decode())
 

@@ -108,7 +108,10 @@ struct stt_solver {
     cudaEvent_t ev_fork = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    cudaGraph_t pgraph[2] = {nullptr, nullptr};
+    cudaGraphExec_t pexec[2] = {nullptr, nullptr};
     long long launches_per_iter = 0;
+    long long phase_launches[2] = {0, 0};
     std::string err;
 };
 
@@ -155,18 +158,30 @@ stt_status enqueue_dual(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
 
 // Frame f's primal step (ST_Tomography.cpp:536-578): forward warp of
 // Y_bc[f-1] along flow[f-1] for f > 0, then the fused primal kernel.
+// With a halo, local frame 0 continues the previous shard: its "f-1" terms
+// come from ytp_halo / ybc_halo / flow_halo.
 stt_status enqueue_primal(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
     const int d[3] = {s->g->nx, s->g->ny, s->g->nz};
     const size_t n = s->n;
     float *fw = s->warpbuf + f * n;
+    const bool first = (f == 0) && !s->cfg.halo;
+    const float *ytp_prev = nullptr, *ybc_prev = nullptr, *flow_prev = nullptr;
     if (f > 0) {
-        SCUDA(s, stt::launch_warp(d, s->st.flow + (size_t)(f - 1) * 3 * n, s->st.ybc + (f - 1) * n, 1, 1.0f, fw, cs),
-              "warp (primal)");
+        ytp_prev = s->st.ytp + (f - 1) * n;
+        ybc_prev = s->st.ybc + (f - 1) * n;
+        flow_prev = s->st.flow + (size_t)(f - 1) * 3 * n;
+    } else if (s->cfg.halo) {
+        ytp_prev = s->st.ytp_halo;
+        ybc_prev = s->st.ybc_halo;
+        flow_prev = s->st.flow_halo;
+    }
+    if (!first) {
+        SCUDA(s, stt::launch_warp(d, flow_prev, ybc_prev, 1, 1.0f, fw, cs), "warp (primal)");
         ++nl;
     }
-    SCUDA(s, stt::launch_pd_primal(d, pdp(s->cfg.pd), f == 0, f > 0 ? s->st.ytp + (f - 1) * n : nullptr,
-                                   s->st.ytp + f * n, f > 0 ? fw : nullptr, s->st.ybc + f * n,
-                                   s->st.ytv + (size_t)f * 3 * n, s->st.vol + f * n, s->st.xprev + f * n, cs),
+    SCUDA(s, stt::launch_pd_primal(d, pdp(s->cfg.pd), first, ytp_prev, s->st.ytp + f * n, first ? nullptr : fw,
+                                   s->st.ybc + f * n, s->st.ytv + (size_t)f * 3 * n, s->st.vol + f * n,
+                                   s->st.xprev + f * n, cs),
           "pd_primal");
     ++nl;
     return STT_OK;
@@ -202,7 +217,9 @@ stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long
     return STT_OK;
 }
 
-stt_status enqueue_batched(stt_solver *s, cudaStream_t main, long long &nl) {
+// Phase 0: the view order, then every frame's dual on its own stream.  With
+// `join` the frame streams rejoin `main` (phases run separately).
+stt_status enqueue_phase0(stt_solver *s, cudaStream_t main, long long &nl, bool join) {
     const int F = s->F;
     SCUDA(s, stt::launch_make_perm(s->cfg.seed, s->counter, F, s->V, s->perm, main), "make_perm");
     ++nl;
@@ -212,6 +229,19 @@ stt_status enqueue_batched(stt_solver *s, cudaStream_t main, long long &nl) {
         stt_status st = enqueue_dual(s, f, s->streams[f], nl);
         if (st) return st;
         SCUDA(s, cudaEventRecord(s->ev_dual[f], s->streams[f]), "event record");
+        if (join) SCUDA(s, cudaStreamWaitEvent(main, s->ev_dual[f], 0), "stream wait");
+    }
+    return STT_OK;
+}
+
+// Phase 1: per frame, after the previous frame's dual, the primal step, SART
+// and the ROI/over-relaxation; the frame chains rejoin `main`.  With `fork`
+// they first wait for `main` (work the caller queued between the phases).
+stt_status enqueue_phase1(stt_solver *s, cudaStream_t main, long long &nl, bool fork) {
+    const int F = s->F;
+    if (fork) {
+        SCUDA(s, cudaEventRecord(s->ev_fork, main), "event record");
+        for (int f = 0; f < F; ++f) SCUDA(s, cudaStreamWaitEvent(s->streams[f], s->ev_fork, 0), "stream wait");
     }
     for (int f = 0; f < F; ++f) {
         cudaStream_t cs = s->streams[f];
@@ -225,19 +255,47 @@ stt_status enqueue_batched(stt_solver *s, cudaStream_t main, long long &nl) {
     return STT_OK;
 }
 
+stt_status enqueue_batched(stt_solver *s, cudaStream_t main, long long &nl) {
+    stt_status st = enqueue_phase0(s, main, nl, false);
+    if (st) return st;
+    return enqueue_phase1(s, main, nl, false);
+}
+
 // The per-view form: frame by frame as the reference loops, each view's
 // forward projection, correction and backprojection as separate launches,
 // and a host synchronisation after every view.
-stt_status run_plain(stt_solver *s, cudaStream_t cs, long long &nl) {
+stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl);
+
+// phase -1: the reference's interleaved frame loop; phase 0: every dual;
+// phase 1: every frame's primal, SART and over-relaxation.
+stt_status run_plain(stt_solver *s, cudaStream_t cs, long long &nl, int phase) {
+    const int F = s->F;
+    for (int f = 0; f < F; ++f) {
+        stt_status st = STT_OK;
+        if (phase <= 0 && (st = enqueue_dual(s, f, cs, nl))) return st;
+        if (phase == 0) continue;
+        if ((st = enqueue_primal(s, f, cs, nl))) return st;
+        if ((st = plain_frame_tail(s, f, cs, nl))) return st;
+    }
+    if (phase == 0) {
+        SCUDA(s, cudaStreamSynchronize(cs), "synchronize");
+        return STT_OK;
+    }
+    ++s->host_iter;
+    // keep the device counter in step so that the modes can be mixed
+    SCUDA(s, cudaMemcpyAsync(s->counter, &s->host_iter, sizeof(unsigned long long), cudaMemcpyHostToDevice, cs),
+          "counter update");
+    SCUDA(s, cudaStreamSynchronize(cs), "synchronize");
+    return STT_OK;
+}
+
+stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
     const stt::GeomDev &g = *s->g;
     const int F = s->F, V = s->V;
     const int d[3] = {g.nx, g.ny, g.nz};
     std::vector<int> perm(V);
     const int voxel = s->cfg.bp_mode == 0;
-    for (int f = 0; f < F; ++f) {
-        stt_status st = enqueue_dual(s, f, cs, nl);
-        if (st) return st;
-        if ((st = enqueue_primal(s, f, cs, nl))) return st;
+    {
         stt::host_perm(s->cfg.seed, s->host_iter, F, f, V, perm.data());
         float *vol = s->st.vol + f * s->n;
         float *corr = s->corr + f * s->npix;
@@ -268,11 +326,6 @@ stt_status run_plain(stt_solver *s, cudaStream_t cs, long long &nl) {
               "roi_apply");
         ++nl;
     }
-    ++s->host_iter;
-    // keep the device counter in step so that the modes can be mixed
-    SCUDA(s, cudaMemcpyAsync(s->counter, &s->host_iter, sizeof(unsigned long long), cudaMemcpyHostToDevice, cs),
-          "counter update");
-    SCUDA(s, cudaStreamSynchronize(cs), "synchronize");
     return STT_OK;
 }
 
@@ -290,6 +343,8 @@ stt_status alloc(stt_solver *s, T *&p, size_t count, const char *what) {
 
 extern "C" {
 
+stt_status stt_solver_iterate_phase(stt_solver *s, int phase, void *stream);
+
 stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_pd_state *state,
                              stt_solver **out) {
     if (!ctx || !cfg || !state || !out) return STT_ERR_INVALID;
@@ -305,6 +360,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     if (!state->vol || !state->xbar || !state->xprev || !state->ytv || !state->ytp || !state->ybc ||
         !state->flow || !state->proj)
         return STT_ERR_INVALID;
+    if (cfg->halo && (!state->ytp_halo || !state->ybc_halo || !state->flow_halo)) return STT_ERR_INVALID;
     stt_solver *s = new stt_solver();
     s->ctx = ctx;
     s->cfg = *cfg;
@@ -355,8 +411,13 @@ stt_status stt_solver_iterate(stt_solver *s, int n_iters, void *stream) {
     for (int it = 0; it < n_iters; ++it) {
         long long nl = 0;
         stt_status st = STT_OK;
+        if (s->cfg.halo) {  // a sharded solve runs its two phases (the caller exchanges halos in between)
+            if ((st = stt_solver_iterate_phase(s, 0, stream))) return st;
+            if ((st = stt_solver_iterate_phase(s, 1, stream))) return st;
+            continue;
+        }
         if (s->cfg.mode == STT_SOLVE_PLAIN) {
-            st = run_plain(s, cs, nl);
+            st = run_plain(s, cs, nl, -1);
         } else if (s->cfg.mode == STT_SOLVE_STREAMS) {
             st = enqueue_batched(s, cs, nl);
             ++s->host_iter;
@@ -388,6 +449,44 @@ stt_status stt_solver_iterate(stt_solver *s, int n_iters, void *stream) {
     return STT_OK;
 }
 
+stt_status stt_solver_iterate_phase(stt_solver *s, int phase, void *stream) {
+    if (!s || (phase != 0 && phase != 1)) return STT_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+    long long nl = 0;
+    stt_status st = STT_OK;
+    if (s->cfg.mode == STT_SOLVE_PLAIN) {
+        st = run_plain(s, cs, nl, phase);
+    } else if (s->cfg.mode == STT_SOLVE_STREAMS) {
+        st = phase == 0 ? enqueue_phase0(s, cs, nl, true) : enqueue_phase1(s, cs, nl, true);
+        if (phase == 1) ++s->host_iter;
+    } else {
+        if (!s->pexec[phase]) {
+            cudaStream_t cap;
+            SCUDA(s, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "capture stream");
+            SCUDA(s, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+            st = phase == 0 ? enqueue_phase0(s, cap, nl, true) : enqueue_phase1(s, cap, nl, true);
+            cudaGraph_t graph = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+            cudaStreamDestroy(cap);
+            if (st) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            if (ce != cudaSuccess) return sfail(s, STT_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ce));
+            s->pgraph[phase] = graph;
+            SCUDA(s, cudaGraphInstantiate(&s->pexec[phase], graph, 0), "graph instantiate");
+            s->phase_launches[phase] = nl;
+        }
+        SCUDA(s, cudaGraphLaunch(s->pexec[phase], cs), "graph launch");
+        nl = s->phase_launches[phase];
+        if (phase == 1) ++s->host_iter;
+    }
+    if (st) return st;
+    s->phase_launches[phase] = nl;
+    s->launches_per_iter = s->phase_launches[0] + s->phase_launches[1];
+    return STT_OK;
+}
+
 stt_status stt_solver_stats(const stt_solver *s, long long *launches_per_iter, unsigned long long *iterations) {
     if (!s) return STT_ERR_INVALID;
     if (launches_per_iter) *launches_per_iter = s->launches_per_iter;
@@ -401,6 +500,10 @@ stt_status stt_solver_destroy(stt_solver *s) {
     if (!s) return STT_OK;
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->graph) cudaGraphDestroy(s->graph);
+    for (int p = 0; p < 2; ++p) {
+        if (s->pexec[p]) cudaGraphExecDestroy(s->pexec[p]);
+        if (s->pgraph[p]) cudaGraphDestroy(s->pgraph[p]);
+    }
     for (auto st : s->streams)
         if (st) cudaStreamDestroy(st);
     for (auto e : s->ev_dual)
