@@ -125,6 +125,21 @@ stt_status stt_bp_voxel(stt_ctx *ctx, const float *corr, float *vol, double alph
 stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, int view,
                       void *stream);
 
+/* Ray-driven backprojection that allocates no device memory.  No counterpart
+ * in the reference: it is stt_bp_ray for callers that cannot let a library
+ * call cudaMalloc (a plugin whose host application owns all device memory, a
+ * real-time loop that cannot take cudaMalloc's synchronisation).  Its
+ * accumulators live in a fixed array compiled into libstt.so,
+ * STT_BP_RAY_NOALLOC_MAX_VOXELS float2 entries (16 MiB per GPU that loads the
+ * library, held until exit); larger volumes are rejected with
+ * STT_ERR_INVALID.  Calls on one device share that array: calls that overlap
+ * on the GPU race, so serialise them.  Every call clears the part it uses
+ * first.  The first call on a device looks up the array's device address;
+ * make it before any stream capture.  Same arguments and result as stt_bp_ray. */
+#define STT_BP_RAY_NOALLOC_MAX_VOXELS (1 << 21)
+stt_status stt_bp_ray_noalloc(stt_ctx *ctx, const float *corr, float *vol, float gmax, int view,
+                              void *stream);
+
 /* ---- SART (ST_Tomography.cpp:616-808) -------------------------------------
  * One SART call for one frame: for i in 0..nperm-1, view = view_offset +
  * perm[i] (perm is HOST): FP + correction, then backprojection (bp_mode 0

@@ -27,7 +27,7 @@ LIB = PKG / "libstt.so"
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
 
-KERNEL_SOURCES = ["stt_capi.cu", "stt_solver.cu", "k_project.cu", "k_voxel.cu", "k_warp.cu"]
+KERNEL_SOURCES = ["stt_capi.cu", "stt_solver.cu", "stt_noalloc.cu", "k_project.cu", "k_voxel.cu", "k_warp.cu"]
 
 
 def _nvcc() -> str:

@@ -448,6 +448,11 @@ static stt_status check_warp_args(const int *dim, const float *vel, const float 
     return STT_OK;
 }
 
+// Records an error on a context for code outside this file (not part of the public header).
+stt_status stt_internal_set_error(stt_ctx *ctx, stt_status st, const char *msg) {
+    return fail(ctx, st, msg ? msg : "");
+}
+
 // Solver access to the context's geometry (not part of the public header).
 stt_status stt_internal_geom(stt_ctx *ctx, const void **geom, const void **views) {
     stt_status st = need_geom(ctx);
