@@ -69,6 +69,9 @@ O.orc_warp_f64.argtypes = [_vp, _vp, _vp, _i, _d, _vp, _i]
 O.orc_warp_vjp_f64.argtypes = [_vp, _vp, _vp, _i, _d, _vp, _vp, _vp]
 O.orc_cubic_at_f32.argtypes = [_vp, _vp, _f, _f, _f]
 O.orc_cubic_at_f32.restype = _f
+O.orc_cubic_at_f64.argtypes = [_vp, _vp, _d, _d, _d]
+O.orc_cubic_at_f64.restype = _d
+O.orc_view_matrices_f32.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp]
 
 REF = None
 if REF_SO.exists():
@@ -375,3 +378,11 @@ def pd_iteration(scan, angles, st, F, V, pp, pd_cut, roi_cut, alpha, bp_mode, or
                                              bp_mode, st["vol"][f], raylen=raylen[f], roi=roi, gmode=1)
             st["xbar"][f] = pd_extrapolate32(dims, pd_cut, st["vol"][f], st["xprev"][f], st["xbar"][f])
     return st
+
+
+def view_matrices32(scan: Scan, view: OView) -> np.ndarray:
+    """P2M, M2V, model-view, V2M of the reference's FP32 pipeline (64 floats)."""
+    out = np.zeros(64, np.float32)
+    g = scan.ogeom()
+    O.orc_view_matrices_f32(C.byref(g), C.byref(view), P(out))
+    return out
