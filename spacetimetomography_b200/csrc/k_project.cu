@@ -2,12 +2,15 @@
 // fused with the SART correction, the ray-driven backprojection scatter and
 // the exact adjoint A^T.
 //
-// One thread per detector pixel.  A 128-thread block covers a 16x8 pixel
-// tile; each warp covers an 8x4 sub-tile so that the 32 rays of a warp stay
-// close together in the volume and their trilinear gathers share L1 lines.
-// The volume is read through the read-only path (ld.global.nc); at the sizes
-// of the headline workloads (256^3 fp32 = 64 MiB) it stays resident in the
-// 126 MB L2.
+// One thread per detector pixel.  A 128-thread block covers 32x4 pixels: each
+// warp is 32 consecutive detector columns of one row, so at every step its 32
+// samples lie along the detector's u axis in the volume.  For views whose rays
+// run mostly along z, u maps to the volume's x axis, which is contiguous in
+// memory; for views whose rays run mostly along x, u maps to z and the forward
+// projector gathers from a z-fastest transposed copy (ViewRec::layout), so
+// either way a warp's gathers touch few cache lines.  The volume is read
+// through the read-only path (ld.global.nc); at the headline sizes (256^3 fp32
+// = 64 MiB) it stays resident in the 126 MB L2.
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
 
@@ -16,31 +19,44 @@ namespace stt {
 namespace {
 
 __device__ __forceinline__ bool tile_pixel(const GeomDev &g, int &i, int &j) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    i = blockIdx.x * 16 + (w & 1) * 8 + (lane & 7);
-    j = blockIdx.y * 8 + (w >> 1) * 4 + (lane >> 3);
+    i = blockIdx.x * 32 + (threadIdx.x & 31);
+    j = blockIdx.y * 4 + (threadIdx.x >> 5);
     return i < g.W && j < g.H;
+}
+
+// Source and strides of the forward projector's gathers for one view.
+__device__ __forceinline__ const float *fp_source(const GeomDev &g, const ViewRec &v, const float *vol,
+                                                  const float *vol_t, Strides &st) {
+    if (vol_t && v.layout == 1) {
+        st = zyx_strides(g);
+        return vol_t;
+    }
+    st = xyz_strides(g);
+    return vol;
 }
 
 // GenerateImage_MT (S/ImageFormationModel/TypicalRayProducer.core.h:168-224)
 // for views [view0, view0 + gridDim.z).
 __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__restrict__ views,
-                                            const float *__restrict__ vol, int view0,
-                                            float *__restrict__ proj, float *__restrict__ raylen,
+                                            const float *__restrict__ vol, const float *__restrict__ vol_t,
+                                            int view0, float *__restrict__ proj, float *__restrict__ raylen,
                                             float *__restrict__ weight) {
     int i, j;
     if (!tile_pixel(g, i, j)) return;
     const int v = blockIdx.z;
+    const ViewRec &vr = views[view0 + v];
+    Strides st;
+    const float *src = fp_source(g, vr, vol, vol_t, st);
     Ray r;
-    make_ray(g, views[view0 + v], i, j, r);
+    make_ray(g, vr, i, j, r);
     Kahan acc{0.0f, 0.0f};
     int count = 0;
     const bool hit = r.tnear < r.tfar;
     if (hit) {
         march(g, r, [&](const float p[3]) {
             Taps t;
-            make_taps(g, p, t);
-            acc.add(tri_value(vol, t) * g.sd);
+            make_taps(g, p, t, st);
+            acc.add(tri_value(src, t) * g.sd);
             ++count;
         });
     }
@@ -56,8 +72,8 @@ __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__re
 // updated where the ray hits, kept where it misses; with no state buffer
 // (ray-based SART, whose producer is reset after every view) a miss gives L = 0.
 __global__ void __launch_bounds__(128) k_fp_corr(const GeomDev g, const ViewRec *__restrict__ views,
-                                                 const float *__restrict__ vol, const ViewSel sel,
-                                                 const float *__restrict__ b_stack,
+                                                 const float *__restrict__ vol, const float *__restrict__ vol_t,
+                                                 const ViewSel sel, const float *__restrict__ b_stack,
                                                  float *__restrict__ raylen_state,
                                                  float *__restrict__ corr) {
     int i, j;
@@ -65,16 +81,19 @@ __global__ void __launch_bounds__(128) k_fp_corr(const GeomDev g, const ViewRec 
     int local;
     const int view = sel_view(sel, local);
     const float *b = b_stack + (size_t)local * g.W * g.H;
+    const ViewRec &vr = views[view];
+    Strides st;
+    const float *src = fp_source(g, vr, vol, vol_t, st);
     Ray r;
-    make_ray(g, views[view], i, j, r);
+    make_ray(g, vr, i, j, r);
     Kahan acc{0.0f, 0.0f};
     const size_t pix = i + (size_t)j * g.W;
     float L;
     if (r.tnear < r.tfar) {
         march(g, r, [&](const float p[3]) {
             Taps t;
-            make_taps(g, p, t);
-            acc.add(tri_value(vol, t) * g.sd);
+            make_taps(g, p, t, st);
+            acc.add(tri_value(src, t) * g.sd);
         });
         L = r.tfar - r.tnear;
         if (raylen_state) raylen_state[pix] = L;
@@ -157,6 +176,39 @@ __global__ void k_correction(long long n, const float *__restrict__ b, const flo
         corr[k] = __fdiv_rn(__fsub_rn(b[k], ax[k]), __fadd_rn(raylen ? raylen[k] : 0.0f, 1.0f));
 }
 
+// z-fastest copy of an x-fastest volume: out[z + y*nz + x*nz*ny] = in[x + y*nx + z*nx*ny],
+// one (x, z) plane of fixed y per block row, 32x32 tiles through shared memory.
+__device__ __forceinline__ void transpose_tile(int nx, int ny, int nz, const float *__restrict__ in,
+                                               float *__restrict__ out) {
+    __shared__ float tile[32][33];
+    const int x0 = blockIdx.x * 32, z0 = blockIdx.y * 32, y = blockIdx.z;
+    const size_t nxy = (size_t)nx * ny, nzy = (size_t)nz * ny;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int z = z0 + r, x = x0 + threadIdx.x;
+        if (x < nx && z < nz) tile[r][threadIdx.x] = __ldg(in + x + (size_t)y * nx + z * nxy);
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int x = x0 + r, z = z0 + threadIdx.x;
+        if (x < nx && z < nz) out[z + (size_t)y * nz + x * nzy] = tile[threadIdx.x][r];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_transpose_xz(int nx, int ny, int nz, const float *__restrict__ in,
+                                                      float *__restrict__ out) {
+    transpose_tile(nx, ny, nz, in, out);
+}
+
+// The transpose, only if the selected view gathers from the z-fastest copy
+// (the choice is read on the device, so a captured graph can hold it).
+__global__ void __launch_bounds__(256) k_transpose_for_view(int nx, int ny, int nz,
+                                                            const ViewRec *__restrict__ views, const ViewSel sel,
+                                                            const float *__restrict__ in, float *__restrict__ out) {
+    int local;
+    if (views[sel_view(sel, local)].layout != 1) return;
+    transpose_tile(nx, ny, nz, in, out);
+}
+
 __global__ void k_fill_zero(long long n, float *__restrict__ p) {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x)
@@ -164,8 +216,10 @@ __global__ void k_fill_zero(long long n, float *__restrict__ p) {
 }
 
 dim3 ray_grid(const GeomDev &g, int nviews) {
-    return dim3((g.W + 15) / 16, (g.H + 7) / 8, nviews);
+    return dim3((g.W + 31) / 32, (g.H + 3) / 4, nviews);
 }
+
+dim3 transpose_grid(const GeomDev &g) { return dim3((g.nx + 31) / 32, (g.nz + 31) / 32, g.ny); }
 
 }  // namespace
 
@@ -175,15 +229,27 @@ int grid_stride_blocks(long long n, int threads) {
     return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
 
-cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, int view0,
+cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, int view0,
                       int nviews, float *proj, float *raylen, float *weight, cudaStream_t s) {
-    k_fp<<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, view0, proj, raylen, weight);
+    k_fp<<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen, weight);
     return cudaGetLastError();
 }
 
-cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const ViewSel &sel,
-                           const float *b_stack, float *raylen_state, float *corr, cudaStream_t s) {
-    k_fp_corr<<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, sel, b_stack, raylen_state, corr);
+cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
+                           const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
+                           cudaStream_t s) {
+    k_fp_corr<<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transpose(const GeomDev &g, const float *in, float *out, cudaStream_t s) {
+    k_transpose_xz<<<transpose_grid(g), dim3(32, 8), 0, s>>>(g.nx, g.ny, g.nz, in, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *in,
+                                      float *out, cudaStream_t s) {
+    k_transpose_for_view<<<transpose_grid(g), dim3(32, 8), 0, s>>>(g.nx, g.ny, g.nz, views, sel, in, out);
     return cudaGetLastError();
 }
 

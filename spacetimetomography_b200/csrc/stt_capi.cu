@@ -25,6 +25,8 @@ struct stt_ctx {
     size_t acc_n = 0;
     float *corr = nullptr;  // W*H correction image used by stt_sart_sweep
     size_t corr_n = 0;
+    float *volt = nullptr;  // z-fastest copy of the volume for views gathering along x
+    size_t volt_n = 0;
 };
 
 namespace {
@@ -97,7 +99,9 @@ void build_view(const stt_geometry &g, double theta, stt::ViewRec &v) {
         }
         v.b[r] = (float)b;
     }
-    for (int k = 0; k < 4; ++k) v.pad[k] = 0.0f;
+    // gather from the z-fastest copy when the central ray runs more along x than z
+    v.layout = std::fabs(s) > std::fabs(c) ? 1 : 0;
+    for (int k = 0; k < 3; ++k) v.pad[k] = 0.0f;
 }
 
 template <typename T>
@@ -140,6 +144,7 @@ stt_status stt_destroy(stt_ctx *ctx) {
     if (ctx->views_d) cudaFree(ctx->views_d);
     if (ctx->acc) cudaFree(ctx->acc);
     if (ctx->corr) cudaFree(ctx->corr);
+    if (ctx->volt) cudaFree(ctx->volt);
     delete ctx;
     return STT_OK;
 }
@@ -258,6 +263,21 @@ stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g) {
     return STT_OK;
 }
 
+// When a view in [view0, view0+nviews) gathers from the z-fastest copy,
+// refresh the context's copy of `vol` and return it in *volt.
+static stt_status transposed_if_needed(stt_ctx *ctx, const float *vol, int view0, int nviews, cudaStream_t s,
+                                       const float **volt) {
+    *volt = nullptr;
+    bool any = false;
+    for (int v = view0; v < view0 + nviews && !any; ++v) any = ctx->views_h[v].layout == 1;
+    if (!any) return STT_OK;
+    stt_status st = ensure(ctx, ctx->volt, ctx->volt_n, (size_t)nvox(ctx), "transposed volume");
+    if (st) return st;
+    STT_CUDA(ctx, stt::launch_transpose(ctx->g, vol, ctx->volt, s), "k_transpose launch");
+    *volt = ctx->volt;
+    return STT_OK;
+}
+
 static stt_status check_views(stt_ctx *ctx, int view0, int nviews) {
     if (view0 < 0 || nviews < 0 || view0 + nviews > ctx->g.n_views)
         return fail(ctx, STT_ERR_INVALID, "view range outside the geometry's view list");
@@ -272,7 +292,9 @@ stt_status stt_fp(stt_ctx *ctx, const float *vol, float *proj, float *raylen, fl
     if ((st = check_views(ctx, view0, nviews))) return st;
     if (nviews == 0) return STT_OK;
     if ((st = set_device(ctx))) return st;
-    STT_CUDA(ctx, stt::launch_fp(ctx->g, ctx->views_d, vol, view0, nviews, proj, raylen, weight, S(stream)),
+    const float *volt = nullptr;
+    if ((st = transposed_if_needed(ctx, vol, view0, nviews, S(stream), &volt))) return st;
+    STT_CUDA(ctx, stt::launch_fp(ctx->g, ctx->views_d, vol, volt, view0, nviews, proj, raylen, weight, S(stream)),
              "k_fp launch");
     return STT_OK;
 }
@@ -285,7 +307,9 @@ stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, flo
     if ((st = check_views(ctx, view, 1))) return st;
     if ((st = set_device(ctx))) return st;
     const stt::ViewSel sel{view, nullptr, 0, view};
-    STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, sel, b, raylen_state, corr, S(stream)),
+    const float *volt = nullptr;
+    if ((st = transposed_if_needed(ctx, vol, view, 1, S(stream), &volt))) return st;
+    STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, b, raylen_state, corr, S(stream)),
              "k_fp_corr launch");
     return STT_OK;
 }
@@ -357,9 +381,11 @@ stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, con
     if (bp_mode == 1 && (st = ensure_acc(ctx, s))) return st;
     for (int i = 0; i < nperm; ++i) {
         const stt::ViewSel sel{view_offset + perm[i], nullptr, 0, view_offset};
+        const float *volt = nullptr;
+        if ((st = transposed_if_needed(ctx, vol, view_offset + perm[i], 1, s, &volt))) return st;
         // ray-based mode: TypicalRayProducer::Initial zeroes the ray lengths
         // after every view, so missed rays see L = 0 (no sticky state)
-        STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, sel, proj_stack,
+        STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, proj_stack,
                                           bp_mode == 0 ? raylen_state : nullptr, ctx->corr, s),
                  "k_fp_corr launch");
         if (bp_mode == 0)

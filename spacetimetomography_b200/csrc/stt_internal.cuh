@@ -18,6 +18,10 @@ namespace stt {
 //   Voxel projection (ST_Tomography.cpp:698-703): camera coordinates of voxel
 //     (x,y,z) are cam = A*(x,y,z) + b (FP32, voxel spacing and centring folded
 //     in); the pixel is (W-1)/2 + cam.x/(-cam.z) * sdd/ds, likewise in y.
+// `layout` selects the volume copy the forward projector gathers from: 0 the
+// x-fastest volume, 1 a z-fastest transposed copy, chosen on the host for views
+// whose central ray runs more along x than along z, so that a warp's 32 rays
+// (consecutive detector columns) sample consecutive addresses.
 struct ViewRec {
     double src[3];
     double det0[3];
@@ -25,7 +29,8 @@ struct ViewRec {
     double dv[3];
     float A[9];
     float b[3];
-    float pad[4];
+    int layout;
+    float pad[3];
 };
 
 struct GeomDev {
@@ -109,13 +114,23 @@ __device__ __forceinline__ void make_ray(const GeomDev &g, const ViewRec &v, int
 
 // Clamped trilinear tap set (S/ImageFormationModel/SingleScalarVolume.core.h:87-120):
 // position clamped to [0, dims-1], base truncated, +1 neighbours clamped.
+// Element strides of the x, y, z axes: (1, nx, nx*ny) for the volume, or
+// (nz*ny, nz, 1) for its z-fastest transposed copy; the values gathered and
+// the interpolation order are the same for both.
+struct Strides {
+    int sx, sy, sz;
+};
+
+__device__ __forceinline__ Strides xyz_strides(const GeomDev &g) { return Strides{1, g.nx, g.nx * g.ny}; }
+__device__ __forceinline__ Strides zyx_strides(const GeomDev &g) { return Strides{g.nz * g.ny, g.nz, 1}; }
+
 struct Taps {
     long long base;
     int dx, dy, dz;   // neighbour offsets (0 at the upper edge)
     float fx, fy, fz;
 };
 
-__device__ __forceinline__ void make_taps(const GeomDev &g, const float p[3], Taps &t) {
+__device__ __forceinline__ void make_taps(const GeomDev &g, const float p[3], Taps &t, const Strides &st) {
     float px = rmax(rmin(p[0], (float)(g.nx - 1)), 0.0f);
     float py = rmax(rmin(p[1], (float)(g.ny - 1)), 0.0f);
     float pz = rmax(rmin(p[2], (float)(g.nz - 1)), 0.0f);
@@ -123,11 +138,14 @@ __device__ __forceinline__ void make_taps(const GeomDev &g, const float p[3], Ta
     t.fx = px - (float)ix;
     t.fy = py - (float)iy;
     t.fz = pz - (float)iz;
-    const long long nxy = (long long)g.nx * g.ny;
-    t.base = ix + (long long)iy * g.nx + (long long)iz * nxy;
-    t.dx = (ix < g.nx - 1) ? 1 : 0;
-    t.dy = (iy < g.ny - 1) ? g.nx : 0;
-    t.dz = (iz < g.nz - 1) ? (int)nxy : 0;
+    t.base = (long long)ix * st.sx + (long long)iy * st.sy + (long long)iz * st.sz;
+    t.dx = (ix < g.nx - 1) ? st.sx : 0;
+    t.dy = (iy < g.ny - 1) ? st.sy : 0;
+    t.dz = (iz < g.nz - 1) ? st.sz : 0;
+}
+
+__device__ __forceinline__ void make_taps(const GeomDev &g, const float p[3], Taps &t) {
+    make_taps(g, p, t, xyz_strides(g));
 }
 
 // x, then y, then z as the reference interpolates.

@@ -16,10 +16,14 @@ struct PdParams {
 
 int grid_stride_blocks(long long n, int threads);
 
-cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, int view0,
+cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, int view0,
                       int nviews, float *proj, float *raylen, float *weight, cudaStream_t s);
-cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const ViewSel &sel,
-                           const float *b_stack, float *raylen_state, float *corr, cudaStream_t s);
+cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
+                           const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
+                           cudaStream_t s);
+cudaError_t launch_transpose(const GeomDev &g, const float *in, float *out, cudaStream_t s);
+cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *in,
+                                      float *out, cudaStream_t s);
 cudaError_t launch_correction(long long n, const float *b, const float *ax, const float *raylen,
                               float *corr, cudaStream_t s);
 cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,

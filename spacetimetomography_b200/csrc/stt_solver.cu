@@ -98,6 +98,7 @@ struct stt_solver {
     float *warpbuf = nullptr;  // F volumes: backward-warped X_bar[f+1], then forward-warped Y_bc[f-1]
     float *corr = nullptr;     // F correction images
     float *ax = nullptr;       // plain form: forward projection image
+    float *volt = nullptr;     // F z-fastest volume copies (views gathering along x)
     float *raylen = nullptr;   // F sticky ray-length images
     float2 *acc = nullptr;     // ray-based BP accumulators, F volumes
     int *perm = nullptr;       // F x V device view order
@@ -197,10 +198,14 @@ stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long
     float *corr = s->corr + f * s->npix;
     const float *stack = s->st.proj + (size_t)f * V * s->npix;
     const int voxel = s->cfg.bp_mode == 0;
+    float *volt = s->volt + f * s->n;
     for (int i = 0; i < V; ++i) {
         const stt::ViewSel sel{0, s->perm + (size_t)f * V, i, f * V};
-        SCUDA(s, stt::launch_fp_corr(g, s->views, vol, sel, stack, voxel ? s->raylen + f * s->npix : nullptr, corr, cs),
+        SCUDA(s, stt::launch_transpose_for_view(g, s->views, sel, vol, volt, cs), "transpose");
+        SCUDA(s, stt::launch_fp_corr(g, s->views, vol, volt, sel, stack, voxel ? s->raylen + f * s->npix : nullptr,
+                                     corr, cs),
               "fp_corr");
+        ++nl;
         if (voxel)
             SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs),
                   "bp_voxel");
@@ -304,8 +309,11 @@ stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl
             const int view = f * V + perm[i];
             const float *b = s->st.proj + ((size_t)f * V + perm[i]) * s->npix;
             const stt::ViewSel sel{view, nullptr, 0, view};
+            float *volt = s->volt + f * s->n;
+            SCUDA(s, stt::launch_transpose_for_view(g, s->views, sel, vol, volt, cs), "transpose");
+            ++nl;
             if (voxel) {
-                SCUDA(s, stt::launch_fp(g, s->views, vol, view, 1, s->ax, rl, nullptr, cs), "fp");
+                SCUDA(s, stt::launch_fp(g, s->views, vol, volt, view, 1, s->ax, rl, nullptr, cs), "fp");
                 SCUDA(s, stt::launch_correction((long long)s->npix, b, s->ax, rl, corr, cs), "correction");
                 SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs),
                       "bp_voxel");
@@ -313,7 +321,7 @@ stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl
             } else {
                 // ray-based: the producer is reset after every view (L = 0 on a miss)
                 SCUDA(s, stt::launch_fill_zero(rl, (long long)s->npix, cs), "fill");
-                SCUDA(s, stt::launch_fp(g, s->views, vol, view, 1, s->ax, rl, nullptr, cs), "fp");
+                SCUDA(s, stt::launch_fp(g, s->views, vol, volt, view, 1, s->ax, rl, nullptr, cs), "fp");
                 SCUDA(s, stt::launch_correction((long long)s->npix, b, s->ax, rl, corr, cs), "correction");
                 SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs),
                       "bp_ray");
@@ -376,6 +384,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     if (!e) e = alloc(s, s->warpbuf, (size_t)F * s->n, "warp buffers");
     if (!e) e = alloc(s, s->corr, (size_t)F * s->npix, "corrections");
     if (!e) e = alloc(s, s->ax, s->npix, "projection");
+    if (!e) e = alloc(s, s->volt, (size_t)F * s->n, "transposed volumes");
     if (!e) e = alloc(s, s->raylen, (size_t)F * s->npix, "ray lengths");
     if (!e) e = alloc(s, s->perm, (size_t)F * s->V, "view order");
     if (!e) e = alloc(s, s->counter, 1, "iteration counter");
@@ -514,6 +523,7 @@ stt_status stt_solver_destroy(stt_solver *s) {
     cudaFree(s->warpbuf);
     cudaFree(s->corr);
     cudaFree(s->ax);
+    cudaFree(s->volt);
     cudaFree(s->raylen);
     cudaFree(s->acc);
     cudaFree(s->perm);
