@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--bp", choices=["voxel", "ray"], default="voxel")
     ap.add_argument("--no-plain", action="store_true", help="skip the per-view (plain) comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-flow", action="store_true", help="skip the optical-flow leg")
     return ap.parse_args()
 
 
@@ -299,6 +300,77 @@ def fp64_sart_check(ctx, st, args, gmax, n_views: int = 6):
 
 
 # ---------------------------------------------------------------------------
+FLOW_BYTES_PER_VOXEL = 152  # minimal state per flow iteration: v 3, y 10, v-extrapolation 3 r/w, grad/ut 4 read
+
+
+def flow_bench(args, dev, stream, rank: int) -> dict:
+    """One level of optical_flow::L1Huber_OF at N^3 between two phantom frames:
+    per-iteration device time (primal + dual over the whole volume), from two
+    solves that differ only in their iteration count."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200 import phantom as ph
+
+    N = args.n
+    dims = (N, N, N)
+    params = ph.ellipsoid_params(30, dims, seed=2024, semi=(5.0 * N / 256, 40.0 * N / 256))
+    T = args.frames
+    i1 = ph.rasterize(ph.displaced_params(params, 0, T, 4.0, 2 * math.pi / N, 0.7), dims, dev)
+    i2 = ph.rasterize(ph.displaced_params(params, 1, T, 4.0, 2 * math.pi / N, 0.7), dims, dev)
+    V = torch.zeros((3,) + dims, device=dev)
+    Y = torch.zeros((10,) + dims, device=dev)
+    cut = (8, 8, 8, 45, 8, 8)
+    roi = tuple(int(c * (N / 256.0)) for c in cut)
+    iters = 200
+
+    def run(max_iter):
+        f = stt.Flow(dims, stt.FlowParams(tol=0.0, max_iter=max_iter, n_warps=1, scales=1, cut=cut), device=dev.index or 0)
+        V.zero_()
+        Y.zero_()
+        torch.cuda.synchronize()
+        f.level(i1, i2, V, Y, roi, stream=stream)  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        f.level(i1, i2, V, Y, roi, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        its, _ = f.stats()
+        f.close()
+        return e0.elapsed_time(e1) / 1000.0, int(its[0])
+
+    t_long, n_long = run(iters - 1)
+    t_short, n_short = run(0)
+    t_it = (t_long - t_short) / (n_long - n_short)
+    peak, peak_kind = peaks()
+    achieved = FLOW_BYTES_PER_VOXEL * N ** 3 / t_it / 1e9
+    out = {"workload": f"L1Huber_OF level, {N}^3, ROI cut {cut}, {iters} iterations, 1 warp",
+           "ms_per_iteration": 1000.0 * t_it, "gvoxel_iter_per_s": N ** 3 / t_it / 1e9,
+           "roofline": {"bound": "hbm", "kernel": "k_flow_primal + k_flow_dual", "achieved": achieved,
+                        "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                        "algorithmic_bytes_per_voxel": FLOW_BYTES_PER_VOXEL,
+                        "moved_bytes_per_voxel": 280,
+                        "note": "moved: y 10 r/w, Kx 10 r/w, v 3 r/w, u 4, tau 3, sigma2 1 (reference layout)"}}
+    if rank == 0 and not args.no_cpu:
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_bind as ob
+
+        n = 64
+        sl = (slice(0, n),) * 3
+        a, b = i1[sl].contiguous().cpu().numpy(), i2[sl].contiguous().cpu().numpy()
+        z3, z10 = np.zeros((3, n, n, n), np.float32), np.zeros((10, n, n, n), np.float32)
+        k = 20
+        t0 = time.perf_counter()
+        ob.flow_level32(a, b, z3, z10, (0,) * 6, tol=0.0, max_iter=k - 1, n_warps=1)
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n ** 3 * k / tc / 1e9, "unit": "Gvoxel-iterations/s", "cores": 1,
+                               "kind": "port",
+                               "sample": f"oracle flow level (one thread, as the reference's residual loop "
+                                         f"requires for determinism), {n}^3 x {k} iterations"}
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -473,6 +545,8 @@ def run_stt(args):
         te = float(tt.item())
     e2e_value = world * F * N ** 3 * V / (te / ksteps) / 1e9
 
+    flow = None if args.no_flow else flow_bench(args, dev, stream, rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_sample(args, os.cpu_count() or 1, gpu_check=fp64_sart_check(ctx, st, args, gmax))
@@ -497,7 +571,8 @@ def run_stt(args):
                 "clocks": clk,
                 "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "cpu_s_per_iter": None if cpu is None else cpu["s_per_iter"],
-                "fp64_check": None if cpu is None else cpu.get("fp64_check")}
+                "fp64_check": None if cpu is None else cpu.get("fp64_check"),
+                "flow": flow}
         print(json.dumps(line), flush=True)
     solver.close()
     ctx.close()

@@ -27,6 +27,8 @@
  *   SART               ST_Tomography::SART        S/ST_Tomo/ST_Tomography.cpp:616-808
  *   primal-dual steps  ST_Tomography::Render      S/ST_Tomo/ST_Tomography.cpp:492-607
  *   warp               warping::warp              S/ST_Tomo/warping.h:116-145
+ *   optical flow       optical_flow::L1Huber_OF_MultiScale3D / L1Huber_OF
+ *                                                 S/ST_Tomo/optical_flow.h:83-734
  */
 #ifndef STT_H
 #define STT_H
@@ -193,6 +195,76 @@ stt_status stt_warp(const int *dim, const float *vel, const float *src, int nc, 
  * vel_bar += J_vel^T out_bar (either may be NULL; both accumulate with atomics). */
 stt_status stt_warp_vjp(const int *dim, const float *vel, const float *src, int nc, float dt,
                         const float *out_bar, float *src_bar, float *vel_bar, void *stream);
+
+/* Warp with aabb = [0, box] over a dim grid (warping.h:11-145 with a general
+ * bounding box), sampling with CImg's nested Catmull-Rom arithmetic in the
+ * reference's operation order: the result equals warping::warp bit for bit.
+ * The multiscale flow warps each pyramid level in full-size units this way
+ * (optical_flow.h:700).  dim and box are HOST arrays. */
+stt_status stt_warp_box(const int *dim, const float *box, const float *vel, const float *src, int nc,
+                        float dt, float *out, void *stream);
+/* CImg::get_gradient("xyz", 0) (CImg.h:34570-34581): central differences with
+ * Neumann boundaries; grad = 3 planes (d/dx, d/dy, d/dz). */
+stt_status stt_image_gradient(const int *dim, const float *img, float *grad, void *stream);
+
+/* ---- optical flow (ST_Tomo/optical_flow.h:83-734) --------------------------
+ * 3D TV-L1 / Huber optical flow by preconditioned primal-dual iterations with
+ * warping, on a pyramid of Deriche-blurred images, as
+ * optical_flow::L1Huber_OF_MultiScale3D (:630-734) and L1Huber_OF (:83-623).
+ * Fields are planar x-fastest volumes: I1 and I2 one plane each, V 3 planes
+ * (flow in voxel units of the full-size grid), Y 10 planes (Y1|Y2|Y3: dual
+ * variables of the gradients of the three flow components, Y4: dual of the
+ * data term).
+ * Stopping rule (optical_flow.h:305-495): the primal-dual residual is formed
+ * every 50 iterations and a warp stops once it is not above tol, else after
+ * max_iter + 1 iterations.  The residual is summed with atomics (the
+ * reference's sum is a racy OpenMP loop), so the iteration a warp stops at can
+ * differ from the reference's only when the residual is within rounding of
+ * tol; everything else follows the reference's float arithmetic exactly.
+ * Outside the ROI the reference reads gradient arrays that it never set; they
+ * are 0 here (this reaches only Y4 outside the ROI, not V).
+ * The reference's Render uses tol 0.1, lambda 1.2, huber 1, eta 0.65,
+ * sigma 0.5, max_iter 3000, norm 4, 3 warps, 3 scales (ST_Tomography.cpp:440-456). */
+typedef struct stt_flow_params {
+    float tol;      /* residual threshold */
+    float lambda;   /* weight of the TV term: radius of the dual ball */
+    float huber;    /* Huber epsilon (norm 4) */
+    float eta;      /* pyramid factor per level */
+    float sigma;    /* Deriche blur of I1 and I2 before the pyramid */
+    int max_iter;   /* a warp runs at most max_iter + 1 iterations */
+    int norm;       /* 4: Huber-regularised TV; anything else: TV */
+    int n_warps;    /* re-linearisations per level */
+    int scales;     /* pyramid levels */
+    int cut[6];     /* ROI at full size: cut from x-, x+, y-, y+, z-, z+ faces */
+} stt_flow_params;
+
+typedef struct stt_flow stt_flow;
+
+/* Allocates every buffer of a multiscale solve for volumes of size dims
+ * (HOST int[3]) on `device`: about 250 bytes per voxel. */
+stt_status stt_flow_create(int device, const int *dims, const stt_flow_params *p, stt_flow **out);
+const char *stt_flow_last_error(const stt_flow *f);
+stt_status stt_flow_destroy(stt_flow *f);
+/* L1Huber_OF_MultiScale3D: V holds the initial flow and receives the
+ * finest-level flow; Y0 (10 planes, NULL = zeros) is the initial dual. */
+stt_status stt_flow_multiscale(stt_flow *f, const float *I1, const float *I2, float *V, const float *Y0,
+                               void *stream);
+/* L1Huber_OF on one level of size dim (HOST, each extent >= 3 and at most the
+ * created size), aabb = [0, box] (HOST float[3]), roi (HOST int[6], same order
+ * as cut).  V and Y are updated in place; Y only inside the ROI. */
+stt_status stt_flow_level(stt_flow *f, const int *dim, const float *box, const int *roi, const float *I1,
+                          const float *I2, float *V, float *Y, void *stream);
+/* Iterations run by each (level, warp) of the last solve, coarse level
+ * first, and the last residual of each (HOST arrays of *n_entries, either may
+ * be NULL).  Synchronises the device. */
+stt_status stt_flow_stats(stt_flow *f, int *n_entries, int *iters, float *err);
+/* CImg::blur(sigma) (Deriche, order 0, Neumann; CImg.h:32917-33050) in place
+ * on nc planes of size dim; dim*nc at most 10x the created volume. */
+stt_status stt_flow_blur(stt_flow *f, const int *dim, int nc, float sigma, float *img, void *stream);
+/* CImg::get_resize(odim, nc, 5) (CImg.h:28432-28560): moving average along
+ * shrinking axes, Catmull-Rom along growing ones, x then y then z. */
+stt_status stt_flow_resize(stt_flow *f, const int *dim, int nc, const float *in, const int *odim, float *out,
+                           void *stream);
 
 /* ---- space-time primal-dual solver (ST_Tomography::Render, ST_Tomography.cpp:492-607) ----
  * One call to stt_solver_iterate runs one primal-dual iteration over all

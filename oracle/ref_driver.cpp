@@ -226,6 +226,16 @@ void ref_warp(const int *dim, const float *vel, const float *src, int nc,
     std::memcpy(out, O.data(), sizeof(float) * O.size());
 }
 
+// warping::warp with aabb = [0, box] over a dim grid (the multiscale flow's case).
+void ref_warp_box(const int *dim, const float *box, const float *vel, const float *src, int nc,
+                  float dt, float *out) {
+    CImg<float> V(vel, dim[0], dim[1], dim[2], 3);
+    CImg<float> S(src, dim[0], dim[1], dim[2], nc);
+    float aabb[6] = {0.0f, box[0], 0.0f, box[1], 0.0f, box[2]};
+    CImg<float> O = warping::warp(dim, aabb, V, S, dt);
+    std::memcpy(out, O.data(), sizeof(float) * O.size());
+}
+
 // CImg::cubic_atXYZ at n points (px, py, pz), channel 0.
 void ref_cubic_at(const int *dim, const float *img, int n, const float *px,
                   const float *py, const float *pz, float *out) {

@@ -24,6 +24,7 @@
 #include "stt_oracle.h"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -838,11 +839,13 @@ inline void cr_w(double d, double w[4], double dw[4]) {
 
 // warping::sample_image (warping.h:49-88): world -> cell grid, clamp to
 // [1, dim-2], Catmull-Rom sample clamped to the 8-corner min/max.
+// box: aabb extents [0, box[a]] (NULL: the cell grid itself, aabb = [0, dim]).
 template <typename R, typename V>
-inline R sample_image(const int *dim, const V *img, const R p[3]) {
+inline R sample_image(const int *dim, const V *img, const R p[3], const R *box = nullptr) {
     R gq[3];
     for (int a = 0; a < 3; ++a) {
-        R gw = (R)dim[a] * (p[a] - (R)0) / ((R)dim[a] - (R)0);
+        const R ext = box ? box[a] : (R)dim[a];
+        R gw = (R)dim[a] * (p[a] - (R)0) / (ext - (R)0);
         gq[a] = (R)(gw - 0.5);
         R hi = (R)(dim[a] - 2);
         R lo = (R)1;
@@ -868,8 +871,11 @@ inline R sample_image(const int *dim, const V *img, const R p[3]) {
 }
 
 // warping::warp / trace (warping.h:100-145): p = cell centre, trace with -dt.
+// box: aabb = [0, box] (NULL: [0, dim]); the multiscale flow warps every level
+// in full-resolution world units (optical_flow.h:700).
 template <typename R>
-void warp_impl(const int *dim, const R *vel, const R *src, int nc, R dt, R *out) {
+void warp_impl(const int *dim, const R *vel, const R *src, int nc, R dt, R *out,
+               const R *box = nullptr) {
     const long n = (long)dim[0] * dim[1] * dim[2];
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < dim[2]; ++k)
@@ -877,17 +883,19 @@ void warp_impl(const int *dim, const R *vel, const R *src, int nc, R dt, R *out)
             for (int i = 0; i < dim[0]; ++i) {
                 R p[3];
                 const int ijk[3] = {i, j, k};
-                for (int a = 0; a < 3; ++a)
-                    p[a] = (R)(0 + ((R)ijk[a] + 0.5) * ((R)dim[a] - 0) / (R)dim[a]);
+                for (int a = 0; a < 3; ++a) {
+                    const R ext = box ? box[a] : (R)dim[a];
+                    p[a] = (R)(0 + ((R)ijk[a] + 0.5) * (ext - 0) / (R)dim[a]);
+                }
                 const R h = -dt;
                 R v1[3], p2[3], v2[3], p0[3], q[3];
-                for (int c = 0; c < 3; ++c) v1[c] = sample_image<R>(dim, vel + c * n, p);
+                for (int c = 0; c < 3; ++c) v1[c] = sample_image<R>(dim, vel + c * n, p, box);
                 for (int c = 0; c < 3; ++c) p2[c] = p[c] + h * v1[c];
-                for (int c = 0; c < 3; ++c) v2[c] = sample_image<R>(dim, vel + c * n, p2);
+                for (int c = 0; c < 3; ++c) v2[c] = sample_image<R>(dim, vel + c * n, p2, box);
                 for (int c = 0; c < 3; ++c) p0[c] = p2[c] - h * v2[c];
                 for (int c = 0; c < 3; ++c) q[c] = p2[c] + (R)(0.5 * (p[c] - p0[c]));
                 long o = i + (long)j * dim[0] + (long)k * dim[0] * dim[1];
-                for (int c = 0; c < nc; ++c) out[o + c * n] = sample_image<R>(dim, src + c * n, q);
+                for (int c = 0; c < nc; ++c) out[o + c * n] = sample_image<R>(dim, src + c * n, q, box);
             }
 }
 
@@ -1017,6 +1025,347 @@ void warp_vjp_impl(const int *dim, const double *vel, const double *src, int nc,
                     for (int t = 0; t < J1[c].nw; ++t) vel_bar[c * n + J1[c].idx[t]] += v1bar * J1[c].w[t];
                 }
             }
+}
+
+
+// ---------------------------------------------------------------------------
+// 3D TV-L1/Huber optical flow (S/ST_Tomo/optical_flow.h:83-734) and the CImg
+// image operations it calls (S/ImageFormationModel/CImg.h).
+
+// CImg::deriche, order 0, Neumann boundaries (CImg.h:32917-33050).
+struct DericheC {
+    float a0, a1, a2, a3, b1, b2, coefp, coefn;
+};
+
+DericheC deriche_coefs(float sigma) {
+    const float nnsigma = sigma < 0.1f ? 0.1f : sigma, alpha = 1.695f / nnsigma,
+                ema = (float)std::exp(-alpha), ema2 = (float)std::exp(-2 * alpha), b1 = -2 * ema,
+                b2 = ema2;
+    const float k = (1 - ema) * (1 - ema) / (1 + 2 * alpha * ema - ema2);
+    DericheC c;
+    c.a0 = k;
+    c.a1 = k * (alpha - 1) * ema;
+    c.a2 = k * (alpha + 1) * ema;
+    c.a3 = -k * ema2;
+    c.b1 = b1;
+    c.b2 = b2;
+    c.coefp = (c.a0 + c.a1) / (1 + b1 + b2);
+    c.coefn = (c.a2 + c.a3) / (1 + b1 + b2);
+    return c;
+}
+
+// _cimg_deriche_apply on one line of N samples spaced `off` apart.
+void deriche_line(float *X, long off, int N, const DericheC &c, std::vector<float> &Y) {
+    float xp = X[0], yb = c.coefp * xp, yp = yb;
+    for (int m = 0; m < N; ++m) {
+        const float xc = X[m * off];
+        const float yc = c.a0 * xc + c.a1 * xp - c.b1 * yp - c.b2 * yb;
+        Y[m] = yc;
+        xp = xc;
+        yb = yp;
+        yp = yc;
+    }
+    float xn = X[(N - 1) * off], xa = xn, yn = c.coefn * xn, ya = yn;
+    for (int m = N - 1; m >= 0; --m) {
+        const float xc = X[m * off];
+        const float yc = c.a2 * xn + c.a3 * xa - c.b1 * yn - c.b2 * ya;
+        xa = xn;
+        xn = xc;
+        ya = yn;
+        yn = yc;
+        X[m * off] = Y[m] + yc;
+    }
+}
+
+// CImg::blur(sigma) (CImg.h:33249-33262, 33275-33278): Deriche along x, y, z
+// (each axis of extent > 1), in place on nc planar channels.
+void blur_impl(const int *d, int nc, float sigma, float *img) {
+    if (sigma < 0.1f) return;  // deriche() returns early for order 0
+    const DericheC c = deriche_coefs(sigma);
+    const long nx = d[0], ny = d[1], nz = d[2], n = nx * ny * nz;
+    std::vector<float> Y(std::max(nx, std::max(ny, nz)));
+    for (int ch = 0; ch < nc; ++ch) {
+        float *I = img + ch * n;
+        if (nx > 1)
+            for (long z = 0; z < nz; ++z)
+                for (long y = 0; y < ny; ++y) deriche_line(I + y * nx + z * nx * ny, 1, (int)nx, c, Y);
+        if (ny > 1)
+            for (long z = 0; z < nz; ++z)
+                for (long x = 0; x < nx; ++x) deriche_line(I + x + z * nx * ny, nx, (int)ny, c, Y);
+        if (nz > 1)
+            for (long y = 0; y < ny; ++y)
+                for (long x = 0; x < nx; ++x) deriche_line(I + x + y * nx, nx * ny, (int)nz, c, Y);
+    }
+}
+
+// One axis of CImg::get_resize(..., 5) (CImg.h:28432-28560): a shrinking axis
+// takes the moving average (resize type 2, :28135-28195); a growing axis is
+// Catmull-Rom interpolated with step (old-1)/(new-1), evaluated in double.
+void resize_axis_impl(const int *d, int nc, const float *in, int axis, int nn, float *out) {
+    int od[3] = {d[0], d[1], d[2]};
+    const int old = d[axis];
+    od[axis] = nn;
+    const long st_in[3] = {1, d[0], (long)d[0] * d[1]};
+    const long st_out[3] = {1, od[0], (long)od[0] * od[1]};
+    const long nin = (long)d[0] * d[1] * d[2], nout = (long)od[0] * od[1] * od[2];
+    // the two coordinates that are not resized
+    const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+    std::vector<float> acc(nn);
+    std::vector<unsigned> off(nn);
+    std::vector<double> foff(nn);
+    if (nn > old) {
+        const double fx = nn > 1 ? (old - 1.0) / (nn - 1) : 0;
+        double curr = 0, prev = 0;
+        for (int x = 0; x < nn; ++x) {
+            foff[x] = curr - (unsigned)curr;
+            prev = curr;
+            curr = std::min(old - 1.0, curr + fx);
+            off[x] = (unsigned)curr - (unsigned)prev;
+        }
+    }
+    for (int ch = 0; ch < nc; ++ch)
+        for (int u = 0; u < d[a2]; ++u)
+            for (int w = 0; w < d[a1]; ++w) {
+                const float *src = in + ch * nin + w * st_in[a1] + u * st_in[a2];
+                float *dst = out + ch * nout + w * st_out[a1] + u * st_out[a2];
+                const long si = st_in[axis], so = st_out[axis];
+                if (nn == old) {
+                    for (int t = 0; t < nn; ++t) dst[t * so] = src[t * si];
+                } else if (nn < old) {
+                    std::fill(acc.begin(), acc.end(), 0.0f);
+                    for (unsigned a = (unsigned)old * nn, b = old, c = nn, s = 0, t = 0; a;) {
+                        const unsigned dd = std::min(b, c);
+                        a -= dd;
+                        b -= dd;
+                        c -= dd;
+                        acc[t] += src[s * si] * dd;
+                        if (!b) {
+                            acc[t] /= old;
+                            ++t;
+                            b = old;
+                        }
+                        if (!c) {
+                            ++s;
+                            c = nn;
+                        }
+                    }
+                    for (int t = 0; t < nn; ++t) dst[t * so] = acc[t];
+                } else {
+                    long s = 0;
+                    for (int x = 0; x < nn; ++x) {
+                        const double t = foff[x], val1 = (double)src[s * si],
+                                     val0 = s > 0 ? (double)src[(s - 1) * si] : val1,
+                                     val2 = s <= old - 2 ? (double)src[(s + 1) * si] : val1,
+                                     val3 = s < old - 2 ? (double)src[(s + 2) * si] : val2,
+                                     val = val1 + 0.5f * (t * (-val0 + val2) +
+                                                          t * t * (2 * val0 - 5 * val1 + 4 * val2 - val3) +
+                                                          t * t * t * (-val0 + 3 * val1 - 3 * val2 + val3));
+                        dst[x * so] = (float)(val < -FLT_MAX ? -FLT_MAX : val > FLT_MAX ? FLT_MAX : val);
+                        s += off[x];
+                    }
+                }
+            }
+}
+
+// get_resize(nx, ny, nz, nc, 5): x, then y, then z.
+void resize_impl(const int *d, int nc, const float *in, const int *od, float *out) {
+    std::vector<float> a(in, in + (size_t)d[0] * d[1] * d[2] * nc), b;
+    int cur[3] = {d[0], d[1], d[2]};
+    for (int axis = 0; axis < 3; ++axis) {
+        if (od[axis] == cur[axis]) continue;
+        int nd[3] = {cur[0], cur[1], cur[2]};
+        nd[axis] = od[axis];
+        b.assign((size_t)nd[0] * nd[1] * nd[2] * nc, 0.0f);
+        resize_axis_impl(cur, nc, a.data(), axis, od[axis], b.data());
+        a.swap(b);
+        cur[axis] = od[axis];
+    }
+    std::memcpy(out, a.data(), sizeof(float) * a.size());
+}
+
+// get_gradient("xyz", 0): central differences, neighbours clamped (CImg.h:34570-34581).
+void gradient_impl(const int *d, const float *I, float *gx, float *gy, float *gz) {
+    const long nx = d[0], ny = d[1], nz = d[2];
+    for (long z = 0; z < nz; ++z)
+        for (long y = 0; y < ny; ++y)
+            for (long x = 0; x < nx; ++x) {
+                auto at = [&](long i, long j, long k) { return I[i + j * nx + k * nx * ny]; };
+                const long p = x + y * nx + z * nx * ny;
+                gx[p] = (at(std::min(x + 1, nx - 1), y, z) - at(std::max(x - 1, 0L), y, z)) / 2;
+                gy[p] = (at(x, std::min(y + 1, ny - 1), z) - at(x, std::max(y - 1, 0L), z)) / 2;
+                gz[p] = (at(x, y, std::min(z + 1, nz - 1)) - at(x, y, std::max(z - 1, 0L))) / 2;
+            }
+}
+
+// Backward / forward differences of S/ImageFormationModel/tools.cpp:126-192.
+inline float dm_(const float *f, long p, int c, int n, long st) {
+    if (c > 0 && c < n - 1) return f[p] - f[p - st];
+    if (c == 0) return f[p];
+    return -f[p - st];
+}
+inline float dp_(const float *f, long p, int c, int n, long st) {
+    return c < n - 1 ? f[p + st] - f[p] : 0.0f;
+}
+
+// optical_flow::L1Huber_OF (optical_flow.h:83-623), one thread, so the
+// residual sums follow the sequential loop order.  V: 3 channels (in/out),
+// Y: Y1|Y2|Y3|Y4 = 10 channels (in/out, written back inside the ROI only, as
+// the reference does).  roi = {x0, x1, y0, y1, z0, z1} cut from each face.
+// The gradient and ut outside the ROI, which the reference leaves unset, are 0.
+// iters, errs (optional, n_warps entries): iterations run per warp and the
+// last residual formed in each warp (1 when none was).
+void flow_level_impl(const int *d, const float *box, const int *roi, const float *I1, const float *I2,
+                     float *V, float *Y, float tol, float lambda, int max_iter, int norm, int n_warps,
+                     float huber, int *iters, float *errs) {
+    const long nx = d[0], ny = d[1], nz = d[2], n = nx * ny * nz, sy = nx, sz = nx * ny;
+    const float sigma1 = std::min(1.0f / 3.0f, std::min(1.0f / 3.0f, 1.0f / 3.0f));
+    const float hf = 1.0f / (1.0f + sigma1 * huber / lambda);
+    std::vector<float> y(Y, Y + 10 * n), kx(10 * n, 0.0f), kty(3 * n, 0.0f), ktyo(3 * n), vo(3 * n);
+    std::vector<float> u(4 * n, 0.0f), tau(3 * n), sig2(n), i2w(n), g(3 * n);
+    for (int w = 0; w < n_warps; ++w) {
+        warp_impl<float>(d, V, I2, 1, -1.0f, i2w.data(), box);
+        gradient_impl(d, i2w.data(), g.data(), g.data() + n, g.data() + 2 * n);
+        for (long k = roi[4]; k < nz - roi[5]; ++k)
+            for (long j = roi[2]; j < ny - roi[3]; ++j)
+                for (long i = roi[0]; i < nx - roi[1]; ++i) {
+                    const long p = i + j * sy + k * sz;
+                    u[p] = g[p];
+                    u[n + p] = g[n + p];
+                    u[2 * n + p] = g[2 * n + p];
+                    u[3 * n + p] = i2w[p] - I1[p] - u[p] * V[p] - u[n + p] * V[n + p] - u[2 * n + p] * V[2 * n + p];
+                }
+        for (long p = 0; p < n; ++p) {
+            for (int c = 0; c < 3; ++c) tau[c * n + p] = 1.0f / (4.0f / 1.0f + std::fabs(u[c * n + p]));
+            sig2[p] = 1.0f / (std::fabs(u[p]) + std::fabs(u[n + p]) + std::fabs(u[2 * n + p]));
+        }
+        int it = 0;
+        float err = 1.0f, pr = 0.0f, dr = 0.0f;
+        while (err > tol && it <= max_iter) {
+            ++it;
+            const bool res = it % 50 == 0;
+            if (res) pr = dr = 0.0f;
+            for (long k = roi[4]; k < nz - roi[5]; ++k)
+                for (long j = roi[2]; j < ny - roi[3]; ++j)
+                    for (long i = roi[0]; i < nx - roi[1]; ++i) {
+                        const long p = i + j * sy + k * sz;
+                        if (res)
+                            for (int c = 0; c < 3; ++c) {
+                                vo[c * n + p] = V[c * n + p];
+                                ktyo[c * n + p] = kty[c * n + p];
+                            }
+                        for (int c = 0; c < 3; ++c) {
+                            const float *yc = y.data() + 3 * c * n;
+                            kty[c * n + p] = -1.0f * dm_(yc, p, (int)i, (int)nx, 1) -
+                                             1.0f * dm_(yc + n, p, (int)j, (int)ny, sy) -
+                                             1.0f * dm_(yc + 2 * n, p, (int)k, (int)nz, sz) + u[c * n + p] * y[9 * n + p];
+                        }
+                        for (int c = 0; c < 3; ++c) V[c * n + p] -= tau[c * n + p] * kty[c * n + p];
+                        if (res) {
+                            float s = 0.0f;
+                            for (int c = 0; c < 3; ++c) {
+                                const float t = std::fabs((vo[c * n + p] - V[c * n + p]) / tau[c * n + p] -
+                                                          ktyo[c * n + p] + kty[c * n + p]);
+                                s = c == 0 ? t : s + t;
+                            }
+                            pr += s;
+                        }
+                    }
+            for (long k = 0; k < nz; ++k)
+                for (long j = 0; j < ny; ++j)
+                    for (long i = 0; i < nx; ++i) {
+                        const long p = i + j * sy + k * sz;
+                        float yold[10], kold[10], yt[9];
+                        for (int q = 0; q < 10; ++q) {
+                            yold[q] = y[q * n + p];
+                            kold[q] = kx[q * n + p];
+                        }
+                        for (int c = 0; c < 3; ++c) {
+                            const float *vc = V + c * n;
+                            kx[(3 * c) * n + p] = 1.0f * dp_(vc, p, (int)i, (int)nx, 1);
+                            kx[(3 * c + 1) * n + p] = 1.0f * dp_(vc, p, (int)j, (int)ny, sy);
+                            kx[(3 * c + 2) * n + p] = 1.0f * dp_(vc, p, (int)k, (int)nz, sz);
+                        }
+                        kx[9 * n + p] = u[p] * V[p] + u[n + p] * V[n + p] + u[2 * n + p] * V[2 * n + p];
+                        for (int q = 0; q < 9; ++q) {
+                            const float kq = kx[q * n + p];
+                            yt[q] = (y[q * n + p] + sigma1 * (kq + kq - kold[q]));
+                            if (norm == 4) yt[q] = yt[q] * hf;
+                        }
+                        for (int c = 0; c < 3; ++c) {
+                            const float *t = yt + 3 * c;
+                            const float dv = std::max(1.0f, std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]) / lambda);
+                            for (int a = 0; a < 3; ++a) y[(3 * c + a) * n + p] = t[a] / dv;
+                        }
+                        const float k4 = kx[9 * n + p];
+                        y[9 * n + p] = std::max(-1.0f, std::min(1.0f, y[9 * n + p] + sig2[p] * (k4 + k4 - kold[9] + u[3 * n + p])));
+                        if (res) {
+                            float s = 0.0f;
+                            for (int q = 0; q < 9; ++q) {
+                                const float t = std::fabs((yold[q] - y[q * n + p]) / sigma1 - kold[q] + kx[q * n + p]);
+                                s = q == 0 ? t : s + t;
+                            }
+                            s = s + std::fabs((yold[9] - y[9 * n + p]) / sig2[p] - kold[9] + k4);
+                            dr += s;
+                        }
+                    }
+            if (res) err = (dr * dr + pr * pr) / (float)n;
+        }
+        if (iters) iters[w] = it;
+        if (errs) errs[w] = err;
+    }
+    for (long k = roi[4]; k < nz - roi[5]; ++k)
+        for (long j = roi[2]; j < ny - roi[3]; ++j)
+            for (long i = roi[0]; i < nx - roi[1]; ++i) {
+                const long p = i + j * sy + k * sz;
+                for (int q = 0; q < 10; ++q) Y[q * n + p] = y[q * n + p];
+            }
+}
+
+// optical_flow::L1Huber_OF_MultiScale3D (optical_flow.h:630-734).  Returns the
+// finest-level flow in Vout; Yin (10 channels, NULL = zeros) is the dual start.
+void flow_multiscale_impl(const int *d, const float *I1, const float *I2, const float *Vin, const float *Yin,
+                          float *Vout, float tol, float lambda, int max_iter, int norm, int n_warps, float eta,
+                          float sigma, int scales, float huber, const int *cut) {
+    const long n = (long)d[0] * d[1] * d[2];
+    std::vector<float> b1(I1, I1 + n), b2(I2, I2 + n);
+    blur_impl(d, 1, sigma, b1.data());
+    blur_impl(d, 1, sigma, b2.data());
+    std::vector<float> y0(10 * n, 0.0f);
+    if (Yin) std::memcpy(y0.data(), Yin, sizeof(float) * 10 * n);
+    struct Level {
+        int d[3];
+        std::vector<float> i1, i2, v, y;
+    };
+    std::vector<Level> L(scales);
+    float t_eta = 1.0f;
+    for (int s = 0; s < scales; ++s) {
+        Level &l = L[scales - 1 - s];  // coarse first after the reverse
+        for (int a = 0; a < 3; ++a) l.d[a] = (int)((float)d[a] * t_eta);
+        const long m = (long)l.d[0] * l.d[1] * l.d[2];
+        l.i1.resize(m);
+        l.i2.resize(m);
+        l.v.resize(3 * m);
+        l.y.resize(10 * m);
+        resize_impl(d, 1, b1.data(), l.d, l.i1.data());
+        resize_impl(d, 1, b2.data(), l.d, l.i2.data());
+        resize_impl(d, 3, Vin, l.d, l.v.data());
+        resize_impl(d, 10, y0.data(), l.d, l.y.data());
+        t_eta = t_eta * eta;
+    }
+    const float box[3] = {(float)d[0], (float)d[1], (float)d[2]};
+    for (int s = 0; s < scales; ++s) {
+        Level &l = L[s];
+        int roi[6];
+        for (int q = 0; q < 6; ++q) roi[q] = (int)((float)cut[q] * ((float)l.d[q / 2] / (float)d[q / 2]));
+        flow_level_impl(l.d, box, roi, l.i1.data(), l.i2.data(), l.v.data(), l.y.data(), tol, lambda, max_iter,
+                        norm, n_warps, huber, nullptr, nullptr);
+        if (s < scales - 1) {
+            Level &nx = L[s + 1];
+            resize_impl(l.d, 3, l.v.data(), nx.d, nx.v.data());
+            resize_impl(l.d, 10, l.y.data(), nx.d, nx.y.data());
+        }
+    }
+    std::memcpy(Vout, L[scales - 1].v.data(), sizeof(float) * 3 * n);
 }
 
 }  // namespace
@@ -1217,6 +1566,38 @@ double orc_cubic_at_f64(const int *dim, const double *img, double x, double y, d
     Cub<double> s;
     cub_setup<double>(dim, x, y, z, s);
     return cub_value<double>(dim, img, s);
+}
+
+void orc_warp_box_f32(const int *dim, const float *box, const float *vel, const float *src, int nc,
+                      float dt, float *out, int nthreads) {
+    set_threads(nthreads);
+    warp_impl<float>(dim, vel, src, nc, dt, out, box);
+}
+
+void orc_blur_f32(const int *dim, int nc, float sigma, float *img) { blur_impl(dim, nc, sigma, img); }
+
+void orc_resize_f32(const int *dim, int nc, const float *in, const int *odim, float *out) {
+    resize_impl(dim, nc, in, odim, out);
+}
+
+void orc_gradient_f32(const int *dim, const float *img, float *gx, float *gy, float *gz) {
+    gradient_impl(dim, img, gx, gy, gz);
+}
+
+void orc_flow_level_f32(const int *dim, const float *box, const int *roi, const float *I1, const float *I2,
+                        float *V, float *Y, float tol, float lambda, int max_iter, int norm, int n_warps,
+                        float huber, int *iters, float *errs) {
+    set_threads(1);
+    flow_level_impl(dim, box, roi, I1, I2, V, Y, tol, lambda, max_iter, norm, n_warps, huber, iters, errs);
+}
+
+void orc_flow_multiscale_f32(const int *dim, const float *I1, const float *I2, const float *Vin,
+                             const float *Yin, float *Vout, float tol, float lambda, int max_iter,
+                             int norm, int n_warps, float eta, float sigma, int scales, float huber,
+                             const int *cut) {
+    set_threads(1);
+    flow_multiscale_impl(dim, I1, I2, Vin, Yin, Vout, tol, lambda, max_iter, norm, n_warps, eta, sigma,
+                         scales, huber, cut);
 }
 
 }  // extern "C"

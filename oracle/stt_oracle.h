@@ -131,6 +131,30 @@ void orc_warp_vjp_f64(const int *dim, const double *vel, const double *src, int 
 float orc_cubic_at_f32(const int *dim, const float *img, float x, float y, float z);
 double orc_cubic_at_f64(const int *dim, const double *img, double x, double y, double z);
 
+/* warping::warp with aabb = [0, box] over a dim grid (the multiscale flow
+ * warps every pyramid level in full-resolution units, optical_flow.h:700). */
+void orc_warp_box_f32(const int *dim, const float *box, const float *vel, const float *src, int nc,
+                      float dt, float *out, int nthreads);
+
+/* CImg::blur(sigma) (Deriche, Neumann) in place on nc planar channels. */
+void orc_blur_f32(const int *dim, int nc, float sigma, float *img);
+/* CImg::get_resize(odim, nc, 5): moving average on shrinking axes, Catmull-Rom
+ * on growing ones, x then y then z. */
+void orc_resize_f32(const int *dim, int nc, const float *in, const int *odim, float *out);
+/* CImg::get_gradient("xyz", 0): central differences, Neumann. */
+void orc_gradient_f32(const int *dim, const float *img, float *gx, float *gy, float *gz);
+/* optical_flow::L1Huber_OF (optical_flow.h:83-623) on one level, one thread.
+ * V: 3 channels, Y: 10 channels (Y1|Y2|Y3|Y4), both in/out; roi = {x0,x1,y0,y1,z0,z1};
+ * box: aabb extents; iters, errs (optional): iterations run per warp and its last residual. */
+void orc_flow_level_f32(const int *dim, const float *box, const int *roi, const float *I1, const float *I2,
+                        float *V, float *Y, float tol, float lambda, int max_iter, int norm, int n_warps,
+                        float huber, int *iters, float *errs);
+/* optical_flow::L1Huber_OF_MultiScale3D (optical_flow.h:630-734); cut: 6 ints. */
+void orc_flow_multiscale_f32(const int *dim, const float *I1, const float *I2, const float *Vin,
+                             const float *Yin, float *Vout, float tol, float lambda, int max_iter,
+                             int norm, int n_warps, float eta, float sigma, int scales, float huber,
+                             const int *cut);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,14 +11,18 @@ from .api import (  # noqa: F401
     SOLVE_PLAIN,
     SOLVE_STREAMS,
     Context,
+    Flow,
     PdParams,
     Solver,
     frame_order,
+    image_gradient,
     lds_angles,
     permutation,
     views_from_rounds,
     warp,
+    warp_box,
     warp_vjp,
 )
+from .api import FlowParams_ as FlowParams  # noqa: F401
 
 __version__ = "0.1.0"

@@ -51,10 +51,16 @@ class PdState(C.Structure):
                 ("ybc_halo", C.c_void_p), ("flow_halo", C.c_void_p)]
 
 
+class FlowParams(C.Structure):
+    _fields_ = [("tol", C.c_float), ("lam", C.c_float), ("huber", C.c_float), ("eta", C.c_float),
+                ("sigma", C.c_float), ("max_iter", C.c_int), ("norm", C.c_int), ("n_warps", C.c_int),
+                ("scales", C.c_int), ("cut", C.c_int * 6)]
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
-            f"{LIB_PATH} is not built; run `python -m spacetimetomography_b200.build` "
+            f"{LIB_PATH} is not built; run `python spacetimetomography_b200/build.py` "
             "(there is no CPU fallback)")
     lib = C.CDLL(str(LIB_PATH))
     vp, i, d, f = C.c_void_p, C.c_int, C.c_double, C.c_float
@@ -83,6 +89,15 @@ def _load() -> C.CDLL:
         "stt_solver_stats": [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_ulonglong)],
         "stt_solver_destroy": [vp],
         "stt_solver_frame_order": [C.c_ulonglong, C.c_ulonglong, i, i, i, vp],
+        "stt_warp_box": [vp, vp, vp, vp, i, f, vp, vp],
+        "stt_image_gradient": [vp, vp, vp, vp],
+        "stt_flow_create": [i, vp, C.POINTER(FlowParams), C.POINTER(vp)],
+        "stt_flow_destroy": [vp],
+        "stt_flow_multiscale": [vp, vp, vp, vp, vp, vp],
+        "stt_flow_level": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
+        "stt_flow_stats": [vp, C.POINTER(i), vp, vp],
+        "stt_flow_blur": [vp, vp, i, f, vp, vp],
+        "stt_flow_resize": [vp, vp, i, vp, vp, vp, vp],
     }
     for name, argtypes in sigs.items():
         fn = getattr(lib, name)
@@ -92,6 +107,8 @@ def _load() -> C.CDLL:
     lib.stt_last_error.restype = C.c_char_p
     lib.stt_solver_last_error.argtypes = [vp]
     lib.stt_solver_last_error.restype = C.c_char_p
+    lib.stt_flow_last_error.argtypes = [vp]
+    lib.stt_flow_last_error.restype = C.c_char_p
     lib.stt_version.argtypes = []
     lib.stt_version.restype = C.c_char_p
     return lib

@@ -14,7 +14,7 @@ from typing import Sequence
 
 import numpy as np
 
-from ._lib import Geometry, PdState, SolveCfg, STTError, check, lib
+from ._lib import FlowParams, Geometry, PdState, SolveCfg, STTError, check, lib
 from ._lib import PdParams as _PdParams
 
 # ROI cut of the reference (ST_Tomography.cpp:114)
@@ -205,6 +205,129 @@ def warp_vjp(flow, src, dt, out_bar, src_bar=None, flow_bar=None, stream=None):
     check(lib.stt_warp_vjp(dim, _ptr(flow), _ptr(src), nc, float(dt), _ptr(out_bar), _ptr(src_bar),
                            _ptr(flow_bar), _stream(stream)))
     return src_bar, flow_bar
+
+
+def _dim3(t):
+    nz, ny, nx = t.shape[-3:]
+    return (C.c_int * 3)(nx, ny, nz)
+
+
+def warp_box(flow, src, dt, box, out=None, stream=None):
+    """warping::warp with aabb = [0, box] (box = (bx, by, bz)); bit-exact CImg sampling."""
+    import torch
+
+    nc = 1 if src.dim() == 3 else src.shape[0]
+    if out is None:
+        out = torch.empty_like(src)
+    check(lib.stt_warp_box(_dim3(src), (C.c_float * 3)(*map(float, box)), _ptr(flow), _ptr(src), nc, float(dt),
+                           _ptr(out), _stream(stream)))
+    return out
+
+
+def image_gradient(img, out=None, stream=None):
+    """CImg::get_gradient("xyz", 0) of a (nz, ny, nx) volume -> (3, nz, ny, nx)."""
+    import torch
+
+    if out is None:
+        out = torch.empty((3,) + tuple(img.shape), device=img.device, dtype=img.dtype)
+    check(lib.stt_image_gradient(_dim3(img), _ptr(img), _ptr(out), _stream(stream)))
+    return out
+
+
+@dataclass
+class FlowParams_:
+    """Parameters of optical_flow::L1Huber_OF_MultiScale3D; defaults are the
+    values ST_Tomography::Render passes (ST_Tomography.cpp:440-456)."""
+
+    tol: float = 0.1
+    lam: float = 1.2
+    huber: float = 1.0
+    eta: float = 0.65
+    sigma: float = 0.5
+    max_iter: int = 3000
+    norm: int = 4
+    n_warps: int = 3
+    scales: int = 3
+    cut: Sequence[int] = field(default_factory=lambda: tuple(REFERENCE_CUT[:6]))
+
+    def c(self) -> FlowParams:
+        return FlowParams(float(self.tol), float(self.lam), float(self.huber), float(self.eta), float(self.sigma),
+                          int(self.max_iter), int(self.norm), int(self.n_warps), int(self.scales),
+                          (C.c_int * 6)(*map(int, self.cut[:6])))
+
+
+class Flow:
+    """stt_flow: the 3D TV-L1/Huber optical flow of optical_flow.h on one GPU.
+
+    Images (nz, ny, nx), flow V (3, nz, ny, nx), dual Y (10, nz, ny, nx); all
+    torch CUDA float32 tensors."""
+
+    def __init__(self, dims, params: FlowParams_ | None = None, device: int = 0):
+        self.params = params or FlowParams_()
+        nz, ny, nx = dims
+        h = C.c_void_p()
+        pc = self.params.c()
+        rc = lib.stt_flow_create(int(device), (C.c_int * 3)(nx, ny, nz), C.byref(pc), C.byref(h))
+        if rc != 0:
+            raise STTError(rc, (lib.stt_last_error(None) or b"flow create failed").decode())
+        self._h = h
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise STTError(rc, (lib.stt_flow_last_error(self._h) or b"").decode(errors="replace"))
+
+    def multiscale(self, I1, I2, V, Y0=None, stream=None):
+        """V: initial flow in, finest flow out (in place)."""
+        self._chk(lib.stt_flow_multiscale(self._h, _ptr(I1), _ptr(I2), _ptr(V), _ptr(Y0), _stream(stream)))
+        return V
+
+    def level(self, I1, I2, V, Y, roi, box=None, stream=None):
+        nz, ny, nx = I1.shape
+        box = (nx, ny, nz) if box is None else box
+        self._chk(lib.stt_flow_level(self._h, _dim3(I1), (C.c_float * 3)(*map(float, box)),
+                                     (C.c_int * 6)(*map(int, roi)), _ptr(I1), _ptr(I2), _ptr(V), _ptr(Y),
+                                     _stream(stream)))
+        return V, Y
+
+    def stats(self):
+        """(iterations, residual) per (level, warp) of the last call; synchronises."""
+        n = C.c_int()
+        self._chk(lib.stt_flow_stats(self._h, C.byref(n), None, None))
+        its = np.zeros(max(n.value, 1), np.int32)
+        err = np.zeros(max(n.value, 1), np.float32)
+        self._chk(lib.stt_flow_stats(self._h, C.byref(n), its.ctypes.data_as(C.c_void_p),
+                                     err.ctypes.data_as(C.c_void_p)))
+        return its[:n.value], err[:n.value]
+
+    def blur(self, img, sigma, stream=None):
+        """CImg::blur(sigma) in place on (nz, ny, nx) or (nc, nz, ny, nx)."""
+        nc = 1 if img.dim() == 3 else img.shape[0]
+        self._chk(lib.stt_flow_blur(self._h, _dim3(img), nc, float(sigma), _ptr(img), _stream(stream)))
+        return img
+
+    def resize(self, img, odim, out=None, stream=None):
+        """CImg::get_resize(odim=(nx, ny, nz), nc, 5)."""
+        import torch
+
+        nc = 1 if img.dim() == 3 else img.shape[0]
+        ox, oy, oz = odim
+        shape = (oz, oy, ox) if img.dim() == 3 else (nc, oz, oy, ox)
+        if out is None:
+            out = torch.empty(shape, device=img.device, dtype=img.dtype)
+        self._chk(lib.stt_flow_resize(self._h, _dim3(img), nc, _ptr(img), (C.c_int * 3)(ox, oy, oz), _ptr(out),
+                                      _stream(stream)))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.stt_flow_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 SOLVE_PLAIN, SOLVE_STREAMS, SOLVE_GRAPH = 0, 1, 2

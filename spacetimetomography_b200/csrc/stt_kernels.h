@@ -47,6 +47,48 @@ cudaError_t launch_roi_apply(const int *dims, const int *roi_cut, const int *pd_
                              const float *xprev, float *xbar, cudaStream_t s);
 cudaError_t launch_roi_mask(const int *dims, const int *cut, float *roi, cudaStream_t s);
 
+// ---- optical flow (k_flow.cu) ----
+struct FlowRoi {
+    int x0, x1, y0, y1, z0, z1;  // cut from each face
+};
+
+struct DericheCoef {
+    float a0, a1, a2, a3, b1, b2, coefp, coefn;
+};
+
+// One axis of a CImg resize: mode 0 = moving average (shrinking), mode 1 =
+// Catmull-Rom (growing) with the per-output (source index, fraction) table
+// written by launch_resize_table.
+struct ResizeAxis {
+    int axis, mode, nc;
+    int ix, iy, iz;  // input extents
+    int ox, oy, oz;  // output extents (differ from the input along `axis` only)
+    int old_n, new_n;
+    const int *src;
+    const double *frac;
+};
+
+cudaError_t launch_warp_box(const int *dim, const float *box, const float *vel, const float *src, int nc,
+                            float dt, float *out, cudaStream_t s);
+cudaError_t launch_flow_setup(const int *d, const FlowRoi &roi, const float *i2w, const float *i1,
+                              const float *v, float *u, float *tau, float *sig2, cudaStream_t s);
+cudaError_t launch_flow_primal(const int *d, const FlowRoi &roi, const float *y, const float *u,
+                               const float *tau, float *v, float *kty, int flags, double *resid,
+                               const int *done, cudaStream_t s);
+cudaError_t launch_flow_dual(const int *d, const float *v, const float *u, const float *sig2, float *y,
+                             float *kx, float sigma1, float hf, float lambda, int huber, int flags,
+                             double *resid, const int *done, cudaStream_t s);
+cudaError_t launch_flow_check(double *resid, long long n, float tol, int it, int is_resid, int is_last,
+                              int *done, int *iters, float *err, cudaStream_t s);
+cudaError_t launch_flow_reset(int *done, double *resid, int *iters, float *err, cudaStream_t s);
+cudaError_t launch_deriche(const int *d, int nc, int axis, const DericheCoef &c, float *img, float *tmp,
+                           cudaStream_t s);
+cudaError_t launch_resize_table(int old_n, int new_n, int *src, double *frac, cudaStream_t s);
+cudaError_t launch_resize_axis(const ResizeAxis &ra, const float *in, float *out, cudaStream_t s);
+cudaError_t launch_gradient(const int *d, const float *img, float *g, cudaStream_t s);
+cudaError_t launch_copy_roi(const int *d, int nc, const FlowRoi &roi, const float *src, float *dst,
+                            cudaStream_t s);
+
 cudaError_t launch_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
                         float *out, cudaStream_t s);
 cudaError_t launch_warp_vjp(const int *dim, const float *vel, const float *src, int nc, float dt,

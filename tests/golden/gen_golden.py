@@ -12,7 +12,11 @@ Cases: forward projection (image, ray length, sample count) of three views on
 an off-centre, non-unit-spacing, non-square scan; the geometry matrices of
 those views; the ray-driven backprojection scatter (contributions, weights);
 warping::warp of a 2-channel volume for two time steps; CImg's cubic sampler
-at points including edges and corners.
+at points including edges and corners.  tests/golden/reference_flow_golden.npz:
+CImg's Deriche blur, cubic/moving-average resize and gradient, the warp over a
+general bounding box, four single-level optical-flow solves (with and without
+an ROI, a full-size bounding box, residual iterations and a tolerance stop)
+and one three-level multiscale solve.
 """
 from __future__ import annotations
 
@@ -87,6 +91,58 @@ def main():
     out.update(cubic_dim=cdim, cubic_img=img, cubic_pts=pts, cubic_val=vals)
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes)")
+    flow_fixtures()
+
+
+FLOW_OUT = HERE / "reference_flow_golden.npz"
+FLOW_DIM = (11, 10, 9)  # nx, ny, nz
+# roi (x0 x1 y0 y1 z0 z1), box, max_iter, tol.  A case that stops on the
+# residual uses no ROI: the reference's residual also sums gradient arrays it
+# leaves unset outside the ROI (optical_flow.h:263-290), so with an ROI its
+# stopping iteration depends on uninitialised memory.
+FLOW_LEVEL_CASES = [
+    ((0, 0, 0, 0, 0, 0), (11, 10, 9), 20, 0.0),
+    ((2, 1, 1, 3, 2, 2), (16, 13, 12), 30, 0.0),
+    ((0, 0, 0, 0, 0, 0), (11, 10, 9), 120, 1e-3),
+    ((0, 0, 0, 0, 0, 0), (11, 10, 9), 130, 1e30),
+]
+FLOW_MS_DIM = (20, 18, 19)
+FLOW_MS_CUT = (3, 2, 2, 4, 1, 3)
+
+
+def flow_fixtures():
+    """Optical flow and the CImg operations under it, from the reference's
+    optical_flow.h / warping.h / CImg.h compiled into oracle/_ref (one thread)."""
+    rng = np.random.default_rng(20261204)
+    nx, ny, nz = FLOW_DIM
+    out = {}
+    img = rng.normal(size=(2, nz, ny, nx)).astype(np.float32)
+    out["img"] = img
+    out["blur_05"] = ob.ref_blur(img, 0.5)
+    out["blur_13"] = ob.ref_blur(img, 1.3)
+    for key, od in (("down", (7, 6, 8)), ("up", (16, 15, 12)), ("mixed", (11, 5, 20))):
+        out[f"resize_{key}"] = ob.ref_resize(img, od)
+        out[f"resize_{key}_dim"] = np.array(od, np.int32)
+    out["grad"] = ob.ref_gradient(img[0])
+    vel = (rng.normal(size=(3, nz, ny, nx)) * 1.5).astype(np.float32)
+    out["vel"] = vel
+    out["warp_box"] = ob.ref_warp_box(vel, img, -1.0, (17, 15, 13))
+    i1 = ob.ref_blur(rng.uniform(0, 1, (nz, ny, nx)).astype(np.float32), 1.0)
+    i2 = ob.ref_blur(rng.uniform(0, 1, (nz, ny, nx)).astype(np.float32), 1.0)
+    v0 = (rng.normal(size=(3, nz, ny, nx)) * 0.3).astype(np.float32)
+    y0 = (rng.normal(size=(10, nz, ny, nx)) * 0.1).astype(np.float32)
+    out.update(I1=i1, I2=i2, V0=v0, Y0=y0)
+    for c, (roi, box, mi, tol) in enumerate(FLOW_LEVEL_CASES):
+        v, y = ob.ref_flow_level(i1, i2, v0, y0, roi, box=box, max_iter=mi, tol=tol, threads=1)
+        out[f"level{c}_V"], out[f"level{c}_Y"] = v, y
+    mx, my, mz = FLOW_MS_DIM
+    m1 = ob.ref_blur(rng.uniform(0, 1, (mz, my, mx)).astype(np.float32), 1.5)
+    m2 = ob.ref_blur(rng.uniform(0, 1, (mz, my, mx)).astype(np.float32), 1.5)
+    mv = (rng.normal(size=(3, mz, my, mx)) * 0.3).astype(np.float32)
+    out.update(ms_I1=m1, ms_I2=m2, ms_V0=mv)
+    out["ms_V"] = ob.ref_flow_multiscale(m1, m2, mv, FLOW_MS_CUT, max_iter=12, threads=1)
+    np.savez_compressed(FLOW_OUT, **out)
+    print(f"wrote {FLOW_OUT} ({FLOW_OUT.stat().st_size} bytes)")
 
 
 if __name__ == "__main__":

@@ -71,6 +71,13 @@ O.orc_cubic_at_f32.argtypes = [_vp, _vp, _f, _f, _f]
 O.orc_cubic_at_f32.restype = _f
 O.orc_cubic_at_f64.argtypes = [_vp, _vp, _d, _d, _d]
 O.orc_cubic_at_f64.restype = _d
+O.orc_warp_box_f32.argtypes = [_vp, _vp, _vp, _vp, _i, _f, _vp, _i]
+O.orc_blur_f32.argtypes = [_vp, _i, _f, _vp]
+O.orc_resize_f32.argtypes = [_vp, _i, _vp, _vp, _vp]
+O.orc_gradient_f32.argtypes = [_vp, _vp, _vp, _vp, _vp]
+O.orc_flow_level_f32.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _i, _i, _i, _f, _vp, _vp]
+O.orc_flow_multiscale_f32.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _i, _i, _i, _f, _f, _i, _f,
+                                      _vp]
 O.orc_view_matrices_f32.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp]
 
 REF = None
@@ -80,6 +87,13 @@ if REF_SO.exists():
     REF.ref_bp_ray_view.argtypes = [_vp, _vp, _i, _i, _d, _d, _d, _vp, _d, _i, _vp, _vp, _vp, _vp]
     REF.ref_warp.argtypes = [_vp, _vp, _vp, _i, _f, _vp]
     REF.ref_cubic_at.argtypes = [_vp, _vp, _i, _vp, _vp, _vp, _vp]
+    REF.ref_warp_box.argtypes = [_vp, _vp, _vp, _vp, _i, _f, _vp]
+    REF.ref_gradient.argtypes = [_vp, _vp, _vp, _vp, _vp]
+    REF.ref_blur.argtypes = [_vp, _i, _vp, _f, _vp]
+    REF.ref_resize_cubic.argtypes = [_vp, _i, _vp, _vp, _vp]
+    REF.ref_flow_level.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _i, _i, _i, _f,
+                                   _vp, _i]
+    REF.ref_flow_multiscale.argtypes = [_vp, _vp, _vp, _vp, _vp, _f, _f, _i, _i, _i, _f, _f, _i, _f, _vp, _i]
 
 
 class Scan:
@@ -385,4 +399,124 @@ def view_matrices32(scan: Scan, view: OView) -> np.ndarray:
     out = np.zeros(64, np.float32)
     g = scan.ogeom()
     O.orc_view_matrices_f32(C.byref(g), C.byref(view), P(out))
+    return out
+
+
+# ---- optical flow and the CImg operations it uses --------------------------
+
+def _dim(a):
+    nz, ny, nx = a.shape[-3:]
+    return np.array([nx, ny, nz], np.int32)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def warp_box32(vel, src, dt, box):
+    nc = 1 if src.ndim == 3 else src.shape[0]
+    out = np.zeros(src.shape, np.float32)
+    O.orc_warp_box_f32(P(_dim(src)), P(np.array(box, np.float32)), P(_f32(vel)), P(_f32(src)), nc, float(dt),
+                       P(out), 0)
+    return out
+
+
+def ref_warp_box(vel, src, dt, box):
+    nc = 1 if src.ndim == 3 else src.shape[0]
+    out = np.zeros(src.shape, np.float32)
+    REF.ref_warp_box(P(_dim(src)), P(np.array(box, np.float32)), P(_f32(vel)), P(_f32(src)), nc, float(dt),
+                     P(out))
+    return out
+
+
+def blur32(img, sigma):
+    nc = 1 if img.ndim == 3 else img.shape[0]
+    out = np.array(img, np.float32, copy=True)
+    O.orc_blur_f32(P(_dim(img)), nc, float(sigma), P(out))
+    return out
+
+
+def ref_blur(img, sigma):
+    nc = 1 if img.ndim == 3 else img.shape[0]
+    out = np.zeros(img.shape, np.float32)
+    REF.ref_blur(P(_dim(img)), nc, P(_f32(img)), float(sigma), P(out))
+    return out
+
+
+def resize32(img, odim):
+    """odim = (nx, ny, nz)."""
+    nc = 1 if img.ndim == 3 else img.shape[0]
+    shape = (odim[2], odim[1], odim[0]) if img.ndim == 3 else (nc, odim[2], odim[1], odim[0])
+    out = np.zeros(shape, np.float32)
+    O.orc_resize_f32(P(_dim(img)), nc, P(_f32(img)), P(np.array(odim, np.int32)), P(out))
+    return out
+
+
+def ref_resize(img, odim):
+    nc = 1 if img.ndim == 3 else img.shape[0]
+    shape = (odim[2], odim[1], odim[0]) if img.ndim == 3 else (nc, odim[2], odim[1], odim[0])
+    out = np.zeros(shape, np.float32)
+    REF.ref_resize_cubic(P(_dim(img)), nc, P(_f32(img)), P(np.array(odim, np.int32)), P(out))
+    return out
+
+
+def gradient32(img):
+    g = np.zeros((3,) + img.shape, np.float32)
+    O.orc_gradient_f32(P(_dim(img)), P(_f32(img)), P(g[0]), P(g[1]), P(g[2]))
+    return g
+
+
+def ref_gradient(img):
+    g = np.zeros((3,) + img.shape, np.float32)
+    REF.ref_gradient(P(_dim(img)), P(_f32(img)), P(g[0]), P(g[1]), P(g[2]))
+    return g
+
+
+def flow_level32(I1, I2, V, Y, roi, box=None, tol=0.0, lam=1.2, max_iter=20, norm=4, n_warps=2, huber=1.0,
+                 errs=False):
+    """Returns (V, Y, iterations per warp[, last residual per warp]); Y is 10 channels (Y1|Y2|Y3|Y4)."""
+    d = _dim(I1)
+    box = np.array(d if box is None else box, np.float32)
+    V = np.array(V, np.float32, copy=True)
+    Y = np.array(Y, np.float32, copy=True)
+    its = np.zeros(n_warps, np.int32)
+    err = np.zeros(n_warps, np.float32)
+    O.orc_flow_level_f32(P(d), P(box), P(np.array(roi, np.int32)), P(_f32(I1)), P(_f32(I2)), P(V), P(Y),
+                         float(tol), float(lam), int(max_iter), int(norm), int(n_warps), float(huber), P(its),
+                         P(err))
+    return (V, Y, its, err) if errs else (V, Y, its)
+
+
+def ref_flow_level(I1, I2, V, Y, roi, box=None, tol=0.0, lam=1.2, max_iter=20, norm=4, n_warps=2, huber=1.0,
+                   threads=1):
+    d = _dim(I1)
+    box = np.array(d if box is None else box, np.int32)
+    V = np.array(V, np.float32, copy=True)
+    Y = np.array(Y, np.float32, copy=True)
+    y1, y2, y3, y4 = (np.ascontiguousarray(Y[a:b]) for a, b in ((0, 3), (3, 6), (6, 9), (9, 10)))
+    REF.ref_flow_level(P(d), P(box), P(_f32(I1)), P(_f32(I2)), P(V), P(y1), P(y2), P(y3), P(y4), float(tol),
+                       float(lam), int(max_iter), int(norm), int(n_warps), float(huber),
+                       P(np.array(roi, np.int32)), threads)
+    return V, np.concatenate([y1, y2, y3, y4])
+
+
+def flow_multiscale32(I1, I2, V, cut, Y=None, tol=0.0, lam=1.2, max_iter=20, norm=4, n_warps=2, eta=0.65,
+                      sigma=0.5, scales=3, huber=1.0):
+    d = _dim(I1)
+    out = np.zeros((3,) + I1.shape, np.float32)
+    O.orc_flow_multiscale_f32(P(d), P(_f32(I1)), P(_f32(I2)), P(_f32(V)), None if Y is None else P(_f32(Y)),
+                              P(out), float(tol), float(lam), int(max_iter), int(norm), int(n_warps), float(eta),
+                              float(sigma), int(scales), float(huber), P(np.array(cut, np.int32)))
+    return out
+
+
+def ref_flow_multiscale(I1, I2, V, cut, tol=0.0, lam=1.2, max_iter=20, norm=4, n_warps=2, eta=0.65, sigma=0.5,
+                        scales=3, huber=1.0, threads=1):
+    d = _dim(I1)
+    out = np.zeros((3,) + I1.shape, np.float32)
+    c8 = np.zeros(8, np.int32)
+    c8[:6] = cut[:6]
+    REF.ref_flow_multiscale(P(d), P(_f32(I1)), P(_f32(I2)), P(_f32(V)), P(out), float(tol), float(lam),
+                            int(max_iter), int(norm), int(n_warps), float(eta), float(sigma), int(scales),
+                            float(huber), P(c8), threads)
     return out

@@ -92,3 +92,22 @@ def test_argument_errors_without_gpu(lib):
     assert msg and b"null" in msg
     assert lib.stt_version().startswith(b"stt ")
     assert C.sizeof(Geometry) == 112  # LP64 layout of stt_geometry
+
+
+def test_flow_argument_checks_without_gpu(lib):
+    """stt_flow_create validates its arguments before touching the device."""
+    from spacetimetomography_b200._lib import FlowParams
+
+    h = C.c_void_p()
+    dims = (C.c_int * 3)(32, 32, 32)
+    bad = [FlowParams(0.1, 1.2, 1.0, 0.65, 0.5, 3000, 4, 3, 0, (C.c_int * 6)(*[0] * 6)),     # scales 0
+           FlowParams(0.1, 0.0, 1.0, 0.65, 0.5, 3000, 4, 3, 3, (C.c_int * 6)(*[0] * 6)),     # lambda 0
+           FlowParams(0.1, 1.2, 1.0, 1.5, 0.5, 3000, 4, 3, 3, (C.c_int * 6)(*[0] * 6)),      # eta > 1
+           FlowParams(0.1, 1.2, 1.0, 0.65, 0.5, 3000, 4, 3, 3, (C.c_int * 6)(-1, 0, 0, 0, 0, 0)),  # cut < 0
+           FlowParams(0.1, 1.2, 1.0, 0.2, 0.5, 3000, 4, 3, 4, (C.c_int * 6)(*[0] * 6))]      # level < 3 voxels
+    for p in bad:
+        assert lib.stt_flow_create(0, dims, C.byref(p), C.byref(h)) == 1
+        assert h.value is None
+        assert lib.stt_last_error(None)
+    assert lib.stt_flow_create(0, (C.c_int * 3)(2, 32, 32), C.byref(FlowParams(
+        0.1, 1.2, 1.0, 0.65, 0.5, 30, 4, 3, 1, (C.c_int * 6)(*[0] * 6))), C.byref(h)) == 1

@@ -173,3 +173,74 @@ def test_permutation_is_a_seeded_shuffle():
     p1, p2 = ob.permutation(5, 50), ob.permutation(5, 50)
     np.testing.assert_array_equal(p1, p2)
     assert sorted(p1.tolist()) == list(range(50)) and not np.array_equal(p1, np.arange(50))
+
+
+# ---- optical flow and the CImg operations it uses --------------------------
+
+FG = np.load(Path(__file__).resolve().parent / "golden" / "reference_flow_golden.npz")
+FLOW_LEVEL_CASES = [  # as tests/golden/gen_golden.py
+    ((0, 0, 0, 0, 0, 0), (11, 10, 9), 20, 0.0),
+    ((2, 1, 1, 3, 2, 2), (16, 13, 12), 30, 0.0),
+    ((0, 0, 0, 0, 0, 0), (11, 10, 9), 120, 1e-3),
+    ((0, 0, 0, 0, 0, 0), (11, 10, 9), 130, 1e30),
+]
+
+
+def test_cimg_image_ops_match_reference_fixture_bitwise():
+    img = FG["img"]
+    np.testing.assert_array_equal(ob.blur32(img, 0.5), FG["blur_05"])
+    np.testing.assert_array_equal(ob.blur32(img, 1.3), FG["blur_13"])
+    for key in ("down", "up", "mixed"):
+        np.testing.assert_array_equal(ob.resize32(img, tuple(FG[f"resize_{key}_dim"])), FG[f"resize_{key}"])
+    np.testing.assert_array_equal(ob.gradient32(img[0]), FG["grad"])
+    np.testing.assert_array_equal(ob.warp_box32(FG["vel"], img, -1.0, (17, 15, 13)), FG["warp_box"])
+
+
+@pytest.mark.parametrize("case", range(len(FLOW_LEVEL_CASES)))
+def test_flow_level_matches_reference_fixture_bitwise(case):
+    roi, box, mi, tol = FLOW_LEVEL_CASES[case]
+    v, y, its = ob.flow_level32(FG["I1"], FG["I2"], FG["V0"], FG["Y0"], roi, box=box, max_iter=mi, tol=tol)
+    np.testing.assert_array_equal(v, FG[f"level{case}_V"])
+    # the reference writes Y back inside the ROI only; outside it Y keeps its input
+    np.testing.assert_array_equal(y, FG[f"level{case}_Y"])
+    if not 1.0 > tol:
+        assert list(its) == [0, 0]  # the residual starts at 1: the loop never runs
+    elif tol == 0.0:
+        assert list(its) == [mi + 1, mi + 1]
+    else:  # stops at a residual iteration (a multiple of 50) or runs out
+        assert all(i == mi + 1 or i % 50 == 0 for i in its)
+
+
+def test_flow_multiscale_matches_reference_fixture_bitwise():
+    v = ob.flow_multiscale32(FG["ms_I1"], FG["ms_I2"], FG["ms_V0"], (3, 2, 2, 4, 1, 3), max_iter=12)
+    np.testing.assert_array_equal(v, FG["ms_V"])
+
+
+@pytest.mark.skipif(ob.REF is None, reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("dims,sigma,odim", [((17, 9, 12), 0.7, (30, 4, 12)), ((8, 8, 8), 2.0, (5, 13, 3))])
+def test_cimg_image_ops_match_live_reference(dims, sigma, odim):
+    rng = np.random.default_rng(sum(dims))
+    nx, ny, nz = dims
+    img = rng.normal(size=(3, nz, ny, nx)).astype(np.float32)
+    np.testing.assert_array_equal(ob.blur32(img, sigma), ob.ref_blur(img, sigma))
+    np.testing.assert_array_equal(ob.resize32(img, odim), ob.ref_resize(img, odim))
+    np.testing.assert_array_equal(ob.gradient32(img[1]), ob.ref_gradient(img[1]))
+
+
+@pytest.mark.skipif(ob.REF is None, reason="reference build (oracle/_ref) not present")
+def test_flow_multiscale_matches_live_reference_with_tolerance_stop():
+    rng = np.random.default_rng(77)
+    shape = (13, 15, 14)
+    i1 = ob.blur32(rng.uniform(0, 1, shape).astype(np.float32), 1.2)
+    i2 = ob.blur32(rng.uniform(0, 1, shape).astype(np.float32), 1.2)
+    v0 = np.zeros((3,) + shape, np.float32)
+    # With an ROI the reference reads its unset gradient arrays outside the ROI
+    # (optical_flow.h:263-290 fill them inside only) and sums them into the
+    # residual, so whether a warp stops at a residual iteration depends on
+    # uninitialised memory (a NaN there stops it even at tol 0).  Cases with
+    # an ROI therefore stay below the first residual iteration (50).
+    for cut, tol, mi in (((1, 1, 2, 1, 0, 1), 0.0, 40), ((0,) * 6, 0.0, 60), ((0,) * 6, 0.5, 75),
+                         ((0,) * 6, 1.0, 10)):
+        a = ob.flow_multiscale32(i1, i2, v0, cut, tol=tol, max_iter=mi, n_warps=2, scales=2, eta=0.7)
+        b = ob.ref_flow_multiscale(i1, i2, v0, cut, tol=tol, max_iter=mi, n_warps=2, scales=2, eta=0.7)
+        np.testing.assert_array_equal(a, b)
