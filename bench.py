@@ -26,6 +26,8 @@ primal-dual loop bodies restated in FP32) on the host's cores.
 from __future__ import annotations
 
 import argparse
+import contextlib
+import ctypes
 import json
 import math
 import os
@@ -59,6 +61,8 @@ def parse_args():
     ap.add_argument("--no-plain", action="store_true", help="skip the per-view (plain) comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-flow", action="store_true", help="skip the optical-flow leg")
+    ap.add_argument("--flow-only", action="store_true",
+                    help="run only the optical-flow leg (one L1Huber_OF level at --n^3) and print its line")
     return ap.parse_args()
 
 
@@ -300,6 +304,24 @@ def fp64_sart_check(ctx, st, args, gmax, n_views: int = 6):
 
 
 # ---------------------------------------------------------------------------
+@contextlib.contextmanager
+def c_stdout_to_stderr():
+    """The reference's C++ code prints progress with std::cout; keep it off
+    stdout, which carries only the JSON line."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        try:
+            ctypes.CDLL(None).fflush(None)
+        except OSError:
+            pass
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 FLOW_BYTES_PER_VOXEL = 152  # minimal state per flow iteration: v 3, y 10, v-extrapolation 3 r/w, grad/ut 4 read
 
 
@@ -350,25 +372,43 @@ def flow_bench(args, dev, stream, rank: int) -> dict:
            "roofline": {"bound": "hbm", "kernel": "k_flow_primal + k_flow_dual", "achieved": achieved,
                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                         "algorithmic_bytes_per_voxel": FLOW_BYTES_PER_VOXEL,
-                        "moved_bytes_per_voxel": 280,
-                        "note": "moved: y 10 r/w, Kx 10 r/w, v 3 r/w, u 4, tau 3, sigma2 1 (reference layout)"}}
+                        "moved_bytes_per_voxel": 212,
+                        "note": "moved per iteration: primal reads y 10, u 3, tau 3, v 3 and writes v 3 (ROI); "
+                                "dual reads v 3, v_old 3, u 4, sigma2 1, y 10 and writes y 10"}}
     if rank == 0 and not args.no_cpu:
-        sys.path.insert(0, str(ROOT / "tests"))
-        import oracle_bind as ob
-
-        n = 64
-        sl = (slice(0, n),) * 3
-        a, b = i1[sl].contiguous().cpu().numpy(), i2[sl].contiguous().cpu().numpy()
-        z3, z10 = np.zeros((3, n, n, n), np.float32), np.zeros((10, n, n, n), np.float32)
-        k = 20
-        t0 = time.perf_counter()
-        ob.flow_level32(a, b, z3, z10, (0,) * 6, tol=0.0, max_iter=k - 1, n_warps=1)
-        tc = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": n ** 3 * k / tc / 1e9, "unit": "Gvoxel-iterations/s", "cores": 1,
-                               "kind": "port",
-                               "sample": f"oracle flow level (one thread, as the reference's residual loop "
-                                         f"requires for determinism), {n}^3 x {k} iterations"}
+        out["cpu_baseline"] = flow_cpu_sample(i1, i2)
     return out
+
+
+def flow_cpu_sample(i1, i2) -> dict:
+    """Per-iteration time of L1Huber_OF on the host cores: the reference's own
+    optical_flow.h (oracle/_ref, OpenMP on every core) when it was built, else
+    the one-thread oracle restatement; two runs that differ only in their
+    iteration count, on the 128^3 corner of the bench images."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_bind as ob
+
+    n, k = 128, 31
+    sl = (slice(0, n),) * 3
+    a, b = i1[sl].contiguous().cpu().numpy(), i2[sl].contiguous().cpu().numpy()
+    z3, z10 = np.zeros((3, n, n, n), np.float32), np.zeros((10, n, n, n), np.float32)
+    cores = os.cpu_count() or 1
+    use_ref = ob.REF is not None
+
+    def run(max_iter):
+        t0 = time.perf_counter()
+        with c_stdout_to_stderr():
+            if use_ref:
+                ob.ref_flow_level(a, b, z3, z10, (0,) * 6, tol=0.0, max_iter=max_iter, n_warps=1, threads=cores)
+            else:
+                ob.flow_level32(a, b, z3, z10, (0,) * 6, tol=0.0, max_iter=max_iter, n_warps=1)
+        return time.perf_counter() - t0
+
+    t_it = (run(k - 1) - run(0)) / (k - 1)
+    return {"value": n ** 3 / t_it / 1e9, "unit": "Gvoxel-iterations/s", "cores": cores if use_ref else 1,
+            "kind": "reference" if use_ref else "port",
+            "sample": f"optical_flow::L1Huber_OF one level, {n}^3, {k} minus 1 iterations, no ROI"
+                      + (" (the reference's code, OpenMP)" if use_ref else " (oracle port, one thread)")}
 
 
 def run_reference(args):
@@ -376,13 +416,14 @@ def run_reference(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_reference_sample(args, threads)
-    vals = []
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        vals.append(cpu_reference_sample(args, threads))
-    wall = time.perf_counter() - t0
+    with c_stdout_to_stderr():
+        for _ in range(args.warmup):
+            cpu_reference_sample(args, threads)
+        vals = []
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            vals.append(cpu_reference_sample(args, threads))
+        wall = time.perf_counter() - t0
     v = statistics.median(r["value"] for r in vals)
     last = vals[-1]
     line = {"impl": "reference", "metric": "projector GUPS over a 4D primal-dual iteration", "value": v,
@@ -549,7 +590,9 @@ def run_stt(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference_sample(args, os.cpu_count() or 1, gpu_check=fp64_sart_check(ctx, st, args, gmax))
+        check = fp64_sart_check(ctx, st, args, gmax)
+        with c_stdout_to_stderr():
+            cpu = cpu_reference_sample(args, os.cpu_count() or 1, gpu_check=check)
 
     if rank == 0:
         line = {"metric": "projector GUPS over a 4D primal-dual iteration", "value": value, "unit": "GUPS",
@@ -582,10 +625,26 @@ def run_stt(args):
     return 0
 
 
+def run_flow_only(args):
+    import torch
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    out = flow_bench(args, dev, stream, 0)
+    line = {"metric": "optical-flow iterations (L1Huber_OF primal + dual)", "value": out["gvoxel_iter_per_s"],
+            "unit": "Gvoxel-iterations/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": out["workload"]}, **out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.flow_only:
+        return run_flow_only(args)
     return run_stt(args)
 
 

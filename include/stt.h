@@ -241,7 +241,7 @@ typedef struct stt_flow_params {
 typedef struct stt_flow stt_flow;
 
 /* Allocates every buffer of a multiscale solve for volumes of size dims
- * (HOST int[3]) on `device`: about 250 bytes per voxel. */
+ * (HOST int[3]) on `device`: about 200 bytes per voxel. */
 stt_status stt_flow_create(int device, const int *dims, const stt_flow_params *p, stt_flow **out);
 const char *stt_flow_last_error(const stt_flow *f);
 stt_status stt_flow_destroy(stt_flow *f);
@@ -259,10 +259,11 @@ stt_status stt_flow_level(stt_flow *f, const int *dim, const float *box, const i
  * be NULL).  Synchronises the device. */
 stt_status stt_flow_stats(stt_flow *f, int *n_entries, int *iters, float *err);
 /* CImg::blur(sigma) (Deriche, order 0, Neumann; CImg.h:32917-33050) in place
- * on nc planes of size dim; dim*nc at most 10x the created volume. */
+ * on nc planes of size dim, each at most the created volume. */
 stt_status stt_flow_blur(stt_flow *f, const int *dim, int nc, float sigma, float *img, void *stream);
 /* CImg::get_resize(odim, nc, 5) (CImg.h:28432-28560): moving average along
- * shrinking axes, Catmull-Rom along growing ones, x then y then z. */
+ * shrinking axes, Catmull-Rom along growing ones, x then y then z.  Every
+ * intermediate plane is at most the created volume; in != out. */
 stt_status stt_flow_resize(stt_flow *f, const int *dim, int nc, const float *in, const int *odim, float *out,
                            void *stream);
 

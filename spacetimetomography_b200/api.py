@@ -262,9 +262,11 @@ class Flow:
     Images (nz, ny, nx), flow V (3, nz, ny, nx), dual Y (10, nz, ny, nx); all
     torch CUDA float32 tensors."""
 
-    def __init__(self, dims, params: FlowParams_ | None = None, device: int = 0):
+    def __init__(self, shape, params: FlowParams_ | None = None, device: int = 0):
+        """shape = (nz, ny, nx) of the full-size images."""
         self.params = params or FlowParams_()
-        nz, ny, nx = dims
+        self.shape = tuple(int(v) for v in shape)
+        nz, ny, nx = self.shape
         h = C.c_void_p()
         pc = self.params.c()
         rc = lib.stt_flow_create(int(device), (C.c_int * 3)(nx, ny, nz), C.byref(pc), C.byref(h))
@@ -278,11 +280,18 @@ class Flow:
 
     def multiscale(self, I1, I2, V, Y0=None, stream=None):
         """V: initial flow in, finest flow out (in place)."""
+        shp = self.shape
+        if tuple(I1.shape) != shp or tuple(I2.shape) != shp or tuple(V.shape) != (3,) + shp or (
+                Y0 is not None and tuple(Y0.shape) != (10,) + shp):
+            raise ValueError(f"multiscale expects images {shp}, V (3,)+{shp}, Y0 (10,)+{shp}")
         self._chk(lib.stt_flow_multiscale(self._h, _ptr(I1), _ptr(I2), _ptr(V), _ptr(Y0), _stream(stream)))
         return V
 
     def level(self, I1, I2, V, Y, roi, box=None, stream=None):
         nz, ny, nx = I1.shape
+        shp = tuple(I1.shape)
+        if tuple(I2.shape) != shp or tuple(V.shape) != (3,) + shp or tuple(Y.shape) != (10,) + shp:
+            raise ValueError("level expects I1, I2 of one shape, V (3,)+shape and Y (10,)+shape")
         box = (nx, ny, nz) if box is None else box
         self._chk(lib.stt_flow_level(self._h, _dim3(I1), (C.c_float * 3)(*map(float, box)),
                                      (C.c_int * 6)(*map(int, roi)), _ptr(I1), _ptr(I2), _ptr(V), _ptr(Y),

@@ -13,7 +13,13 @@
 //
 // Layout: planar x-fastest fields, idx = x + y*nx + z*nx*ny, channel planes of
 // n = nx*ny*nz floats (CImg's layout).  Dual field y: 10 planes Y1|Y2|Y3|Y4.
+// Per iteration the primal step reads y, u, tau and the flow and writes the
+// next flow into a second buffer; the dual step reads both flows (K v and
+// K v_old), u and sigma2 and updates y in place: 53 floats per voxel instead
+// of the 70 of the reference's layout, which also stores K v (10 floats).
+#include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cstdint>
 
 #include "stt_kernels.h"
@@ -134,15 +140,20 @@ __global__ void __launch_bounds__(128) k_warp_box(const Dims d, const float bx, 
 // ut = I2w - I1 - grad.v.  Outside the ROI the reference leaves these arrays
 // unset; here they are 0.  Everywhere: tau_c = 1/(4 + |u_c|) and
 // sigma2 = 1/(|ux| + |uy| + |uz|) (infinite where the gradient vanishes).
+// Before u is replaced, k4prev = u_prev . v keeps the data-term part of the
+// previous warp's last K v, which the first dual step of this warp uses as
+// its K v_old (the reference keeps Kx across warps, optical_flow.h:246, 394).
 __global__ void __launch_bounds__(128) k_flow_setup(const Dims d, const FlowRoi roi, const float *__restrict__ i2w,
                                                     const float *__restrict__ i1, const float *__restrict__ v,
                                                     float *__restrict__ u, float *__restrict__ tau,
-                                                    float *__restrict__ sig2) {
+                                                    float *__restrict__ sig2, float *__restrict__ k4prev) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     if (i >= d.x) return;
     const long long sy = d.x, sz = (long long)d.x * d.y, n = sz * d.z;
     const long long p = i + j * sy + k * sz;
+    const float v1 = __ldg(v + p), v2 = __ldg(v + n + p), v3 = __ldg(v + 2 * n + p);
+    k4prev[p] = u[p] * v1 + u[n + p] * v2 + u[2 * n + p] * v3;
     float ux = 0.0f, uy = 0.0f, uz = 0.0f, ut = 0.0f;
     if (in_roi(roi, d, i, j, k)) {
         const long long xm = i > 0 ? p - 1 : p, xp = i < d.x - 1 ? p + 1 : p;
@@ -151,7 +162,7 @@ __global__ void __launch_bounds__(128) k_flow_setup(const Dims d, const FlowRoi 
         ux = (__ldg(i2w + xp) - __ldg(i2w + xm)) / 2;
         uy = (__ldg(i2w + yp) - __ldg(i2w + ym)) / 2;
         uz = (__ldg(i2w + zp) - __ldg(i2w + zm)) / 2;
-        ut = __ldg(i2w + p) - __ldg(i1 + p) - ux * __ldg(v + p) - uy * __ldg(v + n + p) - uz * __ldg(v + 2 * n + p);
+        ut = __ldg(i2w + p) - __ldg(i1 + p) - ux * v1 - uy * v2 - uz * v3;
     }
     u[p] = ux;
     u[n + p] = uy;
@@ -163,114 +174,182 @@ __global__ void __launch_bounds__(128) k_flow_setup(const Dims d, const FlowRoi 
     sig2[p] = 1.0f / (fabsf(ux) + fabsf(uy) + fabsf(uz));
 }
 
-// Backward difference of S/ImageFormationModel/tools.cpp:146-192 (dxm3, dym3, dzm3).
-__device__ __forceinline__ float dm(const float *__restrict__ f, long long p, int c, int n, long long st) {
-    if (c > 0 && c < n - 1) return __ldg(f + p) - __ldg(f + p - st);
-    if (c == 0) return __ldg(f + p);
-    return -__ldg(f + p - st);
+// Backward difference of S/ImageFormationModel/tools.cpp:146-192 (dxm3, dym3,
+// dzm3) at coordinate c of n along a stride st, from the centre value a and
+// the lower neighbour b (read only when c > 0): interior a - b, first a,
+// last -b.
+__device__ __forceinline__ float dm(float a, float b, int c, int n) {
+    return (c > 0 && c < n - 1) ? a - b : (c == 0 ? a : -b);
 }
 
-// Forward difference of tools.cpp:126-138 (dxp3, dyp3, dzp3).
-__device__ __forceinline__ float dp(const float *__restrict__ f, long long p, int c, int n, long long st) {
-    return c < n - 1 ? __ldg(f + p + st) - __ldg(f + p) : 0.0f;
-}
+// Forward difference of tools.cpp:126-138 (dxp3, dyp3, dzp3): upper
+// neighbour b (read only when c < n-1) minus the centre a, 0 at the last.
+__device__ __forceinline__ float dp(float a, float b, int c, int n) { return c < n - 1 ? b - a : 0.0f; }
 
-// flags: bit 0 = residual iteration (iteration % 50 == 0), bit 1 = keep K^T y
-// for the next iteration's residual.
-constexpr int kResid = 1, kKeepKty = 2;
+// flags: bit 0 = residual iteration (iteration % 50 == 0); bit 1 = keep K^T y
+// for the next iteration's residual; bit 2 = first iteration of the level
+// (K v_old = 0, optical_flow.h:231-243); bit 3 = first iteration of a later
+// warp (the data-term row of K v_old from k4prev).
+constexpr int kResid = 1, kKeepKty = 2, kFirstOfLevel = 4, kFirstOfWarp = 8;
 
 __device__ __forceinline__ void add_resid(double *resid, float r) {
     for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
     if ((threadIdx.x & 31) == 0 && r != 0.0f) atomicAdd(resid, (double)r);
 }
 
+// Offsets inside one level are 32-bit: the host keeps 10 * voxels < 2^31.
+// Every load of a voxel's neighbourhood is issued before the arithmetic.
+
 // Primal step over the ROI (optical_flow.h:314-370):
-// Kty_c = -div_b(y_c) + u_c*y4; v_c -= tau_c*Kty_c.
+// Kty_c = -div_b(y_c) + u_c*y4; v_c -= tau_c*Kty_c, read from v_in and
+// written to v_out (the dual step needs both).  Outside the ROI v_in and
+// v_out hold the same, never-updated values.
 __global__ void __launch_bounds__(128) k_flow_primal(const Dims d, const FlowRoi roi, const float *__restrict__ y,
                                                      const float *__restrict__ u, const float *__restrict__ tau,
-                                                     float *__restrict__ v, float *__restrict__ kty, int flags,
-                                                     double *__restrict__ resid, const int *__restrict__ done) {
+                                                     const float *__restrict__ v_in, float *__restrict__ v_out,
+                                                     float *__restrict__ kty, int flags, double *__restrict__ resid,
+                                                     const int *__restrict__ done) {
     if (*done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     float pr = 0.0f;
     if (i < d.x && in_roi(roi, d, i, j, k)) {
-        const long long sy = d.x, sz = (long long)d.x * d.y, n = sz * d.z;
-        const long long p = i + j * sy + k * sz;
-        const float y4 = __ldg(y + 9 * n + p);
+        const int sy = d.x, sz = d.x * d.y, n = sz * d.z;
+        const long long p = i + (long long)j * sy + (long long)k * sz;
+        const float *yp = y + p;
+        const int ox = i > 0 ? 1 : 0, oy = j > 0 ? sy : 0, oz = k > 0 ? sz : 0;
+        float a[9], b[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const int off = q * n, st = (q % 3 == 0) ? ox : (q % 3 == 1 ? oy : oz);
+            a[q] = __ldg(yp + off);
+            b[q] = __ldg(yp + off - st);
+        }
+        const float y4 = __ldg(yp + 9 * n);
+        float uc[3], vo[3], t[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const float *yc = y + 3 * c * n;
-            const float kt = -1.0f * dm(yc, p, i, d.x, 1) - 1.0f * dm(yc + n, p, j, d.y, sy) -
-                             1.0f * dm(yc + 2 * n, p, k, d.z, sz) + __ldg(u + c * n + p) * y4;
-            const float vo = v[c * n + p];
-            const float t = __ldg(tau + c * n + p);
-            const float vn = vo - t * kt;
-            v[c * n + p] = vn;
+            uc[c] = __ldg(u + p + c * n);
+            vo[c] = __ldg(v_in + p + c * n);
+            t[c] = __ldg(tau + p + c * n);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            // -stepsizeD * dxm3 - ... with unit step sizes: (-1 * x) == -x and 1 * x == x exactly
+            const float kt = -dm(a[3 * c], b[3 * c], i, d.x) - dm(a[3 * c + 1], b[3 * c + 1], j, d.y) -
+                             dm(a[3 * c + 2], b[3 * c + 2], k, d.z) + uc[c] * y4;
+            const float vn = vo[c] - t[c] * kt;
+            v_out[p + c * n] = vn;
             if (flags & kResid) {
-                const float r = fabsf((vo - vn) / t - kty[c * n + p] + kt);
+                const float r = fabsf((vo[c] - vn) / t[c] - kty[p + c * n] + kt);
                 pr = c == 0 ? r : pr + r;
             }
-            if (flags & kKeepKty) kty[c * n + p] = kt;
+            if (flags & kKeepKty) kty[p + c * n] = kt;
         }
     }
     if (flags & kResid) add_resid(resid, pr);
 }
 
-// Dual step over every voxel (optical_flow.h:374-497): Kx = forward
-// differences of v and u.v; over-relaxed ascent y + sigma1*(2Kx - Kx_old),
+// Dual step over every voxel (optical_flow.h:374-497): K v by forward
+// differences of v and u.v; over-relaxed ascent y + sigma1*(2 K v - K v_old),
 // scaled by the Huber factor for norm 4; each y_c projected onto the
-// lambda-ball; y4 clamped to [-1, 1].
+// lambda-ball; y4 clamped to [-1, 1].  K v_old, which the reference stores
+// (10 floats per voxel), is recomputed here from v_old with the same float
+// operations, so it is the same value.
 __global__ void __launch_bounds__(128) k_flow_dual(const Dims d, const float *__restrict__ v,
-                                                   const float *__restrict__ u, const float *__restrict__ sig2,
-                                                   float *__restrict__ y, float *__restrict__ kx, float sigma1, float hf,
-                                                   float lambda, int huber, int flags, double *__restrict__ resid,
+                                                   const float *__restrict__ v_old, const float *__restrict__ u,
+                                                   const float *__restrict__ sig2, const float *__restrict__ k4prev,
+                                                   float *__restrict__ y, float sigma1, float hf, float lambda,
+                                                   float lam2_lo, int huber, int flags, double *__restrict__ resid,
                                                    const int *__restrict__ done) {
     if (*done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     float dr = 0.0f;
     if (i < d.x) {
-        const long long sy = d.x, sz = (long long)d.x * d.y, n = sz * d.z;
-        const long long p = i + j * sy + k * sz;
+        const int sy = d.x, sz = d.x * d.y, n = sz * d.z;
+        const long long p = i + (long long)j * sy + (long long)k * sz;
+        const int ox = i < d.x - 1 ? 1 : 0, oy = j < d.y - 1 ? sy : 0, oz = k < d.z - 1 ? sz : 0;
+        const bool zero_old = flags & kFirstOfLevel;
+        const float *vp = v + p, *op = v_old + p;
+        float vc[3], vx[3], vy[3], vz[3], oc[3], oxv[3], oyv[3], ozv[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const float *vc = v + c * n;
-            const float kn[3] = {1.0f * dp(vc, p, i, d.x, 1), 1.0f * dp(vc, p, j, d.y, sy),
-                                 1.0f * dp(vc, p, k, d.z, sz)};
-            float yt[3], yo[3], ko[3];
+            const int off = c * n;
+            vc[c] = __ldg(vp + off);
+            vx[c] = __ldg(vp + off + ox);
+            vy[c] = __ldg(vp + off + oy);
+            vz[c] = __ldg(vp + off + oz);
+            if (!zero_old) {
+                oc[c] = __ldg(op + off);
+                oxv[c] = __ldg(op + off + ox);
+                oyv[c] = __ldg(op + off + oy);
+                ozv[c] = __ldg(op + off + oz);
+            }
+        }
+        float *yp = y + p;
+        float yo[10];
+#pragma unroll
+        for (int q = 0; q < 10; ++q) yo[q] = yp[q * n];
+        const float u1 = __ldg(u + p), u2 = __ldg(u + p + n), u3 = __ldg(u + p + 2 * n), ut = __ldg(u + p + 3 * n);
+        const float s2 = __ldg(sig2 + p);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            // K v with unit step sizes (stepsizeD = 1: x * 1.0f == x, dropped)
+            const float kn[3] = {dp(vc[c], vx[c], i, d.x), dp(vc[c], vy[c], j, d.y), dp(vc[c], vz[c], k, d.z)};
+            float ko[3] = {0.0f, 0.0f, 0.0f};
+            if (!zero_old) {
+                ko[0] = dp(oc[c], oxv[c], i, d.x);
+                ko[1] = dp(oc[c], oyv[c], j, d.y);
+                ko[2] = dp(oc[c], ozv[c], k, d.z);
+            }
+            float yt[3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                const long long q = (3 * c + a) * n + p;
-                yo[a] = y[q];
-                ko[a] = kx[q];
-                const float t = yo[a] + sigma1 * (kn[a] + kn[a] - ko[a]);
+                const float t = yo[3 * c + a] + sigma1 * (kn[a] + kn[a] - ko[a]);
                 yt[a] = huber ? t * hf : t;
             }
-            const float div = smax(1.0f, sqrtf(yt[0] * yt[0] + yt[1] * yt[1] + yt[2] * yt[2]) / lambda);
+            // divisor = max(1, sqrt(s)/lambda) and y = yt/divisor.  Below
+            // lam2_lo (< lambda^2 with margin) sqrt(s) rounds below lambda, so
+            // the divisor is exactly 1 and y = yt exactly: skip the sqrt and
+            // the divisions.
+            const float ss = yt[0] * yt[0] + yt[1] * yt[1] + yt[2] * yt[2];
+            float yn[3] = {yt[0], yt[1], yt[2]};
+            if (!(ss < lam2_lo)) {
+                const float div = smax(1.0f, sqrtf(ss) / lambda);
+                if (div != 1.0f) {
+                    yn[0] = yt[0] / div;
+                    yn[1] = yt[1] / div;
+                    yn[2] = yt[2] / div;
+                }
+            }
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                const long long q = (3 * c + a) * n + p;
-                const float yn = yt[a] / div;
-                y[q] = yn;
-                kx[q] = kn[a];
+                yp[(3 * c + a) * n] = yn[a];
                 if (flags & kResid) {
-                    const float r = fabsf((yo[a] - yn) / sigma1 - ko[a] + kn[a]);
+                    const float r = fabsf((yo[3 * c + a] - yn[a]) / sigma1 - ko[a] + kn[a]);
                     dr = (c == 0 && a == 0) ? r : dr + r;
                 }
             }
         }
-        const float k4 = __ldg(u + p) * __ldg(v + p) + __ldg(u + n + p) * __ldg(v + n + p) +
-                         __ldg(u + 2 * n + p) * __ldg(v + 2 * n + p);
-        const float k4o = kx[9 * n + p];
-        const float y4o = y[9 * n + p];
-        const float s2 = __ldg(sig2 + p);
-        const float y4 = smax(-1.0f, smin(1.0f, y4o + s2 * (k4 + k4 - k4o + __ldg(u + 3 * n + p))));
-        y[9 * n + p] = y4;
-        kx[9 * n + p] = k4;
-        if (flags & kResid) dr = dr + fabsf((y4o - y4) / s2 - k4o + k4);
+        const float k4 = u1 * vc[0] + u2 * vc[1] + u3 * vc[2];
+        float k4o = 0.0f;
+        if (flags & kFirstOfWarp) k4o = __ldg(k4prev + p);
+        else if (!zero_old) k4o = u1 * oc[0] + u2 * oc[1] + u3 * oc[2];
+        const float y4 = smax(-1.0f, smin(1.0f, yo[9] + s2 * (k4 + k4 - k4o + ut)));
+        yp[9 * n] = y4;
+        if (flags & kResid) dr = dr + fabsf((yo[9] - y4) / s2 - k4o + k4);
     }
     if (flags & kResid) add_resid(resid + 1, dr);
+}
+
+// End of a warp: the flow of the last iteration that ran lies in the second
+// buffer when that count is odd; bring it back to the first.
+__global__ void __launch_bounds__(256) k_flow_settle(long long n3, const int *__restrict__ iters,
+                                                     const float *__restrict__ v_b, float *__restrict__ v_a) {
+    if ((*iters & 1) == 0) return;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n3; q += (long long)gridDim.x * blockDim.x)
+        v_a[q] = v_b[q];
 }
 
 // Stopping rule of optical_flow.h:306, 488-491: after a residual iteration
@@ -457,22 +536,34 @@ cudaError_t launch_warp_box(const int *dim, const float *box, const float *vel, 
 }
 
 cudaError_t launch_flow_setup(const int *d, const FlowRoi &roi, const float *i2w, const float *i1, const float *v,
-                              float *u, float *tau, float *sig2, cudaStream_t s) {
-    k_flow_setup<<<vox_grid(d), 128, 0, s>>>(Dims{d[0], d[1], d[2]}, roi, i2w, i1, v, u, tau, sig2);
+                              float *u, float *tau, float *sig2, float *k4prev, cudaStream_t s) {
+    k_flow_setup<<<vox_grid(d), 128, 0, s>>>(Dims{d[0], d[1], d[2]}, roi, i2w, i1, v, u, tau, sig2, k4prev);
     return cudaGetLastError();
 }
 
 cudaError_t launch_flow_primal(const int *d, const FlowRoi &roi, const float *y, const float *u, const float *tau,
-                               float *v, float *kty, int flags, double *resid, const int *done, cudaStream_t s) {
-    k_flow_primal<<<vox_grid(d), 128, 0, s>>>(Dims{d[0], d[1], d[2]}, roi, y, u, tau, v, kty, flags, resid, done);
+                               const float *v_in, float *v_out, float *kty, int flags, double *resid, const int *done,
+                               cudaStream_t s) {
+    k_flow_primal<<<vox_grid(d), 128, 0, s>>>(Dims{d[0], d[1], d[2]}, roi, y, u, tau, v_in, v_out, kty, flags, resid,
+                                              done);
     return cudaGetLastError();
 }
 
-cudaError_t launch_flow_dual(const int *d, const float *v, const float *u, const float *sig2, float *y, float *kx,
-                             float sigma1, float hf, float lambda, int huber, int flags, double *resid,
-                             const int *done, cudaStream_t s) {
-    k_flow_dual<<<vox_grid(d), 128, 0, s>>>(Dims{d[0], d[1], d[2]}, v, u, sig2, y, kx, sigma1, hf, lambda, huber,
-                                            flags, resid, done);
+cudaError_t launch_flow_dual(const int *d, const float *v, const float *v_old, const float *u, const float *sig2,
+                             const float *k4prev, float *y, float sigma1, float hf, float lambda, int huber, int flags,
+                             double *resid, const int *done, cudaStream_t s) {
+    // lam2_lo = lambda^2 (1 - 2^-20) rounded down: s < lam2_lo gives sqrt(s) < lambda (1 - 2^-21), whose float
+    // rounding stays below lambda, so sqrt(s)/lambda rounds to at most 1.
+    const double l2 = (double)lambda * (double)lambda * (1.0 - 1.0 / 1048576.0);
+    float lam2_lo = (float)l2;
+    if ((double)lam2_lo > l2) lam2_lo = std::nextafter(lam2_lo, 0.0f);
+    k_flow_dual<<<vox_grid(d), 128, 0, s>>>(Dims{d[0], d[1], d[2]}, v, v_old, u, sig2, k4prev, y, sigma1, hf, lambda,
+                                            lam2_lo, huber, flags, resid, done);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flow_settle(long long n3, const int *iters, const float *v_b, float *v_a, cudaStream_t s) {
+    k_flow_settle<<<(unsigned)std::min<long long>((n3 + 255) / 256, 148 * 16), 256, 0, s>>>(n3, iters, v_b, v_a);
     return cudaGetLastError();
 }
 

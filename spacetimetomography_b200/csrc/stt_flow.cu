@@ -62,8 +62,8 @@ struct stt_flow {
     std::vector<float *> pyr1, pyr2;           // the coarser levels of the pyramid
     float *vbuf[2] = {nullptr, nullptr};       // flow of the coarser levels
     float *ybuf[2] = {nullptr, nullptr};       // dual of every level
-    float *yw = nullptr, *kx = nullptr, *kty = nullptr, *u = nullptr, *tau = nullptr, *sig2 = nullptr,
-          *i2w = nullptr;
+    float *yw = nullptr, *vpp = nullptr, *kty = nullptr, *u = nullptr, *tau = nullptr, *sig2 = nullptr,
+          *i2w = nullptr, *k4prev = nullptr;
     int *tsrc = nullptr;
     double *tfrac = nullptr;
     double *resid = nullptr;
@@ -106,17 +106,20 @@ struct stt_flow {
 namespace {
 
 // Deriche blur along x, y, z of every axis longer than 1 (CImg::blur,
-// CImg.h:33249-33262), in place; scratch = f->yw.
+// CImg.h:33249-33262), in place, one channel at a time; scratch = f->i2w.
 stt_status enqueue_blur(stt_flow *f, const int *d, int nc, float sigma, float *img, cudaStream_t s) {
     if (sigma < 0.1f) return STT_OK;  // deriche() leaves the image unchanged
     const stt::DericheCoef c = deriche_coefs(sigma);
-    for (int axis = 0; axis < 3; ++axis)
-        if (d[axis] > 1) FLOW_CUDA(f, stt::launch_deriche(d, nc, axis, c, img, f->yw, s), "k_deriche_line");
+    for (int ch = 0; ch < nc; ++ch)
+        for (int axis = 0; axis < 3; ++axis)
+            if (d[axis] > 1)
+                FLOW_CUDA(f, stt::launch_deriche(d, 1, axis, c, img + ch * vol(d), f->i2w, s), "k_deriche_line");
     return STT_OK;
 }
 
 // get_resize(odim, nc, 5): one pass per axis whose extent changes, x then y
-// then z, ping-ponging through f->yw and f->kx.
+// then z, one channel at a time, ping-ponging through f->i2w and f->sig2
+// (both free between levels).
 stt_status enqueue_resize(stt_flow *f, const int *di, int nc, const float *in, const int *dout, float *out,
                           cudaStream_t s) {
     int axes[3], na = 0;
@@ -128,36 +131,41 @@ stt_status enqueue_resize(stt_flow *f, const int *di, int nc, const float *in, c
                       "resize copy");
         return STT_OK;
     }
-    int cur[3] = {di[0], di[1], di[2]};
-    const float *src = in;
-    for (int q = 0; q < na; ++q) {
-        const int a = axes[q];
-        stt::ResizeAxis ra{};
-        ra.axis = a;
-        ra.nc = nc;
-        ra.ix = cur[0];
-        ra.iy = cur[1];
-        ra.iz = cur[2];
-        ra.old_n = cur[a];
-        ra.new_n = dout[a];
-        cur[a] = dout[a];
-        ra.ox = cur[0];
-        ra.oy = cur[1];
-        ra.oz = cur[2];
-        ra.mode = ra.new_n < ra.old_n ? 0 : 1;
-        if (ra.mode == 1) {
-            FLOW_CUDA(f, stt::launch_resize_table(ra.old_n, ra.new_n, f->tsrc, f->tfrac, s), "k_resize_table");
-            ra.src = f->tsrc;
-            ra.frac = f->tfrac;
+    for (int ch = 0; ch < nc; ++ch) {
+        int cur[3] = {di[0], di[1], di[2]};
+        const float *src = in + ch * vol(di);
+        for (int q = 0; q < na; ++q) {
+            const int a = axes[q];
+            stt::ResizeAxis ra{};
+            ra.axis = a;
+            ra.nc = 1;
+            ra.ix = cur[0];
+            ra.iy = cur[1];
+            ra.iz = cur[2];
+            ra.old_n = cur[a];
+            ra.new_n = dout[a];
+            cur[a] = dout[a];
+            ra.ox = cur[0];
+            ra.oy = cur[1];
+            ra.oz = cur[2];
+            ra.mode = ra.new_n < ra.old_n ? 0 : 1;
+            if (ra.mode == 1) {
+                FLOW_CUDA(f, stt::launch_resize_table(ra.old_n, ra.new_n, f->tsrc, f->tfrac, s), "k_resize_table");
+                ra.src = f->tsrc;
+                ra.frac = f->tfrac;
+            }
+            float *dst = q == na - 1 ? out + ch * vol(dout) : (q % 2 == 0 ? f->i2w : f->sig2);
+            FLOW_CUDA(f, stt::launch_resize_axis(ra, src, dst, s), "k_resize_axis");
+            src = dst;
         }
-        float *dst = q == na - 1 ? out : (q % 2 == 0 ? f->yw : f->kx);
-        FLOW_CUDA(f, stt::launch_resize_axis(ra, src, dst, s), "k_resize_axis");
-        src = dst;
     }
     return STT_OK;
 }
 
-// One L1Huber_OF call (optical_flow.h:83-623) on a level of size d.
+// One L1Huber_OF call (optical_flow.h:83-623) on a level of size d.  The
+// flow alternates between V and f->vpp: iteration `it` reads buffer
+// (it-1)&1 and writes buffer it&1; k_flow_settle brings the last one back
+// into V at the end of every warp.
 stt_status enqueue_level(stt_flow *f, const int *d, const float *box, const int *roi6, const float *i1,
                          const float *i2, float *V, float *Y, int stat0, cudaStream_t s) {
     const stt_flow_params &p = f->p;
@@ -165,23 +173,30 @@ stt_status enqueue_level(stt_flow *f, const int *d, const float *box, const int 
     const stt::FlowRoi roi{roi6[0], roi6[1], roi6[2], roi6[3], roi6[4], roi6[5]};
     const float sigma1 = std::min(1.0f / 3.0f, std::min(1.0f / 3.0f, 1.0f / 3.0f));
     const float hf = 1.0f / (1.0f + sigma1 * p.huber / p.lambda);
+    float *vb[2] = {V, f->vpp};
     FLOW_CUDA(f, cudaMemcpyAsync(f->yw, Y, sizeof(float) * 10 * n, cudaMemcpyDeviceToDevice, s), "copy Y");
-    FLOW_CUDA(f, cudaMemsetAsync(f->kx, 0, sizeof(float) * 10 * n, s), "clear Kx");
+    FLOW_CUDA(f, cudaMemcpyAsync(f->vpp, V, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s), "copy V");
     FLOW_CUDA(f, cudaMemsetAsync(f->kty, 0, sizeof(float) * 3 * n, s), "clear Kty");
     const bool runs = 1.0f > p.tol;  // err starts at 1 (optical_flow.h:305-306)
     const int last = p.max_iter + 1;
+    bool any_dual = false;
     for (int w = 0; w < p.n_warps; ++w) {
         int *it_slot = f->iters + stat0 + w;
         float *err_slot = f->errs + stat0 + w;
         FLOW_CUDA(f, stt::launch_flow_reset(f->done, f->resid, it_slot, err_slot, s), "k_flow_reset");
         FLOW_CUDA(f, stt::launch_warp_box(d, box, V, i2, 1, -1.0f, f->i2w, s), "k_warp_box");
-        FLOW_CUDA(f, stt::launch_flow_setup(d, roi, f->i2w, i1, V, f->u, f->tau, f->sig2, s), "k_flow_setup");
-        if (!runs || last < 1) continue;
+        FLOW_CUDA(f, stt::launch_flow_setup(d, roi, f->i2w, i1, V, f->u, f->tau, f->sig2, f->k4prev, s),
+                  "k_flow_setup");
+        if (!runs) continue;
         for (int it = 1; it <= last; ++it) {
-            const int flags = (it % 50 == 0 ? 1 : 0) | ((it + 1) % 50 == 0 ? 2 : 0);
-            FLOW_CUDA(f, stt::launch_flow_primal(d, roi, f->yw, f->u, f->tau, V, f->kty, flags, f->resid, f->done, s),
+            int flags = (it % 50 == 0 ? 1 : 0) | ((it + 1) % 50 == 0 ? 2 : 0);
+            if (it == 1) flags |= any_dual ? 8 : 4;
+            const float *vin = vb[(it - 1) & 1];
+            float *vout = vb[it & 1];
+            FLOW_CUDA(f, stt::launch_flow_primal(d, roi, f->yw, f->u, f->tau, vin, vout, f->kty, flags, f->resid,
+                                                 f->done, s),
                       "k_flow_primal");
-            FLOW_CUDA(f, stt::launch_flow_dual(d, V, f->u, f->sig2, f->yw, f->kx, sigma1, hf, p.lambda,
+            FLOW_CUDA(f, stt::launch_flow_dual(d, vout, vin, f->u, f->sig2, f->k4prev, f->yw, sigma1, hf, p.lambda,
                                                p.norm == 4 ? 1 : 0, flags, f->resid, f->done, s),
                       "k_flow_dual");
             if ((flags & 1) || it == last)
@@ -189,6 +204,8 @@ stt_status enqueue_level(stt_flow *f, const int *d, const float *box, const int 
                                                     err_slot, s),
                           "k_flow_check");
         }
+        any_dual = true;
+        FLOW_CUDA(f, stt::launch_flow_settle(3 * n, it_slot, f->vpp, V, s), "k_flow_settle");
     }
     FLOW_CUDA(f, stt::launch_copy_roi(d, 10, roi, f->yw, Y, s), "k_copy_roi");
     return STT_OK;
@@ -218,8 +235,8 @@ stt_status stt_flow_create(int device, const int *dims, const stt_flow_params *p
     for (int a = 0; a < 3; ++a)
         if (dims[a] < 3 || dims[a] > kFlowMaxDim)
             return stt_internal_set_error(nullptr, STT_ERR_INVALID, "flow dims must be in [3, 4096]");
-    if (vol(dims) * 10 >= (1LL << 40))
-        return stt_internal_set_error(nullptr, STT_ERR_INVALID, "flow volume too large");
+    if (vol(dims) * 10 >= (1LL << 31))  // the kernels address the 10 dual planes with 32-bit offsets
+        return stt_internal_set_error(nullptr, STT_ERR_INVALID, "flow volume too large (10 * voxels must be < 2^31)");
     // Pyramid sizes (optical_flow.h:659-677): dims * eta^s, eta^s accumulated in float.
     std::vector<Level> lev;
     float t_eta = 1.0f;
@@ -264,7 +281,8 @@ stt_status stt_flow_create(int device, const int *dims, const stt_flow_params *p
         A(&f->ybuf[b], 10 * n);
     }
     A(&f->yw, 10 * n);
-    A(&f->kx, 10 * n);
+    A(&f->vpp, 3 * n);
+    A(&f->k4prev, n);
     A(&f->kty, 3 * n);
     A(&f->u, 4 * n);
     A(&f->tau, 3 * n);
@@ -375,8 +393,8 @@ stt_status stt_flow_blur(stt_flow *f, const int *dim, int nc, float sigma, float
     if (!f) return stt_internal_set_error(nullptr, STT_ERR_INVALID, "null flow");
     if (!dim || !img || nc < 1) return f->fail(STT_ERR_INVALID, "null argument or nc < 1");
     if (dim[0] < 1 || dim[1] < 1 || dim[2] < 1 || dim[0] > kFlowMaxDim || dim[1] > kFlowMaxDim ||
-        dim[2] > kFlowMaxDim || vol(dim) * nc > 10 * f->nmax)
-        return f->fail(STT_ERR_INVALID, "blur size out of range (at most 10x the created volume)");
+        dim[2] > kFlowMaxDim || vol(dim) > f->nmax)
+        return f->fail(STT_ERR_INVALID, "blur size out of range (each channel at most the created volume)");
     FLOW_CUDA(f, cudaSetDevice(f->device), "cudaSetDevice");
     return enqueue_blur(f, dim, nc, sigma, img, S(stream));
 }
@@ -390,8 +408,8 @@ stt_status stt_flow_resize(stt_flow *f, const int *dim, int nc, const float *in,
         if (dim[a] < 2 || odim[a] < 1 || odim[a] > kTableCap)
             return f->fail(STT_ERR_INVALID, "resize extents out of range (input >= 2, output in [1, 8192])");
         cur[a] = odim[a];
-        if (vol(cur) * nc > 10 * f->nmax)
-            return f->fail(STT_ERR_INVALID, "resize intermediate larger than the scratch (10x the created volume)");
+        if (vol(cur) > f->nmax)
+            return f->fail(STT_ERR_INVALID, "resize intermediate larger than the created volume");
     }
     if (in == out) return f->fail(STT_ERR_INVALID, "resize cannot run in place");
     FLOW_CUDA(f, cudaSetDevice(f->device), "cudaSetDevice");

@@ -71,13 +71,14 @@ struct ResizeAxis {
 cudaError_t launch_warp_box(const int *dim, const float *box, const float *vel, const float *src, int nc,
                             float dt, float *out, cudaStream_t s);
 cudaError_t launch_flow_setup(const int *d, const FlowRoi &roi, const float *i2w, const float *i1,
-                              const float *v, float *u, float *tau, float *sig2, cudaStream_t s);
+                              const float *v, float *u, float *tau, float *sig2, float *k4prev, cudaStream_t s);
 cudaError_t launch_flow_primal(const int *d, const FlowRoi &roi, const float *y, const float *u,
-                               const float *tau, float *v, float *kty, int flags, double *resid,
-                               const int *done, cudaStream_t s);
-cudaError_t launch_flow_dual(const int *d, const float *v, const float *u, const float *sig2, float *y,
-                             float *kx, float sigma1, float hf, float lambda, int huber, int flags,
-                             double *resid, const int *done, cudaStream_t s);
+                               const float *tau, const float *v_in, float *v_out, float *kty, int flags,
+                               double *resid, const int *done, cudaStream_t s);
+cudaError_t launch_flow_dual(const int *d, const float *v, const float *v_old, const float *u, const float *sig2,
+                             const float *k4prev, float *y, float sigma1, float hf, float lambda, int huber,
+                             int flags, double *resid, const int *done, cudaStream_t s);
+cudaError_t launch_flow_settle(long long n3, const int *iters, const float *v_b, float *v_a, cudaStream_t s);
 cudaError_t launch_flow_check(double *resid, long long n, float tol, int it, int is_resid, int is_last,
                               int *done, int *iters, float *err, cudaStream_t s);
 cudaError_t launch_flow_reset(int *done, double *resid, int *iters, float *err, cudaStream_t s);

@@ -39,9 +39,10 @@ def _np(t):
     return t.detach().cpu().numpy()
 
 
-def _flow(dims, **kw):
+def _flow(shape, **kw):
+    """shape = (nz, ny, nx), the torch shape of one image."""
     stt = _stt()
-    return stt.Flow(dims, stt.FlowParams(**kw))
+    return stt.Flow(shape, stt.FlowParams(**kw))
 
 
 def _images(shape, seed, smooth=1.2):
@@ -124,7 +125,7 @@ FLOW_LEVEL_CASES = [  # as tests/golden/gen_golden.py
 @pytest.mark.parametrize("case", range(len(FLOW_LEVEL_CASES)))
 def test_flow_level_matches_reference_fixture(cuda, case):
     roi, box, mi, tol = FLOW_LEVEL_CASES[case]
-    f = _flow((11, 10, 9), max_iter=mi, tol=tol, n_warps=2)
+    f = _flow((9, 10, 11), max_iter=mi, tol=tol, n_warps=2)
     V, Y = _t(FG["V0"], cuda), _t(FG["Y0"], cuda)
     f.level(_t(FG["I1"], cuda), _t(FG["I2"], cuda), V, Y, roi, box=box)
     np.testing.assert_array_equal(_np(V), FG[f"level{case}_V"])
@@ -144,7 +145,7 @@ def test_flow_level_bitwise_with_residual_iterations(cuda, roi, norm, huber, lam
     v0 = (rng.normal(size=(3,) + shape) * 0.4).astype(np.float32)
     y0 = (rng.normal(size=(10,) + shape) * 0.05).astype(np.float32)
     box = (25.0, 19.0, 30.0)
-    f = _flow((21, 19, 17), max_iter=159, tol=0.0, n_warps=3, norm=norm, huber=huber, lam=lam)
+    f = _flow(shape, max_iter=159, tol=0.0, n_warps=3, norm=norm, huber=huber, lam=lam)
     V, Y = _t(v0, cuda), _t(y0, cuda)
     f.level(_t(i1, cuda), _t(i2, cuda), V, Y, roi, box=box)
     vo, yo, its = ob.flow_level32(i1, i2, v0, y0, roi, box=box, tol=0.0, lam=lam, max_iter=159, norm=norm,
@@ -165,7 +166,7 @@ def test_flow_level_tolerance_stop(cuda):
     y0 = np.zeros((10,) + shape, np.float32)
     for tol in (0.9, 0.0019, 1.0):
         vo, yo, its_o, err_o = ob.flow_level32(i1, i2, v0, y0, (0,) * 6, tol=tol, max_iter=400, n_warps=2, errs=True)
-        f = _flow((13, 14, 12), max_iter=400, tol=tol, n_warps=2)
+        f = _flow(shape, max_iter=400, tol=tol, n_warps=2)
         V, Y = _t(v0, cuda), _t(y0, cuda)
         f.level(_t(i1, cuda), _t(i2, cuda), V, Y, (0,) * 6)
         np.testing.assert_array_equal(_np(V), vo)
@@ -180,7 +181,7 @@ def test_flow_level_tolerance_stop(cuda):
 
 
 def test_flow_multiscale_matches_reference_fixture(cuda):
-    f = _flow((20, 18, 19), max_iter=12, tol=0.0, n_warps=2, cut=(3, 2, 2, 4, 1, 3))
+    f = _flow(FG["ms_I1"].shape, max_iter=12, tol=0.0, n_warps=2, cut=(3, 2, 2, 4, 1, 3))
     V = _t(FG["ms_V0"], cuda)
     f.multiscale(_t(FG["ms_I1"], cuda), _t(FG["ms_I2"], cuda), V)
     np.testing.assert_array_equal(_np(V), FG["ms_V"])
@@ -193,7 +194,7 @@ def test_flow_multiscale_bitwise(cuda, scales, eta, cut, y0):
     i1, i2, rng = _images(shape, 13, smooth=2.0)
     v0 = (rng.normal(size=(3,) + shape) * 0.2).astype(np.float32)
     Y0 = (rng.normal(size=(10,) + shape) * 0.05).astype(np.float32) if y0 else None
-    f = _flow((48, 64, 40), max_iter=40, tol=0.0, n_warps=2, scales=scales, eta=eta, cut=cut)
+    f = _flow(shape, max_iter=40, tol=0.0, n_warps=2, scales=scales, eta=eta, cut=cut)
     V = _t(v0, cuda)
     f.multiscale(_t(i1, cuda), _t(i2, cuda), V, None if Y0 is None else _t(Y0, cuda))
     ref = ob.flow_multiscale32(i1, i2, v0, cut, Y=Y0, tol=0.0, max_iter=40, n_warps=2, eta=eta, scales=scales)
