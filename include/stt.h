@@ -127,6 +127,16 @@ stt_status stt_bp_voxel(stt_ctx *ctx, const float *corr, float *vol, double alph
 stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, int view,
                       void *stream);
 
+/* The backprojection mode of the reference's projector on its own: one
+ * march of view `view` scattering contrib[v] += c*w and wsum[v] += w for the
+ * 8 trilinear corners of every sample (SingleScalarVolume.core.h:128-143 with
+ * VolumeData::SetProjectionMode(1)); contrib and wsum (nx*ny*nz floats each)
+ * accumulate, as the producer's accumulators do until Initial()
+ * (TypicalRayProducer.cpp:78-96).  Atomic float adds: the summation order,
+ * not the terms, differs from the reference's sequential loop. */
+stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, float *wsum, int view,
+                              void *stream);
+
 /* Ray-driven backprojection that allocates no device memory.  No counterpart
  * in the reference: it is stt_bp_ray for callers that cannot let a library
  * call cudaMalloc (a plugin whose host application owns all device memory, a

@@ -167,6 +167,21 @@ __global__ void k_bp_ray_update(long long n, float2 *__restrict__ acc, float *__
     }
 }
 
+// Adds the scatter accumulators to caller arrays and clears them: the raw
+// contributions and weights of the reference's backprojection mode
+// (SingleScalarVolume.core.h:128-143, read back through
+// TypicalRayProducer::GetContributions / GetTotalWeight).
+__global__ void k_acc_split(long long n, float2 *__restrict__ acc, float *__restrict__ contrib,
+                            float *__restrict__ wsum) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const float2 a = acc[k];
+        contrib[k] += a.x;
+        wsum[k] += a.y;
+        acc[k] = make_float2(0.0f, 0.0f);
+    }
+}
+
 // Stand-alone SART correction (ST_Tomography.cpp:667-676) for the unfused
 // per-view form: the ray lengths are the sticky state k_fp updated on hits.
 __global__ void k_correction(long long n, const float *__restrict__ b, const float *__restrict__ ax,
@@ -266,6 +281,16 @@ cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel 
     if (e != cudaSuccess) return e;
     const long long n = (long long)g.nx * g.ny * g.nz;
     k_bp_ray_update<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, acc, vol, gmax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bp_ray_scatter(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
+                                  float2 *acc, float *contrib, float *wsum, cudaStream_t s) {
+    k_bp_ray_scatter<<<ray_grid(g, 1), 128, 0, s>>>(g, views, sel, corr, acc);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    k_acc_split<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, acc, contrib, wsum);
     return cudaGetLastError();
 }
 

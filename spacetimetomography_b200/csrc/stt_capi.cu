@@ -362,6 +362,20 @@ stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, i
     return STT_OK;
 }
 
+stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, float *wsum, int view,
+                              void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!corr || !contrib || !wsum) return fail(ctx, STT_ERR_INVALID, "null corr, contrib or wsum");
+    if ((st = check_views(ctx, view, 1))) return st;
+    if ((st = set_device(ctx))) return st;
+    if ((st = ensure_acc(ctx, S(stream)))) return st;
+    const stt::ViewSel sel{view, nullptr, 0, view};
+    STT_CUDA(ctx, stt::launch_bp_ray_scatter(ctx->g, ctx->views_d, sel, corr, ctx->acc, contrib, wsum, S(stream)),
+             "k_bp_ray_scatter launch");
+    return STT_OK;
+}
+
 stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, const int *perm,
                           int nperm, int view_offset, double alpha, float gmax, int bp_mode,
                           float *raylen_state, const int *roi_cut, void *stream) {

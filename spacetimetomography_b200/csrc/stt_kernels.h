@@ -28,6 +28,8 @@ cudaError_t launch_correction(long long n, const float *b, const float *ax, cons
                               float *corr, cudaStream_t s);
 cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                           float2 *acc, float *vol, float gmax, cudaStream_t s);
+cudaError_t launch_bp_ray_scatter(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
+                                  float2 *acc, float *contrib, float *wsum, cudaStream_t s);
 cudaError_t launch_fp_adjoint(const GeomDev &g, const ViewRec *views, int view0, int nviews,
                               const float *proj_bar, float *vol_bar, cudaStream_t s);
 cudaError_t launch_fill_zero(float *p, long long n, cudaStream_t s);
