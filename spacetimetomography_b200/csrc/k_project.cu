@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(128) k_fp_corr(const GeomDev g, const ViewRec 
                                                  const float *__restrict__ vol, const float *__restrict__ vol_t,
                                                  const ViewSel sel, const float *__restrict__ b_stack,
                                                  float *__restrict__ raylen_state,
-                                                 float *__restrict__ corr) {
+                                                 float *__restrict__ corr, unsigned long long corr_surf) {
     int i, j;
     if (!tile_pixel(g, i, j)) return;
     int local;
@@ -100,7 +100,10 @@ __global__ void __launch_bounds__(128) k_fp_corr(const GeomDev g, const ViewRec 
     } else {
         L = raylen_state ? raylen_state[pix] : 0.0f;
     }
-    corr[pix] = __fdiv_rn(__fsub_rn(__ldg(b + pix), acc.s), __fadd_rn(L, 1.0f));
+    const float c = __fdiv_rn(__fsub_rn(__ldg(b + pix), acc.s), __fadd_rn(L, 1.0f));
+    corr[pix] = c;
+    // the copy the voxel-driven backprojector gathers from with tld4
+    if (corr_surf) surf2DLayeredwrite(c, corr_surf, i * (int)sizeof(float), j, 0, cudaBoundaryModeZero);
 }
 
 // BP-mode march (SingleScalarVolume.core.h:128-143, UpdateContributionSum
@@ -252,8 +255,8 @@ cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, 
 
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
-                           cudaStream_t s) {
-    k_fp_corr<<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr);
+                           cudaStream_t s, unsigned long long corr_surf) {
+    k_fp_corr<<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf);
     return cudaGetLastError();
 }
 

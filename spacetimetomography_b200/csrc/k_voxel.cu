@@ -36,10 +36,15 @@ struct Cut8 {
 // Voxel-based backprojection (ST_Tomography.cpp:690-730): project the voxel
 // centre, Catmull-Rom 4x4 gather of the correction image (y first, then x),
 // vol += alpha*val, clamp to [0, gmax]; voxels whose footprint leaves
-// [2, W-2) x [2, H-2) are untouched.
+// [2, W-2) x [2, H-2) are untouched.  With TEX the 16 taps come from four
+// tld4 gathers of the correction's one-layer texture copy (one request per
+// 2x2 texels instead of one per texel); the values and the arithmetic are
+// the same.
+template <bool TEX>
 __global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec *__restrict__ views,
                                                   const ViewSel sel, const float *__restrict__ corr,
-                                                  float *__restrict__ vol, float alpha, float gmax) {
+                                                  float *__restrict__ vol, float alpha, float gmax,
+                                                  unsigned long long corr_tex) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y, z = blockIdx.z;
     if (x >= g.nx) return;
@@ -56,13 +61,25 @@ __global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec
     float wx[4], wy[4];
     cr_weights(upx - (float)px, wx);
     cr_weights(upy - (float)py, wy);
-    const float *c0 = corr + (size_t)(py - 1) * g.W + (px - 1);
+    float tap[4][4];  // tap[a][b]: column px-1+a, row py-1+b
+    if (TEX) {
+        const float4 g00 = gather_layer(corr_tex, px - 1, py - 1, 0), g10 = gather_layer(corr_tex, px + 1, py - 1, 0);
+        const float4 g01 = gather_layer(corr_tex, px - 1, py + 1, 0), g11 = gather_layer(corr_tex, px + 1, py + 1, 0);
+        tap[0][0] = g00.w, tap[0][1] = g00.x, tap[0][2] = g01.w, tap[0][3] = g01.x;
+        tap[1][0] = g00.z, tap[1][1] = g00.y, tap[1][2] = g01.z, tap[1][3] = g01.y;
+        tap[2][0] = g10.w, tap[2][1] = g10.x, tap[2][2] = g11.w, tap[2][3] = g11.x;
+        tap[3][0] = g10.z, tap[3][1] = g10.y, tap[3][2] = g11.z, tap[3][3] = g11.y;
+    } else {
+        const float *c0 = corr + (size_t)(py - 1) * g.W + (px - 1);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) tap[a][b] = __ldg(c0 + a + b * g.W);
+    }
     float val = 0.0f;
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-        const float *col = c0 + a;
-        float s = wy[0] * __ldg(col) + wy[1] * __ldg(col + g.W) + wy[2] * __ldg(col + 2 * g.W) +
-                  wy[3] * __ldg(col + 3 * g.W);
+        float s = wy[0] * tap[a][0] + wy[1] * tap[a][1] + wy[2] * tap[a][2] + wy[3] * tap[a][3];
         val += wx[a] * s;
     }
     const size_t o = x + (size_t)y * g.nx + (size_t)z * g.nx * g.ny;
@@ -188,8 +205,11 @@ Cut8 to_cut(const int *c) {
 }  // namespace
 
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                            float *vol, float alpha, float gmax, cudaStream_t s) {
-    k_bp_voxel<<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, sel, corr, vol, alpha, gmax);
+                            float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex) {
+    if (corr_tex)
+        k_bp_voxel<true><<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, sel, corr, vol, alpha, gmax, corr_tex);
+    else
+        k_bp_voxel<false><<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, sel, corr, vol, alpha, gmax, 0);
     return cudaGetLastError();
 }
 

@@ -251,6 +251,17 @@ __device__ __forceinline__ void march(const GeomDev &g, const Ray &r, Visit &&vi
     }
 }
 
+// tld4 of the 2x2 texels {u, u+1} x {v, v+1} of one layer of a layered 2D
+// texture (coordinate (u+1, v+1), point sampling, clamp addressing):
+// .w = (u, v), .z = (u+1, v), .x = (u, v+1), .y = (u+1, v+1).
+__device__ __forceinline__ float4 gather_layer(unsigned long long tex, int u, int v, int layer) {
+    float4 r;
+    asm volatile("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %7}];"
+                 : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+                 : "l"(tex), "r"(layer), "f"((float)u + 1.0f), "f"((float)v + 1.0f));
+    return r;
+}
+
 // Catmull-Rom weights for taps (-1, 0, +1, +2) at fraction d (the cubic of
 // ST_Tomography.cpp:183-186 and CImg's _cubic_atX, written in weight form).
 __device__ __forceinline__ void cr_weights(float d, float w[4]) {

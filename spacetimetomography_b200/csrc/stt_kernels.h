@@ -20,7 +20,7 @@ cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, 
                       int nviews, float *proj, float *raylen, float *weight, cudaStream_t s);
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
-                           cudaStream_t s);
+                           cudaStream_t s, unsigned long long corr_surf = 0);
 cudaError_t launch_transpose(const GeomDev &g, const float *in, float *out, cudaStream_t s);
 cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *in,
                                       float *out, cudaStream_t s);
@@ -35,7 +35,7 @@ cudaError_t launch_fp_adjoint(const GeomDev &g, const ViewRec *views, int view0,
 cudaError_t launch_fill_zero(float *p, long long n, cudaStream_t s);
 
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                            float *vol, float alpha, float gmax, cudaStream_t s);
+                            float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex = 0);
 cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counter, int frames,
                              int views, int *perm, cudaStream_t s);
 cudaError_t launch_pd_dual(const int *dims, const PdParams &p, const float *xf, const float *xf1,

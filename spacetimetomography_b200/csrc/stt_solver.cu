@@ -87,6 +87,15 @@ void host_perm(unsigned long long seed, unsigned long long iter, int frames, int
 // The context internals the solver needs (defined in stt_capi.cu).
 extern "C" stt_status stt_internal_geom(stt_ctx *ctx, const void **geom, const void **views);
 
+// An image held as a one-layer layered CUDA array, with the texture object
+// the voxel-driven backprojector gathers from and the surface object the
+// fused forward projection writes.
+struct LayeredTex {
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    cudaSurfaceObject_t surf = 0;
+};
+
 struct stt_solver {
     stt_ctx *ctx = nullptr;
     stt_solve_cfg cfg{};
@@ -113,10 +122,36 @@ struct stt_solver {
     cudaGraphExec_t pexec[2] = {nullptr, nullptr};
     long long launches_per_iter = 0;
     long long phase_launches[2] = {0, 0};
+    std::vector<LayeredTex> corr_tex;  // batched modes: per frame, the correction as a texture
     std::string err;
 };
 
 namespace {
+
+cudaError_t make_layered(int w, int h, int layers, LayeredTex &o) {
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+    cudaError_t e = cudaMalloc3DArray(&o.arr, &cd, make_cudaExtent(w, h, layers),
+                                      cudaArrayLayered | cudaArraySurfaceLoadStore);
+    if (e != cudaSuccess) return e;
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = o.arr;
+    cudaTextureDesc td{};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    e = cudaCreateTextureObject(&o.tex, &rd, &td, nullptr);
+    if (e != cudaSuccess) return e;
+    return cudaCreateSurfaceObject(&o.surf, &rd);
+}
+
+void free_layered(LayeredTex &o) {
+    if (o.surf) cudaDestroySurfaceObject(o.surf);
+    if (o.tex) cudaDestroyTextureObject(o.tex);
+    if (o.arr) cudaFreeArray(o.arr);
+    o = LayeredTex{};
+}
 
 stt_status sfail(stt_solver *s, stt_status st, const std::string &m) {
     if (s) s->err = m;
@@ -202,12 +237,14 @@ stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long
     for (int i = 0; i < V; ++i) {
         const stt::ViewSel sel{0, s->perm + (size_t)f * V, i, f * V};
         SCUDA(s, stt::launch_transpose_for_view(g, s->views, sel, vol, volt, cs), "transpose");
+        const bool tex = voxel && !s->corr_tex.empty();
         SCUDA(s, stt::launch_fp_corr(g, s->views, vol, volt, sel, stack, voxel ? s->raylen + f * s->npix : nullptr,
-                                     corr, cs),
+                                     corr, cs, tex ? s->corr_tex[f].surf : 0),
               "fp_corr");
         ++nl;
         if (voxel)
-            SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs),
+            SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs,
+                                          tex ? s->corr_tex[f].tex : 0),
                   "bp_voxel");
         else
             SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs),
@@ -393,6 +430,15 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
         stt_solver_destroy(s);
         return e;
     }
+    if (cfg->mode != STT_SOLVE_PLAIN && cfg->bp_mode == 0) {
+        s->corr_tex.resize(F);
+        for (int f = 0; f < F; ++f)
+            if (make_layered(g->W, g->H, 1, s->corr_tex[f]) != cudaSuccess) {
+                cudaGetLastError();
+                stt_solver_destroy(s);
+                return STT_ERR_NOMEM;
+            }
+    }
     cudaError_t ce = cudaMemset(s->raylen, 0, (size_t)F * s->npix * sizeof(float));
     if (ce == cudaSuccess) ce = cudaMemset(s->counter, 0, sizeof(unsigned long long));
     if (ce == cudaSuccess && s->acc) ce = cudaMemset(s->acc, 0, (size_t)F * s->n * sizeof(float2));
@@ -520,6 +566,7 @@ stt_status stt_solver_destroy(stt_solver *s) {
     for (auto e : s->ev_done)
         if (e) cudaEventDestroy(e);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    for (auto &t : s->corr_tex) free_layered(t);
     cudaFree(s->warpbuf);
     cudaFree(s->corr);
     cudaFree(s->ax);
