@@ -102,6 +102,17 @@ stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g);
 stt_status stt_fp(stt_ctx *ctx, const float *vol, float *proj, float *raylen, float *weight,
                   int view0, int nviews, void *stream);
 
+/* Forward projection of a volume stored in FP32 or BF16 (`vol` points to
+ * nx*ny*nz elements of `dtype`; BF16 = the upper 16 bits of an FP32, rounded
+ * by the caller).  BF16 halves the volume's memory and cache footprint; taps
+ * are widened exactly to FP32 and the march and sums are FP32, so the result
+ * equals stt_fp of the widened volume.  Against the FP32 volume it carries
+ * the BF16 rounding of the voxels (relative 2^-9 each), i.e. about 1e-3
+ * relative L2 per projection.  Not in the reference (CImg<float> only). */
+typedef enum stt_dtype { STT_DTYPE_F32 = 0, STT_DTYPE_BF16 = 1 } stt_dtype;
+stt_status stt_fp_typed(stt_ctx *ctx, const void *vol, int dtype, float *proj, float *raylen, float *weight,
+                        int view0, int nviews, void *stream);
+
 /* Forward projection of one view fused with the SART correction
  * (ST_Tomography.cpp:667-676): corr = (b - Ax) / (L + 1), where L is the
  * sticky ray-length state (W*H, updated where the ray hits). */
@@ -167,6 +178,30 @@ stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, con
 /* Host helper: the seeded view permutation that replaces srand(time(0)) +
  * random_shuffle (ST_Tomography.cpp:635-642): SplitMix64 + Fisher-Yates. */
 stt_status stt_permutation(unsigned long long seed, int n, int *perm_out);
+
+/* One SART view (the body of the loop at ST_Tomography.cpp:651-764): forward
+ * projection of view `view` fused with the correction against its projection
+ * b (W*H), then the backprojection (bp_mode 0 voxel-based with alpha, 1
+ * ray-based); stt_sart_sweep with a one-view order, no ROI mask. */
+stt_status stt_sart_view(stt_ctx *ctx, float *vol, const float *b, int view, double alpha, float gmax, int bp_mode,
+                         float *raylen_state, void *stream);
+
+/* Operator norm of the forward projector by power iteration on A^T A (the
+ * exact adjoint stt_fp_vjp), over all views of the geometry, from a seeded
+ * positive start vector; dot products and norms in FP64.  norm_A = sqrt of the
+ * last Rayleigh quotient (a lower bound that converges to ||A||_2); norm_K =
+ * sqrt(norm_A^2 + 12), the bound for K = [A; grad] with the 3D forward-
+ * difference gradient (||grad||^2 <= 12); sigma = tau = 0.99 / norm_K satisfy
+ * sigma*tau*||K||^2 < 1 for a Chambolle-Pock iteration on K.  rel_change: the
+ * last iteration's relative change of the quotient.  Synchronises `stream`.
+ * The reference fixes these steps instead (L = 8, ST_Tomography.cpp:98-102). */
+typedef struct stt_opnorm {
+    double norm_A, norm_K, sigma, tau;
+    int iterations;
+    double rel_change;
+} stt_opnorm;
+stt_status stt_opnorm_power_iter(stt_ctx *ctx, int n_iter, unsigned long long seed, stt_opnorm *out,
+                                 void *stream);
 
 /* ---- primal-dual steps (ST_Tomography.cpp:492-604) -------------------------
  * Parameters as the reference uses them: sigma = CP_sigma, tau = CP_tau,

@@ -57,6 +57,11 @@ class FlowParams(C.Structure):
                 ("scales", C.c_int), ("cut", C.c_int * 6)]
 
 
+class OpNorm(C.Structure):
+    _fields_ = [("norm_A", C.c_double), ("norm_K", C.c_double), ("sigma", C.c_double), ("tau", C.c_double),
+                ("iterations", C.c_int), ("rel_change", C.c_double)]
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
@@ -89,6 +94,9 @@ def _load() -> C.CDLL:
         "stt_solver_stats": [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_ulonglong)],
         "stt_solver_destroy": [vp],
         "stt_solver_frame_order": [C.c_ulonglong, C.c_ulonglong, i, i, i, vp],
+        "stt_fp_typed": [vp, vp, i, vp, vp, vp, i, i, vp],
+        "stt_sart_view": [vp, vp, vp, i, d, f, i, vp, vp],
+        "stt_opnorm_power_iter": [vp, i, C.c_ulonglong, C.POINTER(OpNorm), vp],
         "stt_warp_box": [vp, vp, vp, vp, i, f, vp, vp],
         "stt_image_gradient": [vp, vp, vp, vp],
         "stt_flow_create": [i, vp, C.POINTER(FlowParams), C.POINTER(vp)],

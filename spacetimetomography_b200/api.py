@@ -14,7 +14,7 @@ from typing import Sequence
 
 import numpy as np
 
-from ._lib import FlowParams, Geometry, PdState, SolveCfg, STTError, check, lib
+from ._lib import FlowParams, Geometry, OpNorm, PdState, SolveCfg, STTError, check, lib
 from ._lib import PdParams as _PdParams
 
 # ROI cut of the reference (ST_Tomography.cpp:114)
@@ -129,6 +129,28 @@ class Context:
         self._chk(lib.stt_fp(self._h, _ptr(vol), _ptr(proj), _ptr(raylen), _ptr(weight), view0,
                              nviews, _stream(stream)))
         return proj
+
+    def fp_typed(self, vol, proj, view0=0, nviews=None, raylen=None, weight=None, stream=None):
+        """Forward projection of a float32 or bfloat16 volume (stt_fp_typed)."""
+        import torch
+
+        dtype = {torch.float32: 0, torch.bfloat16: 1}[vol.dtype]
+        nviews = self.n_views - view0 if nviews is None else nviews
+        self._chk(lib.stt_fp_typed(self._h, _ptr(vol), dtype, _ptr(proj), _ptr(raylen), _ptr(weight), view0, nviews,
+                                   _stream(stream)))
+        return proj
+
+    def sart_view(self, vol, b, view, alpha, gmax, bp_mode, raylen_state, stream=None):
+        """One SART view: FP + correction against b (H, W), then backprojection."""
+        self._chk(lib.stt_sart_view(self._h, _ptr(vol), _ptr(b), int(view), float(alpha), float(gmax), int(bp_mode),
+                                    _ptr(raylen_state), _stream(stream)))
+
+    def opnorm(self, n_iter=50, seed=0, stream=None) -> dict:
+        """||A|| by FP64 power iteration on A^T A, and the steps it implies."""
+        o = OpNorm()
+        self._chk(lib.stt_opnorm_power_iter(self._h, int(n_iter), C.c_ulonglong(seed), C.byref(o), _stream(stream)))
+        return {"norm_A": o.norm_A, "norm_K": o.norm_K, "sigma": o.sigma, "tau": o.tau,
+                "iterations": o.iterations, "rel_change": o.rel_change}
 
     def fp_correction(self, vol, b, raylen_state, corr, view, stream=None):
         self._chk(lib.stt_fp_correction(self._h, _ptr(vol), _ptr(b), _ptr(raylen_state), _ptr(corr),

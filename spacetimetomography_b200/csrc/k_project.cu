@@ -25,8 +25,9 @@ __device__ __forceinline__ bool tile_pixel(const GeomDev &g, int &i, int &j) {
 }
 
 // Source and strides of the forward projector's gathers for one view.
-__device__ __forceinline__ const float *fp_source(const GeomDev &g, const ViewRec &v, const float *vol,
-                                                  const float *vol_t, Strides &st) {
+template <typename T>
+__device__ __forceinline__ const T *fp_source(const GeomDev &g, const ViewRec &v, const T *vol, const T *vol_t,
+                                              Strides &st) {
     if (vol_t && v.layout == 1) {
         st = zyx_strides(g);
         return vol_t;
@@ -36,9 +37,11 @@ __device__ __forceinline__ const float *fp_source(const GeomDev &g, const ViewRe
 }
 
 // GenerateImage_MT (S/ImageFormationModel/TypicalRayProducer.core.h:168-224)
-// for views [view0, view0 + gridDim.z).
+// for views [view0, view0 + gridDim.z).  T = float, or unsigned short for a
+// BF16-stored volume (taps widened to FP32; the march and the sums are FP32).
+template <typename T>
 __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__restrict__ views,
-                                            const float *__restrict__ vol, const float *__restrict__ vol_t,
+                                            const T *__restrict__ vol, const T *__restrict__ vol_t,
                                             int view0, float *__restrict__ proj, float *__restrict__ raylen,
                                             float *__restrict__ weight) {
     int i, j;
@@ -46,7 +49,7 @@ __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__re
     const int v = blockIdx.z;
     const ViewRec &vr = views[view0 + v];
     Strides st;
-    const float *src = fp_source(g, vr, vol, vol_t, st);
+    const T *src = fp_source(g, vr, vol, vol_t, st);
     Ray r;
     make_ray(g, vr, i, j, r);
     Kahan acc{0.0f, 0.0f};
@@ -196,9 +199,10 @@ __global__ void k_correction(long long n, const float *__restrict__ b, const flo
 
 // z-fastest copy of an x-fastest volume: out[z + y*nz + x*nz*ny] = in[x + y*nx + z*nx*ny],
 // one (x, z) plane of fixed y per block row, 32x32 tiles through shared memory.
-__device__ __forceinline__ void transpose_tile(int nx, int ny, int nz, const float *__restrict__ in,
-                                               float *__restrict__ out) {
-    __shared__ float tile[32][33];
+template <typename T>
+__device__ __forceinline__ void transpose_tile(int nx, int ny, int nz, const T *__restrict__ in,
+                                               T *__restrict__ out) {
+    __shared__ T tile[32][33];
     const int x0 = blockIdx.x * 32, z0 = blockIdx.y * 32, y = blockIdx.z;
     const size_t nxy = (size_t)nx * ny, nzy = (size_t)nz * ny;
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
@@ -212,8 +216,9 @@ __device__ __forceinline__ void transpose_tile(int nx, int ny, int nz, const flo
     }
 }
 
-__global__ void __launch_bounds__(256) k_transpose_xz(int nx, int ny, int nz, const float *__restrict__ in,
-                                                      float *__restrict__ out) {
+template <typename T>
+__global__ void __launch_bounds__(256) k_transpose_xz(int nx, int ny, int nz, const T *__restrict__ in,
+                                                      T *__restrict__ out) {
     transpose_tile(nx, ny, nz, in, out);
 }
 
@@ -249,7 +254,7 @@ int grid_stride_blocks(long long n, int threads) {
 
 cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, int view0,
                       int nviews, float *proj, float *raylen, float *weight, cudaStream_t s) {
-    k_fp<<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen, weight);
+    k_fp<float><<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen, weight);
     return cudaGetLastError();
 }
 
@@ -261,7 +266,19 @@ cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *
 }
 
 cudaError_t launch_transpose(const GeomDev &g, const float *in, float *out, cudaStream_t s) {
-    k_transpose_xz<<<transpose_grid(g), dim3(32, 8), 0, s>>>(g.nx, g.ny, g.nz, in, out);
+    k_transpose_xz<float><<<transpose_grid(g), dim3(32, 8), 0, s>>>(g.nx, g.ny, g.nz, in, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fp_bf16(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
+                           const unsigned short *vol_t, int view0, int nviews, float *proj, float *raylen,
+                           float *weight, cudaStream_t s) {
+    k_fp<unsigned short><<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen, weight);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_bf16(const GeomDev &g, const unsigned short *in, unsigned short *out, cudaStream_t s) {
+    k_transpose_xz<unsigned short><<<transpose_grid(g), dim3(32, 8), 0, s>>>(g.nx, g.ny, g.nz, in, out);
     return cudaGetLastError();
 }
 

@@ -194,6 +194,45 @@ __global__ void __launch_bounds__(128) k_roi_mask(int nx, int ny, int nz, Cut8 c
     roi[i + (size_t)j * nx + (size_t)k * nx * ny] = roi_value(i, j, k, nx, ny, nz, cut.c);
 }
 
+// ---- FP64 helpers of the power iteration --------------------------------------
+// out[0] += sum a*b (FP64 products and sums; one double atomic per block).
+__global__ void __launch_bounds__(256) k_dot_f64(long long n, const float *__restrict__ a,
+                                                 const float *__restrict__ b, double *__restrict__ out) {
+    double s = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        s += (double)__ldg(a + k) * (double)__ldg(b + k);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __shared__ double part[8];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+        atomicAdd(out, t);
+    }
+}
+
+// x *= 1/sqrt(*norm2) (the factor formed in FP64); x = 0 when the norm is 0.
+__global__ void __launch_bounds__(256) k_scale_inv_sqrt(long long n, float *__restrict__ x,
+                                                        const double *__restrict__ norm2) {
+    const double q = *norm2;
+    const float f = q > 0.0 ? (float)(1.0 / sqrt(q)) : 0.0f;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        x[k] *= f;
+}
+
+// Seeded start vector: uniform in [0.5, 1.5) from SplitMix64 of (seed, index).
+__global__ void __launch_bounds__(256) k_fill_seeded(long long n, unsigned long long seed, float *__restrict__ x) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (unsigned long long)(k + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        z ^= z >> 31;
+        x[k] = 0.5f + (float)(z >> 40) * (1.0f / 16777216.0f);
+    }
+}
+
 dim3 vox_grid(int nx, int ny, int nz) { return dim3((nx + 127) / 128, ny, nz); }
 
 Cut8 to_cut(const int *c) {
@@ -203,6 +242,21 @@ Cut8 to_cut(const int *c) {
 }
 
 }  // namespace
+
+cudaError_t launch_dot_f64(long long n, const float *a, const float *b, double *out, cudaStream_t s) {
+    k_dot_f64<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, a, b, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale_inv_sqrt(long long n, float *x, const double *norm2, cudaStream_t s) {
+    k_scale_inv_sqrt<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, x, norm2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, cudaStream_t s) {
+    k_fill_seeded<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, seed, x);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                             float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex) {

@@ -27,6 +27,12 @@ struct stt_ctx {
     size_t corr_n = 0;
     float *volt = nullptr;  // z-fastest copy of the volume for views gathering along x
     size_t volt_n = 0;
+    unsigned short *volt16 = nullptr;  // the same for a BF16-stored volume
+    size_t volt16_n = 0;
+    float *pw = nullptr;  // power iteration: x, A^T A x, and a chunk of projections
+    size_t pw_n = 0;
+    double *pwd = nullptr;  // power iteration: FP64 sums
+    size_t pwd_n = 0;
 };
 
 namespace {
@@ -145,6 +151,9 @@ stt_status stt_destroy(stt_ctx *ctx) {
     if (ctx->acc) cudaFree(ctx->acc);
     if (ctx->corr) cudaFree(ctx->corr);
     if (ctx->volt) cudaFree(ctx->volt);
+    cudaFree(ctx->volt16);
+    cudaFree(ctx->pw);
+    cudaFree(ctx->pwd);
     delete ctx;
     return STT_OK;
 }
@@ -299,6 +308,32 @@ stt_status stt_fp(stt_ctx *ctx, const float *vol, float *proj, float *raylen, fl
     return STT_OK;
 }
 
+stt_status stt_fp_typed(stt_ctx *ctx, const void *vol, int dtype, float *proj, float *raylen, float *weight,
+                        int view0, int nviews, void *stream) {
+    if (dtype == STT_DTYPE_F32)
+        return stt_fp(ctx, static_cast<const float *>(vol), proj, raylen, weight, view0, nviews, stream);
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (dtype != STT_DTYPE_BF16) return fail(ctx, STT_ERR_INVALID, "dtype must be STT_DTYPE_F32 or STT_DTYPE_BF16");
+    if (!vol || !proj) return fail(ctx, STT_ERR_INVALID, "null vol or proj");
+    if ((st = check_views(ctx, view0, nviews))) return st;
+    if (nviews == 0) return STT_OK;
+    if ((st = set_device(ctx))) return st;
+    const unsigned short *v16 = static_cast<const unsigned short *>(vol);
+    const unsigned short *vt16 = nullptr;
+    bool any = false;
+    for (int v = view0; v < view0 + nviews && !any; ++v) any = ctx->views_h[v].layout == 1;
+    if (any) {
+        if ((st = ensure(ctx, ctx->volt16, ctx->volt16_n, (size_t)nvox(ctx), "transposed BF16 volume"))) return st;
+        STT_CUDA(ctx, stt::launch_transpose_bf16(ctx->g, v16, ctx->volt16, S(stream)), "k_transpose launch");
+        vt16 = ctx->volt16;
+    }
+    STT_CUDA(ctx, stt::launch_fp_bf16(ctx->g, ctx->views_d, v16, vt16, view0, nviews, proj, raylen, weight,
+                                      S(stream)),
+             "k_fp launch");
+    return STT_OK;
+}
+
 stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, float *raylen_state,
                              float *corr, int view, void *stream) {
     stt_status st = need_geom(ctx);
@@ -415,6 +450,57 @@ stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, con
         const int d[3] = {ctx->g.nx, ctx->g.ny, ctx->g.nz};
         STT_CUDA(ctx, stt::launch_roi_apply(d, roi_cut, nullptr, vol, nullptr, nullptr, s), "k_roi_apply launch");
     }
+    return STT_OK;
+}
+
+stt_status stt_sart_view(stt_ctx *ctx, float *vol, const float *b, int view, double alpha, float gmax, int bp_mode,
+                         float *raylen_state, void *stream) {
+    const int first = 0;
+    return stt_sart_sweep(ctx, vol, b, &first, 1, view, alpha, gmax, bp_mode, raylen_state, nullptr, stream);
+}
+
+stt_status stt_opnorm_power_iter(stt_ctx *ctx, int n_iter, unsigned long long seed, stt_opnorm *out, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!out || n_iter < 1) return fail(ctx, STT_ERR_INVALID, "null out or n_iter < 1");
+    if ((st = set_device(ctx))) return st;
+    cudaStream_t s = S(stream);
+    const long long n = nvox(ctx);
+    const long long npix = (long long)ctx->g.W * ctx->g.H;
+    const int nv = ctx->g.n_views;
+    const int chunk = nv < 32 ? nv : 32;  // projections held at once
+    if ((st = ensure(ctx, ctx->pw, ctx->pw_n, (size_t)(2 * n + chunk * npix), "power-iteration vectors"))) return st;
+    if ((st = ensure(ctx, ctx->pwd, ctx->pwd_n, (size_t)(3 * n_iter), "power-iteration sums"))) return st;
+    float *x = ctx->pw, *ax = ctx->pw + n, *y = ctx->pw + 2 * n;
+    STT_CUDA(ctx, cudaMemsetAsync(ctx->pwd, 0, 3 * n_iter * sizeof(double), s), "clear sums");
+    STT_CUDA(ctx, stt::launch_fill_seeded(n, seed, x, s), "k_fill_seeded");
+    STT_CUDA(ctx, stt::launch_dot_f64(n, x, x, ctx->pwd, s), "k_dot_f64");
+    STT_CUDA(ctx, stt::launch_scale_inv_sqrt(n, x, ctx->pwd, s), "k_scale_inv_sqrt");
+    for (int it = 0; it < n_iter; ++it) {
+        double *sums = ctx->pwd + 3 * it;  // [0] unused at it > 0; [1] <x, A^T A x>; [2] |A^T A x|^2
+        STT_CUDA(ctx, stt::launch_fill_zero(ax, n, s), "k_fill_zero");
+        for (int v0 = 0; v0 < nv; v0 += chunk) {
+            const int k = nv - v0 < chunk ? nv - v0 : chunk;
+            if ((st = stt_fp(ctx, x, y, nullptr, nullptr, v0, k, stream))) return st;
+            if ((st = stt_fp_vjp(ctx, y, ax, v0, k, stream))) return st;
+        }
+        STT_CUDA(ctx, stt::launch_dot_f64(n, x, ax, sums + 1, s), "k_dot_f64");
+        STT_CUDA(ctx, stt::launch_dot_f64(n, ax, ax, sums + 2, s), "k_dot_f64");
+        STT_CUDA(ctx, cudaMemcpyAsync(x, ax, n * sizeof(float), cudaMemcpyDeviceToDevice, s), "copy");
+        STT_CUDA(ctx, stt::launch_scale_inv_sqrt(n, x, sums + 2, s), "k_scale_inv_sqrt");
+    }
+    std::vector<double> h(3 * n_iter);
+    STT_CUDA(ctx, cudaMemcpyAsync(h.data(), ctx->pwd, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s),
+             "read sums");
+    STT_CUDA(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const double lam = h[3 * (n_iter - 1) + 1];  // Rayleigh quotient of A^T A at a unit vector
+    const double prev = n_iter > 1 ? h[3 * (n_iter - 2) + 1] : lam;
+    out->norm_A = std::sqrt(lam > 0.0 ? lam : 0.0);
+    out->norm_K = std::sqrt(out->norm_A * out->norm_A + 12.0);
+    out->sigma = 0.99 / out->norm_K;
+    out->tau = 0.99 / out->norm_K;
+    out->iterations = n_iter;
+    out->rel_change = lam > 0.0 ? std::fabs(lam - prev) / lam : 0.0;
     return STT_OK;
 }
 

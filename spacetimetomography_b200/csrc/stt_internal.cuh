@@ -149,12 +149,20 @@ __device__ __forceinline__ void make_taps(const GeomDev &g, const float p[3], Ta
 }
 
 // x, then y, then z as the reference interpolates.
-__device__ __forceinline__ float tri_value(const float *__restrict__ vol, const Taps &t) {
-    const float *p = vol + t.base;
-    float v000 = __ldg(p), v100 = __ldg(p + t.dx);
-    float v010 = __ldg(p + t.dy), v110 = __ldg(p + t.dy + t.dx);
-    float v001 = __ldg(p + t.dz), v101 = __ldg(p + t.dz + t.dx);
-    float v011 = __ldg(p + t.dz + t.dy), v111 = __ldg(p + t.dz + t.dy + t.dx);
+// One stored voxel as float: FP32 as is; BF16 storage (raw 16-bit patterns,
+// the upper half of an FP32) widened exactly.
+__device__ __forceinline__ float ld_voxel(const float *p) { return __ldg(p); }
+__device__ __forceinline__ float ld_voxel(const unsigned short *p) {
+    return __uint_as_float((unsigned)__ldg(p) << 16);
+}
+
+template <typename T>
+__device__ __forceinline__ float tri_value(const T *__restrict__ vol, const Taps &t) {
+    const T *p = vol + t.base;
+    float v000 = ld_voxel(p), v100 = ld_voxel(p + t.dx);
+    float v010 = ld_voxel(p + t.dy), v110 = ld_voxel(p + t.dy + t.dx);
+    float v001 = ld_voxel(p + t.dz), v101 = ld_voxel(p + t.dz + t.dx);
+    float v011 = ld_voxel(p + t.dz + t.dy), v111 = ld_voxel(p + t.dz + t.dy + t.dx);
     float fx1 = 1.0f - t.fx;
     float a = v000 * fx1 + v100 * t.fx;
     float b = v010 * fx1 + v110 * t.fx;

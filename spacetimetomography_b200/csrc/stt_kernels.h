@@ -22,6 +22,10 @@ cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
                            cudaStream_t s, unsigned long long corr_surf = 0);
 cudaError_t launch_transpose(const GeomDev &g, const float *in, float *out, cudaStream_t s);
+cudaError_t launch_fp_bf16(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
+                           const unsigned short *vol_t, int view0, int nviews, float *proj, float *raylen,
+                           float *weight, cudaStream_t s);
+cudaError_t launch_transpose_bf16(const GeomDev &g, const unsigned short *in, unsigned short *out, cudaStream_t s);
 cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *in,
                                       float *out, cudaStream_t s);
 cudaError_t launch_correction(long long n, const float *b, const float *ax, const float *raylen,
@@ -33,6 +37,9 @@ cudaError_t launch_bp_ray_scatter(const GeomDev &g, const ViewRec *views, const 
 cudaError_t launch_fp_adjoint(const GeomDev &g, const ViewRec *views, int view0, int nviews,
                               const float *proj_bar, float *vol_bar, cudaStream_t s);
 cudaError_t launch_fill_zero(float *p, long long n, cudaStream_t s);
+cudaError_t launch_dot_f64(long long n, const float *a, const float *b, double *out, cudaStream_t s);
+cudaError_t launch_scale_inv_sqrt(long long n, float *x, const double *norm2, cudaStream_t s);
+cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, cudaStream_t s);
 
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                             float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex = 0);
