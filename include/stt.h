@@ -373,6 +373,37 @@ stt_status stt_solver_destroy(stt_solver *s);
 stt_status stt_solver_frame_order(unsigned long long seed, unsigned long long iter, int n_frames,
                                   int frame, int views, int *perm_out);
 
+/* ---- batched independent instances (config 4 of the survey's scope) ------
+ * Many single-frame reconstructions of uneven size solved together.  Each
+ * instance is a one-frame primal-dual TV + SART solve -- the iteration of
+ * ST_Tomography::Render with one frame (ST_Tomography.cpp:492-607; its
+ * temporal and brightness-constancy weights are forced to 0) -- on its own
+ * context (geometry, views [0, n_views)) and stream.  stt_batch_iterate runs
+ * one iteration of every instance concurrently (STT_SOLVE_STREAMS) or as one
+ * captured CUDA graph (STT_SOLVE_GRAPH); after it each instance's `vol` holds
+ * its current volume.  The batch owns the instances' solver state (13 volumes
+ * each); `vol` and `proj` stay the caller's and must outlive the batch. */
+typedef struct stt_instance {
+    stt_ctx *ctx;
+    float *vol;           /* nx*ny*nz: start volume in, current volume out */
+    const float *proj;    /* n_views projections (view-major, W*H each) */
+    int n_views;
+    int bp_mode;          /* 0 voxel-based (alpha), 1 ray-based */
+    double alpha;
+    stt_pd_params pd;     /* sigma, tau, tv_w, huber_factor, gmax, cut (tp_w, bc_w ignored) */
+    int roi_cut[8];
+    unsigned long long seed;
+} stt_instance;
+
+typedef struct stt_batch stt_batch;
+stt_status stt_batch_create(const stt_instance *instances, int n, int mode, stt_batch **out);
+stt_status stt_batch_iterate(stt_batch *b, int n_iters, void *stream);
+const char *stt_batch_last_error(const stt_batch *b);
+stt_status stt_batch_destroy(stt_batch *b);
+
+/* Volume size (nx, ny, nz) of a context's geometry (HOST int[3]). */
+stt_status stt_ctx_dims(const stt_ctx *ctx, int *dims);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,6 +10,7 @@ from .api import (  # noqa: F401
     SOLVE_GRAPH,
     SOLVE_PLAIN,
     SOLVE_STREAMS,
+    Batch,
     Context,
     Flow,
     PdParams,

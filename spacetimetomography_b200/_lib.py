@@ -62,6 +62,12 @@ class OpNorm(C.Structure):
                 ("iterations", C.c_int), ("rel_change", C.c_double)]
 
 
+class Instance(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("vol", C.c_void_p), ("proj", C.c_void_p), ("n_views", C.c_int),
+                ("bp_mode", C.c_int), ("alpha", C.c_double), ("pd", PdParams), ("roi_cut", C.c_int * 8),
+                ("seed", C.c_ulonglong)]
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
@@ -97,6 +103,10 @@ def _load() -> C.CDLL:
         "stt_fp_typed": [vp, vp, i, vp, vp, vp, i, i, vp],
         "stt_sart_view": [vp, vp, vp, i, d, f, i, vp, vp],
         "stt_opnorm_power_iter": [vp, i, C.c_ulonglong, C.POINTER(OpNorm), vp],
+        "stt_batch_create": [vp, i, i, C.POINTER(vp)],
+        "stt_batch_iterate": [vp, i, vp],
+        "stt_batch_destroy": [vp],
+        "stt_ctx_dims": [vp, vp],
         "stt_warp_box": [vp, vp, vp, vp, i, f, vp, vp],
         "stt_image_gradient": [vp, vp, vp, vp],
         "stt_flow_create": [i, vp, C.POINTER(FlowParams), C.POINTER(vp)],
@@ -115,6 +125,8 @@ def _load() -> C.CDLL:
     lib.stt_last_error.restype = C.c_char_p
     lib.stt_solver_last_error.argtypes = [vp]
     lib.stt_solver_last_error.restype = C.c_char_p
+    lib.stt_batch_last_error.argtypes = [vp]
+    lib.stt_batch_last_error.restype = C.c_char_p
     lib.stt_flow_last_error.argtypes = [vp]
     lib.stt_flow_last_error.restype = C.c_char_p
     lib.stt_version.argtypes = []

@@ -14,7 +14,7 @@ from typing import Sequence
 
 import numpy as np
 
-from ._lib import FlowParams, Geometry, OpNorm, PdState, SolveCfg, STTError, check, lib
+from ._lib import FlowParams, Geometry, Instance, OpNorm, PdState, SolveCfg, STTError, check, lib
 from ._lib import PdParams as _PdParams
 
 # ROI cut of the reference (ST_Tomography.cpp:114)
@@ -415,6 +415,46 @@ class Solver:
     def close(self):
         if getattr(self, "_h", None):
             lib.stt_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """stt_batch: independent single-frame TV + SART solves of uneven size,
+    iterated together (concurrent streams, or one captured CUDA graph).
+
+    Each instance is a dict: ctx (Context with its geometry), vol (nz, ny, nx)
+    CUDA tensor (start in, result out), proj (V, H, W) CUDA tensor, and
+    optionally bp_mode, alpha, pd (PdParams), roi_cut, seed."""
+
+    def __init__(self, instances, mode: int = SOLVE_GRAPH):
+        self._keep = instances
+        arr = (Instance * len(instances))()
+        for k, d in enumerate(instances):
+            pd = d.get("pd", PdParams())
+            arr[k] = Instance(d["ctx"]._h, d["vol"].data_ptr(), d["proj"].data_ptr(), int(d["proj"].shape[0]),
+                              int(d.get("bp_mode", 0)), float(d.get("alpha", 0.3)), pd.c(),
+                              (C.c_int * 8)(*map(int, d.get("roi_cut", REFERENCE_CUT))),
+                              C.c_ulonglong(int(d.get("seed", 0))))
+        h = C.c_void_p()
+        rc = lib.stt_batch_create(arr, len(instances), int(mode), C.byref(h))
+        if rc != 0:
+            raise STTError(rc, (lib.stt_last_error(None) or b"batch create failed").decode())
+        self._h = h
+
+    def iterate(self, n: int = 1, stream=None):
+        rc = lib.stt_batch_iterate(self._h, int(n), _stream(stream))
+        if rc != 0:
+            raise STTError(rc, (lib.stt_batch_last_error(self._h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.stt_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

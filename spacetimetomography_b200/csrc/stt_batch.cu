@@ -1,0 +1,181 @@
+// stt_batch.cu -- many independent single-frame reconstructions of uneven
+// size solved together: each instance is a one-frame primal-dual TV + SART
+// solve (ST_Tomography::Render's iteration with one frame, whose temporal and
+// brightness-constancy weights are zero) on its own context and stream, and
+// one iteration of all of them is enqueued together -- or captured once into
+// one CUDA graph and replayed.  The instances share nothing, so their views
+// run concurrently and small instances fill the GPU that one alone leaves idle.
+#include <string>
+#include <vector>
+
+#include "stt.h"
+
+struct stt_batch {
+    struct Inst {
+        stt_ctx *ctx = nullptr;
+        stt_solver *solver = nullptr;
+        float *user_vol = nullptr;
+        float *state = nullptr;  // vol 2n | xbar 2n | xprev n | ytv 3n | ytp n | ybc n | flow 3n
+        size_t n = 0;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;
+    };
+    std::vector<Inst> inst;
+    int mode = STT_SOLVE_GRAPH;
+    cudaEvent_t fork = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::string err;
+};
+
+extern "C" stt_status stt_internal_set_error(stt_ctx *ctx, stt_status st, const char *msg);
+
+namespace {
+
+stt_status bfail(stt_batch *b, stt_status st, const std::string &m) {
+    b->err = m;
+    return st;
+}
+
+#define BCUDA(b, call, where)                                                                               \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess) return bfail(b, STT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// One iteration of every instance, enqueued on the instances' streams,
+// forked from and joined back to `main`.
+stt_status enqueue_all(stt_batch *b, cudaStream_t main) {
+    BCUDA(b, cudaEventRecord(b->fork, main), "event record");
+    for (size_t i = 0; i < b->inst.size(); ++i) {
+        stt_batch::Inst &in = b->inst[i];
+        BCUDA(b, cudaStreamWaitEvent(in.stream, b->fork, 0), "stream wait");
+        stt_status st = stt_solver_iterate(in.solver, 1, in.stream);
+        if (st) return bfail(b, st, "instance " + std::to_string(i) + ": " + stt_solver_last_error(in.solver));
+        BCUDA(b, cudaMemcpyAsync(in.user_vol, in.state, in.n * sizeof(float), cudaMemcpyDeviceToDevice, in.stream),
+              "copy result");
+        BCUDA(b, cudaEventRecord(in.done, in.stream), "event record");
+        BCUDA(b, cudaStreamWaitEvent(main, in.done, 0), "stream wait");
+    }
+    return STT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+stt_status stt_batch_create(const stt_instance *instances, int n, int mode, stt_batch **out) {
+    if (!instances || n < 1 || !out) return stt_internal_set_error(nullptr, STT_ERR_INVALID, "null argument or n < 1");
+    if (mode != STT_SOLVE_STREAMS && mode != STT_SOLVE_GRAPH)
+        return stt_internal_set_error(nullptr, STT_ERR_INVALID, "mode must be STT_SOLVE_STREAMS or STT_SOLVE_GRAPH");
+    *out = nullptr;
+    stt_batch *b = new stt_batch;
+    b->mode = mode;
+    b->inst.resize(n);
+    auto bail = [&](stt_status st, const std::string &m) {
+        stt_internal_set_error(nullptr, st, m.c_str());
+        stt_batch_destroy(b);
+        return st;
+    };
+    for (int i = 0; i < n; ++i) {
+        const stt_instance &I = instances[i];
+        stt_batch::Inst &in = b->inst[i];
+        if (!I.ctx || !I.vol || !I.proj || I.n_views < 1)
+            return bail(STT_ERR_INVALID, "instance " + std::to_string(i) + ": null ctx/vol/proj or no views");
+        int dims[3];
+        if (stt_ctx_dims(I.ctx, dims) != STT_OK)
+            return bail(STT_ERR_STATE, "instance " + std::to_string(i) + ": no geometry set on its context");
+        in.ctx = I.ctx;
+        in.user_vol = I.vol;
+        in.n = (size_t)dims[0] * dims[1] * dims[2];
+        const size_t n1 = in.n;
+        if (cudaMalloc(&in.state, 13 * n1 * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(STT_ERR_NOMEM, "instance " + std::to_string(i) + ": cudaMalloc of its solver state failed");
+        }
+        float *vol = in.state, *xbar = vol + 2 * n1, *xprev = xbar + 2 * n1, *ytv = xprev + n1, *ytp = ytv + 3 * n1,
+              *ybc = ytp + n1, *flow = ybc + n1;
+        cudaError_t e = cudaMemset(xprev, 0, 9 * n1 * sizeof(float));  // xprev, ytv, ytp, ybc, flow
+        if (e == cudaSuccess) e = cudaMemcpy(vol, I.vol, n1 * sizeof(float), cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(vol + n1, I.vol, n1 * sizeof(float), cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(xbar, vol, 2 * n1 * sizeof(float), cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&in.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&in.done, cudaEventDisableTiming);
+        if (e != cudaSuccess) return bail(STT_ERR_CUDA, std::string("instance set-up: ") + cudaGetErrorString(e));
+        stt_solve_cfg cfg{};
+        cfg.n_frames = 1;
+        cfg.views_per_frame = I.n_views;
+        cfg.bp_mode = I.bp_mode;
+        cfg.alpha = I.alpha;
+        cfg.pd = I.pd;
+        cfg.pd.tp_w = 0.0f;  // one frame: no temporal or brightness-constancy term
+        cfg.pd.bc_w = 0.0f;
+        for (int q = 0; q < 8; ++q) cfg.roi_cut[q] = I.roi_cut[q];
+        cfg.seed = I.seed;
+        cfg.mode = STT_SOLVE_STREAMS;
+        stt_pd_state state{};
+        state.vol = vol;
+        state.xbar = xbar;
+        state.xprev = xprev;
+        state.ytv = ytv;
+        state.ytp = ytp;
+        state.ybc = ybc;
+        state.flow = flow;
+        state.proj = I.proj;
+        stt_status st = stt_solver_create(I.ctx, &cfg, &state, &in.solver);
+        if (st) return bail(st, "instance " + std::to_string(i) + ": " + stt_last_error(I.ctx));
+    }
+    if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+        return bail(STT_ERR_CUDA, "event create");
+    *out = b;
+    return STT_OK;
+}
+
+stt_status stt_batch_iterate(stt_batch *b, int n_iters, void *stream) {
+    if (!b || n_iters < 0) return STT_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+    for (int it = 0; it < n_iters; ++it) {
+        if (b->mode == STT_SOLVE_STREAMS) {
+            stt_status st = enqueue_all(b, cs);
+            if (st) return st;
+            continue;
+        }
+        if (!b->exec) {
+            cudaStream_t cap;
+            BCUDA(b, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "capture stream");
+            BCUDA(b, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+            stt_status st = enqueue_all(b, cap);
+            cudaGraph_t graph = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+            cudaStreamDestroy(cap);
+            if (st) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            if (ce != cudaSuccess) return bfail(b, STT_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ce));
+            b->graph = graph;
+            BCUDA(b, cudaGraphInstantiate(&b->exec, graph, 0), "graph instantiate");
+        }
+        BCUDA(b, cudaGraphLaunch(b->exec, cs), "graph launch");
+    }
+    return STT_OK;
+}
+
+const char *stt_batch_last_error(const stt_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+stt_status stt_batch_destroy(stt_batch *b) {
+    if (!b) return STT_OK;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (stt_batch::Inst &in : b->inst) {
+        if (in.solver) stt_solver_destroy(in.solver);
+        if (in.done) cudaEventDestroy(in.done);
+        if (in.stream) cudaStreamDestroy(in.stream);
+        cudaFree(in.state);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    delete b;
+    return STT_OK;
+}
+
+}  // extern "C"

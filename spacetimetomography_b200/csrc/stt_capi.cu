@@ -158,6 +158,15 @@ stt_status stt_destroy(stt_ctx *ctx) {
     return STT_OK;
 }
 
+stt_status stt_ctx_dims(const stt_ctx *ctx, int *dims) {
+    if (!ctx || !dims) return STT_ERR_INVALID;
+    if (!ctx->has_geom) return STT_ERR_STATE;
+    dims[0] = ctx->g.nx;
+    dims[1] = ctx->g.ny;
+    dims[2] = ctx->g.nz;
+    return STT_OK;
+}
+
 const char *stt_last_error(const stt_ctx *ctx) {
     return ctx ? ctx->err.c_str() : g_thread_err.c_str();
 }
