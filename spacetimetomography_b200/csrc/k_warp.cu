@@ -6,7 +6,9 @@
 // the centre lands on a node), one clamped tricubic velocity sample at the
 // half-traced point (3 channels sharing one 64-tap stencil) and one clamped
 // tricubic sample of every source channel at the traced point.  Taps come from
-// L1/L2 through the read-only path.
+// L1/L2 through the read-only path; the cell corners of the clamp are taps of
+// the stencil, so a sample is at most 64 loads per channel.  The kernel is
+// bound by L1 load wavefronts, not by HBM.
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
 #include "warp_dev.cuh"
@@ -17,20 +19,50 @@ namespace {
 
 using namespace warpdev;
 
-__global__ void __launch_bounds__(128) k_warp(const Dim3i d, const float *__restrict__ vel,
-                                              const float *__restrict__ src, int nc, float dt,
-                                              float *__restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    if (i >= d.x) return;
-    const size_t n = (size_t)d.x * d.y * d.z;
-    float q[3], p2[3], v1[3], v2[3];
-    trace(d, vel, n, i, j, k, -dt, q, p2, v1, v2);
-    float gq[3] = {to_grid(q[0], d.x, nullptr), to_grid(q[1], d.y, nullptr), to_grid(q[2], d.z, nullptr)};
-    Stencil s;
-    make_stencil(d, gq, s);
-    const size_t o = i + (size_t)j * d.x + (size_t)k * d.x * d.y;
-    for (int c = 0; c < nc; ++c) out[o + c * n] = sample_clamped(src + c * n, s);
+// Blocks of 32 x 4 voxels: a warp is one x-run of 32, so every tap load of a
+// warp reads ~32 consecutive floats, and the block's four rows share most of
+// their stencil rows in L1.  All offsets are 32-bit (the host bounds
+// n * max(nc, 3) below 2^31).
+constexpr int WARP_BX = 32, WARP_BY = 4;
+
+__global__ void __launch_bounds__(WARP_BX *WARP_BY) k_warp(const Dim3i d, const float *__restrict__ vel,
+                                                           const float *__restrict__ src, int nc, float dt,
+                                                           float *__restrict__ out) {
+    const int i = blockIdx.x * WARP_BX + threadIdx.x;
+    const int j = blockIdx.y * WARP_BY + threadIdx.y, k = blockIdx.z;
+    if (i >= d.x || j >= d.y) return;
+    const int n = d.x * d.y * d.z;
+    const float h = -dt;
+    // cell centre (warping.h:25-29); the velocity there is an exact node read
+    const float p[3] = {(float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f};
+    const int ci = min(max(i, 1), d.x - 2), cj = min(max(j, 1), d.y - 2), ck = min(max(k, 1), d.z - 2);
+    const int c = ci + cj * d.x + ck * d.x * d.y;
+    const float v1[3] = {__ldg(vel + c), __ldg(vel + n + c), __ldg(vel + 2 * n + c)};
+    // trace (warping.h:100-114): p2 = p + h v(p); p0 = p2 - h v(p2); q = p2 + (p - p0)/2
+    float p2[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) p2[a] = __fadd_rn(p[a], __fmul_rn(h, v1[a]));
+    const float g2[3] = {to_grid(p2[0], d.x, nullptr), to_grid(p2[1], d.y, nullptr),
+                         to_grid(p2[2], d.z, nullptr)};
+    Cell s2;
+    cell_setup(d, g2, s2);
+    float v2[3];
+    sample_cell<3>(vel, n, s2, v2);
+    float q[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float p0 = __fsub_rn(p2[a], __fmul_rn(h, v2[a]));
+        q[a] = __fadd_rn(p2[a], __fmul_rn(0.5f, __fsub_rn(p[a], p0)));
+    }
+    const float gq[3] = {to_grid(q[0], d.x, nullptr), to_grid(q[1], d.y, nullptr), to_grid(q[2], d.z, nullptr)};
+    Cell s;
+    cell_setup(d, gq, s);
+    const int o = i + j * d.x + k * d.x * d.y;
+    for (int ch = 0; ch < nc; ++ch) {
+        float v[1];
+        sample_cell<1>(src + (size_t)ch * n, 0, s, v);
+        out[o + (size_t)ch * n] = v[0];
+    }
 }
 
 // ---- VJP ---------------------------------------------------------------
@@ -182,7 +214,8 @@ __global__ void __launch_bounds__(128) k_warp_vjp(const Dim3i d, const float *__
 cudaError_t launch_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
                         float *out, cudaStream_t s) {
     Dim3i d{dim[0], dim[1], dim[2]};
-    k_warp<<<dim3((d.x + 127) / 128, d.y, d.z), 128, 0, s>>>(d, vel, src, nc, dt, out);
+    k_warp<<<dim3((d.x + WARP_BX - 1) / WARP_BX, (d.y + WARP_BY - 1) / WARP_BY, d.z), dim3(WARP_BX, WARP_BY), 0,
+             s>>>(d, vel, src, nc, dt, out);
     return cudaGetLastError();
 }
 

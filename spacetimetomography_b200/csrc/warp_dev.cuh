@@ -91,6 +91,87 @@ __device__ __forceinline__ float sample_clamped(const float *__restrict__ img, c
     return (mn < inner) ? inner : mn;
 }
 
+// ---- forward sampler with 32-bit offsets and shared rows -------------------
+// The grid coordinate g is already clamped to [1, dim-2], so with x = (int)g:
+//  * taps x-1, x, x+1 are always inside the image.  CImg takes x instead of
+//    x+1 when the fraction is 0, where the Catmull-Rom weight of that tap is
+//    exactly 0: for finite data both give the same sum, and x+1 is then also
+//    the cell's +1 corner, so the 8 corners are taps 1..2 on every axis and
+//    need no loads of their own;
+//  * tap x+2 leaves the image only when x = dim-2, i.e. g = dim-2 exactly and
+//    the fraction is 0, where its weight is exactly 0: the tap is skipped
+//    (a zero row or tap adds nothing), so no load ever leaves the image.
+struct Axis {
+    int lo;      // element offset of tap 0 (x-1) along this axis
+    bool t3;     // tap 3 (x+2) inside the image
+    float w[4];  // Catmull-Rom weights of the fraction
+};
+
+__device__ __forceinline__ void axis_setup(float g, int stride, int dim, Axis &a) {
+    const int x = (int)g;
+    cr_weights(g - (float)x, a.w);
+    a.lo = (x - 1) * stride;
+    a.t3 = x + 2 < dim;
+}
+
+struct Cell {
+    Axis x, y, z;
+    int sy, sz;  // row and plane strides
+};
+
+__device__ __forceinline__ void cell_setup(const Dim3i d, const float g[3], Cell &c) {
+    c.sy = d.x;
+    c.sz = d.x * d.y;
+    axis_setup(g[0], 1, d.x, c.x);
+    axis_setup(g[1], c.sy, d.y, c.y);
+    axis_setup(g[2], c.sz, d.z, c.z);
+}
+
+// sample_image (warping.h:49-88) of NC planes that share one cell: the
+// Catmull-Rom value of each, clamped to the min/max of its 8 cell corners.
+// Plane p starts at img + p * pstride.  The sums run in the order of
+// sample_clamped above (x taps, then rows, then planes), so both give the
+// same bits.
+template <int NC>
+__device__ __forceinline__ void sample_cell(const float *__restrict__ img, int pstride, const Cell &s,
+                                            float out[NC]) {
+    float val[NC], mn[NC], mx[NC];
+#pragma unroll
+    for (int p = 0; p < NC; ++p) {
+        val[p] = 0.0f;
+        mn[p] = INFINITY;
+        mx[p] = -INFINITY;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        if (c == 3 && !s.z.t3) break;
+        float yv[NC];
+#pragma unroll
+        for (int p = 0; p < NC; ++p) yv[p] = 0.0f;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            if (b == 3 && !s.y.t3) break;
+            const int row = s.x.lo + s.y.lo + b * s.sy + s.z.lo + c * s.sz;
+#pragma unroll
+            for (int p = 0; p < NC; ++p) {
+                const float *r = img + p * pstride + row;
+                const float t0 = __ldg(r), t1 = __ldg(r + 1), t2 = __ldg(r + 2);
+                const float t3 = s.x.t3 ? __ldg(r + 3) : 0.0f;
+                const float xv = s.x.w[0] * t0 + s.x.w[1] * t1 + s.x.w[2] * t2 + s.x.w[3] * t3;
+                yv[p] += s.y.w[b] * xv;
+                if ((b == 1 || b == 2) && (c == 1 || c == 2)) {
+                    mn[p] = fminf(mn[p], fminf(t1, t2));
+                    mx[p] = fmaxf(mx[p], fmaxf(t1, t2));
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < NC; ++p) val[p] += s.z.w[c] * yv[p];
+    }
+#pragma unroll
+    for (int p = 0; p < NC; ++p) out[p] = fmaxf(mn[p], fminf(val[p], mx[p]));
+}
+
 __device__ __forceinline__ void trace(const Dim3i d, const float *__restrict__ vel, size_t n, int i,
                                       int j, int k, float h, float q[3], float p2[3], float v1[3],
                                       float v2[3]) {
