@@ -1,0 +1,321 @@
+// k_fp_slab.cu -- forward projection + SART correction with the volume staged
+// into shared memory by TMA, slab by slab.
+//
+// A block is the 32x4-pixel detector tile of k_fp_corr: 128 nearly parallel
+// rays.  Along the volume copy's slowest axis (z for the x-fastest volume, x
+// for the z-fastest copy: the axis the rays of the view mostly run along) the
+// block walks slabs of SB-1 planes.  For each slab it loads, with one
+// cp.async.bulk.tensor.3d, the FB x YB x SB box (fast, y, slow) that holds
+// every trilinear tap of its rays' samples in those planes, double-buffered
+// behind an mbarrier, and every ray takes the samples whose base plane lies
+// in the slab from shared memory.  The 8 taps of a sample are then 8 shared
+// loads at fixed offsets, in place of 8 global gathers whose warp-wide
+// requests touch several cache lines each.
+//
+// Each ray keeps its own march (MarchGen: the samples of march(), in order)
+// and its own Kahan sum; a slab only decides where a sample's taps are read.
+// A sample whose taps are not in the box (a ray outside the box's extent, the
+// pre-entry restart of the march walking back, a timed-out copy) reads them
+// from global memory, and the samples left after the last slab are drained the
+// same way, so the ray sums are those of k_fp_corr bit for bit.
+#include <climits>
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "stt_internal.cuh"
+#include "stt_kernels.h"
+#include "stt_tma.cuh"
+
+namespace stt {
+
+namespace {
+
+constexpr int FB = 48, YB = 8, SB = 12;  // staged box (fast, y, slow), floats; FB*4 is a multiple of 16
+constexpr int BOXN = FB * YB * SB;
+constexpr unsigned BOX_BYTES = BOXN * sizeof(float);
+constexpr int SLAB = SB - 1;                     // base planes per slab; the box also holds their +1 plane
+constexpr long long WAIT_CYCLES = 200000000LL;  // about 0.1 s: a copy that never lands is an error
+constexpr int WARPS = 4;                         // 128-thread blocks
+
+__device__ __forceinline__ int warp_min(int v) { return __reduce_min_sync(0xffffffffu, v); }
+
+// Block-wide minima of (a, b), through red[0..2*WARPS).  One barrier.
+__device__ __forceinline__ void block_min2(int &a, int &b, int *red) {
+    a = warp_min(a);
+    b = warp_min(b);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[2 * w] = a;
+        red[2 * w + 1] = b;
+    }
+    __syncthreads();
+    a = red[0];
+    b = red[1];
+#pragma unroll
+    for (int k = 1; k < WARPS; ++k) {
+        a = min(a, red[2 * k]);
+        b = min(b, red[2 * k + 1]);
+    }
+}
+
+template <bool ZF>
+struct SlabAxes {
+    static constexpr int F = ZF ? 2 : 0;  // contiguous axis of the copy
+    static constexpr int S = ZF ? 0 : 2;  // slowest axis: the slab axis
+};
+
+// Lowest (fast, y) base coordinates of the taps of this ray's samples whose
+// slow coordinate lies in [m0, m0 + SLAB), with a voxel of margin; INT_MAX
+// when the ray has none there.
+template <bool ZF>
+__device__ __forceinline__ void ray_box_low(const GeomDev &g, const Ray &r, bool hit, int m0, int &lf, int &ly) {
+    constexpr int F = SlabAxes<ZF>::F, S = SlabAxes<ZF>::S;
+    lf = INT_MAX;
+    ly = INT_MAX;
+    if (!hit) return;
+    const float ta = __fdividef((float)m0 - 0.5f - r.vz[S], r.vu[S]);
+    const float tb = __fdividef((float)(m0 + SLAB) + 0.5f - r.vz[S], r.vu[S]);
+    const float tl = fmaxf(fminf(ta, tb), r.tnear - g.sd), th = fminf(fmaxf(ta, tb), r.tfar + g.sd);
+    if (!(tl <= th)) return;
+    const int dimF = ZF ? g.nz : g.nx;
+    const float f = fminf(r.vz[F] + r.vu[F] * tl, r.vz[F] + r.vu[F] * th);
+    const float y = fminf(r.vz[1] + r.vu[1] * tl, r.vz[1] + r.vu[1] * th);
+    lf = (int)floorf(fminf(fmaxf(f, 0.0f), (float)(dimF - 1))) - 1;
+    ly = (int)floorf(fminf(fmaxf(y, 0.0f), (float)(g.ny - 1))) - 1;
+}
+
+// The march of one ray of the block, summed into `acc`, taps from the staged
+// slabs where they are held.
+template <bool ZF>
+__device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap *map, const float *__restrict__ src,
+                                             bool hit, const Ray &r, float *buf, uint64_t *bar, int *red_s,
+                                             int (*red)[2 * WARPS], volatile int *dead, int *status, Kahan &acc) {
+    constexpr int S = SlabAxes<ZF>::S;
+    const int dimS = ZF ? g.nx : g.nz;
+    const Strides st = ZF ? zyx_strides(g) : xyz_strides(g);
+    MarchGen m;
+    if (hit) m.init(g, r);
+    else m.phase = 2;
+
+    // The base planes the block's rays span and the direction they run in.
+    int lo = INT_MAX, nhi = INT_MAX, up = 0;
+    if (hit) {
+        const float a = r.vz[S] + r.vu[S] * r.tnear, b = r.vz[S] + r.vu[S] * r.tfar;
+        const float pl = fminf(fmaxf(fminf(a, b), 0.0f), (float)(dimS - 1));
+        const float ph = fminf(fmaxf(fmaxf(a, b), 0.0f), (float)(dimS - 1));
+        lo = min((int)pl, dimS - 2);
+        nhi = -min((int)ph, dimS - 2);
+        up = r.vu[S] > 0.0f ? 1 : -1;
+    }
+    lo = warp_min(lo);
+    nhi = warp_min(nhi);
+    up = __reduce_add_sync(0xffffffffu, up);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red_s[3 * w] = lo;
+        red_s[3 * w + 1] = nhi;
+        red_s[3 * w + 2] = up;
+    }
+    if (threadIdx.x == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::fence_barrier_init();
+        tma::prefetch_map(map);
+        *dead = 0;
+    }
+    __syncthreads();
+    lo = red_s[0];
+    nhi = red_s[1];
+    up = red_s[2];
+#pragma unroll
+    for (int k = 1; k < WARPS; ++k) {
+        lo = min(lo, red_s[3 * k]);
+        nhi = min(nhi, red_s[3 * k + 1]);
+        up += red_s[3 * k + 2];
+    }
+    if (lo == INT_MAX) return;  // no ray of the block hits the volume
+    const int hi = -nhi;
+    const bool fwd = up >= 0;
+    const int nslab = (hi - lo) / SLAB + 1;
+    auto slab_m0 = [&](int k) { return fwd ? lo + k * SLAB : hi - (SLAB - 1) - k * SLAB; };
+
+    // slab 0
+    int f0, y0;
+    {
+        ray_box_low<ZF>(g, r, hit, slab_m0(0), f0, y0);
+        block_min2(f0, y0, red[0]);
+        if (f0 == INT_MAX) f0 = y0 = 0;
+        f0 = (f0 >> 2) << 2;  // the box's innermost coordinate starts on 16 bytes
+        if (threadIdx.x == 0) {
+            tma::mbar_arrive_expect_tx(&bar[0], BOX_BYTES);
+            tma::load_box_3d(buf, map, f0, y0, slab_m0(0), &bar[0]);
+        }
+    }
+    bool gave_up = false;  // a copy did not land: the remaining samples read global memory
+    for (int k = 0; k < nslab; ++k) {
+        // issue slab k+1 into the other buffer (free since the barrier that ended slab k-1)
+        int fn = 0, yn = 0;
+        if (k + 1 < nslab && !gave_up) {
+            ray_box_low<ZF>(g, r, hit, slab_m0(k + 1), fn, yn);
+            block_min2(fn, yn, red[(k + 1) & 1]);
+            if (fn == INT_MAX) fn = yn = 0;
+            fn = (fn >> 2) << 2;
+            if (threadIdx.x == 0) {
+                const int nb = (k + 1) & 1;
+                tma::mbar_arrive_expect_tx(&bar[nb], BOX_BYTES);
+                tma::load_box_3d(buf + nb * BOXN, map, fn, yn, slab_m0(k + 1), &bar[nb]);
+            }
+        }
+        bool staged = false;
+        if (!gave_up) {
+            staged = tma::mbar_wait(&bar[k & 1], (k >> 1) & 1, WAIT_CYCLES);
+            if (!staged) {
+                *dead = 1;
+                if (status) atomicExch(status, 1);
+            }
+        }
+        const float *bx = buf + (k & 1) * BOXN;
+        const int m0 = slab_m0(k);
+        while (m.peek()) {
+            FpCell c;
+            fp_cell(g, m.pos, c);
+            const int bs = ZF ? c.ix : c.iz;
+            if (fwd ? bs > m0 + SLAB - 1 : bs < m0) break;  // belongs to a later slab
+            const unsigned of = (unsigned)((ZF ? c.iz : c.ix) - f0), oy = (unsigned)(c.iy - y0),
+                           os = (unsigned)(bs - m0);
+            float v[8];
+            if (staged && of <= FB - 2 && oy <= YB - 2 && os <= SB - 2) {
+                const float *q = bx + (os * YB + oy) * FB + of;
+                if (!ZF) {  // fast = x, slow = z
+                    v[0] = q[0], v[1] = q[1], v[2] = q[FB], v[3] = q[FB + 1];
+                    v[4] = q[FB * YB], v[5] = q[FB * YB + 1], v[6] = q[FB * YB + FB], v[7] = q[FB * YB + FB + 1];
+                } else {  // fast = z, slow = x
+                    v[0] = q[0], v[4] = q[1], v[2] = q[FB], v[6] = q[FB + 1];
+                    v[1] = q[FB * YB], v[5] = q[FB * YB + 1], v[3] = q[FB * YB + FB], v[7] = q[FB * YB + FB + 1];
+                }
+            } else {
+                fp_corners<ZF ? 2 : 0, int>(src, st, c, v);
+            }
+            acc.add(__fmul_rn(trilerp(v, c), g.sd));
+            m.advance();
+        }
+        __syncthreads();  // every ray is done with buffer k&1 before slab k+2 is loaded into it
+        gave_up = *dead != 0;
+        f0 = fn;
+        y0 = yn;
+    }
+    // samples outside the planes the slabs covered
+    while (m.peek()) {
+        FpCell c;
+        fp_cell(g, m.pos, c);
+        float v[8];
+        fp_corners<ZF ? 2 : 0, int>(src, st, c, v);
+        acc.add(__fmul_rn(trilerp(v, c), g.sd));
+        m.advance();
+    }
+}
+
+// k_fp_corr (GenerateImage_MT + the correction of ST_Tomography.cpp:667-676)
+// with slab-staged gathers.  map_x covers `vol` (x-fastest), map_z `vol_t`
+// (z-fastest), both with the box FB x YB x SB.
+__global__ void __launch_bounds__(128) k_fp_corr_slab(const GeomDev g, const ViewRec *__restrict__ views,
+                                                      const __grid_constant__ CUtensorMap map_x,
+                                                      const __grid_constant__ CUtensorMap map_z,
+                                                      const float *__restrict__ vol, const float *__restrict__ vol_t,
+                                                      const ViewSel sel, const float *__restrict__ b_stack,
+                                                      float *__restrict__ raylen_state, float *__restrict__ corr,
+                                                      unsigned long long corr_surf, int *status) {
+    __shared__ alignas(128) float buf[2 * BOXN];
+    __shared__ uint64_t bar[2];
+    __shared__ int red[2][2 * WARPS];
+    __shared__ int red_s[3 * WARPS];
+    __shared__ int dead;
+    const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * 4 + (threadIdx.x >> 5);
+    const bool valid = i < g.W && j < g.H;
+    int local;
+    const int view = sel_view(sel, local);
+    const ViewRec &vr = views[view];
+    if (!vr.staged) return;  // the gather kernel projects this view (uniform over the block)
+    Ray r;
+    bool hit = false;
+    if (valid) {
+        make_ray(g, vr, i, j, r);
+        hit = r.tnear < r.tfar;
+    }
+    Kahan acc{0.0f, 0.0f};
+    if (vol_t && vr.layout == 1)
+        slab_ray_sum<true>(g, &map_z, vol_t, hit, r, buf, bar, red_s, red, &dead, status, acc);
+    else
+        slab_ray_sum<false>(g, &map_x, vol, hit, r, buf, bar, red_s, red, &dead, status, acc);
+    if (!valid) return;
+    const float *b = b_stack + (size_t)local * g.W * g.H;
+    const size_t pix = i + (size_t)j * g.W;
+    float L;
+    if (hit) {
+        L = r.tfar - r.tnear;
+        if (raylen_state) raylen_state[pix] = L;
+    } else {
+        L = raylen_state ? raylen_state[pix] : 0.0f;
+    }
+    const float c = __fdiv_rn(__fsub_rn(__ldg(b + pix), acc.s), __fadd_rn(L, 1.0f));
+    corr[pix] = c;
+    if (corr_surf) surf2DLayeredwrite(c, corr_surf, i * (int)sizeof(float), j, 0, cudaBoundaryModeZero);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// A 3D FP32 tensor map (fast, mid, slow) over `ptr` with the slab box.
+bool encode_box_map(CUtensorMap *m, const float *ptr, int fast, int mid, int slow) {
+    const PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn || !ptr || (reinterpret_cast<uintptr_t>(ptr) & 15) || (fast & 3)) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)fast, (cuuint64_t)mid, (cuuint64_t)slow};
+    const cuuint64_t strides[2] = {(cuuint64_t)fast * sizeof(float), (cuuint64_t)fast * mid * sizeof(float)};
+    const cuuint32_t box[3] = {FB, YB, SB};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(ptr), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m) {
+    m = FpSlabMaps{};
+    if ((long long)g.nx * g.ny * g.nz >= (1LL << 31)) return false;  // 32-bit fallback offsets
+    if (!encode_box_map(&m.x, vol, g.nx, g.ny, g.nz)) return false;
+    if (vol_t && !encode_box_map(&m.z, vol_t, g.nz, g.ny, g.nx)) return false;
+    m.ok = 1;
+    m.has_z = vol_t != nullptr;
+    return true;
+}
+
+cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const float *vol,
+                                const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state,
+                                float *corr, cudaStream_t s, unsigned long long corr_surf, int *status) {
+    if (!m.ok || (vol_t && !m.has_z)) return cudaErrorInvalidValue;
+    static const bool carve = [] {
+        cudaFuncSetAttribute(k_fp_corr_slab, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        cudaGetLastError();
+        return true;
+    }();
+    (void)carve;
+    k_fp_corr_slab<<<dim3((g.W + 31) / 32, (g.H + 3) / 4, 1), 128, 0, s>>>(g, views, m.x, m.z, vol, vol_t, sel, b_stack,
+                                                                          raylen_state, corr, corr_surf, status);
+    return cudaGetLastError();
+}
+
+}  // namespace stt

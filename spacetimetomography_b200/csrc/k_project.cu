@@ -24,22 +24,51 @@ __device__ __forceinline__ bool tile_pixel(const GeomDev &g, int &i, int &j) {
     return i < g.W && j < g.H;
 }
 
-// Source and strides of the forward projector's gathers for one view.
-template <typename T>
-__device__ __forceinline__ const T *fp_source(const GeomDev &g, const ViewRec &v, const T *vol, const T *vol_t,
-                                              Strides &st) {
-    if (vol_t && v.layout == 1) {
-        st = zyx_strides(g);
-        return vol_t;
-    }
-    st = xyz_strides(g);
-    return vol;
+// The ray sum of one forward-projector ray (hit rays only), gathered from the
+// z-fastest transposed copy for layout-1 views when one is given, else from
+// the volume.  Samples go two at a time where the march allows: both
+// samples' 16 taps are loaded before either is interpolated.
+template <int FAST, typename I, typename T>
+__device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__restrict__ src, const Strides &st,
+                                                 const Ray &r, int *count) {
+    Kahan acc{0.0f, 0.0f};
+    int n = 0;
+    march_pairs(
+        g, r,
+        [&](const float p[3]) {
+            FpCell c;
+            fp_cell(g, p, c);
+            float v[8];
+            fp_corners<FAST, I>(src, st, c, v);
+            acc.add(__fmul_rn(trilerp(v, c), g.sd));
+            ++n;
+        },
+        [&](const float p[3], const float q[3]) {
+            FpCell c, e;
+            fp_cell(g, p, c);
+            fp_cell(g, q, e);
+            float v[8], w[8];
+            fp_corners<FAST, I>(src, st, c, v);
+            fp_corners<FAST, I>(src, st, e, w);
+            acc.add(__fmul_rn(trilerp(v, c), g.sd));
+            acc.add(__fmul_rn(trilerp(w, e), g.sd));
+            n += 2;
+        });
+    if (count) *count = n;
+    return acc.s;
+}
+
+template <typename I, typename T>
+__device__ __forceinline__ float fp_ray_sum(const GeomDev &g, const ViewRec &v, const T *__restrict__ vol,
+                                            const T *__restrict__ vol_t, const Ray &r, int *count) {
+    if (vol_t && v.layout == 1) return fp_ray_sum_from<2, I>(g, vol_t, zyx_strides(g), r, count);
+    return fp_ray_sum_from<0, I>(g, vol, xyz_strides(g), r, count);
 }
 
 // GenerateImage_MT (S/ImageFormationModel/TypicalRayProducer.core.h:168-224)
 // for views [view0, view0 + gridDim.z).  T = float, or unsigned short for a
 // BF16-stored volume (taps widened to FP32; the march and the sums are FP32).
-template <typename T>
+template <typename I, typename T>
 __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__restrict__ views,
                                             const T *__restrict__ vol, const T *__restrict__ vol_t,
                                             int view0, float *__restrict__ proj, float *__restrict__ raylen,
@@ -48,23 +77,13 @@ __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__re
     if (!tile_pixel(g, i, j)) return;
     const int v = blockIdx.z;
     const ViewRec &vr = views[view0 + v];
-    Strides st;
-    const T *src = fp_source(g, vr, vol, vol_t, st);
     Ray r;
     make_ray(g, vr, i, j, r);
-    Kahan acc{0.0f, 0.0f};
     int count = 0;
     const bool hit = r.tnear < r.tfar;
-    if (hit) {
-        march(g, r, [&](const float p[3]) {
-            Taps t;
-            make_taps(g, p, t, st);
-            acc.add(tri_value(src, t) * g.sd);
-            ++count;
-        });
-    }
+    const float sum = hit ? fp_ray_sum<I>(g, vr, vol, vol_t, r, &count) : 0.0f;
     const size_t o = (size_t)v * g.W * g.H + i + (size_t)j * g.W;
-    proj[o] = acc.s;
+    proj[o] = sum;
     if (raylen && hit) raylen[o] = r.tfar - r.tnear;
     if (weight) weight[o] = (float)count;
 }
@@ -74,36 +93,32 @@ __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__re
 // c = (b - Ax) / (L + 1)).  L is the sticky ray length of the producer:
 // updated where the ray hits, kept where it misses; with no state buffer
 // (ray-based SART, whose producer is reset after every view) a miss gives L = 0.
+template <typename I>
 __global__ void __launch_bounds__(128) k_fp_corr(const GeomDev g, const ViewRec *__restrict__ views,
                                                  const float *__restrict__ vol, const float *__restrict__ vol_t,
                                                  const ViewSel sel, const float *__restrict__ b_stack,
                                                  float *__restrict__ raylen_state,
-                                                 float *__restrict__ corr, unsigned long long corr_surf) {
+                                                 float *__restrict__ corr, unsigned long long corr_surf,
+                                                 int skip_staged) {
     int i, j;
     if (!tile_pixel(g, i, j)) return;
     int local;
     const int view = sel_view(sel, local);
     const float *b = b_stack + (size_t)local * g.W * g.H;
     const ViewRec &vr = views[view];
-    Strides st;
-    const float *src = fp_source(g, vr, vol, vol_t, st);
+    if (skip_staged && vr.staged) return;  // the slab-staged kernel projects this view
     Ray r;
     make_ray(g, vr, i, j, r);
-    Kahan acc{0.0f, 0.0f};
     const size_t pix = i + (size_t)j * g.W;
-    float L;
+    float L, sum = 0.0f;
     if (r.tnear < r.tfar) {
-        march(g, r, [&](const float p[3]) {
-            Taps t;
-            make_taps(g, p, t, st);
-            acc.add(tri_value(src, t) * g.sd);
-        });
+        sum = fp_ray_sum<I>(g, vr, vol, vol_t, r, nullptr);
         L = r.tfar - r.tnear;
         if (raylen_state) raylen_state[pix] = L;
     } else {
         L = raylen_state ? raylen_state[pix] : 0.0f;
     }
-    const float c = __fdiv_rn(__fsub_rn(__ldg(b + pix), acc.s), __fadd_rn(L, 1.0f));
+    const float c = __fdiv_rn(__fsub_rn(__ldg(b + pix), sum), __fadd_rn(L, 1.0f));
     corr[pix] = c;
     // the copy the voxel-driven backprojector gathers from with tld4
     if (corr_surf) surf2DLayeredwrite(c, corr_surf, i * (int)sizeof(float), j, 0, cudaBoundaryModeZero);
@@ -197,22 +212,57 @@ __global__ void k_correction(long long n, const float *__restrict__ b, const flo
         corr[k] = __fdiv_rn(__fsub_rn(b[k], ax[k]), __fadd_rn(raylen ? raylen[k] : 0.0f, 1.0f));
 }
 
-// z-fastest copy of an x-fastest volume: out[z + y*nz + x*nz*ny] = in[x + y*nx + z*nx*ny],
-// one (x, z) plane of fixed y per block row, 32x32 tiles through shared memory.
+// z-fastest copy of an x-fastest volume: out[z + y*nz + x*nz*ny] = in[x + y*nx + z*nx*ny].
+// One 64x64 (x, z) tile of one y plane per block of 32x8 threads, through
+// shared memory.  Interior tiles move two elements per access (8-byte float2
+// or 4-byte ushort2 rows) when nx and nz are even and both arrays aligned to
+// a pair; edge tiles move one.
+template <typename T>
+struct Pair2;
+template <>
+struct Pair2<float> {
+    typedef float2 type;
+};
+template <>
+struct Pair2<unsigned short> {
+    typedef ushort2 type;
+};
+
 template <typename T>
 __device__ __forceinline__ void transpose_tile(int nx, int ny, int nz, const T *__restrict__ in,
                                                T *__restrict__ out) {
-    __shared__ T tile[32][33];
-    const int x0 = blockIdx.x * 32, z0 = blockIdx.y * 32, y = blockIdx.z;
+    typedef typename Pair2<T>::type P;
+    __shared__ T tile[64][65];  // tile[z - z0][x - x0]
+    const int x0 = blockIdx.x * 64, z0 = blockIdx.y * 64, y = blockIdx.z;
     const size_t nxy = (size_t)nx * ny, nzy = (size_t)nz * ny;
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-        const int z = z0 + r, x = x0 + threadIdx.x;
-        if (x < nx && z < nz) tile[r][threadIdx.x] = __ldg(in + x + (size_t)y * nx + z * nxy);
-    }
-    __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-        const int x = x0 + r, z = z0 + threadIdx.x;
-        if (x < nx && z < nz) out[z + (size_t)y * nz + x * nzy] = tile[threadIdx.x][r];
+    const T *src = in + (size_t)y * nx + x0 + (size_t)z0 * nxy;
+    T *dst = out + (size_t)y * nz + z0 + (size_t)x0 * nzy;
+    const int tx = threadIdx.x;
+    const bool pairs = x0 + 64 <= nx && z0 + 64 <= nz && !(nx & 1) && !(nz & 1) &&
+                       !(((uintptr_t)in | (uintptr_t)out) % sizeof(P));
+    if (pairs) {
+#pragma unroll
+        for (int r = threadIdx.y; r < 64; r += 8) {
+            const P v = reinterpret_cast<const P *>(src + r * nxy)[tx];
+            tile[r][2 * tx] = v.x;
+            tile[r][2 * tx + 1] = v.y;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = threadIdx.y; r < 64; r += 8) {
+            P v;
+            v.x = tile[2 * tx][r];
+            v.y = tile[2 * tx + 1][r];
+            reinterpret_cast<P *>(dst + r * nzy)[tx] = v;
+        }
+    } else {
+        for (int r = threadIdx.y; r < 64; r += 8)
+            for (int c = tx; c < 64; c += 32)
+                if (x0 + c < nx && z0 + r < nz) tile[r][c] = src[c + r * nxy];
+        __syncthreads();
+        for (int r = threadIdx.y; r < 64; r += 8)
+            for (int c = tx; c < 64; c += 32)
+                if (x0 + r < nx && z0 + c < nz) dst[c + r * nzy] = tile[c][r];
     }
 }
 
@@ -238,11 +288,14 @@ __global__ void k_fill_zero(long long n, float *__restrict__ p) {
         p[k] = 0.0f;
 }
 
+// 32-bit gather offsets when every voxel index fits.
+bool small_volume(const GeomDev &g) { return (long long)g.nx * g.ny * g.nz < (1LL << 31); }
+
 dim3 ray_grid(const GeomDev &g, int nviews) {
     return dim3((g.W + 31) / 32, (g.H + 3) / 4, nviews);
 }
 
-dim3 transpose_grid(const GeomDev &g) { return dim3((g.nx + 31) / 32, (g.nz + 31) / 32, g.ny); }
+dim3 transpose_grid(const GeomDev &g) { return dim3((g.nx + 63) / 64, (g.nz + 63) / 64, g.ny); }
 
 }  // namespace
 
@@ -254,14 +307,28 @@ int grid_stride_blocks(long long n, int threads) {
 
 cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, int view0,
                       int nviews, float *proj, float *raylen, float *weight, cudaStream_t s) {
-    k_fp<float><<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen, weight);
+    if (small_volume(g))
+        k_fp<int, float><<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen, weight);
+    else
+        k_fp<long long, float><<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen, weight);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
-                           cudaStream_t s, unsigned long long corr_surf) {
-    k_fp_corr<<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf);
+                           cudaStream_t s, unsigned long long corr_surf, const FpSlabMaps *maps, int *status) {
+    const int skip = maps && maps->ok && (!vol_t || maps->has_z);
+    if (skip) {
+        cudaError_t e = launch_fp_corr_slab(g, views, *maps, vol, vol_t, sel, b_stack, raylen_state, corr, s,
+                                            corr_surf, status);
+        if (e != cudaSuccess) return e;
+    }
+    if (small_volume(g))
+        k_fp_corr<int><<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf,
+                                                      skip);
+    else
+        k_fp_corr<long long><<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr,
+                                                            corr_surf, skip);
     return cudaGetLastError();
 }
 
@@ -273,7 +340,11 @@ cudaError_t launch_transpose(const GeomDev &g, const float *in, float *out, cuda
 cudaError_t launch_fp_bf16(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
                            const unsigned short *vol_t, int view0, int nviews, float *proj, float *raylen,
                            float *weight, cudaStream_t s) {
-    k_fp<unsigned short><<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen, weight);
+    if (small_volume(g))
+        k_fp<int, unsigned short><<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen, weight);
+    else
+        k_fp<long long, unsigned short><<<ray_grid(g, nviews), 128, 0, s>>>(g, views, vol, vol_t, view0, proj, raylen,
+                                                                            weight);
     return cudaGetLastError();
 }
 

@@ -107,7 +107,8 @@ void build_view(const stt_geometry &g, double theta, stt::ViewRec &v) {
     }
     // gather from the z-fastest copy when the central ray runs more along x than z
     v.layout = std::fabs(s) > std::fabs(c) ? 1 : 0;
-    for (int k = 0; k < 3; ++k) v.pad[k] = 0.0f;
+    v.staged = std::fmin(std::fabs(s), std::fabs(c)) > 0.4226 ? 1 : 0;  // sin 25 degrees
+    for (int k = 0; k < 2; ++k) v.pad[k] = 0.0f;
 }
 
 template <typename T>
@@ -353,7 +354,9 @@ stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, flo
     const stt::ViewSel sel{view, nullptr, 0, view};
     const float *volt = nullptr;
     if ((st = transposed_if_needed(ctx, vol, view, 1, S(stream), &volt))) return st;
-    STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, b, raylen_state, corr, S(stream)),
+    stt::FpSlabMaps maps;
+    stt::make_fp_slab_maps(ctx->g, vol, volt, maps);
+    STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, b, raylen_state, corr, S(stream), 0, &maps),
              "k_fp_corr launch");
     return STT_OK;
 }
@@ -441,10 +444,12 @@ stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, con
         const stt::ViewSel sel{view_offset + perm[i], nullptr, 0, view_offset};
         const float *volt = nullptr;
         if ((st = transposed_if_needed(ctx, vol, view_offset + perm[i], 1, s, &volt))) return st;
+        stt::FpSlabMaps maps;
+        stt::make_fp_slab_maps(ctx->g, vol, volt, maps);
         // ray-based mode: TypicalRayProducer::Initial zeroes the ray lengths
         // after every view, so missed rays see L = 0 (no sticky state)
         STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, proj_stack,
-                                          bp_mode == 0 ? raylen_state : nullptr, ctx->corr, s),
+                                          bp_mode == 0 ? raylen_state : nullptr, ctx->corr, s, 0, &maps),
                  "k_fp_corr launch");
         if (bp_mode == 0)
             STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, sel, ctx->corr, vol, (float)alpha, gmax, s),

@@ -21,7 +21,11 @@ namespace stt {
 // `layout` selects the volume copy the forward projector gathers from: 0 the
 // x-fastest volume, 1 a z-fastest transposed copy, chosen on the host for views
 // whose central ray runs more along x than along z, so that a warp's 32 rays
-// (consecutive detector columns) sample consecutive addresses.
+// (consecutive detector columns) sample consecutive addresses.  `staged` marks
+// the oblique views (central ray more than 25 degrees off both x and z), whose
+// gathers spread over several planes per warp request: the forward projector
+// with the SART correction stages their volume slabs into shared memory
+// (k_fp_slab.cu) when it can.
 struct ViewRec {
     double src[3];
     double det0[3];
@@ -30,7 +34,8 @@ struct ViewRec {
     float A[9];
     float b[3];
     int layout;
-    float pad[3];
+    int staged;
+    float pad[2];
 };
 
 struct GeomDev {
@@ -67,13 +72,15 @@ __device__ __forceinline__ int sel_view(const ViewSel &s, int &local) {
     return s.base + local;
 }
 
-// Compensated (Kahan) accumulator for ray sums.
+// Compensated (Kahan) accumulator for ray sums.  Every operation is rounded
+// on its own (no contraction), so kernels that add the same samples in the
+// same order get the same bits whatever the compiler fuses around them.
 struct Kahan {
     float s, c;
     __device__ __forceinline__ void add(float v) {
-        float y = v - c;
-        float t = s + y;
-        c = (t - s) - y;
+        const float y = __fsub_rn(v, c);
+        const float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
         s = t;
     }
 };
@@ -148,7 +155,6 @@ __device__ __forceinline__ void make_taps(const GeomDev &g, const float p[3], Ta
     make_taps(g, p, t, xyz_strides(g));
 }
 
-// x, then y, then z as the reference interpolates.
 // One stored voxel as float: FP32 as is; BF16 storage (raw 16-bit patterns,
 // the upper half of an FP32) widened exactly.
 __device__ __forceinline__ float ld_voxel(const float *p) { return __ldg(p); }
@@ -156,22 +162,78 @@ __device__ __forceinline__ float ld_voxel(const unsigned short *p) {
     return __uint_as_float((unsigned)__ldg(p) << 16);
 }
 
-template <typename T>
-__device__ __forceinline__ float tri_value(const T *__restrict__ vol, const Taps &t) {
-    const T *p = vol + t.base;
-    float v000 = ld_voxel(p), v100 = ld_voxel(p + t.dx);
-    float v010 = ld_voxel(p + t.dy), v110 = ld_voxel(p + t.dy + t.dx);
-    float v001 = ld_voxel(p + t.dz), v101 = ld_voxel(p + t.dz + t.dx);
-    float v011 = ld_voxel(p + t.dz + t.dy), v111 = ld_voxel(p + t.dz + t.dy + t.dx);
-    float fx1 = 1.0f - t.fx;
-    float a = v000 * fx1 + v100 * t.fx;
-    float b = v010 * fx1 + v110 * t.fx;
-    float c = v001 * fx1 + v101 * t.fx;
-    float d = v011 * fx1 + v111 * t.fx;
-    float fy1 = 1.0f - t.fy;
-    a = a * fy1 + b * t.fy;
-    c = c * fy1 + d * t.fy;
-    return a * (1.0f - t.fz) + c * t.fz;
+// The forward projector's sample: the clamped trilinear value of
+// SingleScalarVolume.core.h:87-120, lerped x, then y, then z as the reference
+// does.  The position is clamped to [0, dims-1] as in make_taps, but the base
+// is capped at dims-2, so the +1 neighbours are always one stride away and no
+// tap offset is selected per sample.  Where the reference's base is dims-1
+// (position exactly dims-1, fraction 0, +1 neighbour collapsed onto the base)
+// this base is dims-2 with fraction exactly 1: the lerp then returns the
+// dims-1 value exactly, as the reference's does, and the y and z lerps see the
+// same operands.
+struct FpCell {
+    int ix, iy, iz;    // base voxel, each capped at dims-2
+    float fx, fy, fz;  // fractions in [0, 1]
+};
+
+__device__ __forceinline__ void fp_cell(const GeomDev &g, const float p[3], FpCell &c) {
+    const float px = rmax(rmin(p[0], (float)(g.nx - 1)), 0.0f);
+    const float py = rmax(rmin(p[1], (float)(g.ny - 1)), 0.0f);
+    const float pz = rmax(rmin(p[2], (float)(g.nz - 1)), 0.0f);
+    c.ix = min((int)px, g.nx - 2);
+    c.iy = min((int)py, g.ny - 2);
+    c.iz = min((int)pz, g.nz - 2);
+    c.fx = px - (float)c.ix;
+    c.fy = py - (float)c.iy;
+    c.fz = pz - (float)c.iz;
+}
+
+// v[k] is the corner (x + (k&1), y + ((k>>1)&1), z + (k>>2)).  Each lerp
+// a*(1-f) + b*f is one explicit multiply and one fused multiply-add, so every
+// kernel that interpolates the same corners gets the same bits.
+__device__ __forceinline__ float lerp1(float a, float b, float f1, float f) {
+    return __fmaf_rn(b, f, __fmul_rn(a, f1));
+}
+
+__device__ __forceinline__ float trilerp(const float v[8], const FpCell &c) {
+    const float fx1 = __fsub_rn(1.0f, c.fx), fy1 = __fsub_rn(1.0f, c.fy), fz1 = __fsub_rn(1.0f, c.fz);
+    const float a = lerp1(v[0], v[1], fx1, c.fx);
+    const float b = lerp1(v[2], v[3], fx1, c.fx);
+    const float d0 = lerp1(v[4], v[5], fx1, c.fx);
+    const float d1 = lerp1(v[6], v[7], fx1, c.fx);
+    return lerp1(lerp1(a, b, fy1, c.fy), lerp1(d0, d1, fy1, c.fy), fz1, c.fz);
+}
+
+// The 8 corners of a cell from a volume array: FAST is its contiguous axis
+// (0: x, the volume; 2: z, its transposed copy), whose +1 neighbour is the
+// next element.  I is the index type: int when the volume has fewer than
+// 2^31 voxels.
+template <int FAST, typename I, typename T>
+__device__ __forceinline__ void fp_corners(const T *__restrict__ src, const Strides &st, const FpCell &c, float v[8]) {
+    const I idx = (I)c.ix * st.sx + (I)c.iy * st.sy + (I)c.iz * st.sz;
+    if (FAST == 0) {  // rows along x at (y, z), (y+1, z), (y, z+1), (y+1, z+1)
+        const I r00 = idx, r10 = idx + st.sy, r01 = idx + st.sz, r11 = r01 + st.sy;
+        v[0] = ld_voxel(src + r00), v[1] = ld_voxel(src + r00 + 1);
+        v[2] = ld_voxel(src + r10), v[3] = ld_voxel(src + r10 + 1);
+        v[4] = ld_voxel(src + r01), v[5] = ld_voxel(src + r01 + 1);
+        v[6] = ld_voxel(src + r11), v[7] = ld_voxel(src + r11 + 1);
+    } else {  // runs along z at (x, y), (x+1, y), (x, y+1), (x+1, y+1)
+        const I r00 = idx, r10 = idx + st.sx, r01 = idx + st.sy, r11 = r10 + st.sy;
+        v[0] = ld_voxel(src + r00), v[4] = ld_voxel(src + r00 + 1);
+        v[1] = ld_voxel(src + r10), v[5] = ld_voxel(src + r10 + 1);
+        v[2] = ld_voxel(src + r01), v[6] = ld_voxel(src + r01 + 1);
+        v[3] = ld_voxel(src + r11), v[7] = ld_voxel(src + r11 + 1);
+    }
+}
+
+template <int FAST, typename I, typename T>
+__device__ __forceinline__ float fp_sample(const GeomDev &g, const T *__restrict__ src, const Strides &st,
+                                           const float p[3]) {
+    FpCell c;
+    fp_cell(g, p, c);
+    float v[8];
+    fp_corners<FAST, I>(src, st, c, v);
+    return trilerp(v, c);
 }
 
 // Corner weights in the order of SingleScalarVolume.core.h:104-105.
@@ -202,6 +264,96 @@ __device__ __forceinline__ long long tap_index(const Taps &t, int k) {
 // box up to the split's far end, and so does this march.  `visit(pos)` is
 // called per sample.  Loops are bounded by the segment's own extent
 // ((tb - t)/sd + 2 samples), at most 16 segments, and 2^22 samples per ray.
+// Splits and steps of the march (RayCaster.core.h:62-128): the per-sample
+// step vu*sd, the first split point along each axis and the split spacing.
+struct MarchDda {
+    float tmax[3], tdelta[3], step[3];
+};
+
+__device__ __forceinline__ void march_dda(const GeomDev &g, const Ray &r, const float pos1[3], MarchDda &d) {
+    const int dims[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        d.step[k] = __fmul_rn(r.vu[k], g.sd);
+        const int b = dims[k];
+        if (r.vu[k] == 0.0f) {
+            d.tmax[k] = r.tfar;
+            d.tdelta[k] = 0.0f;
+        } else if (r.vu[k] < 0.0f) {
+            int blk = ((int)ceilf(pos1[k] - 0.5f) - 1) / b;
+            d.tmax[k] = __fdiv_rn(__fsub_rn(__fadd_rn((float)(blk * b), 0.5f), r.vz[k]), r.vu[k]);
+            d.tdelta[k] = __fdiv_rn((float)(-b), r.vu[k]);
+        } else {
+            int blk = ((int)floorf(pos1[k] - 0.5f)) / b;
+            d.tmax[k] = __fdiv_rn(__fsub_rn(__fadd_rn((float)((blk + 1) * b), 0.5f), r.vz[k]), r.vu[k]);
+            d.tdelta[k] = __fdiv_rn((float)b, r.vu[k]);
+        }
+    }
+}
+
+__device__ __forceinline__ void march_split(MarchDda &d) {
+    if (d.tmax[0] < d.tmax[1]) {
+        if (d.tmax[0] < d.tmax[2]) d.tmax[0] += d.tdelta[0];
+        else d.tmax[2] += d.tdelta[2];
+    } else {
+        if (d.tmax[1] < d.tmax[2]) d.tmax[1] += d.tdelta[1];
+        else d.tmax[2] += d.tdelta[2];
+    }
+}
+
+// The march, handing the samples of a segment out two at a time where two
+// remain: visit2(p, q) gets consecutive samples p, q (in that order), visit(p)
+// the entry sample and a segment's odd last one.  The samples and their order
+// are those of march(); a caller that issues both samples' loads before using
+// either keeps twice the loads in flight.
+template <typename Visit, typename Visit2>
+__device__ __forceinline__ void march_pairs(const GeomDev &g, const Ray &r, Visit &&visit, Visit2 &&visit2) {
+    const float sd = g.sd;
+    const float tnear = r.tnear, tfar = r.tfar;
+    float t1 = tnear;
+    float pos1[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) pos1[k] = __fadd_rn(r.vz[k], __fmul_rn(r.vu[k], t1));
+    visit(pos1);
+    MarchDda d;
+    march_dda(g, r, pos1, d);
+    constexpr int kMaxSamples = 1 << 22;
+    int budget = kMaxSamples;
+    for (int seg = 0; seg < 16 && t1 < tfar && budget > 0; ++seg) {
+        float tb = rmin(rmin(d.tmax[0], d.tmax[1]), d.tmax[2]);
+        if (tb > tfar) tb = tfar;
+        float t = __fadd_rn(__fmul_rn(ceilf(__fdiv_rn(__fsub_rn(t1, tnear), sd)), sd), tnear);
+        float pos[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(r.vz[k], __fmul_rn(r.vu[k], t));
+        // fminf drops a NaN extent; the t < tb test then ends the segment
+        const int cap = (int)fminf(ceilf(__fdiv_rn(tb - t, sd)) + 2.0f, (float)budget);
+        budget -= cap > 0 ? cap : 0;
+        int n = 0;
+        while (n < cap && t < tb) {
+            const float t2 = __fadd_rn(t, sd);
+            if (n + 1 < cap && t2 < tb) {
+                float q[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) q[k] = __fadd_rn(pos[k], d.step[k]);
+                visit2(pos, q);
+                t = __fadd_rn(t2, sd);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(q[k], d.step[k]);
+                n += 2;
+            } else {
+                visit(pos);
+                t = t2;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(pos[k], d.step[k]);
+                ++n;
+            }
+        }
+        march_split(d);
+        t1 = tb;
+    }
+}
+
 template <typename Visit>
 __device__ __forceinline__ void march(const GeomDev &g, const Ray &r, Visit &&visit) {
     const float sd = g.sd;
@@ -211,29 +363,12 @@ __device__ __forceinline__ void march(const GeomDev &g, const Ray &r, Visit &&vi
 #pragma unroll
     for (int k = 0; k < 3; ++k) pos1[k] = __fadd_rn(r.vz[k], __fmul_rn(r.vu[k], t1));
     visit(pos1);
-    const int dims[3] = {g.nx, g.ny, g.nz};
-    float tmax[3], tdelta[3], step[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        step[k] = __fmul_rn(r.vu[k], sd);
-        const int b = dims[k];
-        if (r.vu[k] == 0.0f) {
-            tmax[k] = tfar;
-            tdelta[k] = 0.0f;
-        } else if (r.vu[k] < 0.0f) {
-            int blk = ((int)ceilf(pos1[k] - 0.5f) - 1) / b;
-            tmax[k] = __fdiv_rn(__fsub_rn(__fadd_rn((float)(blk * b), 0.5f), r.vz[k]), r.vu[k]);
-            tdelta[k] = __fdiv_rn((float)(-b), r.vu[k]);
-        } else {
-            int blk = ((int)floorf(pos1[k] - 0.5f)) / b;
-            tmax[k] = __fdiv_rn(__fsub_rn(__fadd_rn((float)((blk + 1) * b), 0.5f), r.vz[k]), r.vu[k]);
-            tdelta[k] = __fdiv_rn((float)b, r.vu[k]);
-        }
-    }
+    MarchDda d;
+    march_dda(g, r, pos1, d);
     constexpr int kMaxSamples = 1 << 22;
     int budget = kMaxSamples;
     for (int seg = 0; seg < 16 && t1 < tfar && budget > 0; ++seg) {
-        float tb = rmin(rmin(tmax[0], tmax[1]), tmax[2]);
+        float tb = rmin(rmin(d.tmax[0], d.tmax[1]), d.tmax[2]);
         if (tb > tfar) tb = tfar;
         float t = __fadd_rn(__fmul_rn(ceilf(__fdiv_rn(__fsub_rn(t1, tnear), sd)), sd), tnear);
         float pos[3];
@@ -246,18 +381,84 @@ __device__ __forceinline__ void march(const GeomDev &g, const Ray &r, Visit &&vi
             visit(pos);
             t = __fadd_rn(t, sd);
 #pragma unroll
-            for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(pos[k], step[k]);
+            for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(pos[k], d.step[k]);
         }
-        if (tmax[0] < tmax[1]) {
-            if (tmax[0] < tmax[2]) tmax[0] += tdelta[0];
-            else tmax[2] += tdelta[2];
-        } else {
-            if (tmax[1] < tmax[2]) tmax[1] += tdelta[1];
-            else tmax[2] += tdelta[2];
-        }
+        march_split(d);
         t1 = tb;
     }
 }
+
+// march() as a resumable generator, for kernels that interleave the samples
+// of many rays with block-wide steps: peek() makes `pos` the next sample (false
+// when the ray is done), advance() moves past it.  The same samples in the
+// same order, from the same float operations: the entry sample, then each
+// segment restarted at ceil((t1 - tnear)/sd)*sd + tnear, with the same caps.
+struct MarchGen {
+    float vz[3], vu[3];
+    MarchDda d;
+    float pos[3];
+    float tnear, tfar, sd, t1, t, tb;
+    int seg, n, cap, budget;
+    int phase;  // 0: entry sample pending, 1: in a segment, 2: done
+
+    __device__ __forceinline__ void init(const GeomDev &g, const Ray &r) {
+        sd = g.sd;
+        tnear = r.tnear;
+        tfar = r.tfar;
+        t1 = tnear;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            vz[k] = r.vz[k];
+            vu[k] = r.vu[k];
+            pos[k] = __fadd_rn(vz[k], __fmul_rn(vu[k], t1));
+        }
+        march_dda(g, r, pos, d);
+        seg = 0;
+        budget = 1 << 22;
+        phase = 0;
+    }
+
+    __device__ __forceinline__ void start_segment() {
+        if (seg < 16 && t1 < tfar && budget > 0) {
+            tb = rmin(rmin(d.tmax[0], d.tmax[1]), d.tmax[2]);
+            if (tb > tfar) tb = tfar;
+            t = __fadd_rn(__fmul_rn(ceilf(__fdiv_rn(__fsub_rn(t1, tnear), sd)), sd), tnear);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(vz[k], __fmul_rn(vu[k], t));
+            cap = (int)fminf(ceilf(__fdiv_rn(tb - t, sd)) + 2.0f, (float)budget);
+            budget -= cap > 0 ? cap : 0;
+            n = 0;
+            phase = 1;
+        } else {
+            phase = 2;
+        }
+    }
+
+    __device__ __forceinline__ void end_segment() {
+        march_split(d);
+        t1 = tb;
+        ++seg;
+    }
+
+    __device__ __forceinline__ bool peek() {
+        while (phase == 1 && !(n < cap && t < tb)) {
+            end_segment();
+            start_segment();
+        }
+        return phase != 2;
+    }
+
+    __device__ __forceinline__ void advance() {
+        if (phase == 0) {  // the entry sample is done; segment 0 starts at tnear
+            start_segment();
+            return;
+        }
+        t = __fadd_rn(t, sd);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(pos[k], d.step[k]);
+        ++n;
+    }
+};
 
 // tld4 of the 2x2 texels {u, u+1} x {v, v+1} of one layer of a layered 2D
 // texture (coordinate (u+1, v+1), point sampling, clamp addressing):

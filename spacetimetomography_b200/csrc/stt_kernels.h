@@ -1,6 +1,7 @@
 // stt_kernels.h -- host-side launch wrappers of the kernels in k_*.cu.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace stt {
@@ -18,9 +19,28 @@ int grid_stride_blocks(long long n, int threads);
 
 cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, int view0,
                       int nviews, float *proj, float *raylen, float *weight, cudaStream_t s);
+// Slab-staged forward projector (k_fp_slab.cu) for the views marked `staged`:
+// the same outputs as the gather form bit for bit, the volume read through
+// TMA boxes.  The tensor maps cover the volume and its z-fastest copy (vol_t
+// may be null: then every view gathers from vol); make_fp_slab_maps returns
+// false where the form does not apply (x or z extent not a multiple of 4, an
+// array not 16-byte aligned, 2^31 voxels or more).  `status` (may be null) is
+// set to 1 if a box copy did not land within the wait limit.
+struct FpSlabMaps {
+    CUtensorMap x, z;
+    int ok, has_z;
+};
+bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m);
+cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const float *vol,
+                                const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state,
+                                float *corr, cudaStream_t s, unsigned long long corr_surf, int *status);
+// Forward projection of one view fused with the SART correction.  With usable
+// slab maps, staged views run in the slab-staged kernel and the others in the
+// gather kernel (both are launched; each leaves the other's views alone).
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
-                           cudaStream_t s, unsigned long long corr_surf = 0);
+                           cudaStream_t s, unsigned long long corr_surf = 0, const FpSlabMaps *maps = nullptr,
+                           int *status = nullptr);
 cudaError_t launch_transpose(const GeomDev &g, const float *in, float *out, cudaStream_t s);
 cudaError_t launch_fp_bf16(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
                            const unsigned short *vol_t, int view0, int nviews, float *proj, float *raylen,

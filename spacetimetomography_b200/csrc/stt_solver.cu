@@ -123,6 +123,7 @@ struct stt_solver {
     long long launches_per_iter = 0;
     long long phase_launches[2] = {0, 0};
     std::vector<LayeredTex> corr_tex;  // batched modes: per frame, the correction as a texture
+    std::vector<stt::FpSlabMaps> fpmaps;  // batched modes: per frame, TMA maps of the volume and its copy
     std::string err;
 };
 
@@ -239,9 +240,10 @@ stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long
         SCUDA(s, stt::launch_transpose_for_view(g, s->views, sel, vol, volt, cs), "transpose");
         const bool tex = voxel && !s->corr_tex.empty();
         SCUDA(s, stt::launch_fp_corr(g, s->views, vol, volt, sel, stack, voxel ? s->raylen + f * s->npix : nullptr,
-                                     corr, cs, tex ? s->corr_tex[f].surf : 0),
+                                     corr, cs, tex ? s->corr_tex[f].surf : 0,
+                                     s->fpmaps.empty() ? nullptr : &s->fpmaps[f]),
               "fp_corr");
-        ++nl;
+        nl += (!s->fpmaps.empty() && s->fpmaps[f].ok) ? 2 : 1;  // slab-staged + gather kernels, or gather only
         if (voxel)
             SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs,
                                           tex ? s->corr_tex[f].tex : 0),
@@ -429,6 +431,11 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     if (e) {
         stt_solver_destroy(s);
         return e;
+    }
+    if (cfg->mode != STT_SOLVE_PLAIN) {
+        s->fpmaps.resize(F);
+        for (int f = 0; f < F; ++f)  // where the maps do not apply, ok stays 0 and every view gathers
+            stt::make_fp_slab_maps(*g, s->st.vol + f * s->n, s->volt + f * s->n, s->fpmaps[f]);
     }
     if (cfg->mode != STT_SOLVE_PLAIN && cfg->bp_mode == 0) {
         s->corr_tex.resize(F);

@@ -1,0 +1,75 @@
+// stt_tma.cuh -- the Blackwell bulk-copy primitives the slab-staged projector
+// uses, as inline PTX: shared-memory mbarriers (init, arrive with an expected
+// transaction count, bounded parity wait) and the tiled TMA load of a 3D box
+// from a tensor map into this CTA's shared memory.  Loads only: no multicast,
+// no cluster, no peer memory.
+#pragma once
+
+#include <cuda.h>
+#include <stdint.h>
+
+namespace stt {
+namespace tma {
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// Makes the initialised barriers visible to the TMA unit.
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// One arrival that also announces `bytes` of incoming transactions.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n"
+        " .reg .pred p;\n"
+        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Waits for the phase with parity `parity` to complete, for at most about
+// `max_cycles` SM clocks; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long max_cycles) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > max_cycles) return false;
+    return true;
+}
+
+// TMA load of the box at coordinates (c0, c1, c2) (innermost first) of a 3D
+// tiled tensor map into `dst`; completion is signalled on `bar`.  c0 times the
+// element size must be a multiple of 16 bytes; coordinates outside the tensor
+// read as zero.
+__device__ __forceinline__ void load_box_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void prefetch_map(const CUtensorMap *map) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+}  // namespace tma
+}  // namespace stt
