@@ -5,6 +5,8 @@
 // voxel along x, blocks of 128 threads, grid (ceil(nx/128), ny, nz), so every
 // warp reads and writes 128 contiguous bytes per array.  The stencil
 // neighbours (x+-1, y+-1, z+-1) come from L1/L2.
+#include <climits>
+
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
 
@@ -36,35 +38,54 @@ struct Cut8 {
 // Voxel-based backprojection (ST_Tomography.cpp:690-730): project the voxel
 // centre, Catmull-Rom 4x4 gather of the correction image (y first, then x),
 // vol += alpha*val, clamp to [0, gmax]; voxels whose footprint leaves
-// [2, W-2) x [2, H-2) are untouched.  With TEX the 16 taps come from four
-// tld4 gathers of the correction's one-layer texture copy (one request per
-// 2x2 texels instead of one per texel); the values and the arithmetic are
-// the same.
+// [2, W-2) x [2, H-2) are untouched.  Every product and sum is rounded on its
+// own (explicit intrinsics), so the per-voxel and the column forms below give
+// the same bits.
+
+// Camera coordinate r of voxel (fx, fy, fz): A[r]*(x, y, z) + b[r].
+__device__ __forceinline__ float bp_cam(const ViewRec &v, int r, float fx, float fy, float fz) {
+    return __fadd_rn(__fmaf_rn(v.A[3 * r + 2], fz, __fmaf_rn(v.A[3 * r + 1], fy, __fmul_rn(v.A[3 * r], fx))), v.b[r]);
+}
+
+// Detector coordinate c + cam/(-depth) * sdd/ds.
+__device__ __forceinline__ float bp_pixel(float c, float cam, float ndepth, float sdd_ds) {
+    return __fmaf_rn(__fdiv_rn(cam, ndepth), sdd_ds, c);
+}
+
+// Catmull-Rom weights of taps (-1, 0, +1, +2) at fraction d.
+__device__ __forceinline__ void bp_weights(float d, float w[4]) {
+    const float d2 = __fmul_rn(d, d), d3 = __fmul_rn(d2, d);
+    w[0] = __fmul_rn(0.5f, __fsub_rn(__fmaf_rn(2.0f, d2, -d), d3));
+    w[1] = __fadd_rn(1.0f, __fmul_rn(0.5f, __fmaf_rn(3.0f, d3, __fmul_rn(-5.0f, d2))));
+    w[2] = __fmul_rn(0.5f, __fmaf_rn(-3.0f, d3, __fmaf_rn(4.0f, d2, d)));
+    w[3] = __fmul_rn(0.5f, __fsub_rn(d3, d2));
+}
+
+// sum_a wx[a] * sum_b wy[b] * tap[a][b]; tap[a][b] is column px-1+a, row py-1+b.
+__device__ __forceinline__ float bp_sum(const float tap[4][4], const float wx[4], const float wy[4]) {
+    float val = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const float s = __fmaf_rn(wy[3], tap[a][3],
+                                  __fmaf_rn(wy[2], tap[a][2], __fmaf_rn(wy[1], tap[a][1], __fmul_rn(wy[0], tap[a][0]))));
+        val = a == 0 ? __fmul_rn(wx[0], s) : __fmaf_rn(wx[a], s, val);
+    }
+    return val;
+}
+
+__device__ __forceinline__ void bp_update(float *__restrict__ vol, size_t o, float alpha, float val, float gmax) {
+    const float nv = __fmaf_rn(alpha, val, vol[o]);
+    vol[o] = rmax(rmin(gmax, nv), 0.0f);
+}
+
+// The 4x4 footprint at (px, py): four tld4 gathers of the correction's
+// one-layer texture copy (TEX), or sixteen loads.
 template <bool TEX>
-__global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec *__restrict__ views,
-                                                  const ViewSel sel, const float *__restrict__ corr,
-                                                  float *__restrict__ vol, float alpha, float gmax,
-                                                  unsigned long long corr_tex) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y, z = blockIdx.z;
-    if (x >= g.nx) return;
-    int local;
-    const ViewRec &v = views[sel_view(sel, local)];
-    const float fx = (float)x, fy = (float)y, fz = (float)z;
-    const float cxm = v.A[0] * fx + v.A[1] * fy + v.A[2] * fz + v.b[0];
-    const float cym = v.A[3] * fx + v.A[4] * fy + v.A[5] * fz + v.b[1];
-    const float czm = v.A[6] * fx + v.A[7] * fy + v.A[8] * fz + v.b[2];
-    const float upx = g.cx + __fdiv_rn(cxm, -czm) * g.sdd_ds;
-    const float upy = g.cy + __fdiv_rn(cym, -czm) * g.sdd_ds;
-    if (!(upx >= 2.0f && upx < (float)(g.W - 2) && upy >= 2.0f && upy < (float)(g.H - 2))) return;
-    const int px = (int)upx, py = (int)upy;
-    float wx[4], wy[4];
-    cr_weights(upx - (float)px, wx);
-    cr_weights(upy - (float)py, wy);
-    float tap[4][4];  // tap[a][b]: column px-1+a, row py-1+b
+__device__ __forceinline__ void bp_taps(const GeomDev &g, const float *__restrict__ corr, unsigned long long tex,
+                                        int px, int py, float tap[4][4]) {
     if (TEX) {
-        const float4 g00 = gather_layer(corr_tex, px - 1, py - 1, 0), g10 = gather_layer(corr_tex, px + 1, py - 1, 0);
-        const float4 g01 = gather_layer(corr_tex, px - 1, py + 1, 0), g11 = gather_layer(corr_tex, px + 1, py + 1, 0);
+        const float4 g00 = gather_layer(tex, px - 1, py - 1, 0), g10 = gather_layer(tex, px + 1, py - 1, 0);
+        const float4 g01 = gather_layer(tex, px - 1, py + 1, 0), g11 = gather_layer(tex, px + 1, py + 1, 0);
         tap[0][0] = g00.w, tap[0][1] = g00.x, tap[0][2] = g01.w, tap[0][3] = g01.x;
         tap[1][0] = g00.z, tap[1][1] = g00.y, tap[1][2] = g01.z, tap[1][3] = g01.y;
         tap[2][0] = g10.w, tap[2][1] = g10.x, tap[2][2] = g11.w, tap[2][3] = g11.x;
@@ -76,15 +97,99 @@ __global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec
 #pragma unroll
             for (int b = 0; b < 4; ++b) tap[a][b] = __ldg(c0 + a + b * g.W);
     }
-    float val = 0.0f;
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        float s = wy[0] * tap[a][0] + wy[1] * tap[a][1] + wy[2] * tap[a][2] + wy[3] * tap[a][3];
-        val += wx[a] * s;
+}
+
+// One voxel, everything computed for it alone.
+template <bool TEX>
+__device__ __forceinline__ void bp_voxel_at(const GeomDev &g, const ViewRec &v, const float *__restrict__ corr,
+                                            unsigned long long tex, float *__restrict__ vol, int x, int y, int z,
+                                            float alpha, float gmax) {
+    const float fx = (float)x, fy = (float)y, fz = (float)z;
+    const float ndepth = -bp_cam(v, 2, fx, fy, fz);
+    const float upx = bp_pixel(g.cx, bp_cam(v, 0, fx, fy, fz), ndepth, g.sdd_ds);
+    const float upy = bp_pixel(g.cy, bp_cam(v, 1, fx, fy, fz), ndepth, g.sdd_ds);
+    if (!(upx >= 2.0f && upx < (float)(g.W - 2) && upy >= 2.0f && upy < (float)(g.H - 2))) return;
+    const int px = (int)upx, py = (int)upy;
+    float wx[4], wy[4], tap[4][4];
+    bp_weights(upx - (float)px, wx);
+    bp_weights(upy - (float)py, wy);
+    bp_taps<TEX>(g, corr, tex, px, py, tap);
+    bp_update(vol, x + (size_t)y * g.nx + (size_t)z * g.nx * g.ny, alpha, bp_sum(tap, wx, wy), gmax);
+}
+
+template <bool TEX>
+__global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec *__restrict__ views,
+                                                  const ViewSel sel, const float *__restrict__ corr,
+                                                  float *__restrict__ vol, float alpha, float gmax,
+                                                  unsigned long long corr_tex) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= g.nx) return;
+    int local;
+    const ViewRec &v = views[sel_view(sel, local)];
+    bp_voxel_at<TEX>(g, v, corr, corr_tex, vol, x, blockIdx.y, blockIdx.z, alpha, gmax);
+}
+
+// Column form, texture taps: one thread per (x, z) walks K voxels up y.  For
+// a view whose matrix has A[1] == A[7] == 0 (every rotation about y) the
+// voxel's detector column and depth do not depend on y: they are computed
+// once (the y term of their sums is an exact zero, so the values are the
+// per-voxel ones).  The detector row moves by about sdd/sid per voxel, and
+// the 4x4 window's rows are kept in registers: a step of s = 0, 1 or 2 rows
+// reuses two of them and gathers the two new ones (2 tld4 instead of 4).
+constexpr int BP_COL = 16;
+
+__global__ void __launch_bounds__(128) k_bp_voxel_cols(const GeomDev g, const ViewRec *__restrict__ views,
+                                                       const ViewSel sel, float *__restrict__ vol, float alpha,
+                                                       float gmax, unsigned long long tex) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y0 = blockIdx.y * BP_COL, z = blockIdx.z;
+    if (x >= g.nx) return;
+    int local;
+    const ViewRec &v = views[sel_view(sel, local)];
+    const int y1 = min(y0 + BP_COL, g.ny);
+    if (!(v.A[1] == 0.0f && v.A[7] == 0.0f)) {
+        for (int y = y0; y < y1; ++y) bp_voxel_at<true>(g, v, nullptr, tex, vol, x, y, z, alpha, gmax);
+        return;
     }
-    const size_t o = x + (size_t)y * g.nx + (size_t)z * g.nx * g.ny;
-    float nv = vol[o] + alpha * val;
-    vol[o] = rmax(rmin(gmax, nv), 0.0f);
+    const float fx = (float)x, fz = (float)z;
+    const float ndepth = -bp_cam(v, 2, fx, (float)y0, fz);
+    const float upx = bp_pixel(g.cx, bp_cam(v, 0, fx, (float)y0, fz), ndepth, g.sdd_ds);
+    if (!(upx >= 2.0f && upx < (float)(g.W - 2))) return;
+    const int px = (int)upx;
+    float wx[4];
+    bp_weights(upx - (float)px, wx);
+    float R[4][4];  // R[a][b]: column px-1+a, row pyc-1+b
+    int pyc = INT_MIN / 2;
+    for (int y = y0; y < y1; ++y) {
+        const float upy = bp_pixel(g.cy, bp_cam(v, 1, fx, (float)y, fz), ndepth, g.sdd_ds);
+        if (!(upy >= 2.0f && upy < (float)(g.H - 2))) continue;
+        const int py = (int)upy;
+        float wy[4];
+        bp_weights(upy - (float)py, wy);
+        const int s = py - pyc;
+        float r0[4], r1[4];  // rows py-1, py
+        if (s >= 0 && s <= 2) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                r0[a] = s == 0 ? R[a][0] : (s == 1 ? R[a][1] : R[a][2]);
+                r1[a] = s == 0 ? R[a][1] : (s == 1 ? R[a][2] : R[a][3]);
+            }
+        } else {
+            const float4 gc = gather_layer(tex, px - 1, py - 1, 0), gd = gather_layer(tex, px + 1, py - 1, 0);
+            r0[0] = gc.w, r0[1] = gc.z, r0[2] = gd.w, r0[3] = gd.z;
+            r1[0] = gc.x, r1[1] = gc.y, r1[2] = gd.x, r1[3] = gd.y;
+        }
+        const float4 ga = gather_layer(tex, px - 1, py + 1, 0), gb = gather_layer(tex, px + 1, py + 1, 0);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            R[a][0] = r0[a];
+            R[a][1] = r1[a];
+        }
+        R[0][2] = ga.w, R[1][2] = ga.z, R[2][2] = gb.w, R[3][2] = gb.z;  // row py+1
+        R[0][3] = ga.x, R[1][3] = ga.y, R[2][3] = gb.x, R[3][3] = gb.y;  // row py+2
+        pyc = py;
+        bp_update(vol, x + (size_t)y * g.nx + (size_t)z * g.nx * g.ny, alpha, bp_sum(R, wx, wy), gmax);
+    }
 }
 
 // Dual step of one frame (ST_Tomography.cpp:504-534), fused:
@@ -261,7 +366,8 @@ cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, c
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                             float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex) {
     if (corr_tex)
-        k_bp_voxel<true><<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, sel, corr, vol, alpha, gmax, corr_tex);
+        k_bp_voxel_cols<<<dim3((g.nx + 127) / 128, (g.ny + BP_COL - 1) / BP_COL, g.nz), 128, 0, s>>>(
+            g, views, sel, vol, alpha, gmax, corr_tex);
     else
         k_bp_voxel<false><<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, sel, corr, vol, alpha, gmax, 0);
     return cudaGetLastError();
