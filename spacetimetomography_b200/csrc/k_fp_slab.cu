@@ -35,7 +35,7 @@ constexpr int BOXN = FB * YB * SB;
 constexpr unsigned BOX_BYTES = BOXN * sizeof(float);
 constexpr int SLAB = SB - 1;                     // base planes per slab; the box also holds their +1 plane
 constexpr long long WAIT_CYCLES = 200000000LL;  // about 0.1 s: a copy that never lands is an error
-constexpr int WARPS = 4;                         // 128-thread blocks
+constexpr int WARPS = 4;                         // a block is 32 x WARPS detector pixels, one warp per row
 
 __device__ __forceinline__ int warp_min(int v) { return __reduce_min_sync(0xffffffffu, v); }
 
@@ -176,11 +176,12 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
         }
         const float *bx = buf + (k & 1) * BOXN;
         const int m0 = slab_m0(k);
-        while (m.peek()) {
+        // one sample: false (and nothing added) when it belongs to a later slab
+        auto take = [&](const float p[3]) -> bool {
             FpCell c;
-            fp_cell(g, m.pos, c);
+            fp_cell(g, p, c);
             const int bs = ZF ? c.ix : c.iz;
-            if (fwd ? bs > m0 + SLAB - 1 : bs < m0) break;  // belongs to a later slab
+            if (fwd ? bs > m0 + SLAB - 1 : bs < m0) return false;
             const unsigned of = (unsigned)((ZF ? c.iz : c.ix) - f0), oy = (unsigned)(c.iy - y0),
                            os = (unsigned)(bs - m0);
             float v[8];
@@ -197,7 +198,32 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
                 fp_corners<ZF ? 2 : 0, int>(src, st, c, v);
             }
             acc.add(__fmul_rn(trilerp(v, c), g.sd));
-            m.advance();
+            return true;
+        };
+        bool later = false;
+        while (!later && m.peek()) {
+            if (m.phase == 0) {  // the entry sample
+                later = !take(m.pos);
+                if (!later) m.advance();
+                continue;
+            }
+            // the rest of the current segment, from registers
+            float t = m.t, p[3] = {m.pos[0], m.pos[1], m.pos[2]};
+            int n = m.n;
+            do {
+                if (!take(p)) {
+                    later = true;
+                    break;
+                }
+                t = __fadd_rn(t, m.sd);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) p[a] = __fadd_rn(p[a], m.d.step[a]);
+                ++n;
+            } while (n < m.cap && t < m.tb);
+            m.t = t;
+            m.n = n;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) m.pos[a] = p[a];
         }
         __syncthreads();  // every ray is done with buffer k&1 before slab k+2 is loaded into it
         gave_up = *dead != 0;
@@ -218,7 +244,7 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
 // k_fp_corr (GenerateImage_MT + the correction of ST_Tomography.cpp:667-676)
 // with slab-staged gathers.  map_x covers `vol` (x-fastest), map_z `vol_t`
 // (z-fastest), both with the box FB x YB x SB.
-__global__ void __launch_bounds__(128) k_fp_corr_slab(const GeomDev g, const ViewRec *__restrict__ views,
+__global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, const ViewRec *__restrict__ views,
                                                       const __grid_constant__ CUtensorMap map_x,
                                                       const __grid_constant__ CUtensorMap map_z,
                                                       const float *__restrict__ vol, const float *__restrict__ vol_t,
@@ -231,7 +257,7 @@ __global__ void __launch_bounds__(128) k_fp_corr_slab(const GeomDev g, const Vie
     __shared__ int red_s[3 * WARPS];
     __shared__ int dead;
     const int i = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int j = blockIdx.y * 4 + (threadIdx.x >> 5);
+    const int j = blockIdx.y * WARPS + (threadIdx.x >> 5);
     const bool valid = i < g.W && j < g.H;
     int local;
     const int view = sel_view(sel, local);
@@ -313,7 +339,7 @@ cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const Fp
         return true;
     }();
     (void)carve;
-    k_fp_corr_slab<<<dim3((g.W + 31) / 32, (g.H + 3) / 4, 1), 128, 0, s>>>(g, views, m.x, m.z, vol, vol_t, sel, b_stack,
+    k_fp_corr_slab<<<dim3((g.W + 31) / 32, (g.H + WARPS - 1) / WARPS, 1), 32 * WARPS, 0, s>>>(g, views, m.x, m.z, vol, vol_t, sel, b_stack,
                                                                           raylen_state, corr, corr_surf, status);
     return cudaGetLastError();
 }

@@ -26,14 +26,16 @@ __device__ __forceinline__ bool tile_pixel(const GeomDev &g, int &i, int &j) {
 
 // The ray sum of one forward-projector ray (hit rays only), gathered from the
 // z-fastest transposed copy for layout-1 views when one is given, else from
-// the volume.  Samples go two at a time where the march allows: both
-// samples' 16 taps are loaded before either is interpolated.
+// the volume.  Samples go FP_GROUP at a time where the march allows: all
+// their taps are loaded before any is interpolated.
+constexpr int FP_GROUP = 4;
+
 template <int FAST, typename I, typename T>
 __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__restrict__ src, const Strides &st,
                                                  const Ray &r, int *count) {
     Kahan acc{0.0f, 0.0f};
     int n = 0;
-    march_pairs(
+    march_groups<FP_GROUP>(
         g, r,
         [&](const float p[3]) {
             FpCell c;
@@ -43,16 +45,17 @@ __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__re
             acc.add(__fmul_rn(trilerp(v, c), g.sd));
             ++n;
         },
-        [&](const float p[3], const float q[3]) {
-            FpCell c, e;
-            fp_cell(g, p, c);
-            fp_cell(g, q, e);
-            float v[8], w[8];
-            fp_corners<FAST, I>(src, st, c, v);
-            fp_corners<FAST, I>(src, st, e, w);
-            acc.add(__fmul_rn(trilerp(v, c), g.sd));
-            acc.add(__fmul_rn(trilerp(w, e), g.sd));
-            n += 2;
+        [&](const float (*p)[3]) {
+            FpCell c[FP_GROUP];
+            float v[FP_GROUP][8];
+#pragma unroll
+            for (int i = 0; i < FP_GROUP; ++i) {
+                fp_cell(g, p[i], c[i]);
+                fp_corners<FAST, I>(src, st, c[i], v[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < FP_GROUP; ++i) acc.add(__fmul_rn(trilerp(v[i], c[i]), g.sd));
+            n += FP_GROUP;
         });
     if (count) *count = n;
     return acc.s;

@@ -301,13 +301,14 @@ __device__ __forceinline__ void march_split(MarchDda &d) {
     }
 }
 
-// The march, handing the samples of a segment out two at a time where two
-// remain: visit2(p, q) gets consecutive samples p, q (in that order), visit(p)
-// the entry sample and a segment's odd last one.  The samples and their order
-// are those of march(); a caller that issues both samples' loads before using
-// either keeps twice the loads in flight.
-template <typename Visit, typename Visit2>
-__device__ __forceinline__ void march_pairs(const GeomDev &g, const Ray &r, Visit &&visit, Visit2 &&visit2) {
+// The march, handing the samples of a segment out G at a time where G
+// remain: visitg(p) gets consecutive samples p[0..G) (in that order), visit(p)
+// the entry sample and the last ones of a segment.  The samples and their
+// order are those of march() (t only grows, so the G-th sample inside the
+// segment implies the ones before it); a caller that issues all G samples'
+// loads before using any keeps G times the loads in flight.
+template <int G, typename Visit, typename VisitG>
+__device__ __forceinline__ void march_groups(const GeomDev &g, const Ray &r, Visit &&visit, VisitG &&visitg) {
     const float sd = g.sd;
     const float tnear = r.tnear, tfar = r.tfar;
     float t1 = tnear;
@@ -331,19 +332,25 @@ __device__ __forceinline__ void march_pairs(const GeomDev &g, const Ray &r, Visi
         budget -= cap > 0 ? cap : 0;
         int n = 0;
         while (n < cap && t < tb) {
-            const float t2 = __fadd_rn(t, sd);
-            if (n + 1 < cap && t2 < tb) {
-                float q[3];
+            float tl = t;  // time of the group's last sample
 #pragma unroll
-                for (int k = 0; k < 3; ++k) q[k] = __fadd_rn(pos[k], d.step[k]);
-                visit2(pos, q);
-                t = __fadd_rn(t2, sd);
+            for (int i = 1; i < G; ++i) tl = __fadd_rn(tl, sd);
+            if (n + G - 1 < cap && tl < tb) {
+                float p[G][3];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(q[k], d.step[k]);
-                n += 2;
+                for (int k = 0; k < 3; ++k) p[0][k] = pos[k];
+#pragma unroll
+                for (int i = 1; i < G; ++i)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) p[i][k] = __fadd_rn(p[i - 1][k], d.step[k]);
+                visitg(p);
+                t = __fadd_rn(tl, sd);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(p[G - 1][k], d.step[k]);
+                n += G;
             } else {
                 visit(pos);
-                t = t2;
+                t = __fadd_rn(t, sd);
 #pragma unroll
                 for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(pos[k], d.step[k]);
                 ++n;
