@@ -138,7 +138,11 @@ __global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec
 // reuses two of them and gathers the two new ones (2 tld4 instead of 4).
 constexpr int BP_COL = 16;
 
-__global__ void __launch_bounds__(128) k_bp_voxel_cols(const GeomDev g, const ViewRec *__restrict__ views,
+// Ten 128-thread blocks per SM (48 registers, no spills): the walk is bound
+// by texture latency, so the extra warps pay (10 blocks: 104.1 ms per
+// iteration of the 10 x 256^3 solve against 106.6 ms with the compiler's
+// 52 registers and 9 blocks).
+__global__ void __launch_bounds__(128, 10) k_bp_voxel_cols(const GeomDev g, const ViewRec *__restrict__ views,
                                                        const ViewSel sel, float *__restrict__ vol, float alpha,
                                                        float gmax, unsigned long long tex) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
