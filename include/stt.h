@@ -115,7 +115,10 @@ stt_status stt_fp_typed(stt_ctx *ctx, const void *vol, int dtype, float *proj, f
 
 /* Forward projection of one view fused with the SART correction
  * (ST_Tomography.cpp:667-676): corr = (b - Ax) / (L + 1), where L is the
- * sticky ray-length state (W*H, updated where the ray hits). */
+ * sticky ray-length state (W*H, updated where the ray hits).  Views whose
+ * central ray is more than 25 degrees off both x and z are projected with the
+ * volume staged into shared memory by TMA when nx and nz are multiples of 4
+ * and vol is 16-byte aligned; the result is the same bits either way. */
 stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, float *raylen_state,
                              float *corr, int view, void *stream);
 
