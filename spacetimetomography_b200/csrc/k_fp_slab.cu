@@ -318,6 +318,20 @@ bool encode_box_map(CUtensorMap *m, const float *ptr, int fast, int mid, int slo
 
 }  // namespace
 
+bool encode_planes_map(CUtensorMap *m, const float *ptr, int nx, int ny, int nz, int nc, const unsigned box[4]) {
+    const PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn || !ptr || (reinterpret_cast<uintptr_t>(ptr) & 15) || (nx & 3) || ((box[0] * sizeof(float)) & 15))
+        return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nc};
+    const cuuint64_t row = (cuuint64_t)nx * sizeof(float);
+    const cuuint64_t strides[3] = {row, row * ny, row * ny * nz};
+    const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(ptr), dims, strides, bx, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m) {
     m = FpSlabMaps{};
     if ((long long)g.nx * g.ny * g.nz >= (1LL << 31)) return false;  // 32-bit fallback offsets

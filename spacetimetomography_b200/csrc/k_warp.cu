@@ -9,8 +9,11 @@
 // L1/L2 through the read-only path; the cell corners of the clamp are taps of
 // the stencil, so a sample is at most 64 loads per channel.  The kernel is
 // bound by L1 load wavefronts, not by HBM.
+#include <climits>
+
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
+#include "stt_tma.cuh"
 #include "warp_dev.cuh"
 
 namespace stt {
@@ -48,6 +51,108 @@ __global__ void __launch_bounds__(WARP_BX *WARP_BY) k_warp(const Dim3i d, const 
     cell_setup(d, g2, s2);
     float v2[3];
     sample_cell<3>(vel, n, s2, v2);
+    float q[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float p0 = __fsub_rn(p2[a], __fmul_rn(h, v2[a]));
+        q[a] = __fadd_rn(p2[a], __fmul_rn(0.5f, __fsub_rn(p[a], p0)));
+    }
+    const float gq[3] = {to_grid(q[0], d.x, nullptr), to_grid(q[1], d.y, nullptr), to_grid(q[2], d.z, nullptr)};
+    Cell s;
+    cell_setup(d, gq, s);
+    const int o = i + j * d.x + k * d.x * d.y;
+    for (int ch = 0; ch < nc; ++ch) {
+        float v[1];
+        sample_cell<1>(src + (size_t)ch * n, 0, s, v);
+        out[o + (size_t)ch * n] = v[0];
+    }
+}
+
+// Staged form: the three velocity planes around the block's half-traced
+// points come into shared memory with one 4D TMA box, and the velocity sample
+// (three quarters of the warp's taps) reads them there.  Each thread finds the
+// first tap of its velocity stencil after the exact centre read; the block's
+// minimum places the box (x rounded down to 16 bytes); a stencil that does not
+// fit in the box (a rough flow, a copy that did not land within the bounded
+// wait) reads global memory.  The taps and the arithmetic are those of k_warp,
+// so the outputs are the same bits.  The source sample stays on the L1 path.
+constexpr int VX = 40, VY = 10, VZ = 6;  // velocity box (x, y, z) per plane; VX*4 is a multiple of 16
+constexpr int VBOX = VX * VY * VZ;
+constexpr long long WARP_WAIT_CYCLES = 200000000LL;  // about 0.1 s
+
+__global__ void __launch_bounds__(WARP_BX *WARP_BY) k_warp_staged(const Dim3i d,
+                                                                  const __grid_constant__ CUtensorMap vmap,
+                                                                  const float *__restrict__ vel,
+                                                                  const float *__restrict__ src, int nc, float dt,
+                                                                  float *__restrict__ out) {
+    __shared__ alignas(128) float vbox[3 * VBOX];
+    __shared__ uint64_t bar;
+    __shared__ int red[3 * WARP_BY];
+    const int i = blockIdx.x * WARP_BX + threadIdx.x;
+    const int j = blockIdx.y * WARP_BY + threadIdx.y, k = blockIdx.z;
+    const bool live = i < d.x && j < d.y;
+    const int n = d.x * d.y * d.z;
+    const float h = -dt;
+    const float p[3] = {(float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f};
+    float p2[3] = {0.0f, 0.0f, 0.0f}, g2[3] = {1.0f, 1.0f, 1.0f};
+    int b0[3] = {INT_MAX, INT_MAX, INT_MAX};  // first tap of the velocity stencil
+    if (live) {
+        // cell centre (warping.h:25-29); the velocity there is an exact node read
+        const int ci = min(max(i, 1), d.x - 2), cj = min(max(j, 1), d.y - 2), ck = min(max(k, 1), d.z - 2);
+        const int c = ci + cj * d.x + ck * d.x * d.y;
+        const float v1[3] = {__ldg(vel + c), __ldg(vel + n + c), __ldg(vel + 2 * n + c)};
+        // trace (warping.h:100-114): p2 = p + h v(p); p0 = p2 - h v(p2); q = p2 + (p - p0)/2
+#pragma unroll
+        for (int a = 0; a < 3; ++a) p2[a] = __fadd_rn(p[a], __fmul_rn(h, v1[a]));
+        g2[0] = to_grid(p2[0], d.x, nullptr);
+        g2[1] = to_grid(p2[1], d.y, nullptr);
+        g2[2] = to_grid(p2[2], d.z, nullptr);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) b0[a] = (int)g2[a] - 1;
+    }
+    int m[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) m[a] = __reduce_min_sync(0xffffffffu, b0[a]);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) red[3 * threadIdx.y + a] = m[a];
+    }
+    const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+    if (lead) {
+        tma::mbar_init(&bar, 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        m[a] = red[a];
+#pragma unroll
+        for (int w = 1; w < WARP_BY; ++w) m[a] = min(m[a], red[3 * w + a]);
+    }
+    const bool any = m[0] != INT_MAX;  // uniform: some voxel of the block is inside the volume
+    const int ox = (m[0] >> 2) << 2, oy = m[1], oz = m[2];
+    if (any && lead) {
+        tma::mbar_arrive_expect_tx(&bar, 3u * VBOX * sizeof(float));
+        tma::load_box_4d(vbox, &vmap, ox, oy, oz, 0, &bar);
+    }
+    bool staged = false;
+    if (any) staged = tma::mbar_wait(&bar, 0, WARP_WAIT_CYCLES);
+    if (!live) return;
+    Cell s2;
+    cell_setup(d, g2, s2);
+    float v2[3];
+    const unsigned lx = (unsigned)(b0[0] - ox), ly = (unsigned)(b0[1] - oy), lz = (unsigned)(b0[2] - oz);
+    if (staged && lx <= VX - 4 && ly <= VY - 4 && lz <= VZ - 4) {
+        Cell sl = s2;  // the same weights and edge flags, box-local offsets
+        sl.sy = VX;
+        sl.sz = VX * VY;
+        sl.x.lo = (int)lx;
+        sl.y.lo = (int)ly * VX;
+        sl.z.lo = (int)lz * VX * VY;
+        sample_cell<3, true>(vbox, VBOX, sl, v2);
+    } else {
+        sample_cell<3>(vel, n, s2, v2);
+    }
     float q[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -214,8 +319,13 @@ __global__ void __launch_bounds__(128) k_warp_vjp(const Dim3i d, const float *__
 cudaError_t launch_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
                         float *out, cudaStream_t s) {
     Dim3i d{dim[0], dim[1], dim[2]};
-    k_warp<<<dim3((d.x + WARP_BX - 1) / WARP_BX, (d.y + WARP_BY - 1) / WARP_BY, d.z), dim3(WARP_BX, WARP_BY), 0,
-             s>>>(d, vel, src, nc, dt, out);
+    const dim3 grid((d.x + WARP_BX - 1) / WARP_BX, (d.y + WARP_BY - 1) / WARP_BY, d.z), block(WARP_BX, WARP_BY);
+    CUtensorMap vmap;
+    const unsigned box[4] = {VX, VY, VZ, 3};
+    if (encode_planes_map(&vmap, vel, d.x, d.y, d.z, 3, box))
+        k_warp_staged<<<grid, block, 0, s>>>(d, vmap, vel, src, nc, dt, out);
+    else
+        k_warp<<<grid, block, 0, s>>>(d, vel, src, nc, dt, out);
     return cudaGetLastError();
 }
 

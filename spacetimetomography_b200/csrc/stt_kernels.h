@@ -31,6 +31,10 @@ struct FpSlabMaps {
     int ok, has_z;
 };
 bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m);
+// A 4D FP32 tensor map over nc planar volumes (x fastest, then y, z, plane)
+// with the given box (x, y, z, plane); false where TMA cannot address them
+// (nx not a multiple of 4, ptr not 16-byte aligned, box row not 16 bytes).
+bool encode_planes_map(CUtensorMap *m, const float *ptr, int nx, int ny, int nz, int nc, const unsigned box[4]);
 cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const float *vol,
                                 const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state,
                                 float *corr, cudaStream_t s, unsigned long long corr_surf, int *status);

@@ -127,12 +127,20 @@ __device__ __forceinline__ void cell_setup(const Dim3i d, const float g[3], Cell
     axis_setup(g[2], c.sz, d.z, c.z);
 }
 
+// A tap: read-only global load, or a plain load when SHARED (img then points
+// into shared memory, which the global read-only path cannot address).
+template <bool SHARED>
+__device__ __forceinline__ float ld_tap(const float *p) {
+    if (SHARED) return *p;
+    return __ldg(p);
+}
+
 // sample_image (warping.h:49-88) of NC planes that share one cell: the
 // Catmull-Rom value of each, clamped to the min/max of its 8 cell corners.
 // Plane p starts at img + p * pstride.  The sums run in the order of
 // sample_clamped above (x taps, then rows, then planes), so both give the
 // same bits.
-template <int NC>
+template <int NC, bool SHARED = false>
 __device__ __forceinline__ void sample_cell(const float *__restrict__ img, int pstride, const Cell &s,
                                             float out[NC]) {
     float val[NC], mn[NC], mx[NC];
@@ -155,8 +163,8 @@ __device__ __forceinline__ void sample_cell(const float *__restrict__ img, int p
 #pragma unroll
             for (int p = 0; p < NC; ++p) {
                 const float *r = img + p * pstride + row;
-                const float t0 = __ldg(r), t1 = __ldg(r + 1), t2 = __ldg(r + 2);
-                const float t3 = s.x.t3 ? __ldg(r + 3) : 0.0f;
+                const float t0 = ld_tap<SHARED>(r), t1 = ld_tap<SHARED>(r + 1), t2 = ld_tap<SHARED>(r + 2);
+                const float t3 = s.x.t3 ? ld_tap<SHARED>(r + 3) : 0.0f;
                 const float xv = s.x.w[0] * t0 + s.x.w[1] * t1 + s.x.w[2] * t2 + s.x.w[3] * t3;
                 yv[p] += s.y.w[b] * xv;
                 if ((b == 1 || b == 2) && (c == 1 || c == 2)) {
