@@ -555,35 +555,86 @@ def run_stt(args):
         sp.close()
 
     # ---- end to end through the C ABI with host buffers ----
+    # Every step uploads its inputs (volume, flow, projections) from pinned
+    # host memory and reads its result back.  On one GPU the steps alternate
+    # between two state sets and two solvers, so step i+1's upload and step
+    # i-1's read-back run on copy streams while step i computes; every copy is
+    # still inside the timed region.
     host = {k: st[k].detach().cpu().pin_memory() for k in ("vol", "flow", "proj")}
-    out_host = torch.empty_like(st["vol"][:F], device="cpu").pin_memory()
     h2d = sum(v.numel() * 4 for v in host.values())
-    d2h = out_host.numel() * 4
-
-    def e2e_step():
-        with torch.cuda.stream(stream):
-            for k_, v_ in host.items():
-                st[k_].copy_(v_, non_blocking=True)
-            st["xbar"].copy_(st["vol"])
-            for k_ in ("ytv", "ytp", "ybc"):
-                st[k_].zero_()
-        step(solver)
-        with torch.cuda.stream(stream):
-            out_host.copy_(st["vol"][:F], non_blocking=True)
-
-    e2e_step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    d2h = st["vol"][:F].numel() * 4
     ksteps = max(1, min(args.steps, 3))
-    q0.record(stream)
-    for _ in range(ksteps):
+
+    def reset_duals(s_):
+        s_["xbar"].copy_(s_["vol"])
+        for k_ in ("ytv", "ytp", "ybc"):
+            s_[k_].zero_()
+
+    if world == 1:
+        st2 = {k: torch.zeros_like(v) for k, v in st.items()}
+        solver2 = stt.Solver(ctx, st2, F, V, pd, alpha=0.3, bp_mode=bp_mode, seed=99, mode=stt.SOLVE_GRAPH)
+        sets = [(st, solver), (st2, solver2)]
+        outs = [torch.empty_like(st["vol"][:F], device="cpu").pin_memory() for _ in range(2)]
+        up, down = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+        ev = {k: [torch.cuda.Event() for _ in range(2)] for k in ("free", "uploaded", "computed")}
+        for b in range(2):
+            ev["free"][b].record(down)
+
+        def e2e_step_pipe(i):
+            b = i % 2
+            s_, sol = sets[b]
+            up.wait_event(ev["free"][b])
+            with torch.cuda.stream(up):
+                for k_, v_ in host.items():
+                    s_[k_].copy_(v_, non_blocking=True)
+            ev["uploaded"][b].record(up)
+            stream.wait_event(ev["uploaded"][b])
+            with torch.cuda.stream(stream):
+                reset_duals(s_)
+            sol.iterate(1, stream)
+            ev["computed"][b].record(stream)
+            down.wait_event(ev["computed"][b])
+            with torch.cuda.stream(down):
+                outs[b].copy_(s_["vol"][:F], non_blocking=True)
+            ev["free"][b].record(down)
+
+        for i in range(2):  # untimed: the second solver's graph is captured here
+            e2e_step_pipe(i)
+        torch.cuda.synchronize()
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ksteps = max(1, args.steps)  # the pipeline's fill and drain are inside the timed region
+        q0.record(up)
+        for i in range(ksteps):
+            e2e_step_pipe(i)
+        up.wait_stream(down)
+        up.wait_stream(stream)
+        q1.record(up)
+        torch.cuda.synchronize()
+        te = q0.elapsed_time(q1) / 1000.0
+        solver2.close()
+        del st2
+    else:
+        out_host = torch.empty_like(st["vol"][:F], device="cpu").pin_memory()
+
+        def e2e_step():
+            with torch.cuda.stream(stream):
+                for k_, v_ in host.items():
+                    st[k_].copy_(v_, non_blocking=True)
+                reset_duals(st)
+            step(solver)
+            with torch.cuda.stream(stream):
+                out_host.copy_(st["vol"][:F], non_blocking=True)
+
         e2e_step()
-    q1.record(stream)
-    torch.cuda.synchronize()
-    te = q0.elapsed_time(q1) / 1000.0
-    if world > 1:
+        torch.cuda.synchronize()
+        dist.barrier()
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        for _ in range(ksteps):
+            e2e_step()
+        q1.record(stream)
+        torch.cuda.synchronize()
+        te = q0.elapsed_time(q1) / 1000.0
         tt = torch.tensor([te], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         te = float(tt.item())
