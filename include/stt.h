@@ -77,6 +77,22 @@ const char *stt_last_error(const stt_ctx *ctx);
 /* Library version string, e.g. "stt 0.1.0 sm_100a". */
 const char *stt_version(void);
 
+/* Bounded device-side waits.  No counterpart in the reference (CPU code, no
+ * device waits).  The TMA-staged kernels (the slab forward projector of
+ * stt_fp_correction / stt_sart_sweep / the solver, the staged warp) wait for
+ * their shared-memory copies for at most about 0.1 s.  A copy that does not
+ * land in time is an error: the kernel takes those taps from global memory
+ * instead (the same result), waits once more, again bounded, so that no block
+ * exits with a copy still writing into its shared memory, and raises a status
+ * flag.  stt_poll_status synchronises `stream` and returns STT_ERR_TIMEOUT
+ * (message in stt_last_error) if a launch of this context raised the flag
+ * since the last poll, clearing it; otherwise STT_OK.  stt_solver_poll_status
+ * and stt_batch_poll_status do the same for a solver or a batch, and
+ * stt_warp_poll_status for stt_warp / stt_warp_box calls on the current
+ * device. */
+stt_status stt_poll_status(stt_ctx *ctx, void *stream);
+stt_status stt_warp_poll_status(void *stream);
+
 /* Host helper: angles (radians) of the reference's view list.  Round r of
  * `rounds` starts at start_deg[r] (host); views k = 0..views_per_round-1 sit
  * step_deg apart; angles_out (host) receives rounds*views_per_round values.
@@ -371,6 +387,8 @@ stt_status stt_solver_iterate_phase(stt_solver *s, int phase, void *stream);
 stt_status stt_solver_stats(const stt_solver *s, long long *launches_per_iter,
                             unsigned long long *iterations);
 const char *stt_solver_last_error(const stt_solver *s);
+/* See stt_poll_status. */
+stt_status stt_solver_poll_status(stt_solver *s, void *stream);
 stt_status stt_solver_destroy(stt_solver *s);
 /* Host copy of the view order frame `frame` uses in iteration `iter` (HOST perm_out). */
 stt_status stt_solver_frame_order(unsigned long long seed, unsigned long long iter, int n_frames,
@@ -402,6 +420,8 @@ typedef struct stt_batch stt_batch;
 stt_status stt_batch_create(const stt_instance *instances, int n, int mode, stt_batch **out);
 stt_status stt_batch_iterate(stt_batch *b, int n_iters, void *stream);
 const char *stt_batch_last_error(const stt_batch *b);
+/* See stt_poll_status: polls every instance's solver. */
+stt_status stt_batch_poll_status(stt_batch *b, void *stream);
 stt_status stt_batch_destroy(stt_batch *b);
 
 /* Volume size (nx, ny, nz) of a context's geometry (HOST int[3]). */

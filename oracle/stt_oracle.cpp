@@ -1434,9 +1434,9 @@ int orc_fp_adjoint_f32(const orc_geom *g, int gmode, const orc_view *v, const fl
 }
 
 int orc_bp_voxel_f32(const orc_geom *g, int gmode, const orc_view *v, const float *corr,
-                     float alpha, float gmax, float *vol, int nthreads) {
+                     double alpha, float gmax, float *vol, int nthreads) {
     set_threads(nthreads);
-    return bp_voxel_impl<float>(*g, gmode, *v, corr, (double)alpha, gmax, vol);
+    return bp_voxel_impl<float>(*g, gmode, *v, corr, alpha, gmax, vol);
 }
 
 int orc_bp_voxel_f64(const orc_geom *g, const orc_view *v, const double *corr, double alpha,
@@ -1455,10 +1455,10 @@ void orc_bp_ray_update_f32(long n, const float *contrib, const float *wsum, floa
 }
 
 int orc_sart_f32(const orc_geom *g, int gmode, const orc_view *views, const int *perm, int nv,
-                 const float *proj, float alpha, float gmax, int bp_mode, float *vol,
+                 const float *proj, double alpha, float gmax, int bp_mode, float *vol,
                  float *raylen_state, const float *roi, int nthreads) {
     set_threads(nthreads);
-    return sart_impl<float>(*g, gmode, views, perm, nv, proj, (double)alpha, gmax, bp_mode, vol,
+    return sart_impl<float>(*g, gmode, views, perm, nv, proj, alpha, gmax, bp_mode, vol,
                             raylen_state, roi);
 }
 

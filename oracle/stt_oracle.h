@@ -62,9 +62,11 @@ int orc_fp_adjoint_f64(const orc_geom *g, const orc_view *v, const double *proj_
 int orc_fp_adjoint_f32(const orc_geom *g, int gmode, const orc_view *v,
                        const float *proj_bar, float *vol_bar);
 
-/* Voxel-driven BP (ST_Tomography.cpp:690-730): vol = clamp(vol + alpha*bicubic(c)). */
+/* Voxel-driven BP (ST_Tomography.cpp:690-730): vol = clamp(vol + alpha*bicubic(c)).
+ * alpha is a double, as the reference's m_alpha (:91): the update is formed in
+ * double and rounded to float once. */
 int orc_bp_voxel_f32(const orc_geom *g, int gmode, const orc_view *v, const float *corr,
-                     float alpha, float gmax, float *vol, int nthreads);
+                     double alpha, float gmax, float *vol, int nthreads);
 int orc_bp_voxel_f64(const orc_geom *g, const orc_view *v, const double *corr,
                      double alpha, double gmax, double *vol, int nthreads);
 
@@ -81,7 +83,7 @@ void orc_bp_ray_update_f32(long n, const float *contrib, const float *wsum, floa
  * ray-length buffer (W*H, caller-owned, zero at construction); roi (optional)
  * multiplies the volume after the sweep. */
 int orc_sart_f32(const orc_geom *g, int gmode, const orc_view *views, const int *perm, int nv,
-                 const float *proj, float alpha, float gmax, int bp_mode, float *vol,
+                 const float *proj, double alpha, float gmax, int bp_mode, float *vol,
                  float *raylen_state, const float *roi, int nthreads);
 int orc_sart_f64(const orc_geom *g, const orc_view *views, const int *perm, int nv,
                  const double *proj, double alpha, double gmax, int bp_mode, double *vol,

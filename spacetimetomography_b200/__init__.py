@@ -22,6 +22,7 @@ from .api import (  # noqa: F401
     views_from_rounds,
     warp,
     warp_box,
+    warp_poll_status,
     warp_vjp,
 )
 from .api import FlowParams_ as FlowParams  # noqa: F401

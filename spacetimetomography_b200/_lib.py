@@ -116,6 +116,10 @@ def _load() -> C.CDLL:
         "stt_flow_stats": [vp, C.POINTER(i), vp, vp],
         "stt_flow_blur": [vp, vp, i, f, vp, vp],
         "stt_flow_resize": [vp, vp, i, vp, vp, vp, vp],
+        "stt_poll_status": [vp, vp],
+        "stt_solver_poll_status": [vp, vp],
+        "stt_batch_poll_status": [vp, vp],
+        "stt_warp_poll_status": [vp],
     }
     for name, argtypes in sigs.items():
         fn = getattr(lib, name)

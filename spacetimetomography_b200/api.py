@@ -152,6 +152,11 @@ class Context:
         return {"norm_A": o.norm_A, "norm_K": o.norm_K, "sigma": o.sigma, "tau": o.tau,
                 "iterations": o.iterations, "rel_change": o.rel_change}
 
+    def poll_status(self, stream=None):
+        """Raises STTError (STT_ERR_TIMEOUT) if a bounded device-side wait of
+        this context's launches gave up since the last poll; synchronises."""
+        self._chk(lib.stt_poll_status(self._h, _stream(stream)))
+
     def fp_correction(self, vol, b, raylen_state, corr, view, stream=None):
         self._chk(lib.stt_fp_correction(self._h, _ptr(vol), _ptr(b), _ptr(raylen_state), _ptr(corr),
                                         view, _stream(stream)))
@@ -217,6 +222,12 @@ def warp(flow, src, dt, out=None, stream=None):
         out = torch.empty_like(src)
     check(lib.stt_warp(dim, _ptr(flow), _ptr(src), nc, float(dt), _ptr(out), _stream(stream)))
     return out
+
+
+def warp_poll_status(stream=None):
+    """Raises STTError (STT_ERR_TIMEOUT) if a bounded wait of a standalone warp
+    on the current device gave up since the last poll; synchronises."""
+    check(lib.stt_warp_poll_status(_stream(stream)))
 
 
 def warp_vjp(flow, src, dt, out_bar, src_bar=None, flow_bar=None, stream=None):
@@ -407,6 +418,12 @@ class Solver:
         if rc != 0:
             raise STTError(rc, lib.stt_solver_last_error(self._h).decode())
 
+    def poll_status(self, stream=None):
+        """See Context.poll_status."""
+        rc = lib.stt_solver_poll_status(self._h, _stream(stream))
+        if rc != 0:
+            raise STTError(rc, lib.stt_solver_last_error(self._h).decode())
+
     def stats(self):
         nl, it = C.c_longlong(), C.c_ulonglong()
         check(lib.stt_solver_stats(self._h, C.byref(nl), C.byref(it)))
@@ -449,6 +466,12 @@ class Batch:
 
     def iterate(self, n: int = 1, stream=None):
         rc = lib.stt_batch_iterate(self._h, int(n), _stream(stream))
+        if rc != 0:
+            raise STTError(rc, (lib.stt_batch_last_error(self._h) or b"").decode())
+
+    def poll_status(self, stream=None):
+        """See Context.poll_status."""
+        rc = lib.stt_batch_poll_status(self._h, _stream(stream))
         if rc != 0:
             raise STTError(rc, (lib.stt_batch_last_error(self._h) or b"").decode())
 

@@ -563,7 +563,7 @@ cudaError_t launch_flow_dual(const int *d, const float *v, const float *v_old, c
 }
 
 cudaError_t launch_flow_settle(long long n3, const int *iters, const float *v_b, float *v_a, cudaStream_t s) {
-    k_flow_settle<<<(unsigned)std::min<long long>((n3 + 255) / 256, 148 * 16), 256, 0, s>>>(n3, iters, v_b, v_a);
+    k_flow_settle<<<grid_stride_blocks(n3, 256), 256, 0, s>>>(n3, iters, v_b, v_a);
     return cudaGetLastError();
 }
 

@@ -152,6 +152,7 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
         }
     }
     bool gave_up = false;  // a copy did not land: the remaining samples read global memory
+    int drain0 = 0, drain1 = -1;  // after a give-up: the slabs whose copies may still be in flight
     for (int k = 0; k < nslab; ++k) {
         // issue slab k+1 into the other buffer (free since the barrier that ended slab k-1)
         int fn = 0, yn = 0;
@@ -169,9 +170,9 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
         bool staged = false;
         if (!gave_up) {
             staged = tma::mbar_wait(&bar[k & 1], (k >> 1) & 1, WAIT_CYCLES);
-            if (!staged) {
+            if (!staged) {  // an error: reported through the status word, the block stops staging
                 *dead = 1;
-                if (status) atomicExch(status, 1);
+                if (status) atomicExch(status, STT_WAIT_TIMEOUT_FLAG);
             }
         }
         const float *bx = buf + (k & 1) * BOXN;
@@ -226,9 +227,20 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
             for (int a = 0; a < 3; ++a) m.pos[a] = p[a];
         }
         __syncthreads();  // every ray is done with buffer k&1 before slab k+2 is loaded into it
+        if (*dead != 0 && !gave_up) {
+            // slab k's copy did not land in time, and slab k+1's was issued before that wait
+            drain0 = k;
+            drain1 = k + 1 < nslab ? k + 1 : k;
+        }
         gave_up = *dead != 0;
         f0 = fn;
         y0 = yn;
+    }
+    if (gave_up) {
+        // No block exits with a bulk copy still writing into its shared memory:
+        // wait (again bounded) for every copy issued but not seen to land.  The
+        // buffers are not read again; the samples above went to global memory.
+        for (int k = drain0; k <= drain1; ++k) tma::mbar_wait(&bar[k & 1], (k >> 1) & 1, WAIT_CYCLES);
     }
     // samples outside the planes the slabs covered
     while (m.peek()) {

@@ -302,9 +302,29 @@ dim3 transpose_grid(const GeomDev &g) { return dim3((g.nx + 63) / 64, (g.nz + 63
 
 }  // namespace
 
+int sm_count() {
+    // multiProcessorCount of each device, read once per device (148 on B200)
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 148;
+    }
+    if (!cached[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            n = 148;
+        }
+        cached[dev] = n;
+    }
+    return cached[dev];
+}
+
 int grid_stride_blocks(long long n, int threads) {
     long long b = (n + threads - 1) / threads;
-    const long long cap = 148LL * 16;  // 16 resident 256-thread blocks per SM on 148 SMs
+    // grid-stride loops: at most 8 resident 256-thread blocks per SM (2048 threads)
+    const long long cap = (long long)sm_count() * (2048 / (threads > 0 ? threads : 256));
     return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
 

@@ -80,11 +80,15 @@ constexpr int VX = 40, VY = 10, VZ = 6;  // velocity box (x, y, z) per plane; VX
 constexpr int VBOX = VX * VY * VZ;
 constexpr long long WARP_WAIT_CYCLES = 200000000LL;  // about 0.1 s
 
+// Status word of the warps launched without one (stt_warp, stt_warp_box on
+// their own): one per device, read and cleared by stt_warp_poll_status.
+__device__ int g_warp_wait_status;
+
 __global__ void __launch_bounds__(WARP_BX *WARP_BY) k_warp_staged(const Dim3i d,
                                                                   const __grid_constant__ CUtensorMap vmap,
                                                                   const float *__restrict__ vel,
                                                                   const float *__restrict__ src, int nc, float dt,
-                                                                  float *__restrict__ out) {
+                                                                  float *__restrict__ out, int *status) {
     __shared__ alignas(128) float vbox[3 * VBOX];
     __shared__ uint64_t bar;
     __shared__ int red[3 * WARP_BY];
@@ -136,7 +140,17 @@ __global__ void __launch_bounds__(WARP_BX *WARP_BY) k_warp_staged(const Dim3i d,
         tma::load_box_4d(vbox, &vmap, ox, oy, oz, 0, &bar);
     }
     bool staged = false;
-    if (any) staged = tma::mbar_wait(&bar, 0, WARP_WAIT_CYCLES);
+    if (any) {
+        staged = tma::mbar_wait(&bar, 0, WARP_WAIT_CYCLES);
+        if (!staged) {
+            // An error, reported through the status word.  The velocity sample
+            // reads global memory instead (same bits); the box is not read, but
+            // the block waits (bounded) once more so that it does not exit with
+            // the copy still writing into its shared memory.
+            atomicExch(status ? status : &g_warp_wait_status, STT_WAIT_TIMEOUT_FLAG);
+            tma::mbar_wait(&bar, 0, WARP_WAIT_CYCLES);
+        }
+    }
     if (!live) return;
     Cell s2;
     cell_setup(d, g2, s2);
@@ -316,14 +330,26 @@ __global__ void __launch_bounds__(128) k_warp_vjp(const Dim3i d, const float *__
 
 }  // namespace
 
+cudaError_t warp_poll_status(int *flag, cudaStream_t s) {
+    *flag = 0;
+    cudaError_t e = cudaMemcpyFromSymbolAsync(flag, g_warp_wait_status, sizeof(int), 0, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && *flag) {
+        const int zero = 0;
+        e = cudaMemcpyToSymbolAsync(g_warp_wait_status, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    return e;
+}
+
 cudaError_t launch_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
-                        float *out, cudaStream_t s) {
+                        float *out, cudaStream_t s, int *status) {
     Dim3i d{dim[0], dim[1], dim[2]};
     const dim3 grid((d.x + WARP_BX - 1) / WARP_BX, (d.y + WARP_BY - 1) / WARP_BY, d.z), block(WARP_BX, WARP_BY);
     CUtensorMap vmap;
     const unsigned box[4] = {VX, VY, VZ, 3};
     if (encode_planes_map(&vmap, vel, d.x, d.y, d.z, 3, box))
-        k_warp_staged<<<grid, block, 0, s>>>(d, vmap, vel, src, nc, dt, out);
+        k_warp_staged<<<grid, block, 0, s>>>(d, vmap, vel, src, nc, dt, out, status);
     else
         k_warp<<<grid, block, 0, s>>>(d, vel, src, nc, dt, out);
     return cudaGetLastError();

@@ -161,6 +161,19 @@ stt_status stt_batch_iterate(stt_batch *b, int n_iters, void *stream) {
     return STT_OK;
 }
 
+stt_status stt_batch_poll_status(stt_batch *b, void *stream) {
+    if (!b) return STT_ERR_INVALID;
+    stt_status worst = STT_OK;
+    for (size_t i = 0; i < b->inst.size(); ++i) {
+        const stt_status st = stt_solver_poll_status(b->inst[i].solver, stream);
+        if (st != STT_OK && worst == STT_OK) {
+            worst = st;
+            bfail(b, st, "instance " + std::to_string(i) + ": " + stt_solver_last_error(b->inst[i].solver));
+        }
+    }
+    return worst;
+}
+
 const char *stt_batch_last_error(const stt_batch *b) { return b ? b->err.c_str() : "null batch"; }
 
 stt_status stt_batch_destroy(stt_batch *b) {

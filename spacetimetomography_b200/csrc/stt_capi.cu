@@ -33,6 +33,8 @@ struct stt_ctx {
     size_t pw_n = 0;
     double *pwd = nullptr;  // power iteration: FP64 sums
     size_t pwd_n = 0;
+    int *status = nullptr;  // raised by a bounded device-side wait that gave up (stt_poll_status)
+    size_t status_n = 0;
 };
 
 namespace {
@@ -155,6 +157,7 @@ stt_status stt_destroy(stt_ctx *ctx) {
     cudaFree(ctx->volt16);
     cudaFree(ctx->pw);
     cudaFree(ctx->pwd);
+    cudaFree(ctx->status);
     delete ctx;
     return STT_OK;
 }
@@ -250,6 +253,10 @@ stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g) {
         return fail(ctx, STT_ERR_INVALID, "sid must exceed the volume half-diagonal plus the offset");
     stt_status st = set_device(ctx);
     if (st) return st;
+    if (!ctx->status) {
+        if ((st = ensure(ctx, ctx->status, ctx->status_n, 4, "status word"))) return st;
+        STT_CUDA(ctx, cudaMemset(ctx->status, 0, 4 * sizeof(int)), "cudaMemset(status word)");
+    }
     ctx->views_h.resize(g->n_views);
     for (int v = 0; v < g->n_views; ++v) build_view(*g, g->angles_rad[v], ctx->views_h[v]);
     if (g->n_views > 0) {
@@ -356,7 +363,8 @@ stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, flo
     if ((st = transposed_if_needed(ctx, vol, view, 1, S(stream), &volt))) return st;
     stt::FpSlabMaps maps;
     stt::make_fp_slab_maps(ctx->g, vol, volt, maps);
-    STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, b, raylen_state, corr, S(stream), 0, &maps),
+    STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, b, raylen_state, corr, S(stream), 0, &maps,
+                                      ctx->status),
              "k_fp_corr launch");
     return STT_OK;
 }
@@ -449,7 +457,7 @@ stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, con
         // ray-based mode: TypicalRayProducer::Initial zeroes the ray lengths
         // after every view, so missed rays see L = 0 (no sticky state)
         STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, proj_stack,
-                                          bp_mode == 0 ? raylen_state : nullptr, ctx->corr, s, 0, &maps),
+                                          bp_mode == 0 ? raylen_state : nullptr, ctx->corr, s, 0, &maps, ctx->status),
                  "k_fp_corr launch");
         if (bp_mode == 0)
             STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, sel, ctx->corr, vol, (float)alpha, gmax, s),
@@ -601,6 +609,31 @@ stt_status stt_internal_geom(stt_ctx *ctx, const void **geom, const void **views
     *geom = &ctx->g;
     *views = ctx->views_d;
     return STT_OK;
+}
+
+stt_status stt_poll_status(stt_ctx *ctx, void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if ((st = set_device(ctx))) return st;
+    int flag = 0;
+    STT_CUDA(ctx, cudaMemcpyAsync(&flag, ctx->status, sizeof(int), cudaMemcpyDeviceToHost, S(stream)),
+             "read status word");
+    STT_CUDA(ctx, cudaStreamSynchronize(S(stream)), "cudaStreamSynchronize");
+    if (!flag) return STT_OK;
+    STT_CUDA(ctx, cudaMemsetAsync(ctx->status, 0, sizeof(int), S(stream)), "clear status word");
+    STT_CUDA(ctx, cudaStreamSynchronize(S(stream)), "cudaStreamSynchronize");
+    return fail(ctx, STT_ERR_TIMEOUT,
+                "a bounded device-side wait gave up: a TMA copy into shared memory did not land within about "
+                "0.1 s (the results were computed from global memory instead)");
+}
+
+stt_status stt_warp_poll_status(void *stream) {
+    int flag = 0;
+    STT_CUDA(nullptr, stt::warp_poll_status(&flag, S(stream)), "warp status word");
+    if (!flag) return STT_OK;
+    return fail(nullptr, STT_ERR_TIMEOUT,
+                "a bounded device-side wait of a staged warp gave up: its velocity box did not land within about "
+                "0.1 s (the warp read global memory instead)");
 }
 
 stt_status stt_warp(const int *dim, const float *vel, const float *src, int nc, float dt, float *out,

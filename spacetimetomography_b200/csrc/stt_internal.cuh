@@ -48,6 +48,11 @@ struct GeomDev {
     float sdd_ds;      // sdd / ds
 };
 
+// Value a kernel writes to its status word when a bounded wait gave up (a
+// TMA copy into shared memory that did not land within about 0.1 s).  The
+// host reads it with stt_poll_status / stt_solver_poll_status.
+#define STT_WAIT_TIMEOUT_FLAG 1
+
 // The reference clamps with the macros max(a,b) = a>b?a:b, min(a,b) = a<b?a:b
 // (ST_Tomography.cpp:167-173); their NaN behaviour (NaN -> the second operand
 // of max) is part of the semantics, so fminf/fmaxf are not used for them.

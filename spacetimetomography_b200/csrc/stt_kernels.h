@@ -15,6 +15,8 @@ struct PdParams {
     int cut[8];
 };
 
+// Multiprocessor count of the current device (cached per device).
+int sm_count();
 int grid_stride_blocks(long long n, int threads);
 
 cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, int view0,
@@ -123,8 +125,13 @@ cudaError_t launch_gradient(const int *d, const float *img, float *g, cudaStream
 cudaError_t launch_copy_roi(const int *d, int nc, const FlowRoi &roi, const float *src, float *dst,
                             cudaStream_t s);
 
+// `status` (may be null: then a per-device word read by warp_poll_status) is
+// set when the staged kernel's bounded wait for its velocity box gave up.
 cudaError_t launch_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
-                        float *out, cudaStream_t s);
+                        float *out, cudaStream_t s, int *status = nullptr);
+// Reads and clears the per-device status word of warps launched without one
+// (synchronises `s`); *flag is non-zero if a bounded wait gave up.
+cudaError_t warp_poll_status(int *flag, cudaStream_t s);
 cudaError_t launch_warp_vjp(const int *dim, const float *vel, const float *src, int nc, float dt,
                             const float *out_bar, float *src_bar, float *vel_bar, cudaStream_t s);
 

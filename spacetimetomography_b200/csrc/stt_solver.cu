@@ -112,6 +112,7 @@ struct stt_solver {
     float2 *acc = nullptr;     // ray-based BP accumulators, F volumes
     int *perm = nullptr;       // F x V device view order
     unsigned long long *counter = nullptr;
+    int *status = nullptr;     // raised by a bounded device-side wait that gave up
     unsigned long long host_iter = 0;
     std::vector<cudaStream_t> streams;
     std::vector<cudaEvent_t> ev_dual, ev_done;
@@ -184,7 +185,8 @@ stt_status enqueue_dual(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
     const int d[3] = {s->g->nx, s->g->ny, s->g->nz};
     const size_t n = s->n;
     float *bw = s->warpbuf + f * n;
-    SCUDA(s, stt::launch_warp(d, s->st.flow + (size_t)f * 3 * n, s->st.xbar + (f + 1) * n, 1, -1.0f, bw, cs),
+    SCUDA(s, stt::launch_warp(d, s->st.flow + (size_t)f * 3 * n, s->st.xbar + (f + 1) * n, 1, -1.0f, bw, cs,
+                              s->status),
           "warp (dual)");
     SCUDA(s, stt::launch_pd_dual(d, pdp(s->cfg.pd), s->st.xbar + f * n, s->st.xbar + (f + 1) * n, bw,
                                  s->st.ytv + (size_t)f * 3 * n, s->st.ytp + f * n, s->st.ybc + f * n, cs),
@@ -213,7 +215,7 @@ stt_status enqueue_primal(stt_solver *s, int f, cudaStream_t cs, long long &nl) 
         flow_prev = s->st.flow_halo;
     }
     if (!first) {
-        SCUDA(s, stt::launch_warp(d, flow_prev, ybc_prev, 1, 1.0f, fw, cs), "warp (primal)");
+        SCUDA(s, stt::launch_warp(d, flow_prev, ybc_prev, 1, 1.0f, fw, cs, s->status), "warp (primal)");
         ++nl;
     }
     SCUDA(s, stt::launch_pd_primal(d, pdp(s->cfg.pd), first, ytp_prev, s->st.ytp + f * n, first ? nullptr : fw,
@@ -241,7 +243,7 @@ stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long
         const bool tex = voxel && !s->corr_tex.empty();
         SCUDA(s, stt::launch_fp_corr(g, s->views, vol, volt, sel, stack, voxel ? s->raylen + f * s->npix : nullptr,
                                      corr, cs, tex ? s->corr_tex[f].surf : 0,
-                                     s->fpmaps.empty() ? nullptr : &s->fpmaps[f]),
+                                     s->fpmaps.empty() ? nullptr : &s->fpmaps[f], s->status),
               "fp_corr");
         nl += (!s->fpmaps.empty() && s->fpmaps[f].ok) ? 2 : 1;  // slab-staged + gather kernels, or gather only
         if (voxel)
@@ -427,6 +429,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     if (!e) e = alloc(s, s->raylen, (size_t)F * s->npix, "ray lengths");
     if (!e) e = alloc(s, s->perm, (size_t)F * s->V, "view order");
     if (!e) e = alloc(s, s->counter, 1, "iteration counter");
+    if (!e) e = alloc(s, s->status, 1, "status word");
     if (!e && cfg->bp_mode == 1) e = alloc(s, s->acc, (size_t)F * s->n, "ray-BP accumulators");
     if (e) {
         stt_solver_destroy(s);
@@ -448,6 +451,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     }
     cudaError_t ce = cudaMemset(s->raylen, 0, (size_t)F * s->npix * sizeof(float));
     if (ce == cudaSuccess) ce = cudaMemset(s->counter, 0, sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaMemset(s->status, 0, sizeof(int));
     if (ce == cudaSuccess && s->acc) ce = cudaMemset(s->acc, 0, (size_t)F * s->n * sizeof(float2));
     s->streams.resize(F);
     s->ev_dual.resize(F);
@@ -556,6 +560,20 @@ stt_status stt_solver_stats(const stt_solver *s, long long *launches_per_iter, u
     return STT_OK;
 }
 
+stt_status stt_solver_poll_status(stt_solver *s, void *stream) {
+    if (!s) return STT_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+    int flag = 0;
+    SCUDA(s, cudaMemcpyAsync(&flag, s->status, sizeof(int), cudaMemcpyDeviceToHost, cs), "read status word");
+    SCUDA(s, cudaStreamSynchronize(cs), "cudaStreamSynchronize");
+    if (!flag) return STT_OK;
+    SCUDA(s, cudaMemsetAsync(s->status, 0, sizeof(int), cs), "clear status word");
+    SCUDA(s, cudaStreamSynchronize(cs), "cudaStreamSynchronize");
+    return sfail(s, STT_ERR_TIMEOUT,
+                 "a bounded device-side wait gave up: a TMA copy into shared memory did not land within about 0.1 s "
+                 "(the results were computed from global memory instead)");
+}
+
 const char *stt_solver_last_error(const stt_solver *s) { return s ? s->err.c_str() : ""; }
 
 stt_status stt_solver_destroy(stt_solver *s) {
@@ -582,6 +600,7 @@ stt_status stt_solver_destroy(stt_solver *s) {
     cudaFree(s->acc);
     cudaFree(s->perm);
     cudaFree(s->counter);
+    cudaFree(s->status);
     delete s;
     return STT_OK;
 }

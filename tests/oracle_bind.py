@@ -50,11 +50,11 @@ O.orc_fp_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp, _vp, _vp,
 O.orc_bp_ray_scatter_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp, _vp]
 O.orc_fp_adjoint_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp]
 O.orc_fp_adjoint_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp]
-O.orc_bp_voxel_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _f, _f, _vp, _i]
+O.orc_bp_voxel_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _d, _f, _vp, _i]
 O.orc_bp_voxel_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _d, _d, _vp, _i]
 O.orc_correction_f32.argtypes = [_i, _vp, _vp, _vp, _vp]
 O.orc_bp_ray_update_f32.argtypes = [C.c_long, _vp, _vp, _f, _vp]
-O.orc_sart_f32.argtypes = [C.POINTER(OGeom), _i, _vp, _vp, _i, _vp, _f, _f, _i, _vp, _vp, _vp, _i]
+O.orc_sart_f32.argtypes = [C.POINTER(OGeom), _i, _vp, _vp, _i, _vp, _d, _f, _i, _vp, _vp, _vp, _i]
 O.orc_sart_f64.argtypes = [C.POINTER(OGeom), _vp, _vp, _i, _vp, _d, _d, _i, _vp, _vp, _vp, _i]
 O.orc_roi_mask_f32.argtypes = [_vp, _vp, _vp]
 O.orc_permutation.argtypes = [C.c_ulonglong, _i, _vp]
@@ -94,6 +94,28 @@ if REF_SO.exists():
     REF.ref_flow_level.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _i, _i, _i, _f,
                                    _vp, _i]
     REF.ref_flow_multiscale.argtypes = [_vp, _vp, _vp, _vp, _vp, _f, _f, _i, _i, _i, _f, _f, _i, _f, _vp, _i]
+
+
+REF_ST_SO = ROOT / "oracle" / "_ref" / "libstt_ref_st.so"
+
+
+class RefStCfg(C.Structure):
+    """ref_st_cfg of oracle/ref_st_driver.cpp."""
+    _fields_ = [("dims", C.c_int * 3), ("sp", C.c_float * 3), ("W", C.c_int), ("H", C.c_int), ("ds", C.c_double),
+                ("sid", C.c_double), ("sdd", C.c_double), ("oxyz", C.c_double * 3), ("nframes", C.c_int),
+                ("nrounds", C.c_int), ("bp_mode", C.c_int), ("alpha", C.c_double), ("tv_w", C.c_double),
+                ("tp_w", C.c_double), ("bc_w", C.c_double), ("huber", C.c_double), ("cut", C.c_int * 8),
+                ("joint_iters", C.c_int), ("gmax", C.c_float), ("threads", C.c_int)]
+
+
+REF_ST = None
+if REF_ST_SO.exists():
+    REF_ST = C.CDLL(str(REF_ST_SO))
+    REF_ST.ref_st_run.argtypes = [C.POINTER(RefStCfg), _vp, C.c_char_p] + [_vp] * 3 + [_i] + [_vp] * 7 + [_vp, _vp,
+                                                                                                        _vp]
+    REF_ST.ref_st_shuffle.argtypes = [C.c_uint, _i, _vp]
+    REF_ST.ref_st_last_run_seconds.argtypes = []
+    REF_ST.ref_st_last_run_seconds.restype = C.c_double
 
 
 class Scan:
@@ -519,4 +541,55 @@ def ref_flow_multiscale(I1, I2, V, cut, tol=0.0, lam=1.2, max_iter=20, norm=4, n
     REF.ref_flow_multiscale(P(d), P(_f32(I1)), P(_f32(I2)), P(_f32(V)), P(out), float(tol), float(lam),
                             int(max_iter), int(norm), int(n_warps), float(eta), float(sigma), int(scales),
                             float(huber), P(c8), threads)
+    return out
+
+
+# ---- the reference's own ST_Tomography (oracle/_ref/libstt_ref_st.so) -------
+
+def ref_st_run(scan: Scan, start_deg, proj, vols, flows, *, rounds=1, bp_mode=0, alpha=0.3, tv_w=0.05, tp_w=0.3,
+               bc_w=0.2, huber=0.01, cut=(3, 3, 3, 5, 3, 3, 6, 5), mode=0, joint_iters=2, gmax=0.0, threads=1,
+               full=True):
+    """Runs the reference's ST_Tomography: mode 0 = SART(f) for every frame,
+    mode 1 = Render (the joint loop).  start_deg: (F, rounds); proj: (F, V, H, W)
+    with V = 10 * rounds; vols: (F, nz, ny, nx); flows: (F, 3, nz, ny, nx).
+    Returns a dict of the outputs (only `vol` unless full), the srand seeds,
+    G_Max and the seconds the SART calls / Render took."""
+    import tempfile
+
+    F = len(vols)
+    nx, ny, nz = scan.dims
+    W, H = scan.det
+    cfg = RefStCfg((C.c_int * 3)(*scan.dims), (C.c_float * 3)(*scan.sp), W, H, float(scan.ds), float(scan.sid),
+                   float(scan.sdd), (C.c_double * 3)(*scan.off), F, rounds, bp_mode, float(alpha), float(tv_w),
+                   float(tp_w), float(bc_w), float(huber), (C.c_int * 8)(*cut), joint_iters, float(gmax), threads)
+    sd = np.ascontiguousarray(np.asarray(start_deg, np.float32).reshape(F, rounds))
+    pr = np.ascontiguousarray(proj, np.float32)
+    vo = np.ascontiguousarray(vols, np.float32)
+    fl = np.ascontiguousarray(flows, np.float32)
+    out = dict(vol=np.zeros((F, nz, ny, nx), np.float32))
+    if full:
+        out.update(xbar=np.zeros((F + 1, nz, ny, nx), np.float32), xprev=np.zeros((F + 1, nz, ny, nx), np.float32),
+                   ytv=np.zeros((F + 1, 3, nz, ny, nx), np.float32), ytp=np.zeros((F + 1, nz, ny, nx), np.float32),
+                   ybc=np.zeros((F + 1, nz, ny, nx), np.float32), flow=np.zeros((F, 3, nz, ny, nx), np.float32))
+    g = out.get
+    seeds = np.zeros(4096, np.uint32)
+    nseeds = C.c_int(len(seeds))
+    gm = C.c_float()
+    with tempfile.TemporaryDirectory() as wd:
+        (Path(wd) / "FlowOutput").mkdir()
+        rc = REF_ST.ref_st_run(C.byref(cfg), P(sd), wd.encode(), P(pr), P(vo), P(fl), mode, P(out["vol"]),
+                               P(g("xbar")), P(g("xprev")), P(g("ytv")), P(g("ytp")), P(g("ybc")),
+                               P(g("flow")), P(seeds), C.byref(nseeds), C.byref(gm))
+    if rc != 0:
+        raise RuntimeError(f"ref_st_run failed: {rc}")
+    out["seeds"] = seeds[:nseeds.value].copy()
+    out["gmax"] = float(gm.value)
+    out["seconds"] = float(REF_ST.ref_st_last_run_seconds())
+    return out
+
+
+def ref_st_shuffle(seed: int, n: int) -> np.ndarray:
+    """The view order the reference's SART draws after srand(seed)."""
+    out = np.zeros(n, np.int32)
+    REF_ST.ref_st_shuffle(int(seed), n, P(out))
     return out
