@@ -505,7 +505,7 @@ def run_stt(args):
 
     def make_solver(mode):
         return stt.Solver(ctx, st, F, V, pd, alpha=0.3, bp_mode=bp_mode, seed=99, mode=mode,
-                          halo=(halo is not None and rank > 0))
+                          halo=(halo is not None and rank > 0), frame_offset=rank * F, total_frames=world * F)
 
     solver = make_solver(stt.SOLVE_GRAPH)
 

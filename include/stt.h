@@ -364,6 +364,12 @@ typedef struct stt_solve_cfg {
      * (the previous shard's last frame) and xbar[F] holds the next shard's
      * X_bar[0].  The caller exchanges them between the two phases. */
     int halo;
+    /* Place of these frames in the whole sequence (frame sharding): local
+     * frame f is frame frame_offset + f of total_frames (0 = n_frames).  The
+     * view order of each frame is drawn from its place in the sequence, so
+     * shards draw the orders the unsharded solve would. */
+    int frame_offset;
+    int total_frames;
 } stt_solve_cfg;
 
 typedef struct stt_pd_state {
@@ -390,7 +396,9 @@ const char *stt_solver_last_error(const stt_solver *s);
 /* See stt_poll_status. */
 stt_status stt_solver_poll_status(stt_solver *s, void *stream);
 stt_status stt_solver_destroy(stt_solver *s);
-/* Host copy of the view order frame `frame` uses in iteration `iter` (HOST perm_out). */
+/* Host copy of the view order frame `frame` of a sequence of n_frames uses in
+ * iteration `iter` (HOST perm_out); for a shard, frame and n_frames are its
+ * frame_offset + local frame and total_frames. */
 stt_status stt_solver_frame_order(unsigned long long seed, unsigned long long iter, int n_frames,
                                   int frame, int views, int *perm_out);
 

@@ -41,7 +41,8 @@ class PdParams(C.Structure):
 class SolveCfg(C.Structure):
     _fields_ = [("n_frames", C.c_int), ("views_per_frame", C.c_int), ("bp_mode", C.c_int),
                 ("alpha", C.c_double), ("pd", PdParams), ("roi_cut", C.c_int * 8),
-                ("seed", C.c_ulonglong), ("mode", C.c_int), ("halo", C.c_int)]
+                ("seed", C.c_ulonglong), ("mode", C.c_int), ("halo", C.c_int), ("frame_offset", C.c_int),
+                ("total_frames", C.c_int)]
 
 
 class PdState(C.Structure):

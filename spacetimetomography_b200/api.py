@@ -392,13 +392,17 @@ class Solver:
 
     def __init__(self, ctx: Context, state: dict, n_frames: int, views_per_frame: int,
                  pd: PdParams, alpha: float = 0.3, bp_mode: int = 0, roi_cut=REFERENCE_CUT,
-                 seed: int = 0, mode: int = SOLVE_GRAPH, halo: bool = False):
+                 seed: int = 0, mode: int = SOLVE_GRAPH, halo: bool = False, frame_offset: int = 0,
+                 total_frames: int = 0):
         """halo=True: local frame 0 continues a previous shard (state needs
-        ytp_halo, ybc_halo, flow_halo; see spacetimetomography_b200.halo)."""
+        ytp_halo, ybc_halo, flow_halo; see spacetimetomography_b200.halo).
+        frame_offset / total_frames: the shard's place in the whole sequence
+        (its view orders are those of the unsharded solve)."""
         self.ctx = ctx
         self.state = state  # keeps the tensors alive
         cfg = SolveCfg(n_frames, views_per_frame, bp_mode, float(alpha), pd.c(),
-                       (C.c_int * 8)(*map(int, roi_cut)), C.c_ulonglong(seed), mode, int(bool(halo)))
+                       (C.c_int * 8)(*map(int, roi_cut)), C.c_ulonglong(seed), mode, int(bool(halo)),
+                       int(frame_offset), int(total_frames))
         keys = ("vol", "xbar", "xprev", "ytv", "ytp", "ybc", "flow", "proj", "ytp_halo", "ybc_halo",
                 "flow_halo")
         st = PdState(*[state[k].data_ptr() if k in state else None for k in keys])

@@ -69,8 +69,10 @@ cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, c
 
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                             float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex = 0);
-cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counter, int frames,
-                             int views, int *perm, cudaStream_t s);
+// View orders of `frames` local frames (at most 1024), local frame f being
+// frame frame0 + f of a sequence of `total`; advances *counter.
+cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counter, int frames, int total,
+                             int frame0, int views, int *perm, cudaStream_t s);
 cudaError_t launch_pd_dual(const int *dims, const PdParams &p, const float *xf, const float *xf1,
                            const float *bw, float *ytv, float *ytp, float *ybc, cudaStream_t s);
 cudaError_t launch_pd_primal(const int *dims, const PdParams &p, int first, const float *ytp_prev,

@@ -35,23 +35,26 @@ __device__ __host__ __forceinline__ unsigned long long splitmix(unsigned long lo
 }
 
 // Seed of frame f's view order in PD iteration `iter` (the reference reseeds
-// with time(0) in every SART call, ST_Tomography.cpp:635).
+// with time(0) in every SART call, ST_Tomography.cpp:635).  f is the frame's
+// index in the whole sequence of `frames`, so that shards of a frame-sharded
+// solve draw the orders the unsharded solve would.
 __device__ __host__ __forceinline__ unsigned long long frame_seed(unsigned long long seed,
                                                                  unsigned long long iter, int frames,
                                                                  int f) {
     return seed + 0x9E3779B97F4A7C15ull * (iter * (unsigned long long)frames + (unsigned long long)f + 1ull);
 }
 
-// One thread per frame: Fisher-Yates with SplitMix64 (the same stream as
-// stt_permutation), then thread 0 advances the iteration counter.
-__global__ void k_make_perm(unsigned long long seed, unsigned long long *counter, int frames, int views,
-                            int *perm) {
+// One thread per local frame: Fisher-Yates with SplitMix64 (the same stream
+// as stt_permutation), then thread 0 advances the iteration counter.  Local
+// frame f is frame frame0 + f of a sequence of `total` frames.
+__global__ void k_make_perm(unsigned long long seed, unsigned long long *counter, int frames, int total, int frame0,
+                            int views, int *perm) {
     const int f = threadIdx.x + blockIdx.x * blockDim.x;
     const unsigned long long iter = *counter;
     if (f < frames) {
         int *p = perm + (size_t)f * views;
         for (int i = 0; i < views; ++i) p[i] = i;
-        unsigned long long s = frame_seed(seed, iter, frames, f);
+        unsigned long long s = frame_seed(seed, iter, total, frame0 + f);
         for (int i = views - 1; i > 0; --i) {
             const int j = (int)(splitmix(s) % (unsigned long long)(i + 1));
             const int t = p[i];
@@ -65,9 +68,10 @@ __global__ void k_make_perm(unsigned long long seed, unsigned long long *counter
 
 }  // namespace
 
-cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counter, int frames, int views,
-                             int *perm, cudaStream_t s) {
-    k_make_perm<<<1, ((frames + 31) / 32) * 32, 0, s>>>(seed, counter, frames, views, perm);
+cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counter, int frames, int total,
+                             int frame0, int views, int *perm, cudaStream_t s) {
+    if (frames > 1024) return cudaErrorInvalidValue;  // one block, one thread per frame
+    k_make_perm<<<1, ((frames + 31) / 32) * 32, 0, s>>>(seed, counter, frames, total, frame0, views, perm);
     return cudaGetLastError();
 }
 
@@ -103,6 +107,7 @@ struct stt_solver {
     const stt::GeomDev *g = nullptr;
     const stt::ViewRec *views = nullptr;
     int F = 0, V = 0;
+    int total_frames = 0;  // frames of the whole (possibly sharded) sequence
     size_t n = 0, npix = 0;
     float *warpbuf = nullptr;  // F volumes: backward-warped X_bar[f+1], then forward-warped Y_bc[f-1]
     float *corr = nullptr;     // F correction images
@@ -267,7 +272,9 @@ stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long
 // `join` the frame streams rejoin `main` (phases run separately).
 stt_status enqueue_phase0(stt_solver *s, cudaStream_t main, long long &nl, bool join) {
     const int F = s->F;
-    SCUDA(s, stt::launch_make_perm(s->cfg.seed, s->counter, F, s->V, s->perm, main), "make_perm");
+    SCUDA(s, stt::launch_make_perm(s->cfg.seed, s->counter, F, s->total_frames, s->cfg.frame_offset, s->V, s->perm,
+                                   main),
+          "make_perm");
     ++nl;
     SCUDA(s, cudaEventRecord(s->ev_fork, main), "event record");
     for (int f = 0; f < F; ++f) SCUDA(s, cudaStreamWaitEvent(s->streams[f], s->ev_fork, 0), "stream wait");
@@ -337,12 +344,12 @@ stt_status run_plain(stt_solver *s, cudaStream_t cs, long long &nl, int phase) {
 
 stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
     const stt::GeomDev &g = *s->g;
-    const int F = s->F, V = s->V;
+    const int V = s->V;
     const int d[3] = {g.nx, g.ny, g.nz};
     std::vector<int> perm(V);
     const int voxel = s->cfg.bp_mode == 0;
     {
-        stt::host_perm(s->cfg.seed, s->host_iter, F, f, V, perm.data());
+        stt::host_perm(s->cfg.seed, s->host_iter, s->total_frames, s->cfg.frame_offset + f, V, perm.data());
         float *vol = s->st.vol + f * s->n;
         float *corr = s->corr + f * s->npix;
         float *rl = s->raylen + f * s->npix;
@@ -410,6 +417,9 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
         !state->flow || !state->proj)
         return STT_ERR_INVALID;
     if (cfg->halo && (!state->ytp_halo || !state->ybc_halo || !state->flow_halo)) return STT_ERR_INVALID;
+    if (cfg->n_frames > 1024) return STT_ERR_INVALID;
+    const int total = cfg->total_frames > 0 ? cfg->total_frames : cfg->n_frames;
+    if (cfg->frame_offset < 0 || (long long)cfg->frame_offset + cfg->n_frames > total) return STT_ERR_INVALID;
     stt_solver *s = new stt_solver();
     s->ctx = ctx;
     s->cfg = *cfg;
@@ -418,6 +428,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     s->views = (const stt::ViewRec *)vp;
     s->F = cfg->n_frames;
     s->V = cfg->views_per_frame;
+    s->total_frames = total;
     s->n = (size_t)g->nx * g->ny * g->nz;
     s->npix = (size_t)g->W * g->H;
     const int F = s->F;

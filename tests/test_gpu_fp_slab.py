@@ -61,3 +61,5 @@ def test_slab_staged_fp_correction_equals_gather(cuda, case):
         staged += min(abs(math.sin(a)), abs(math.cos(a))) > 0.4226
         assert hit.any()
     assert staged >= 6  # the slab kernel had views to project
+    ctx.poll_status()  # no bounded wait of the staged kernel gave up
+    ctx.close()
