@@ -46,6 +46,30 @@ sys.path.insert(0, str(ROOT))
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC_FILE = ROOT / "profiles" / "fp_corr_traffic.json"
 
+# The single-frame workloads (the headline is the 4D iteration above).  Every
+# one uses 1 mm voxels and detector pixels, sid 600 mm, sdd 1000 mm, views
+# equally spaced over 360 degrees and seeded ellipsoid phantoms (centres in the
+# inner 80 %, semi-axes 5-40 voxels at 256^3, scaled with the volume, additive
+# densities 0.1-1).
+CONFIG_SPECS = {
+    1: dict(workload="plain single-frame SART, 128^3 FP32, 128 views over 360 deg, 128^2 detector, voxel-based BP, "
+                     "alpha 0.3, 20 iterations, 1% Gaussian noise on the sinogram",
+            n=128, det=128, views=128, ellipsoids=12, porous=False, noise=0.01, solve="sart", iters=20,
+            bps=("voxel",), alpha=0.3, roi=None),
+    2: dict(workload="single-frame primal-dual TV + SART, 256^3 FP32, 360 views over 360 deg, 512^2 detector, "
+                     "sigma = tau = 0.2, lambda 0.01, Huber 0.01, 20 outer iterations of 1 SART sweep, "
+                     "voxel- and ray-based BP",
+            n=256, det=512, views=360, ellipsoids=30, porous=False, noise=0.0, solve="pd", iters=20,
+            bps=("voxel", "ray"), alpha=0.3, sigma=0.2, tau=0.2, lam=0.01, huber=0.01,
+            roi=(8, 8, 8, 45, 8, 8, 30, 20)),
+    5: dict(workload="single-frame primal-dual TV + SART, 512^3 FP32, 720 views over 360 deg, 1024^2 detector, "
+                     "100 ellipsoids on a 0.5-density porous background of random spheres (radius 2-6), "
+                     "10 outer iterations, voxel- and ray-based BP",
+            n=512, det=1024, views=720, ellipsoids=100, porous=True, noise=0.0, solve="pd", iters=10,
+            bps=("voxel", "ray"), alpha=0.3, sigma=0.9 / 8.0, tau=1.0, lam=0.01, huber=0.01,
+            roi=(16, 16, 16, 90, 16, 16, 60, 40)),
+}
+
 
 def parse_args():
     ap = argparse.ArgumentParser()
@@ -66,6 +90,14 @@ def parse_args():
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--flow-only", action="store_true",
                     help="run only the optical-flow leg (one L1Huber_OF level at --n^3) and print its line")
+    ap.add_argument("--config", type=int, choices=sorted(CONFIG_SPECS), default=None,
+                    help="run only the single-frame workload of that number (1: 128^3 SART, 2: 256^3 PD TV, "
+                         "5: 512^3 PD TV) and print its own line")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="default run: skip the single-frame workloads' sub-lines")
+    ap.add_argument("--fp-probe", action="store_true",
+                    help="with --config: only project a few views with the fused forward projector "
+                         "(a small command for ncu captures at that size)")
     return ap.parse_args()
 
 
@@ -438,6 +470,378 @@ def flow_cpu_sample(i1, i2) -> dict:
                       + (" (the reference's code, OpenMP)" if use_ref else " (oracle port, one thread)")}
 
 
+# ---------------------------------------------------------------------------
+# Single-frame workloads (CONFIG_SPECS)
+
+def config_problem(cid: int, dev):
+    """The workload's context (geometry), phantom and sinogram on the device;
+    G_Max = max(sinogram)/4 as SetData forms it (ST_Tomography.cpp:356-357)."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200 import phantom as ph
+
+    c = CONFIG_SPECS[cid]
+    N, D, V = c["n"], c["det"], c["views"]
+    dims = (N, N, N)
+    ang = ph.equispaced_views(V)
+    ctx = stt.Context(dev.index or 0)
+    ctx.set_geometry(dims, (1.0, 1.0, 1.0), (D, D), 1.0, 600.0, 1000.0, ang)
+    s = N / 256.0
+    bg = ph.porous_background(dims, 77, N ** 3 // 1000, device=dev) if c["porous"] else None
+    truth = ph.rasterize(ph.ellipsoid_params(c["ellipsoids"], dims, seed=100 + cid, semi=(5.0 * s, 40.0 * s)), dims,
+                         dev, background=bg)
+    proj = torch.empty((V, D, D), device=dev)
+    ctx.fp(truth, proj)
+    if c["noise"] > 0:
+        proj = ph.add_noise(proj, c["noise"], seed=cid)
+    torch.cuda.synchronize()
+    return ctx, truth, proj.contiguous(), float(proj.max().item()) / 4.0
+
+
+def _timed(stream, fn, reps: int) -> float:
+    """Seconds per call of fn() over `reps` calls, CUDA events on `stream`."""
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1000.0 / max(reps, 1)
+
+
+def _pd_state(N, proj, dev):
+    import torch
+
+    z = lambda *s: torch.zeros(s, device=dev)  # noqa: E731
+    return dict(vol=z(2, N, N, N), xbar=z(2, N, N, N), xprev=z(1, N, N, N), ytv=z(1, 3, N, N, N), ytp=z(1, N, N, N),
+                ybc=z(1, N, N, N), flow=z(1, 3, N, N, N), proj=proj[None])
+
+
+def config_solve(cid, ctx, proj, truth, gmax, bp, dev, stream, iters: int, reps: int) -> dict:
+    """One solve of the workload; times `reps` of its iterations after one
+    warm-up iteration and reports the error to the phantom after `iters`."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+
+    c = CONFIG_SPECS[cid]
+    N, V = c["n"], c["views"]
+    bp_mode = 0 if bp == "voxel" else 1
+    if c["solve"] == "sart":
+        vol = torch.zeros((N, N, N), device=dev)
+        state = torch.zeros(proj.shape[1:], device=dev)
+        it = [0]
+
+        def one():
+            ctx.sart_sweep(vol, proj, stt.permutation(1000 * cid + it[0], V), c["alpha"], gmax, bp_mode, state,
+                           stream=stream)
+            it[0] += 1
+        one()
+        t = _timed(stream, one, reps)
+        for _ in range(max(0, iters - 1 - reps)):
+            one()
+        launches = None
+        result = vol
+    else:
+        st = _pd_state(N, proj, dev)
+        sg, lam = c["sigma"], c["lam"]
+        pd = stt.PdParams(sigma=sg, tau=c["tau"], tv_w=lam, tp_w=0.0, bc_w=0.0,
+                          huber_factor=1.0 / (1.0 + sg * c["huber"] / lam), gmax=gmax, cut=c["roi"])
+        solver = stt.Solver(ctx, st, 1, V, pd, alpha=c["alpha"], bp_mode=bp_mode, roi_cut=c["roi"], seed=cid,
+                            mode=stt.SOLVE_GRAPH)
+
+        def one():
+            solver.iterate(1, stream)
+        one()
+        t = _timed(stream, one, reps)
+        for _ in range(max(0, iters - 1 - reps)):
+            one()
+        torch.cuda.synchronize()
+        solver.poll_status(stream)
+        launches = solver.stats()[0]
+        result = st["vol"][0]
+    torch.cuda.synchronize()
+    err = float((result - truth).norm() / truth.norm())
+    out = {"s_per_iter": t, "gups": N ** 3 * V / t / 1e9, "iterations_run": max(iters, 1 + reps),
+           "rel_l2_to_phantom": err, "launches_per_iter": launches}
+    if c["solve"] != "sart":
+        solver.close()
+    return out
+
+
+def fp_bp_split(ctx, c, vol, proj, gmax, dev, stream) -> dict:
+    """Per-view times of the fused forward projector (stt_fp_correction, which
+    also writes the z-fastest copy for x-dominant views) and of the two
+    backprojectors through the per-view ABI, the samples per view (the
+    reference's sample counts, stt_fp's weight output) and the FP roofline."""
+    import torch
+
+    N, D, V = c["n"], c["det"], c["views"]
+    nv = min(V, 32)
+    views = [int(v) for v in np.linspace(0, V - 1, nv)]
+    corr = torch.empty((D, D), device=dev)
+    rl = torch.zeros((D, D), device=dev)
+    for v in views[:3]:
+        ctx.fp_correction(vol, proj[v], rl, corr, v, stream=stream)
+    it = iter(views * 2)
+    t_fp = _timed(stream, lambda: (lambda v: ctx.fp_correction(vol, proj[v], rl, corr, v, stream=stream))(next(it)), nv)
+    scratch = vol.clone()
+    it = iter(views * 2)
+    t_bpv = _timed(stream, lambda: (lambda v: ctx.bp_voxel(corr, scratch, 0.3, gmax, v, stream=stream))(next(it)), nv)
+    it = iter(views * 2)
+    t_bpr = _timed(stream, lambda: (lambda v: ctx.bp_ray(corr, scratch, gmax, v, stream=stream))(next(it)), nv)
+    w = torch.zeros((4, D, D), device=dev)
+    img = torch.zeros((4, D, D), device=dev)
+    samples = 0.0
+    for k, v in enumerate(views[::max(1, nv // 4)][:4]):
+        ctx.fp(vol, img[k:k + 1], view0=v, nviews=1, weight=w[k:k + 1], stream=stream)
+    torch.cuda.synchronize()
+    samples = float(w.sum().item()) / 4
+    ctx.poll_status(stream)
+    del scratch
+    peak, peak_kind = peaks()
+    fp_bytes = 4 * N ** 3 + 12 * D * D
+    key = f"{N}x{D}"
+    traffic = None
+    if TRAFFIC_FILE.exists():
+        traffic = json.loads(TRAFFIC_FILE.read_text()).get(key)
+    return {"views_timed": nv, "fp_s_per_view": t_fp, "bp_voxel_s_per_view": t_bpv, "bp_ray_s_per_view": t_bpr,
+            "fp_gups": N ** 3 / t_fp / 1e9, "bp_voxel_gups": N ** 3 / t_bpv / 1e9, "bp_ray_gups": N ** 3 / t_bpr / 1e9,
+            "samples_per_view": samples, "fp_gsamples_per_s": samples / t_fp / 1e9,
+            "roofline": {"bound": "hbm", "kernel": "k_fp_corr / k_fp_corr_slab (forward projection + correction)",
+                         "achieved": fp_bytes / t_fp / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": fp_bytes / t_fp / 1e9 / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": fp_bytes, "traffic": traffic,
+                         "note": ("volume L2-resident (%.0f MiB < 126 MB L2)" % (4 * N ** 3 / 2 ** 20))
+                         if 4 * N ** 3 < 126e6 else "volume larger than L2: streamed from HBM every view"}}
+
+
+def config_e2e(cid, ctx, proj, gmax, dev, stream) -> dict:
+    """One step end to end: the step's inputs (sinogram, start volume) from
+    pinned host memory to the device, one iteration (voxel-based BP), the
+    volume back to pinned host memory; all inside the timed region."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+
+    c = CONFIG_SPECS[cid]
+    N, V = c["n"], c["views"]
+    hproj = proj.detach().cpu().pin_memory()
+    hvol = torch.zeros((N, N, N)).pin_memory()
+    hout = torch.empty((N, N, N)).pin_memory()
+    if c["solve"] == "sart":
+        vol = torch.empty((N, N, N), device=dev)
+        state = torch.zeros(proj.shape[1:], device=dev)
+        dproj = torch.empty_like(proj)
+
+        def step():
+            with torch.cuda.stream(stream):
+                dproj.copy_(hproj, non_blocking=True)
+                vol.copy_(hvol, non_blocking=True)
+                state.zero_()
+            ctx.sart_sweep(vol, dproj, stt.permutation(7, V), c["alpha"], gmax, 0, state, stream=stream)
+            with torch.cuda.stream(stream):
+                hout.copy_(vol, non_blocking=True)
+        step()
+        t = _timed(stream, step, 2)
+    else:
+        dproj = torch.empty_like(proj)
+        st = _pd_state(N, dproj, dev)
+        sg, lam = c["sigma"], c["lam"]
+        pd = stt.PdParams(sigma=sg, tau=c["tau"], tv_w=lam, tp_w=0.0, bc_w=0.0,
+                          huber_factor=1.0 / (1.0 + sg * c["huber"] / lam), gmax=gmax, cut=c["roi"])
+        solver = stt.Solver(ctx, st, 1, V, pd, alpha=c["alpha"], bp_mode=0, roi_cut=c["roi"], seed=cid,
+                            mode=stt.SOLVE_GRAPH)
+
+        def step():
+            with torch.cuda.stream(stream):
+                dproj.copy_(hproj, non_blocking=True)
+                st["vol"][0].copy_(hvol, non_blocking=True)
+                st["vol"][1].copy_(st["vol"][0])
+                st["xbar"].copy_(st["vol"])
+                for k in ("xprev", "ytv", "ytp", "ybc"):
+                    st[k].zero_()
+            solver.iterate(1, stream)
+            with torch.cuda.stream(stream):
+                hout.copy_(st["vol"][0], non_blocking=True)
+        step()
+        t = _timed(stream, step, 2)
+        solver.close()
+    return {"value": N ** 3 * V / t / 1e9, "unit": "GUPS", "h2d_bytes_per_step": hproj.numel() * 4 + hvol.numel() * 4,
+            "d2h_bytes_per_step": hout.numel() * 4, "s_per_step": t}
+
+
+def config_fp64_check(cid, ctx, truth, proj, gmax, dev, stream) -> dict:
+    """Error of the CUDA path against the FP64 oracle on a bounded sample at
+    the workload's full size: one SART sweep over a few views from the
+    phantom scaled by 0.8 (configs 1 and 2); at 512^3 (whose FP64 projection
+    of a 1024^2 view takes minutes on the host) the forward projection of a
+    64-row band of one view and the voxel backprojection of one view's
+    correction."""
+    import torch
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_bind as ob
+
+    c = CONFIG_SPECS[cid]
+    N, D, V = c["n"], c["det"], c["views"]
+    scan = ob.Scan(N, (D, D))
+    ang = np.arange(V) * (2 * math.pi / V)
+    threads = os.cpu_count() or 1
+    if N <= 256:
+        nv = 8 if N <= 128 else 3
+        order = [int(v) for v in np.linspace(0, V - 1, nv)]
+        v0 = (truth * 0.8).contiguous()
+        g = v0.clone()
+        state = torch.zeros((D, D), device=dev)
+        ctx.sart_sweep(g, proj, order, c["alpha"], gmax, 0, state, stream=stream)
+        torch.cuda.synchronize()
+        views = [ob.view_angle(a) for a in ang]
+        ref, _ = ob.sart64(scan, views, order, proj.cpu().numpy().astype(np.float64), c["alpha"], gmax, 0,
+                           v0.cpu().numpy().astype(np.float64), threads=threads)
+        return {"sart_rel_l2_vs_fp64": ob.rel_l2(g.cpu().numpy(), ref),
+                "sample": f"one SART sweep over {nv} of the {V} views from 0.8 x phantom, voxel-based BP"}
+    rows = slice(D // 2 - 32, D // 2 + 32)
+    v = V // 8  # an oblique view (45 degrees)
+    img = torch.zeros((1, D, D), device=dev)
+    ctx.fp(truth, img, view0=v, nviews=1, stream=stream)
+    torch.cuda.synchronize()
+    ref_band = ob.fp64_rows(scan, ob.view_angle(ang[v]), truth.cpu().numpy().astype(np.float64), rows.start,
+                            rows.stop - rows.start, threads=threads)
+    fp_err = ob.rel_l2(img[0, rows].cpu().numpy(), ref_band)
+    corr = torch.zeros((D, D), device=dev)
+    rl = torch.zeros((D, D), device=dev)
+    ctx.fp_correction((truth * 0.8).contiguous(), proj[v], rl, corr, v, stream=stream)
+    vol = (truth * 0.8).contiguous()
+    ctx.bp_voxel(corr, vol, c["alpha"], gmax, v, stream=stream)
+    torch.cuda.synchronize()
+    base = (truth * 0.8).cpu().numpy().astype(np.float64)
+    ref_vol = ob.bp_voxel64(scan, ob.view_angle(ang[v]), corr.cpu().numpy().astype(np.float64), c["alpha"], gmax,
+                            base.copy())
+    upd = vol.cpu().numpy().astype(np.float64) - base
+    bp_err = ob.rel_l2(upd, ref_vol - base)
+    return {"fp_band_rel_l2_vs_fp64": fp_err, "bp_voxel_update_rel_l2_vs_fp64": bp_err,
+            "sample": f"view {v} (45 deg): forward projection of detector rows {rows.start}-{rows.stop - 1}, and the "
+                      "voxel backprojection of its correction (the update it adds to 0.8 x phantom)"}
+
+
+def config_cpu_baseline(cid, args) -> dict:
+    """The reference's own SART call (10 views of FP + correction + voxel BP +
+    ROI mask, oracle/_ref) timed on the host cores at a bounded size, scaled to
+    one iteration of the workload: at 128^3 and 256^3 at the workload's own
+    size; at 512^3 / 1024^2 at 256^3 / 512^2, scaled by 8 (the per-view work
+    of both the projector, W*H rays of N/sd samples, and the voxel
+    backprojection, N^3 voxels, grows 8-fold)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_bind as ob
+
+    c = CONFIG_SPECS[cid]
+    if ob.REF_ST is None:
+        return None
+    ph = phantom_module()
+    N, D = (c["n"], c["det"]) if c["n"] <= 256 else (256, 512)
+    scale = 1.0 if c["n"] <= 256 else 8.0
+    threads = os.cpu_count() or 1
+    dims = (N, N, N)
+    vol = ph.ellipsoid_phantom(dims, c["ellipsoids"], seed=100 + cid, semi=(5.0 * N / 256, 40.0 * N / 256)).numpy()
+    scan = ob.Scan(N, (D, D))
+    views = [ob.view_round(13.0, k) for k in range(REF_SART_VIEWS)]
+    proj = np.stack([ob.fp32(scan, v, vol, gmode=0, threads=threads)[0] for v in views])
+    with c_stdout_to_stderr():
+        out = ob.ref_st_run(scan, [[13.0]], proj[None], vol[None], np.zeros((1, 3) + vol.shape, np.float32),
+                            bp_mode=0, alpha=c["alpha"], cut=(8, 8, 8, 45, 8, 8, 30, 20), mode=0, threads=threads,
+                            full=False)
+    t_iter = out["seconds"] * scale * c["views"] / REF_SART_VIEWS
+    return {"value": c["n"] ** 3 * c["views"] / t_iter / 1e9, "unit": "GUPS", "cores": threads, "kind": "reference",
+            "sample": f"the reference's ST_Tomography::SART over {REF_SART_VIEWS} views at {N}^3 / {D}^2 "
+                      f"(oracle/_ref), {threads} OpenMP threads, scaled to {c['views']} views"
+                      + (" and by 8 to 512^3 / 1024^2" if scale != 1.0 else "")
+                      + ("; the primal-dual steps (under 1 % of the iteration on the host) are not in the sample"
+                         if c["solve"] == "pd" else ""),
+            "s_per_iter": t_iter}
+
+
+def config_bench(cid, args, dev, stream, rank=0, full=False) -> dict:
+    """The line of one single-frame workload (see CONFIG_SPECS).  full: run
+    the whole configured solve per variant; otherwise a warm-up and two timed
+    iterations (as the default run's sub-line)."""
+    import torch
+
+    c = CONFIG_SPECS[cid]
+    N, D, V = c["n"], c["det"], c["views"]
+    ctx, truth, proj, gmax = config_problem(cid, dev)
+    out = {"config": {"workload": c["workload"], "volume": [N] * 3, "detector": [D, D], "views": V,
+                      "iterations": c["iters"], "data": "synthetic (seeded phantom)"},
+           "metric": "projector GUPS over one iteration", "unit": "GUPS", "dtype": "f32", "variants": {}}
+    reps = 3 if N <= 256 else 2
+    for bp in c["bps"]:
+        out["variants"][f"f32_{bp}"] = config_solve(cid, ctx, proj, truth, gmax, bp, dev, stream,
+                                                    c["iters"] if full else 1 + reps, reps)
+        torch.cuda.empty_cache()
+    out["value"] = out["variants"]["f32_voxel"]["gups"]
+    out["ms_per_step"] = 1000.0 * out["variants"]["f32_voxel"]["s_per_iter"]
+    split = fp_bp_split(ctx, c, (truth * 0.8).contiguous(), proj, gmax, dev, stream)
+    out["roofline"] = split.pop("roofline")
+    out["fp_bp"] = split
+    out["e2e"] = config_e2e(cid, ctx, proj, gmax, dev, stream)
+    if rank == 0 and not args.no_cpu:
+        out["fp64_check"] = config_fp64_check(cid, ctx, truth, proj, gmax, dev, stream)
+        out["cpu_baseline"] = config_cpu_baseline(cid, args)
+    ctx.close()
+    del truth, proj
+    torch.cuda.empty_cache()
+    return out
+
+
+def fp_probe(cid, dev, stream) -> None:
+    """A few fused forward projections at the workload's size and nothing else
+    (the command ncu captures for the roofline's traffic at that size)."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200 import phantom as ph
+
+    c = CONFIG_SPECS[cid]
+    N, D, V = c["n"], c["det"], c["views"]
+    ctx = stt.Context(dev.index or 0)
+    ctx.set_geometry((N, N, N), (1.0, 1.0, 1.0), (D, D), 1.0, 600.0, 1000.0, ph.equispaced_views(V))
+    vol = ph.rasterize(ph.ellipsoid_params(c["ellipsoids"], (N, N, N), seed=100 + cid,
+                                           semi=(5.0 * N / 256, 40.0 * N / 256)), (N, N, N), dev)
+    b = torch.zeros((D, D), device=dev)
+    rl = torch.zeros((D, D), device=dev)
+    corr = torch.zeros((D, D), device=dev)
+    for v in (0, V // 8, V // 4, 3 * V // 8):  # 0, 45, 90, 135 degrees
+        ctx.fp_correction(vol, b, rl, corr, v, stream=stream)
+    torch.cuda.synchronize()
+    ctx.poll_status(stream)
+    ctx.close()
+
+
+def run_config_only(args) -> int:
+    import torch
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    if args.fp_probe:
+        fp_probe(args.config, dev, stream)
+        return 0
+    clocks = ClockSampler(0)
+    clocks.start()
+    out = config_bench(args.config, args, dev, stream, full=True)
+    clk = clocks.stop()
+    line = {"metric": out["metric"], "value": out["value"], "unit": "GUPS", "n_gpus": 1, "steps": None,
+            "warmup": 1, "ms_per_step": out["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "clocks": clk,
+            **{k: v for k, v in out.items() if k not in ("metric", "value", "ms_per_step", "unit", "dtype")}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     """The reference arm: the reference's own CPU code on this host's cores (see
     cpu_reference_sample).  A step is one bounded sample; ms_per_step is its
@@ -578,13 +982,16 @@ def run_stt(args):
         plain = p0.elapsed_time(p1) / 1000.0
         sp.close()
 
-    # ---- end to end through the C ABI with host buffers ----
-    # Every step uploads its inputs (volume, flow, projections) from pinned
-    # host memory and reads its result back.  On one GPU the steps alternate
-    # between two state sets and two solvers, so step i+1's upload and step
-    # i-1's read-back run on copy streams while step i computes; every copy is
-    # still inside the timed region.
-    host = {k: st[k].detach().cpu().pin_memory() for k in ("vol", "flow", "proj")}
+    # ---- end to end with host buffers ----
+    # Every step uploads its inputs (volumes, flows, projections) from pinned
+    # host memory and reads its result back.  On one GPU this goes through the
+    # host-buffer entry points of include/stt_host.h (stt_host_solver_*, the
+    # call a host application makes): two slots, so step i+1's upload and step
+    # i-1's read-back overlap step i's compute; every copy, the pipeline's fill
+    # and its drain are inside the timed region (between two device events,
+    # the host having waited for every step).
+    host = {"vol": st["vol"][:F].detach().cpu().pin_memory(), "flow": st["flow"].detach().cpu().pin_memory(),
+            "proj": st["proj"].detach().cpu().pin_memory()}
     h2d = sum(v.numel() * 4 for v in host.values())
     d2h = st["vol"][:F].numel() * 4
     ksteps = max(1, min(args.steps, 3))
@@ -595,48 +1002,27 @@ def run_stt(args):
             s_[k_].zero_()
 
     if world == 1:
-        st2 = {k: torch.zeros_like(v) for k, v in st.items()}
-        solver2 = stt.Solver(ctx, st2, F, V, pd, alpha=0.3, bp_mode=bp_mode, seed=99, mode=stt.SOLVE_GRAPH)
-        sets = [(st, solver), (st2, solver2)]
+        from spacetimetomography_b200.host import HostSolver
+
+        hs = HostSolver((N, N, N), (1.0, 1.0, 1.0), (args.det, args.det), 1.0, 600.0, 1000.0, angles_for(args, 0),
+                        F, V, pd, alpha=0.3, bp_mode=bp_mode, seed=99, slots=2, device=local)
         outs = [torch.empty_like(st["vol"][:F], device="cpu").pin_memory() for _ in range(2)]
-        up, down = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
-        ev = {k: [torch.cuda.Event() for _ in range(2)] for k in ("free", "uploaded", "computed")}
-        for b in range(2):
-            ev["free"][b].record(down)
-
-        def e2e_step_pipe(i):
-            b = i % 2
-            s_, sol = sets[b]
-            up.wait_event(ev["free"][b])
-            with torch.cuda.stream(up):
-                for k_, v_ in host.items():
-                    s_[k_].copy_(v_, non_blocking=True)
-            ev["uploaded"][b].record(up)
-            stream.wait_event(ev["uploaded"][b])
-            with torch.cuda.stream(stream):
-                reset_duals(s_)
-            sol.iterate(1, stream)
-            ev["computed"][b].record(stream)
-            down.wait_event(ev["computed"][b])
-            with torch.cuda.stream(down):
-                outs[b].copy_(s_["vol"][:F], non_blocking=True)
-            ev["free"][b].record(down)
-
-        for i in range(2):  # untimed: the second solver's graph is captured here
-            e2e_step_pipe(i)
-        torch.cuda.synchronize()
+        for i in range(2):  # untimed: both slots capture their graphs here
+            hs.submit(host["vol"], host["flow"], host["proj"], 1, outs[i % 2])
+        while hs.pending():
+            hs.wait()
         q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ksteps = max(1, args.steps)  # the pipeline's fill and drain are inside the timed region
-        q0.record(up)
+        ksteps = max(1, args.steps)
+        torch.cuda.synchronize()
+        q0.record(stream)
         for i in range(ksteps):
-            e2e_step_pipe(i)
-        up.wait_stream(down)
-        up.wait_stream(stream)
-        q1.record(up)
+            hs.submit(host["vol"], host["flow"], host["proj"], 1, outs[i % 2])
+        while hs.pending():
+            hs.wait()
+        q1.record(stream)
         torch.cuda.synchronize()
         te = q0.elapsed_time(q1) / 1000.0
-        solver2.close()
-        del st2
+        hs.close()
     else:
         out_host = torch.empty_like(st["vol"][:F], device="cpu").pin_memory()
 
@@ -666,6 +1052,16 @@ def run_stt(args):
 
     flow = None if args.no_flow else flow_bench(args, dev, stream, rank)
 
+    # the single-frame workloads, one sub-line each (rank 0, one GPU)
+    configs = None
+    if not args.no_configs and world == 1:
+        configs = {}
+        for cid in sorted(CONFIG_SPECS):
+            try:
+                configs[str(cid)] = config_bench(cid, args, dev, stream, rank)
+            except Exception as e:  # a failing sub-line must not cost the headline line
+                configs[str(cid)] = {"error": f"{type(e).__name__}: {e}"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         check = fp64_sart_check(ctx, st, args, gmax)
@@ -687,6 +1083,8 @@ def run_stt(args):
                              "algorithmic_bytes_per_launch": fp_bytes, "launch_s": t_fp,
                              "note": "volume is L2-resident; the kernel is bound by gather (L1/L2) throughput"},
                 "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "through": ("stt_host_solver_submit/_wait (include/stt_host.h), 2 slots" if world == 1
+                                    else "torch pinned copies around the sharded solver"),
                         "steps": ksteps},
                 "gpu_launches": launches_per_iter * args.steps,
                 "launches_per_iter": launches_per_iter,
@@ -694,7 +1092,8 @@ def run_stt(args):
                 "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "cpu_s_per_iter": None if cpu is None else cpu["s_per_iter"],
                 "fp64_check": None if cpu is None else cpu.get("fp64_check"),
-                "flow": flow}
+                "flow": flow,
+                "configs": configs}
         print(json.dumps(line), flush=True)
     solver.close()
     ctx.close()
@@ -802,6 +1201,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config is not None:
+        return run_config_only(args)
     if args.flow_only:
         return run_flow_only(args)
     if args.batch_only:

@@ -389,6 +389,10 @@ stt_status stt_solver_iterate(stt_solver *s, int n_iters, void *stream);
  * SART, ROI mask and over-relaxation.  Phase 0 then phase 1 equals one
  * stt_solver_iterate step; sharded solves exchange halos in between. */
 stt_status stt_solver_iterate_phase(stt_solver *s, int phase, void *stream);
+/* Makes the next iteration iteration number `iter` (its view orders are those
+ * of that iteration); 0 restarts the sequence of orders.  Enqueued on
+ * `stream` (iterations enqueued after it on that stream see it). */
+stt_status stt_solver_set_iteration(stt_solver *s, unsigned long long iter, void *stream);
 /* Kernel launches per iteration and iterations run so far. */
 stt_status stt_solver_stats(const stt_solver *s, long long *launches_per_iter,
                             unsigned long long *iterations);

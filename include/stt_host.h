@@ -61,6 +61,41 @@ int stt_analyze_read(const char *hdr_path, int *w, int *h, int *d, int *c, float
 
 void stt_host_free(void *p);
 
+/* ---- the space-time primal-dual solve on host buffers ---------------------
+ * Replaces ST_Tomography::Render's image phase (S/ST_Tomo/ST_Tomography.cpp:
+ * 475-607: per frame the backward warp and dual step, the forward warp and
+ * primal step, SART(f), the ROI mask and the over-relaxation), for callers
+ * whose volumes, flows and projections live in host memory, as they do in the
+ * reference (CImg lists, VolumeData.h:97-98, ST_Tomography.cpp:355).
+ *
+ * stt_host_solver_create: geometry and solve configuration as for
+ * stt_set_geometry / stt_solver_create (cfg->halo must be 0; use
+ * STT_SOLVE_GRAPH); `slots` (1..8) complete copies of the device state are
+ * allocated on the current stt_host_set_device device, so that with 2 slots a
+ * step's upload and the previous step's read-back overlap a step's compute.
+ *
+ * stt_host_solver_submit: one step on the next slot (waiting first for that
+ * slot's previous step if it is still pending): uploads vol (F volumes, x
+ * fastest; the last is duplicated on the device as VolumeData.cpp:124-126
+ * does), flow (F x 3 planar volumes) and proj (F x V images, view-major),
+ * sets X_bar = vol and zero duals, runs n_iters iterations from the first
+ * view order, and copies the F volumes back into vol_out (HOST, may be NULL).
+ * It only enqueues: the host buffers must stay valid and vol_out unread until
+ * stt_host_solver_wait has completed the step.  Page-locked buffers
+ * (cudaHostAlloc / cudaHostRegister) make the copies asynchronous.
+ *
+ * stt_host_solver_wait: completes the oldest pending step (its vol_out is
+ * filled); returns STT_ERR_TIMEOUT if a bounded device-side wait of that step
+ * gave up (see stt_poll_status).  stt_host_solver_pending: steps submitted and
+ * not yet waited for. */
+typedef struct stt_host_solver stt_host_solver;
+int stt_host_solver_create(const stt_geometry *g, const stt_solve_cfg *cfg, int slots, stt_host_solver **out);
+int stt_host_solver_submit(stt_host_solver *h, const float *vol, const float *flow, const float *proj, int n_iters,
+                           float *vol_out);
+int stt_host_solver_wait(stt_host_solver *h);
+int stt_host_solver_pending(const stt_host_solver *h);
+int stt_host_solver_destroy(stt_host_solver *h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -479,15 +479,16 @@ void set_threads(int n) {
 // GenerateImage_MT (TypicalRayProducer.core.h:123-225) for one view.
 template <typename R>
 int fp_impl(const orc_geom &g, int gmode, const orc_view &v, const R *vol, R *img, R *raylen,
-            R *weight) {
+            R *weight, int j0 = 0, int j1 = -1) {
     const int dims[3] = {g.nx, g.ny, g.nz};
     View32 V32;
     View64 V64;
     if (gmode == 0) make_view32(g, v, V32);
     else make_view64(g, v, V64);
     const R sd = sample_distance<R>(g);
+    if (j1 < 0 || j1 > g.H) j1 = g.H;
 #pragma omp parallel for schedule(dynamic, 4)
-    for (int j = 0; j < g.H; ++j) {
+    for (int j = j0; j < j1; ++j) {
         for (int i = 0; i < g.W; ++i) {
             long pix = i + (long)j * g.W;
             RaySetup<R> rs;
@@ -1410,6 +1411,13 @@ int orc_fp_f32(const orc_geom *g, int gmode, const orc_view *v, const float *vol
                float *raylen, float *weight, int nthreads) {
     set_threads(nthreads);
     return fp_impl<float>(*g, gmode, *v, vol, img, raylen, weight);
+}
+
+int orc_fp_rows_f64(const orc_geom *g, const orc_view *v, const double *vol, int row0, int row1, double *img,
+                    int nthreads) {
+    set_threads(nthreads);
+    if (row0 < 0 || row1 < row0) return -1;
+    return fp_impl<double>(*g, 1, *v, vol, img, nullptr, nullptr, row0, row1);
 }
 
 int orc_fp_f64(const orc_geom *g, const orc_view *v, const double *vol, double *img,

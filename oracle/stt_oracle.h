@@ -52,6 +52,12 @@ int orc_fp_f32(const orc_geom *g, int gmode, const orc_view *v, const float *vol
 int orc_fp_f64(const orc_geom *g, const orc_view *v, const double *vol,
                double *img, double *raylen, double *weight, int nthreads);
 
+/* orc_fp_f64 on detector rows [row0, row1) only (img is the full W*H image;
+ * other rows are left as they are): a band of a view whose full FP64
+ * projection would take minutes. */
+int orc_fp_rows_f64(const orc_geom *g, const orc_view *v, const double *vol, int row0, int row1,
+                    double *img, int nthreads);
+
 /* Ray-driven BP scatter (SingleScalarVolume.core.h:73-84,128-143): adds
  * c[pix]*w to contrib and w to wsum, sequentially in pixel order. */
 int orc_bp_ray_scatter_f32(const orc_geom *g, int gmode, const orc_view *v,

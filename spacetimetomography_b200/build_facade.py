@@ -26,7 +26,7 @@ LIB = PKG / "libstt.so"
 FACADE_LIB = PKG / "libstt_facade.so"
 CLI = PKG / "bin" / "st_tomography"
 CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
-LIB_SOURCES = ["host_api.cpp", "tiff_io.cpp", "reference_api.cpp"]
+LIB_SOURCES = ["host_api.cpp", "host_solver.cpp", "tiff_io.cpp", "reference_api.cpp"]
 CLI_SOURCES = ["st_tomography_main.cpp"]
 
 

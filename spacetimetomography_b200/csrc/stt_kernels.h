@@ -69,6 +69,8 @@ cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, c
 
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                             float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex = 0);
+// Sets the solver's device-side iteration counter (stream-ordered, no host memory read).
+cudaError_t launch_set_counter(unsigned long long *counter, unsigned long long v, cudaStream_t s);
 // View orders of `frames` local frames (at most 1024), local frame f being
 // frame frame0 + f of a sequence of `total`; advances *counter.
 cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counter, int frames, int total,

@@ -75,6 +75,13 @@ cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counte
     return cudaGetLastError();
 }
 
+__global__ void k_set_counter(unsigned long long *counter, unsigned long long v) { *counter = v; }
+
+cudaError_t launch_set_counter(unsigned long long *counter, unsigned long long v, cudaStream_t s) {
+    k_set_counter<<<1, 1, 0, s>>>(counter, v);
+    return cudaGetLastError();
+}
+
 void host_perm(unsigned long long seed, unsigned long long iter, int frames, int f, int views, int *p) {
     for (int i = 0; i < views; ++i) p[i] = i;
     unsigned long long s = frame_seed(seed, iter, frames, f);
@@ -561,6 +568,13 @@ stt_status stt_solver_iterate_phase(stt_solver *s, int phase, void *stream) {
     if (st) return st;
     s->phase_launches[phase] = nl;
     s->launches_per_iter = s->phase_launches[0] + s->phase_launches[1];
+    return STT_OK;
+}
+
+stt_status stt_solver_set_iteration(stt_solver *s, unsigned long long iter, void *stream) {
+    if (!s) return STT_ERR_INVALID;
+    s->host_iter = iter;
+    SCUDA(s, stt::launch_set_counter(s->counter, iter, reinterpret_cast<cudaStream_t>(stream)), "counter update");
     return STT_OK;
 }
 

@@ -74,26 +74,32 @@ def rasterize(params, dims, device="cpu", background=None):
     return vol
 
 
-def porous_background(dims, seed: int, count: int, radius=(2.0, 6.0), density=0.5, device="cpu"):
-    """Uniform-random spheres of the given density (the 512^3 workload's background)."""
+def porous_background(dims, seed: int, count: int, radius=(2.0, 6.0), density=0.5, device="cpu",
+                      chunk: int = 4096):
+    """Uniform-random spheres of the given density (the 512^3 workload's
+    background): `count` centres uniform over the volume, radii uniform in
+    `radius`; a voxel whose centre lies in any sphere gets `density`.  The
+    spheres are rasterised `chunk` at a time over their bounding boxes."""
     import torch
 
     rng = np.random.default_rng(seed)
     nx, ny, nz = dims
-    bg = torch.zeros((nz, ny, nx), dtype=torch.float32, device=device)
-    for _ in range(count):
-        c = rng.uniform([0, 0, 0], [nx - 1, ny - 1, nz - 1])
-        r = rng.uniform(*radius)
-        lo = [max(0, int(c[k] - r - 1)) for k in range(3)]
-        hi = [min(dims[k], int(c[k] + r + 2)) for k in range(3)]
-        Z, Y, X = torch.meshgrid(torch.arange(lo[2], hi[2], device=device, dtype=torch.float32),
-                                 torch.arange(lo[1], hi[1], device=device, dtype=torch.float32),
-                                 torch.arange(lo[0], hi[0], device=device, dtype=torch.float32),
-                                 indexing="ij")
-        ins = (X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 <= r * r
-        bg[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] = torch.where(
-            ins, torch.full_like(X, density), bg[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]])
-    return bg
+    centres = rng.uniform([0, 0, 0], [nx - 1, ny - 1, nz - 1], (count, 3))
+    radii = rng.uniform(radius[0], radius[1], count)
+    bg = torch.zeros(nz * ny * nx, dtype=torch.float32, device=device)
+    rmax = int(math.ceil(radius[1])) + 1
+    o = torch.arange(-rmax, rmax + 1, device=device, dtype=torch.float32)
+    oz, oy, ox = torch.meshgrid(o, o, o, indexing="ij")
+    offs = torch.stack([ox.reshape(-1), oy.reshape(-1), oz.reshape(-1)], 1)  # (K, 3) integer offsets
+    lim = torch.tensor([nx - 1, ny - 1, nz - 1], device=device, dtype=torch.float32)
+    for s in range(0, count, chunk):
+        c = torch.as_tensor(centres[s:s + chunk], device=device, dtype=torch.float32)
+        r = torch.as_tensor(radii[s:s + chunk], device=device, dtype=torch.float32)
+        p = torch.floor(c)[:, None, :] + offs[None]  # (m, K, 3) voxel centres around each sphere
+        inside = (((p - c[:, None, :]) ** 2).sum(-1) <= (r * r)[:, None]) & (p >= 0).all(-1) & (p <= lim).all(-1)
+        q = p[inside].long()
+        bg[q[:, 0] + nx * (q[:, 1] + ny * q[:, 2])] = density
+    return bg.view(nz, ny, nx)
 
 
 def ellipsoid_phantom(dims, n: int, seed: int, semi=(5.0, 40.0), device="cpu"):

@@ -47,6 +47,7 @@ O.orc_view_from_round.argtypes = [_d, _i, C.POINTER(OView)]
 O.orc_view_from_angle.argtypes = [_d, C.POINTER(OView)]
 O.orc_fp_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp, _vp, _vp, _i]
 O.orc_fp_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp, _vp, _vp, _i]
+O.orc_fp_rows_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _i, _i, _vp, _i]
 O.orc_bp_ray_scatter_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp, _vp]
 O.orc_fp_adjoint_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp]
 O.orc_fp_adjoint_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp]
@@ -173,6 +174,17 @@ def fp64(scan: Scan, view: OView, vol: np.ndarray, threads: int = 0):
     O.orc_fp_f64(C.byref(g), C.byref(view), P(np.ascontiguousarray(vol, np.float64)), P(img), P(rl),
                  P(wt), threads)
     return img, rl, wt
+
+
+def fp64_rows(scan: Scan, view: OView, vol: np.ndarray, row0: int, nrows: int, threads: int = 0):
+    """FP64 projection of detector rows [row0, row0 + nrows) only: (nrows, W)."""
+    W, H = scan.det
+    img = np.zeros((H, W), np.float64)
+    g = scan.ogeom()
+    if O.orc_fp_rows_f64(C.byref(g), C.byref(view), P(np.ascontiguousarray(vol, np.float64)), row0, row0 + nrows,
+                         P(img), threads) != 0:
+        raise ValueError("bad row range")
+    return img[row0:row0 + nrows].copy()
 
 
 def ref_fp(scan: Scan, start_deg: float, k: int, vol: np.ndarray, threads: int = 0):

@@ -244,3 +244,13 @@ def test_flow_multiscale_matches_live_reference_with_tolerance_stop():
         a = ob.flow_multiscale32(i1, i2, v0, cut, tol=tol, max_iter=mi, n_warps=2, scales=2, eta=0.7)
         b = ob.ref_flow_multiscale(i1, i2, v0, cut, tol=tol, max_iter=mi, n_warps=2, scales=2, eta=0.7)
         np.testing.assert_array_equal(a, b)
+
+
+def test_fp64_row_band_equals_the_full_projection():
+    """The band projection used to check 1024^2 views is the full FP64
+    projection restricted to its rows."""
+    s = ob.Scan((20, 18, 16), (24, 20), spacing=1.1, off=(0.5, -0.3, 0.8))
+    vol = np.random.default_rng(4).uniform(0, 1, (16, 18, 20))
+    v = ob.view_angle(0.7)
+    full = ob.fp64(s, v, vol)[0]
+    np.testing.assert_array_equal(ob.fp64_rows(s, v, vol, 5, 7), full[5:12])
