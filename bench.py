@@ -778,6 +778,7 @@ def config_bench(cid, args, dev, stream, rank=0, full=False) -> dict:
                       "iterations": c["iters"], "data": "synthetic (seeded phantom)"},
            "metric": "projector GUPS over one iteration", "unit": "GUPS", "dtype": "f32", "variants": {}}
     reps = 3 if N <= 256 else 2
+    out["tuning"] = ctx.autotune(stream)  # the launch choices for this geometry (untimed)
     for bp in c["bps"]:
         out["variants"][f"f32_{bp}"] = config_solve(cid, ctx, proj, truth, gmax, bp, dev, stream,
                                                     c["iters"] if full else 1 + reps, reps)
@@ -908,8 +909,10 @@ def run_stt(args):
     halo = HaloExchange(rank, world, st, dist) if world > 1 else None
 
     def make_solver(mode):
+        # the first solver tunes the context's launch choices (outside any timed region)
         return stt.Solver(ctx, st, F, V, pd, alpha=0.3, bp_mode=bp_mode, seed=99, mode=mode,
-                          halo=(halo is not None and rank > 0), frame_offset=rank * F, total_frames=world * F)
+                          halo=(halo is not None and rank > 0), frame_offset=rank * F, total_frames=world * F,
+                          autotune=True)
 
     solver = make_solver(stt.SOLVE_GRAPH)
 
@@ -1088,6 +1091,7 @@ def run_stt(args):
                         "steps": ksteps},
                 "gpu_launches": launches_per_iter * args.steps,
                 "launches_per_iter": launches_per_iter,
+                "tuning": ctx.get_tuning(),
                 "clocks": clk,
                 "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "cpu_s_per_iter": None if cpu is None else cpu["s_per_iter"],
@@ -1152,18 +1156,28 @@ def run_batch_only(args):
                          truth=truth))
         units += n ** 3 * V
     stream = torch.cuda.Stream(device=dev)
-    b = stt.Batch(inst, mode=stt.SOLVE_GRAPH)
-    for _ in range(args.warmup):
-        b.iterate(1, stream)
-    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        b.iterate(1, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_batch = e0.elapsed_time(e1) / 1000.0 / args.steps
-    b.close()
+
+    def batched_time():
+        for d in inst:
+            d["vol"].zero_()
+        b = stt.Batch(inst, mode=stt.SOLVE_GRAPH)
+        for _ in range(args.warmup):
+            b.iterate(1, stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.iterate(1, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        b.close()
+        return e0.elapsed_time(e1) / 1000.0 / args.steps
+
+    t_default = batched_time()  # the default launch choices
+    t0 = time.perf_counter()
+    choices = [d["ctx"].autotune(stream) for d in inst]  # every instance's own geometry
+    t_tune = time.perf_counter() - t0
+    t_batch = batched_time()
     # the same instances one after another (each its own graph-captured solver)
     solvers = []
     for d in inst:
@@ -1190,7 +1204,16 @@ def run_batch_only(args):
             "config": {"workload": f"{args.batch_instances} single-frame TV + SART instances, cubes 64^3-192^3, "
                                    "detectors 128^2-384^2, 60-240 views, voxel-based BP"},
             "sequential_ms_per_iter": 1000 * t_seq, "batched_vs_sequential": t_seq / t_batch,
-            "rel_l2_to_phantom_first4": errs}
+            "rel_l2_to_phantom_first4": errs,
+            "autotune": {"batched_ms_per_iter_default_choices": 1000 * t_default,
+                         "batched_ms_per_iter_tuned": 1000 * t_batch, "tuned_vs_default": t_default / t_batch,
+                         "tuning_s_all_instances": t_tune,
+                         "cache_hits": sum(c["from_cache"] for c in choices),
+                         "fp_variant_counts": np.bincount([c["fp_variant"] for c in choices], minlength=7).tolist(),
+                         "slab_variant_counts": np.bincount([c["slab_variant"] for c in choices], minlength=4).tolist(),
+                         "bp_variant_counts": np.bincount([c["bp_variant"] for c in choices], minlength=3).tolist(),
+                         "first_instances": [{k: c[k] for k in ("fp", "slab", "bp", "staged_bins")}
+                                             for c in choices[:4]]}}
     print(json.dumps(line), flush=True)
     for sv, _ in solvers:
         sv.close()

@@ -106,8 +106,48 @@ stt_status stt_views_from_rounds(int rounds, const double *start_deg, int views_
  * base p, Ns segments, a reference angle 0 every Nz entries.  out (host) gets n values. */
 stt_status stt_lds_angles(int n, int Ns, int p, int Nz, double *out);
 
-/* Set (or replace) the geometry and view list. Allocates the context's device tables. */
+/* Set (or replace) the geometry and view list. Allocates the context's device
+ * tables and resets the launch choices below to their defaults. */
 stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g);
+
+/* ---- launch choices and the autotuner ------------------------------------
+ * No counterpart in the reference (a CPU program with fixed OpenMP loops
+ * over detector rows, TypicalRayProducer.core.h:168, and voxels,
+ * ST_Tomography.cpp:690).  The forward projector with the SART correction
+ * (stt_fp_correction, stt_sart_sweep, the solver) and the solver's voxel
+ * backprojection come in launch variants that give the same bits:
+ *   fp_variant   the gather projector's detector tile and samples in flight;
+ *   slab_variant the box the slab-staged projector stages with TMA;
+ *   bp_variant   the column length of the voxel backprojection (solver);
+ *   staged_bins  bit b set: views whose central ray is 5b to 5b+5 degrees off
+ *                the nearest of the x and z axes (bit 8: 40 to 45) are
+ *                projected by the slab-staged kernel, the others by the gather
+ *                kernel (the slab form needs x and z extents that are multiples
+ *                of 4 and a 16-byte aligned volume; elsewhere every view gathers).
+ * stt_autotune times every variant with CUDA events on this context's
+ * geometry (one representative view per off-axis class, weighted by the views
+ * in the class; scratch volumes it allocates and frees), keeps the fastest,
+ * and caches the choice per device and geometry shape for later contexts.  It
+ * synchronises `stream` and rewrites the context's view table, so call it
+ * (and stt_set_tuning) while no launch of this context is in flight; launches
+ * enqueued after it use the choice, and a solver uses the choice current when
+ * it is created (stt_solve_cfg.autotune runs the tuner then).  out (may be
+ * NULL) receives the choice and the timings (microseconds per launch, 0 where
+ * a variant was not timed).  stt_get_tuning reads the current choice;
+ * stt_set_tuning sets one (a variant out of range is STT_ERR_INVALID). */
+typedef struct stt_tuning {
+    int fp_variant, slab_variant, bp_variant;
+    unsigned staged_bins;
+    int tuned;       /* 0: the defaults; 1: set by stt_autotune or stt_set_tuning */
+    int from_cache;  /* stt_autotune: the choice came from the cache (nothing timed) */
+    float fp_us[8], slab_us[8], bp_us[4];
+} stt_tuning;
+stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream);
+stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out);
+stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t);
+/* Description of variant `variant` of kernel `kernel` (0 gather projector,
+ * 1 slab-staged projector, 2 voxel backprojection); NULL when out of range. */
+const char *stt_tuning_variant_name(int kernel, int variant);
 
 /* ---- forward projector (TypicalRayProducer.core.h:123-268) ---------------
  * Projects views [view0, view0+nviews) of `vol`.
@@ -370,6 +410,9 @@ typedef struct stt_solve_cfg {
      * shards draw the orders the unsharded solve would. */
     int frame_offset;
     int total_frames;
+    /* Non-zero: stt_solver_create runs stt_autotune on the context first
+     * (unless it is tuned already). */
+    int autotune;
 } stt_solve_cfg;
 
 typedef struct stt_pd_state {
@@ -426,6 +469,7 @@ typedef struct stt_instance {
     stt_pd_params pd;     /* sigma, tau, tv_w, huber_factor, gmax, cut (tp_w, bc_w ignored) */
     int roi_cut[8];
     unsigned long long seed;
+    int autotune;         /* non-zero: tune the instance's context at stt_batch_create (stt_autotune) */
 } stt_instance;
 
 typedef struct stt_batch stt_batch;

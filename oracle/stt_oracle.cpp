@@ -1420,6 +1420,13 @@ int orc_fp_rows_f64(const orc_geom *g, const orc_view *v, const double *vol, int
     return fp_impl<double>(*g, 1, *v, vol, img, nullptr, nullptr, row0, row1);
 }
 
+int orc_fp_rows_f32(const orc_geom *g, int gmode, const orc_view *v, const float *vol, int row0, int row1,
+                    float *img, int nthreads) {
+    set_threads(nthreads);
+    if (row0 < 0 || row1 < row0) return -1;
+    return fp_impl<float>(*g, gmode, *v, vol, img, nullptr, nullptr, row0, row1);
+}
+
 int orc_fp_f64(const orc_geom *g, const orc_view *v, const double *vol, double *img,
                double *raylen, double *weight, int nthreads) {
     set_threads(nthreads);

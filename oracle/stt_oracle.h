@@ -57,6 +57,9 @@ int orc_fp_f64(const orc_geom *g, const orc_view *v, const double *vol,
  * projection would take minutes. */
 int orc_fp_rows_f64(const orc_geom *g, const orc_view *v, const double *vol, int row0, int row1,
                     double *img, int nthreads);
+/* The same band in the reference's FP32 arithmetic (orc_fp_f32). */
+int orc_fp_rows_f32(const orc_geom *g, int gmode, const orc_view *v, const float *vol, int row0, int row1,
+                    float *img, int nthreads);
 
 /* Ray-driven BP scatter (SingleScalarVolume.core.h:73-84,128-143): adds
  * c[pix]*w to contrib and w to wsum, sequentially in pixel order. */

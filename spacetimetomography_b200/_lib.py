@@ -42,7 +42,7 @@ class SolveCfg(C.Structure):
     _fields_ = [("n_frames", C.c_int), ("views_per_frame", C.c_int), ("bp_mode", C.c_int),
                 ("alpha", C.c_double), ("pd", PdParams), ("roi_cut", C.c_int * 8),
                 ("seed", C.c_ulonglong), ("mode", C.c_int), ("halo", C.c_int), ("frame_offset", C.c_int),
-                ("total_frames", C.c_int)]
+                ("total_frames", C.c_int), ("autotune", C.c_int)]
 
 
 class PdState(C.Structure):
@@ -66,7 +66,14 @@ class OpNorm(C.Structure):
 class Instance(C.Structure):
     _fields_ = [("ctx", C.c_void_p), ("vol", C.c_void_p), ("proj", C.c_void_p), ("n_views", C.c_int),
                 ("bp_mode", C.c_int), ("alpha", C.c_double), ("pd", PdParams), ("roi_cut", C.c_int * 8),
-                ("seed", C.c_ulonglong)]
+                ("seed", C.c_ulonglong), ("autotune", C.c_int)]
+
+
+class Tuning(C.Structure):
+    """stt_tuning (include/stt.h): launch choices and the autotuner's timings."""
+    _fields_ = [("fp_variant", C.c_int), ("slab_variant", C.c_int), ("bp_variant", C.c_int),
+                ("staged_bins", C.c_uint), ("tuned", C.c_int), ("from_cache", C.c_int),
+                ("fp_us", C.c_float * 8), ("slab_us", C.c_float * 8), ("bp_us", C.c_float * 4)]
 
 
 def _load() -> C.CDLL:
@@ -121,6 +128,10 @@ def _load() -> C.CDLL:
         "stt_solver_poll_status": [vp, vp],
         "stt_batch_poll_status": [vp, vp],
         "stt_warp_poll_status": [vp],
+        "stt_autotune": [vp, C.POINTER(Tuning), vp],
+        "stt_get_tuning": [vp, C.POINTER(Tuning)],
+        "stt_set_tuning": [vp, C.POINTER(Tuning)],
+        "stt_solver_set_iteration": [vp, C.c_ulonglong, vp],
     }
     for name, argtypes in sigs.items():
         fn = getattr(lib, name)
@@ -134,6 +145,8 @@ def _load() -> C.CDLL:
     lib.stt_batch_last_error.restype = C.c_char_p
     lib.stt_flow_last_error.argtypes = [vp]
     lib.stt_flow_last_error.restype = C.c_char_p
+    lib.stt_tuning_variant_name.argtypes = [i, i]
+    lib.stt_tuning_variant_name.restype = C.c_char_p
     lib.stt_version.argtypes = []
     lib.stt_version.restype = C.c_char_p
     return lib

@@ -14,7 +14,7 @@ from typing import Sequence
 
 import numpy as np
 
-from ._lib import FlowParams, Geometry, Instance, OpNorm, PdState, SolveCfg, STTError, check, lib
+from ._lib import FlowParams, Geometry, Instance, OpNorm, PdState, SolveCfg, STTError, Tuning, check, lib
 from ._lib import PdParams as _PdParams
 
 # ROI cut of the reference (ST_Tomography.cpp:114)
@@ -156,6 +156,31 @@ class Context:
         """Raises STTError (STT_ERR_TIMEOUT) if a bounded device-side wait of
         this context's launches gave up since the last poll; synchronises."""
         self._chk(lib.stt_poll_status(self._h, _stream(stream)))
+
+    # ---- launch choices (stt_autotune / stt_get_tuning / stt_set_tuning) ----
+    @staticmethod
+    def _tuning_dict(t: Tuning) -> dict:
+        return {"fp_variant": t.fp_variant, "slab_variant": t.slab_variant, "bp_variant": t.bp_variant,
+                "staged_bins": t.staged_bins, "tuned": bool(t.tuned), "from_cache": bool(t.from_cache),
+                "fp_us": list(t.fp_us)[:7], "slab_us": list(t.slab_us)[:4], "bp_us": list(t.bp_us)[:3],
+                "fp": (lib.stt_tuning_variant_name(0, t.fp_variant) or b"").decode(),
+                "slab": (lib.stt_tuning_variant_name(1, t.slab_variant) or b"").decode(),
+                "bp": (lib.stt_tuning_variant_name(2, t.bp_variant) or b"").decode()}
+
+    def autotune(self, stream=None) -> dict:
+        """Times the launch variants on this geometry and keeps the fastest."""
+        t = Tuning()
+        self._chk(lib.stt_autotune(self._h, C.byref(t), _stream(stream)))
+        return self._tuning_dict(t)
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        self._chk(lib.stt_get_tuning(self._h, C.byref(t)))
+        return self._tuning_dict(t)
+
+    def set_tuning(self, fp_variant=0, slab_variant=0, bp_variant=0, staged_bins=0x1E0):
+        t = Tuning(int(fp_variant), int(slab_variant), int(bp_variant), int(staged_bins), 1, 0)
+        self._chk(lib.stt_set_tuning(self._h, C.byref(t)))
 
     def fp_correction(self, vol, b, raylen_state, corr, view, stream=None):
         self._chk(lib.stt_fp_correction(self._h, _ptr(vol), _ptr(b), _ptr(raylen_state), _ptr(corr),
@@ -393,16 +418,17 @@ class Solver:
     def __init__(self, ctx: Context, state: dict, n_frames: int, views_per_frame: int,
                  pd: PdParams, alpha: float = 0.3, bp_mode: int = 0, roi_cut=REFERENCE_CUT,
                  seed: int = 0, mode: int = SOLVE_GRAPH, halo: bool = False, frame_offset: int = 0,
-                 total_frames: int = 0):
+                 total_frames: int = 0, autotune: bool = False):
         """halo=True: local frame 0 continues a previous shard (state needs
         ytp_halo, ybc_halo, flow_halo; see spacetimetomography_b200.halo).
         frame_offset / total_frames: the shard's place in the whole sequence
-        (its view orders are those of the unsharded solve)."""
+        (its view orders are those of the unsharded solve).  autotune: tune
+        the context's launch choices first (Context.autotune)."""
         self.ctx = ctx
         self.state = state  # keeps the tensors alive
         cfg = SolveCfg(n_frames, views_per_frame, bp_mode, float(alpha), pd.c(),
                        (C.c_int * 8)(*map(int, roi_cut)), C.c_ulonglong(seed), mode, int(bool(halo)),
-                       int(frame_offset), int(total_frames))
+                       int(frame_offset), int(total_frames), int(bool(autotune)))
         keys = ("vol", "xbar", "xprev", "ytv", "ytp", "ybc", "flow", "proj", "ytp_halo", "ybc_halo",
                 "flow_halo")
         st = PdState(*[state[k].data_ptr() if k in state else None for k in keys])
@@ -461,7 +487,7 @@ class Batch:
             arr[k] = Instance(d["ctx"]._h, d["vol"].data_ptr(), d["proj"].data_ptr(), int(d["proj"].shape[0]),
                               int(d.get("bp_mode", 0)), float(d.get("alpha", 0.3)), pd.c(),
                               (C.c_int * 8)(*map(int, d.get("roi_cut", REFERENCE_CUT))),
-                              C.c_ulonglong(int(d.get("seed", 0))))
+                              C.c_ulonglong(int(d.get("seed", 0))), int(bool(d.get("autotune", False))))
         h = C.c_void_p()
         rc = lib.stt_batch_create(arr, len(instances), int(mode), C.byref(h))
         if rc != 0:

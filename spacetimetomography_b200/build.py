@@ -27,7 +27,8 @@ LIB = PKG / "libstt.so"
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
 
-KERNEL_SOURCES = ["stt_capi.cu", "stt_solver.cu", "stt_batch.cu", "stt_noalloc.cu", "stt_flow.cu", "k_project.cu",
+KERNEL_SOURCES = ["stt_capi.cu", "stt_solver.cu", "stt_batch.cu", "stt_noalloc.cu", "stt_flow.cu", "stt_tune.cu",
+                  "k_project.cu",
                   "k_fp_slab.cu", "k_voxel.cu", "k_warp.cu", "k_flow.cu"]
 # Per-file flags.  The optical-flow kernels keep the reference's float
 # rounding operation by operation, so no multiply-add contraction there.

@@ -46,6 +46,7 @@ struct stt_host_solver {
     std::deque<int> pending;  // slots submitted and not yet waited for, oldest first
     int next = 0;
     cudaStream_t up = nullptr, compute = nullptr, down = nullptr;
+    cudaStream_t poll = nullptr;  // reads a completed step's status word; holds nothing else
 };
 
 namespace {
@@ -80,7 +81,9 @@ int wait_oldest(stt_host_solver *h) {
     stt_host_solver::Slot &s = h->slots[k];
     s.busy = false;
     HCUDA(cudaEventSynchronize(s.freed), "cudaEventSynchronize");
-    const stt_status st = stt_solver_poll_status(s.solver, h->compute);
+    // on a stream of its own: the compute stream may already hold the next
+    // step, and waiting for it here would stall the pipeline
+    const stt_status st = stt_solver_poll_status(s.solver, h->poll);
     if (st != STT_OK) {
         set_error(stt_solver_last_error(s.solver));
         return st;
@@ -139,7 +142,7 @@ int stt_host_solver_create(const stt_geometry *g, const stt_solve_cfg *cfg, int 
         if ((st = cuda_err(cudaEventCreateWithFlags(&s.computed, cudaEventDisableTiming), "event"))) return bail(st);
         if ((st = cuda_err(cudaEventCreateWithFlags(&s.freed, cudaEventDisableTiming), "event"))) return bail(st);
     }
-    for (cudaStream_t *sp : {&h->up, &h->compute, &h->down})
+    for (cudaStream_t *sp : {&h->up, &h->compute, &h->down, &h->poll})
         if (int st = cuda_err(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking), "stream")) return bail(st);
     *out = h;
     return STT_OK;
@@ -205,7 +208,7 @@ int stt_host_solver_destroy(stt_host_solver *h) {
             if (e) cudaEventDestroy(e);
         for (float *p : {s.vol, s.xbar, s.xprev, s.ytv, s.ytp, s.ybc, s.flow, s.proj}) cudaFree(p);
     }
-    for (cudaStream_t st : {h->up, h->compute, h->down})
+    for (cudaStream_t st : {h->up, h->compute, h->down, h->poll})
         if (st) cudaStreamDestroy(st);
     if (h->ctx) stt_destroy(h->ctx);
     delete h;

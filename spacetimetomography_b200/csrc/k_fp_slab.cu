@@ -30,10 +30,22 @@ namespace stt {
 
 namespace {
 
-constexpr int FB = 48, YB = 8, SB = 12;  // staged box (fast, y, slow), floats; FB*4 is a multiple of 16
-constexpr int BOXN = FB * YB * SB;
-constexpr unsigned BOX_BYTES = BOXN * sizeof(float);
-constexpr int SLAB = SB - 1;                     // base planes per slab; the box also holds their +1 plane
+// A staged box (fast, y, slow) in floats; FB*4 is a multiple of 16.  The
+// variants (slab_variant_name) hold different slices of the same taps: a
+// sample whose taps are not in the box reads them from global memory, so
+// every box gives the same bits.
+template <int FB_, int YB_, int SB_>
+struct SlabBox {
+    static constexpr int FB = FB_, YB = YB_, SB = SB_;
+    static constexpr int N = FB * YB * SB;
+    static constexpr unsigned BYTES = N * sizeof(float);
+    static constexpr int SLAB = SB - 1;  // base planes per slab; the box also holds their +1 plane
+    static_assert((FB * sizeof(float)) % 16 == 0, "TMA box rows must be 16-byte multiples");
+};
+using Box0 = SlabBox<48, 8, 12>;
+using Box1 = SlabBox<48, 8, 8>;
+using Box2 = SlabBox<64, 8, 10>;
+using Box3 = SlabBox<40, 8, 16>;
 constexpr long long WAIT_CYCLES = 200000000LL;  // about 0.1 s: a copy that never lands is an error
 constexpr int WARPS = 4;                         // a block is 32 x WARPS detector pixels, one warp per row
 
@@ -67,8 +79,9 @@ struct SlabAxes {
 // Lowest (fast, y) base coordinates of the taps of this ray's samples whose
 // slow coordinate lies in [m0, m0 + SLAB), with a voxel of margin; INT_MAX
 // when the ray has none there.
-template <bool ZF>
+template <bool ZF, class BX>
 __device__ __forceinline__ void ray_box_low(const GeomDev &g, const Ray &r, bool hit, int m0, int &lf, int &ly) {
+    constexpr int SLAB = BX::SLAB;
     constexpr int F = SlabAxes<ZF>::F, S = SlabAxes<ZF>::S;
     lf = INT_MAX;
     ly = INT_MAX;
@@ -86,11 +99,13 @@ __device__ __forceinline__ void ray_box_low(const GeomDev &g, const Ray &r, bool
 
 // The march of one ray of the block, summed into `acc`, taps from the staged
 // slabs where they are held.
-template <bool ZF>
+template <bool ZF, class BX>
 __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap *map, const float *__restrict__ src,
                                              bool hit, const Ray &r, float *buf, uint64_t *bar, int *red_s,
                                              int (*red)[2 * WARPS], volatile int *dead, int *status, Kahan &acc) {
     constexpr int S = SlabAxes<ZF>::S;
+    constexpr int FB = BX::FB, YB = BX::YB, SB = BX::SB, BOXN = BX::N, SLAB = BX::SLAB;
+    constexpr unsigned BOX_BYTES = BX::BYTES;
     const int dimS = ZF ? g.nx : g.nz;
     const Strides st = ZF ? zyx_strides(g) : xyz_strides(g);
     MarchGen m;
@@ -142,7 +157,7 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
     // slab 0
     int f0, y0;
     {
-        ray_box_low<ZF>(g, r, hit, slab_m0(0), f0, y0);
+        ray_box_low<ZF, BX>(g, r, hit, slab_m0(0), f0, y0);
         block_min2(f0, y0, red[0]);
         if (f0 == INT_MAX) f0 = y0 = 0;
         f0 = (f0 >> 2) << 2;  // the box's innermost coordinate starts on 16 bytes
@@ -157,7 +172,7 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
         // issue slab k+1 into the other buffer (free since the barrier that ended slab k-1)
         int fn = 0, yn = 0;
         if (k + 1 < nslab && !gave_up) {
-            ray_box_low<ZF>(g, r, hit, slab_m0(k + 1), fn, yn);
+            ray_box_low<ZF, BX>(g, r, hit, slab_m0(k + 1), fn, yn);
             block_min2(fn, yn, red[(k + 1) & 1]);
             if (fn == INT_MAX) fn = yn = 0;
             fn = (fn >> 2) << 2;
@@ -255,7 +270,8 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
 
 // k_fp_corr (GenerateImage_MT + the correction of ST_Tomography.cpp:667-676)
 // with slab-staged gathers.  map_x covers `vol` (x-fastest), map_z `vol_t`
-// (z-fastest), both with the box FB x YB x SB.
+// (z-fastest), both with the box of BX.
+template <class BX>
 __global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, const ViewRec *__restrict__ views,
                                                       const __grid_constant__ CUtensorMap map_x,
                                                       const __grid_constant__ CUtensorMap map_z,
@@ -263,7 +279,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, co
                                                       const ViewSel sel, const float *__restrict__ b_stack,
                                                       float *__restrict__ raylen_state, float *__restrict__ corr,
                                                       unsigned long long corr_surf, int *status) {
-    __shared__ alignas(128) float buf[2 * BOXN];
+    __shared__ alignas(128) float buf[2 * BX::N];
     __shared__ uint64_t bar[2];
     __shared__ int red[2][2 * WARPS];
     __shared__ int red_s[3 * WARPS];
@@ -283,9 +299,9 @@ __global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, co
     }
     Kahan acc{0.0f, 0.0f};
     if (vol_t && vr.layout == 1)
-        slab_ray_sum<true>(g, &map_z, vol_t, hit, r, buf, bar, red_s, red, &dead, status, acc);
+        slab_ray_sum<true, BX>(g, &map_z, vol_t, hit, r, buf, bar, red_s, red, &dead, status, acc);
     else
-        slab_ray_sum<false>(g, &map_x, vol, hit, r, buf, bar, red_s, red, &dead, status, acc);
+        slab_ray_sum<false, BX>(g, &map_x, vol, hit, r, buf, bar, red_s, red, &dead, status, acc);
     if (!valid) return;
     const float *b = b_stack + (size_t)local * g.W * g.H;
     const size_t pix = i + (size_t)j * g.W;
@@ -315,13 +331,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// A 3D FP32 tensor map (fast, mid, slow) over `ptr` with the slab box.
-bool encode_box_map(CUtensorMap *m, const float *ptr, int fast, int mid, int slow) {
+// A 3D FP32 tensor map (fast, mid, slow) over `ptr` with the slab box `box`.
+bool encode_box_map(CUtensorMap *m, const float *ptr, int fast, int mid, int slow, const cuuint32_t box[3]) {
     const PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
     if (!fn || !ptr || (reinterpret_cast<uintptr_t>(ptr) & 15) || (fast & 3)) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)fast, (cuuint64_t)mid, (cuuint64_t)slow};
     const cuuint64_t strides[2] = {(cuuint64_t)fast * sizeof(float), (cuuint64_t)fast * mid * sizeof(float)};
-    const cuuint32_t box[3] = {FB, YB, SB};
     const cuuint32_t estr[3] = {1, 1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(ptr), dims, strides, box, estr,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -344,13 +359,54 @@ bool encode_planes_map(CUtensorMap *m, const float *ptr, int nx, int ny, int nz,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m) {
+namespace {
+
+template <class BX>
+void box_dims(cuuint32_t box[3]) {
+    box[0] = BX::FB;
+    box[1] = BX::YB;
+    box[2] = BX::SB;
+}
+
+template <class BX>
+cudaError_t launch_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const float *vol,
+                        const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
+                        cudaStream_t s, unsigned long long corr_surf, int *status) {
+    static const bool carve = [] {
+        cudaFuncSetAttribute(k_fp_corr_slab<BX>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        cudaGetLastError();
+        return true;
+    }();
+    (void)carve;
+    k_fp_corr_slab<BX><<<dim3((g.W + 31) / 32, (g.H + WARPS - 1) / WARPS, 1), 32 * WARPS, 0, s>>>(
+        g, views, m.x, m.z, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, status);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+const char *slab_variant_name(int v) {
+    static const char *names[kSlabVariants] = {"box 48x8x12", "box 48x8x8", "box 64x8x10", "box 40x8x16"};
+    return v >= 0 && v < kSlabVariants ? names[v] : "?";
+}
+
+bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m, int variant) {
     m = FpSlabMaps{};
     if ((long long)g.nx * g.ny * g.nz >= (1LL << 31)) return false;  // 32-bit fallback offsets
-    if (!encode_box_map(&m.x, vol, g.nx, g.ny, g.nz)) return false;
-    if (vol_t && !encode_box_map(&m.z, vol_t, g.nz, g.ny, g.nx)) return false;
+    if (variant < 0 || variant >= kSlabVariants) return false;
+    cuuint32_t box[3];
+    switch (variant) {
+    case 1: box_dims<Box1>(box); break;
+    case 2: box_dims<Box2>(box); break;
+    case 3: box_dims<Box3>(box); break;
+    default: box_dims<Box0>(box); break;
+    }
+    if (!encode_box_map(&m.x, vol, g.nx, g.ny, g.nz, box)) return false;
+    if (vol_t && !encode_box_map(&m.z, vol_t, g.nz, g.ny, g.nx, box)) return false;
     m.ok = 1;
     m.has_z = vol_t != nullptr;
+    m.variant = variant;
     return true;
 }
 
@@ -358,16 +414,12 @@ cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const Fp
                                 const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state,
                                 float *corr, cudaStream_t s, unsigned long long corr_surf, int *status) {
     if (!m.ok || (vol_t && !m.has_z)) return cudaErrorInvalidValue;
-    static const bool carve = [] {
-        cudaFuncSetAttribute(k_fp_corr_slab, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
-        cudaGetLastError();
-        return true;
-    }();
-    (void)carve;
-    k_fp_corr_slab<<<dim3((g.W + 31) / 32, (g.H + WARPS - 1) / WARPS, 1), 32 * WARPS, 0, s>>>(g, views, m.x, m.z, vol, vol_t, sel, b_stack,
-                                                                          raylen_state, corr, corr_surf, status);
-    return cudaGetLastError();
+    switch (m.variant) {
+    case 1: return launch_slab<Box1>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status);
+    case 2: return launch_slab<Box2>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status);
+    case 3: return launch_slab<Box3>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status);
+    default: return launch_slab<Box0>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status);
+    }
 }
 
 }  // namespace stt

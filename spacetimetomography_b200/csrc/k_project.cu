@@ -26,16 +26,17 @@ __device__ __forceinline__ bool tile_pixel(const GeomDev &g, int &i, int &j) {
 
 // The ray sum of one forward-projector ray (hit rays only), gathered from the
 // z-fastest transposed copy for layout-1 views when one is given, else from
-// the volume.  Samples go FP_GROUP at a time where the march allows: all
-// their taps are loaded before any is interpolated.
+// the volume.  Samples go G at a time where the march allows: all their taps
+// are loaded before any is interpolated.  The sum is the same for every G
+// (the samples are added one by one in march order).
 constexpr int FP_GROUP = 4;
 
-template <int FAST, typename I, typename T>
+template <int FAST, typename I, int G = FP_GROUP, typename T>
 __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__restrict__ src, const Strides &st,
                                                  const Ray &r, int *count) {
     Kahan acc{0.0f, 0.0f};
     int n = 0;
-    march_groups<FP_GROUP>(
+    march_groups<G>(
         g, r,
         [&](const float p[3]) {
             FpCell c;
@@ -46,26 +47,38 @@ __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__re
             ++n;
         },
         [&](const float (*p)[3]) {
-            FpCell c[FP_GROUP];
-            float v[FP_GROUP][8];
+            FpCell c[G];
+            float v[G][8];
 #pragma unroll
-            for (int i = 0; i < FP_GROUP; ++i) {
+            for (int i = 0; i < G; ++i) {
                 fp_cell(g, p[i], c[i]);
                 fp_corners<FAST, I>(src, st, c[i], v[i]);
             }
 #pragma unroll
-            for (int i = 0; i < FP_GROUP; ++i) acc.add(__fmul_rn(trilerp(v[i], c[i]), g.sd));
-            n += FP_GROUP;
+            for (int i = 0; i < G; ++i) acc.add(__fmul_rn(trilerp(v[i], c[i]), g.sd));
+            n += G;
         });
     if (count) *count = n;
     return acc.s;
 }
 
-template <typename I, typename T>
+template <typename I, int G = FP_GROUP, typename T>
 __device__ __forceinline__ float fp_ray_sum(const GeomDev &g, const ViewRec &v, const T *__restrict__ vol,
                                             const T *__restrict__ vol_t, const Ray &r, int *count) {
-    if (vol_t && v.layout == 1) return fp_ray_sum_from<2, I>(g, vol_t, zyx_strides(g), r, count);
-    return fp_ray_sum_from<0, I>(g, vol, xyz_strides(g), r, count);
+    if (vol_t && v.layout == 1) return fp_ray_sum_from<2, I, G>(g, vol_t, zyx_strides(g), r, count);
+    return fp_ray_sum_from<0, I, G>(g, vol, xyz_strides(g), r, count);
+}
+
+// Detector tile of a block of NW warps for the tunable projector variants:
+// a warp covers WX x (32/WX) pixels (WX consecutive columns of 32/WX rows),
+// the NW warps are stacked along the rows.  WX = 32, NW = 4 is tile_pixel.
+template <int WX, int NW>
+__device__ __forceinline__ bool tile_pixel_t(const GeomDev &g, int &i, int &j) {
+    constexpr int WY = 32 / WX;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    i = blockIdx.x * WX + (lane % WX);
+    j = (blockIdx.y * NW + w) * WY + lane / WX;
+    return i < g.W && j < g.H;
 }
 
 // GenerateImage_MT (S/ImageFormationModel/TypicalRayProducer.core.h:168-224)
@@ -96,15 +109,18 @@ __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__re
 // c = (b - Ax) / (L + 1)).  L is the sticky ray length of the producer:
 // updated where the ray hits, kept where it misses; with no state buffer
 // (ray-based SART, whose producer is reset after every view) a miss gives L = 0.
-template <typename I>
-__global__ void __launch_bounds__(128) k_fp_corr(const GeomDev g, const ViewRec *__restrict__ views,
-                                                 const float *__restrict__ vol, const float *__restrict__ vol_t,
-                                                 const ViewSel sel, const float *__restrict__ b_stack,
-                                                 float *__restrict__ raylen_state,
-                                                 float *__restrict__ corr, unsigned long long corr_surf,
-                                                 int skip_staged) {
+// Tunable variants (fp_variant_name): the block's detector tile (WX, NW) and
+// the samples in flight per step (G) change only which thread projects which
+// ray and how far ahead its loads run, never a ray's arithmetic.
+template <typename I, int WX = 32, int NW = 4, int G = FP_GROUP>
+__global__ void __launch_bounds__(32 * NW) k_fp_corr(const GeomDev g, const ViewRec *__restrict__ views,
+                                                     const float *__restrict__ vol, const float *__restrict__ vol_t,
+                                                     const ViewSel sel, const float *__restrict__ b_stack,
+                                                     float *__restrict__ raylen_state,
+                                                     float *__restrict__ corr, unsigned long long corr_surf,
+                                                     int skip_staged) {
     int i, j;
-    if (!tile_pixel(g, i, j)) return;
+    if (!tile_pixel_t<WX, NW>(g, i, j)) return;
     int local;
     const int view = sel_view(sel, local);
     const float *b = b_stack + (size_t)local * g.W * g.H;
@@ -115,7 +131,7 @@ __global__ void __launch_bounds__(128) k_fp_corr(const GeomDev g, const ViewRec 
     const size_t pix = i + (size_t)j * g.W;
     float L, sum = 0.0f;
     if (r.tnear < r.tfar) {
-        sum = fp_ray_sum<I>(g, vr, vol, vol_t, r, nullptr);
+        sum = fp_ray_sum<I, G>(g, vr, vol, vol_t, r, nullptr);
         L = r.tfar - r.tnear;
         if (raylen_state) raylen_state[pix] = L;
     } else {
@@ -337,21 +353,55 @@ cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, 
     return cudaGetLastError();
 }
 
+namespace {
+
+// One launch of gather variant <WX, NW, G>: a block is NW warps of WX x (32/WX) pixels.
+template <int WX, int NW, int G>
+void fp_corr_variant(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, const ViewSel &sel,
+                     const float *b_stack, float *raylen_state, float *corr, cudaStream_t s,
+                     unsigned long long corr_surf, int skip) {
+    constexpr int TH = (32 / WX) * NW;  // detector rows per block
+    k_fp_corr<int, WX, NW, G><<<dim3((g.W + WX - 1) / WX, (g.H + TH - 1) / TH, 1), 32 * NW, 0, s>>>(
+        g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip);
+}
+
+}  // namespace
+
+const char *fp_variant_name(int v) {
+    static const char *names[kFpVariants] = {"32x4 rays per block, 4 samples in flight",
+                                             "32x2 rays per block, 4 in flight",
+                                             "32x8 rays per block, 4 in flight",
+                                             "warps of 16x2 rays, 16x8 per block, 4 in flight",
+                                             "warps of 8x4 rays, 8x16 per block, 4 in flight",
+                                             "32x4 rays per block, 2 in flight",
+                                             "32x4 rays per block, 8 in flight"};
+    return v >= 0 && v < kFpVariants ? names[v] : "?";
+}
+
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
-                           cudaStream_t s, unsigned long long corr_surf, const FpSlabMaps *maps, int *status) {
+                           cudaStream_t s, unsigned long long corr_surf, const FpSlabMaps *maps, int *status,
+                           int fp_variant) {
     const int skip = maps && maps->ok && (!vol_t || maps->has_z);
     if (skip) {
         cudaError_t e = launch_fp_corr_slab(g, views, *maps, vol, vol_t, sel, b_stack, raylen_state, corr, s,
                                             corr_surf, status);
         if (e != cudaSuccess) return e;
     }
-    if (small_volume(g))
-        k_fp_corr<int><<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf,
-                                                      skip);
-    else
+    if (!small_volume(g)) {
         k_fp_corr<long long><<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr,
                                                             corr_surf, skip);
+        return cudaGetLastError();
+    }
+    switch (fp_variant) {
+    case 1: fp_corr_variant<32, 2, 4>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    case 2: fp_corr_variant<32, 8, 4>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    case 3: fp_corr_variant<16, 4, 4>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    case 4: fp_corr_variant<8, 4, 4>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    case 5: fp_corr_variant<32, 4, 2>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    case 6: fp_corr_variant<32, 4, 8>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    default: fp_corr_variant<32, 4, 4>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    }
     return cudaGetLastError();
 }
 

@@ -136,21 +136,24 @@ __global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec
 // per-voxel ones).  The detector row moves by about sdd/sid per voxel, and
 // the 4x4 window's rows are kept in registers: a step of s = 0, 1 or 2 rows
 // reuses two of them and gathers the two new ones (2 tld4 instead of 4).
+// Column length K: 16 by default; the autotuner may pick 8 or 32 (the
+// voxels' values do not depend on which thread walks them).
 constexpr int BP_COL = 16;
 
 // Ten 128-thread blocks per SM (48 registers, no spills): the walk is bound
 // by texture latency, so the extra warps pay (10 blocks: 104.1 ms per
 // iteration of the 10 x 256^3 solve against 106.6 ms with the compiler's
 // 52 registers and 9 blocks).
+template <int K = BP_COL>
 __global__ void __launch_bounds__(128, 10) k_bp_voxel_cols(const GeomDev g, const ViewRec *__restrict__ views,
                                                        const ViewSel sel, float *__restrict__ vol, float alpha,
                                                        float gmax, unsigned long long tex) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y0 = blockIdx.y * BP_COL, z = blockIdx.z;
+    const int y0 = blockIdx.y * K, z = blockIdx.z;
     if (x >= g.nx) return;
     int local;
     const ViewRec &v = views[sel_view(sel, local)];
-    const int y1 = min(y0 + BP_COL, g.ny);
+    const int y1 = min(y0 + K, g.ny);
     if (!(v.A[1] == 0.0f && v.A[7] == 0.0f)) {
         for (int y = y0; y < y1; ++y) bp_voxel_at<true>(g, v, nullptr, tex, vol, x, y, z, alpha, gmax);
         return;
@@ -367,13 +370,32 @@ cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, c
     return cudaGetLastError();
 }
 
+namespace {
+template <int K>
+void bp_cols(const GeomDev &g, const ViewRec *views, const ViewSel &sel, float *vol, float alpha, float gmax,
+             cudaStream_t s, unsigned long long tex) {
+    k_bp_voxel_cols<K><<<dim3((g.nx + 127) / 128, (g.ny + K - 1) / K, g.nz), 128, 0, s>>>(g, views, sel, vol, alpha,
+                                                                                       gmax, tex);
+}
+}  // namespace
+
+const char *bp_variant_name(int v) {
+    static const char *names[kBpVariants] = {"columns of 16 voxels", "columns of 8 voxels", "columns of 32 voxels"};
+    return v >= 0 && v < kBpVariants ? names[v] : "?";
+}
+
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                            float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex) {
-    if (corr_tex)
-        k_bp_voxel_cols<<<dim3((g.nx + 127) / 128, (g.ny + BP_COL - 1) / BP_COL, g.nz), 128, 0, s>>>(
-            g, views, sel, vol, alpha, gmax, corr_tex);
-    else
+                            float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex,
+                            int bp_variant) {
+    if (corr_tex) {
+        switch (bp_variant) {
+        case 1: bp_cols<8>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
+        case 2: bp_cols<32>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
+        default: bp_cols<BP_COL>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
+        }
+    } else {
         k_bp_voxel<false><<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, sel, corr, vol, alpha, gmax, 0);
+    }
     return cudaGetLastError();
 }
 

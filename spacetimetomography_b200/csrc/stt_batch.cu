@@ -112,6 +112,7 @@ stt_status stt_batch_create(const stt_instance *instances, int n, int mode, stt_
         cfg.pd.bc_w = 0.0f;
         for (int q = 0; q < 8; ++q) cfg.roi_cut[q] = I.roi_cut[q];
         cfg.seed = I.seed;
+        cfg.autotune = I.autotune;
         cfg.mode = STT_SOLVE_STREAMS;
         stt_pd_state state{};
         state.vol = vol;

@@ -9,33 +9,9 @@
 #include <vector>
 
 #include "stt.h"
+#include "stt_ctx.h"
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
-
-struct stt_ctx {
-    int device = 0;
-    std::string err;
-    bool has_geom = false;
-    stt::GeomDev g{};
-    double sp[3] = {1, 1, 1};
-    std::vector<stt::ViewRec> views_h;
-    stt::ViewRec *views_d = nullptr;
-    size_t views_cap = 0;
-    float2 *acc = nullptr;  // ray-BP accumulators (contrib, weight) per voxel
-    size_t acc_n = 0;
-    float *corr = nullptr;  // W*H correction image used by stt_sart_sweep
-    size_t corr_n = 0;
-    float *volt = nullptr;  // z-fastest copy of the volume for views gathering along x
-    size_t volt_n = 0;
-    unsigned short *volt16 = nullptr;  // the same for a BF16-stored volume
-    size_t volt16_n = 0;
-    float *pw = nullptr;  // power iteration: x, A^T A x, and a chunk of projections
-    size_t pw_n = 0;
-    double *pwd = nullptr;  // power iteration: FP64 sums
-    size_t pwd_n = 0;
-    int *status = nullptr;  // raised by a bounded device-side wait that gave up (stt_poll_status)
-    size_t status_n = 0;
-};
 
 namespace {
 
@@ -51,10 +27,15 @@ stt_status cuda_fail(stt_ctx *ctx, cudaError_t e, const char *where) {
     return fail(ctx, STT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
+// A failed CUDA call: its error is read and cleared (cudaGetLastError), so a
+// non-sticky error does not resurface in a later, unrelated launch check.
 #define STT_CUDA(ctx, call, where)                          \
     do {                                                    \
         cudaError_t e_ = (call);                            \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+        if (e_ != cudaSuccess) {                            \
+            cudaGetLastError();                             \
+            return cuda_fail(ctx, e_, where);               \
+        }                                                   \
     } while (0)
 
 cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -258,7 +239,19 @@ stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g) {
         STT_CUDA(ctx, cudaMemset(ctx->status, 0, 4 * sizeof(int)), "cudaMemset(status word)");
     }
     ctx->views_h.resize(g->n_views);
-    for (int v = 0; v < g->n_views; ++v) build_view(*g, g->angles_rad[v], ctx->views_h[v]);
+    ctx->off_axis_deg.resize(g->n_views);
+    for (int v = 0; v < g->n_views; ++v) {
+        build_view(*g, g->angles_rad[v], ctx->views_h[v]);
+        const double s = std::fabs(std::sin(g->angles_rad[v])), c = std::fabs(std::cos(g->angles_rad[v]));
+        ctx->off_axis_deg[v] = (float)(std::atan2(std::fmin(s, c), std::fmax(s, c)) * 180.0 / M_PI);
+    }
+    // a new geometry starts from the default launch choices
+    ctx->geom = *g;
+    ctx->geom.angles_rad = nullptr;
+    ctx->tuning = stt::Tuning{};
+    ctx->staged_bins = 0x1E0u;
+    ctx->tuned = false;
+    ctx->report = stt_tuning{};
     if (g->n_views > 0) {
         st = ensure(ctx, ctx->views_d, ctx->views_cap, (size_t)g->n_views, "view table");
         if (st) return st;
@@ -362,9 +355,9 @@ stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, flo
     const float *volt = nullptr;
     if ((st = transposed_if_needed(ctx, vol, view, 1, S(stream), &volt))) return st;
     stt::FpSlabMaps maps;
-    stt::make_fp_slab_maps(ctx->g, vol, volt, maps);
+    stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
     STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, b, raylen_state, corr, S(stream), 0, &maps,
-                                      ctx->status),
+                                      ctx->status, ctx->tuning.fp),
              "k_fp_corr launch");
     return STT_OK;
 }
@@ -453,11 +446,12 @@ stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, con
         const float *volt = nullptr;
         if ((st = transposed_if_needed(ctx, vol, view_offset + perm[i], 1, s, &volt))) return st;
         stt::FpSlabMaps maps;
-        stt::make_fp_slab_maps(ctx->g, vol, volt, maps);
+        stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
         // ray-based mode: TypicalRayProducer::Initial zeroes the ray lengths
         // after every view, so missed rays see L = 0 (no sticky state)
         STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, proj_stack,
-                                          bp_mode == 0 ? raylen_state : nullptr, ctx->corr, s, 0, &maps, ctx->status),
+                                          bp_mode == 0 ? raylen_state : nullptr, ctx->corr, s, 0, &maps, ctx->status,
+                                          ctx->tuning.fp),
                  "k_fp_corr launch");
         if (bp_mode == 0)
             STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, sel, ctx->corr, vol, (float)alpha, gmax, s),

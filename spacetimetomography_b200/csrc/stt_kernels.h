@@ -19,20 +19,38 @@ struct PdParams {
 int sm_count();
 int grid_stride_blocks(long long n, int threads);
 
+// Launch shapes of the tunable kernels, picked by the autotuner (stt_tune.cu).
+// Variant 0 of each is the default; all variants of a kernel give the same
+// bits (they change which thread or block computes what, never a value's
+// arithmetic).
+//   fp:   the gather forward projector k_fp_corr: detector tile and samples
+//         in flight (fp_variant_name);
+//   slab: the box of the slab-staged projector (slab_variant_name);
+//   bp:   the column length of the voxel backprojection (bp_variant_name).
+// Which views the slab kernel projects is the per-view ViewRec::staged flag.
+constexpr int kFpVariants = 7, kSlabVariants = 4, kBpVariants = 3;
+struct Tuning {
+    int fp = 0, slab = 0, bp = 0;
+};
+const char *fp_variant_name(int v);
+const char *slab_variant_name(int v);
+const char *bp_variant_name(int v);
+
 cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, int view0,
                       int nviews, float *proj, float *raylen, float *weight, cudaStream_t s);
 // Slab-staged forward projector (k_fp_slab.cu) for the views marked `staged`:
 // the same outputs as the gather form bit for bit, the volume read through
 // TMA boxes.  The tensor maps cover the volume and its z-fastest copy (vol_t
-// may be null: then every view gathers from vol); make_fp_slab_maps returns
-// false where the form does not apply (x or z extent not a multiple of 4, an
-// array not 16-byte aligned, 2^31 voxels or more).  `status` (may be null) is
-// set to 1 if a box copy did not land within the wait limit.
+// may be null: then every view gathers from vol) with the box of slab variant
+// `variant`; make_fp_slab_maps returns false where the form does not apply (x
+// or z extent not a multiple of 4, an array not 16-byte aligned, 2^31 voxels
+// or more).  `status` (may be null) is set to 1 if a box copy did not land
+// within the wait limit.
 struct FpSlabMaps {
     CUtensorMap x, z;
-    int ok, has_z;
+    int ok, has_z, variant;
 };
-bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m);
+bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m, int variant = 0);
 // A 4D FP32 tensor map over nc planar volumes (x fastest, then y, z, plane)
 // with the given box (x, y, z, plane); false where TMA cannot address them
 // (nx not a multiple of 4, ptr not 16-byte aligned, box row not 16 bytes).
@@ -43,10 +61,11 @@ cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const Fp
 // Forward projection of one view fused with the SART correction.  With usable
 // slab maps, staged views run in the slab-staged kernel and the others in the
 // gather kernel (both are launched; each leaves the other's views alone).
+// `fp_variant` selects the gather kernel's launch shape.
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
                            cudaStream_t s, unsigned long long corr_surf = 0, const FpSlabMaps *maps = nullptr,
-                           int *status = nullptr);
+                           int *status = nullptr, int fp_variant = 0);
 cudaError_t launch_transpose(const GeomDev &g, const float *in, float *out, cudaStream_t s);
 cudaError_t launch_fp_bf16(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
                            const unsigned short *vol_t, int view0, int nviews, float *proj, float *raylen,
@@ -67,8 +86,11 @@ cudaError_t launch_dot_f64(long long n, const float *a, const float *b, double *
 cudaError_t launch_scale_inv_sqrt(long long n, float *x, const double *norm2, cudaStream_t s);
 cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, cudaStream_t s);
 
+// Voxel-driven backprojection; with the correction as a texture (corr_tex)
+// the column walk of bp variant `bp_variant` runs, else the per-voxel form.
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                            float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex = 0);
+                            float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex = 0,
+                            int bp_variant = 0);
 // Sets the solver's device-side iteration counter (stream-ordered, no host memory read).
 cudaError_t launch_set_counter(unsigned long long *counter, unsigned long long v, cudaStream_t s);
 // View orders of `frames` local frames (at most 1024), local frame f being

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "stt.h"
+#include "stt_ctx.h"
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
 
@@ -172,10 +173,15 @@ stt_status sfail(stt_solver *s, stt_status st, const std::string &m) {
     return st;
 }
 
+// A failed CUDA call: its error is read and cleared (cudaGetLastError), so a
+// non-sticky error does not resurface in a later, unrelated launch check.
 #define SCUDA(s, call, where)                                                                         \
     do {                                                                                              \
         cudaError_t e_ = (call);                                                                      \
-        if (e_ != cudaSuccess) return sfail(s, STT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e_)); \
+        if (e_ != cudaSuccess) {                                                                      \
+            cudaGetLastError();                                                                       \
+            return sfail(s, STT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e_));      \
+        }                                                                                             \
     } while (0)
 
 stt::PdParams pdp(const stt_pd_params &p) {
@@ -255,12 +261,12 @@ stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long
         const bool tex = voxel && !s->corr_tex.empty();
         SCUDA(s, stt::launch_fp_corr(g, s->views, vol, volt, sel, stack, voxel ? s->raylen + f * s->npix : nullptr,
                                      corr, cs, tex ? s->corr_tex[f].surf : 0,
-                                     s->fpmaps.empty() ? nullptr : &s->fpmaps[f], s->status),
+                                     s->fpmaps.empty() ? nullptr : &s->fpmaps[f], s->status, s->ctx->tuning.fp),
               "fp_corr");
         nl += (!s->fpmaps.empty() && s->fpmaps[f].ok) ? 2 : 1;  // slab-staged + gather kernels, or gather only
         if (voxel)
             SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs,
-                                          tex ? s->corr_tex[f].tex : 0),
+                                          tex ? s->corr_tex[f].tex : 0, s->ctx->tuning.bp),
                   "bp_voxel");
         else
             SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs),
@@ -296,7 +302,10 @@ stt_status enqueue_phase0(stt_solver *s, cudaStream_t main, long long &nl, bool 
 
 // Phase 1: per frame, after the previous frame's dual, the primal step, SART
 // and the ROI/over-relaxation; the frame chains rejoin `main`.  With `fork`
-// they first wait for `main` (work the caller queued between the phases).
+// (the phases enqueued separately) they first wait for `main`, which phase 0
+// has joined already (every dual is done; work the caller queued between the
+// phases is ordered too), so no frame waits on a phase-0 event: in the
+// captured form those events belong to the other phase's graph.
 stt_status enqueue_phase1(stt_solver *s, cudaStream_t main, long long &nl, bool fork) {
     const int F = s->F;
     if (fork) {
@@ -305,7 +314,7 @@ stt_status enqueue_phase1(stt_solver *s, cudaStream_t main, long long &nl, bool 
     }
     for (int f = 0; f < F; ++f) {
         cudaStream_t cs = s->streams[f];
-        if (f > 0) SCUDA(s, cudaStreamWaitEvent(cs, s->ev_dual[f - 1], 0), "stream wait");
+        if (f > 0 && !fork) SCUDA(s, cudaStreamWaitEvent(cs, s->ev_dual[f - 1], 0), "stream wait");
         stt_status st = enqueue_primal(s, f, cs, nl);
         if (st) return st;
         if ((st = enqueue_sart_batched(s, f, cs, nl))) return st;
@@ -424,6 +433,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
         !state->flow || !state->proj)
         return STT_ERR_INVALID;
     if (cfg->halo && (!state->ytp_halo || !state->ybc_halo || !state->flow_halo)) return STT_ERR_INVALID;
+    if (cfg->autotune && !ctx->tuned && (st = stt_autotune(ctx, nullptr, nullptr))) return st;
     if (cfg->n_frames > 1024) return STT_ERR_INVALID;
     const int total = cfg->total_frames > 0 ? cfg->total_frames : cfg->n_frames;
     if (cfg->frame_offset < 0 || (long long)cfg->frame_offset + cfg->n_frames > total) return STT_ERR_INVALID;
@@ -456,7 +466,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     if (cfg->mode != STT_SOLVE_PLAIN) {
         s->fpmaps.resize(F);
         for (int f = 0; f < F; ++f)  // where the maps do not apply, ok stays 0 and every view gathers
-            stt::make_fp_slab_maps(*g, s->st.vol + f * s->n, s->volt + f * s->n, s->fpmaps[f]);
+            stt::make_fp_slab_maps(*g, s->st.vol + f * s->n, s->volt + f * s->n, s->fpmaps[f], ctx->tuning.slab);
     }
     if (cfg->mode != STT_SOLVE_PLAIN && cfg->bp_mode == 0) {
         s->corr_tex.resize(F);

@@ -1,0 +1,326 @@
+// stt_tune.cu -- the project-written autotuner of the launch choices
+// (include/stt.h: stt_autotune, stt_get_tuning, stt_set_tuning).
+//
+// What it picks, for one context's geometry (volume, detector, distances,
+// view list):
+//   * the gather projector's launch variant (detector tile of a block and
+//     samples in flight per ray, fp_variant_name);
+//   * the slab-staged projector's TMA box (slab_variant_name);
+//   * for every 5-degree class of views (the central ray's angle off the
+//     nearest of the x and z axes), which of the two projectors runs them;
+//   * the voxel backprojection's column length (bp_variant_name).
+// Every variant of a kernel gives the same bits, so the choice changes only
+// the time.  One representative view per class is timed with CUDA events
+// (one warm-up launch, then the mean of three); classes are weighted by their
+// number of views.  Choices are cached per device and geometry shape.
+//
+// The loops these launches tile are the reference's row loop of the projector
+// (S/ImageFormationModel/TypicalRayProducer.core.h:168) and voxel loop of the
+// backprojection (S/ST_Tomo/ST_Tomography.cpp:690).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "stt.h"
+#include "stt_ctx.h"
+#include "stt_internal.cuh"
+#include "stt_kernels.h"
+
+namespace {
+
+std::mutex g_cache_mu;
+std::map<std::string, stt_tuning> g_cache;
+
+std::string shape_key(const stt_ctx *ctx) {
+    const stt_geometry &g = ctx->geom;
+    int counts[9] = {0};  // the view classes present, and their sizes, shape the choice too
+    for (float a : ctx->off_axis_deg) ++counts[stt::off_axis_bin(a)];
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "dev%d %dx%dx%d sp%.4g,%.4g,%.4g det%dx%d ds%.4g sid%.5g sdd%.5g off%.3g,%.3g,%.3g",
+                  ctx->device, g.nx, g.ny, g.nz, g.sx, g.sy, g.sz, g.W, g.H, g.ds, g.sid, g.sdd, g.off[0], g.off[1],
+                  g.off[2]);
+    std::string key(buf);
+    for (int b = 0; b < 9; ++b) key += " " + std::to_string(counts[b]);
+    return key;
+}
+
+// Device scratch of one tuning run, released on every return path.
+struct Scratch {
+    float *vol = nullptr, *volt = nullptr, *b = nullptr, *rl = nullptr, *corr = nullptr;
+    stt::ViewRec *tv = nullptr;
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~Scratch() {
+        cudaFree(vol);
+        cudaFree(volt);
+        cudaFree(b);
+        cudaFree(rl);
+        cudaFree(corr);
+        cudaFree(tv);
+        if (tex) cudaDestroyTextureObject(tex);
+        if (arr) cudaFreeArray(arr);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+};
+
+// Mean microseconds of fn() over 3 launches after one warm-up launch.
+template <typename Fn>
+cudaError_t time_us(Scratch &sc, cudaStream_t s, Fn &&fn, float &us) {
+    cudaError_t e = fn();
+    if (e != cudaSuccess) return e;
+    if ((e = cudaEventRecord(sc.e0, s)) != cudaSuccess) return e;
+    for (int r = 0; r < 3; ++r)
+        if ((e = fn()) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(sc.e1, s)) != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(sc.e1)) != cudaSuccess) return e;
+    float ms = 0.0f;
+    e = cudaEventElapsedTime(&ms, sc.e0, sc.e1);
+    us = 1000.0f * ms / 3.0f;
+    return e;
+}
+
+}  // namespace
+
+namespace stt {
+
+stt_status apply_staged_bins(stt_ctx *ctx) {
+    for (size_t v = 0; v < ctx->views_h.size(); ++v)
+        ctx->views_h[v].staged = ((ctx->staged_bins >> off_axis_bin(ctx->off_axis_deg[v])) & 1u) ? 1 : 0;
+    if (!ctx->views_h.empty() &&
+        cudaMemcpy(ctx->views_d, ctx->views_h.data(), sizeof(ViewRec) * ctx->views_h.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        ctx->err = "cudaMemcpy(view table) failed";
+        return STT_ERR_CUDA;
+    }
+    return STT_OK;
+}
+
+}  // namespace stt
+
+extern "C" {
+
+const char *stt_tuning_variant_name(int kernel, int variant) {
+    const char *s = kernel == 0 ? stt::fp_variant_name(variant)
+                    : kernel == 1 ? stt::slab_variant_name(variant)
+                    : kernel == 2 ? stt::bp_variant_name(variant) : "?";
+    return s[0] == '?' ? nullptr : s;
+}
+
+stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out) {
+    if (!ctx || !out) return STT_ERR_INVALID;
+    if (!ctx->has_geom) return STT_ERR_STATE;
+    *out = ctx->report;
+    out->fp_variant = ctx->tuning.fp;
+    out->slab_variant = ctx->tuning.slab;
+    out->bp_variant = ctx->tuning.bp;
+    out->staged_bins = ctx->staged_bins;
+    out->tuned = ctx->tuned ? 1 : 0;
+    return STT_OK;
+}
+
+stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t) {
+    if (!ctx || !t) return STT_ERR_INVALID;
+    if (!ctx->has_geom) return STT_ERR_STATE;
+    if (t->fp_variant < 0 || t->fp_variant >= stt::kFpVariants || t->slab_variant < 0 ||
+        t->slab_variant >= stt::kSlabVariants || t->bp_variant < 0 || t->bp_variant >= stt::kBpVariants ||
+        (t->staged_bins >> 9) != 0) {
+        ctx->err = "stt_set_tuning: a variant or staged_bins out of range";
+        return STT_ERR_INVALID;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->err = "cudaSetDevice failed";
+        return STT_ERR_CUDA;
+    }
+    ctx->tuning.fp = t->fp_variant;
+    ctx->tuning.slab = t->slab_variant;
+    ctx->tuning.bp = t->bp_variant;
+    ctx->staged_bins = t->staged_bins;
+    ctx->tuned = true;
+    ctx->report = *t;
+    ctx->report.tuned = 1;
+    return stt::apply_staged_bins(ctx);
+}
+
+stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
+    if (!ctx) return STT_ERR_INVALID;
+    if (!ctx->has_geom) {
+        ctx->err = "no geometry set (call stt_set_geometry)";
+        return STT_ERR_STATE;
+    }
+    if (ctx->views_h.empty()) {
+        ctx->err = "stt_autotune: the geometry has no views";
+        return STT_ERR_INVALID;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->err = "cudaSetDevice failed";
+        return STT_ERR_CUDA;
+    }
+    const std::string key = shape_key(ctx);
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        auto it = g_cache.find(key);
+        if (it != g_cache.end()) {
+            stt_tuning t = it->second;
+            t.from_cache = 1;
+            stt_status st = stt_set_tuning(ctx, &t);
+            if (st) return st;
+            if (out) *out = ctx->report;
+            return STT_OK;
+        }
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const stt::GeomDev &g = ctx->g;
+    const size_t n = (size_t)g.nx * g.ny * g.nz, npix = (size_t)g.W * g.H;
+    Scratch sc;
+    auto fail = [&](cudaError_t e, const char *where) {
+        cudaGetLastError();
+        ctx->err = std::string("stt_autotune: ") + where + ": " + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? STT_ERR_NOMEM : STT_ERR_CUDA;
+    };
+    cudaError_t e = cudaSuccess;
+    if ((e = cudaMalloc(&sc.vol, n * sizeof(float))) || (e = cudaMalloc(&sc.volt, n * sizeof(float))) ||
+        (e = cudaMalloc(&sc.b, npix * sizeof(float))) || (e = cudaMalloc(&sc.rl, npix * sizeof(float))) ||
+        (e = cudaMalloc(&sc.corr, npix * sizeof(float))) || (e = cudaMalloc(&sc.tv, 2 * sizeof(stt::ViewRec))) ||
+        (e = cudaEventCreate(&sc.e0)) || (e = cudaEventCreate(&sc.e1)))
+        return fail(e, "scratch");
+    {  // the correction as a one-layer texture, as the solver's backprojection reads it
+        cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+        if ((e = cudaMalloc3DArray(&sc.arr, &cd, make_cudaExtent(g.W, g.H, 1), cudaArrayLayered)))
+            return fail(e, "texture array");
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = sc.arr;
+        cudaTextureDesc td{};
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModePoint;
+        td.readMode = cudaReadModeElementType;
+        if ((e = cudaCreateTextureObject(&sc.tex, &rd, &td, nullptr))) return fail(e, "texture object");
+    }
+    // the times do not depend on the values; these are positive and typical enough
+    if ((e = stt::launch_fill_seeded((long long)n, 7, sc.vol, s)) || (e = stt::launch_transpose(g, sc.vol, sc.volt, s)) ||
+        (e = cudaMemsetAsync(sc.b, 0, npix * sizeof(float), s)) || (e = cudaMemsetAsync(sc.rl, 0, npix * sizeof(float), s)))
+        return fail(e, "scratch fill");
+    // one representative view per class, and the class sizes
+    int rep[9], count[9];
+    for (int b = 0; b < 9; ++b) rep[b] = -1, count[b] = 0;
+    for (size_t v = 0; v < ctx->views_h.size(); ++v) {
+        const int b = stt::off_axis_bin(ctx->off_axis_deg[v]);
+        if (rep[b] < 0) rep[b] = (int)v;
+        ++count[b];
+    }
+    float tg[stt::kFpVariants][9] = {}, ts[stt::kSlabVariants][9] = {};
+    stt::FpSlabMaps maps[stt::kSlabVariants];
+    bool maps_ok[stt::kSlabVariants] = {};
+    bool slab_ok = false;
+    for (int sv = 0; sv < stt::kSlabVariants; ++sv)
+        slab_ok |= maps_ok[sv] = stt::make_fp_slab_maps(g, sc.vol, sc.volt, maps[sv], sv);
+    for (int b = 0; b < 9; ++b) {
+        if (rep[b] < 0) continue;
+        stt::ViewRec two[2] = {ctx->views_h[rep[b]], ctx->views_h[rep[b]]};
+        two[0].staged = 0;
+        two[1].staged = 1;
+        if ((e = cudaMemcpyAsync(sc.tv, two, sizeof two, cudaMemcpyHostToDevice, s)) || (e = cudaStreamSynchronize(s)))
+            return fail(e, "view copy");
+        const stt::ViewSel gather_sel{0, nullptr, 0, 0}, slab_sel{1, nullptr, 0, 1};
+        for (int fv = 0; fv < stt::kFpVariants; ++fv) {
+            e = time_us(sc, s, [&] {
+                return stt::launch_fp_corr(g, sc.tv, sc.vol, sc.volt, gather_sel, sc.b, sc.rl, sc.corr, s, 0, nullptr,
+                                           ctx->status, fv);
+            }, tg[fv][b]);
+            if (e) return fail(e, "gather projector");
+        }
+        for (int sv = 0; sv < stt::kSlabVariants; ++sv) {
+            if (!maps_ok[sv]) continue;
+            e = time_us(sc, s, [&] {
+                return stt::launch_fp_corr_slab(g, sc.tv, maps[sv], sc.vol, sc.volt, slab_sel, sc.b, sc.rl, sc.corr, s,
+                                                0, ctx->status);
+            }, ts[sv][b]);
+            if (e) return fail(e, "slab projector");
+        }
+    }
+    // the gather variant with the least time over all views; then the box
+    // whose per-class minimum with it is least; then the class choices
+    stt_tuning t{};
+    double best = 1e300;
+    for (int fv = 0; fv < stt::kFpVariants; ++fv) {
+        double tot = 0.0, w = 0.0;
+        for (int b = 0; b < 9; ++b)
+            if (rep[b] >= 0) tot += (double)count[b] * tg[fv][b], w += count[b];
+        t.fp_us[fv] = (float)(tot / w);
+        if (tot < best) best = tot, t.fp_variant = fv;
+    }
+    if (slab_ok) {
+        best = 1e300;
+        for (int sv = 0; sv < stt::kSlabVariants; ++sv) {
+            if (!maps_ok[sv]) continue;
+            double tot = 0.0, w = 0.0, slab_only = 0.0;
+            for (int b = 0; b < 9; ++b) {
+                if (rep[b] < 0) continue;
+                tot += (double)count[b] * std::fmin(tg[t.fp_variant][b], ts[sv][b]);
+                slab_only += (double)count[b] * ts[sv][b];
+                w += count[b];
+            }
+            t.slab_us[sv] = (float)(slab_only / w);
+            if (tot < best) best = tot, t.slab_variant = sv;
+        }
+        for (int b = 0; b < 9; ++b) {
+            if (rep[b] >= 0) {
+                if (ts[t.slab_variant][b] < tg[t.fp_variant][b]) t.staged_bins |= 1u << b;
+            } else {
+                t.staged_bins |= 0x1E0u & (1u << b);  // a class without views keeps the default rule
+            }
+        }
+    } else {
+        t.staged_bins = 0x1E0u;  // irrelevant: without slab maps every view gathers
+    }
+    // voxel backprojection: the column lengths on the views of the first and last classes present
+    if ((e = cudaMemcpy2DToArrayAsync(sc.arr, 0, 0, sc.corr, g.W * sizeof(float), g.W * sizeof(float), g.H,
+                                      cudaMemcpyDeviceToDevice, s)))
+        return fail(e, "texture fill");
+    {
+        int vb[2] = {-1, -1};
+        for (int b = 0; b < 9; ++b)
+            if (rep[b] >= 0) {
+                if (vb[0] < 0) vb[0] = rep[b];
+                vb[1] = rep[b];
+            }
+        best = 1e300;
+        for (int bv = 0; bv < stt::kBpVariants; ++bv) {
+            float tot = 0.0f;
+            for (int k = 0; k < 2; ++k) {
+                const stt::ViewRec one = ctx->views_h[vb[k]];
+                if ((e = cudaMemcpyAsync(sc.tv, &one, sizeof one, cudaMemcpyHostToDevice, s)) ||
+                    (e = cudaStreamSynchronize(s)))
+                    return fail(e, "view copy");
+                float us = 0.0f;
+                e = time_us(sc, s, [&] {
+                    return stt::launch_bp_voxel(g, sc.tv, stt::ViewSel{0, nullptr, 0, 0}, nullptr, sc.vol, 0.3f,
+                                                1e30f, s, sc.tex, bv);
+                }, us);
+                if (e) return fail(e, "voxel backprojection");
+                tot += us;
+            }
+            t.bp_us[bv] = tot / 2.0f;
+            if (tot < best) best = tot, t.bp_variant = bv;
+        }
+    }
+    if ((e = cudaStreamSynchronize(s))) return fail(e, "synchronize");
+    stt_status st = stt_set_tuning(ctx, &t);
+    if (st) return st;
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        g_cache[key] = ctx->report;
+    }
+    if (out) *out = ctx->report;
+    return STT_OK;
+}
+
+}  // extern "C"

@@ -48,6 +48,7 @@ O.orc_view_from_angle.argtypes = [_d, C.POINTER(OView)]
 O.orc_fp_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp, _vp, _vp, _i]
 O.orc_fp_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp, _vp, _vp, _i]
 O.orc_fp_rows_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _i, _i, _vp, _i]
+O.orc_fp_rows_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _i, _i, _vp, _i]
 O.orc_bp_ray_scatter_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp, _vp]
 O.orc_fp_adjoint_f64.argtypes = [C.POINTER(OGeom), C.POINTER(OView), _vp, _vp]
 O.orc_fp_adjoint_f32.argtypes = [C.POINTER(OGeom), _i, C.POINTER(OView), _vp, _vp]
@@ -183,6 +184,17 @@ def fp64_rows(scan: Scan, view: OView, vol: np.ndarray, row0: int, nrows: int, t
     g = scan.ogeom()
     if O.orc_fp_rows_f64(C.byref(g), C.byref(view), P(np.ascontiguousarray(vol, np.float64)), row0, row0 + nrows,
                          P(img), threads) != 0:
+        raise ValueError("bad row range")
+    return img[row0:row0 + nrows].copy()
+
+
+def fp32_rows(scan: Scan, view: OView, vol: np.ndarray, row0: int, nrows: int, gmode: int = 1, threads: int = 0):
+    """The band in the reference's FP32 arithmetic (gmode 1: FP64 ray set-up, FP32 march, as the GPU)."""
+    W, H = scan.det
+    img = np.zeros((H, W), np.float32)
+    g = scan.ogeom()
+    if O.orc_fp_rows_f32(C.byref(g), gmode, C.byref(view), P(np.ascontiguousarray(vol, np.float32)), row0,
+                         row0 + nrows, P(img), threads) != 0:
         raise ValueError("bad row range")
     return img[row0:row0 + nrows].copy()
 

@@ -63,13 +63,26 @@ def test_sart_sweep_at_full_size_vs_fp64(cuda, n, det, views, nsweep, bp_mode):
     ctx.sart_sweep(vol, proj, order, 0.3, gmax, bp_mode, state)
     torch.cuda.synchronize()
     ctx.poll_status()
-    ref, _ = ob.sart64(scan, [ob.view_angle(a) for a in angles], order, proj.cpu().numpy().astype(np.float64), 0.3,
+    views = [ob.view_angle(a) for a in angles]
+    got = vol.cpu().numpy()
+    # the reference's FP32 arithmetic (the restatement, pinned bit for bit to the
+    # reference's SART): the same within float rounding (and atomic order)
+    ref32, _ = ob.sart32(scan, views, order, proj.cpu().numpy(), 0.3, gmax, bp_mode, start.cpu().numpy(), gmode=1)
+    assert ob.rel_l2(got, ref32) < 1e-5, ob.rel_l2(got, ref32)
+    ref, _ = ob.sart64(scan, views, order, proj.cpu().numpy().astype(np.float64), 0.3,
                        gmax, bp_mode, start.cpu().numpy().astype(np.float64))
-    upd = vol.cpu().numpy().astype(np.float64) - start.cpu().numpy()
-    e = ob.rel_l2(vol.cpu().numpy(), ref)
-    e_upd = ob.rel_l2(upd, ref - start.cpu().numpy())
-    assert e < 1e-4, e
-    assert e_upd < (1e-3 if bp_mode == 0 else 1e-2), e_upd  # the update alone, a much smaller vector
+    e = ob.rel_l2(got, ref)
+    if bp_mode == 0:
+        assert e < 1e-4, e
+    else:
+        # The ray-driven update is contrib/weight per voxel: a voxel that one
+        # evaluation's samples barely touch (weight ~1e-6) takes the whole
+        # correction there and none in the other (0/0 -> 0).  Where the FP32
+        # march and the FP64 one touch a voxel differently, the two differ by a
+        # full correction value: the reference's FP32 arithmetic itself lies
+        # about 1e-3 from FP64 at 256^3 / 512^2 (measured 8.4e-4), so the FP64
+        # error of this path is held to 2e-3.
+        assert e < 2e-3, e
     ctx.close()
 
 
@@ -100,16 +113,17 @@ def test_dot_product_adjoint_at_full_size(cuda, n, det, views):
 def test_data_gradient_fp64_finite_difference_256(cuda):
     """d/de f(x + e d) at e = 0 for f = |A x - b|^2 / 2 on one view: the GPU's
     <A^T (A x - b), d> against an FP64 central difference of the oracle's f
-    (exact for this quadratic up to rounding)."""
+    (exact for this quadratic up to rounding).  The direction d is a second,
+    non-negative phantom: a zero-mean random d would make the inner product a
+    near-cancelling sum whose value the rounding of single samples decides."""
     import torch
 
     n, det = 256, 512
     scan = ob.Scan(n, det)
     angle = 0.7
     ctx = _ctx(scan, [angle])
-    rng = np.random.default_rng(9)
     x = _phantom(n, 30, 7, cuda)
-    d = torch.from_numpy(rng.uniform(-1, 1, (n, n, n)).astype(np.float32)).to(cuda)
+    d = (_phantom(n, 20, 8, cuda) + 0.05).contiguous()
     b = torch.zeros((1, det, det), device=cuda)
     ctx.fp((x * 1.1).contiguous(), b)
     ax = torch.zeros((1, det, det), device=cuda)
@@ -141,10 +155,18 @@ def test_512_band_and_voxel_backprojection_vs_fp64(cuda):
     img = torch.zeros((1, det, det), device=cuda)
     ctx.fp(truth, img, view0=v, nviews=1)
     torch.cuda.synchronize()
-    t64 = truth.cpu().numpy().astype(np.float64)
+    t32 = truth.cpu().numpy()
     r0 = det // 2 - 32
-    band = ob.fp64_rows(scan, ob.view_angle(angles[v]), t64, r0, 64)
-    assert ob.rel_l2(img[0, r0:r0 + 64].cpu().numpy(), band) < 1e-5
+    got = img[0, r0:r0 + 64].cpu().numpy()
+    # the reference's FP32 arithmetic: the same within float rounding
+    band32 = ob.fp32_rows(scan, ob.view_angle(angles[v]), t32, r0, 64)
+    assert ob.rel_l2(got, band32) < 1e-5, ob.rel_l2(got, band32)
+    # FP64: the reference's march steps its sample positions in FP32 (t += sd,
+    # pos += step over ~600 samples per ray here), and at 512^3 the porous
+    # background's sharp sphere edges turn that position drift into ~1e-4 of
+    # the line integrals (measured 1.1e-4); held to 2e-4
+    band = ob.fp64_rows(scan, ob.view_angle(angles[v]), t32.astype(np.float64), r0, 64)
+    assert ob.rel_l2(got, band) < 2e-4, ob.rel_l2(got, band)
     # one view's correction and its voxel backprojection
     b = torch.zeros((det, det), device=cuda)
     ctx.fp(truth, b[None], view0=v, nviews=1)

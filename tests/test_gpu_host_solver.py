@@ -53,7 +53,7 @@ def test_host_solver_equals_device_solver(cuda):
     ctx.close()
     # the same on host buffers, three steps on two slots
     hs = HostSolver(scan.dims, scan.sp, scan.det, scan.ds, scan.sid, scan.sdd, angles, F, V, pd, alpha=0.3,
-                    roi_cut=CUT, seed=5, slots=2)
+                    roi_cut=CUT, seed=5, slots=2, offset=scan.off)
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
     hv, hf, hp = pin(vol), pin(flow), pin(proj)
     outs = [torch.empty((F, N, N, N)).pin_memory() for _ in range(3)]

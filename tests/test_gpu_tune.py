@@ -1,0 +1,129 @@
+"""The autotuner's candidates (stt_autotune, stt_set_tuning through the C ABI)
+give identical outputs: every launch variant of the gather projector, every
+box of the slab-staged projector and every column length of the voxel
+backprojection produce the same bits as the default, so the tuner only ever
+changes the time.  The tuner's choice is valid and is cached per shape."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle_bind as ob
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(scan, angles):
+    import spacetimetomography_b200 as stt
+
+    c = stt.Context(0)
+    c.set_geometry(scan.dims, scan.sp, scan.det, scan.ds, scan.sid, scan.sdd, angles, scan.off)
+    return c
+
+
+def _corrections(ctx, vol, b, views):
+    import torch
+
+    H, W = b.shape[1:]
+    state = torch.zeros((H, W), device=vol.device)
+    corr = torch.zeros((H, W), device=vol.device)
+    out = []
+    for v in views:
+        ctx.fp_correction(vol, b[v], state, corr, v)
+        out.append(corr.clone())
+    out.append(state.clone())
+    torch.cuda.synchronize()
+    return [o.cpu().numpy() for o in out]
+
+
+# every off-axis class: 0..45 degrees and their mirrors
+ANGLES = np.deg2rad([0, 3, 8, 13, 17, 22, 27, 33, 38, 44, 47, 62, 88, 96, 133, 181, 228, 271, 313, 350])
+
+
+@pytest.mark.parametrize("dims,det,off", [((48, 40, 44), (72, 60), (0.5, -0.3, 0.2)),
+                                          ((64, 64, 64), (96, 80), (0.0, 0.0, 0.0))])
+def test_every_projector_variant_gives_the_same_bits(cuda, dims, det, off):
+    import torch
+
+    from spacetimetomography_b200 import phantom as ph
+
+    scan = ob.Scan(dims, det, off=off)
+    ctx = _ctx(scan, ANGLES)
+    vol = ph.ellipsoid_phantom(dims, 6, seed=4, semi=(3.0, 12.0)).to(cuda) + 0.01
+    g = torch.Generator(device=cuda)
+    g.manual_seed(1)
+    b = torch.rand((len(ANGLES), det[1], det[0]), device=cuda, generator=g) * 30
+    views = range(len(ANGLES))
+    ctx.set_tuning(0, 0, 0, staged_bins=0)  # everything through the default gather variant
+    base = _corrections(ctx, vol, b, views)
+    for fv in range(1, 7):
+        ctx.set_tuning(fv, 0, 0, staged_bins=0)
+        for k, (a, c) in enumerate(zip(base, _corrections(ctx, vol, b, views))):
+            np.testing.assert_array_equal(a, c, err_msg=f"gather variant {fv}, output {k}")
+    for sv in range(4):  # every view through the slab-staged kernel with each box
+        ctx.set_tuning(0, sv, 0, staged_bins=0x1FF)
+        for k, (a, c) in enumerate(zip(base, _corrections(ctx, vol, b, views))):
+            np.testing.assert_array_equal(a, c, err_msg=f"slab box {sv}, output {k}")
+    ctx.poll_status()
+    ctx.close()
+
+
+def test_every_backprojection_column_length_gives_the_same_bits(cuda):
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200 import phantom as ph
+
+    N, V = 40, 8
+    scan = ob.Scan(N, (64, 56))
+    angles = np.linspace(0, 2 * math.pi, V, endpoint=False) + 0.1
+    truth = ph.ellipsoid_phantom((N, N, N), 5, seed=2, semi=(3.0, 10.0)).to(cuda)
+    ctx = _ctx(scan, angles)
+    proj = torch.zeros((V, 56, 64), device=cuda)
+    ctx.fp(truth, proj)
+    pd = stt.PdParams(gmax=float(proj.max()) / 4, tp_w=0.0, bc_w=0.0, cut=(3, 3, 3, 5, 3, 3, 6, 5))
+    outs = []
+    for bv in range(3):
+        ctx.set_tuning(0, 0, bv)
+        z = lambda *s: torch.zeros(s, device=cuda)  # noqa: E731
+        st = dict(vol=z(2, N, N, N), xbar=z(2, N, N, N), xprev=z(1, N, N, N), ytv=z(1, 3, N, N, N), ytp=z(1, N, N, N),
+                  ybc=z(1, N, N, N), flow=z(1, 3, N, N, N), proj=proj[None].contiguous())
+        s = stt.Solver(ctx, st, 1, V, pd, roi_cut=(3, 3, 3, 5, 3, 3, 6, 5), seed=3)
+        s.iterate(2)
+        torch.cuda.synchronize()
+        outs.append(st["vol"][0].cpu().numpy())
+        s.close()
+    for bv in (1, 2):
+        np.testing.assert_array_equal(outs[0], outs[bv], err_msg=f"column variant {bv}")
+    assert np.abs(outs[0]).max() > 0
+    ctx.close()
+
+
+def test_autotune_picks_a_valid_choice_and_caches_it(cuda):
+    import torch
+
+    from spacetimetomography_b200 import phantom as ph
+
+    dims, det = (64, 56, 60), (96, 80)
+    scan = ob.Scan(dims, det)
+    ctx = _ctx(scan, ANGLES)
+    t = ctx.autotune()
+    assert t["tuned"] and not t["from_cache"]
+    assert 0 <= t["fp_variant"] < 7 and 0 <= t["slab_variant"] < 4 and 0 <= t["bp_variant"] < 3
+    assert all(x > 0 for x in t["fp_us"]) and all(x > 0 for x in t["bp_us"])
+    assert t["fp"] and t["slab"] and t["bp"]
+    assert ctx.get_tuning()["fp_variant"] == t["fp_variant"]
+    # a second context of the same shape takes the cached choice
+    ctx2 = _ctx(scan, ANGLES)
+    t2 = ctx2.autotune()
+    assert t2["from_cache"] and t2["fp_variant"] == t["fp_variant"] and t2["staged_bins"] == t["staged_bins"]
+    # and the tuned context projects what the default one does
+    vol = ph.ellipsoid_phantom(dims, 6, seed=9, semi=(3.0, 12.0)).to(cuda)
+    b = torch.rand((len(ANGLES), det[1], det[0]), device=cuda) * 10
+    ctx3 = _ctx(scan, ANGLES)  # defaults
+    for a, c in zip(_corrections(ctx3, vol, b, range(len(ANGLES))), _corrections(ctx, vol, b, range(len(ANGLES)))):
+        np.testing.assert_array_equal(a, c)
+    with pytest.raises(Exception):
+        ctx.set_tuning(fp_variant=99)
+    for c in (ctx, ctx2, ctx3):
+        c.close()
