@@ -67,7 +67,7 @@ CONFIG_SPECS = {
                      "10 outer iterations, voxel- and ray-based BP",
             n=512, det=1024, views=720, ellipsoids=100, porous=True, noise=0.0, solve="pd", iters=10,
             bps=("voxel", "ray"), alpha=0.3, sigma=0.9 / 8.0, tau=1.0, lam=0.01, huber=0.01,
-            roi=(16, 16, 16, 90, 16, 16, 60, 40)),
+            roi=(16, 16, 16, 90, 16, 16, 60, 40), storages=("f32", "bf16")),
 }
 
 
@@ -513,17 +513,24 @@ def _timed(stream, fn, reps: int) -> float:
     return e0.elapsed_time(e1) / 1000.0 / max(reps, 1)
 
 
-def _pd_state(N, proj, dev):
+def _pd_state(N, proj, dev, storage="f32"):
+    """A one-frame solver state; storage "bf16": the primal volumes and the
+    sinogram in torch.bfloat16 (stt_solve_cfg.storage)."""
     import torch
 
     z = lambda *s: torch.zeros(s, device=dev)  # noqa: E731
-    return dict(vol=z(2, N, N, N), xbar=z(2, N, N, N), xprev=z(1, N, N, N), ytv=z(1, 3, N, N, N), ytp=z(1, N, N, N),
-                ybc=z(1, N, N, N), flow=z(1, 3, N, N, N), proj=proj[None])
+    zp = lambda *s: torch.zeros(s, device=dev, dtype=torch.bfloat16 if storage == "bf16" else torch.float32)  # noqa
+    p = proj[None] if storage == "f32" else proj[None].to(torch.bfloat16)
+    return dict(vol=zp(2, N, N, N), xbar=zp(2, N, N, N), xprev=zp(1, N, N, N), ytv=z(1, 3, N, N, N),
+                ytp=z(1, N, N, N), ybc=z(1, N, N, N), flow=z(1, 3, N, N, N), proj=p)
 
 
-def config_solve(cid, ctx, proj, truth, gmax, bp, dev, stream, iters: int, reps: int) -> dict:
+def config_solve(cid, ctx, proj, truth, gmax, bp, dev, stream, iters: int, reps: int, storage="f32",
+                 keep=False) -> dict:
     """One solve of the workload; times `reps` of its iterations after one
-    warm-up iteration and reports the error to the phantom after `iters`."""
+    warm-up iteration and reports the error to the phantom after `iters`.
+    storage "bf16": the primal volumes and the sinogram stored in BF16.  keep:
+    the result volume (FP32) is returned under "_result"."""
     import torch
 
     import spacetimetomography_b200 as stt
@@ -547,12 +554,12 @@ def config_solve(cid, ctx, proj, truth, gmax, bp, dev, stream, iters: int, reps:
         launches = None
         result = vol
     else:
-        st = _pd_state(N, proj, dev)
+        st = _pd_state(N, proj, dev, storage)
         sg, lam = c["sigma"], c["lam"]
         pd = stt.PdParams(sigma=sg, tau=c["tau"], tv_w=lam, tp_w=0.0, bc_w=0.0,
                           huber_factor=1.0 / (1.0 + sg * c["huber"] / lam), gmax=gmax, cut=c["roi"])
         solver = stt.Solver(ctx, st, 1, V, pd, alpha=c["alpha"], bp_mode=bp_mode, roi_cut=c["roi"], seed=cid,
-                            mode=stt.SOLVE_GRAPH)
+                            mode=stt.SOLVE_GRAPH, storage=storage)
 
         def one():
             solver.iterate(1, stream)
@@ -563,11 +570,13 @@ def config_solve(cid, ctx, proj, truth, gmax, bp, dev, stream, iters: int, reps:
         torch.cuda.synchronize()
         solver.poll_status(stream)
         launches = solver.stats()[0]
-        result = st["vol"][0]
+        result = st["vol"][0].float()
     torch.cuda.synchronize()
     err = float((result - truth).norm() / truth.norm())
     out = {"s_per_iter": t, "gups": N ** 3 * V / t / 1e9, "iterations_run": max(iters, 1 + reps),
-           "rel_l2_to_phantom": err, "launches_per_iter": launches}
+           "rel_l2_to_phantom": err, "launches_per_iter": launches, "storage": storage}
+    if keep:
+        out["_result"] = result.clone()
     if c["solve"] != "sart":
         solver.close()
     return out
@@ -601,6 +610,18 @@ def fp_bp_split(ctx, c, vol, proj, gmax, dev, stream) -> dict:
         ctx.fp(vol, img[k:k + 1], view0=v, nviews=1, weight=w[k:k + 1], stream=stream)
     torch.cuda.synchronize()
     samples = float(w.sum().item()) / 4
+    # the gather ceiling over the same views: the projector's gathers and
+    # interpolation alone (stt_gather_ceiling), its own samples counted
+    gimg = torch.empty((D, D), device=dev)
+    gcount = torch.zeros((D, D), dtype=torch.int32, device=dev)
+    gsamples = 0
+    for v in views:
+        ctx.gather_ceiling(vol, v, gimg, gcount, stream=stream)
+        torch.cuda.synchronize()
+        gsamples += int(gcount.sum().item())
+    it = iter(views * 2)
+    t_gc = _timed(stream, lambda: (lambda v: ctx.gather_ceiling(vol, v, gimg, stream=stream))(next(it)), nv)
+    ceiling = gsamples / len(views) / t_gc / 1e9
     ctx.poll_status(stream)
     del scratch
     peak, peak_kind = peaks()
@@ -612,6 +633,11 @@ def fp_bp_split(ctx, c, vol, proj, gmax, dev, stream) -> dict:
     return {"views_timed": nv, "fp_s_per_view": t_fp, "bp_voxel_s_per_view": t_bpv, "bp_ray_s_per_view": t_bpr,
             "fp_gups": N ** 3 / t_fp / 1e9, "bp_voxel_gups": N ** 3 / t_bpv / 1e9, "bp_ray_gups": N ** 3 / t_bpr / 1e9,
             "samples_per_view": samples, "fp_gsamples_per_s": samples / t_fp / 1e9,
+            "gather_ceiling": {"gsamples_per_s": ceiling, "s_per_view": t_gc,
+                               "samples_per_view": gsamples / len(views),
+                               "fp_frac": samples / t_fp / 1e9 / ceiling,
+                               "kernel": "k_gather_ceiling (stt_gather_ceiling): the projector's cell, 8 gathers "
+                                         "and trilinear interpolation per sample, packed pairs, no march control"},
             "roofline": {"bound": "hbm", "kernel": "k_fp_corr / k_fp_corr_slab (forward projection + correction)",
                          "achieved": fp_bytes / t_fp / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": fp_bytes / t_fp / 1e9 / peak, "peak_source": peak_kind,
@@ -779,9 +805,21 @@ def config_bench(cid, args, dev, stream, rank=0, full=False) -> dict:
            "metric": "projector GUPS over one iteration", "unit": "GUPS", "dtype": "f32", "variants": {}}
     reps = 3 if N <= 256 else 2
     out["tuning"] = ctx.autotune(stream)  # the launch choices for this geometry (untimed)
+    storages = c.get("storages", ("f32",))
     for bp in c["bps"]:
-        out["variants"][f"f32_{bp}"] = config_solve(cid, ctx, proj, truth, gmax, bp, dev, stream,
-                                                    c["iters"] if full else 1 + reps, reps)
+        res = {}
+        for sto in storages:
+            v = config_solve(cid, ctx, proj, truth, gmax, bp, dev, stream, c["iters"] if full else 1 + reps, reps,
+                             storage=sto, keep=len(storages) > 1)
+            res[sto] = v.pop("_result", None)
+            out["variants"][f"{sto}_{bp}"] = v
+            torch.cuda.empty_cache()
+        if "bf16" in res and "f32" in res:
+            # BF16 storage against FP32 storage after the same iterations (the
+            # FP32 solve's own error against FP64 is the fp64_check leg's)
+            a, b = res["bf16"], res["f32"]
+            out["variants"][f"bf16_{bp}"]["rel_l2_to_f32_storage"] = float((a - b).norm() / b.norm())
+        del res
         torch.cuda.empty_cache()
     out["value"] = out["variants"]["f32_voxel"]["gups"]
     out["ms_per_step"] = 1000.0 * out["variants"]["f32_voxel"]["s_per_iter"]

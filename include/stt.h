@@ -140,7 +140,7 @@ typedef struct stt_tuning {
     unsigned staged_bins;
     int tuned;       /* 0: the defaults; 1: set by stt_autotune or stt_set_tuning */
     int from_cache;  /* stt_autotune: the choice came from the cache (nothing timed) */
-    float fp_us[8], slab_us[8], bp_us[4];
+    float fp_us[12], slab_us[8], bp_us[4];
 } stt_tuning;
 stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream);
 stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out);
@@ -189,6 +189,11 @@ stt_status stt_fp_vjp(stt_ctx *ctx, const float *proj_bar, float *vol_bar, int v
  * outside [2, W-2) x [2, H-2) are left unchanged.  Deterministic. */
 stt_status stt_bp_voxel(stt_ctx *ctx, const float *corr, float *vol, double alpha, float gmax,
                         int view, void *stream);
+/* stt_bp_voxel on a volume stored as `dtype` (STT_DTYPE_BF16: each voxel is
+ * read widened to FP32, updated as in FP32 and stored rounded to nearest
+ * even; the correction stays FP32). */
+stt_status stt_bp_voxel_typed(stt_ctx *ctx, const float *corr, void *vol, int dtype, double alpha, float gmax,
+                              int view, void *stream);
 
 /* Ray-driven (ST_Tomography.cpp:733-764, SingleScalarVolume.core.h:73-84):
  * scatters corr*w and w along every ray into the context's accumulators, then
@@ -196,6 +201,10 @@ stt_status stt_bp_voxel(stt_ctx *ctx, const float *corr, float *vol, double alph
  * accumulators reset.  Atomics: result is order-nondeterministic in the last bits. */
 stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, int view,
                       void *stream);
+/* stt_bp_ray on a volume stored as `dtype` (FP32 accumulators; BF16: the
+ * normalised update is added in FP32 and stored rounded to nearest even). */
+stt_status stt_bp_ray_typed(stt_ctx *ctx, const float *corr, void *vol, int dtype, float gmax, int view,
+                            void *stream);
 
 /* The backprojection mode of the reference's projector on its own: one
  * march of view `view` scattering contrib[v] += c*w and wsum[v] += w for the
@@ -205,6 +214,19 @@ stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, i
  * (TypicalRayProducer.cpp:78-96).  Atomic float adds: the summation order,
  * not the terms, differs from the reference's sequential loop. */
 stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, float *wsum, int view,
+                              void *stream);
+
+/* The gather ceiling of the forward projector (a measurement; no
+ * counterpart in the reference).  Every ray of view `view` takes as many
+ * samples as its clip length holds, at the projector's step from its entry
+ * point, with the projector's cell, 8-corner gather and trilinear
+ * interpolation (packed != 0: pairs of samples in packed FP32x2
+ * instructions) and none of the march's control (no block splits, no
+ * per-sample bound checks, a plain sum).  out[W*H] receives the sums times the
+ * step, count[W*H] (may be NULL) the samples per ray.  Timed against stt_fp,
+ * it says how far the projector is from the rate its gathers alone reach.
+ * Volumes below 2^31 voxels. */
+stt_status stt_gather_ceiling(stt_ctx *ctx, const float *vol, int view, int packed, float *out, int *count,
                               void *stream);
 
 /* Ray-driven backprojection that allocates no device memory.  No counterpart
@@ -233,6 +255,15 @@ stt_status stt_bp_ray_noalloc(stt_ctx *ctx, const float *corr, float *vol, float
 stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, const int *perm,
                           int nperm, int view_offset, double alpha, float gmax, int bp_mode,
                           float *raylen_state, const int *roi_cut, void *stream);
+/* stt_sart_sweep with the volume and the projection stack both stored as
+ * `dtype`.  STT_DTYPE_BF16: the forward projector gathers from the BF16
+ * volume (taps widened exactly to FP32; FP32 march, Kahan sums and
+ * correction), every view's backprojection stores its update rounded to
+ * nearest even, and every view gathers (no slab staging).  The ray-length
+ * state, the corrections and the accumulators stay FP32. */
+stt_status stt_sart_sweep_typed(stt_ctx *ctx, void *vol, int dtype, const void *proj_stack, const int *perm,
+                                int nperm, int view_offset, double alpha, float gmax, int bp_mode,
+                                float *raylen_state, const int *roi_cut, void *stream);
 
 /* Host helper: the seeded view permutation that replaces srand(time(0)) +
  * random_shuffle (ST_Tomography.cpp:635-642): SplitMix64 + Fisher-Yates. */
@@ -295,6 +326,10 @@ stt_status stt_roi_mask(stt_ctx *ctx, const int *cut, float *roi, void *stream);
  * vel: 3 planar channels.  dim (HOST) is independent of the geometry. */
 stt_status stt_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
                     float *out, void *stream);
+/* stt_warp of a source stored as `dtype` (STT_DTYPE_BF16: taps widened
+ * exactly to FP32); the flow and the output are FP32. */
+stt_status stt_warp_typed(const int *dim, const float *vel, const void *src, int dtype, int nc, float dt,
+                          float *out, void *stream);
 /* Vector-Jacobian product of stt_warp: src_bar += J_src^T out_bar and
  * vel_bar += J_vel^T out_bar (either may be NULL; both accumulate with atomics). */
 stt_status stt_warp_vjp(const int *dim, const float *vel, const float *src, int nc, float dt,
@@ -413,6 +448,16 @@ typedef struct stt_solve_cfg {
     /* Non-zero: stt_solver_create runs stt_autotune on the context first
      * (unless it is tuned already). */
     int autotune;
+    /* Storage of the primal volumes and the sinogram (stt_dtype).
+     * STT_DTYPE_BF16: state.vol, xbar, xprev and proj point to arrays of BF16
+     * values (the upper 16 bits of an FP32; pass them cast to float*), half
+     * the memory of FP32.  Every kernel widens what it reads exactly to FP32,
+     * computes in FP32 as the FP32 solve does, and rounds what it stores to
+     * nearest even; the duals (ytv, ytp, ybc), the flow and all scratch stay
+     * FP32, and the forward projector gathers for every view (no slab
+     * staging).  A result then carries the BF16 rounding of every stored
+     * update. */
+    int storage;
 } stt_solve_cfg;
 
 typedef struct stt_pd_state {
@@ -470,6 +515,8 @@ typedef struct stt_instance {
     int roi_cut[8];
     unsigned long long seed;
     int autotune;         /* non-zero: tune the instance's context at stt_batch_create (stt_autotune) */
+    int storage;          /* stt_dtype of vol and proj (and of the instance's primal state): see
+                             stt_solve_cfg.storage */
 } stt_instance;
 
 typedef struct stt_batch stt_batch;

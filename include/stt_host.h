@@ -69,8 +69,8 @@ void stt_host_free(void *p);
  * reference (CImg lists, VolumeData.h:97-98, ST_Tomography.cpp:355).
  *
  * stt_host_solver_create: geometry and solve configuration as for
- * stt_set_geometry / stt_solver_create (cfg->halo must be 0; use
- * STT_SOLVE_GRAPH); `slots` (1..8) complete copies of the device state are
+ * stt_set_geometry / stt_solver_create (cfg->halo must be 0, cfg->storage
+ * STT_DTYPE_F32; use STT_SOLVE_GRAPH); `slots` (1..8) complete copies of the device state are
  * allocated on the current stt_host_set_device device, so that with 2 slots a
  * step's upload and the previous step's read-back overlap a step's compute.
  *

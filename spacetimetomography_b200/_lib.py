@@ -42,7 +42,7 @@ class SolveCfg(C.Structure):
     _fields_ = [("n_frames", C.c_int), ("views_per_frame", C.c_int), ("bp_mode", C.c_int),
                 ("alpha", C.c_double), ("pd", PdParams), ("roi_cut", C.c_int * 8),
                 ("seed", C.c_ulonglong), ("mode", C.c_int), ("halo", C.c_int), ("frame_offset", C.c_int),
-                ("total_frames", C.c_int), ("autotune", C.c_int)]
+                ("total_frames", C.c_int), ("autotune", C.c_int), ("storage", C.c_int)]
 
 
 class PdState(C.Structure):
@@ -66,14 +66,14 @@ class OpNorm(C.Structure):
 class Instance(C.Structure):
     _fields_ = [("ctx", C.c_void_p), ("vol", C.c_void_p), ("proj", C.c_void_p), ("n_views", C.c_int),
                 ("bp_mode", C.c_int), ("alpha", C.c_double), ("pd", PdParams), ("roi_cut", C.c_int * 8),
-                ("seed", C.c_ulonglong), ("autotune", C.c_int)]
+                ("seed", C.c_ulonglong), ("autotune", C.c_int), ("storage", C.c_int)]
 
 
 class Tuning(C.Structure):
     """stt_tuning (include/stt.h): launch choices and the autotuner's timings."""
     _fields_ = [("fp_variant", C.c_int), ("slab_variant", C.c_int), ("bp_variant", C.c_int),
                 ("staged_bins", C.c_uint), ("tuned", C.c_int), ("from_cache", C.c_int),
-                ("fp_us", C.c_float * 8), ("slab_us", C.c_float * 8), ("bp_us", C.c_float * 4)]
+                ("fp_us", C.c_float * 12), ("slab_us", C.c_float * 8), ("bp_us", C.c_float * 4)]
 
 
 def _load() -> C.CDLL:
@@ -95,6 +95,12 @@ def _load() -> C.CDLL:
         "stt_fp_vjp": [vp, vp, vp, i, i, vp],
         "stt_bp_voxel": [vp, vp, vp, d, f, i, vp],
         "stt_bp_ray": [vp, vp, vp, f, i, vp],
+        "stt_bp_ray_scatter": [vp, vp, vp, vp, i, vp],
+        "stt_gather_ceiling": [vp, vp, i, i, vp, vp, vp],
+        "stt_sart_sweep_typed": [vp, vp, i, vp, vp, i, i, d, f, i, vp, vp, vp],
+        "stt_bp_voxel_typed": [vp, vp, vp, i, d, f, i, vp],
+        "stt_bp_ray_typed": [vp, vp, vp, i, f, i, vp],
+        "stt_warp_typed": [vp, vp, vp, i, i, f, vp, vp],
         "stt_sart_sweep": [vp, vp, vp, vp, i, i, d, f, i, vp, vp, vp],
         "stt_pd_dual": [vp, C.POINTER(PdParams), vp, vp, vp, vp, vp, vp, vp],
         "stt_pd_primal": [vp, C.POINTER(PdParams), i, vp, vp, vp, vp, vp, vp, vp, vp],

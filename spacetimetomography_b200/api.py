@@ -21,6 +21,17 @@ from ._lib import PdParams as _PdParams
 REFERENCE_CUT = (8, 8, 8, 45, 8, 8, 30, 20)
 
 
+def _dtype_code(t) -> int:
+    """stt_dtype of a tensor's storage: float32 -> STT_DTYPE_F32, bfloat16 -> STT_DTYPE_BF16."""
+    import torch
+
+    if t.dtype == torch.float32:
+        return 0
+    if t.dtype == torch.bfloat16:
+        return 1
+    raise ValueError(f"libstt stores float32 or bfloat16, not {t.dtype}")
+
+
 def _ptr(t) -> C.c_void_p | None:
     if t is None:
         return None
@@ -162,7 +173,7 @@ class Context:
     def _tuning_dict(t: Tuning) -> dict:
         return {"fp_variant": t.fp_variant, "slab_variant": t.slab_variant, "bp_variant": t.bp_variant,
                 "staged_bins": t.staged_bins, "tuned": bool(t.tuned), "from_cache": bool(t.from_cache),
-                "fp_us": list(t.fp_us)[:7], "slab_us": list(t.slab_us)[:4], "bp_us": list(t.bp_us)[:3],
+                "fp_us": list(t.fp_us)[:10], "slab_us": list(t.slab_us)[:4], "bp_us": list(t.bp_us)[:3],
                 "fp": (lib.stt_tuning_variant_name(0, t.fp_variant) or b"").decode(),
                 "slab": (lib.stt_tuning_variant_name(1, t.slab_variant) or b"").decode(),
                 "bp": (lib.stt_tuning_variant_name(2, t.bp_variant) or b"").decode()}
@@ -194,22 +205,41 @@ class Context:
         return vol_bar
 
     def bp_voxel(self, corr, vol, alpha, gmax, view, stream=None):
-        self._chk(lib.stt_bp_voxel(self._h, _ptr(corr), _ptr(vol), float(alpha), float(gmax), view,
-                                   _stream(stream)))
+        """vol: float32, or bfloat16 (BF16 storage, stt_bp_voxel_typed)."""
+        self._chk(lib.stt_bp_voxel_typed(self._h, _ptr(corr), _ptr(vol), _dtype_code(vol), float(alpha),
+                                         float(gmax), view, _stream(stream)))
         return vol
 
     def bp_ray(self, corr, vol, gmax, view, stream=None):
-        self._chk(lib.stt_bp_ray(self._h, _ptr(corr), _ptr(vol), float(gmax), view, _stream(stream)))
+        """vol: float32, or bfloat16 (BF16 storage, stt_bp_ray_typed)."""
+        self._chk(lib.stt_bp_ray_typed(self._h, _ptr(corr), _ptr(vol), _dtype_code(vol), float(gmax), view,
+                                       _stream(stream)))
         return vol
+
+    def gather_ceiling(self, vol, view, out, count=None, packed=True, stream=None):
+        """stt_gather_ceiling: the projector's gathers and interpolation alone
+        along view `view`'s rays (a measurement kernel)."""
+        self._chk(lib.stt_gather_ceiling(self._h, _ptr(vol), view, int(packed), _ptr(out),
+                                         _ptr(count) if count is not None else None, _stream(stream)))
+
+    def bp_ray_scatter(self, corr, contrib, wsum, view, stream=None):
+        """The ray-driven backprojection's raw accumulation: contrib += c*w and
+        wsum += w over every sample's 8 corners (stt_bp_ray_scatter)."""
+        self._chk(lib.stt_bp_ray_scatter(self._h, _ptr(corr), _ptr(contrib), _ptr(wsum), view, _stream(stream)))
 
     def sart_sweep(self, vol, proj_stack, perm, alpha, gmax, bp_mode, raylen_state,
                    view_offset=0, roi_cut=None, stream=None):
+        """vol and proj_stack: both float32, or both bfloat16 (BF16 storage,
+        stt_sart_sweep_typed)."""
         perm = np.ascontiguousarray(perm, dtype=np.int32)
         cut = None if roi_cut is None else (C.c_int * 8)(*map(int, roi_cut))
-        self._chk(lib.stt_sart_sweep(self._h, _ptr(vol), _ptr(proj_stack),
-                                     perm.ctypes.data_as(C.c_void_p), len(perm), view_offset,
-                                     float(alpha), float(gmax), int(bp_mode), _ptr(raylen_state),
-                                     cut, _stream(stream)))
+        code = _dtype_code(vol)
+        if _dtype_code(proj_stack) != code:
+            raise ValueError("vol and proj_stack must have the same dtype")
+        self._chk(lib.stt_sart_sweep_typed(self._h, _ptr(vol), code, _ptr(proj_stack),
+                                           perm.ctypes.data_as(C.c_void_p), len(perm), view_offset,
+                                           float(alpha), float(gmax), int(bp_mode), _ptr(raylen_state),
+                                           cut, _stream(stream)))
         return vol
 
     # ---- primal-dual -------------------------------------------------------
@@ -244,8 +274,9 @@ def warp(flow, src, dt, out=None, stream=None):
     nz, ny, nx = src.shape[-3:]
     dim = (C.c_int * 3)(nx, ny, nz)
     if out is None:
-        out = torch.empty_like(src)
-    check(lib.stt_warp(dim, _ptr(flow), _ptr(src), nc, float(dt), _ptr(out), _stream(stream)))
+        out = torch.empty_like(src, dtype=torch.float32)
+    check(lib.stt_warp_typed(dim, _ptr(flow), _ptr(src), _dtype_code(src), nc, float(dt), _ptr(out),
+                             _stream(stream)))
     return out
 
 
@@ -418,17 +449,28 @@ class Solver:
     def __init__(self, ctx: Context, state: dict, n_frames: int, views_per_frame: int,
                  pd: PdParams, alpha: float = 0.3, bp_mode: int = 0, roi_cut=REFERENCE_CUT,
                  seed: int = 0, mode: int = SOLVE_GRAPH, halo: bool = False, frame_offset: int = 0,
-                 total_frames: int = 0, autotune: bool = False):
+                 total_frames: int = 0, autotune: bool = False, storage: str = "f32"):
         """halo=True: local frame 0 continues a previous shard (state needs
         ytp_halo, ybc_halo, flow_halo; see spacetimetomography_b200.halo).
         frame_offset / total_frames: the shard's place in the whole sequence
         (its view orders are those of the unsharded solve).  autotune: tune
-        the context's launch choices first (Context.autotune)."""
+        the context's launch choices first (Context.autotune).
+        storage="bf16": vol, xbar, xprev and proj are torch.bfloat16 tensors
+        (stt_solve_cfg.storage = STT_DTYPE_BF16); every other array stays
+        float32."""
+        import torch
+
+        if storage not in ("f32", "bf16"):
+            raise ValueError("storage must be 'f32' or 'bf16'")
+        want = torch.bfloat16 if storage == "bf16" else torch.float32
+        for k in ("vol", "xbar", "xprev", "proj"):
+            if state[k].dtype != want:
+                raise ValueError(f"state[{k!r}] must be {want} for storage={storage!r}")
         self.ctx = ctx
         self.state = state  # keeps the tensors alive
         cfg = SolveCfg(n_frames, views_per_frame, bp_mode, float(alpha), pd.c(),
                        (C.c_int * 8)(*map(int, roi_cut)), C.c_ulonglong(seed), mode, int(bool(halo)),
-                       int(frame_offset), int(total_frames), int(bool(autotune)))
+                       int(frame_offset), int(total_frames), int(bool(autotune)), 1 if storage == "bf16" else 0)
         keys = ("vol", "xbar", "xprev", "ytv", "ytp", "ybc", "flow", "proj", "ytp_halo", "ybc_halo",
                 "flow_halo")
         st = PdState(*[state[k].data_ptr() if k in state else None for k in keys])
@@ -477,17 +519,25 @@ class Batch:
 
     Each instance is a dict: ctx (Context with its geometry), vol (nz, ny, nx)
     CUDA tensor (start in, result out), proj (V, H, W) CUDA tensor, and
-    optionally bp_mode, alpha, pd (PdParams), roi_cut, seed."""
+    optionally bp_mode, alpha, pd (PdParams), roi_cut, seed, autotune and
+    storage ("f32", or "bf16" with vol and proj torch.bfloat16 tensors)."""
 
     def __init__(self, instances, mode: int = SOLVE_GRAPH):
+        import torch
+
         self._keep = instances
         arr = (Instance * len(instances))()
         for k, d in enumerate(instances):
             pd = d.get("pd", PdParams())
+            storage = d.get("storage", "f32")
+            want = {"f32": torch.float32, "bf16": torch.bfloat16}.get(storage)
+            if want is None or d["vol"].dtype != want or d["proj"].dtype != want:
+                raise ValueError(f"instance {k}: vol and proj must be {want} for storage={storage!r}")
             arr[k] = Instance(d["ctx"]._h, d["vol"].data_ptr(), d["proj"].data_ptr(), int(d["proj"].shape[0]),
                               int(d.get("bp_mode", 0)), float(d.get("alpha", 0.3)), pd.c(),
                               (C.c_int * 8)(*map(int, d.get("roi_cut", REFERENCE_CUT))),
-                              C.c_ulonglong(int(d.get("seed", 0))), int(bool(d.get("autotune", False))))
+                              C.c_ulonglong(int(d.get("seed", 0))), int(bool(d.get("autotune", False))),
+                              1 if storage == "bf16" else 0)
         h = C.c_void_p()
         rc = lib.stt_batch_create(arr, len(instances), int(mode), C.byref(h))
         if rc != 0:

@@ -98,6 +98,8 @@ extern "C" {
 int stt_host_solver_create(const stt_geometry *g, const stt_solve_cfg *cfg, int slots, stt_host_solver **out) {
     if (!g || !cfg || !out || slots < 1 || slots > 8) return set_error("null argument or slots outside 1..8"), STT_ERR_INVALID;
     if (cfg->halo) return set_error("the host solver runs whole sequences (no halo)"), STT_ERR_UNSUPPORTED;
+    if (cfg->storage != STT_DTYPE_F32)
+        return set_error("the host solver takes FP32 host arrays (storage must be STT_DTYPE_F32)"), STT_ERR_UNSUPPORTED;
     *out = nullptr;
     stt_host_solver *h = new stt_host_solver();
     h->device = stt_facade::g_device;

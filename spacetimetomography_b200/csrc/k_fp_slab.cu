@@ -24,6 +24,7 @@
 
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
+#include "stt_slab.cuh"
 #include "stt_tma.cuh"
 
 namespace stt {
@@ -49,116 +50,38 @@ using Box3 = SlabBox<40, 8, 16>;
 constexpr long long WAIT_CYCLES = 200000000LL;  // about 0.1 s: a copy that never lands is an error
 constexpr int WARPS = 4;                         // a block is 32 x WARPS detector pixels, one warp per row
 
-__device__ __forceinline__ int warp_min(int v) { return __reduce_min_sync(0xffffffffu, v); }
-
-// Block-wide minima of (a, b), through red[0..2*WARPS).  One barrier.
-__device__ __forceinline__ void block_min2(int &a, int &b, int *red) {
-    a = warp_min(a);
-    b = warp_min(b);
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-        red[2 * w] = a;
-        red[2 * w + 1] = b;
-    }
-    __syncthreads();
-    a = red[0];
-    b = red[1];
-#pragma unroll
-    for (int k = 1; k < WARPS; ++k) {
-        a = min(a, red[2 * k]);
-        b = min(b, red[2 * k + 1]);
-    }
-}
-
-template <bool ZF>
-struct SlabAxes {
-    static constexpr int F = ZF ? 2 : 0;  // contiguous axis of the copy
-    static constexpr int S = ZF ? 0 : 2;  // slowest axis: the slab axis
-};
-
-// Lowest (fast, y) base coordinates of the taps of this ray's samples whose
-// slow coordinate lies in [m0, m0 + SLAB), with a voxel of margin; INT_MAX
-// when the ray has none there.
-template <bool ZF, class BX>
-__device__ __forceinline__ void ray_box_low(const GeomDev &g, const Ray &r, bool hit, int m0, int &lf, int &ly) {
-    constexpr int SLAB = BX::SLAB;
-    constexpr int F = SlabAxes<ZF>::F, S = SlabAxes<ZF>::S;
-    lf = INT_MAX;
-    ly = INT_MAX;
-    if (!hit) return;
-    const float ta = __fdividef((float)m0 - 0.5f - r.vz[S], r.vu[S]);
-    const float tb = __fdividef((float)(m0 + SLAB) + 0.5f - r.vz[S], r.vu[S]);
-    const float tl = fmaxf(fminf(ta, tb), r.tnear - g.sd), th = fminf(fmaxf(ta, tb), r.tfar + g.sd);
-    if (!(tl <= th)) return;
-    const int dimF = ZF ? g.nz : g.nx;
-    const float f = fminf(r.vz[F] + r.vu[F] * tl, r.vz[F] + r.vu[F] * th);
-    const float y = fminf(r.vz[1] + r.vu[1] * tl, r.vz[1] + r.vu[1] * th);
-    lf = (int)floorf(fminf(fmaxf(f, 0.0f), (float)(dimF - 1))) - 1;
-    ly = (int)floorf(fminf(fmaxf(y, 0.0f), (float)(g.ny - 1))) - 1;
-}
-
 // The march of one ray of the block, summed into `acc`, taps from the staged
 // slabs where they are held.
 template <bool ZF, class BX>
 __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap *map, const float *__restrict__ src,
                                              bool hit, const Ray &r, float *buf, uint64_t *bar, int *red_s,
                                              int (*red)[2 * WARPS], volatile int *dead, int *status, Kahan &acc) {
-    constexpr int S = SlabAxes<ZF>::S;
     constexpr int FB = BX::FB, YB = BX::YB, SB = BX::SB, BOXN = BX::N, SLAB = BX::SLAB;
     constexpr unsigned BOX_BYTES = BX::BYTES;
-    const int dimS = ZF ? g.nx : g.nz;
     const Strides st = ZF ? zyx_strides(g) : xyz_strides(g);
     MarchGen m;
     if (hit) m.init(g, r);
     else m.phase = 2;
 
     // The base planes the block's rays span and the direction they run in.
-    int lo = INT_MAX, nhi = INT_MAX, up = 0;
-    if (hit) {
-        const float a = r.vz[S] + r.vu[S] * r.tnear, b = r.vz[S] + r.vu[S] * r.tfar;
-        const float pl = fminf(fmaxf(fminf(a, b), 0.0f), (float)(dimS - 1));
-        const float ph = fminf(fmaxf(fmaxf(a, b), 0.0f), (float)(dimS - 1));
-        lo = min((int)pl, dimS - 2);
-        nhi = -min((int)ph, dimS - 2);
-        up = r.vu[S] > 0.0f ? 1 : -1;
-    }
-    lo = warp_min(lo);
-    nhi = warp_min(nhi);
-    up = __reduce_add_sync(0xffffffffu, up);
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-        red_s[3 * w] = lo;
-        red_s[3 * w + 1] = nhi;
-        red_s[3 * w + 2] = up;
-    }
-    if (threadIdx.x == 0) {
+    int lo, hi;
+    bool fwd;
+    slab::block_span<ZF, WARPS>(g, r, hit, red_s, lo, hi, fwd, [&] {
         tma::mbar_init(&bar[0], 1);
         tma::mbar_init(&bar[1], 1);
         tma::fence_barrier_init();
         tma::prefetch_map(map);
         *dead = 0;
-    }
-    __syncthreads();
-    lo = red_s[0];
-    nhi = red_s[1];
-    up = red_s[2];
-#pragma unroll
-    for (int k = 1; k < WARPS; ++k) {
-        lo = min(lo, red_s[3 * k]);
-        nhi = min(nhi, red_s[3 * k + 1]);
-        up += red_s[3 * k + 2];
-    }
+    });
     if (lo == INT_MAX) return;  // no ray of the block hits the volume
-    const int hi = -nhi;
-    const bool fwd = up >= 0;
     const int nslab = (hi - lo) / SLAB + 1;
     auto slab_m0 = [&](int k) { return fwd ? lo + k * SLAB : hi - (SLAB - 1) - k * SLAB; };
 
     // slab 0
     int f0, y0;
     {
-        ray_box_low<ZF, BX>(g, r, hit, slab_m0(0), f0, y0);
-        block_min2(f0, y0, red[0]);
+        slab::ray_box_low<ZF, SLAB>(g, r, hit, slab_m0(0), f0, y0);
+        slab::block_min2<WARPS>(f0, y0, red[0]);
         if (f0 == INT_MAX) f0 = y0 = 0;
         f0 = (f0 >> 2) << 2;  // the box's innermost coordinate starts on 16 bytes
         if (threadIdx.x == 0) {
@@ -172,8 +95,8 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
         // issue slab k+1 into the other buffer (free since the barrier that ended slab k-1)
         int fn = 0, yn = 0;
         if (k + 1 < nslab && !gave_up) {
-            ray_box_low<ZF, BX>(g, r, hit, slab_m0(k + 1), fn, yn);
-            block_min2(fn, yn, red[(k + 1) & 1]);
+            slab::ray_box_low<ZF, SLAB>(g, r, hit, slab_m0(k + 1), fn, yn);
+            slab::block_min2<WARPS>(fn, yn, red[(k + 1) & 1]);
             if (fn == INT_MAX) fn = yn = 0;
             fn = (fn >> 2) << 2;
             if (threadIdx.x == 0) {

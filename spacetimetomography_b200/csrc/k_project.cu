@@ -31,7 +31,7 @@ __device__ __forceinline__ bool tile_pixel(const GeomDev &g, int &i, int &j) {
 // (the samples are added one by one in march order).
 constexpr int FP_GROUP = 4;
 
-template <int FAST, typename I, int G = FP_GROUP, typename T>
+template <int FAST, typename I, int G = FP_GROUP, bool PK = false, typename T>
 __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__restrict__ src, const Strides &st,
                                                  const Ray &r, int *count) {
     Kahan acc{0.0f, 0.0f};
@@ -49,24 +49,41 @@ __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__re
         [&](const float (*p)[3]) {
             FpCell c[G];
             float v[G][8];
+            if constexpr (PK) {  // pairs of samples in the packed FP32x2 instructions
+                static_assert(G % 2 == 0, "samples go in packed pairs");
 #pragma unroll
-            for (int i = 0; i < G; ++i) {
-                fp_cell(g, p[i], c[i]);
-                fp_corners<FAST, I>(src, st, c[i], v[i]);
+                for (int i = 0; i < G; i += 2) {
+                    fp_cell2(g, p[i], p[i + 1], c[i], c[i + 1]);
+                    fp_corners<FAST, I>(src, st, c[i], v[i]);
+                    fp_corners<FAST, I>(src, st, c[i + 1], v[i + 1]);
+                }
+                const float2 sd2 = make_float2(g.sd, g.sd);
+#pragma unroll
+                for (int i = 0; i < G; i += 2) {
+                    const float2 s = __fmul2_rn(trilerp2(v[i], v[i + 1], c[i], c[i + 1]), sd2);
+                    acc.add(s.x);
+                    acc.add(s.y);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < G; ++i) {
+                    fp_cell(g, p[i], c[i]);
+                    fp_corners<FAST, I>(src, st, c[i], v[i]);
+                }
+#pragma unroll
+                for (int i = 0; i < G; ++i) acc.add(__fmul_rn(trilerp(v[i], c[i]), g.sd));
             }
-#pragma unroll
-            for (int i = 0; i < G; ++i) acc.add(__fmul_rn(trilerp(v[i], c[i]), g.sd));
             n += G;
         });
     if (count) *count = n;
     return acc.s;
 }
 
-template <typename I, int G = FP_GROUP, typename T>
+template <typename I, int G = FP_GROUP, bool PK = false, typename T>
 __device__ __forceinline__ float fp_ray_sum(const GeomDev &g, const ViewRec &v, const T *__restrict__ vol,
                                             const T *__restrict__ vol_t, const Ray &r, int *count) {
-    if (vol_t && v.layout == 1) return fp_ray_sum_from<2, I, G>(g, vol_t, zyx_strides(g), r, count);
-    return fp_ray_sum_from<0, I, G>(g, vol, xyz_strides(g), r, count);
+    if (vol_t && v.layout == 1) return fp_ray_sum_from<2, I, G, PK>(g, vol_t, zyx_strides(g), r, count);
+    return fp_ray_sum_from<0, I, G, PK>(g, vol, xyz_strides(g), r, count);
 }
 
 // Detector tile of a block of NW warps for the tunable projector variants:
@@ -109,13 +126,18 @@ __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__re
 // c = (b - Ax) / (L + 1)).  L is the sticky ray length of the producer:
 // updated where the ray hits, kept where it misses; with no state buffer
 // (ray-based SART, whose producer is reset after every view) a miss gives L = 0.
-// Tunable variants (fp_variant_name): the block's detector tile (WX, NW) and
-// the samples in flight per step (G) change only which thread projects which
-// ray and how far ahead its loads run, never a ray's arithmetic.
-template <typename I, int WX = 32, int NW = 4, int G = FP_GROUP>
+// Tunable variants (fp_variant_name): the block's detector tile (WX, NW), the
+// samples in flight per step (G) and whether pairs of samples share packed
+// FP32x2 instructions (PK) change only which thread projects which ray, how
+// far ahead its loads run and how many instructions carry the same roundings,
+// never a ray's arithmetic.
+// T, B: the storage of the volume and of the sinogram stack (float, or BF16
+// bits widened exactly to FP32).
+template <typename I, int WX = 32, int NW = 4, int G = FP_GROUP, bool PK = false, typename T = float,
+          typename B = float>
 __global__ void __launch_bounds__(32 * NW) k_fp_corr(const GeomDev g, const ViewRec *__restrict__ views,
-                                                     const float *__restrict__ vol, const float *__restrict__ vol_t,
-                                                     const ViewSel sel, const float *__restrict__ b_stack,
+                                                     const T *__restrict__ vol, const T *__restrict__ vol_t,
+                                                     const ViewSel sel, const B *__restrict__ b_stack,
                                                      float *__restrict__ raylen_state,
                                                      float *__restrict__ corr, unsigned long long corr_surf,
                                                      int skip_staged) {
@@ -123,7 +145,7 @@ __global__ void __launch_bounds__(32 * NW) k_fp_corr(const GeomDev g, const View
     if (!tile_pixel_t<WX, NW>(g, i, j)) return;
     int local;
     const int view = sel_view(sel, local);
-    const float *b = b_stack + (size_t)local * g.W * g.H;
+    const B *b = b_stack + (size_t)local * g.W * g.H;
     const ViewRec &vr = views[view];
     if (skip_staged && vr.staged) return;  // the slab-staged kernel projects this view
     Ray r;
@@ -131,13 +153,13 @@ __global__ void __launch_bounds__(32 * NW) k_fp_corr(const GeomDev g, const View
     const size_t pix = i + (size_t)j * g.W;
     float L, sum = 0.0f;
     if (r.tnear < r.tfar) {
-        sum = fp_ray_sum<I, G>(g, vr, vol, vol_t, r, nullptr);
+        sum = fp_ray_sum<I, G, PK>(g, vr, vol, vol_t, r, nullptr);
         L = r.tfar - r.tnear;
         if (raylen_state) raylen_state[pix] = L;
     } else {
         L = raylen_state ? raylen_state[pix] : 0.0f;
     }
-    const float c = __fdiv_rn(__fsub_rn(__ldg(b + pix), sum), __fadd_rn(L, 1.0f));
+    const float c = __fdiv_rn(__fsub_rn(ld_voxel(b + pix), sum), __fadd_rn(L, 1.0f));
     corr[pix] = c;
     // the copy the voxel-driven backprojector gathers from with tld4
     if (corr_surf) surf2DLayeredwrite(c, corr_surf, i * (int)sizeof(float), j, 0, cudaBoundaryModeZero);
@@ -196,13 +218,13 @@ __global__ void __launch_bounds__(128) k_fp_adjoint(const GeomDev g, const ViewR
 // Ray-BP normalisation (ST_Tomography.cpp:746-762): vol += contrib/weight,
 // clamped with the reference macros so 0/0 = NaN becomes 0; the accumulator
 // is reset for the next view (TypicalRayProducer::Initial, TypicalRayProducer.cpp:91-95).
-__global__ void k_bp_ray_update(long long n, float2 *__restrict__ acc, float *__restrict__ vol,
-                                float gmax) {
+template <typename T>
+__global__ void k_bp_ray_update(long long n, float2 *__restrict__ acc, T *__restrict__ vol, float gmax) {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x) {
         float2 a = acc[k];
-        float v = vol[k] + __fdiv_rn(a.x, a.y);
-        vol[k] = rmax(rmin(gmax, v), 0.0f);
+        float v = ld_stored(vol + k) + __fdiv_rn(a.x, a.y);
+        st_stored(vol + k, rmax(rmin(gmax, v), 0.0f));
         acc[k] = make_float2(0.0f, 0.0f);
     }
 }
@@ -224,11 +246,12 @@ __global__ void k_acc_split(long long n, float2 *__restrict__ acc, float *__rest
 
 // Stand-alone SART correction (ST_Tomography.cpp:667-676) for the unfused
 // per-view form: the ray lengths are the sticky state k_fp updated on hits.
-__global__ void k_correction(long long n, const float *__restrict__ b, const float *__restrict__ ax,
+template <typename B>
+__global__ void k_correction(long long n, const B *__restrict__ b, const float *__restrict__ ax,
                              const float *__restrict__ raylen, float *__restrict__ corr) {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x)
-        corr[k] = __fdiv_rn(__fsub_rn(b[k], ax[k]), __fadd_rn(raylen ? raylen[k] : 0.0f, 1.0f));
+        corr[k] = __fdiv_rn(__fsub_rn(ld_voxel(b + k), ax[k]), __fadd_rn(raylen ? raylen[k] : 0.0f, 1.0f));
 }
 
 // z-fastest copy of an x-fastest volume: out[z + y*nz + x*nz*ny] = in[x + y*nx + z*nx*ny].
@@ -293,9 +316,10 @@ __global__ void __launch_bounds__(256) k_transpose_xz(int nx, int ny, int nz, co
 
 // The transpose, only if the selected view gathers from the z-fastest copy
 // (the choice is read on the device, so a captured graph can hold it).
+template <typename T>
 __global__ void __launch_bounds__(256) k_transpose_for_view(int nx, int ny, int nz,
                                                             const ViewRec *__restrict__ views, const ViewSel sel,
-                                                            const float *__restrict__ in, float *__restrict__ out) {
+                                                            const T *__restrict__ in, T *__restrict__ out) {
     int local;
     if (views[sel_view(sel, local)].layout != 1) return;
     transpose_tile(nx, ny, nz, in, out);
@@ -315,6 +339,80 @@ dim3 ray_grid(const GeomDev &g, int nviews) {
 }
 
 dim3 transpose_grid(const GeomDev &g) { return dim3((g.nx + 63) / 64, (g.nz + 63) / 64, g.ny); }
+
+// The gather ceiling of the forward projector: each ray of one view takes as
+// many samples as its clip length holds, at the projector's step from its
+// entry point, with the projector's cell, 8-corner gather and trilinear
+// interpolation (G = 4 samples' loads in flight, packed pairs when PK), and
+// none of its march control (no segment splits, no per-sample bound, a plain
+// sum).  No counterpart in the reference: a measurement of the rate the
+// gathers alone reach on a volume, the on-chip roofline of the projectors.
+template <int FAST, bool PK>
+__global__ void __launch_bounds__(128) k_gather_ceiling(const GeomDev g, const ViewRec *__restrict__ views, int view,
+                                                        const float *__restrict__ src, float *__restrict__ out,
+                                                        int *__restrict__ count) {
+    int i, j;
+    if (!tile_pixel(g, i, j)) return;
+    Ray r;
+    make_ray(g, views[view], i, j, r);
+    const size_t pix = i + (size_t)j * g.W;
+    float sum = 0.0f;
+    int n = 0;
+    if (r.tnear < r.tfar) {
+        const Strides st = FAST ? zyx_strides(g) : xyz_strides(g);
+        n = min((int)((r.tfar - r.tnear) / g.sd) + 1, 1 << 22);
+        float p[3], step[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            p[k] = __fmaf_rn(r.vu[k], r.tnear, r.vz[k]);  // explicit roundings: every instantiation alike
+            step[k] = __fmul_rn(r.vu[k], g.sd);
+        }
+        constexpr int G = 4;
+        int k = 0;
+        for (; k + G <= n; k += G) {
+            float q[G][3];
+            FpCell c[G];
+            float v[G][8];
+#pragma unroll
+            for (int s = 0; s < G; ++s)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) q[s][a] = __fmaf_rn((float)s, step[a], p[a]);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) p[a] = __fmaf_rn((float)G, step[a], p[a]);
+            if constexpr (PK) {
+#pragma unroll
+                for (int s = 0; s < G; s += 2) fp_cell2(g, q[s], q[s + 1], c[s], c[s + 1]);
+            } else {
+#pragma unroll
+                for (int s = 0; s < G; ++s) fp_cell(g, q[s], c[s]);
+            }
+#pragma unroll
+            for (int s = 0; s < G; ++s) fp_corners<FAST, int>(src, st, c[s], v[s]);
+            if constexpr (PK) {
+#pragma unroll
+                for (int s = 0; s < G; s += 2) {
+                    const float2 t = trilerp2(v[s], v[s + 1], c[s], c[s + 1]);
+                    sum = __fadd_rn(sum, __fadd_rn(t.x, t.y));
+                }
+            } else {  // the same additions as the packed form
+#pragma unroll
+                for (int s = 0; s < G; s += 2)
+                    sum = __fadd_rn(sum, __fadd_rn(trilerp(v[s], c[s]), trilerp(v[s + 1], c[s + 1])));
+            }
+        }
+        for (; k < n; ++k) {
+            FpCell c;
+            fp_cell(g, p, c);
+            float v[8];
+            fp_corners<FAST, int>(src, st, c, v);
+            sum = __fadd_rn(sum, trilerp(v, c));
+#pragma unroll
+            for (int a = 0; a < 3; ++a) p[a] = __fadd_rn(p[a], step[a]);
+        }
+    }
+    out[pix] = __fmul_rn(sum, g.sd);
+    if (count) count[pix] = n;
+}
 
 }  // namespace
 
@@ -355,13 +453,13 @@ cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, 
 
 namespace {
 
-// One launch of gather variant <WX, NW, G>: a block is NW warps of WX x (32/WX) pixels.
-template <int WX, int NW, int G>
+// One launch of gather variant <WX, NW, G, PK>: a block is NW warps of WX x (32/WX) pixels.
+template <int WX, int NW, int G, bool PK = false>
 void fp_corr_variant(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, const ViewSel &sel,
                      const float *b_stack, float *raylen_state, float *corr, cudaStream_t s,
                      unsigned long long corr_surf, int skip) {
     constexpr int TH = (32 / WX) * NW;  // detector rows per block
-    k_fp_corr<int, WX, NW, G><<<dim3((g.W + WX - 1) / WX, (g.H + TH - 1) / TH, 1), 32 * NW, 0, s>>>(
+    k_fp_corr<int, WX, NW, G, PK><<<dim3((g.W + WX - 1) / WX, (g.H + TH - 1) / TH, 1), 32 * NW, 0, s>>>(
         g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip);
 }
 
@@ -374,7 +472,10 @@ const char *fp_variant_name(int v) {
                                              "warps of 16x2 rays, 16x8 per block, 4 in flight",
                                              "warps of 8x4 rays, 8x16 per block, 4 in flight",
                                              "32x4 rays per block, 2 in flight",
-                                             "32x4 rays per block, 8 in flight"};
+                                             "32x4 rays per block, 8 in flight",
+                                             "32x4 rays per block, 4 in flight, packed pairs",
+                                             "32x4 rays per block, 8 in flight, packed pairs",
+                                             "32x8 rays per block, 4 in flight, packed pairs"};
     return v >= 0 && v < kFpVariants ? names[v] : "?";
 }
 
@@ -400,6 +501,9 @@ cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *
     case 4: fp_corr_variant<8, 4, 4>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
     case 5: fp_corr_variant<32, 4, 2>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
     case 6: fp_corr_variant<32, 4, 8>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    case 7: fp_corr_variant<32, 4, 4, true>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    case 8: fp_corr_variant<32, 4, 8, true>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    case 9: fp_corr_variant<32, 8, 4, true>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
     default: fp_corr_variant<32, 4, 4>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
     }
     return cudaGetLastError();
@@ -428,30 +532,71 @@ cudaError_t launch_transpose_bf16(const GeomDev &g, const unsigned short *in, un
 
 cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *in,
                                       float *out, cudaStream_t s) {
-    k_transpose_for_view<<<transpose_grid(g), dim3(32, 8), 0, s>>>(g.nx, g.ny, g.nz, views, sel, in, out);
+    k_transpose_for_view<float><<<transpose_grid(g), dim3(32, 8), 0, s>>>(g.nx, g.ny, g.nz, views, sel, in, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, const ViewSel &sel,
+                                      const unsigned short *in, unsigned short *out, cudaStream_t s) {
+    k_transpose_for_view<unsigned short><<<transpose_grid(g), dim3(32, 8), 0, s>>>(g.nx, g.ny, g.nz, views, sel, in,
+                                                                                  out);
     return cudaGetLastError();
 }
 
 cudaError_t launch_correction(long long n, const float *b, const float *ax, const float *raylen,
                               float *corr, cudaStream_t s) {
-    k_correction<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, b, ax, raylen, corr);
+    k_correction<float><<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, b, ax, raylen, corr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_correction(long long n, const unsigned short *b, const float *ax, const float *raylen,
+                              float *corr, cudaStream_t s) {
+    k_correction<unsigned short><<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, b, ax, raylen, corr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
+                           const unsigned short *vol_t, const ViewSel &sel, const unsigned short *b_stack,
+                           float *raylen_state, float *corr, cudaStream_t s, unsigned long long corr_surf) {
+    typedef unsigned short U;
+    if (small_volume(g))
+        k_fp_corr<int, 32, 4, FP_GROUP, false, U, U><<<ray_grid(g, 1), 128, 0, s>>>(
+            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, 0);
+    else
+        k_fp_corr<long long, 32, 4, FP_GROUP, false, U, U><<<ray_grid(g, 1), 128, 0, s>>>(
+            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, 0);
+    return cudaGetLastError();
+}
+
+// The scatter of the ray-driven backprojection: slab-staged below 2^31 voxels.
+static cudaError_t bp_ray_scatter_any(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
+                                      float2 *acc, cudaStream_t s) {
+    if (small_volume(g)) return launch_bp_ray_scatter_slab(g, views, sel, corr, acc, s);
+    k_bp_ray_scatter<<<ray_grid(g, 1), 128, 0, s>>>(g, views, sel, corr, acc);
     return cudaGetLastError();
 }
 
 cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                           float2 *acc, float *vol, float gmax, cudaStream_t s) {
-    k_bp_ray_scatter<<<ray_grid(g, 1), 128, 0, s>>>(g, views, sel, corr, acc);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = bp_ray_scatter_any(g, views, sel, corr, acc, s);
     if (e != cudaSuccess) return e;
     const long long n = (long long)g.nx * g.ny * g.nz;
-    k_bp_ray_update<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, acc, vol, gmax);
+    k_bp_ray_update<float><<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, acc, vol, gmax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
+                          float2 *acc, unsigned short *vol, float gmax, cudaStream_t s) {
+    cudaError_t e = bp_ray_scatter_any(g, views, sel, corr, acc, s);
+    if (e != cudaSuccess) return e;
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    k_bp_ray_update<unsigned short><<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, acc, vol, gmax);
     return cudaGetLastError();
 }
 
 cudaError_t launch_bp_ray_scatter(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                                   float2 *acc, float *contrib, float *wsum, cudaStream_t s) {
-    k_bp_ray_scatter<<<ray_grid(g, 1), 128, 0, s>>>(g, views, sel, corr, acc);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = bp_ray_scatter_any(g, views, sel, corr, acc, s);
     if (e != cudaSuccess) return e;
     const long long n = (long long)g.nx * g.ny * g.nz;
     k_acc_split<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, acc, contrib, wsum);
@@ -461,6 +606,19 @@ cudaError_t launch_bp_ray_scatter(const GeomDev &g, const ViewRec *views, const 
 cudaError_t launch_fp_adjoint(const GeomDev &g, const ViewRec *views, int view0, int nviews,
                               const float *proj_bar, float *vol_bar, cudaStream_t s) {
     k_fp_adjoint<<<ray_grid(g, nviews), 128, 0, s>>>(g, views, view0, proj_bar, vol_bar);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_ceiling(const GeomDev &g, const ViewRec *views, const ViewRec &host_view, int view,
+                                  const float *vol, const float *vol_t, int packed, float *out, int *count,
+                                  cudaStream_t s) {
+    if (!small_volume(g)) return cudaErrorInvalidValue;
+    const bool zf = vol_t && host_view.layout == 1;
+    const float *src = zf ? vol_t : vol;
+    if (zf && packed) k_gather_ceiling<2, true><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, out, count);
+    else if (zf) k_gather_ceiling<2, false><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, out, count);
+    else if (packed) k_gather_ceiling<0, true><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, out, count);
+    else k_gather_ceiling<0, false><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, out, count);
     return cudaGetLastError();
 }
 

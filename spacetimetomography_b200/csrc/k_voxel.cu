@@ -73,9 +73,12 @@ __device__ __forceinline__ float bp_sum(const float tap[4][4], const float wx[4]
     return val;
 }
 
-__device__ __forceinline__ void bp_update(float *__restrict__ vol, size_t o, float alpha, float val, float gmax) {
-    const float nv = __fmaf_rn(alpha, val, vol[o]);
-    vol[o] = rmax(rmin(gmax, nv), 0.0f);
+// T: the volume's storage (float, or BF16 bits widened to FP32 and rounded
+// back to nearest even on store).
+template <typename T>
+__device__ __forceinline__ void bp_update(T *__restrict__ vol, size_t o, float alpha, float val, float gmax) {
+    const float nv = __fmaf_rn(alpha, val, ld_stored(vol + o));
+    st_stored(vol + o, rmax(rmin(gmax, nv), 0.0f));
 }
 
 // The 4x4 footprint at (px, py): four tld4 gathers of the correction's
@@ -100,9 +103,9 @@ __device__ __forceinline__ void bp_taps(const GeomDev &g, const float *__restric
 }
 
 // One voxel, everything computed for it alone.
-template <bool TEX>
+template <bool TEX, typename T>
 __device__ __forceinline__ void bp_voxel_at(const GeomDev &g, const ViewRec &v, const float *__restrict__ corr,
-                                            unsigned long long tex, float *__restrict__ vol, int x, int y, int z,
+                                            unsigned long long tex, T *__restrict__ vol, int x, int y, int z,
                                             float alpha, float gmax) {
     const float fx = (float)x, fy = (float)y, fz = (float)z;
     const float ndepth = -bp_cam(v, 2, fx, fy, fz);
@@ -117,10 +120,10 @@ __device__ __forceinline__ void bp_voxel_at(const GeomDev &g, const ViewRec &v, 
     bp_update(vol, x + (size_t)y * g.nx + (size_t)z * g.nx * g.ny, alpha, bp_sum(tap, wx, wy), gmax);
 }
 
-template <bool TEX>
+template <bool TEX, typename T>
 __global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec *__restrict__ views,
                                                   const ViewSel sel, const float *__restrict__ corr,
-                                                  float *__restrict__ vol, float alpha, float gmax,
+                                                  T *__restrict__ vol, float alpha, float gmax,
                                                   unsigned long long corr_tex) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= g.nx) return;
@@ -144,9 +147,9 @@ constexpr int BP_COL = 16;
 // by texture latency, so the extra warps pay (10 blocks: 104.1 ms per
 // iteration of the 10 x 256^3 solve against 106.6 ms with the compiler's
 // 52 registers and 9 blocks).
-template <int K = BP_COL>
+template <int K = BP_COL, typename T = float>
 __global__ void __launch_bounds__(128, 10) k_bp_voxel_cols(const GeomDev g, const ViewRec *__restrict__ views,
-                                                       const ViewSel sel, float *__restrict__ vol, float alpha,
+                                                       const ViewSel sel, T *__restrict__ vol, float alpha,
                                                        float gmax, unsigned long long tex) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y0 = blockIdx.y * K, z = blockIdx.z;
@@ -203,10 +206,12 @@ __global__ void __launch_bounds__(128, 10) k_bp_voxel_cols(const GeomDev g, cons
 //   whole volume:     ytp += sigma*(xf1 - xf);  ybc += sigma*(bw - xf)
 //   interior & ROI:   ytv_c += sigma*(xf(p+e_c) - xf(p))*hf, clamp +-tv_w;
 //                     ytp = ytp*tp_w/(tp_w + 2 sigma);  ybc clamp +-bc_w
+// T: the storage of X_bar (the duals and the warped bw are FP32).
+template <typename T>
 __global__ void __launch_bounds__(128) k_pd_dual(int nx, int ny, int nz, float sigma, float tv_w,
                                                  float tp_w, float bc_w, float hf, Cut8 cut,
-                                                 const float *__restrict__ xf,
-                                                 const float *__restrict__ xf1,
+                                                 const T *__restrict__ xf,
+                                                 const T *__restrict__ xf1,
                                                  const float *__restrict__ bw, float *__restrict__ ytv,
                                                  float *__restrict__ ytp, float *__restrict__ ybc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -214,15 +219,15 @@ __global__ void __launch_bounds__(128) k_pd_dual(int nx, int ny, int nz, float s
     if (i >= nx) return;
     const size_t sy = nx, sz = (size_t)nx * ny, n = sz * nz;
     const size_t p = i + j * sy + k * sz;
-    const float x0 = __ldg(xf + p);
-    float tp = ytp[p] + sigma * (__ldg(xf1 + p) - x0);
+    const float x0 = ld_voxel(xf + p);
+    float tp = ytp[p] + sigma * (ld_voxel(xf1 + p) - x0);
     float bc = ybc[p] + sigma * (__ldg(bw + p) - x0);
     const bool inner = i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < nz - 1 &&
                        !roi_out(i, j, k, nx, ny, nz, cut.c);
     if (inner) {
-        float y0 = ytv[p] + sigma * (__ldg(xf + p + 1) - x0) * hf;
-        float y1 = ytv[p + n] + sigma * (__ldg(xf + p + sy) - x0) * hf;
-        float y2 = ytv[p + 2 * n] + sigma * (__ldg(xf + p + sz) - x0) * hf;
+        float y0 = ytv[p] + sigma * (ld_voxel(xf + p + 1) - x0) * hf;
+        float y1 = ytv[p + n] + sigma * (ld_voxel(xf + p + sy) - x0) * hf;
+        float y2 = ytv[p + 2 * n] + sigma * (ld_voxel(xf + p + sz) - x0) * hf;
         ytv[p] = rmax(-tv_w, rmin(tv_w, y0));
         ytv[p + n] = rmax(-tv_w, rmin(tv_w, y1));
         ytv[p + 2 * n] = rmax(-tv_w, rmin(tv_w, y2));
@@ -237,6 +242,8 @@ __global__ void __launch_bounds__(128) k_pd_dual(int nx, int ny, int nz, float s
 // vol -= tau*(-ytp); vol -= tau*(-ybc) for the first frame, otherwise
 // vol -= tau*(ytp_prev - ytp); vol -= tau*(fw - ybc); then on the interior
 // ROI vol -= tau*(-div ytv) and clamp to [0, gmax].
+// T: the storage of vol and xprev (the duals and the warped fw are FP32).
+template <typename T>
 __global__ void __launch_bounds__(128) k_pd_primal(int nx, int ny, int nz, float tau, float gmax,
                                                    Cut8 cut, int first,
                                                    const float *__restrict__ ytp_prev,
@@ -244,14 +251,14 @@ __global__ void __launch_bounds__(128) k_pd_primal(int nx, int ny, int nz, float
                                                    const float *__restrict__ fw,
                                                    const float *__restrict__ ybc,
                                                    const float *__restrict__ ytv,
-                                                   float *__restrict__ vol, float *__restrict__ xprev) {
+                                                   T *__restrict__ vol, T *__restrict__ xprev) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     if (i >= nx) return;
     const size_t sy = nx, sz = (size_t)nx * ny, n = sz * nz;
     const size_t p = i + j * sy + k * sz;
-    float v = vol[p];
-    xprev[p] = v;
+    float v = ld_stored(vol + p);
+    st_stored(xprev + p, v);
     if (first) {
         v = v - tau * (-__ldg(ytp + p));
         v = v - tau * (-__ldg(ybc + p));
@@ -268,35 +275,37 @@ __global__ void __launch_bounds__(128) k_pd_primal(int nx, int ny, int nz, float
         v = v - tau * y;
         v = rmax(rmin(gmax, v), 0.0f);
     }
-    vol[p] = v;
+    st_stored(vol + p, v);
 }
 
 // Over-relaxation (ST_Tomography.cpp:586-604): xbar = 2*vol - xprev in the ROI box.
+template <typename T>
 __global__ void __launch_bounds__(128) k_pd_extrapolate(int nx, int ny, int nz, Cut8 cut,
-                                                        const float *__restrict__ vol,
-                                                        const float *__restrict__ xprev,
-                                                        float *__restrict__ xbar) {
+                                                        const T *__restrict__ vol,
+                                                        const T *__restrict__ xprev,
+                                                        T *__restrict__ xbar) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     if (i >= nx || roi_out(i, j, k, nx, ny, nz, cut.c)) return;
     const size_t p = i + (size_t)j * nx + (size_t)k * nx * ny;
-    xbar[p] = 2.0f * __ldg(vol + p) - __ldg(xprev + p);
+    st_stored(xbar + p, 2.0f * ld_voxel(vol + p) - ld_voxel(xprev + p));
 }
 
 // End of a SART call (ST_Tomography.cpp:793-804) optionally fused with the
 // over-relaxation that follows it in the primal-dual loop (:586-604):
 // vol *= roi; if xbar: xbar = 2*vol - xprev in the ROI box.
+template <typename T>
 __global__ void __launch_bounds__(128) k_roi_apply(int nx, int ny, int nz, Cut8 cut, Cut8 pdcut,
-                                                   float *__restrict__ vol,
-                                                   const float *__restrict__ xprev,
-                                                   float *__restrict__ xbar) {
+                                                   T *__restrict__ vol,
+                                                   const T *__restrict__ xprev,
+                                                   T *__restrict__ xbar) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     if (i >= nx) return;
     const size_t p = i + (size_t)j * nx + (size_t)k * nx * ny;
-    float v = vol[p] * roi_value(i, j, k, nx, ny, nz, cut.c);
-    vol[p] = v;
-    if (xbar && !roi_out(i, j, k, nx, ny, nz, pdcut.c)) xbar[p] = 2.0f * v - __ldg(xprev + p);
+    const float v = ld_stored(vol + p) * roi_value(i, j, k, nx, ny, nz, cut.c);  // (a product by 0 or 1: exact)
+    st_stored(vol + p, v);
+    if (xbar && !roi_out(i, j, k, nx, ny, nz, pdcut.c)) st_stored(xbar + p, 2.0f * v - ld_voxel(xprev + p));
 }
 
 __global__ void __launch_bounds__(128) k_roi_mask(int nx, int ny, int nz, Cut8 cut, float *__restrict__ roi) {
@@ -371,11 +380,56 @@ cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, c
 }
 
 namespace {
-template <int K>
-void bp_cols(const GeomDev &g, const ViewRec *views, const ViewSel &sel, float *vol, float alpha, float gmax,
+template <int K, typename T>
+void bp_cols(const GeomDev &g, const ViewRec *views, const ViewSel &sel, T *vol, float alpha, float gmax,
              cudaStream_t s, unsigned long long tex) {
-    k_bp_voxel_cols<K><<<dim3((g.nx + 127) / 128, (g.ny + K - 1) / K, g.nz), 128, 0, s>>>(g, views, sel, vol, alpha,
-                                                                                       gmax, tex);
+    k_bp_voxel_cols<K, T><<<dim3((g.nx + 127) / 128, (g.ny + K - 1) / K, g.nz), 128, 0, s>>>(g, views, sel, vol,
+                                                                                          alpha, gmax, tex);
+}
+
+template <typename T>
+cudaError_t bp_voxel_any(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr, T *vol,
+                         float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex, int bp_variant) {
+    if (corr_tex) {
+        switch (bp_variant) {
+        case 1: bp_cols<8>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
+        case 2: bp_cols<32>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
+        default: bp_cols<BP_COL>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
+        }
+    } else {
+        k_bp_voxel<false, T><<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, sel, corr, vol, alpha, gmax, 0);
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t pd_dual_any(const int *d, const PdParams &p, const T *xf, const T *xf1, const float *bw, float *ytv,
+                        float *ytp, float *ybc, cudaStream_t s) {
+    k_pd_dual<T><<<vox_grid(d[0], d[1], d[2]), 128, 0, s>>>(d[0], d[1], d[2], p.sigma, p.tv_w, p.tp_w, p.bc_w, p.hf,
+                                                            to_cut(p.cut), xf, xf1, bw, ytv, ytp, ybc);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t pd_primal_any(const int *d, const PdParams &p, int first, const float *ytp_prev, const float *ytp,
+                          const float *fw, const float *ybc, const float *ytv, T *vol, T *xprev, cudaStream_t s) {
+    k_pd_primal<T><<<vox_grid(d[0], d[1], d[2]), 128, 0, s>>>(d[0], d[1], d[2], p.tau, p.gmax, to_cut(p.cut), first,
+                                                              ytp_prev, ytp, fw, ybc, ytv, vol, xprev);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t roi_apply_any(const int *d, const int *roi_cut, const int *pd_cut, T *vol, const T *xprev, T *xbar,
+                          cudaStream_t s) {
+    k_roi_apply<T><<<vox_grid(d[0], d[1], d[2]), 128, 0, s>>>(d[0], d[1], d[2], to_cut(roi_cut), to_cut(pd_cut), vol,
+                                                              xprev, xbar);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t pd_extrapolate_any(const int *d, const int *cut, const T *vol, const T *xprev, T *xbar, cudaStream_t s) {
+    k_pd_extrapolate<T><<<vox_grid(d[0], d[1], d[2]), 128, 0, s>>>(d[0], d[1], d[2], to_cut(cut), vol, xprev, xbar);
+    return cudaGetLastError();
 }
 }  // namespace
 
@@ -387,47 +441,55 @@ const char *bp_variant_name(int v) {
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                             float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex,
                             int bp_variant) {
-    if (corr_tex) {
-        switch (bp_variant) {
-        case 1: bp_cols<8>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
-        case 2: bp_cols<32>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
-        default: bp_cols<BP_COL>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
-        }
-    } else {
-        k_bp_voxel<false><<<vox_grid(g.nx, g.ny, g.nz), 128, 0, s>>>(g, views, sel, corr, vol, alpha, gmax, 0);
-    }
-    return cudaGetLastError();
+    return bp_voxel_any(g, views, sel, corr, vol, alpha, gmax, s, corr_tex, bp_variant);
+}
+
+cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
+                            unsigned short *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex,
+                            int bp_variant) {
+    return bp_voxel_any(g, views, sel, corr, vol, alpha, gmax, s, corr_tex, bp_variant);
 }
 
 cudaError_t launch_pd_dual(const int *d, const PdParams &p, const float *xf, const float *xf1,
                            const float *bw, float *ytv, float *ytp, float *ybc, cudaStream_t s) {
-    k_pd_dual<<<vox_grid(d[0], d[1], d[2]), 128, 0, s>>>(d[0], d[1], d[2], p.sigma, p.tv_w, p.tp_w,
-                                                         p.bc_w, p.hf, to_cut(p.cut), xf, xf1, bw,
-                                                         ytv, ytp, ybc);
-    return cudaGetLastError();
+    return pd_dual_any(d, p, xf, xf1, bw, ytv, ytp, ybc, s);
+}
+
+cudaError_t launch_pd_dual(const int *d, const PdParams &p, const unsigned short *xf, const unsigned short *xf1,
+                           const float *bw, float *ytv, float *ytp, float *ybc, cudaStream_t s) {
+    return pd_dual_any(d, p, xf, xf1, bw, ytv, ytp, ybc, s);
 }
 
 cudaError_t launch_pd_primal(const int *d, const PdParams &p, int first, const float *ytp_prev,
                              const float *ytp, const float *fw, const float *ybc, const float *ytv,
                              float *vol, float *xprev, cudaStream_t s) {
-    k_pd_primal<<<vox_grid(d[0], d[1], d[2]), 128, 0, s>>>(d[0], d[1], d[2], p.tau, p.gmax,
-                                                           to_cut(p.cut), first, ytp_prev, ytp, fw,
-                                                           ybc, ytv, vol, xprev);
-    return cudaGetLastError();
+    return pd_primal_any(d, p, first, ytp_prev, ytp, fw, ybc, ytv, vol, xprev, s);
+}
+
+cudaError_t launch_pd_primal(const int *d, const PdParams &p, int first, const float *ytp_prev,
+                             const float *ytp, const float *fw, const float *ybc, const float *ytv,
+                             unsigned short *vol, unsigned short *xprev, cudaStream_t s) {
+    return pd_primal_any(d, p, first, ytp_prev, ytp, fw, ybc, ytv, vol, xprev, s);
 }
 
 cudaError_t launch_pd_extrapolate(const int *d, const int *cut, const float *vol, const float *xprev,
                                   float *xbar, cudaStream_t s) {
-    k_pd_extrapolate<<<vox_grid(d[0], d[1], d[2]), 128, 0, s>>>(d[0], d[1], d[2], to_cut(cut), vol,
-                                                                xprev, xbar);
-    return cudaGetLastError();
+    return pd_extrapolate_any(d, cut, vol, xprev, xbar, s);
+}
+
+cudaError_t launch_pd_extrapolate(const int *d, const int *cut, const unsigned short *vol,
+                                  const unsigned short *xprev, unsigned short *xbar, cudaStream_t s) {
+    return pd_extrapolate_any(d, cut, vol, xprev, xbar, s);
 }
 
 cudaError_t launch_roi_apply(const int *d, const int *roi_cut, const int *pd_cut, float *vol,
                              const float *xprev, float *xbar, cudaStream_t s) {
-    k_roi_apply<<<vox_grid(d[0], d[1], d[2]), 128, 0, s>>>(d[0], d[1], d[2], to_cut(roi_cut),
-                                                           to_cut(pd_cut), vol, xprev, xbar);
-    return cudaGetLastError();
+    return roi_apply_any(d, roi_cut, pd_cut, vol, xprev, xbar, s);
+}
+
+cudaError_t launch_roi_apply(const int *d, const int *roi_cut, const int *pd_cut, unsigned short *vol,
+                             const unsigned short *xprev, unsigned short *xbar, cudaStream_t s) {
+    return roi_apply_any(d, roi_cut, pd_cut, vol, xprev, xbar, s);
 }
 
 cudaError_t launch_roi_mask(const int *d, const int *cut, float *roi, cudaStream_t s) {

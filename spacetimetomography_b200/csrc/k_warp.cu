@@ -28,8 +28,10 @@ using namespace warpdev;
 // n * max(nc, 3) below 2^31).
 constexpr int WARP_BX = 32, WARP_BY = 4;
 
+// T: the source's storage (float, or BF16 bits widened exactly to FP32).
+template <typename T>
 __global__ void __launch_bounds__(WARP_BX *WARP_BY) k_warp(const Dim3i d, const float *__restrict__ vel,
-                                                           const float *__restrict__ src, int nc, float dt,
+                                                           const T *__restrict__ src, int nc, float dt,
                                                            float *__restrict__ out) {
     const int i = blockIdx.x * WARP_BX + threadIdx.x;
     const int j = blockIdx.y * WARP_BY + threadIdx.y, k = blockIdx.z;
@@ -84,10 +86,11 @@ constexpr long long WARP_WAIT_CYCLES = 200000000LL;  // about 0.1 s
 // their own): one per device, read and cleared by stt_warp_poll_status.
 __device__ int g_warp_wait_status;
 
+template <typename T>
 __global__ void __launch_bounds__(WARP_BX *WARP_BY) k_warp_staged(const Dim3i d,
                                                                   const __grid_constant__ CUtensorMap vmap,
                                                                   const float *__restrict__ vel,
-                                                                  const float *__restrict__ src, int nc, float dt,
+                                                                  const T *__restrict__ src, int nc, float dt,
                                                                   float *__restrict__ out, int *status) {
     __shared__ alignas(128) float vbox[3 * VBOX];
     __shared__ uint64_t bar;
@@ -342,17 +345,30 @@ cudaError_t warp_poll_status(int *flag, cudaStream_t s) {
     return e;
 }
 
-cudaError_t launch_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
-                        float *out, cudaStream_t s, int *status) {
+namespace {
+template <typename T>
+cudaError_t warp_any(const int *dim, const float *vel, const T *src, int nc, float dt, float *out, cudaStream_t s,
+                     int *status) {
     Dim3i d{dim[0], dim[1], dim[2]};
     const dim3 grid((d.x + WARP_BX - 1) / WARP_BX, (d.y + WARP_BY - 1) / WARP_BY, d.z), block(WARP_BX, WARP_BY);
     CUtensorMap vmap;
     const unsigned box[4] = {VX, VY, VZ, 3};
     if (encode_planes_map(&vmap, vel, d.x, d.y, d.z, 3, box))
-        k_warp_staged<<<grid, block, 0, s>>>(d, vmap, vel, src, nc, dt, out, status);
+        k_warp_staged<T><<<grid, block, 0, s>>>(d, vmap, vel, src, nc, dt, out, status);
     else
-        k_warp<<<grid, block, 0, s>>>(d, vel, src, nc, dt, out);
+        k_warp<T><<<grid, block, 0, s>>>(d, vel, src, nc, dt, out);
     return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
+                        float *out, cudaStream_t s, int *status) {
+    return warp_any(dim, vel, src, nc, dt, out, s, status);
+}
+
+cudaError_t launch_warp(const int *dim, const float *vel, const unsigned short *src, int nc, float dt,
+                        float *out, cudaStream_t s, int *status) {
+    return warp_any(dim, vel, src, nc, dt, out, s, status);
 }
 
 cudaError_t launch_warp_vjp(const int *dim, const float *vel, const float *src, int nc, float dt,

@@ -14,9 +14,10 @@ struct stt_batch {
     struct Inst {
         stt_ctx *ctx = nullptr;
         stt_solver *solver = nullptr;
-        float *user_vol = nullptr;
-        float *state = nullptr;  // vol 2n | xbar 2n | xprev n | ytv 3n | ytp n | ybc n | flow 3n
+        float *user_vol = nullptr;  // (BF16 values when the instance's storage is BF16)
+        unsigned char *state = nullptr;  // vol 2n | xbar 2n | xprev n (storage), then FP32 ytv 3n | ytp n | ybc n | flow 3n
         size_t n = 0;
+        size_t es = 4;  // bytes per stored primal value
         cudaStream_t stream = nullptr;
         cudaEvent_t done = nullptr;
     };
@@ -52,7 +53,7 @@ stt_status enqueue_all(stt_batch *b, cudaStream_t main) {
         BCUDA(b, cudaStreamWaitEvent(in.stream, b->fork, 0), "stream wait");
         stt_status st = stt_solver_iterate(in.solver, 1, in.stream);
         if (st) return bfail(b, st, "instance " + std::to_string(i) + ": " + stt_solver_last_error(in.solver));
-        BCUDA(b, cudaMemcpyAsync(in.user_vol, in.state, in.n * sizeof(float), cudaMemcpyDeviceToDevice, in.stream),
+        BCUDA(b, cudaMemcpyAsync(in.user_vol, in.state, in.n * in.es, cudaMemcpyDeviceToDevice, in.stream),
               "copy result");
         BCUDA(b, cudaEventRecord(in.done, in.stream), "event record");
         BCUDA(b, cudaStreamWaitEvent(main, in.done, 0), "stream wait");
@@ -87,18 +88,24 @@ stt_status stt_batch_create(const stt_instance *instances, int n, int mode, stt_
             return bail(STT_ERR_STATE, "instance " + std::to_string(i) + ": no geometry set on its context");
         in.ctx = I.ctx;
         in.user_vol = I.vol;
+        if (I.storage != STT_DTYPE_F32 && I.storage != STT_DTYPE_BF16)
+            return bail(STT_ERR_INVALID, "instance " + std::to_string(i) + ": storage must be F32 or BF16");
         in.n = (size_t)dims[0] * dims[1] * dims[2];
-        const size_t n1 = in.n;
-        if (cudaMalloc(&in.state, 13 * n1 * sizeof(float)) != cudaSuccess) {
+        in.es = I.storage == STT_DTYPE_BF16 ? 2 : 4;
+        const size_t n1 = in.n, es = in.es;
+        const size_t primal = ((5 * n1 * es + 255) / 256) * 256;  // the FP32 duals start 256-byte aligned
+        if (cudaMalloc(&in.state, primal + 8 * n1 * sizeof(float)) != cudaSuccess) {
             cudaGetLastError();
             return bail(STT_ERR_NOMEM, "instance " + std::to_string(i) + ": cudaMalloc of its solver state failed");
         }
-        float *vol = in.state, *xbar = vol + 2 * n1, *xprev = xbar + 2 * n1, *ytv = xprev + n1, *ytp = ytv + 3 * n1,
-              *ybc = ytp + n1, *flow = ybc + n1;
-        cudaError_t e = cudaMemset(xprev, 0, 9 * n1 * sizeof(float));  // xprev, ytv, ytp, ybc, flow
-        if (e == cudaSuccess) e = cudaMemcpy(vol, I.vol, n1 * sizeof(float), cudaMemcpyDeviceToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(vol + n1, I.vol, n1 * sizeof(float), cudaMemcpyDeviceToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(xbar, vol, 2 * n1 * sizeof(float), cudaMemcpyDeviceToDevice);
+        unsigned char *vol = in.state, *xbar = vol + 2 * n1 * es, *xprev = xbar + 2 * n1 * es;
+        float *ytv = reinterpret_cast<float *>(in.state + primal), *ytp = ytv + 3 * n1, *ybc = ytp + n1,
+              *flow = ybc + n1;
+        cudaError_t e = cudaMemset(xprev, 0, n1 * es);
+        if (e == cudaSuccess) e = cudaMemset(ytv, 0, 8 * n1 * sizeof(float));  // ytv, ytp, ybc, flow
+        if (e == cudaSuccess) e = cudaMemcpy(vol, I.vol, n1 * es, cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(vol + n1 * es, I.vol, n1 * es, cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(xbar, vol, 2 * n1 * es, cudaMemcpyDeviceToDevice);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&in.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&in.done, cudaEventDisableTiming);
         if (e != cudaSuccess) return bail(STT_ERR_CUDA, std::string("instance set-up: ") + cudaGetErrorString(e));
@@ -113,11 +120,12 @@ stt_status stt_batch_create(const stt_instance *instances, int n, int mode, stt_
         for (int q = 0; q < 8; ++q) cfg.roi_cut[q] = I.roi_cut[q];
         cfg.seed = I.seed;
         cfg.autotune = I.autotune;
+        cfg.storage = I.storage;
         cfg.mode = STT_SOLVE_STREAMS;
-        stt_pd_state state{};
-        state.vol = vol;
-        state.xbar = xbar;
-        state.xprev = xprev;
+        stt_pd_state state{};  // (BF16 storage: the primal pointers address BF16 arrays)
+        state.vol = reinterpret_cast<float *>(vol);
+        state.xbar = reinterpret_cast<float *>(xbar);
+        state.xprev = reinterpret_cast<float *>(xprev);
         state.ytv = ytv;
         state.ytp = ytp;
         state.ybc = ybc;

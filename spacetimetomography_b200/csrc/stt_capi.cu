@@ -284,6 +284,10 @@ stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g) {
 
 // When a view in [view0, view0+nviews) gathers from the z-fastest copy,
 // refresh the context's copy of `vol` and return it in *volt.
+}  // extern "C"
+
+// The z-fastest copy of the volume when a view in [view0, view0 + nviews)
+// gathers along x (FP32 and BF16 storage).
 static stt_status transposed_if_needed(stt_ctx *ctx, const float *vol, int view0, int nviews, cudaStream_t s,
                                        const float **volt) {
     *volt = nullptr;
@@ -296,6 +300,21 @@ static stt_status transposed_if_needed(stt_ctx *ctx, const float *vol, int view0
     *volt = ctx->volt;
     return STT_OK;
 }
+
+static stt_status transposed_if_needed(stt_ctx *ctx, const unsigned short *vol, int view0, int nviews,
+                                       cudaStream_t s, const unsigned short **volt) {
+    *volt = nullptr;
+    bool any = false;
+    for (int v = view0; v < view0 + nviews && !any; ++v) any = ctx->views_h[v].layout == 1;
+    if (!any) return STT_OK;
+    stt_status st = ensure(ctx, ctx->volt16, ctx->volt16_n, (size_t)nvox(ctx), "transposed BF16 volume");
+    if (st) return st;
+    STT_CUDA(ctx, stt::launch_transpose_bf16(ctx->g, vol, ctx->volt16, s), "k_transpose launch");
+    *volt = ctx->volt16;
+    return STT_OK;
+}
+
+extern "C" {
 
 static stt_status check_views(stt_ctx *ctx, int view0, int nviews) {
     if (view0 < 0 || nviews < 0 || view0 + nviews > ctx->g.n_views)
@@ -362,6 +381,23 @@ stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, flo
     return STT_OK;
 }
 
+stt_status stt_gather_ceiling(stt_ctx *ctx, const float *vol, int view, int packed, float *out, int *count,
+                              void *stream) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!vol || !out) return fail(ctx, STT_ERR_INVALID, "null vol or out");
+    if ((st = check_views(ctx, view, 1))) return st;
+    if ((long long)ctx->g.nx * ctx->g.ny * ctx->g.nz >= (1LL << 31))
+        return fail(ctx, STT_ERR_UNSUPPORTED, "the gather ceiling takes volumes below 2^31 voxels");
+    if ((st = set_device(ctx))) return st;
+    const float *volt = nullptr;
+    if ((st = transposed_if_needed(ctx, vol, view, 1, S(stream), &volt))) return st;
+    STT_CUDA(ctx, stt::launch_gather_ceiling(ctx->g, ctx->views_d, ctx->views_h[view], view, vol, volt, packed, out,
+                                             count, S(stream)),
+             "k_gather_ceiling launch");
+    return STT_OK;
+}
+
 stt_status stt_fp_vjp(stt_ctx *ctx, const float *proj_bar, float *vol_bar, int view0, int nviews,
                       void *stream) {
     stt_status st = need_geom(ctx);
@@ -388,6 +424,22 @@ stt_status stt_bp_voxel(stt_ctx *ctx, const float *corr, float *vol, double alph
     return STT_OK;
 }
 
+stt_status stt_bp_voxel_typed(stt_ctx *ctx, const float *corr, void *vol, int dtype, double alpha, float gmax,
+                              int view, void *stream) {
+    if (dtype == STT_DTYPE_F32) return stt_bp_voxel(ctx, corr, static_cast<float *>(vol), alpha, gmax, view, stream);
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (dtype != STT_DTYPE_BF16) return fail(ctx, STT_ERR_INVALID, "dtype must be STT_DTYPE_F32 or STT_DTYPE_BF16");
+    if (!corr || !vol) return fail(ctx, STT_ERR_INVALID, "null corr or vol");
+    if ((st = check_views(ctx, view, 1))) return st;
+    if ((st = set_device(ctx))) return st;
+    const stt::ViewSel sel{view, nullptr, 0, view};
+    STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, sel, corr, static_cast<unsigned short *>(vol),
+                                       (float)alpha, gmax, S(stream)),
+             "k_bp_voxel launch");
+    return STT_OK;
+}
+
 static stt_status ensure_acc(stt_ctx *ctx, cudaStream_t s) {
     const size_t n = (size_t)nvox(ctx);
     if (ctx->acc && ctx->acc_n >= n) return STT_OK;
@@ -410,6 +462,23 @@ stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, i
     return STT_OK;
 }
 
+stt_status stt_bp_ray_typed(stt_ctx *ctx, const float *corr, void *vol, int dtype, float gmax, int view,
+                            void *stream) {
+    if (dtype == STT_DTYPE_F32) return stt_bp_ray(ctx, corr, static_cast<float *>(vol), gmax, view, stream);
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (dtype != STT_DTYPE_BF16) return fail(ctx, STT_ERR_INVALID, "dtype must be STT_DTYPE_F32 or STT_DTYPE_BF16");
+    if (!corr || !vol) return fail(ctx, STT_ERR_INVALID, "null corr or vol");
+    if ((st = check_views(ctx, view, 1))) return st;
+    if ((st = set_device(ctx))) return st;
+    if ((st = ensure_acc(ctx, S(stream)))) return st;
+    const stt::ViewSel sel{view, nullptr, 0, view};
+    STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, sel, corr, ctx->acc, static_cast<unsigned short *>(vol),
+                                     gmax, S(stream)),
+             "k_bp_ray launch");
+    return STT_OK;
+}
+
 stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, float *wsum, int view,
                               void *stream) {
     stt_status st = need_geom(ctx);
@@ -424,9 +493,56 @@ stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, f
     return STT_OK;
 }
 
+}  // extern "C"
+
+// The fused forward projection of one view of a sweep: FP32 through the tuned
+// gather variant and, where its maps apply, the slab-staged kernel; BF16
+// through the gather kernel.
+static cudaError_t sweep_fp_corr(stt_ctx *ctx, const float *vol, const float *volt, const stt::ViewSel &sel,
+                                 const float *stack, float *rl, cudaStream_t s) {
+    stt::FpSlabMaps maps;
+    stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
+    return stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, stack, rl, ctx->corr, s, 0, &maps, ctx->status,
+                               ctx->tuning.fp);
+}
+
+static cudaError_t sweep_fp_corr(stt_ctx *ctx, const unsigned short *vol, const unsigned short *volt,
+                                 const stt::ViewSel &sel, const unsigned short *stack, float *rl, cudaStream_t s) {
+    return stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, stack, rl, ctx->corr, s);
+}
+
+template <typename T>
+static stt_status sart_sweep_t(stt_ctx *ctx, T *vol, const T *proj_stack, const int *perm, int nperm,
+                               int view_offset, double alpha, float gmax, int bp_mode, float *raylen_state,
+                               const int *roi_cut, void *stream);
+
+extern "C" {
+
 stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, const int *perm,
                           int nperm, int view_offset, double alpha, float gmax, int bp_mode,
                           float *raylen_state, const int *roi_cut, void *stream) {
+    return sart_sweep_t(ctx, vol, proj_stack, perm, nperm, view_offset, alpha, gmax, bp_mode, raylen_state, roi_cut,
+                        stream);
+}
+
+stt_status stt_sart_sweep_typed(stt_ctx *ctx, void *vol, int dtype, const void *proj_stack, const int *perm,
+                                int nperm, int view_offset, double alpha, float gmax, int bp_mode,
+                                float *raylen_state, const int *roi_cut, void *stream) {
+    if (dtype == STT_DTYPE_F32)
+        return sart_sweep_t(ctx, static_cast<float *>(vol), static_cast<const float *>(proj_stack), perm, nperm,
+                            view_offset, alpha, gmax, bp_mode, raylen_state, roi_cut, stream);
+    if (dtype == STT_DTYPE_BF16)
+        return sart_sweep_t(ctx, static_cast<unsigned short *>(vol), static_cast<const unsigned short *>(proj_stack),
+                            perm, nperm, view_offset, alpha, gmax, bp_mode, raylen_state, roi_cut, stream);
+    return fail(ctx, STT_ERR_INVALID, "dtype must be STT_DTYPE_F32 or STT_DTYPE_BF16");
+}
+
+}  // extern "C"
+
+template <typename T>
+static stt_status sart_sweep_t(stt_ctx *ctx, T *vol, const T *proj_stack, const int *perm, int nperm,
+                               int view_offset, double alpha, float gmax, int bp_mode, float *raylen_state,
+                               const int *roi_cut, void *stream) {
     stt_status st = need_geom(ctx);
     if (st) return st;
     if (!vol || !proj_stack || (nperm > 0 && !perm)) return fail(ctx, STT_ERR_INVALID, "null argument");
@@ -443,15 +559,11 @@ stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, con
     if (bp_mode == 1 && (st = ensure_acc(ctx, s))) return st;
     for (int i = 0; i < nperm; ++i) {
         const stt::ViewSel sel{view_offset + perm[i], nullptr, 0, view_offset};
-        const float *volt = nullptr;
+        const T *volt = nullptr;
         if ((st = transposed_if_needed(ctx, vol, view_offset + perm[i], 1, s, &volt))) return st;
-        stt::FpSlabMaps maps;
-        stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
         // ray-based mode: TypicalRayProducer::Initial zeroes the ray lengths
         // after every view, so missed rays see L = 0 (no sticky state)
-        STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, proj_stack,
-                                          bp_mode == 0 ? raylen_state : nullptr, ctx->corr, s, 0, &maps, ctx->status,
-                                          ctx->tuning.fp),
+        STT_CUDA(ctx, sweep_fp_corr(ctx, vol, volt, sel, proj_stack, bp_mode == 0 ? raylen_state : nullptr, s),
                  "k_fp_corr launch");
         if (bp_mode == 0)
             STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, sel, ctx->corr, vol, (float)alpha, gmax, s),
@@ -464,10 +576,13 @@ stt_status stt_sart_sweep(stt_ctx *ctx, float *vol, const float *proj_stack, con
         STT_CUDA(ctx, cudaMemsetAsync(raylen_state, 0, npix * sizeof(float), s), "cudaMemsetAsync(raylen)");
     if (roi_cut) {
         const int d[3] = {ctx->g.nx, ctx->g.ny, ctx->g.nz};
-        STT_CUDA(ctx, stt::launch_roi_apply(d, roi_cut, nullptr, vol, nullptr, nullptr, s), "k_roi_apply launch");
+        STT_CUDA(ctx, stt::launch_roi_apply(d, roi_cut, nullptr, vol, (const T *)nullptr, (T *)nullptr, s),
+                 "k_roi_apply launch");
     }
     return STT_OK;
 }
+
+extern "C" {
 
 stt_status stt_sart_view(stt_ctx *ctx, float *vol, const float *b, int view, double alpha, float gmax, int bp_mode,
                          float *raylen_state, void *stream) {
@@ -636,6 +751,19 @@ stt_status stt_warp(const int *dim, const float *vel, const float *src, int nc, 
     if (st) return st;
     if (!out) return fail(nullptr, STT_ERR_INVALID, "null out");
     STT_CUDA(nullptr, stt::launch_warp(dim, vel, src, nc, dt, out, S(stream)), "k_warp launch");
+    return STT_OK;
+}
+
+stt_status stt_warp_typed(const int *dim, const float *vel, const void *src, int dtype, int nc, float dt, float *out,
+                          void *stream) {
+    if (dtype == STT_DTYPE_F32) return stt_warp(dim, vel, static_cast<const float *>(src), nc, dt, out, stream);
+    if (dtype != STT_DTYPE_BF16) return fail(nullptr, STT_ERR_INVALID, "dtype must be STT_DTYPE_F32 or STT_DTYPE_BF16");
+    // the argument checks of the FP32 form (they read no element of src)
+    stt_status st = check_warp_args(dim, vel, static_cast<const float *>(src), nc);
+    if (st) return st;
+    if (!out) return fail(nullptr, STT_ERR_INVALID, "null out");
+    STT_CUDA(nullptr, stt::launch_warp(dim, vel, static_cast<const unsigned short *>(src), nc, dt, out, S(stream)),
+             "k_warp launch");
     return STT_OK;
 }
 

@@ -7,6 +7,7 @@
 #ifndef cuda_runtime_h
 #include <cuda_runtime.h>
 #endif
+#include <cuda_bf16.h>
 #include <stdint.h>
 
 namespace stt {
@@ -167,6 +168,16 @@ __device__ __forceinline__ float ld_voxel(const unsigned short *p) {
     return __uint_as_float((unsigned)__ldg(p) << 16);
 }
 
+// Read-write arrays of either storage: a plain load widened to FP32, and a
+// store of an FP32 value (BF16: rounded to nearest even by the CUDA
+// conversion).  Arithmetic on stored values is always FP32.
+__device__ __forceinline__ float ld_stored(const float *p) { return *p; }
+__device__ __forceinline__ float ld_stored(const unsigned short *p) { return __uint_as_float((unsigned)*p << 16); }
+__device__ __forceinline__ void st_stored(float *p, float v) { *p = v; }
+__device__ __forceinline__ void st_stored(unsigned short *p, float v) {
+    *p = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+}
+
 // The forward projector's sample: the clamped trilinear value of
 // SingleScalarVolume.core.h:87-120, lerped x, then y, then z as the reference
 // does.  The position is clamped to [0, dims-1] as in make_taps, but the base
@@ -207,6 +218,48 @@ __device__ __forceinline__ float trilerp(const float v[8], const FpCell &c) {
     const float d0 = lerp1(v[4], v[5], fx1, c.fx);
     const float d1 = lerp1(v[6], v[7], fx1, c.fx);
     return lerp1(lerp1(a, b, fy1, c.fy), lerp1(d0, d1, fy1, c.fy), fz1, c.fz);
+}
+
+// Two samples' cells and interpolations in the packed FP32x2 instructions of
+// sm_100 (one instruction per pair of lanes).  Each lane is rounded as the
+// scalar instruction it replaces, so trilerp2 returns bit for bit
+// (trilerp(va, ca), trilerp(vb, cb)): 1 - f and p - floor(p) are fused
+// multiply-adds with a multiplier of -1 (the product is exact, so the one
+// rounding is that of the subtraction).
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+__device__ __forceinline__ void fp_cell2(const GeomDev &g, const float pa[3], const float pb[3], FpCell &ca,
+                                         FpCell &cb) {
+    float qa[3], qb[3];
+    const float hi[3] = {(float)(g.nx - 1), (float)(g.ny - 1), (float)(g.nz - 1)};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        qa[k] = rmax(rmin(pa[k], hi[k]), 0.0f);
+        qb[k] = rmax(rmin(pb[k], hi[k]), 0.0f);
+    }
+    ca.ix = min((int)qa[0], g.nx - 2), cb.ix = min((int)qb[0], g.nx - 2);
+    ca.iy = min((int)qa[1], g.ny - 2), cb.iy = min((int)qb[1], g.ny - 2);
+    ca.iz = min((int)qa[2], g.nz - 2), cb.iz = min((int)qb[2], g.nz - 2);
+    const float2 m1 = f2(-1.0f, -1.0f);
+    const float2 fx = __ffma2_rn(f2((float)ca.ix, (float)cb.ix), m1, f2(qa[0], qb[0]));
+    const float2 fy = __ffma2_rn(f2((float)ca.iy, (float)cb.iy), m1, f2(qa[1], qb[1]));
+    const float2 fz = __ffma2_rn(f2((float)ca.iz, (float)cb.iz), m1, f2(qa[2], qb[2]));
+    ca.fx = fx.x, cb.fx = fx.y, ca.fy = fy.x, cb.fy = fy.y, ca.fz = fz.x, cb.fz = fz.y;
+}
+
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 f1, float2 f) {
+    return __ffma2_rn(b, f, __fmul2_rn(a, f1));
+}
+
+__device__ __forceinline__ float2 trilerp2(const float va[8], const float vb[8], const FpCell &ca, const FpCell &cb) {
+    const float2 m1 = f2(-1.0f, -1.0f), one = f2(1.0f, 1.0f);
+    const float2 fx = f2(ca.fx, cb.fx), fy = f2(ca.fy, cb.fy), fz = f2(ca.fz, cb.fz);
+    const float2 fx1 = __ffma2_rn(m1, fx, one), fy1 = __ffma2_rn(m1, fy, one), fz1 = __ffma2_rn(m1, fz, one);
+    const float2 a = lerp2(f2(va[0], vb[0]), f2(va[1], vb[1]), fx1, fx);
+    const float2 b = lerp2(f2(va[2], vb[2]), f2(va[3], vb[3]), fx1, fx);
+    const float2 d0 = lerp2(f2(va[4], vb[4]), f2(va[5], vb[5]), fx1, fx);
+    const float2 d1 = lerp2(f2(va[6], vb[6]), f2(va[7], vb[7]), fx1, fx);
+    return lerp2(lerp2(a, b, fy1, fy), lerp2(d0, d1, fy1, fy), fz1, fz);
 }
 
 // The 8 corners of a cell from a volume array: FAST is its contiguous axis
@@ -336,28 +389,31 @@ __device__ __forceinline__ void march_groups(const GeomDev &g, const Ray &r, Vis
         const int cap = (int)fminf(ceilf(__fdiv_rn(tb - t, sd)) + 2.0f, (float)budget);
         budget -= cap > 0 ? cap : 0;
         int n = 0;
+        // (x, y) and (t, z) advance as packed pairs: the same float additions
+        const float2 sxy = make_float2(d.step[0], d.step[1]), stz = make_float2(sd, d.step[2]);
         while (n < cap && t < tb) {
-            float tl = t;  // time of the group's last sample
+            float2 xy[G], tz[G];  // the group's samples; tz[G-1].x is the time of its last
+            xy[0] = make_float2(pos[0], pos[1]);
+            tz[0] = make_float2(t, pos[2]);
 #pragma unroll
-            for (int i = 1; i < G; ++i) tl = __fadd_rn(tl, sd);
-            if (n + G - 1 < cap && tl < tb) {
+            for (int i = 1; i < G; ++i) {
+                xy[i] = __fadd2_rn(xy[i - 1], sxy);
+                tz[i] = __fadd2_rn(tz[i - 1], stz);
+            }
+            if (n + G - 1 < cap && tz[G - 1].x < tb) {
                 float p[G][3];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) p[0][k] = pos[k];
-#pragma unroll
-                for (int i = 1; i < G; ++i)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) p[i][k] = __fadd_rn(p[i - 1][k], d.step[k]);
+                for (int i = 0; i < G; ++i) p[i][0] = xy[i].x, p[i][1] = xy[i].y, p[i][2] = tz[i].y;
                 visitg(p);
-                t = __fadd_rn(tl, sd);
-#pragma unroll
-                for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(p[G - 1][k], d.step[k]);
+                const float2 nxy = __fadd2_rn(xy[G - 1], sxy), ntz = __fadd2_rn(tz[G - 1], stz);
+                t = ntz.x;
+                pos[0] = nxy.x, pos[1] = nxy.y, pos[2] = ntz.y;
                 n += G;
             } else {
                 visit(pos);
-                t = __fadd_rn(t, sd);
-#pragma unroll
-                for (int k = 0; k < 3; ++k) pos[k] = __fadd_rn(pos[k], d.step[k]);
+                const float2 nxy = __fadd2_rn(xy[0], sxy), ntz = __fadd2_rn(tz[0], stz);
+                t = ntz.x;
+                pos[0] = nxy.x, pos[1] = nxy.y, pos[2] = ntz.y;
                 ++n;
             }
         }

@@ -28,7 +28,7 @@ int grid_stride_blocks(long long n, int threads);
 //   slab: the box of the slab-staged projector (slab_variant_name);
 //   bp:   the column length of the voxel backprojection (bp_variant_name).
 // Which views the slab kernel projects is the per-view ViewRec::staged flag.
-constexpr int kFpVariants = 7, kSlabVariants = 4, kBpVariants = 3;
+constexpr int kFpVariants = 10, kSlabVariants = 4, kBpVariants = 3;
 struct Tuning {
     int fp = 0, slab = 0, bp = 0;
 };
@@ -73,14 +73,43 @@ cudaError_t launch_fp_bf16(const GeomDev &g, const ViewRec *views, const unsigne
 cudaError_t launch_transpose_bf16(const GeomDev &g, const unsigned short *in, unsigned short *out, cudaStream_t s);
 cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *in,
                                       float *out, cudaStream_t s);
+cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, const ViewSel &sel,
+                                      const unsigned short *in, unsigned short *out, cudaStream_t s);
+
+// BF16 storage (the raw upper halves of FP32 values; the solver's
+// stt_solve_cfg.storage): the overloads below on unsigned short arrays read
+// stored values widened exactly to FP32, compute as their FP32 forms do, and
+// round what they store to nearest even.  Duals, flows, corrections and
+// accumulators stay FP32.
+// The fused forward projection of a BF16 volume against a BF16 sinogram: the
+// gather kernel for every view (no slab staging).
+cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
+                           const unsigned short *vol_t, const ViewSel &sel, const unsigned short *b_stack,
+                           float *raylen_state, float *corr, cudaStream_t s, unsigned long long corr_surf = 0);
+cudaError_t launch_correction(long long n, const unsigned short *b, const float *ax, const float *raylen,
+                              float *corr, cudaStream_t s);
 cudaError_t launch_correction(long long n, const float *b, const float *ax, const float *raylen,
                               float *corr, cudaStream_t s);
+// Ray-driven backprojection: the scatter into acc (interleaved contribution,
+// weight), then vol += contribution/weight and acc cleared.  The scatter
+// accumulates each block's samples in a shared-memory box per slab
+// (k_bp_slab.cu) below 2^31 voxels, else with a global atomic per corner.
 cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                           float2 *acc, float *vol, float gmax, cudaStream_t s);
+cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
+                          float2 *acc, unsigned short *vol, float gmax, cudaStream_t s);
+cudaError_t launch_bp_ray_scatter_slab(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
+                                       float2 *acc, cudaStream_t s);
 cudaError_t launch_bp_ray_scatter(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                                   float2 *acc, float *contrib, float *wsum, cudaStream_t s);
 cudaError_t launch_fp_adjoint(const GeomDev &g, const ViewRec *views, int view0, int nviews,
                               const float *proj_bar, float *vol_bar, cudaStream_t s);
+// The gather ceiling (k_project.cu): one view's rays sampled at the
+// projector's step with its gathers and interpolation and none of its march
+// control; `host_view` is the view's record (its layout picks vol_t).
+cudaError_t launch_gather_ceiling(const GeomDev &g, const ViewRec *views, const ViewRec &host_view, int view,
+                                  const float *vol, const float *vol_t, int packed, float *out, int *count,
+                                  cudaStream_t s);
 cudaError_t launch_fill_zero(float *p, long long n, cudaStream_t s);
 cudaError_t launch_dot_f64(long long n, const float *a, const float *b, double *out, cudaStream_t s);
 cudaError_t launch_scale_inv_sqrt(long long n, float *x, const double *norm2, cudaStream_t s);
@@ -91,6 +120,9 @@ cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, c
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                             float *vol, float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex = 0,
                             int bp_variant = 0);
+cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
+                            unsigned short *vol, float alpha, float gmax, cudaStream_t s,
+                            unsigned long long corr_tex = 0, int bp_variant = 0);
 // Sets the solver's device-side iteration counter (stream-ordered, no host memory read).
 cudaError_t launch_set_counter(unsigned long long *counter, unsigned long long v, cudaStream_t s);
 // View orders of `frames` local frames (at most 1024), local frame f being
@@ -99,13 +131,22 @@ cudaError_t launch_make_perm(unsigned long long seed, unsigned long long *counte
                              int frame0, int views, int *perm, cudaStream_t s);
 cudaError_t launch_pd_dual(const int *dims, const PdParams &p, const float *xf, const float *xf1,
                            const float *bw, float *ytv, float *ytp, float *ybc, cudaStream_t s);
+cudaError_t launch_pd_dual(const int *dims, const PdParams &p, const unsigned short *xf, const unsigned short *xf1,
+                           const float *bw, float *ytv, float *ytp, float *ybc, cudaStream_t s);
 cudaError_t launch_pd_primal(const int *dims, const PdParams &p, int first, const float *ytp_prev,
                              const float *ytp, const float *fw, const float *ybc, const float *ytv,
                              float *vol, float *xprev, cudaStream_t s);
+cudaError_t launch_pd_primal(const int *dims, const PdParams &p, int first, const float *ytp_prev,
+                             const float *ytp, const float *fw, const float *ybc, const float *ytv,
+                             unsigned short *vol, unsigned short *xprev, cudaStream_t s);
 cudaError_t launch_pd_extrapolate(const int *dims, const int *cut, const float *vol,
                                   const float *xprev, float *xbar, cudaStream_t s);
+cudaError_t launch_pd_extrapolate(const int *dims, const int *cut, const unsigned short *vol,
+                                  const unsigned short *xprev, unsigned short *xbar, cudaStream_t s);
 cudaError_t launch_roi_apply(const int *dims, const int *roi_cut, const int *pd_cut, float *vol,
                              const float *xprev, float *xbar, cudaStream_t s);
+cudaError_t launch_roi_apply(const int *dims, const int *roi_cut, const int *pd_cut, unsigned short *vol,
+                             const unsigned short *xprev, unsigned short *xbar, cudaStream_t s);
 cudaError_t launch_roi_mask(const int *dims, const int *cut, float *roi, cudaStream_t s);
 
 // ---- optical flow (k_flow.cu) ----
@@ -154,6 +195,9 @@ cudaError_t launch_copy_roi(const int *d, int nc, const FlowRoi &roi, const floa
 // `status` (may be null: then a per-device word read by warp_poll_status) is
 // set when the staged kernel's bounded wait for its velocity box gave up.
 cudaError_t launch_warp(const int *dim, const float *vel, const float *src, int nc, float dt,
+                        float *out, cudaStream_t s, int *status = nullptr);
+// The warp of a BF16-stored source (taps widened to FP32; FP32 flow and output).
+cudaError_t launch_warp(const int *dim, const float *vel, const unsigned short *src, int nc, float dt,
                         float *out, cudaStream_t s, int *status = nullptr);
 // Reads and clears the per-device status word of warps launched without one
 // (synchronises `s`); *flag is non-zero if a bounded wait gave up.

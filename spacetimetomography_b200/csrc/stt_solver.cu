@@ -120,7 +120,7 @@ struct stt_solver {
     float *warpbuf = nullptr;  // F volumes: backward-warped X_bar[f+1], then forward-warped Y_bc[f-1]
     float *corr = nullptr;     // F correction images
     float *ax = nullptr;       // plain form: forward projection image
-    float *volt = nullptr;     // F z-fastest volume copies (views gathering along x)
+    void *volt = nullptr;      // F z-fastest volume copies (views gathering along x), in the state's storage
     float *raylen = nullptr;   // F sticky ray-length images
     float2 *acc = nullptr;     // ray-based BP accumulators, F volumes
     int *perm = nullptr;       // F x V device view order
@@ -197,17 +197,24 @@ stt::PdParams pdp(const stt_pd_params &p) {
     return q;
 }
 
+// The primal volumes (vol, xbar, xprev) and the sinogram stack in the state's
+// storage T: float, or BF16 bits (unsigned short) with stt_solve_cfg.storage.
+template <typename T>
+T *vol_of(stt_solver *s, float *base, int f) {
+    return reinterpret_cast<T *>(base) + (size_t)f * s->n;
+}
+
 // Frame f's dual step: backward warp of X_bar[f+1] along flow[f]
 // (ST_Tomography.cpp:502-503) then the fused dual kernel (:504-534).
+template <typename T>
 stt_status enqueue_dual(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
     const int d[3] = {s->g->nx, s->g->ny, s->g->nz};
     const size_t n = s->n;
     float *bw = s->warpbuf + f * n;
-    SCUDA(s, stt::launch_warp(d, s->st.flow + (size_t)f * 3 * n, s->st.xbar + (f + 1) * n, 1, -1.0f, bw, cs,
-                              s->status),
-          "warp (dual)");
-    SCUDA(s, stt::launch_pd_dual(d, pdp(s->cfg.pd), s->st.xbar + f * n, s->st.xbar + (f + 1) * n, bw,
-                                 s->st.ytv + (size_t)f * 3 * n, s->st.ytp + f * n, s->st.ybc + f * n, cs),
+    const T *xf = vol_of<T>(s, s->st.xbar, f), *xf1 = vol_of<T>(s, s->st.xbar, f + 1);
+    SCUDA(s, stt::launch_warp(d, s->st.flow + (size_t)f * 3 * n, xf1, 1, -1.0f, bw, cs, s->status), "warp (dual)");
+    SCUDA(s, stt::launch_pd_dual(d, pdp(s->cfg.pd), xf, xf1, bw, s->st.ytv + (size_t)f * 3 * n, s->st.ytp + f * n,
+                                 s->st.ybc + f * n, cs),
           "pd_dual");
     nl += 2;
     return STT_OK;
@@ -217,6 +224,7 @@ stt_status enqueue_dual(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
 // Y_bc[f-1] along flow[f-1] for f > 0, then the fused primal kernel.
 // With a halo, local frame 0 continues the previous shard: its "f-1" terms
 // come from ytp_halo / ybc_halo / flow_halo.
+template <typename T>
 stt_status enqueue_primal(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
     const int d[3] = {s->g->nx, s->g->ny, s->g->nz};
     const size_t n = s->n;
@@ -237,8 +245,8 @@ stt_status enqueue_primal(stt_solver *s, int f, cudaStream_t cs, long long &nl) 
         ++nl;
     }
     SCUDA(s, stt::launch_pd_primal(d, pdp(s->cfg.pd), first, ytp_prev, s->st.ytp + f * n, first ? nullptr : fw,
-                                   s->st.ybc + f * n, s->st.ytv + (size_t)f * 3 * n, s->st.vol + f * n,
-                                   s->st.xprev + f * n, cs),
+                                   s->st.ybc + f * n, s->st.ytv + (size_t)f * 3 * n, vol_of<T>(s, s->st.vol, f),
+                                   vol_of<T>(s, s->st.xprev, f), cs),
           "pd_primal");
     ++nl;
     return STT_OK;
@@ -247,23 +255,41 @@ stt_status enqueue_primal(stt_solver *s, int f, cudaStream_t cs, long long &nl) 
 // SART(f) (ST_Tomography.cpp:616-808) as fused launches, views read from the
 // device-side order, then the ROI mask (:793-804) fused with the
 // over-relaxation X_bar[f] = 2V - X_prev (:586-604).
+// The fused forward projection of one view: FP32 storage through the tuned
+// gather variant and, where the maps apply, the slab-staged kernel; BF16
+// storage through the gather kernel.  Returns the kernels launched.
+int fp_corr(stt_solver *s, int f, const float *vol, const float *volt, const stt::ViewSel &sel, const float *stack,
+            float *rl, float *corr, cudaStream_t cs, unsigned long long surf, cudaError_t &e) {
+    const stt::FpSlabMaps *maps = s->fpmaps.empty() ? nullptr : &s->fpmaps[f];
+    e = stt::launch_fp_corr(*s->g, s->views, vol, volt, sel, stack, rl, corr, cs, surf, maps, s->status,
+                            s->ctx->tuning.fp);
+    return (maps && maps->ok) ? 2 : 1;  // slab-staged + gather kernels, or gather only
+}
+
+int fp_corr(stt_solver *s, int, const unsigned short *vol, const unsigned short *volt, const stt::ViewSel &sel,
+            const unsigned short *stack, float *rl, float *corr, cudaStream_t cs, unsigned long long surf,
+            cudaError_t &e) {
+    e = stt::launch_fp_corr(*s->g, s->views, vol, volt, sel, stack, rl, corr, cs, surf);
+    return 1;
+}
+
+template <typename T>
 stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
     const stt::GeomDev &g = *s->g;
     const int V = s->V;
-    float *vol = s->st.vol + f * s->n;
+    T *vol = vol_of<T>(s, s->st.vol, f);
     float *corr = s->corr + f * s->npix;
-    const float *stack = s->st.proj + (size_t)f * V * s->npix;
+    const T *stack = reinterpret_cast<const T *>(s->st.proj) + (size_t)f * V * s->npix;
     const int voxel = s->cfg.bp_mode == 0;
-    float *volt = s->volt + f * s->n;
+    T *volt = reinterpret_cast<T *>(s->volt) + f * s->n;
     for (int i = 0; i < V; ++i) {
         const stt::ViewSel sel{0, s->perm + (size_t)f * V, i, f * V};
         SCUDA(s, stt::launch_transpose_for_view(g, s->views, sel, vol, volt, cs), "transpose");
         const bool tex = voxel && !s->corr_tex.empty();
-        SCUDA(s, stt::launch_fp_corr(g, s->views, vol, volt, sel, stack, voxel ? s->raylen + f * s->npix : nullptr,
-                                     corr, cs, tex ? s->corr_tex[f].surf : 0,
-                                     s->fpmaps.empty() ? nullptr : &s->fpmaps[f], s->status, s->ctx->tuning.fp),
-              "fp_corr");
-        nl += (!s->fpmaps.empty() && s->fpmaps[f].ok) ? 2 : 1;  // slab-staged + gather kernels, or gather only
+        cudaError_t e = cudaSuccess;
+        nl += fp_corr(s, f, vol, volt, sel, stack, voxel ? s->raylen + f * s->npix : nullptr, corr, cs,
+                      tex ? s->corr_tex[f].surf : 0, e);
+        SCUDA(s, e, "fp_corr");
         if (voxel)
             SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs,
                                           tex ? s->corr_tex[f].tex : 0, s->ctx->tuning.bp),
@@ -274,12 +300,14 @@ stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long
         nl += voxel ? 2 : 3;
     }
     const int d[3] = {g.nx, g.ny, g.nz};
-    SCUDA(s, stt::launch_roi_apply(d, s->cfg.roi_cut, s->cfg.pd.cut, vol, s->st.xprev + f * s->n,
-                                   s->st.xbar + f * s->n, cs),
+    SCUDA(s, stt::launch_roi_apply(d, s->cfg.roi_cut, s->cfg.pd.cut, vol, vol_of<T>(s, s->st.xprev, f),
+                                   vol_of<T>(s, s->st.xbar, f), cs),
           "roi_apply");
     ++nl;
     return STT_OK;
 }
+
+bool bf16(const stt_solver *s) { return s->cfg.storage == STT_DTYPE_BF16; }
 
 // Phase 0: the view order, then every frame's dual on its own stream.  With
 // `join` the frame streams rejoin `main` (phases run separately).
@@ -292,7 +320,8 @@ stt_status enqueue_phase0(stt_solver *s, cudaStream_t main, long long &nl, bool 
     SCUDA(s, cudaEventRecord(s->ev_fork, main), "event record");
     for (int f = 0; f < F; ++f) SCUDA(s, cudaStreamWaitEvent(s->streams[f], s->ev_fork, 0), "stream wait");
     for (int f = 0; f < F; ++f) {
-        stt_status st = enqueue_dual(s, f, s->streams[f], nl);
+        stt_status st = bf16(s) ? enqueue_dual<unsigned short>(s, f, s->streams[f], nl)
+                                : enqueue_dual<float>(s, f, s->streams[f], nl);
         if (st) return st;
         SCUDA(s, cudaEventRecord(s->ev_dual[f], s->streams[f]), "event record");
         if (join) SCUDA(s, cudaStreamWaitEvent(main, s->ev_dual[f], 0), "stream wait");
@@ -315,9 +344,11 @@ stt_status enqueue_phase1(stt_solver *s, cudaStream_t main, long long &nl, bool 
     for (int f = 0; f < F; ++f) {
         cudaStream_t cs = s->streams[f];
         if (f > 0 && !fork) SCUDA(s, cudaStreamWaitEvent(cs, s->ev_dual[f - 1], 0), "stream wait");
-        stt_status st = enqueue_primal(s, f, cs, nl);
+        stt_status st = bf16(s) ? enqueue_primal<unsigned short>(s, f, cs, nl) : enqueue_primal<float>(s, f, cs, nl);
         if (st) return st;
-        if ((st = enqueue_sart_batched(s, f, cs, nl))) return st;
+        if ((st = bf16(s) ? enqueue_sart_batched<unsigned short>(s, f, cs, nl)
+                          : enqueue_sart_batched<float>(s, f, cs, nl)))
+            return st;
         SCUDA(s, cudaEventRecord(s->ev_done[f], cs), "event record");
         SCUDA(s, cudaStreamWaitEvent(main, s->ev_done[f], 0), "stream wait");
     }
@@ -333,18 +364,20 @@ stt_status enqueue_batched(stt_solver *s, cudaStream_t main, long long &nl) {
 // The per-view form: frame by frame as the reference loops, each view's
 // forward projection, correction and backprojection as separate launches,
 // and a host synchronisation after every view.
+template <typename T>
 stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl);
 
 // phase -1: the reference's interleaved frame loop; phase 0: every dual;
 // phase 1: every frame's primal, SART and over-relaxation.
-stt_status run_plain(stt_solver *s, cudaStream_t cs, long long &nl, int phase) {
+template <typename T>
+stt_status run_plain_t(stt_solver *s, cudaStream_t cs, long long &nl, int phase) {
     const int F = s->F;
     for (int f = 0; f < F; ++f) {
         stt_status st = STT_OK;
-        if (phase <= 0 && (st = enqueue_dual(s, f, cs, nl))) return st;
+        if (phase <= 0 && (st = enqueue_dual<T>(s, f, cs, nl))) return st;
         if (phase == 0) continue;
-        if ((st = enqueue_primal(s, f, cs, nl))) return st;
-        if ((st = plain_frame_tail(s, f, cs, nl))) return st;
+        if ((st = enqueue_primal<T>(s, f, cs, nl))) return st;
+        if ((st = plain_frame_tail<T>(s, f, cs, nl))) return st;
     }
     if (phase == 0) {
         SCUDA(s, cudaStreamSynchronize(cs), "synchronize");
@@ -358,6 +391,21 @@ stt_status run_plain(stt_solver *s, cudaStream_t cs, long long &nl, int phase) {
     return STT_OK;
 }
 
+stt_status run_plain(stt_solver *s, cudaStream_t cs, long long &nl, int phase) {
+    return bf16(s) ? run_plain_t<unsigned short>(s, cs, nl, phase) : run_plain_t<float>(s, cs, nl, phase);
+}
+
+cudaError_t fp_view(const stt::GeomDev &g, const stt::ViewRec *views, const float *vol, const float *volt, int view,
+                    float *ax, float *rl, cudaStream_t cs) {
+    return stt::launch_fp(g, views, vol, volt, view, 1, ax, rl, nullptr, cs);
+}
+
+cudaError_t fp_view(const stt::GeomDev &g, const stt::ViewRec *views, const unsigned short *vol,
+                    const unsigned short *volt, int view, float *ax, float *rl, cudaStream_t cs) {
+    return stt::launch_fp_bf16(g, views, vol, volt, view, 1, ax, rl, nullptr, cs);
+}
+
+template <typename T>
 stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl) {
     const stt::GeomDev &g = *s->g;
     const int V = s->V;
@@ -366,18 +414,18 @@ stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl
     const int voxel = s->cfg.bp_mode == 0;
     {
         stt::host_perm(s->cfg.seed, s->host_iter, s->total_frames, s->cfg.frame_offset + f, V, perm.data());
-        float *vol = s->st.vol + f * s->n;
+        T *vol = vol_of<T>(s, s->st.vol, f);
         float *corr = s->corr + f * s->npix;
         float *rl = s->raylen + f * s->npix;
         for (int i = 0; i < V; ++i) {
             const int view = f * V + perm[i];
-            const float *b = s->st.proj + ((size_t)f * V + perm[i]) * s->npix;
+            const T *b = reinterpret_cast<const T *>(s->st.proj) + ((size_t)f * V + perm[i]) * s->npix;
             const stt::ViewSel sel{view, nullptr, 0, view};
-            float *volt = s->volt + f * s->n;
+            T *volt = reinterpret_cast<T *>(s->volt) + f * s->n;
             SCUDA(s, stt::launch_transpose_for_view(g, s->views, sel, vol, volt, cs), "transpose");
             ++nl;
             if (voxel) {
-                SCUDA(s, stt::launch_fp(g, s->views, vol, volt, view, 1, s->ax, rl, nullptr, cs), "fp");
+                SCUDA(s, fp_view(g, s->views, vol, volt, view, s->ax, rl, cs), "fp");
                 SCUDA(s, stt::launch_correction((long long)s->npix, b, s->ax, rl, corr, cs), "correction");
                 SCUDA(s, stt::launch_bp_voxel(g, s->views, sel, corr, vol, (float)s->cfg.alpha, s->cfg.pd.gmax, cs),
                       "bp_voxel");
@@ -385,7 +433,7 @@ stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl
             } else {
                 // ray-based: the producer is reset after every view (L = 0 on a miss)
                 SCUDA(s, stt::launch_fill_zero(rl, (long long)s->npix, cs), "fill");
-                SCUDA(s, stt::launch_fp(g, s->views, vol, volt, view, 1, s->ax, rl, nullptr, cs), "fp");
+                SCUDA(s, fp_view(g, s->views, vol, volt, view, s->ax, rl, cs), "fp");
                 SCUDA(s, stt::launch_correction((long long)s->npix, b, s->ax, rl, corr, cs), "correction");
                 SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs),
                       "bp_ray");
@@ -393,8 +441,8 @@ stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl
             }
             SCUDA(s, cudaStreamSynchronize(cs), "per-view synchronize");
         }
-        SCUDA(s, stt::launch_roi_apply(d, s->cfg.roi_cut, s->cfg.pd.cut, vol, s->st.xprev + f * s->n,
-                                       s->st.xbar + f * s->n, cs),
+        SCUDA(s, stt::launch_roi_apply(d, s->cfg.roi_cut, s->cfg.pd.cut, vol, vol_of<T>(s, s->st.xprev, f),
+                                       vol_of<T>(s, s->st.xbar, f), cs),
               "roi_apply");
         ++nl;
     }
@@ -429,6 +477,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
         return STT_ERR_INVALID;
     if (cfg->bp_mode != 0 && cfg->bp_mode != 1) return STT_ERR_INVALID;
     if (cfg->mode < STT_SOLVE_PLAIN || cfg->mode > STT_SOLVE_GRAPH) return STT_ERR_INVALID;
+    if (cfg->storage != STT_DTYPE_F32 && cfg->storage != STT_DTYPE_BF16) return STT_ERR_INVALID;
     if (!state->vol || !state->xbar || !state->xprev || !state->ytv || !state->ytp || !state->ybc ||
         !state->flow || !state->proj)
         return STT_ERR_INVALID;
@@ -453,7 +502,11 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     if (!e) e = alloc(s, s->warpbuf, (size_t)F * s->n, "warp buffers");
     if (!e) e = alloc(s, s->corr, (size_t)F * s->npix, "corrections");
     if (!e) e = alloc(s, s->ax, s->npix, "projection");
-    if (!e) e = alloc(s, s->volt, (size_t)F * s->n, "transposed volumes");
+    if (!e) {
+        unsigned char *vt = nullptr;
+        e = alloc(s, vt, (size_t)F * s->n * (cfg->storage == STT_DTYPE_BF16 ? 2 : 4), "transposed volumes");
+        s->volt = vt;
+    }
     if (!e) e = alloc(s, s->raylen, (size_t)F * s->npix, "ray lengths");
     if (!e) e = alloc(s, s->perm, (size_t)F * s->V, "view order");
     if (!e) e = alloc(s, s->counter, 1, "iteration counter");
@@ -463,10 +516,11 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
         stt_solver_destroy(s);
         return e;
     }
-    if (cfg->mode != STT_SOLVE_PLAIN) {
+    if (cfg->mode != STT_SOLVE_PLAIN && cfg->storage == STT_DTYPE_F32) {
         s->fpmaps.resize(F);
         for (int f = 0; f < F; ++f)  // where the maps do not apply, ok stays 0 and every view gathers
-            stt::make_fp_slab_maps(*g, s->st.vol + f * s->n, s->volt + f * s->n, s->fpmaps[f], ctx->tuning.slab);
+            stt::make_fp_slab_maps(*g, s->st.vol + f * s->n, static_cast<float *>(s->volt) + f * s->n, s->fpmaps[f],
+                                   ctx->tuning.slab);
     }
     if (cfg->mode != STT_SOLVE_PLAIN && cfg->bp_mode == 0) {
         s->corr_tex.resize(F);

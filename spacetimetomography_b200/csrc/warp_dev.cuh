@@ -127,12 +127,13 @@ __device__ __forceinline__ void cell_setup(const Dim3i d, const float g[3], Cell
     axis_setup(g[2], c.sz, d.z, c.z);
 }
 
-// A tap: read-only global load, or a plain load when SHARED (img then points
-// into shared memory, which the global read-only path cannot address).
-template <bool SHARED>
-__device__ __forceinline__ float ld_tap(const float *p) {
-    if (SHARED) return *p;
-    return __ldg(p);
+// A tap: read-only global load (a BF16-stored image widened exactly), or a
+// plain load when SHARED (img then points into shared memory, which the
+// global read-only path cannot address).
+template <bool SHARED, typename T>
+__device__ __forceinline__ float ld_tap(const T *p) {
+    if constexpr (SHARED) return *p;
+    else return ld_voxel(p);
 }
 
 // sample_image (warping.h:49-88) of NC planes that share one cell: the
@@ -140,8 +141,8 @@ __device__ __forceinline__ float ld_tap(const float *p) {
 // Plane p starts at img + p * pstride.  The sums run in the order of
 // sample_clamped above (x taps, then rows, then planes), so both give the
 // same bits.
-template <int NC, bool SHARED = false>
-__device__ __forceinline__ void sample_cell(const float *__restrict__ img, int pstride, const Cell &s,
+template <int NC, bool SHARED = false, typename T = float>
+__device__ __forceinline__ void sample_cell(const T *__restrict__ img, int pstride, const Cell &s,
                                             float out[NC]) {
     float val[NC], mn[NC], mx[NC];
 #pragma unroll
@@ -162,7 +163,7 @@ __device__ __forceinline__ void sample_cell(const float *__restrict__ img, int p
             const int row = s.x.lo + s.y.lo + b * s.sy + s.z.lo + c * s.sz;
 #pragma unroll
             for (int p = 0; p < NC; ++p) {
-                const float *r = img + p * pstride + row;
+                const T *r = img + p * pstride + row;
                 const float t0 = ld_tap<SHARED>(r), t1 = ld_tap<SHARED>(r + 1), t2 = ld_tap<SHARED>(r + 2);
                 const float t3 = s.x.t3 ? ld_tap<SHARED>(r + 3) : 0.0f;
                 const float xv = s.x.w[0] * t0 + s.x.w[1] * t1 + s.x.w[2] * t2 + s.x.w[3] * t3;

@@ -440,6 +440,45 @@ def pd_iteration(scan, angles, st, F, V, pp, pd_cut, roi_cut, alpha, bp_mode, or
     return st
 
 
+def bf16_round(a) -> np.ndarray:
+    """FP32 values rounded to the nearest BF16 (ties to even), as FP32: what a
+    BF16 store keeps (finite inputs)."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).reshape(np.shape(a))
+
+
+def pd_iteration_bf16(scan, angles, st, F, V, pp, pd_cut, roi_cut, alpha, bp_mode, orders, raylen):
+    """pd_iteration in the FP32 arithmetic with BF16 storage of the primal
+    volumes (vol, xbar, xprev): every value stored into them is rounded to the
+    nearest BF16 -- after the primal step, after each view's backprojection
+    inside SART, and after the over-relaxation -- while the duals, the warped
+    volumes and the ray lengths stay FP32.  st["proj"] (and the volumes) must
+    already hold BF16 values.  The rounding after each view is why SART runs
+    here one view per call."""
+    dims = scan.dims
+    st = {k: np.array(v, np.float32, copy=True) for k, v in st.items()}
+    roi = roi_mask(dims, roi_cut)
+    views = [view_angle(a) for a in angles]
+    opd = OPd(*pp, (C.c_int * 8)(*pd_cut))
+    for f in range(F):
+        bw = warp32(st["flow"][f], st["xbar"][f + 1], -1.0)
+        st["ytv"][f], st["ytp"][f], st["ybc"][f] = pd_dual32(dims, opd, st["xbar"][f], st["xbar"][f + 1], bw,
+                                                             st["ytv"][f], st["ytp"][f], st["ybc"][f])
+        z = np.zeros_like(st["vol"][f])
+        fw = z if f == 0 else warp32(st["flow"][f - 1], st["ybc"][f - 1], 1.0)
+        v, xp = pd_primal32(dims, opd, f == 0, z if f == 0 else st["ytp"][f - 1], st["ytp"][f], fw, st["ybc"][f],
+                            st["ytv"][f], st["vol"][f])
+        v, st["xprev"][f] = bf16_round(v), bf16_round(xp)
+        for k in orders[f]:
+            v, raylen[f] = sart32(scan, views[f * V:(f + 1) * V], [int(k)], st["proj"][f], alpha, pp[6], bp_mode, v,
+                                  raylen=raylen[f], gmode=1)
+            v = bf16_round(v)
+        st["vol"][f] = bf16_round(v * roi)
+        st["xbar"][f] = bf16_round(pd_extrapolate32(dims, pd_cut, st["vol"][f], st["xprev"][f], st["xbar"][f]))
+    return st
+
+
 def view_matrices32(scan: Scan, view: OView) -> np.ndarray:
     """P2M, M2V, model-view, V2M of the reference's FP32 pipeline (64 floats)."""
     out = np.zeros(64, np.float32)

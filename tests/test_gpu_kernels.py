@@ -356,3 +356,54 @@ def test_warp_vjp(cuda):
     rs, rv = ob.warp_vjp64(vel.astype(np.float64), src.astype(np.float64), 1.0, obar.astype(np.float64))
     assert ob.rel_l2(_np(sb), rs) < 1e-5
     assert ob.rel_l2(_np(vb), rv) < 1e-4
+
+
+@pytest.mark.parametrize("dims,det,off", [((96, 80, 112), (160, 144), (1.5, -0.7, 2.0)),
+                                          ((128, 128, 128), (192, 192), (0.0, 0.0, 0.0))])
+def test_bp_ray_scatter_slab_vs_sequential_oracle(cuda, dims, det, off):
+    """The slab-staged scatter (shared-memory box per slab, k_bp_slab.cu)
+    against the oracle's sequential scatter in FP32, on sizes where a block
+    walks many slabs: views along both axes, oblique views, an off-centre
+    volume and rays that miss."""
+    import torch
+
+    scan = ob.Scan(dims, det, off=off)
+    angles = np.array([0.0, 0.2, 0.7, 1.3, 1.5708, 2.6, 3.9, 5.5])
+    ctx = make_ctx(scan, angles)
+    rng = np.random.default_rng(5)
+    W, H = det
+    nx, ny, nz = dims
+    for v, a in enumerate(angles):
+        corr = rng.normal(size=(H, W)).astype(np.float32)
+        c = torch.zeros((nz, ny, nx), device=cuda)
+        w = torch.zeros((nz, ny, nx), device=cuda)
+        ctx.bp_ray_scatter(_t(corr, cuda), c, w, v)
+        c_ref, w_ref = ob.bp_ray_scatter32(scan, ob.view_angle(a), corr, gmode=1)
+        assert ob.rel_l2(_np(w), w_ref) < 1e-5, (v, ob.rel_l2(_np(w), w_ref))
+        assert ob.rel_l2(_np(c), c_ref) < 1e-5, (v, ob.rel_l2(_np(c), c_ref))
+    ctx.close()
+
+
+def test_gather_ceiling_packed_pairs_equal_scalar(cuda):
+    """The gather ceiling in packed FP32x2 pairs (fp_cell2/trilerp2, the
+    helpers of the packed projector variants) gives the scalar form's bits,
+    and its sums track the projector's (same rays, nearly the same samples)."""
+    import torch
+
+    scan = ob.Scan((64, 56, 72), (96, 80), off=(0.7, -1.1, 0.4))
+    angles = np.array([0.0, 0.3, 0.9, 1.5708, 2.4])
+    ctx = make_ctx(scan, angles)
+    vol = _t(phantom(scan.dims, seed=3), cuda)
+    W, H = scan.det
+    for v in range(len(angles)):
+        a = torch.zeros((H, W), device=cuda)
+        b = torch.zeros((H, W), device=cuda)
+        n = torch.zeros((H, W), dtype=torch.int32, device=cuda)
+        ctx.gather_ceiling(vol, v, a, n, packed=True)
+        ctx.gather_ceiling(vol, v, b, packed=False)
+        np.testing.assert_array_equal(_np(a), _np(b))
+        proj = torch.zeros((1, H, W), device=cuda)
+        ctx.fp(vol, proj, view0=v, nviews=1)
+        assert ob.rel_l2(_np(a), _np(proj)[0]) < 0.05
+        assert int(n.sum()) > 0
+    ctx.close()

@@ -56,7 +56,7 @@ def test_every_projector_variant_gives_the_same_bits(cuda, dims, det, off):
     views = range(len(ANGLES))
     ctx.set_tuning(0, 0, 0, staged_bins=0)  # everything through the default gather variant
     base = _corrections(ctx, vol, b, views)
-    for fv in range(1, 7):
+    for fv in range(1, 10):  # tiles, samples in flight, packed FP32x2 pairs
         ctx.set_tuning(fv, 0, 0, staged_bins=0)
         for k, (a, c) in enumerate(zip(base, _corrections(ctx, vol, b, views))):
             np.testing.assert_array_equal(a, c, err_msg=f"gather variant {fv}, output {k}")

@@ -254,3 +254,15 @@ def test_fp64_row_band_equals_the_full_projection():
     v = ob.view_angle(0.7)
     full = ob.fp64(s, v, vol)[0]
     np.testing.assert_array_equal(ob.fp64_rows(s, v, vol, 5, 7), full[5:12])
+
+
+def test_bf16_rounding_of_the_emulation_matches_torch():
+    """oracle_bind.bf16_round (the BF16 store of the storage-mode emulation)
+    rounds as torch's float32 -> bfloat16 conversion: nearest, ties to even."""
+    import torch
+
+    rng = np.random.default_rng(0)
+    a = np.concatenate([rng.normal(size=4096).astype(np.float32) * 10.0 ** rng.integers(-30, 30, 4096),
+                        np.array([1.0, 1.00390625, 1.005859375, -0.0, 0.0, 3.0e38], np.float32)]).astype(np.float32)
+    ref = torch.from_numpy(a).to(torch.bfloat16).float().numpy()
+    np.testing.assert_array_equal(ob.bf16_round(a), ref)
