@@ -1216,6 +1216,29 @@ def run_batch_only(args):
     choices = [d["ctx"].autotune(stream) for d in inst]  # every instance's own geometry
     t_tune = time.perf_counter() - t0
     t_batch = batched_time()
+    f32_result = [d["vol"].clone() for d in inst]
+    # BF16 storage of the same instances (volumes and sinograms in BF16, FP32
+    # arithmetic), the same iterations from the same start
+    inst16 = [dict(d, vol=torch.zeros_like(d["vol"], dtype=torch.bfloat16), proj=d["proj"].to(torch.bfloat16),
+                   storage="bf16") for d in inst]
+    for d in inst16:
+        d.pop("truth")
+    b16 = stt.Batch(inst16, mode=stt.SOLVE_GRAPH)
+    for _ in range(args.warmup):
+        b16.iterate(1, stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        b16.iterate(1, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_b16 = e0.elapsed_time(e1) / 1000.0 / args.steps
+    b16.close()
+    num = sum(float((d["vol"].float() - r).norm() ** 2) for d, r in zip(inst16, f32_result))
+    den = sum(float(r.norm() ** 2) for r in f32_result)
+    bf16_vs_f32 = math.sqrt(num / den)
+    bf16_err = [float((d["vol"].float() - o["truth"]).norm() / o["truth"].norm()) for d, o in zip(inst16[:4], inst)]
+    del inst16
     # the same instances one after another (each its own graph-captured solver)
     solvers = []
     for d in inst:
@@ -1243,12 +1266,17 @@ def run_batch_only(args):
                                    "detectors 128^2-384^2, 60-240 views, voxel-based BP"},
             "sequential_ms_per_iter": 1000 * t_seq, "batched_vs_sequential": t_seq / t_batch,
             "rel_l2_to_phantom_first4": errs,
+            "bf16_storage": {"ms_per_iter": 1000 * t_b16, "gups": units / t_b16 / 1e9,
+                             "rel_l2_to_f32_storage": bf16_vs_f32, "rel_l2_to_phantom_first4": bf16_err,
+                             "iterations": args.warmup + args.steps,
+                             "note": "volumes and sinograms stored in BF16, FP32 arithmetic; compared with the "
+                                     "FP32-storage batch after the same iterations from the same start"},
             "autotune": {"batched_ms_per_iter_default_choices": 1000 * t_default,
                          "batched_ms_per_iter_tuned": 1000 * t_batch, "tuned_vs_default": t_default / t_batch,
                          "tuning_s_all_instances": t_tune,
                          "cache_hits": sum(c["from_cache"] for c in choices),
-                         "fp_variant_counts": np.bincount([c["fp_variant"] for c in choices], minlength=7).tolist(),
-                         "slab_variant_counts": np.bincount([c["slab_variant"] for c in choices], minlength=4).tolist(),
+                         "fp_variant_counts": np.bincount([c["fp_variant"] for c in choices], minlength=10).tolist(),
+                         "slab_variant_counts": np.bincount([c["slab_variant"] for c in choices], minlength=8).tolist(),
                          "bp_variant_counts": np.bincount([c["bp_variant"] for c in choices], minlength=3).tolist(),
                          "first_instances": [{k: c[k] for k in ("fp", "slab", "bp", "staged_bins")}
                                              for c in choices[:4]]}}

@@ -173,7 +173,7 @@ class Context:
     def _tuning_dict(t: Tuning) -> dict:
         return {"fp_variant": t.fp_variant, "slab_variant": t.slab_variant, "bp_variant": t.bp_variant,
                 "staged_bins": t.staged_bins, "tuned": bool(t.tuned), "from_cache": bool(t.from_cache),
-                "fp_us": list(t.fp_us)[:10], "slab_us": list(t.slab_us)[:4], "bp_us": list(t.bp_us)[:3],
+                "fp_us": list(t.fp_us)[:10], "slab_us": list(t.slab_us)[:8], "bp_us": list(t.bp_us)[:3],
                 "fp": (lib.stt_tuning_variant_name(0, t.fp_variant) or b"").decode(),
                 "slab": (lib.stt_tuning_variant_name(1, t.slab_variant) or b"").decode(),
                 "bp": (lib.stt_tuning_variant_name(2, t.bp_variant) or b"").decode()}

@@ -51,8 +51,11 @@ constexpr long long WAIT_CYCLES = 200000000LL;  // about 0.1 s: a copy that neve
 constexpr int WARPS = 4;                         // a block is 32 x WARPS detector pixels, one warp per row
 
 // The march of one ray of the block, summed into `acc`, taps from the staged
-// slabs where they are held.
-template <bool ZF, class BX>
+// slabs where they are held.  PK: inside a segment, two samples at a time in
+// the packed FP32x2 instructions (fp_cell2, trilerp2, the paired march step);
+// the same samples are added in the same order with the same roundings, so
+// the sum is the same bits.
+template <bool ZF, class BX, bool PK>
 __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap *map, const float *__restrict__ src,
                                              bool hit, const Ray &r, float *buf, uint64_t *bar, int *red_s,
                                              int (*red)[2 * WARPS], volatile int *dead, int *status, Kahan &acc) {
@@ -115,15 +118,13 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
         }
         const float *bx = buf + (k & 1) * BOXN;
         const int m0 = slab_m0(k);
-        // one sample: false (and nothing added) when it belongs to a later slab
-        auto take = [&](const float p[3]) -> bool {
-            FpCell c;
-            fp_cell(g, p, c);
-            const int bs = ZF ? c.ix : c.iz;
-            if (fwd ? bs > m0 + SLAB - 1 : bs < m0) return false;
+        // the base plane of a cell along the slab axis, and whether it belongs to a later slab
+        auto plane = [&](const FpCell &c) { return ZF ? c.ix : c.iz; };
+        auto is_later = [&](int bs) { return fwd ? bs > m0 + SLAB - 1 : bs < m0; };
+        // a cell's 8 corners: from the staged box when they lie in it, else global memory
+        auto corners = [&](const FpCell &c, int bs, float v[8]) {
             const unsigned of = (unsigned)((ZF ? c.iz : c.ix) - f0), oy = (unsigned)(c.iy - y0),
                            os = (unsigned)(bs - m0);
-            float v[8];
             if (staged && of <= FB - 2 && oy <= YB - 2 && os <= SB - 2) {
                 const float *q = bx + (os * YB + oy) * FB + of;
                 if (!ZF) {  // fast = x, slow = z
@@ -136,8 +137,35 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
             } else {
                 fp_corners<ZF ? 2 : 0, int>(src, st, c, v);
             }
+        };
+        // one sample: false (and nothing added) when it belongs to a later slab
+        auto take = [&](const float p[3]) -> bool {
+            FpCell c;
+            fp_cell(g, p, c);
+            const int bs = plane(c);
+            if (is_later(bs)) return false;
+            float v[8];
+            corners(c, bs, v);
             acc.add(__fmul_rn(trilerp(v, c), g.sd));
             return true;
+        };
+        // two consecutive samples: how many were added before one belonged to a later slab
+        auto take2 = [&](const float pa[3], const float pb[3]) -> int {
+            FpCell ca, cb;
+            fp_cell2(g, pa, pb, ca, cb);
+            const int ba = plane(ca), bb = plane(cb);
+            if (is_later(ba)) return 0;
+            float va[8], vb[8];
+            corners(ca, ba, va);
+            if (is_later(bb)) {
+                acc.add(__fmul_rn(trilerp(va, ca), g.sd));
+                return 1;
+            }
+            corners(cb, bb, vb);
+            const float2 s2 = __fmul2_rn(trilerp2(va, vb, ca, cb), make_float2(g.sd, g.sd));
+            acc.add(s2.x);
+            acc.add(s2.y);
+            return 2;
         };
         bool later = false;
         while (!later && m.peek()) {
@@ -146,18 +174,39 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
                 if (!later) m.advance();
                 continue;
             }
-            // the rest of the current segment, from registers
+            // the rest of the current segment, from registers; (x, y) and
+            // (t, z) advance as packed pairs (the same float additions)
             float t = m.t, p[3] = {m.pos[0], m.pos[1], m.pos[2]};
             int n = m.n;
+            const float2 sxy = make_float2(m.d.step[0], m.d.step[1]), stz = make_float2(m.sd, m.d.step[2]);
             do {
-                if (!take(p)) {
-                    later = true;
-                    break;
+                const float2 xy1 = __fadd2_rn(make_float2(p[0], p[1]), sxy);
+                const float2 tz1 = __fadd2_rn(make_float2(t, p[2]), stz);
+                if (PK && n + 1 < m.cap && tz1.x < m.tb) {  // the segment holds this sample and the next
+                    const float q[3] = {xy1.x, xy1.y, tz1.y};
+                    const int took = take2(p, q);
+                    if (took < 2) {
+                        if (took == 1) {
+                            t = tz1.x;
+                            p[0] = q[0], p[1] = q[1], p[2] = q[2];
+                            ++n;
+                        }
+                        later = true;
+                        break;
+                    }
+                    const float2 xy2 = __fadd2_rn(xy1, sxy), tz2 = __fadd2_rn(tz1, stz);
+                    t = tz2.x;
+                    p[0] = xy2.x, p[1] = xy2.y, p[2] = tz2.y;
+                    n += 2;
+                } else {
+                    if (!take(p)) {
+                        later = true;
+                        break;
+                    }
+                    t = tz1.x;
+                    p[0] = xy1.x, p[1] = xy1.y, p[2] = tz1.y;
+                    ++n;
                 }
-                t = __fadd_rn(t, m.sd);
-#pragma unroll
-                for (int a = 0; a < 3; ++a) p[a] = __fadd_rn(p[a], m.d.step[a]);
-                ++n;
             } while (n < m.cap && t < m.tb);
             m.t = t;
             m.n = n;
@@ -194,7 +243,7 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
 // k_fp_corr (GenerateImage_MT + the correction of ST_Tomography.cpp:667-676)
 // with slab-staged gathers.  map_x covers `vol` (x-fastest), map_z `vol_t`
 // (z-fastest), both with the box of BX.
-template <class BX>
+template <class BX, bool PK>
 __global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, const ViewRec *__restrict__ views,
                                                       const __grid_constant__ CUtensorMap map_x,
                                                       const __grid_constant__ CUtensorMap map_z,
@@ -222,9 +271,9 @@ __global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, co
     }
     Kahan acc{0.0f, 0.0f};
     if (vol_t && vr.layout == 1)
-        slab_ray_sum<true, BX>(g, &map_z, vol_t, hit, r, buf, bar, red_s, red, &dead, status, acc);
+        slab_ray_sum<true, BX, PK>(g, &map_z, vol_t, hit, r, buf, bar, red_s, red, &dead, status, acc);
     else
-        slab_ray_sum<false, BX>(g, &map_x, vol, hit, r, buf, bar, red_s, red, &dead, status, acc);
+        slab_ray_sum<false, BX, PK>(g, &map_x, vol, hit, r, buf, bar, red_s, red, &dead, status, acc);
     if (!valid) return;
     const float *b = b_stack + (size_t)local * g.W * g.H;
     const size_t pix = i + (size_t)j * g.W;
@@ -291,18 +340,18 @@ void box_dims(cuuint32_t box[3]) {
     box[2] = BX::SB;
 }
 
-template <class BX>
+template <class BX, bool PK>
 cudaError_t launch_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const float *vol,
                         const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
                         cudaStream_t s, unsigned long long corr_surf, int *status) {
     static const bool carve = [] {
-        cudaFuncSetAttribute(k_fp_corr_slab<BX>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        cudaFuncSetAttribute(k_fp_corr_slab<BX, PK>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared);
         cudaGetLastError();
         return true;
     }();
     (void)carve;
-    k_fp_corr_slab<BX><<<dim3((g.W + 31) / 32, (g.H + WARPS - 1) / WARPS, 1), 32 * WARPS, 0, s>>>(
+    k_fp_corr_slab<BX, PK><<<dim3((g.W + 31) / 32, (g.H + WARPS - 1) / WARPS, 1), 32 * WARPS, 0, s>>>(
         g, views, m.x, m.z, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, status);
     return cudaGetLastError();
 }
@@ -310,7 +359,9 @@ cudaError_t launch_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps
 }  // namespace
 
 const char *slab_variant_name(int v) {
-    static const char *names[kSlabVariants] = {"box 48x8x12", "box 48x8x8", "box 64x8x10", "box 40x8x16"};
+    static const char *names[kSlabVariants] = {"box 48x8x12", "box 48x8x8", "box 64x8x10", "box 40x8x16",
+                                               "box 48x8x12, packed pairs", "box 48x8x8, packed pairs",
+                                               "box 64x8x10, packed pairs", "box 40x8x16, packed pairs"};
     return v >= 0 && v < kSlabVariants ? names[v] : "?";
 }
 
@@ -319,7 +370,7 @@ bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, F
     if ((long long)g.nx * g.ny * g.nz >= (1LL << 31)) return false;  // 32-bit fallback offsets
     if (variant < 0 || variant >= kSlabVariants) return false;
     cuuint32_t box[3];
-    switch (variant) {
+    switch (variant & 3) {  // variants 4..7: the boxes of 0..3 with packed sample pairs
     case 1: box_dims<Box1>(box); break;
     case 2: box_dims<Box2>(box); break;
     case 3: box_dims<Box3>(box); break;
@@ -337,12 +388,18 @@ cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const Fp
                                 const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state,
                                 float *corr, cudaStream_t s, unsigned long long corr_surf, int *status) {
     if (!m.ok || (vol_t && !m.has_z)) return cudaErrorInvalidValue;
+#define STT_SLAB(B, P) launch_slab<B, P>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status)
     switch (m.variant) {
-    case 1: return launch_slab<Box1>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status);
-    case 2: return launch_slab<Box2>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status);
-    case 3: return launch_slab<Box3>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status);
-    default: return launch_slab<Box0>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status);
+    case 1: return STT_SLAB(Box1, false);
+    case 2: return STT_SLAB(Box2, false);
+    case 3: return STT_SLAB(Box3, false);
+    case 4: return STT_SLAB(Box0, true);
+    case 5: return STT_SLAB(Box1, true);
+    case 6: return STT_SLAB(Box2, true);
+    case 7: return STT_SLAB(Box3, true);
+    default: return STT_SLAB(Box0, false);
     }
+#undef STT_SLAB
 }
 
 }  // namespace stt

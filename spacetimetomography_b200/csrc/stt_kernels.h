@@ -28,7 +28,7 @@ int grid_stride_blocks(long long n, int threads);
 //   slab: the box of the slab-staged projector (slab_variant_name);
 //   bp:   the column length of the voxel backprojection (bp_variant_name).
 // Which views the slab kernel projects is the per-view ViewRec::staged flag.
-constexpr int kFpVariants = 10, kSlabVariants = 4, kBpVariants = 3;
+constexpr int kFpVariants = 10, kSlabVariants = 8, kBpVariants = 3;
 struct Tuning {
     int fp = 0, slab = 0, bp = 0;
 };

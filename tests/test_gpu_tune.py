@@ -60,7 +60,7 @@ def test_every_projector_variant_gives_the_same_bits(cuda, dims, det, off):
         ctx.set_tuning(fv, 0, 0, staged_bins=0)
         for k, (a, c) in enumerate(zip(base, _corrections(ctx, vol, b, views))):
             np.testing.assert_array_equal(a, c, err_msg=f"gather variant {fv}, output {k}")
-    for sv in range(4):  # every view through the slab-staged kernel with each box
+    for sv in range(8):  # every view through the slab-staged kernel with each box, scalar and packed
         ctx.set_tuning(0, sv, 0, staged_bins=0x1FF)
         for k, (a, c) in enumerate(zip(base, _corrections(ctx, vol, b, views))):
             np.testing.assert_array_equal(a, c, err_msg=f"slab box {sv}, output {k}")
