@@ -93,6 +93,10 @@ def parse_args():
     ap.add_argument("--config", type=int, choices=sorted(CONFIG_SPECS), default=None,
                     help="run only the single-frame workload of that number (1: 128^3 SART, 2: 256^3 PD TV, "
                          "5: 512^3 PD TV) and print its own line")
+    ap.add_argument("--bp-ray-probe", action="store_true",
+                    help="with --config: only run a few ray-driven backprojections at the workload's size")
+    ap.add_argument("--fp64-pd-check", action="store_true",
+                    help="run only the full-size FP64 check of one 4D primal-dual iteration (two frames) and print it")
     ap.add_argument("--no-configs", action="store_true",
                     help="default run: skip the single-frame workloads' sub-lines")
     ap.add_argument("--fp-probe", action="store_true",
@@ -360,6 +364,73 @@ def fp64_sart_check(ctx, st, args, gmax, n_views: int = 6):
                 "sample": f"SART over {n_views} views of frame 0 at {N}^3/{D}^2 from the solver's current state"}
 
     return run
+
+
+def fp64_pd_iteration_check(args, dev, stream, ob) -> dict:
+    """One whole 4D primal-dual iteration at the workload's full size against
+    the FP64 oracle, per state: two frames of the sequence (frame 0 takes the
+    first-frame primal, frame 1 the forward warp of frame 0's Y_bc), every
+    view of each frame (36 at the default size), from a state one GPU
+    iteration into the solve (non-zero duals).  The GPU's graph-captured
+    solver and the oracle's reference-ordered loop (backward warp, dual,
+    forward warp, primal, SART with voxel BP, ROI mask, over-relaxation) start
+    from the same FP32 state; the sticky ray lengths start at zero in both."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200 import phantom as ph
+
+    N, V, D, F = args.n, args.views, args.det, 2
+    dims = (N, N, N)
+    ang = angles_for(args, 0)[:F * V]
+    ctx = stt.Context(dev.index or 0)
+    ctx.set_geometry(dims, (1.0, 1.0, 1.0), (D, D), 1.0, 600.0, 1000.0, ang)
+    params = ph.ellipsoid_params(30, dims, seed=2024, semi=(5.0 * N / 256, 40.0 * N / 256))
+    proj = torch.empty((F, V, D, D), device=dev)
+    flow = torch.empty((F, 3, N, N, N), device=dev)
+    vol = torch.empty((F + 1, N, N, N), device=dev)
+    for f in range(F):
+        truth = ph.rasterize(ph.displaced_params(params, f, args.frames, 4.0, 2 * math.pi / N, 0.7), dims, dev)
+        ctx.fp(truth, proj[f], view0=f * V, nviews=V)
+        flow[f] = ph.deformation_flow(dims, f, f + 1, args.frames, 4.0, 2 * math.pi / N, 0.7, device=dev)
+        vol[f] = truth * 0.8
+    vol[F] = vol[F - 1]
+    torch.cuda.synchronize()
+    gmax = float(proj[0].max().item() / 4.0)
+    pd = pd_params(gmax)
+    z = lambda *s_: torch.zeros(s_, device=dev)  # noqa: E731
+    st = dict(vol=vol, xbar=vol.clone(), xprev=z(F, N, N, N), ytv=z(F, 3, N, N, N), ytp=z(F, N, N, N),
+              ybc=z(F, N, N, N), flow=flow, proj=proj)
+    s1 = stt.Solver(ctx, st, F, V, pd, alpha=0.3, bp_mode=0, seed=5, mode=stt.SOLVE_GRAPH)
+    s1.iterate(1, stream)  # into the solve: non-zero duals
+    torch.cuda.synchronize()
+    s1.close()
+    start = {k: v.detach().cpu().numpy().copy() for k, v in st.items()}
+    s2 = stt.Solver(ctx, st, F, V, pd, alpha=0.3, bp_mode=0, seed=11, mode=stt.SOLVE_GRAPH)
+    s2.iterate(1, stream)
+    torch.cuda.synchronize()
+    s2.poll_status(stream)
+    s2.close()
+    gpu = {k: v.detach().cpu().numpy() for k, v in st.items()}
+    ctx.close()
+    del st, proj, flow, vol
+    torch.cuda.empty_cache()
+    pp = [pd.sigma, pd.tau, pd.tv_w, pd.tp_w, pd.bc_w, pd.huber_factor, gmax]
+    scan = ob.Scan(N, (D, D))
+    orders = [stt.frame_order(11, 0, F, f, V) for f in range(F)]
+    raylen = [np.zeros((D, D), np.float64) for _ in range(F)]
+    t0 = time.perf_counter()
+    from spacetimetomography_b200.api import REFERENCE_CUT
+
+    ref = ob.pd_iteration(scan, ang, start, F, V, pp, tuple(pd.cut), REFERENCE_CUT, 0.3, 0, orders, raylen,
+                          fp64=True)
+    t_ref = time.perf_counter() - t0
+    out = {k: [ob.rel_l2(gpu[k][f], ref[k][f]) for f in range(F)]
+           for k in ("vol", "xbar", "xprev", "ytv", "ytp", "ybc")}
+    out["sample"] = (f"one PD iteration of frames 0-1 at {N}^3/{D}^2, {V} views each, from one GPU iteration into "
+                     "the solve; per state, per frame: relative L2 of the GPU (FP32) against the FP64 oracle")
+    out["oracle_s"] = t_ref
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -860,6 +931,29 @@ def fp_probe(cid, dev, stream) -> None:
     ctx.close()
 
 
+def bp_ray_probe(cid, dev, stream) -> None:
+    """A few ray-driven backprojections (the slab-staged scatter and the
+    normalising update) at the workload's size and nothing else (the command
+    ncu captures for the scatter's profile)."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200 import phantom as ph
+
+    c = CONFIG_SPECS[cid]
+    N, D, V = c["n"], c["det"], c["views"]
+    ctx = stt.Context(dev.index or 0)
+    ctx.set_geometry((N, N, N), (1.0, 1.0, 1.0), (D, D), 1.0, 600.0, 1000.0, ph.equispaced_views(V))
+    vol = torch.zeros((N, N, N), device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    corr = torch.rand((D, D), device=dev, generator=g) - 0.5
+    for v in (0, V // 8, V // 4, 3 * V // 8):  # 0, 45, 90, 135 degrees
+        ctx.bp_ray(corr, vol, 1e9, v, stream=stream)
+    torch.cuda.synchronize()
+    ctx.close()
+
+
 def run_config_only(args) -> int:
     import torch
 
@@ -868,6 +962,9 @@ def run_config_only(args) -> int:
     stream = torch.cuda.Stream(device=dev)
     if args.fp_probe:
         fp_probe(args.config, dev, stream)
+        return 0
+    if args.bp_ray_probe:
+        bp_ray_probe(args.config, dev, stream)
         return 0
     clocks = ClockSampler(0)
     clocks.start()
@@ -1109,6 +1206,11 @@ def run_stt(args):
         with c_stdout_to_stderr():
             threads = os.cpu_count() or 1
             cpu = cpu_reference_sample(args, threads, cpu_sample_inputs(args, threads), gpu_check=check)
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_bind as ob
+
+        with c_stdout_to_stderr():
+            cpu["fp64_pd_iteration"] = fp64_pd_iteration_check(args, dev, stream, ob)
 
     if rank == 0:
         line = {"metric": "projector GUPS over a 4D primal-dual iteration", "value": value, "unit": "GUPS",
@@ -1134,6 +1236,7 @@ def run_stt(args):
                 "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "cpu_s_per_iter": None if cpu is None else cpu["s_per_iter"],
                 "fp64_check": None if cpu is None else cpu.get("fp64_check"),
+                "fp64_pd_iteration": None if cpu is None else cpu.get("fp64_pd_iteration"),
                 "flow": flow,
                 "configs": configs}
         print(json.dumps(line), flush=True)
@@ -1296,6 +1399,18 @@ def main():
         return run_flow_only(args)
     if args.batch_only:
         return run_batch_only(args)
+    if args.fp64_pd_check:
+        import torch
+
+        torch.cuda.set_device(0)
+        dev = torch.device("cuda", 0)
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_bind as ob
+
+        with c_stdout_to_stderr():
+            out = fp64_pd_iteration_check(args, dev, torch.cuda.Stream(device=dev), ob)
+        print(json.dumps({"fp64_pd_iteration": out}), flush=True)
+        return 0
     return run_stt(args)
 
 
