@@ -212,21 +212,29 @@ __device__ __forceinline__ void sample_d(const float *__restrict__ img, const St
     cr_dweights(s.dx, dwx);
     cr_dweights(s.dy, dwy);
     cr_dweights(s.dz, dwz);
+    // Separable sums in the forward sampler's order (x taps, then rows, then
+    // planes): per row its value and x-slope, per plane its value and x- and
+    // y-slopes, then the sample's value and gradient.
     float val = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+        float pv = 0.0f, px = 0.0f, py = 0.0f;
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const float *row = img + s.yo[b] + s.zo[c];
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                float v = __ldg(row + s.xo[a]);
-                val += s.wx[a] * s.wy[b] * s.wz[c] * v;
-                gx += dwx[a] * s.wy[b] * s.wz[c] * v;
-                gy += s.wx[a] * dwy[b] * s.wz[c] * v;
-                gz += s.wx[a] * s.wy[b] * dwz[c] * v;
-            }
+            const float t0 = __ldg(row + s.xo[0]), t1 = __ldg(row + s.xo[1]), t2 = __ldg(row + s.xo[2]),
+                        t3 = __ldg(row + s.xo[3]);
+            const float xv = s.wx[0] * t0 + s.wx[1] * t1 + s.wx[2] * t2 + s.wx[3] * t3;
+            const float xd = dwx[0] * t0 + dwx[1] * t1 + dwx[2] * t2 + dwx[3] * t3;
+            pv += s.wy[b] * xv;
+            px += s.wy[b] * xd;
+            py += dwy[b] * xv;
         }
+        val += s.wz[c] * pv;
+        gx += s.wz[c] * px;
+        gy += s.wz[c] * py;
+        gz += dwz[c] * pv;
+    }
     long long imn = s.c0, imx = s.c0;
     float mn = __ldg(img + s.c0), mx = mn;
     const int off[7] = {s.sx1, s.sx1 + s.sy1, s.sy1, s.sz1, s.sx1 + s.sz1, s.sx1 + s.sy1 + s.sz1,
@@ -257,7 +265,7 @@ __device__ __forceinline__ void scatter_sample(float *__restrict__ bar, const St
         atomicAdd(bar + r.corner, g);
         return;
     }
-#pragma unroll
+#pragma unroll 1
     for (int c = 0; c < 4; ++c)
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
@@ -313,7 +321,7 @@ __global__ void __launch_bounds__(128) k_warp_vjp(const Dim3i d, const float *__
     float v2bar[3], p2bar[3] = {0.5f * qbar[0], 0.5f * qbar[1], 0.5f * qbar[2]};
 #pragma unroll
     for (int a = 0; a < 3; ++a) v2bar[a] = 0.5f * h * qbar[a];
-#pragma unroll
+#pragma unroll 1
     for (int a = 0; a < 3; ++a) {
         SampleD r;
         sample_d(vel + a * n, s2, c2, r);
