@@ -769,7 +769,9 @@ def config_e2e(cid, ctx, proj, gmax, dev, stream) -> dict:
         t = _timed(stream, step, 2)
         solver.close()
     return {"value": N ** 3 * V / t / 1e9, "unit": "GUPS", "h2d_bytes_per_step": hproj.numel() * 4 + hvol.numel() * 4,
-            "d2h_bytes_per_step": hout.numel() * 4, "s_per_step": t}
+            "d2h_bytes_per_step": hout.numel() * 4, "s_per_step": t,
+            "through": "pinned host copies on the solve's stream around stt_sart_sweep / stt_solver_iterate, in line "
+                       "(no overlap of one step's copies with another's compute)"}
 
 
 def config_fp64_check(cid, ctx, truth, proj, gmax, dev, stream) -> dict:

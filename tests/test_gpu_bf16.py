@@ -157,3 +157,90 @@ def test_bf16_batch_equals_own_solves(cuda):
         assert float(a["vol"].float().abs().sum()) > 0
     for r in inst + ref:
         r["ctx"].close()
+
+
+def _bf16(t):
+    import torch
+
+    return t.to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("bp_mode", [0, 1])
+def test_bf16_sart_sweep_equals_rounded_fp32_views(cuda, bp_mode):
+    """stt_sart_sweep_typed(BF16) against the FP32 sweep run one view at a time
+    on the widened volume, rounded to BF16 after each view: the same bits with
+    voxel BP (gathers only), within a few rounding flips with ray BP (float
+    atomics)."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+
+    scan = ob.Scan((40, 36, 44), (64, 56), off=(0.4, -0.3, 0.2))
+    V = 9
+    angles = np.linspace(0, 2 * np.pi, V, endpoint=False) + 0.2
+    ctx = stt.Context(0)
+    ctx.set_geometry(scan.dims, scan.sp, scan.det, scan.ds, scan.sid, scan.sdd, angles, scan.off)
+    from spacetimetomography_b200 import phantom as ph
+
+    truth = ph.ellipsoid_phantom(scan.dims, 5, seed=4, semi=(3.0, 10.0)).to(cuda)
+    proj = torch.zeros((V,) + scan.det[::-1], device=cuda)
+    ctx.fp(truth, proj)
+    proj16 = _bf16(proj)
+    start = _bf16(truth * 0.7)
+    perm = stt.permutation(3, V)
+    gmax = float(proj.max()) / 4
+    a = start.clone()
+    rl = torch.zeros(scan.det[::-1], device=cuda)
+    ctx.sart_sweep(a, proj16, perm, 0.3, gmax, bp_mode, rl)
+    b = start.float()
+    rl2 = torch.zeros(scan.det[::-1], device=cuda)
+    pf = proj16.float()
+    for k in perm:
+        ctx.sart_sweep(b, pf, [int(k)], 0.3, gmax, bp_mode, rl2)
+        b = b.to(torch.bfloat16).float()
+    torch.cuda.synchronize()
+    if bp_mode == 0:
+        np.testing.assert_array_equal(a.float().cpu().numpy(), b.cpu().numpy())
+    else:
+        assert ob.rel_l2(a.float().cpu().numpy(), b.cpu().numpy()) < 3e-3
+    ctx.close()
+
+
+def test_bf16_voxel_bp_and_warp_entry_points(cuda):
+    """stt_bp_voxel_typed(BF16) equals the FP32 backprojection of the widened
+    volume rounded to BF16; stt_warp_typed(BF16) equals the FP32 warp of the
+    widened source (within an ulp: two compiled instantiations of the sampler
+    may contract differently); stt_bp_ray_typed(BF16) is within BF16 rounding
+    flips of the rounded FP32 form."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+
+    scan = ob.Scan((48, 40, 36), (72, 64))
+    angles = np.array([0.3, 1.9])
+    ctx = stt.Context(0)
+    ctx.set_geometry(scan.dims, scan.sp, scan.det, scan.ds, scan.sid, scan.sdd, angles, scan.off)
+    g = torch.Generator(device=cuda)
+    g.manual_seed(2)
+    vol16 = _bf16(torch.rand(scan.dims[::-1], device=cuda, generator=g))
+    corr = torch.randn(scan.det[::-1], device=cuda, generator=g)
+    a = vol16.clone()
+    ctx.bp_voxel(corr, a, 0.3, 5.0, 1)
+    b = vol16.float()
+    ctx.bp_voxel(corr, b, 0.3, 5.0, 1)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(a.float().cpu().numpy(), _bf16(b).float().cpu().numpy())
+    a = vol16.clone()
+    ctx.bp_ray(corr, a, 5.0, 0)
+    b = vol16.float()
+    ctx.bp_ray(corr, b, 5.0, 0)
+    torch.cuda.synchronize()
+    assert ob.rel_l2(a.float().cpu().numpy(), _bf16(b).float().cpu().numpy()) < 1e-3
+    nz, ny, nx = scan.dims[::-1]
+    flow = torch.randn((3, nz, ny, nx), device=cuda, generator=g) * 0.7
+    w16 = stt.warp(flow, vol16, -1.0)
+    w32 = stt.warp(flow, vol16.float(), -1.0)
+    torch.cuda.synchronize()
+    assert w16.dtype == torch.float32
+    assert ob.rel_l2(w16.cpu().numpy(), w32.cpu().numpy()) < 1e-6
+    ctx.close()
