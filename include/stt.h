@@ -141,12 +141,16 @@ typedef struct stt_tuning {
     int tuned;       /* 0: the defaults; 1: set by stt_autotune or stt_set_tuning */
     int from_cache;  /* stt_autotune: the choice came from the cache (nothing timed) */
     float fp_us[12], slab_us[8], bp_us[4];
+    int ray_variant;  /* the ray-driven backprojection's scatter (kernel 3 of stt_tuning_variant_name);
+                         untuned: the shared-memory slab box from 2^26 voxels on, else global atomics */
+    float ray_us[2];
 } stt_tuning;
 stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream);
 stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out);
 stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t);
 /* Description of variant `variant` of kernel `kernel` (0 gather projector,
- * 1 slab-staged projector, 2 voxel backprojection); NULL when out of range. */
+ * 1 slab-staged projector, 2 voxel backprojection, 3 ray backprojection
+ * scatter); NULL when out of range. */
 const char *stt_tuning_variant_name(int kernel, int variant);
 
 /* ---- forward projector (TypicalRayProducer.core.h:123-268) ---------------

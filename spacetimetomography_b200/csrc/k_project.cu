@@ -568,17 +568,26 @@ cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const unsigne
     return cudaGetLastError();
 }
 
-// The scatter of the ray-driven backprojection: slab-staged below 2^31 voxels.
+const char *ray_variant_name(int v) {
+    static const char *names[kRayVariants] = {"global vector atomic per corner", "shared-memory box per slab"};
+    return v >= 0 && v < kRayVariants ? names[v] : "?";
+}
+
+int default_ray_variant(const GeomDev &g) { return (long long)g.nx * g.ny * g.nz >= (1LL << 26) ? 1 : 0; }
+
+// The scatter of the ray-driven backprojection: ray variant 1 (the slab box,
+// below 2^31 voxels) or 0 (a global vector atomic per corner).
 static cudaError_t bp_ray_scatter_any(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                                      float2 *acc, cudaStream_t s) {
-    if (small_volume(g)) return launch_bp_ray_scatter_slab(g, views, sel, corr, acc, s);
+                                      float2 *acc, cudaStream_t s, int ray_variant) {
+    if (ray_variant < 0) ray_variant = default_ray_variant(g);
+    if (ray_variant == 1 && small_volume(g)) return launch_bp_ray_scatter_slab(g, views, sel, corr, acc, s);
     k_bp_ray_scatter<<<ray_grid(g, 1), 128, 0, s>>>(g, views, sel, corr, acc);
     return cudaGetLastError();
 }
 
 cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                          float2 *acc, float *vol, float gmax, cudaStream_t s) {
-    cudaError_t e = bp_ray_scatter_any(g, views, sel, corr, acc, s);
+                          float2 *acc, float *vol, float gmax, cudaStream_t s, int ray_variant) {
+    cudaError_t e = bp_ray_scatter_any(g, views, sel, corr, acc, s, ray_variant);
     if (e != cudaSuccess) return e;
     const long long n = (long long)g.nx * g.ny * g.nz;
     k_bp_ray_update<float><<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, acc, vol, gmax);
@@ -586,8 +595,8 @@ cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel 
 }
 
 cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                          float2 *acc, unsigned short *vol, float gmax, cudaStream_t s) {
-    cudaError_t e = bp_ray_scatter_any(g, views, sel, corr, acc, s);
+                          float2 *acc, unsigned short *vol, float gmax, cudaStream_t s, int ray_variant) {
+    cudaError_t e = bp_ray_scatter_any(g, views, sel, corr, acc, s, ray_variant);
     if (e != cudaSuccess) return e;
     const long long n = (long long)g.nx * g.ny * g.nz;
     k_bp_ray_update<unsigned short><<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, acc, vol, gmax);
@@ -595,8 +604,8 @@ cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel 
 }
 
 cudaError_t launch_bp_ray_scatter(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                                  float2 *acc, float *contrib, float *wsum, cudaStream_t s) {
-    cudaError_t e = bp_ray_scatter_any(g, views, sel, corr, acc, s);
+                                  float2 *acc, float *contrib, float *wsum, cudaStream_t s, int ray_variant) {
+    cudaError_t e = bp_ray_scatter_any(g, views, sel, corr, acc, s, ray_variant);
     if (e != cudaSuccess) return e;
     const long long n = (long long)g.nx * g.ny * g.nz;
     k_acc_split<<<grid_stride_blocks(n, 256), 256, 0, s>>>(n, acc, contrib, wsum);

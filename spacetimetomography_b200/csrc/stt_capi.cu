@@ -278,6 +278,7 @@ stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g) {
     ctx->sp[0] = g->sx;
     ctx->sp[1] = g->sy;
     ctx->sp[2] = g->sz;
+    ctx->tuning.ray = stt::default_ray_variant(d);  // (depends on the volume size just set)
     ctx->has_geom = true;
     return STT_OK;
 }
@@ -457,7 +458,7 @@ stt_status stt_bp_ray(stt_ctx *ctx, const float *corr, float *vol, float gmax, i
     if ((st = set_device(ctx))) return st;
     if ((st = ensure_acc(ctx, S(stream)))) return st;
     const stt::ViewSel sel{view, nullptr, 0, view};
-    STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, sel, corr, ctx->acc, vol, gmax, S(stream)),
+    STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, sel, corr, ctx->acc, vol, gmax, S(stream), ctx->tuning.ray),
              "k_bp_ray launch");
     return STT_OK;
 }
@@ -474,7 +475,7 @@ stt_status stt_bp_ray_typed(stt_ctx *ctx, const float *corr, void *vol, int dtyp
     if ((st = ensure_acc(ctx, S(stream)))) return st;
     const stt::ViewSel sel{view, nullptr, 0, view};
     STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, sel, corr, ctx->acc, static_cast<unsigned short *>(vol),
-                                     gmax, S(stream)),
+                                     gmax, S(stream), ctx->tuning.ray),
              "k_bp_ray launch");
     return STT_OK;
 }
@@ -488,7 +489,8 @@ stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, f
     if ((st = set_device(ctx))) return st;
     if ((st = ensure_acc(ctx, S(stream)))) return st;
     const stt::ViewSel sel{view, nullptr, 0, view};
-    STT_CUDA(ctx, stt::launch_bp_ray_scatter(ctx->g, ctx->views_d, sel, corr, ctx->acc, contrib, wsum, S(stream)),
+    STT_CUDA(ctx, stt::launch_bp_ray_scatter(ctx->g, ctx->views_d, sel, corr, ctx->acc, contrib, wsum, S(stream),
+                                             ctx->tuning.ray),
              "k_bp_ray_scatter launch");
     return STT_OK;
 }
@@ -569,7 +571,8 @@ static stt_status sart_sweep_t(stt_ctx *ctx, T *vol, const T *proj_stack, const 
             STT_CUDA(ctx, stt::launch_bp_voxel(ctx->g, ctx->views_d, sel, ctx->corr, vol, (float)alpha, gmax, s),
                      "k_bp_voxel launch");
         else
-            STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, sel, ctx->corr, ctx->acc, vol, gmax, s),
+            STT_CUDA(ctx, stt::launch_bp_ray(ctx->g, ctx->views_d, sel, ctx->corr, ctx->acc, vol, gmax, s,
+                                             ctx->tuning.ray),
                      "k_bp_ray launch");
     }
     if (bp_mode == 1 && raylen_state)

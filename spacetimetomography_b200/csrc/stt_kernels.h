@@ -26,15 +26,23 @@ int grid_stride_blocks(long long n, int threads);
 //   fp:   the gather forward projector k_fp_corr: detector tile and samples
 //         in flight (fp_variant_name);
 //   slab: the box of the slab-staged projector (slab_variant_name);
-//   bp:   the column length of the voxel backprojection (bp_variant_name).
+//   bp:   the column length of the voxel backprojection (bp_variant_name);
+//   ray:  the scatter of the ray-driven backprojection (ray_variant_name):
+//         0 one global vector atomic per corner, 1 a shared-memory box per
+//         slab (volumes below 2^31 voxels).  Its sums differ in float order
+//         only (as any two atomic runs do), not in their terms.
 // Which views the slab kernel projects is the per-view ViewRec::staged flag.
-constexpr int kFpVariants = 10, kSlabVariants = 8, kBpVariants = 3;
+constexpr int kFpVariants = 10, kSlabVariants = 8, kBpVariants = 3, kRayVariants = 2;
 struct Tuning {
-    int fp = 0, slab = 0, bp = 0;
+    int fp = 0, slab = 0, bp = 0, ray = 0;
 };
 const char *fp_variant_name(int v);
 const char *slab_variant_name(int v);
 const char *bp_variant_name(int v);
+const char *ray_variant_name(int v);
+// The scatter an untuned context uses: the slab box from 2^26 voxels on (at
+// 512^3 it is the faster form; at 256^3 and below the global scatter is).
+int default_ray_variant(const GeomDev &g);
 
 cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, int view0,
                       int nviews, float *proj, float *raylen, float *weight, cudaStream_t s);
@@ -91,17 +99,17 @@ cudaError_t launch_correction(long long n, const unsigned short *b, const float 
 cudaError_t launch_correction(long long n, const float *b, const float *ax, const float *raylen,
                               float *corr, cudaStream_t s);
 // Ray-driven backprojection: the scatter into acc (interleaved contribution,
-// weight), then vol += contribution/weight and acc cleared.  The scatter
-// accumulates each block's samples in a shared-memory box per slab
-// (k_bp_slab.cu) below 2^31 voxels, else with a global atomic per corner.
+// weight), then vol += contribution/weight and acc cleared.  The scatter is
+// ray variant `ray_variant` (-1: default_ray_variant): a global atomic per
+// corner, or a shared-memory box per slab (k_bp_slab.cu, below 2^31 voxels).
 cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                          float2 *acc, float *vol, float gmax, cudaStream_t s);
+                          float2 *acc, float *vol, float gmax, cudaStream_t s, int ray_variant = -1);
 cudaError_t launch_bp_ray(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                          float2 *acc, unsigned short *vol, float gmax, cudaStream_t s);
+                          float2 *acc, unsigned short *vol, float gmax, cudaStream_t s, int ray_variant = -1);
 cudaError_t launch_bp_ray_scatter_slab(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
                                        float2 *acc, cudaStream_t s);
 cudaError_t launch_bp_ray_scatter(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,
-                                  float2 *acc, float *contrib, float *wsum, cudaStream_t s);
+                                  float2 *acc, float *contrib, float *wsum, cudaStream_t s, int ray_variant = -1);
 cudaError_t launch_fp_adjoint(const GeomDev &g, const ViewRec *views, int view0, int nviews,
                               const float *proj_bar, float *vol_bar, cudaStream_t s);
 // The gather ceiling (k_project.cu): one view's rays sampled at the

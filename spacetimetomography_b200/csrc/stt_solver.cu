@@ -295,7 +295,8 @@ stt_status enqueue_sart_batched(stt_solver *s, int f, cudaStream_t cs, long long
                                           tex ? s->corr_tex[f].tex : 0, s->ctx->tuning.bp),
                   "bp_voxel");
         else
-            SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs),
+            SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs,
+                                        s->ctx->tuning.ray),
                   "bp_ray");
         nl += voxel ? 2 : 3;
     }
@@ -435,7 +436,8 @@ stt_status plain_frame_tail(stt_solver *s, int f, cudaStream_t cs, long long &nl
                 SCUDA(s, stt::launch_fill_zero(rl, (long long)s->npix, cs), "fill");
                 SCUDA(s, fp_view(g, s->views, vol, volt, view, s->ax, rl, cs), "fp");
                 SCUDA(s, stt::launch_correction((long long)s->npix, b, s->ax, rl, corr, cs), "correction");
-                SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs),
+                SCUDA(s, stt::launch_bp_ray(g, s->views, sel, corr, s->acc + f * s->n, vol, s->cfg.pd.gmax, cs,
+                                            s->ctx->tuning.ray),
                       "bp_ray");
                 nl += 5;
             }

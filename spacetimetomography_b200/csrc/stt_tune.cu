@@ -50,6 +50,7 @@ std::string shape_key(const stt_ctx *ctx) {
 // Device scratch of one tuning run, released on every return path.
 struct Scratch {
     float *vol = nullptr, *volt = nullptr, *b = nullptr, *rl = nullptr, *corr = nullptr;
+    float2 *acc = nullptr;
     stt::ViewRec *tv = nullptr;
     cudaArray_t arr = nullptr;
     cudaTextureObject_t tex = 0;
@@ -60,6 +61,7 @@ struct Scratch {
         cudaFree(b);
         cudaFree(rl);
         cudaFree(corr);
+        cudaFree(acc);
         cudaFree(tv);
         if (tex) cudaDestroyTextureObject(tex);
         if (arr) cudaFreeArray(arr);
@@ -108,7 +110,8 @@ extern "C" {
 const char *stt_tuning_variant_name(int kernel, int variant) {
     const char *s = kernel == 0 ? stt::fp_variant_name(variant)
                     : kernel == 1 ? stt::slab_variant_name(variant)
-                    : kernel == 2 ? stt::bp_variant_name(variant) : "?";
+                    : kernel == 2 ? stt::bp_variant_name(variant)
+                    : kernel == 3 ? stt::ray_variant_name(variant) : "?";
     return s[0] == '?' ? nullptr : s;
 }
 
@@ -119,6 +122,7 @@ stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out) {
     out->fp_variant = ctx->tuning.fp;
     out->slab_variant = ctx->tuning.slab;
     out->bp_variant = ctx->tuning.bp;
+    out->ray_variant = ctx->tuning.ray;
     out->staged_bins = ctx->staged_bins;
     out->tuned = ctx->tuned ? 1 : 0;
     return STT_OK;
@@ -129,7 +133,7 @@ stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t) {
     if (!ctx->has_geom) return STT_ERR_STATE;
     if (t->fp_variant < 0 || t->fp_variant >= stt::kFpVariants || t->slab_variant < 0 ||
         t->slab_variant >= stt::kSlabVariants || t->bp_variant < 0 || t->bp_variant >= stt::kBpVariants ||
-        (t->staged_bins >> 9) != 0) {
+        t->ray_variant < 0 || t->ray_variant >= stt::kRayVariants || (t->staged_bins >> 9) != 0) {
         ctx->err = "stt_set_tuning: a variant or staged_bins out of range";
         return STT_ERR_INVALID;
     }
@@ -141,6 +145,7 @@ stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t) {
     ctx->tuning.fp = t->fp_variant;
     ctx->tuning.slab = t->slab_variant;
     ctx->tuning.bp = t->bp_variant;
+    ctx->tuning.ray = t->ray_variant;
     ctx->staged_bins = t->staged_bins;
     ctx->tuned = true;
     ctx->report = *t;
@@ -310,6 +315,29 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
             }
             t.bp_us[bv] = tot / 2.0f;
             if (tot < best) best = tot, t.bp_variant = bv;
+        }
+    }
+    // ray backprojection: both scatters (with the update) on the view of the largest class
+    {
+        int vb = -1;
+        for (int b = 0; b < 9; ++b)
+            if (rep[b] >= 0 && (vb < 0 || count[b] > count[stt::off_axis_bin(ctx->off_axis_deg[vb])])) vb = rep[b];
+        const stt::ViewRec one = ctx->views_h[vb];
+        if ((e = cudaMalloc(&sc.acc, n * sizeof(float2))) || (e = cudaMemsetAsync(sc.acc, 0, n * sizeof(float2), s)) ||
+            (e = cudaMemcpyAsync(sc.tv, &one, sizeof one, cudaMemcpyHostToDevice, s)) || (e = cudaStreamSynchronize(s)))
+            return fail(e, "ray backprojection scratch");
+        const bool slab_ok_ray = n < (1ull << 31);
+        best = 1e300;
+        for (int rv = 0; rv < stt::kRayVariants; ++rv) {
+            if (rv == 1 && !slab_ok_ray) continue;
+            float us = 0.0f;
+            e = time_us(sc, s, [&] {
+                return stt::launch_bp_ray(g, sc.tv, stt::ViewSel{0, nullptr, 0, 0}, sc.corr, sc.acc, sc.vol, 1e30f, s,
+                                          rv);
+            }, us);
+            if (e) return fail(e, "ray backprojection");
+            t.ray_us[rv] = us;
+            if (us < best) best = us, t.ray_variant = rv;
         }
     }
     if ((e = cudaStreamSynchronize(s))) return fail(e, "synchronize");

@@ -109,9 +109,10 @@ def test_autotune_picks_a_valid_choice_and_caches_it(cuda):
     ctx = _ctx(scan, ANGLES)
     t = ctx.autotune()
     assert t["tuned"] and not t["from_cache"]
-    assert 0 <= t["fp_variant"] < 7 and 0 <= t["slab_variant"] < 4 and 0 <= t["bp_variant"] < 3
-    assert all(x > 0 for x in t["fp_us"]) and all(x > 0 for x in t["bp_us"])
-    assert t["fp"] and t["slab"] and t["bp"]
+    assert 0 <= t["fp_variant"] < 10 and 0 <= t["slab_variant"] < 8 and 0 <= t["bp_variant"] < 3
+    assert 0 <= t["ray_variant"] < 2
+    assert all(x > 0 for x in t["fp_us"]) and all(x > 0 for x in t["bp_us"]) and all(x > 0 for x in t["ray_us"])
+    assert t["fp"] and t["slab"] and t["bp"] and t["ray"]
     assert ctx.get_tuning()["fp_variant"] == t["fp_variant"]
     # a second context of the same shape takes the cached choice
     ctx2 = _ctx(scan, ANGLES)
@@ -127,3 +128,34 @@ def test_autotune_picks_a_valid_choice_and_caches_it(cuda):
         ctx.set_tuning(fp_variant=99)
     for c in (ctx, ctx2, ctx3):
         c.close()
+
+
+def test_both_ray_backprojection_scatters_agree(cuda):
+    """The two scatters of the ray-driven backprojection (global vector atomics;
+    a shared-memory box per slab) add the same terms in different float
+    orders: the same result within atomic-order rounding, on a geometry with
+    oblique and axis views and rays that miss."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+
+    scan = ob.Scan((72, 64, 80), (120, 104), off=(0.6, -0.4, 1.1))
+    ctx = _ctx(scan, ANGLES[:8])
+    g = torch.Generator(device=cuda)
+    g.manual_seed(4)
+    corr = torch.randn((scan.det[1], scan.det[0]), device=cuda, generator=g)
+    out = []
+    for rv in (0, 1):
+        ctx.set_tuning(0, 0, 0, ray_variant=rv)
+        assert ctx.get_tuning()["ray_variant"] == rv
+        c = torch.zeros(scan.dims[::-1], device=cuda)
+        w = torch.zeros(scan.dims[::-1], device=cuda)
+        for v in range(8):
+            ctx.bp_ray_scatter(corr, c, w, v)
+        torch.cuda.synchronize()
+        out.append((c.cpu().numpy(), w.cpu().numpy()))
+    assert ob.rel_l2(out[1][0], out[0][0]) < 1e-5 and ob.rel_l2(out[1][1], out[0][1]) < 1e-5
+    assert float(np.abs(out[0][1]).sum()) > 0
+    with pytest.raises(stt.STTError):
+        ctx.set_tuning(0, 0, 0, ray_variant=2)
+    ctx.close()
