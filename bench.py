@@ -1107,6 +1107,29 @@ def run_stt(args):
     fp_bytes = 4 * N ** 3 + 12 * args.det * args.det  # volume read + b read, corr write, ray length (per view)
     peak, peak_kind = peaks()
     achieved = fp_bytes / t_fp / 1e9
+    # samples per view and the gather ceiling over the same frame's views
+    w = torch.zeros((1, args.det, args.det), device=dev)
+    img = torch.zeros((1, args.det, args.det), device=dev)
+    gimg = torch.empty((args.det, args.det), device=dev)
+    gcount = torch.zeros((args.det, args.det), dtype=torch.int32, device=dev)
+    samples = gsamples = 0.0
+    for v in range(V):
+        ctx.fp(vol0, img, view0=v, nviews=1, weight=w, stream=stream)
+        ctx.gather_ceiling(vol0, v, gimg, gcount, stream=stream)
+        torch.cuda.synchronize()
+        samples += float(w.sum().item())
+        gsamples += float(gcount.sum().item())
+    e2.record(stream)
+    for v in range(V):
+        ctx.gather_ceiling(vol0, v, gimg, stream=stream)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    t_gc = e2.elapsed_time(e3) / 1000.0 / V
+    fp_samples = {"fp_s_per_view": t_fp, "samples_per_view": samples / V, "fp_gsamples_per_s": samples / V / t_fp / 1e9,
+                  "gather_ceiling_gsamples_per_s": gsamples / V / t_gc / 1e9,
+                  "fp_frac_of_gather_ceiling": (samples / V / t_fp) / (gsamples / V / t_gc),
+                  "views": f"the {V} views of frame 0, FP fused with the correction (stt_fp_correction, transposes "
+                           "included); the gather ceiling is stt_gather_ceiling on the same views"}
 
     # ---- the per-view GPU form ----
     plain = None
@@ -1227,6 +1250,7 @@ def run_stt(args):
                              "peak_source": peak_kind, "traffic": traffic_per_launch(args),
                              "algorithmic_bytes_per_launch": fp_bytes, "launch_s": t_fp,
                              "note": "volume is L2-resident; the kernel is bound by gather (L1/L2) throughput"},
+                "fp_samples": fp_samples,
                 "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "through": ("stt_host_solver_submit/_wait (include/stt_host.h), 2 slots" if world == 1
                                     else "torch pinned copies around the sharded solver"),
