@@ -1387,6 +1387,24 @@ def run_batch_only(args):
     e1.record(stream)
     torch.cuda.synchronize()
     t_seq = e0.elapsed_time(e1) / 1000.0
+    # the same instances in the plain per-view form (every view's launches
+    # from the host loop, a host synchronisation after each view), one after
+    # another: the form batching replaces
+    plain = []
+    for d, (_, st) in zip(inst, solvers):
+        plain.append(stt.Solver(d["ctx"], st, 1, d["proj"].shape[0], d["pd"], alpha=0.3, seed=d["seed"],
+                                mode=stt.SOLVE_PLAIN))
+    for sv in plain[:2]:
+        sv.iterate(1, stream)  # warm-up
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for sv in plain:
+        sv.iterate(1, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_plain = e0.elapsed_time(e1) / 1000.0
+    for sv in plain:
+        sv.close()
     errs = [float((d["vol"] - d["truth"]).norm() / d["truth"].norm()) for d in inst[:4]]
     line = {"metric": "projector GUPS over one batched iteration of independent instances", "value": units / t_batch / 1e9,
             "unit": "GUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_batch,
@@ -1394,6 +1412,9 @@ def run_batch_only(args):
             "config": {"workload": f"{args.batch_instances} single-frame TV + SART instances, cubes 64^3-192^3, "
                                    "detectors 128^2-384^2, 60-240 views, voxel-based BP"},
             "sequential_ms_per_iter": 1000 * t_seq, "batched_vs_sequential": t_seq / t_batch,
+            "plain_ms_per_iter": 1000 * t_plain, "batched_vs_plain": t_plain / t_batch,
+            "plain_note": "the same instances one after another in the per-view form (STT_SOLVE_PLAIN: each "
+                          "view's launches from a host loop, a host synchronisation per view)",
             "rel_l2_to_phantom_first4": errs,
             "bf16_storage": {"ms_per_iter": 1000 * t_b16, "gups": units / t_b16 / 1e9,
                              "rel_l2_to_f32_storage": bf16_vs_f32, "rel_l2_to_phantom_first4": bf16_err,
