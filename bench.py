@@ -934,9 +934,10 @@ def fp_probe(cid, dev, stream) -> None:
 
 
 def bp_ray_probe(cid, dev, stream) -> None:
-    """A few ray-driven backprojections (the slab-staged scatter and the
-    normalising update) at the workload's size and nothing else (the command
-    ncu captures for the scatter's profile)."""
+    """A few ray-driven backprojections at the workload's size, each view with
+    both scatters (global atomics, then the shared-memory slab box) and the
+    normalising update, and nothing else (the command ncu captures for the
+    scatters' profile)."""
     import torch
 
     import spacetimetomography_b200 as stt
@@ -951,7 +952,9 @@ def bp_ray_probe(cid, dev, stream) -> None:
     g.manual_seed(3)
     corr = torch.rand((D, D), device=dev, generator=g) - 0.5
     for v in (0, V // 8, V // 4, 3 * V // 8):  # 0, 45, 90, 135 degrees
-        ctx.bp_ray(corr, vol, 1e9, v, stream=stream)
+        for rv in (0, 1):  # both scatters: global vector atomics, the shared-memory slab box
+            ctx.set_tuning(ray_variant=rv)
+            ctx.bp_ray(corr, vol, 1e9, v, stream=stream)
     torch.cuda.synchronize()
     ctx.close()
 
