@@ -140,7 +140,7 @@ typedef struct stt_tuning {
     unsigned staged_bins;
     int tuned;       /* 0: the defaults; 1: set by stt_autotune or stt_set_tuning */
     int from_cache;  /* stt_autotune: the choice came from the cache (nothing timed) */
-    float fp_us[12], slab_us[8], bp_us[4];
+    float fp_us[12], slab_us[8], bp_us[8];
     int ray_variant;  /* the ray-driven backprojection's scatter (kernel 3 of stt_tuning_variant_name);
                          untuned: the shared-memory slab box from 2^26 voxels on, else global atomics */
     float ray_us[2];

@@ -307,7 +307,7 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
                     return fail(e, "view copy");
                 float us = 0.0f;
                 e = time_us(sc, s, [&] {
-                    return stt::launch_bp_voxel(g, sc.tv, stt::ViewSel{0, nullptr, 0, 0}, nullptr, sc.vol, 0.3f,
+                    return stt::launch_bp_voxel(g, sc.tv, stt::ViewSel{0, nullptr, 0, 0}, sc.corr, sc.vol, 0.3f,
                                                 1e30f, s, sc.tex, bv);
                 }, us);
                 if (e) return fail(e, "voxel backprojection");

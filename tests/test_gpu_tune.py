@@ -68,33 +68,44 @@ def test_every_projector_variant_gives_the_same_bits(cuda, dims, det, off):
     ctx.close()
 
 
-def test_every_backprojection_column_length_gives_the_same_bits(cuda):
+# a small scan whose blocks' detector boxes fit the staged tiles, and a highly
+# magnified one (sid 350 mm) where a 128-voxel x-run spans more than the
+# 256-pixel tile, so blocks and voxels fall back to the texture gathers
+BP_SCANS = [dict(n=40, det=(64, 56), sid=600.0), dict(n=(160, 48, 96), det=(480, 160), sid=350.0)]
+
+
+@pytest.mark.parametrize("sc", BP_SCANS)
+def test_every_backprojection_variant_gives_the_same_bits(cuda, sc):
+    """Column lengths 16/8/32 with texture gathers and the two shared-memory
+    tiles of the correction: the same solve bit for bit."""
     import torch
 
     import spacetimetomography_b200 as stt
     from spacetimetomography_b200 import phantom as ph
 
-    N, V = 40, 8
-    scan = ob.Scan(N, (64, 56))
+    V = 8
+    scan = ob.Scan(sc["n"], sc["det"], sid=sc["sid"])
+    nx, ny, nz = scan.dims
+    W, H = scan.det
     angles = np.linspace(0, 2 * math.pi, V, endpoint=False) + 0.1
-    truth = ph.ellipsoid_phantom((N, N, N), 5, seed=2, semi=(3.0, 10.0)).to(cuda)
+    truth = ph.ellipsoid_phantom(scan.dims, 5, seed=2, semi=(3.0, 10.0)).to(cuda)
     ctx = _ctx(scan, angles)
-    proj = torch.zeros((V, 56, 64), device=cuda)
+    proj = torch.zeros((V, H, W), device=cuda)
     ctx.fp(truth, proj)
     pd = stt.PdParams(gmax=float(proj.max()) / 4, tp_w=0.0, bc_w=0.0, cut=(3, 3, 3, 5, 3, 3, 6, 5))
     outs = []
-    for bv in range(3):
+    for bv in range(5):
         ctx.set_tuning(0, 0, bv)
         z = lambda *s: torch.zeros(s, device=cuda)  # noqa: E731
-        st = dict(vol=z(2, N, N, N), xbar=z(2, N, N, N), xprev=z(1, N, N, N), ytv=z(1, 3, N, N, N), ytp=z(1, N, N, N),
-                  ybc=z(1, N, N, N), flow=z(1, 3, N, N, N), proj=proj[None].contiguous())
+        st = dict(vol=z(2, nz, ny, nx), xbar=z(2, nz, ny, nx), xprev=z(1, nz, ny, nx), ytv=z(1, 3, nz, ny, nx),
+                  ytp=z(1, nz, ny, nx), ybc=z(1, nz, ny, nx), flow=z(1, 3, nz, ny, nx), proj=proj[None].contiguous())
         s = stt.Solver(ctx, st, 1, V, pd, roi_cut=(3, 3, 3, 5, 3, 3, 6, 5), seed=3)
         s.iterate(2)
         torch.cuda.synchronize()
         outs.append(st["vol"][0].cpu().numpy())
         s.close()
-    for bv in (1, 2):
-        np.testing.assert_array_equal(outs[0], outs[bv], err_msg=f"column variant {bv}")
+    for bv in range(1, 5):
+        np.testing.assert_array_equal(outs[0], outs[bv], err_msg=f"backprojection variant {bv}")
     assert np.abs(outs[0]).max() > 0
     ctx.close()
 
@@ -109,7 +120,7 @@ def test_autotune_picks_a_valid_choice_and_caches_it(cuda):
     ctx = _ctx(scan, ANGLES)
     t = ctx.autotune()
     assert t["tuned"] and not t["from_cache"]
-    assert 0 <= t["fp_variant"] < 10 and 0 <= t["slab_variant"] < 8 and 0 <= t["bp_variant"] < 3
+    assert 0 <= t["fp_variant"] < 10 and 0 <= t["slab_variant"] < 8 and 0 <= t["bp_variant"] < 5
     assert 0 <= t["ray_variant"] < 2
     assert all(x > 0 for x in t["fp_us"]) and all(x > 0 for x in t["bp_us"]) and all(x > 0 for x in t["ray_us"])
     assert t["fp"] and t["slab"] and t["bp"] and t["ray"]
