@@ -103,7 +103,12 @@ def test_solver_matches_oracle(cuda, bp_mode):
         for k in ("vol", "xbar", "xprev", "ytv", "ytp", "ybc"):
             e = ob.rel_l2(out[k][:F], ref[k][:F])
             # The duals accumulate finite differences of X_bar (a derivative of
-            # the volume), so FP32-vs-FP64 rounding of the volumes shows up
-            # amplified there; the solve's outputs are held to 1e-4.
-            t = tol if (not fp64 or k in ("vol", "xbar", "xprev")) else 10 * tol
+            # the volume), so the FP32-vs-FP64 rounding of the volumes after the
+            # first iteration's SART (X_bar 6e-5 here) shows up amplified in the
+            # second iteration's duals: measured Y_tv 1.4e-4 (voxel BP) and
+            # 1.7e-4 (ray BP), Y_tp and Y_bc at most 1.0e-4.  The volumes are
+            # held to 1e-4, the duals to 3e-4.  (From a common FP32 state, one
+            # full-size iteration's duals are within 1e-5 of FP64: the dual step
+            # itself adds no more than rounding.)
+            t = tol if (not fp64 or k in ("vol", "xbar", "xprev")) else 3 * tol
             assert e < t, (k, "fp64" if fp64 else "fp32", e)
