@@ -113,3 +113,31 @@ def test_flow_argument_checks_without_gpu(lib):
         assert lib.stt_last_error(None)
     assert lib.stt_flow_create(0, (C.c_int * 3)(2, 32, 32), C.byref(FlowParams(
         0.1, 1.2, 1.0, 0.65, 0.5, 30, 4, 3, 1, (C.c_int * 6)(*[0] * 6))), C.byref(h)) == 1
+
+
+def test_tuning_variant_names_and_struct_layout(lib):
+    """stt_tuning_variant_name names every variant of the four tuned kernels
+    and returns NULL past them; the ctypes stt_tuning matches the header's
+    layout (the host reads the tuner's report through it)."""
+    from spacetimetomography_b200._lib import SolveCfg, Instance, Tuning
+
+    counts = {0: 10, 1: 8, 2: 5, 3: 2}  # gather projector, slab projector, voxel BP, ray-BP scatter
+    for kernel, n in counts.items():
+        names = [lib.stt_tuning_variant_name(kernel, v) for v in range(n)]
+        assert all(names) and len(set(names)) == n, (kernel, names)
+        assert lib.stt_tuning_variant_name(kernel, n) is None
+        assert lib.stt_tuning_variant_name(kernel, -1) is None
+    assert lib.stt_tuning_variant_name(4, 0) is None
+    # int fp, slab, bp; unsigned bins; int tuned, from_cache; float fp_us[12], slab_us[8], bp_us[8];
+    # int ray_variant; float ray_us[2]
+    assert C.sizeof(Tuning) == 6 * 4 + (12 + 8 + 8) * 4 + 4 + 2 * 4
+    assert Tuning.ray_variant.offset == 6 * 4 + 28 * 4
+    assert SolveCfg.storage.offset > SolveCfg.autotune.offset and Instance.storage.offset > Instance.autotune.offset
+
+
+def test_typed_entry_points_reject_bad_dtypes_without_gpu(lib):
+    """The BF16-storage entry points check their dtype before touching the device."""
+    assert lib.stt_warp_typed(None, None, None, 7, 1, 1.0, None, None) == 1
+    assert lib.stt_sart_sweep_typed(None, None, 7, None, None, 0, 0, 0.3, 1.0, 0, None, None, None) != 0
+    assert lib.stt_bp_voxel_typed(None, None, None, 7, 0.3, 1.0, 0, None) != 0
+    assert lib.stt_bp_ray_typed(None, None, None, 7, 1.0, 0, None) != 0
