@@ -173,7 +173,7 @@ class Context:
     def _tuning_dict(t: Tuning) -> dict:
         return {"fp_variant": t.fp_variant, "slab_variant": t.slab_variant, "bp_variant": t.bp_variant,
                 "staged_bins": t.staged_bins, "tuned": bool(t.tuned), "from_cache": bool(t.from_cache),
-                "fp_us": list(t.fp_us)[:10], "slab_us": list(t.slab_us)[:8], "bp_us": list(t.bp_us)[:5],
+                "fp_us": list(t.fp_us)[:10], "slab_us": list(t.slab_us)[:8], "bp_us": list(t.bp_us)[:3],
                 "ray_variant": t.ray_variant, "ray_us": list(t.ray_us),
                 "ray": (lib.stt_tuning_variant_name(3, t.ray_variant) or b"").decode(),
                 "fp": (lib.stt_tuning_variant_name(0, t.fp_variant) or b"").decode(),

@@ -202,126 +202,6 @@ __global__ void __launch_bounds__(128, 10) k_bp_voxel_cols(const GeomDev g, cons
     }
 }
 
-// Column form with the correction staged in shared memory: for a rotation
-// about y a block's voxels (an x-run of 128 at one z, K voxels up y) project
-// into a detector box bounded by the projections of its corners (the
-// detector column is a Mobius function of x, the row one of x and linear in
-// y, so both are monotonic there).  The block copies that box of the
-// correction image (L2-resident) into a TW x TH tile once, and every voxel
-// reads its window rows from the tile instead of gathering them from the
-// texture: the same taps and the same arithmetic, so the same bits as
-// k_bp_voxel_cols.  A block whose box does not fit the tile gathers from the
-// texture, and so does any voxel whose window is not inside the box (the box
-// has a pixel of margin for FP32 rounding of the corners' projections; the
-// check makes every tile read in bounds whatever the rounding).
-template <int K, int TW, int TH, typename T>
-__global__ void __launch_bounds__(128) k_bp_voxel_tile(const GeomDev g, const ViewRec *__restrict__ views,
-                                                       const ViewSel sel, const float *__restrict__ corr,
-                                                       T *__restrict__ vol, float alpha, float gmax,
-                                                       unsigned long long tex) {
-    __shared__ float tile[TH * TW];
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y0 = blockIdx.y * K, z = blockIdx.z;
-    const bool live = x < g.nx;
-    int local;
-    const ViewRec &v = views[sel_view(sel, local)];
-    const int y1 = min(y0 + K, g.ny);
-    if (!(v.A[1] == 0.0f && v.A[7] == 0.0f)) {  // uniform over the launch: no tile
-        if (live)
-            for (int y = y0; y < y1; ++y) bp_voxel_at<true>(g, v, nullptr, tex, vol, x, y, z, alpha, gmax);
-        return;
-    }
-    const float fz = (float)z;
-    // the block's detector box from its corner voxels, with the window's margin
-    int bx0 = 0, by0 = 0, bw = 0, bh = 0;
-    {
-        const int xa = blockIdx.x * blockDim.x, xb = min(xa + (int)blockDim.x, g.nx) - 1;
-        float plo = 3.0e38f, phi = -3.0e38f, qlo = 3.0e38f, qhi = -3.0e38f;
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const float fx = (float)(c ? xb : xa);
-            const float nd = -bp_cam(v, 2, fx, (float)y0, fz);
-            const float up = bp_pixel(g.cx, bp_cam(v, 0, fx, (float)y0, fz), nd, g.sdd_ds);
-            plo = fminf(plo, up), phi = fmaxf(phi, up);
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                const float uq = bp_pixel(g.cy, bp_cam(v, 1, fx, (float)(r ? y1 - 1 : y0), fz), nd, g.sdd_ds);
-                qlo = fminf(qlo, uq), qhi = fmaxf(qhi, uq);
-            }
-        }
-        // windows of used voxels lie in [2, W-2) x [2, H-2) and span px-1..px+2;
-        // one more pixel each side for rounding
-        bx0 = max((int)floorf(fmaxf(plo, 2.0f)) - 2, 0);
-        by0 = max((int)floorf(fmaxf(qlo, 2.0f)) - 2, 0);
-        const int bx1 = min((int)floorf(fminf(phi, (float)(g.W - 3))) + 3, g.W - 1);
-        const int by1 = min((int)floorf(fminf(qhi, (float)(g.H - 3))) + 3, g.H - 1);
-        bw = bx1 - bx0 + 1;
-        bh = by1 - by0 + 1;
-    }
-    const bool staged = bw > 0 && bh > 0 && bw <= TW && bh <= TH;  // uniform over the block
-    if (staged) {
-        for (int q = threadIdx.x; q < bw * bh; q += blockDim.x) {
-            const int r = q / bw, c = q - r * bw;
-            tile[r * TW + c] = __ldg(corr + (size_t)(by0 + r) * g.W + (bx0 + c));
-        }
-    }
-    __syncthreads();
-    if (!live) return;
-    const float fx = (float)x;
-    const float ndepth = -bp_cam(v, 2, fx, (float)y0, fz);
-    const float upx = bp_pixel(g.cx, bp_cam(v, 0, fx, (float)y0, fz), ndepth, g.sdd_ds);
-    if (!(upx >= 2.0f && upx < (float)(g.W - 2))) return;
-    const int px = (int)upx;
-    float wx[4];
-    bp_weights(upx - (float)px, wx);
-    float R[4][4];  // R[a][b]: column px-1+a, row pyc-1+b
-    int pyc = INT_MIN / 2;
-    // the window's columns inside the tile (then every row test below keeps the reads in bounds)
-    const bool in_x = staged && px - 1 >= bx0 && px + 2 <= bx0 + bw - 1;
-    const float *trow = tile + (in_x ? px - 1 - bx0 : 0);  // column px-1 of the tile
-    for (int y = y0; y < y1; ++y) {
-        const float upy = bp_pixel(g.cy, bp_cam(v, 1, fx, (float)y, fz), ndepth, g.sdd_ds);
-        if (!(upy >= 2.0f && upy < (float)(g.H - 2))) continue;
-        const int py = (int)upy;
-        float wy[4];
-        bp_weights(upy - (float)py, wy);
-        const int s = py - pyc;
-        const bool in = in_x && py - 1 >= by0 && py + 2 <= by0 + bh - 1;
-        float r0[4], r1[4];  // rows py-1, py
-        if (s >= 0 && s <= 2) {
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                r0[a] = s == 0 ? R[a][0] : (s == 1 ? R[a][1] : R[a][2]);
-                r1[a] = s == 0 ? R[a][1] : (s == 1 ? R[a][2] : R[a][3]);
-            }
-        } else if (in) {
-            const float *p0 = trow + (py - 1 - by0) * TW;
-#pragma unroll
-            for (int a = 0; a < 4; ++a) r0[a] = p0[a], r1[a] = p0[TW + a];
-        } else {
-            const float4 gc = gather_layer(tex, px - 1, py - 1, 0), gd = gather_layer(tex, px + 1, py - 1, 0);
-            r0[0] = gc.w, r0[1] = gc.z, r0[2] = gd.w, r0[3] = gd.z;
-            r1[0] = gc.x, r1[1] = gc.y, r1[2] = gd.x, r1[3] = gd.y;
-        }
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            R[a][0] = r0[a];
-            R[a][1] = r1[a];
-        }
-        if (in) {
-            const float *p2 = trow + (py + 1 - by0) * TW;
-#pragma unroll
-            for (int a = 0; a < 4; ++a) R[a][2] = p2[a], R[a][3] = p2[TW + a];
-        } else {
-            const float4 ga = gather_layer(tex, px - 1, py + 1, 0), gb = gather_layer(tex, px + 1, py + 1, 0);
-            R[0][2] = ga.w, R[1][2] = ga.z, R[2][2] = gb.w, R[3][2] = gb.z;  // row py+1
-            R[0][3] = ga.x, R[1][3] = ga.y, R[2][3] = gb.x, R[3][3] = gb.y;  // row py+2
-        }
-        pyc = py;
-        bp_update(vol, x + (size_t)y * g.nx + (size_t)z * g.nx * g.ny, alpha, bp_sum(R, wx, wy), gmax);
-    }
-}
-
 // Dual step of one frame (ST_Tomography.cpp:504-534), fused:
 //   whole volume:     ytp += sigma*(xf1 - xf);  ybc += sigma*(bw - xf)
 //   interior & ROI:   ytv_c += sigma*(xf(p+e_c) - xf(p))*hf, clamp +-tv_w;
@@ -507,20 +387,10 @@ void bp_cols(const GeomDev &g, const ViewRec *views, const ViewSel &sel, T *vol,
                                                                                           alpha, gmax, tex);
 }
 
-template <int K, int TW, int TH, typename T>
-void bp_tile(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr, T *vol, float alpha,
-             float gmax, cudaStream_t s, unsigned long long tex) {
-    k_bp_voxel_tile<K, TW, TH, T><<<dim3((g.nx + 127) / 128, (g.ny + K - 1) / K, g.nz), 128, 0, s>>>(
-        g, views, sel, corr, vol, alpha, gmax, tex);
-}
-
 template <typename T>
 cudaError_t bp_voxel_any(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr, T *vol,
                          float alpha, float gmax, cudaStream_t s, unsigned long long corr_tex, int bp_variant) {
-    if (corr_tex && corr && bp_variant >= 3) {  // the staged tiles read corr, the fall-back the texture
-        if (bp_variant == 3) bp_tile<16, 256, 40>(g, views, sel, corr, vol, alpha, gmax, s, corr_tex);
-        else bp_tile<8, 256, 24>(g, views, sel, corr, vol, alpha, gmax, s, corr_tex);
-    } else if (corr_tex) {
+    if (corr_tex) {
         switch (bp_variant) {
         case 1: bp_cols<8>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
         case 2: bp_cols<32>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
@@ -564,9 +434,7 @@ cudaError_t pd_extrapolate_any(const int *d, const int *cut, const T *vol, const
 }  // namespace
 
 const char *bp_variant_name(int v) {
-    static const char *names[kBpVariants] = {"columns of 16 voxels", "columns of 8 voxels", "columns of 32 voxels",
-                                             "columns of 16, correction staged in a 256x40 tile",
-                                             "columns of 8, correction staged in a 256x24 tile"};
+    static const char *names[kBpVariants] = {"columns of 16 voxels", "columns of 8 voxels", "columns of 32 voxels"};
     return v >= 0 && v < kBpVariants ? names[v] : "?";
 }
 

@@ -26,15 +26,13 @@ int grid_stride_blocks(long long n, int threads);
 //   fp:   the gather forward projector k_fp_corr: detector tile and samples
 //         in flight (fp_variant_name);
 //   slab: the box of the slab-staged projector (slab_variant_name);
-//   bp:   the column length of the voxel backprojection and where its
-//         windows come from (texture gathers, or a shared-memory tile of the
-//         correction: bp_variant_name);
+//   bp:   the column length of the voxel backprojection (bp_variant_name);
 //   ray:  the scatter of the ray-driven backprojection (ray_variant_name):
 //         0 one global vector atomic per corner, 1 a shared-memory box per
 //         slab (volumes below 2^31 voxels).  Its sums differ in float order
 //         only (as any two atomic runs do), not in their terms.
 // Which views the slab kernel projects is the per-view ViewRec::staged flag.
-constexpr int kFpVariants = 10, kSlabVariants = 8, kBpVariants = 5, kRayVariants = 2;
+constexpr int kFpVariants = 10, kSlabVariants = 8, kBpVariants = 3, kRayVariants = 2;
 struct Tuning {
     int fp = 0, slab = 0, bp = 0, ray = 0;
 };

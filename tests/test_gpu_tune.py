@@ -68,16 +68,14 @@ def test_every_projector_variant_gives_the_same_bits(cuda, dims, det, off):
     ctx.close()
 
 
-# a small scan whose blocks' detector boxes fit the staged tiles, and a highly
-# magnified one (sid 350 mm) where a 128-voxel x-run spans more than the
-# 256-pixel tile, so blocks and voxels fall back to the texture gathers
+# a small scan, and a highly magnified one (sid 350 mm) where a column's
+# detector rows move by up to three pixels per voxel
 BP_SCANS = [dict(n=40, det=(64, 56), sid=600.0), dict(n=(160, 48, 96), det=(480, 160), sid=350.0)]
 
 
 @pytest.mark.parametrize("sc", BP_SCANS)
 def test_every_backprojection_variant_gives_the_same_bits(cuda, sc):
-    """Column lengths 16/8/32 with texture gathers and the two shared-memory
-    tiles of the correction: the same solve bit for bit."""
+    """Column lengths 16, 8 and 32: the same solve bit for bit."""
     import torch
 
     import spacetimetomography_b200 as stt
@@ -94,7 +92,7 @@ def test_every_backprojection_variant_gives_the_same_bits(cuda, sc):
     ctx.fp(truth, proj)
     pd = stt.PdParams(gmax=float(proj.max()) / 4, tp_w=0.0, bc_w=0.0, cut=(3, 3, 3, 5, 3, 3, 6, 5))
     outs = []
-    for bv in range(5):
+    for bv in range(3):
         ctx.set_tuning(0, 0, bv)
         z = lambda *s: torch.zeros(s, device=cuda)  # noqa: E731
         st = dict(vol=z(2, nz, ny, nx), xbar=z(2, nz, ny, nx), xprev=z(1, nz, ny, nx), ytv=z(1, 3, nz, ny, nx),
@@ -104,7 +102,7 @@ def test_every_backprojection_variant_gives_the_same_bits(cuda, sc):
         torch.cuda.synchronize()
         outs.append(st["vol"][0].cpu().numpy())
         s.close()
-    for bv in range(1, 5):
+    for bv in range(1, 3):
         np.testing.assert_array_equal(outs[0], outs[bv], err_msg=f"backprojection variant {bv}")
     assert np.abs(outs[0]).max() > 0
     ctx.close()
@@ -120,7 +118,7 @@ def test_autotune_picks_a_valid_choice_and_caches_it(cuda):
     ctx = _ctx(scan, ANGLES)
     t = ctx.autotune()
     assert t["tuned"] and not t["from_cache"]
-    assert 0 <= t["fp_variant"] < 10 and 0 <= t["slab_variant"] < 8 and 0 <= t["bp_variant"] < 5
+    assert 0 <= t["fp_variant"] < 10 and 0 <= t["slab_variant"] < 8 and 0 <= t["bp_variant"] < 3
     assert 0 <= t["ray_variant"] < 2
     assert all(x > 0 for x in t["fp_us"]) and all(x > 0 for x in t["bp_us"]) and all(x > 0 for x in t["ray_us"])
     assert t["fp"] and t["slab"] and t["bp"] and t["ray"]
