@@ -31,18 +31,21 @@ namespace stt {
 
 namespace {
 
-// A staged box (fast, y, slow) in floats; FB*4 is a multiple of 16.  The
-// variants (slab_variant_name) hold different slices of the same taps: a
-// sample whose taps are not in the box reads them from global memory, so
-// every box gives the same bits.
+// A staged box (fast, y, slow) of voxels; its rows (FB voxels of FP32 or
+// BF16) are multiples of 16 bytes.  The variants (slab_variant_name) hold
+// different slices of the same taps: a sample whose taps are not in the box
+// reads them from global memory, so every box gives the same bits.
 template <int FB_, int YB_, int SB_>
 struct SlabBox {
     static constexpr int FB = FB_, YB = YB_, SB = SB_;
     static constexpr int N = FB * YB * SB;
-    static constexpr unsigned BYTES = N * sizeof(float);
     static constexpr int SLAB = SB - 1;  // base planes per slab; the box also holds their +1 plane
-    static_assert((FB * sizeof(float)) % 16 == 0, "TMA box rows must be 16-byte multiples");
+    static_assert(FB % 8 == 0, "TMA box rows must be 16-byte multiples in FP32 and BF16");
 };
+
+// A staged voxel widened to FP32 (shared memory: plain loads).
+__device__ __forceinline__ float sm_voxel(const float *p) { return *p; }
+__device__ __forceinline__ float sm_voxel(const unsigned short *p) { return __uint_as_float((unsigned)*p << 16); }
 using Box0 = SlabBox<48, 8, 12>;
 using Box1 = SlabBox<48, 8, 8>;
 using Box2 = SlabBox<64, 8, 10>;
@@ -55,12 +58,14 @@ constexpr int WARPS = 4;                         // a block is 32 x WARPS detect
 // the packed FP32x2 instructions (fp_cell2, trilerp2, the paired march step);
 // the same samples are added in the same order with the same roundings, so
 // the sum is the same bits.
-template <bool ZF, class BX, bool PK>
-__device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap *map, const float *__restrict__ src,
-                                             bool hit, const Ray &r, float *buf, uint64_t *bar, int *red_s,
+// T: the volume's storage (float, or BF16 bits widened exactly to FP32).
+template <bool ZF, class BX, bool PK, typename T>
+__device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap *map, const T *__restrict__ src,
+                                             bool hit, const Ray &r, T *buf, uint64_t *bar, int *red_s,
                                              int (*red)[2 * WARPS], volatile int *dead, int *status, Kahan &acc) {
     constexpr int FB = BX::FB, YB = BX::YB, SB = BX::SB, BOXN = BX::N, SLAB = BX::SLAB;
-    constexpr unsigned BOX_BYTES = BX::BYTES;
+    constexpr unsigned BOX_BYTES = BX::N * sizeof(T);
+    constexpr int ALIGN = 16 / sizeof(T);  // a TMA box starts on 16 bytes along its innermost axis
     const Strides st = ZF ? zyx_strides(g) : xyz_strides(g);
     MarchGen m;
     if (hit) m.init(g, r);
@@ -86,7 +91,7 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
         slab::ray_box_low<ZF, SLAB>(g, r, hit, slab_m0(0), f0, y0);
         slab::block_min2<WARPS>(f0, y0, red[0]);
         if (f0 == INT_MAX) f0 = y0 = 0;
-        f0 = (f0 >> 2) << 2;  // the box's innermost coordinate starts on 16 bytes
+        f0 &= ~(ALIGN - 1);  // the box's innermost coordinate starts on 16 bytes (rounded down, also below 0)
         if (threadIdx.x == 0) {
             tma::mbar_arrive_expect_tx(&bar[0], BOX_BYTES);
             tma::load_box_3d(buf, map, f0, y0, slab_m0(0), &bar[0]);
@@ -101,7 +106,7 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
             slab::ray_box_low<ZF, SLAB>(g, r, hit, slab_m0(k + 1), fn, yn);
             slab::block_min2<WARPS>(fn, yn, red[(k + 1) & 1]);
             if (fn == INT_MAX) fn = yn = 0;
-            fn = (fn >> 2) << 2;
+            fn &= ~(ALIGN - 1);
             if (threadIdx.x == 0) {
                 const int nb = (k + 1) & 1;
                 tma::mbar_arrive_expect_tx(&bar[nb], BOX_BYTES);
@@ -116,7 +121,7 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
                 if (status) atomicExch(status, STT_WAIT_TIMEOUT_FLAG);
             }
         }
-        const float *bx = buf + (k & 1) * BOXN;
+        const T *bx = buf + (k & 1) * BOXN;
         const int m0 = slab_m0(k);
         // the base plane of a cell along the slab axis, and whether it belongs to a later slab
         auto plane = [&](const FpCell &c) { return ZF ? c.ix : c.iz; };
@@ -126,13 +131,16 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
             const unsigned of = (unsigned)((ZF ? c.iz : c.ix) - f0), oy = (unsigned)(c.iy - y0),
                            os = (unsigned)(bs - m0);
             if (staged && of <= FB - 2 && oy <= YB - 2 && os <= SB - 2) {
-                const float *q = bx + (os * YB + oy) * FB + of;
+                const T *q = bx + (os * YB + oy) * FB + of;
+                constexpr int P = FB * YB;  // plane stride
                 if (!ZF) {  // fast = x, slow = z
-                    v[0] = q[0], v[1] = q[1], v[2] = q[FB], v[3] = q[FB + 1];
-                    v[4] = q[FB * YB], v[5] = q[FB * YB + 1], v[6] = q[FB * YB + FB], v[7] = q[FB * YB + FB + 1];
+                    v[0] = sm_voxel(q), v[1] = sm_voxel(q + 1), v[2] = sm_voxel(q + FB), v[3] = sm_voxel(q + FB + 1);
+                    v[4] = sm_voxel(q + P), v[5] = sm_voxel(q + P + 1), v[6] = sm_voxel(q + P + FB),
+                    v[7] = sm_voxel(q + P + FB + 1);
                 } else {  // fast = z, slow = x
-                    v[0] = q[0], v[4] = q[1], v[2] = q[FB], v[6] = q[FB + 1];
-                    v[1] = q[FB * YB], v[5] = q[FB * YB + 1], v[3] = q[FB * YB + FB], v[7] = q[FB * YB + FB + 1];
+                    v[0] = sm_voxel(q), v[4] = sm_voxel(q + 1), v[2] = sm_voxel(q + FB), v[6] = sm_voxel(q + FB + 1);
+                    v[1] = sm_voxel(q + P), v[5] = sm_voxel(q + P + 1), v[3] = sm_voxel(q + P + FB),
+                    v[7] = sm_voxel(q + P + FB + 1);
                 }
             } else {
                 fp_corners<ZF ? 2 : 0, int>(src, st, c, v);
@@ -242,16 +250,17 @@ __device__ __forceinline__ void slab_ray_sum(const GeomDev &g, const CUtensorMap
 
 // k_fp_corr (GenerateImage_MT + the correction of ST_Tomography.cpp:667-676)
 // with slab-staged gathers.  map_x covers `vol` (x-fastest), map_z `vol_t`
-// (z-fastest), both with the box of BX.
-template <class BX, bool PK>
+// (z-fastest), both with the box of BX; T and B are the storages of the
+// volume and of the sinogram stack.
+template <class BX, bool PK, typename T = float, typename B = float>
 __global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, const ViewRec *__restrict__ views,
                                                       const __grid_constant__ CUtensorMap map_x,
                                                       const __grid_constant__ CUtensorMap map_z,
-                                                      const float *__restrict__ vol, const float *__restrict__ vol_t,
-                                                      const ViewSel sel, const float *__restrict__ b_stack,
+                                                      const T *__restrict__ vol, const T *__restrict__ vol_t,
+                                                      const ViewSel sel, const B *__restrict__ b_stack,
                                                       float *__restrict__ raylen_state, float *__restrict__ corr,
                                                       unsigned long long corr_surf, int *status) {
-    __shared__ alignas(128) float buf[2 * BX::N];
+    __shared__ alignas(128) T buf[2 * BX::N];
     __shared__ uint64_t bar[2];
     __shared__ int red[2][2 * WARPS];
     __shared__ int red_s[3 * WARPS];
@@ -271,11 +280,11 @@ __global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, co
     }
     Kahan acc{0.0f, 0.0f};
     if (vol_t && vr.layout == 1)
-        slab_ray_sum<true, BX, PK>(g, &map_z, vol_t, hit, r, buf, bar, red_s, red, &dead, status, acc);
+        slab_ray_sum<true, BX, PK, T>(g, &map_z, vol_t, hit, r, buf, bar, red_s, red, &dead, status, acc);
     else
-        slab_ray_sum<false, BX, PK>(g, &map_x, vol, hit, r, buf, bar, red_s, red, &dead, status, acc);
+        slab_ray_sum<false, BX, PK, T>(g, &map_x, vol, hit, r, buf, bar, red_s, red, &dead, status, acc);
     if (!valid) return;
-    const float *b = b_stack + (size_t)local * g.W * g.H;
+    const B *b = b_stack + (size_t)local * g.W * g.H;
     const size_t pix = i + (size_t)j * g.W;
     float L;
     if (hit) {
@@ -284,7 +293,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, co
     } else {
         L = raylen_state ? raylen_state[pix] : 0.0f;
     }
-    const float c = __fdiv_rn(__fsub_rn(__ldg(b + pix), acc.s), __fadd_rn(L, 1.0f));
+    const float c = __fdiv_rn(__fsub_rn(ld_voxel(b + pix), acc.s), __fadd_rn(L, 1.0f));
     corr[pix] = c;
     if (corr_surf) surf2DLayeredwrite(c, corr_surf, i * (int)sizeof(float), j, 0, cudaBoundaryModeZero);
 }
@@ -303,15 +312,19 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// A 3D FP32 tensor map (fast, mid, slow) over `ptr` with the slab box `box`.
-bool encode_box_map(CUtensorMap *m, const float *ptr, int fast, int mid, int slow, const cuuint32_t box[3]) {
+// A 3D tensor map (fast, mid, slow) over `ptr` with the slab box `box`:
+// FP32 elements, or 16-bit ones (BF16 bits, copied as they are).  The rows
+// must be whole multiples of 16 bytes (fast a multiple of 4 or 8 elements).
+bool encode_box_map(CUtensorMap *m, const void *ptr, size_t esize, int fast, int mid, int slow,
+                    const cuuint32_t box[3]) {
     const PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
-    if (!fn || !ptr || (reinterpret_cast<uintptr_t>(ptr) & 15) || (fast & 3)) return false;
+    if (!fn || !ptr || (reinterpret_cast<uintptr_t>(ptr) & 15) || ((size_t)fast * esize) % 16) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)fast, (cuuint64_t)mid, (cuuint64_t)slow};
-    const cuuint64_t strides[2] = {(cuuint64_t)fast * sizeof(float), (cuuint64_t)fast * mid * sizeof(float)};
+    const cuuint64_t strides[2] = {(cuuint64_t)fast * esize, (cuuint64_t)fast * mid * esize};
     const cuuint32_t estr[3] = {1, 1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(ptr), dims, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+    const CUtensorMapDataType dt = esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
+    return fn(m, dt, 3, const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -340,18 +353,18 @@ void box_dims(cuuint32_t box[3]) {
     box[2] = BX::SB;
 }
 
-template <class BX, bool PK>
-cudaError_t launch_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const float *vol,
-                        const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
+template <class BX, bool PK, typename T, typename B>
+cudaError_t launch_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const T *vol,
+                        const T *vol_t, const ViewSel &sel, const B *b_stack, float *raylen_state, float *corr,
                         cudaStream_t s, unsigned long long corr_surf, int *status) {
     static const bool carve = [] {
-        cudaFuncSetAttribute(k_fp_corr_slab<BX, PK>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        cudaFuncSetAttribute(k_fp_corr_slab<BX, PK, T, B>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared);
         cudaGetLastError();
         return true;
     }();
     (void)carve;
-    k_fp_corr_slab<BX, PK><<<dim3((g.W + 31) / 32, (g.H + WARPS - 1) / WARPS, 1), 32 * WARPS, 0, s>>>(
+    k_fp_corr_slab<BX, PK, T, B><<<dim3((g.W + 31) / 32, (g.H + WARPS - 1) / WARPS, 1), 32 * WARPS, 0, s>>>(
         g, views, m.x, m.z, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, status);
     return cudaGetLastError();
 }
@@ -365,7 +378,8 @@ const char *slab_variant_name(int v) {
     return v >= 0 && v < kSlabVariants ? names[v] : "?";
 }
 
-bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m, int variant) {
+static bool make_maps(const GeomDev &g, const void *vol, const void *vol_t, size_t esize, FpSlabMaps &m,
+                      int variant) {
     m = FpSlabMaps{};
     if ((long long)g.nx * g.ny * g.nz >= (1LL << 31)) return false;  // 32-bit fallback offsets
     if (variant < 0 || variant >= kSlabVariants) return false;
@@ -376,19 +390,47 @@ bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, F
     case 3: box_dims<Box3>(box); break;
     default: box_dims<Box0>(box); break;
     }
-    if (!encode_box_map(&m.x, vol, g.nx, g.ny, g.nz, box)) return false;
-    if (vol_t && !encode_box_map(&m.z, vol_t, g.nz, g.ny, g.nx, box)) return false;
+    if (!encode_box_map(&m.x, vol, esize, g.nx, g.ny, g.nz, box)) return false;
+    if (vol_t && !encode_box_map(&m.z, vol_t, esize, g.nz, g.ny, g.nx, box)) return false;
     m.ok = 1;
     m.has_z = vol_t != nullptr;
     m.variant = variant;
+    m.esize = (int)esize;
     return true;
+}
+
+bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m, int variant) {
+    return make_maps(g, vol, vol_t, sizeof(float), m, variant);
+}
+
+bool make_fp_slab_maps(const GeomDev &g, const unsigned short *vol, const unsigned short *vol_t, FpSlabMaps &m,
+                       int variant) {
+    return make_maps(g, vol, vol_t, sizeof(unsigned short), m, variant & 3);  // scalar boxes in BF16
+}
+
+cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const unsigned short *vol,
+                                const unsigned short *vol_t, const ViewSel &sel, const unsigned short *b_stack,
+                                float *raylen_state, float *corr, cudaStream_t s, unsigned long long corr_surf,
+                                int *status) {
+    if (!m.ok || m.esize != 2 || (vol_t && !m.has_z)) return cudaErrorInvalidValue;
+    typedef unsigned short U;
+#define STT_SLAB16(BOX) \
+    launch_slab<BOX, false, U, U>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status)
+    switch (m.variant & 3) {
+    case 1: return STT_SLAB16(Box1);
+    case 2: return STT_SLAB16(Box2);
+    case 3: return STT_SLAB16(Box3);
+    default: return STT_SLAB16(Box0);
+    }
+#undef STT_SLAB16
 }
 
 cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const float *vol,
                                 const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state,
                                 float *corr, cudaStream_t s, unsigned long long corr_surf, int *status) {
-    if (!m.ok || (vol_t && !m.has_z)) return cudaErrorInvalidValue;
-#define STT_SLAB(B, P) launch_slab<B, P>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, status)
+    if (!m.ok || m.esize != 4 || (vol_t && !m.has_z)) return cudaErrorInvalidValue;
+#define STT_SLAB(B, P) launch_slab<B, P, float, float>(g, views, m, vol, vol_t, sel, b_stack, raylen_state, corr, s, \
+                                                      corr_surf, status)
     switch (m.variant) {
     case 1: return STT_SLAB(Box1, false);
     case 2: return STT_SLAB(Box2, false);

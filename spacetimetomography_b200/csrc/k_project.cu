@@ -483,7 +483,7 @@ cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
                            cudaStream_t s, unsigned long long corr_surf, const FpSlabMaps *maps, int *status,
                            int fp_variant) {
-    const int skip = maps && maps->ok && (!vol_t || maps->has_z);
+    const int skip = maps && maps->ok && maps->esize == 4 && (!vol_t || maps->has_z);
     if (skip) {
         cudaError_t e = launch_fp_corr_slab(g, views, *maps, vol, vol_t, sel, b_stack, raylen_state, corr, s,
                                             corr_surf, status);
@@ -557,14 +557,21 @@ cudaError_t launch_correction(long long n, const unsigned short *b, const float 
 
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
                            const unsigned short *vol_t, const ViewSel &sel, const unsigned short *b_stack,
-                           float *raylen_state, float *corr, cudaStream_t s, unsigned long long corr_surf) {
+                           float *raylen_state, float *corr, cudaStream_t s, unsigned long long corr_surf,
+                           const FpSlabMaps *maps, int *status) {
     typedef unsigned short U;
+    const int skip = maps && maps->ok && maps->esize == 2 && (!vol_t || maps->has_z);
+    if (skip) {
+        cudaError_t e = launch_fp_corr_slab(g, views, *maps, vol, vol_t, sel, b_stack, raylen_state, corr, s,
+                                            corr_surf, status);
+        if (e != cudaSuccess) return e;
+    }
     if (small_volume(g))
         k_fp_corr<int, 32, 4, FP_GROUP, false, U, U><<<ray_grid(g, 1), 128, 0, s>>>(
-            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, 0);
+            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip);
     else
         k_fp_corr<long long, 32, 4, FP_GROUP, false, U, U><<<ray_grid(g, 1), 128, 0, s>>>(
-            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, 0);
+            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip);
     return cudaGetLastError();
 }
 

@@ -499,7 +499,7 @@ stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, f
 
 // The fused forward projection of one view of a sweep: FP32 through the tuned
 // gather variant and, where its maps apply, the slab-staged kernel; BF16
-// through the gather kernel.
+// through the gather kernel and the slab kernel's BF16 boxes.
 static cudaError_t sweep_fp_corr(stt_ctx *ctx, const float *vol, const float *volt, const stt::ViewSel &sel,
                                  const float *stack, float *rl, cudaStream_t s) {
     stt::FpSlabMaps maps;
@@ -510,7 +510,9 @@ static cudaError_t sweep_fp_corr(stt_ctx *ctx, const float *vol, const float *vo
 
 static cudaError_t sweep_fp_corr(stt_ctx *ctx, const unsigned short *vol, const unsigned short *volt,
                                  const stt::ViewSel &sel, const unsigned short *stack, float *rl, cudaStream_t s) {
-    return stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, stack, rl, ctx->corr, s);
+    stt::FpSlabMaps maps;
+    stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
+    return stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, stack, rl, ctx->corr, s, 0, &maps, ctx->status);
 }
 
 template <typename T>

@@ -57,8 +57,12 @@ cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, 
 struct FpSlabMaps {
     CUtensorMap x, z;
     int ok, has_z, variant;
+    int esize;  // bytes per voxel: 4 (FP32) or 2 (BF16)
 };
 bool make_fp_slab_maps(const GeomDev &g, const float *vol, const float *vol_t, FpSlabMaps &m, int variant = 0);
+// BF16 storage: the scalar boxes (variant & 3); x and z extents multiples of 8.
+bool make_fp_slab_maps(const GeomDev &g, const unsigned short *vol, const unsigned short *vol_t, FpSlabMaps &m,
+                       int variant = 0);
 // A 4D FP32 tensor map over nc planar volumes (x fastest, then y, z, plane)
 // with the given box (x, y, z, plane); false where TMA cannot address them
 // (nx not a multiple of 4, ptr not 16-byte aligned, box row not 16 bytes).
@@ -66,6 +70,10 @@ bool encode_planes_map(CUtensorMap *m, const float *ptr, int nx, int ny, int nz,
 cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m, const float *vol,
                                 const float *vol_t, const ViewSel &sel, const float *b_stack, float *raylen_state,
                                 float *corr, cudaStream_t s, unsigned long long corr_surf, int *status);
+cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const FpSlabMaps &m,
+                                const unsigned short *vol, const unsigned short *vol_t, const ViewSel &sel,
+                                const unsigned short *b_stack, float *raylen_state, float *corr, cudaStream_t s,
+                                unsigned long long corr_surf, int *status);
 // Forward projection of one view fused with the SART correction.  With usable
 // slab maps, staged views run in the slab-staged kernel and the others in the
 // gather kernel (both are launched; each leaves the other's views alone).
@@ -89,11 +97,13 @@ cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, co
 // stored values widened exactly to FP32, compute as their FP32 forms do, and
 // round what they store to nearest even.  Duals, flows, corrections and
 // accumulators stay FP32.
-// The fused forward projection of a BF16 volume against a BF16 sinogram: the
-// gather kernel for every view (no slab staging).
+// The fused forward projection of a BF16 volume against a BF16 sinogram:
+// with usable BF16 slab maps the staged views run in the slab kernel (BF16
+// boxes), the others in the gather kernel; without them every view gathers.
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
                            const unsigned short *vol_t, const ViewSel &sel, const unsigned short *b_stack,
-                           float *raylen_state, float *corr, cudaStream_t s, unsigned long long corr_surf = 0);
+                           float *raylen_state, float *corr, cudaStream_t s, unsigned long long corr_surf = 0,
+                           const FpSlabMaps *maps = nullptr, int *status = nullptr);
 cudaError_t launch_correction(long long n, const unsigned short *b, const float *ax, const float *raylen,
                               float *corr, cudaStream_t s);
 cudaError_t launch_correction(long long n, const float *b, const float *ax, const float *raylen,

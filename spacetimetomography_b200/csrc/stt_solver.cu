@@ -266,11 +266,12 @@ int fp_corr(stt_solver *s, int f, const float *vol, const float *volt, const stt
     return (maps && maps->ok) ? 2 : 1;  // slab-staged + gather kernels, or gather only
 }
 
-int fp_corr(stt_solver *s, int, const unsigned short *vol, const unsigned short *volt, const stt::ViewSel &sel,
+int fp_corr(stt_solver *s, int f, const unsigned short *vol, const unsigned short *volt, const stt::ViewSel &sel,
             const unsigned short *stack, float *rl, float *corr, cudaStream_t cs, unsigned long long surf,
             cudaError_t &e) {
-    e = stt::launch_fp_corr(*s->g, s->views, vol, volt, sel, stack, rl, corr, cs, surf);
-    return 1;
+    const stt::FpSlabMaps *maps = s->fpmaps.empty() ? nullptr : &s->fpmaps[f];
+    e = stt::launch_fp_corr(*s->g, s->views, vol, volt, sel, stack, rl, corr, cs, surf, maps, s->status);
+    return (maps && maps->ok) ? 2 : 1;
 }
 
 template <typename T>
@@ -518,11 +519,17 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
         stt_solver_destroy(s);
         return e;
     }
-    if (cfg->mode != STT_SOLVE_PLAIN && cfg->storage == STT_DTYPE_F32) {
+    if (cfg->mode != STT_SOLVE_PLAIN) {
         s->fpmaps.resize(F);
-        for (int f = 0; f < F; ++f)  // where the maps do not apply, ok stays 0 and every view gathers
-            stt::make_fp_slab_maps(*g, s->st.vol + f * s->n, static_cast<float *>(s->volt) + f * s->n, s->fpmaps[f],
-                                   ctx->tuning.slab);
+        for (int f = 0; f < F; ++f) {  // where the maps do not apply, ok stays 0 and every view gathers
+            if (cfg->storage == STT_DTYPE_F32)
+                stt::make_fp_slab_maps(*g, s->st.vol + f * s->n, static_cast<float *>(s->volt) + f * s->n,
+                                       s->fpmaps[f], ctx->tuning.slab);
+            else
+                stt::make_fp_slab_maps(*g, reinterpret_cast<const unsigned short *>(s->st.vol) + f * s->n,
+                                       static_cast<unsigned short *>(s->volt) + f * s->n, s->fpmaps[f],
+                                       ctx->tuning.slab);
+        }
     }
     if (cfg->mode != STT_SOLVE_PLAIN && cfg->bp_mode == 0) {
         s->corr_tex.resize(F);

@@ -166,17 +166,21 @@ def _bf16(t):
     return t.to(torch.bfloat16)
 
 
+# (40, 36, 44): nz is not a multiple of 8, so the BF16 sweep gathers every
+# view; (48, 40, 56): the BF16 slab maps apply and the oblique views go
+# through the slab-staged kernel's BF16 boxes
+@pytest.mark.parametrize("dims", [(40, 36, 44), (48, 40, 56)])
 @pytest.mark.parametrize("bp_mode", [0, 1])
-def test_bf16_sart_sweep_equals_rounded_fp32_views(cuda, bp_mode):
+def test_bf16_sart_sweep_equals_rounded_fp32_views(cuda, bp_mode, dims):
     """stt_sart_sweep_typed(BF16) against the FP32 sweep run one view at a time
     on the widened volume, rounded to BF16 after each view: the same bits with
-    voxel BP (gathers only), within a few rounding flips with ray BP (float
-    atomics)."""
+    voxel BP (the BF16 gather and slab projectors add what the FP32 ones do),
+    within a few rounding flips with ray BP (float atomics)."""
     import torch
 
     import spacetimetomography_b200 as stt
 
-    scan = ob.Scan((40, 36, 44), (64, 56), off=(0.4, -0.3, 0.2))
+    scan = ob.Scan(dims, (64, 56), off=(0.4, -0.3, 0.2))
     V = 9
     angles = np.linspace(0, 2 * np.pi, V, endpoint=False) + 0.2
     ctx = stt.Context(0)
