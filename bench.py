@@ -95,6 +95,8 @@ def parse_args():
                          "5: 512^3 PD TV) and print its own line")
     ap.add_argument("--bp-ray-probe", action="store_true",
                     help="with --config: only run a few ray-driven backprojections at the workload's size")
+    ap.add_argument("--iter-probe", action="store_true",
+                    help="only the headline solver's warm-up and one iteration in an NVTX range (for ncu's launch list)")
     ap.add_argument("--fp64-pd-check", action="store_true",
                     help="run only the full-size FP64 check of one 4D primal-dual iteration (two frames) and print it")
     ap.add_argument("--no-configs", action="store_true",
@@ -1277,6 +1279,36 @@ def run_stt(args):
     return 0
 
 
+def run_iter_probe(args) -> int:
+    """The headline workload's solver (tuned), one warm-up iteration, then one
+    iteration inside the NVTX range "pd_iteration" and nothing else: the
+    command whose launch list ncu records (--nvtx --nvtx-include
+    "pd_iteration/")."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    ctx, st, gmax, _ = build_problem(args, dev, 0)
+    stream = torch.cuda.Stream(device=dev)
+    s = stt.Solver(ctx, st, args.frames, args.views, pd_params(gmax), alpha=0.3, bp_mode=0 if args.bp == "voxel" else 1,
+                   seed=99, mode=stt.SOLVE_GRAPH, autotune=True)
+    with torch.cuda.stream(stream):
+        st["xbar"].copy_(st["vol"])
+    s.iterate(1, stream)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("pd_iteration")
+    s.iterate(1, stream)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    s.poll_status(stream)
+    print(json.dumps({"launches_per_iter": s.stats()[0], "tuning": ctx.get_tuning()}), flush=True)
+    s.close()
+    ctx.close()
+    return 0
+
+
 def run_flow_only(args):
     import torch
 
@@ -1449,6 +1481,8 @@ def main():
         return run_flow_only(args)
     if args.batch_only:
         return run_batch_only(args)
+    if args.iter_probe:
+        return run_iter_probe(args)
     if args.fp64_pd_check:
         import torch
 
