@@ -144,6 +144,8 @@ typedef struct stt_tuning {
     int ray_variant;  /* the ray-driven backprojection's scatter (kernel 3 of stt_tuning_variant_name);
                          untuned: the shared-memory slab box from 2^26 voxels on, else global atomics */
     float ray_us[2];
+    unsigned staged_bins_bf16;  /* staged_bins for a BF16-stored volume (stt_solve_cfg.storage,
+                                   stt_sart_sweep_typed): its gathers and boxes move half the bytes */
 } stt_tuning;
 stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream);
 stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out);

@@ -74,7 +74,7 @@ class Tuning(C.Structure):
     _fields_ = [("fp_variant", C.c_int), ("slab_variant", C.c_int), ("bp_variant", C.c_int),
                 ("staged_bins", C.c_uint), ("tuned", C.c_int), ("from_cache", C.c_int),
                 ("fp_us", C.c_float * 12), ("slab_us", C.c_float * 8), ("bp_us", C.c_float * 8),
-                ("ray_variant", C.c_int), ("ray_us", C.c_float * 2)]
+                ("ray_variant", C.c_int), ("ray_us", C.c_float * 2), ("staged_bins_bf16", C.c_uint)]
 
 
 def _load() -> C.CDLL:

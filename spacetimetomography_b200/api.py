@@ -174,7 +174,7 @@ class Context:
         return {"fp_variant": t.fp_variant, "slab_variant": t.slab_variant, "bp_variant": t.bp_variant,
                 "staged_bins": t.staged_bins, "tuned": bool(t.tuned), "from_cache": bool(t.from_cache),
                 "fp_us": list(t.fp_us)[:10], "slab_us": list(t.slab_us)[:8], "bp_us": list(t.bp_us)[:3],
-                "ray_variant": t.ray_variant, "ray_us": list(t.ray_us),
+                "ray_variant": t.ray_variant, "ray_us": list(t.ray_us), "staged_bins_bf16": t.staged_bins_bf16,
                 "ray": (lib.stt_tuning_variant_name(3, t.ray_variant) or b"").decode(),
                 "fp": (lib.stt_tuning_variant_name(0, t.fp_variant) or b"").decode(),
                 "slab": (lib.stt_tuning_variant_name(1, t.slab_variant) or b"").decode(),
@@ -191,12 +191,15 @@ class Context:
         self._chk(lib.stt_get_tuning(self._h, C.byref(t)))
         return self._tuning_dict(t)
 
-    def set_tuning(self, fp_variant=0, slab_variant=0, bp_variant=0, staged_bins=0x1E0, ray_variant=None):
-        """ray_variant None keeps the context's current ray-scatter choice."""
+    def set_tuning(self, fp_variant=0, slab_variant=0, bp_variant=0, staged_bins=0x1E0, ray_variant=None,
+                   staged_bins_bf16=None):
+        """ray_variant None keeps the context's current ray-scatter choice;
+        staged_bins_bf16 None takes staged_bins."""
         if ray_variant is None:
             ray_variant = self.get_tuning()["ray_variant"]
         t = Tuning(int(fp_variant), int(slab_variant), int(bp_variant), int(staged_bins), 1, 0)
         t.ray_variant = int(ray_variant)
+        t.staged_bins_bf16 = int(staged_bins if staged_bins_bf16 is None else staged_bins_bf16)
         self._chk(lib.stt_set_tuning(self._h, C.byref(t)))
 
     def fp_correction(self, vol, b, raylen_state, corr, view, stream=None):

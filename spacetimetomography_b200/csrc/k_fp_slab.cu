@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_fp_corr_slab(const GeomDev g, co
     int local;
     const int view = sel_view(sel, local);
     const ViewRec &vr = views[view];
-    if (!vr.staged) return;  // the gather kernel projects this view (uniform over the block)
+    if (!view_staged<T>(vr)) return;  // the gather kernel projects this view (uniform over the block)
     Ray r;
     bool hit = false;
     if (valid) {

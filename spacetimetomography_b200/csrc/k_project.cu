@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(32 * NW) k_fp_corr(const GeomDev g, const View
     const int view = sel_view(sel, local);
     const B *b = b_stack + (size_t)local * g.W * g.H;
     const ViewRec &vr = views[view];
-    if (skip_staged && vr.staged) return;  // the slab-staged kernel projects this view
+    if (skip_staged && view_staged<T>(vr)) return;  // the slab-staged kernel projects this view
     Ray r;
     make_ray(g, vr, i, j, r);
     const size_t pix = i + (size_t)j * g.W;

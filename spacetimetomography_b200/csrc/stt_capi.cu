@@ -91,7 +91,8 @@ void build_view(const stt_geometry &g, double theta, stt::ViewRec &v) {
     // gather from the z-fastest copy when the central ray runs more along x than z
     v.layout = std::fabs(s) > std::fabs(c) ? 1 : 0;
     v.staged = std::fmin(std::fabs(s), std::fabs(c)) > 0.4226 ? 1 : 0;  // sin 25 degrees
-    for (int k = 0; k < 2; ++k) v.pad[k] = 0.0f;
+    v.staged16 = v.staged;
+    v.pad = 0.0f;
 }
 
 template <typename T>
@@ -249,7 +250,7 @@ stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g) {
     ctx->geom = *g;
     ctx->geom.angles_rad = nullptr;
     ctx->tuning = stt::Tuning{};
-    ctx->staged_bins = 0x1E0u;
+    ctx->staged_bins = ctx->staged_bins16 = 0x1E0u;
     ctx->tuned = false;
     ctx->report = stt_tuning{};
     if (g->n_views > 0) {

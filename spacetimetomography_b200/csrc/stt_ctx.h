@@ -40,6 +40,7 @@ struct stt_ctx {
     // (0x1E0, 25-45 degrees, is the rule build_view applies by default).
     stt::Tuning tuning{};
     unsigned staged_bins = 0x1E0u;
+    unsigned staged_bins16 = 0x1E0u;  // the same for a BF16-stored volume (ViewRec::staged16)
     bool tuned = false;
     stt_tuning report{};
 };
@@ -50,6 +51,6 @@ inline int off_axis_bin(float deg) {
     int b = (int)(deg / 5.0f);
     return b < 0 ? 0 : (b > 8 ? 8 : b);
 }
-// Applies ctx->staged_bins to every view (host and device tables).
+// Applies ctx->staged_bins and staged_bins16 to every view (host and device tables).
 stt_status apply_staged_bins(stt_ctx *ctx);
 }  // namespace stt

@@ -26,7 +26,9 @@ namespace stt {
 // the oblique views (central ray more than 25 degrees off both x and z), whose
 // gathers spread over several planes per warp request: the forward projector
 // with the SART correction stages their volume slabs into shared memory
-// (k_fp_slab.cu) when it can.
+// (k_fp_slab.cu) when it can.  `staged16` is the same choice for a BF16-stored
+// volume (its gathers and boxes move half the bytes, so the faster projector
+// can differ; the autotuner sets both).
 struct ViewRec {
     double src[3];
     double det0[3];
@@ -36,8 +38,15 @@ struct ViewRec {
     float b[3];
     int layout;
     int staged;
-    float pad[2];
+    int staged16;
+    float pad;
 };
+
+// Whether a view goes to the slab-staged projector, for a volume stored as T.
+template <typename T>
+__device__ __forceinline__ bool view_staged(const ViewRec &v) {
+    return sizeof(T) == 2 ? v.staged16 != 0 : v.staged != 0;
+}
 
 struct GeomDev {
     int nx, ny, nz;

@@ -51,6 +51,7 @@ std::string shape_key(const stt_ctx *ctx) {
 struct Scratch {
     float *vol = nullptr, *volt = nullptr, *b = nullptr, *rl = nullptr, *corr = nullptr;
     float2 *acc = nullptr;
+    unsigned short *vol16 = nullptr, *volt16 = nullptr, *b16 = nullptr;  // BF16 copies for the BF16 choice
     stt::ViewRec *tv = nullptr;
     cudaArray_t arr = nullptr;
     cudaTextureObject_t tex = 0;
@@ -62,6 +63,9 @@ struct Scratch {
         cudaFree(rl);
         cudaFree(corr);
         cudaFree(acc);
+        cudaFree(vol16);
+        cudaFree(volt16);
+        cudaFree(b16);
         cudaFree(tv);
         if (tex) cudaDestroyTextureObject(tex);
         if (arr) cudaFreeArray(arr);
@@ -91,8 +95,11 @@ cudaError_t time_us(Scratch &sc, cudaStream_t s, Fn &&fn, float &us) {
 namespace stt {
 
 stt_status apply_staged_bins(stt_ctx *ctx) {
-    for (size_t v = 0; v < ctx->views_h.size(); ++v)
-        ctx->views_h[v].staged = ((ctx->staged_bins >> off_axis_bin(ctx->off_axis_deg[v])) & 1u) ? 1 : 0;
+    for (size_t v = 0; v < ctx->views_h.size(); ++v) {
+        const int b = off_axis_bin(ctx->off_axis_deg[v]);
+        ctx->views_h[v].staged = ((ctx->staged_bins >> b) & 1u) ? 1 : 0;
+        ctx->views_h[v].staged16 = ((ctx->staged_bins16 >> b) & 1u) ? 1 : 0;
+    }
     if (!ctx->views_h.empty() &&
         cudaMemcpy(ctx->views_d, ctx->views_h.data(), sizeof(ViewRec) * ctx->views_h.size(), cudaMemcpyHostToDevice) !=
             cudaSuccess) {
@@ -124,6 +131,7 @@ stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out) {
     out->bp_variant = ctx->tuning.bp;
     out->ray_variant = ctx->tuning.ray;
     out->staged_bins = ctx->staged_bins;
+    out->staged_bins_bf16 = ctx->staged_bins16;
     out->tuned = ctx->tuned ? 1 : 0;
     return STT_OK;
 }
@@ -133,7 +141,8 @@ stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t) {
     if (!ctx->has_geom) return STT_ERR_STATE;
     if (t->fp_variant < 0 || t->fp_variant >= stt::kFpVariants || t->slab_variant < 0 ||
         t->slab_variant >= stt::kSlabVariants || t->bp_variant < 0 || t->bp_variant >= stt::kBpVariants ||
-        t->ray_variant < 0 || t->ray_variant >= stt::kRayVariants || (t->staged_bins >> 9) != 0) {
+        t->ray_variant < 0 || t->ray_variant >= stt::kRayVariants || (t->staged_bins >> 9) != 0 ||
+        (t->staged_bins_bf16 >> 9) != 0) {
         ctx->err = "stt_set_tuning: a variant or staged_bins out of range";
         return STT_ERR_INVALID;
     }
@@ -147,6 +156,7 @@ stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t) {
     ctx->tuning.bp = t->bp_variant;
     ctx->tuning.ray = t->ray_variant;
     ctx->staged_bins = t->staged_bins;
+    ctx->staged_bins16 = t->staged_bins_bf16;
     ctx->tuned = true;
     ctx->report = *t;
     ctx->report.tuned = 1;
@@ -285,6 +295,47 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
         }
     } else {
         t.staged_bins = 0x1E0u;  // irrelevant: without slab maps every view gathers
+    }
+    // BF16 storage: the gather kernel against the slab kernel's BF16 box (the
+    // box just chosen) per class; a BF16 volume's gathers move half the bytes,
+    // so the faster projector can differ from the FP32 choice
+    t.staged_bins_bf16 = 0x1E0u;  // irrelevant where the BF16 maps do not apply
+    {
+        if ((e = cudaMalloc(&sc.vol16, n * sizeof(unsigned short))) ||
+            (e = cudaMalloc(&sc.volt16, n * sizeof(unsigned short))) ||
+            (e = cudaMalloc(&sc.b16, npix * sizeof(unsigned short))) ||
+            (e = cudaMemsetAsync(sc.vol16, 0x3F, n * sizeof(unsigned short), s)) ||  // 0x3F3F: about 0.75
+            (e = cudaMemsetAsync(sc.volt16, 0x3F, n * sizeof(unsigned short), s)) ||
+            (e = cudaMemsetAsync(sc.b16, 0, npix * sizeof(unsigned short), s)))
+            return fail(e, "BF16 scratch");
+        stt::FpSlabMaps m16;
+        if (stt::make_fp_slab_maps(g, sc.vol16, sc.volt16, m16, t.slab_variant)) {
+            t.staged_bins_bf16 = 0;
+            for (int b = 0; b < 9; ++b) {
+                if (rep[b] < 0) {
+                    t.staged_bins_bf16 |= 0x1E0u & (1u << b);
+                    continue;
+                }
+                stt::ViewRec two[2] = {ctx->views_h[rep[b]], ctx->views_h[rep[b]]};
+                two[0].staged16 = 0;
+                two[1].staged16 = 1;
+                if ((e = cudaMemcpyAsync(sc.tv, two, sizeof two, cudaMemcpyHostToDevice, s)) ||
+                    (e = cudaStreamSynchronize(s)))
+                    return fail(e, "view copy");
+                float tg16 = 0.0f, ts16 = 0.0f;
+                e = time_us(sc, s, [&] {
+                    return stt::launch_fp_corr(g, sc.tv, sc.vol16, sc.volt16, stt::ViewSel{0, nullptr, 0, 0}, sc.b16,
+                                               sc.rl, sc.corr, s, 0, nullptr, ctx->status);
+                }, tg16);
+                if (e) return fail(e, "BF16 gather projector");
+                e = time_us(sc, s, [&] {
+                    return stt::launch_fp_corr_slab(g, sc.tv, m16, sc.vol16, sc.volt16, stt::ViewSel{1, nullptr, 0, 1},
+                                                    sc.b16, sc.rl, sc.corr, s, 0, ctx->status);
+                }, ts16);
+                if (e) return fail(e, "BF16 slab projector");
+                if (ts16 < tg16) t.staged_bins_bf16 |= 1u << b;
+            }
+        }
     }
     // voxel backprojection: the column lengths on the views of the first and last classes present
     if ((e = cudaMemcpy2DToArrayAsync(sc.arr, 0, 0, sc.corr, g.W * sizeof(float), g.W * sizeof(float), g.H,

@@ -129,8 +129,8 @@ def test_tuning_variant_names_and_struct_layout(lib):
         assert lib.stt_tuning_variant_name(kernel, -1) is None
     assert lib.stt_tuning_variant_name(4, 0) is None
     # int fp, slab, bp; unsigned bins; int tuned, from_cache; float fp_us[12], slab_us[8], bp_us[8];
-    # int ray_variant; float ray_us[2]
-    assert C.sizeof(Tuning) == 6 * 4 + (12 + 8 + 8) * 4 + 4 + 2 * 4
+    # int ray_variant; float ray_us[2]; unsigned staged_bins_bf16
+    assert C.sizeof(Tuning) == 6 * 4 + (12 + 8 + 8) * 4 + 4 + 2 * 4 + 4
     assert Tuning.ray_variant.offset == 6 * 4 + 28 * 4
     assert SolveCfg.storage.offset > SolveCfg.autotune.offset and Instance.storage.offset > Instance.autotune.offset
 

@@ -120,6 +120,7 @@ def test_autotune_picks_a_valid_choice_and_caches_it(cuda):
     assert t["tuned"] and not t["from_cache"]
     assert 0 <= t["fp_variant"] < 10 and 0 <= t["slab_variant"] < 8 and 0 <= t["bp_variant"] < 3
     assert 0 <= t["ray_variant"] < 2
+    assert 0 <= t["staged_bins"] < 512 and 0 <= t["staged_bins_bf16"] < 512
     assert all(x > 0 for x in t["fp_us"]) and all(x > 0 for x in t["bp_us"]) and all(x > 0 for x in t["ray_us"])
     assert t["fp"] and t["slab"] and t["bp"] and t["ray"]
     assert ctx.get_tuning()["fp_variant"] == t["fp_variant"]
