@@ -316,6 +316,10 @@ static stt_status transposed_if_needed(stt_ctx *ctx, const unsigned short *vol, 
     return STT_OK;
 }
 
+// The staged-class mask for a volume of this storage (0: no view is staged).
+static unsigned staged_mask(const stt_ctx *ctx, const float *) { return ctx->staged_bins; }
+static unsigned staged_mask(const stt_ctx *ctx, const unsigned short *) { return ctx->staged_bins16; }
+
 extern "C" {
 
 static stt_status check_views(stt_ctx *ctx, int view0, int nviews) {
@@ -375,8 +379,8 @@ stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, flo
     const stt::ViewSel sel{view, nullptr, 0, view};
     const float *volt = nullptr;
     if ((st = transposed_if_needed(ctx, vol, view, 1, S(stream), &volt))) return st;
-    stt::FpSlabMaps maps;
-    stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
+    stt::FpSlabMaps maps{};  // ok = 0: every view gathers, one launch
+    if (staged_mask(ctx, vol)) stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
     STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, b, raylen_state, corr, S(stream), 0, &maps,
                                       ctx->status, ctx->tuning.fp),
              "k_fp_corr launch");
@@ -503,16 +507,16 @@ stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, f
 // through the gather kernel and the slab kernel's BF16 boxes.
 static cudaError_t sweep_fp_corr(stt_ctx *ctx, const float *vol, const float *volt, const stt::ViewSel &sel,
                                  const float *stack, float *rl, cudaStream_t s) {
-    stt::FpSlabMaps maps;
-    stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
+    stt::FpSlabMaps maps{};  // ok = 0: every view gathers, one launch
+    if (staged_mask(ctx, vol)) stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
     return stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, stack, rl, ctx->corr, s, 0, &maps, ctx->status,
                                ctx->tuning.fp);
 }
 
 static cudaError_t sweep_fp_corr(stt_ctx *ctx, const unsigned short *vol, const unsigned short *volt,
                                  const stt::ViewSel &sel, const unsigned short *stack, float *rl, cudaStream_t s) {
-    stt::FpSlabMaps maps;
-    stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
+    stt::FpSlabMaps maps{};  // ok = 0: every view gathers, one launch
+    if (staged_mask(ctx, vol)) stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
     return stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, stack, rl, ctx->corr, s, 0, &maps, ctx->status);
 }
 

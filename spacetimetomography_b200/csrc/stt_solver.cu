@@ -519,7 +519,10 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
         stt_solver_destroy(s);
         return e;
     }
-    if (cfg->mode != STT_SOLVE_PLAIN) {
+    // no views staged for this storage (the tuner found one gather launch per
+    // view faster than the two kernels): no maps, one launch per view
+    const bool any_staged = (cfg->storage == STT_DTYPE_F32 ? ctx->staged_bins : ctx->staged_bins16) != 0;
+    if (cfg->mode != STT_SOLVE_PLAIN && any_staged) {
         s->fpmaps.resize(F);
         for (int f = 0; f < F; ++f) {  // where the maps do not apply, ok stays 0 and every view gathers
             if (cfg->storage == STT_DTYPE_F32)

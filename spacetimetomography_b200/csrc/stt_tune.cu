@@ -232,6 +232,7 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
         ++count[b];
     }
     float tg[stt::kFpVariants][9] = {}, ts[stt::kSlabVariants][9] = {};
+    float t_idle = 0.0f;  // a slab launch on a view it does not project (returns at once)
     stt::FpSlabMaps maps[stt::kSlabVariants];
     bool maps_ok[stt::kSlabVariants] = {};
     bool slab_ok = false;
@@ -251,6 +252,15 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
                                            ctx->status, fv);
             }, tg[fv][b]);
             if (e) return fail(e, "gather projector");
+        }
+        if (slab_ok && t_idle == 0.0f) {
+            int sv0 = 0;
+            while (!maps_ok[sv0]) ++sv0;
+            e = time_us(sc, s, [&] {
+                return stt::launch_fp_corr_slab(g, sc.tv, maps[sv0], sc.vol, sc.volt, gather_sel, sc.b, sc.rl, sc.corr,
+                                                s, 0, ctx->status);
+            }, t_idle);
+            if (e) return fail(e, "idle slab launch");
         }
         for (int sv = 0; sv < stt::kSlabVariants; ++sv) {
             if (!maps_ok[sv]) continue;
@@ -293,6 +303,17 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
                 t.staged_bins |= 0x1E0u & (1u << b);  // a class without views keeps the default rule
             }
         }
+        // With any view staged, every view launches both kernels and the one
+        // with nothing to do costs an idle launch; gathering every view is one
+        // launch.  Keep the split only where it wins with that cost counted.
+        double split = 0.0, gather_all = 0.0;
+        for (int b = 0; b < 9; ++b) {
+            if (rep[b] < 0) continue;
+            const double own = ((t.staged_bins >> b) & 1u) ? ts[t.slab_variant][b] : tg[t.fp_variant][b];
+            split += (double)count[b] * (own + t_idle);
+            gather_all += (double)count[b] * tg[t.fp_variant][b];
+        }
+        if (split >= gather_all) t.staged_bins = 0;
     } else {
         t.staged_bins = 0x1E0u;  // irrelevant: without slab maps every view gathers
     }
@@ -311,6 +332,8 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
         stt::FpSlabMaps m16;
         if (stt::make_fp_slab_maps(g, sc.vol16, sc.volt16, m16, t.slab_variant)) {
             t.staged_bins_bf16 = 0;
+            double split = 0.0, gather_all = 0.0;
+            float t_idle16 = 0.0f;
             for (int b = 0; b < 9; ++b) {
                 if (rep[b] < 0) {
                     t.staged_bins_bf16 |= 0x1E0u & (1u << b);
@@ -333,8 +356,19 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
                                                     sc.b16, sc.rl, sc.corr, s, 0, ctx->status);
                 }, ts16);
                 if (e) return fail(e, "BF16 slab projector");
+                if (t_idle16 == 0.0f) {
+                    e = time_us(sc, s, [&] {
+                        return stt::launch_fp_corr_slab(g, sc.tv, m16, sc.vol16, sc.volt16,
+                                                        stt::ViewSel{0, nullptr, 0, 0}, sc.b16, sc.rl, sc.corr, s, 0,
+                                                        ctx->status);
+                    }, t_idle16);
+                    if (e) return fail(e, "idle BF16 slab launch");
+                }
                 if (ts16 < tg16) t.staged_bins_bf16 |= 1u << b;
+                split += (double)count[b] * (std::fmin(ts16, tg16) + t_idle16);
+                gather_all += (double)count[b] * tg16;
             }
+            if (split >= gather_all) t.staged_bins_bf16 = 0;  // (as for FP32 above)
         }
     }
     // voxel backprojection: the column lengths on the views of the first and last classes present
