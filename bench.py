@@ -93,6 +93,8 @@ def parse_args():
     ap.add_argument("--config", type=int, choices=sorted(CONFIG_SPECS), default=None,
                     help="run only the single-frame workload of that number (1: 128^3 SART, 2: 256^3 PD TV, "
                          "5: 512^3 PD TV) and print its own line")
+    ap.add_argument("--tuned", action="store_true",
+                    help="with --fp-probe: autotune first, projections inside the NVTX range fp_probe")
     ap.add_argument("--bp-ray-probe", action="store_true",
                     help="with --config: only run a few ray-driven backprojections at the workload's size")
     ap.add_argument("--iter-probe", action="store_true",
@@ -911,9 +913,11 @@ def config_bench(cid, args, dev, stream, rank=0, full=False) -> dict:
     return out
 
 
-def fp_probe(cid, dev, stream) -> None:
+def fp_probe(cid, dev, stream, tuned=False) -> None:
     """A few fused forward projections at the workload's size and nothing else
-    (the command ncu captures for the roofline's traffic at that size)."""
+    (the command ncu captures for the roofline's traffic at that size).  With
+    `tuned` the context is autotuned first and the projections run inside the
+    NVTX range "fp_probe" (so that a capture can skip the tuner's launches)."""
     import torch
 
     import spacetimetomography_b200 as stt
@@ -928,9 +932,15 @@ def fp_probe(cid, dev, stream) -> None:
     b = torch.zeros((D, D), device=dev)
     rl = torch.zeros((D, D), device=dev)
     corr = torch.zeros((D, D), device=dev)
+    if tuned:
+        ctx.autotune(stream)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("fp_probe")
     for v in (0, V // 8, V // 4, 3 * V // 8):  # 0, 45, 90, 135 degrees
         ctx.fp_correction(vol, b, rl, corr, v, stream=stream)
     torch.cuda.synchronize()
+    if tuned:
+        torch.cuda.nvtx.range_pop()
     ctx.poll_status(stream)
     ctx.close()
 
@@ -968,7 +978,7 @@ def run_config_only(args) -> int:
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(device=dev)
     if args.fp_probe:
-        fp_probe(args.config, dev, stream)
+        fp_probe(args.config, dev, stream, tuned=args.tuned)
         return 0
     if args.bp_ray_probe:
         bp_ray_probe(args.config, dev, stream)
