@@ -1370,10 +1370,13 @@ def run_batch_only(args):
     stream = torch.cuda.Stream(device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
+    staging = {}
+
     def batched_time():
         for d in inst:
             d["vol"].zero_()
         b = stt.Batch(inst, mode=stt.SOLVE_GRAPH)
+        staging["f32"] = b.staging()
         for _ in range(args.warmup):
             b.iterate(1, stream)
         torch.cuda.synchronize()
@@ -1388,6 +1391,8 @@ def run_batch_only(args):
     t_default = batched_time()  # the default launch choices
     t0 = time.perf_counter()
     choices = [d["ctx"].autotune(stream) for d in inst]  # every instance's own geometry
+    for d in inst:
+        d["autotune"] = True  # the batch then also chooses its projector split as a whole (stt_batch_staging)
     t_tune = time.perf_counter() - t0
     t_batch = batched_time()
     f32_result = [d["vol"].clone() for d in inst]
@@ -1398,6 +1403,7 @@ def run_batch_only(args):
     for d in inst16:
         d.pop("truth")
     b16 = stt.Batch(inst16, mode=stt.SOLVE_GRAPH)
+    staging["bf16"] = b16.staging()
     for _ in range(args.warmup):
         b16.iterate(1, stream)
     torch.cuda.synchronize()
@@ -1413,6 +1419,11 @@ def run_batch_only(args):
     bf16_vs_f32 = math.sqrt(num / den)
     bf16_err = [float((d["vol"].float() - o["truth"]).norm() / o["truth"].norm()) for d, o in zip(inst16[:4], inst)]
     del inst16
+    # the instances' own tuned choices again (the batches may have set their
+    # staged masks to 0), for the one-after-another forms below
+    for d, c in zip(inst, choices):
+        d["ctx"].set_tuning(c["fp_variant"], c["slab_variant"], c["bp_variant"], staged_bins=c["staged_bins"],
+                            ray_variant=c["ray_variant"], staged_bins_bf16=c["staged_bins_bf16"])
     # the same instances one after another (each its own graph-captured solver)
     solvers = []
     for d in inst:
@@ -1469,6 +1480,7 @@ def run_batch_only(args):
             "autotune": {"batched_ms_per_iter_default_choices": 1000 * t_default,
                          "batched_ms_per_iter_tuned": 1000 * t_batch, "tuned_vs_default": t_default / t_batch,
                          "tuning_s_all_instances": t_tune,
+                         "batch_staging": staging,
                          "cache_hits": sum(c["from_cache"] for c in choices),
                          "fp_variant_counts": np.bincount([c["fp_variant"] for c in choices], minlength=10).tolist(),
                          "slab_variant_counts": np.bincount([c["slab_variant"] for c in choices], minlength=8).tolist(),

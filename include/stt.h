@@ -525,8 +525,20 @@ typedef struct stt_instance {
                              stt_solve_cfg.storage */
 } stt_instance;
 
+/* When any instance asks for autotuning, stt_batch_create also chooses, for
+ * the batch as a whole, between the instances' tuned split of the views
+ * between the two forward projectors and every view gathering: it times one
+ * batched iteration each way (results not written to the instances' vol),
+ * keeps the faster (when it is the gather, each instance's context keeps a
+ * staged mask of 0 for its storage: stt_get_tuning shows it), and starts the
+ * solve from the untouched start volumes with fresh solvers.  Instances tuned alone on an idle GPU favour the
+ * slab-staged projector, whose shared memory limits how many of the other
+ * instances' blocks run beside it.  stt_batch_staging reports the choice: timed
+ * (0 when no instance asked for tuning or no view was staged), all_gather, and
+ * the two iteration times in ms (any pointer may be NULL). */
 typedef struct stt_batch stt_batch;
 stt_status stt_batch_create(const stt_instance *instances, int n, int mode, stt_batch **out);
+stt_status stt_batch_staging(const stt_batch *b, int *timed, int *all_gather, float *ms_split, float *ms_gather);
 stt_status stt_batch_iterate(stt_batch *b, int n_iters, void *stream);
 const char *stt_batch_last_error(const stt_batch *b);
 /* See stt_poll_status: polls every instance's solver. */

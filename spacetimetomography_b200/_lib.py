@@ -121,6 +121,7 @@ def _load() -> C.CDLL:
         "stt_batch_create": [vp, i, i, C.POINTER(vp)],
         "stt_batch_iterate": [vp, i, vp],
         "stt_batch_destroy": [vp],
+        "stt_batch_staging": [vp, vp, vp, vp, vp],
         "stt_ctx_dims": [vp, vp],
         "stt_warp_box": [vp, vp, vp, vp, i, f, vp, vp],
         "stt_image_gradient": [vp, vp, vp, vp],

@@ -553,6 +553,15 @@ class Batch:
             raise STTError(rc, (lib.stt_last_error(None) or b"batch create failed").decode())
         self._h = h
 
+    def staging(self) -> dict:
+        """stt_batch_staging: the batch-level choice between the instances'
+        tuned projector split and every view gathering."""
+        timed, gather = C.c_int(), C.c_int()
+        ms_split, ms_gather = C.c_float(), C.c_float()
+        check(lib.stt_batch_staging(self._h, C.byref(timed), C.byref(gather), C.byref(ms_split), C.byref(ms_gather)))
+        return {"timed": bool(timed.value), "all_gather": bool(gather.value), "ms_split": ms_split.value,
+                "ms_gather": ms_gather.value}
+
     def iterate(self, n: int = 1, stream=None):
         rc = lib.stt_batch_iterate(self._h, int(n), _stream(stream))
         if rc != 0:

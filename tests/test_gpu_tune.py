@@ -169,3 +169,45 @@ def test_both_ray_backprojection_scatters_agree(cuda):
     with pytest.raises(stt.STTError):
         ctx.set_tuning(0, 0, 0, ray_variant=2)
     ctx.close()
+
+
+def test_batch_staging_choice_leaves_the_solve_unchanged(cuda):
+    """A batch whose instances ask for tuning times its projector split both
+    ways at creation (stt_batch_staging) without touching the callers' start
+    volumes: after two iterations its volumes equal those of an untuned batch
+    of the same instances bit for bit (voxel BP; every projector and
+    backprojection variant gives the same bits)."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200 import phantom as ph
+
+    shapes = [((48, 40, 48), (72, 64), 14), ((64, 48, 56), (96, 72), 11), ((40, 40, 40), (64, 64), 9)]
+    cut = (2, 2, 2, 2, 2, 2, 3, 3)
+    runs = []
+    for tuned in (False, True):
+        items = []
+        for k, (dims, det, nv) in enumerate(shapes):
+            ctx = stt.Context(0)
+            ctx.set_geometry(dims, (1.0, 1.0, 1.0), det, 1.0, 600.0, 1000.0,
+                             np.linspace(0, 2 * math.pi, nv, endpoint=False) + 0.2)
+            truth = ph.ellipsoid_phantom(dims, 5, seed=20 + k, semi=(3.0, 10.0)).to(cuda)
+            proj = torch.zeros((nv, det[1], det[0]), device=cuda)
+            ctx.fp(truth, proj)
+            pd = stt.PdParams(tv_w=0.02, tp_w=0.0, bc_w=0.0, huber_factor=0.9, gmax=float(proj.max()) / 4, cut=cut)
+            items.append(dict(ctx=ctx, vol=(truth * 0.5).contiguous(), proj=proj, pd=pd, roi_cut=cut, seed=7 + k,
+                              autotune=tuned))
+        b = stt.Batch(items, mode=stt.SOLVE_GRAPH)
+        info = b.staging()
+        assert set(info) == {"timed", "all_gather", "ms_split", "ms_gather"}
+        if tuned and info["timed"]:
+            assert info["ms_split"] > 0 and info["ms_gather"] > 0
+        b.iterate(2)
+        torch.cuda.synchronize()
+        b.poll_status()
+        b.close()
+        runs.append([d["vol"].cpu().numpy() for d in items])
+        for d in items:
+            d["ctx"].close()
+    for a, c in zip(*runs):
+        np.testing.assert_array_equal(a, c)
