@@ -11,8 +11,9 @@
 //   * the voxel backprojection's column length (bp_variant_name).
 // Every variant of a kernel gives the same bits, so the choice changes only
 // the time.  One representative view per class is timed with CUDA events
-// (one warm-up launch, then the mean of three); classes are weighted by their
-// number of views.  Choices are cached per device and geometry shape.
+// (one warm-up launch, then the fastest of three rounds of three); classes
+// are weighted by their number of views.  Choices are cached per device and
+// geometry shape.
 //
 // The loops these launches tile are the reference's row loop of the projector
 // (S/ImageFormationModel/TypicalRayProducer.core.h:168) and voxel loop of the
@@ -74,20 +75,26 @@ struct Scratch {
     }
 };
 
-// Mean microseconds of fn() over 3 launches after one warm-up launch.
+// Microseconds of one launch of fn(): after one warm-up launch, the fastest of
+// three rounds of three launches (the least disturbed round: choices between
+// variants a few percent apart must not follow the noise).
 template <typename Fn>
 cudaError_t time_us(Scratch &sc, cudaStream_t s, Fn &&fn, float &us) {
     cudaError_t e = fn();
     if (e != cudaSuccess) return e;
-    if ((e = cudaEventRecord(sc.e0, s)) != cudaSuccess) return e;
-    for (int r = 0; r < 3; ++r)
-        if ((e = fn()) != cudaSuccess) return e;
-    if ((e = cudaEventRecord(sc.e1, s)) != cudaSuccess) return e;
-    if ((e = cudaEventSynchronize(sc.e1)) != cudaSuccess) return e;
-    float ms = 0.0f;
-    e = cudaEventElapsedTime(&ms, sc.e0, sc.e1);
-    us = 1000.0f * ms / 3.0f;
-    return e;
+    float best = 3.0e38f;
+    for (int round = 0; round < 3; ++round) {
+        if ((e = cudaEventRecord(sc.e0, s)) != cudaSuccess) return e;
+        for (int r = 0; r < 3; ++r)
+            if ((e = fn()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(sc.e1, s)) != cudaSuccess) return e;
+        if ((e = cudaEventSynchronize(sc.e1)) != cudaSuccess) return e;
+        float ms = 0.0f;
+        if ((e = cudaEventElapsedTime(&ms, sc.e0, sc.e1)) != cudaSuccess) return e;
+        best = ms < best ? ms : best;
+    }
+    us = 1000.0f * best / 3.0f;
+    return cudaSuccess;
 }
 
 }  // namespace
