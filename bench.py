@@ -95,6 +95,11 @@ def parse_args():
                          "5: 512^3 PD TV) and print its own line")
     ap.add_argument("--tuned", action="store_true",
                     help="with --fp-probe: autotune first, projections inside the NVTX range fp_probe")
+    ap.add_argument("--tuning", default=None,
+                    help="with --fp-probe --tuned or --iter-probe: launch choices (a JSON object or key=value,... "
+                         "with the keys of the printed tuning: fp_variant, slab_variant, bp_variant, staged_bins, "
+                         "ray_variant, staged_bins_bf16) set instead of autotuning, so that a run under ncu, whose "
+                         "interception gaps fall inside the tuner's event timings, makes the choices of a plain run")
     ap.add_argument("--bp-ray-probe", action="store_true",
                     help="with --config: only run a few ray-driven backprojections at the workload's size")
     ap.add_argument("--iter-probe", action="store_true",
@@ -588,6 +593,32 @@ def _timed(stream, fn, reps: int) -> float:
     return e0.elapsed_time(e1) / 1000.0 / max(reps, 1)
 
 
+def gather_ceilings(ctx, vol, views, D, dev, stream) -> dict:
+    """The gather ceiling (stt_gather_ceiling) over `views`, in both corner
+    fetches: eight loads per sample, and two tld4 texture gathers (where the
+    textures bind).  Samples per view and Gsamples/s of each, and which fetch
+    the tuned projector uses."""
+    import torch
+
+    gimg = torch.empty((D, D), device=dev)
+    gcount = torch.zeros((D, D), dtype=torch.int32, device=dev)
+    out = {}
+    forms = [("loads", False)] + ([("tld4", True)] if ctx.fp_texture_ok(vol) else [])
+    for name, tex in forms:
+        gsamples = 0
+        for v in views:
+            ctx.gather_ceiling(vol, v, gimg, gcount, stream=stream, texture=tex)
+            torch.cuda.synchronize()
+            gsamples += int(gcount.sum().item())
+        it = iter(list(views) * 2)
+        t = _timed(stream, lambda: (lambda v: ctx.gather_ceiling(vol, v, gimg, stream=stream, texture=tex))(next(it)),
+                   len(views))
+        out[name] = {"gsamples_per_s": gsamples / len(views) / t / 1e9, "s_per_view": t,
+                     "samples_per_view": gsamples / len(views)}
+    out["projector_fetch"] = "tld4" if ctx.get_tuning()["fp_variant"] in (10, 11) and "tld4" in out else "loads"
+    return out
+
+
 def _pd_state(N, proj, dev, storage="f32"):
     """A one-frame solver state; storage "bf16": the primal volumes and the
     sinogram in torch.bfloat16 (stt_solve_cfg.storage)."""
@@ -686,17 +717,10 @@ def fp_bp_split(ctx, c, vol, proj, gmax, dev, stream) -> dict:
     torch.cuda.synchronize()
     samples = float(w.sum().item()) / 4
     # the gather ceiling over the same views: the projector's gathers and
-    # interpolation alone (stt_gather_ceiling), its own samples counted
-    gimg = torch.empty((D, D), device=dev)
-    gcount = torch.zeros((D, D), dtype=torch.int32, device=dev)
-    gsamples = 0
-    for v in views:
-        ctx.gather_ceiling(vol, v, gimg, gcount, stream=stream)
-        torch.cuda.synchronize()
-        gsamples += int(gcount.sum().item())
-    it = iter(views * 2)
-    t_gc = _timed(stream, lambda: (lambda v: ctx.gather_ceiling(vol, v, gimg, stream=stream))(next(it)), nv)
-    ceiling = gsamples / len(views) / t_gc / 1e9
+    # interpolation alone (stt_gather_ceiling), its own samples counted, in
+    # the corner fetch the tuned projector uses
+    gc = gather_ceilings(ctx, vol, views, D, dev, stream)
+    ceiling = gc[gc["projector_fetch"]]["gsamples_per_s"]
     ctx.poll_status(stream)
     del scratch
     peak, peak_kind = peaks()
@@ -708,11 +732,10 @@ def fp_bp_split(ctx, c, vol, proj, gmax, dev, stream) -> dict:
     return {"views_timed": nv, "fp_s_per_view": t_fp, "bp_voxel_s_per_view": t_bpv, "bp_ray_s_per_view": t_bpr,
             "fp_gups": N ** 3 / t_fp / 1e9, "bp_voxel_gups": N ** 3 / t_bpv / 1e9, "bp_ray_gups": N ** 3 / t_bpr / 1e9,
             "samples_per_view": samples, "fp_gsamples_per_s": samples / t_fp / 1e9,
-            "gather_ceiling": {"gsamples_per_s": ceiling, "s_per_view": t_gc,
-                               "samples_per_view": gsamples / len(views),
-                               "fp_frac": samples / t_fp / 1e9 / ceiling,
-                               "kernel": "k_gather_ceiling (stt_gather_ceiling): the projector's cell, 8 gathers "
-                                         "and trilinear interpolation per sample, packed pairs, no march control"},
+            "gather_ceiling": {**gc, "fp_frac": samples / t_fp / 1e9 / ceiling,
+                               "kernel": "k_gather_ceiling (stt_gather_ceiling): the projector's cell, its 8 corners "
+                                         "(8 loads, or 2 tld4 gathers) and trilinear interpolation per sample, packed "
+                                         "pairs, no march control; fp_frac against the projector's own fetch"},
             "roofline": {"bound": "hbm", "kernel": "k_fp_corr / k_fp_corr_slab (forward projection + correction)",
                          "achieved": fp_bytes / t_fp / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": fp_bytes / t_fp / 1e9 / peak, "peak_source": peak_kind,
@@ -913,11 +936,30 @@ def config_bench(cid, args, dev, stream, rank=0, full=False) -> dict:
     return out
 
 
-def fp_probe(cid, dev, stream, tuned=False) -> None:
+_TUNING_KEYS = ("fp_variant", "slab_variant", "bp_variant", "staged_bins", "ray_variant", "staged_bins_bf16")
+
+
+def tune_or_set(ctx, stream, tuning_json) -> dict:
+    """Autotunes the context, or sets the choices a JSON object names."""
+    if tuning_json is None:
+        return ctx.autotune(stream)
+    if tuning_json.lstrip().startswith("{"):
+        t = json.loads(tuning_json)
+    else:  # key=value,key=value
+        t = dict(kv.split("=", 1) for kv in tuning_json.split(",") if kv)
+    unknown = set(t) - set(_TUNING_KEYS)
+    if unknown:
+        raise SystemExit(f"--tuning: unknown keys {sorted(unknown)}")
+    ctx.set_tuning(**{k: int(t[k]) for k in _TUNING_KEYS if k in t})
+    return ctx.get_tuning()
+
+
+def fp_probe(cid, dev, stream, tuned=False, tuning=None) -> None:
     """A few fused forward projections at the workload's size and nothing else
     (the command ncu captures for the roofline's traffic at that size).  With
-    `tuned` the context is autotuned first and the projections run inside the
-    NVTX range "fp_probe" (so that a capture can skip the tuner's launches)."""
+    `tuned` the context is autotuned first (or given the choices `tuning`
+    names) and the projections run inside the NVTX range "fp_probe" (so that a
+    capture can skip the tuner's launches)."""
     import torch
 
     import spacetimetomography_b200 as stt
@@ -933,7 +975,7 @@ def fp_probe(cid, dev, stream, tuned=False) -> None:
     rl = torch.zeros((D, D), device=dev)
     corr = torch.zeros((D, D), device=dev)
     if tuned:
-        ctx.autotune(stream)
+        print(json.dumps({"tuning": tune_or_set(ctx, stream, tuning)}), flush=True)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("fp_probe")
     for v in (0, V // 8, V // 4, 3 * V // 8):  # 0, 45, 90, 135 degrees
@@ -978,7 +1020,7 @@ def run_config_only(args) -> int:
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(device=dev)
     if args.fp_probe:
-        fp_probe(args.config, dev, stream, tuned=args.tuned)
+        fp_probe(args.config, dev, stream, tuned=args.tuned, tuning=args.tuning)
         return 0
     if args.bp_ray_probe:
         bp_ray_probe(args.config, dev, stream)
@@ -1125,26 +1167,19 @@ def run_stt(args):
     # samples per view and the gather ceiling over the same frame's views
     w = torch.zeros((1, args.det, args.det), device=dev)
     img = torch.zeros((1, args.det, args.det), device=dev)
-    gimg = torch.empty((args.det, args.det), device=dev)
-    gcount = torch.zeros((args.det, args.det), dtype=torch.int32, device=dev)
-    samples = gsamples = 0.0
+    samples = 0.0
     for v in range(V):
         ctx.fp(vol0, img, view0=v, nviews=1, weight=w, stream=stream)
-        ctx.gather_ceiling(vol0, v, gimg, gcount, stream=stream)
         torch.cuda.synchronize()
         samples += float(w.sum().item())
-        gsamples += float(gcount.sum().item())
-    e2.record(stream)
-    for v in range(V):
-        ctx.gather_ceiling(vol0, v, gimg, stream=stream)
-    e3.record(stream)
-    torch.cuda.synchronize()
-    t_gc = e2.elapsed_time(e3) / 1000.0 / V
+    gc = gather_ceilings(ctx, vol0, range(V), args.det, dev, stream)
+    ceil = gc[gc["projector_fetch"]]["gsamples_per_s"]
     fp_samples = {"fp_s_per_view": t_fp, "samples_per_view": samples / V, "fp_gsamples_per_s": samples / V / t_fp / 1e9,
-                  "gather_ceiling_gsamples_per_s": gsamples / V / t_gc / 1e9,
-                  "fp_frac_of_gather_ceiling": (samples / V / t_fp) / (gsamples / V / t_gc),
+                  "gather_ceiling_gsamples_per_s": ceil, "gather_ceilings": gc,
+                  "fp_frac_of_gather_ceiling": (samples / V / t_fp / 1e9) / ceil,
                   "views": f"the {V} views of frame 0, FP fused with the correction (stt_fp_correction, transposes "
-                           "included); the gather ceiling is stt_gather_ceiling on the same views"}
+                           "included); the gather ceiling is stt_gather_ceiling on the same views, in the corner "
+                           "fetch the tuned projector uses (projector_fetch)"}
 
     # ---- the per-view GPU form ----
     plain = None
@@ -1290,7 +1325,8 @@ def run_stt(args):
 
 
 def run_iter_probe(args) -> int:
-    """The headline workload's solver (tuned), one warm-up iteration, then one
+    """The headline workload's solver (tuned, or with the choices --tuning
+    names), one warm-up iteration, then one
     iteration inside the NVTX range "pd_iteration" and nothing else: the
     command whose launch list ncu records (--nvtx --nvtx-include
     "pd_iteration/")."""
@@ -1302,8 +1338,10 @@ def run_iter_probe(args) -> int:
     dev = torch.device("cuda", 0)
     ctx, st, gmax, _ = build_problem(args, dev, 0)
     stream = torch.cuda.Stream(device=dev)
+    if args.tuning is not None:
+        tune_or_set(ctx, stream, args.tuning)
     s = stt.Solver(ctx, st, args.frames, args.views, pd_params(gmax), alpha=0.3, bp_mode=0 if args.bp == "voxel" else 1,
-                   seed=99, mode=stt.SOLVE_GRAPH, autotune=True)
+                   seed=99, mode=stt.SOLVE_GRAPH, autotune=args.tuning is None)
     with torch.cuda.stream(stream):
         st["xbar"].copy_(st["vol"])
     s.iterate(1, stream)

@@ -117,6 +117,11 @@ stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g);
  * (stt_fp_correction, stt_sart_sweep, the solver) and the solver's voxel
  * backprojection come in launch variants that give the same bits:
  *   fp_variant   the gather projector's detector tile and samples in flight;
+ *                variants 10 and 11 fetch a sample's 8 corners as two tld4
+ *                gathers of the FP32 volume bound as a pitch-linear 2D texture
+ *                (the context keeps one texture object per array it is given,
+ *                until stt_destroy; where the device's texture limits do not
+ *                admit the array, the load-based variant of the same shape runs);
  *   slab_variant the box the slab-staged projector stages with TMA;
  *   bp_variant   the column length of the voxel backprojection (solver);
  *   staged_bins  bit b set: views whose central ray is 5b to 5b+5 degrees off
@@ -150,6 +155,11 @@ typedef struct stt_tuning {
 stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream);
 stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out);
 stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t);
+/* Whether the tld4 gather variants (fp_variant 10, 11) bind `vol` on this
+ * device: *ok = 1 when the device's limits on pitch-linear 2D textures admit
+ * the volume (nx*ny texels a row, nz rows, its base aligned) and its z-fastest
+ * copy; 0 when those variants run as their load-based forms for it. */
+stt_status stt_fp_texture_ok(stt_ctx *ctx, const float *vol, int *ok);
 /* Description of variant `variant` of kernel `kernel` (0 gather projector,
  * 1 slab-staged projector, 2 voxel backprojection, 3 ray backprojection
  * scatter); NULL when out of range. */
@@ -226,12 +236,14 @@ stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, f
  * counterpart in the reference).  Every ray of view `view` takes as many
  * samples as its clip length holds, at the projector's step from its entry
  * point, with the projector's cell, 8-corner gather and trilinear
- * interpolation (packed != 0: pairs of samples in packed FP32x2
- * instructions) and none of the march's control (no block splits, no
- * per-sample bound checks, a plain sum).  out[W*H] receives the sums times the
- * step, count[W*H] (may be NULL) the samples per ray.  Timed against stt_fp,
- * it says how far the projector is from the rate its gathers alone reach.
- * Volumes below 2^31 voxels. */
+ * interpolation (packed bit 0: pairs of samples in packed FP32x2
+ * instructions; bit 1: packed pairs with the corners as tld4 texture gathers,
+ * as fp_variant 10 and 11 fetch them, STT_ERR_UNSUPPORTED where
+ * stt_fp_texture_ok says no) and none of the march's control (no block
+ * splits, no per-sample bound checks, a plain sum).  out[W*H] receives the
+ * sums times the step, count[W*H] (may be NULL) the samples per ray.  Timed
+ * against stt_fp, it says how far the projector is from the rate its gathers
+ * alone reach.  Volumes below 2^31 voxels. */
 stt_status stt_gather_ceiling(stt_ctx *ctx, const float *vol, int view, int packed, float *out, int *count,
                               void *stream);
 

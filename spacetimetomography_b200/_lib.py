@@ -98,6 +98,7 @@ def _load() -> C.CDLL:
         "stt_bp_ray": [vp, vp, vp, f, i, vp],
         "stt_bp_ray_scatter": [vp, vp, vp, vp, i, vp],
         "stt_gather_ceiling": [vp, vp, i, i, vp, vp, vp],
+        "stt_fp_texture_ok": [vp, vp, vp],
         "stt_sart_sweep_typed": [vp, vp, i, vp, vp, i, i, d, f, i, vp, vp, vp],
         "stt_bp_voxel_typed": [vp, vp, vp, i, d, f, i, vp],
         "stt_bp_ray_typed": [vp, vp, vp, i, f, i, vp],

@@ -173,7 +173,7 @@ class Context:
     def _tuning_dict(t: Tuning) -> dict:
         return {"fp_variant": t.fp_variant, "slab_variant": t.slab_variant, "bp_variant": t.bp_variant,
                 "staged_bins": t.staged_bins, "tuned": bool(t.tuned), "from_cache": bool(t.from_cache),
-                "fp_us": list(t.fp_us)[:10], "slab_us": list(t.slab_us)[:8], "bp_us": list(t.bp_us)[:3],
+                "fp_us": list(t.fp_us)[:12], "slab_us": list(t.slab_us)[:8], "bp_us": list(t.bp_us)[:3],
                 "ray_variant": t.ray_variant, "ray_us": list(t.ray_us), "staged_bins_bf16": t.staged_bins_bf16,
                 "ray": (lib.stt_tuning_variant_name(3, t.ray_variant) or b"").decode(),
                 "fp": (lib.stt_tuning_variant_name(0, t.fp_variant) or b"").decode(),
@@ -225,11 +225,20 @@ class Context:
                                        _stream(stream)))
         return vol
 
-    def gather_ceiling(self, vol, view, out, count=None, packed=True, stream=None):
+    def gather_ceiling(self, vol, view, out, count=None, packed=True, stream=None, texture=False):
         """stt_gather_ceiling: the projector's gathers and interpolation alone
-        along view `view`'s rays (a measurement kernel)."""
-        self._chk(lib.stt_gather_ceiling(self._h, _ptr(vol), view, int(packed), _ptr(out),
+        along view `view`'s rays (a measurement kernel); `texture`: the
+        corners as tld4 gathers (packed pairs)."""
+        mode = 2 | 1 if texture else int(bool(packed))
+        self._chk(lib.stt_gather_ceiling(self._h, _ptr(vol), view, mode, _ptr(out),
                                          _ptr(count) if count is not None else None, _stream(stream)))
+
+    def fp_texture_ok(self, vol) -> bool:
+        """Whether the tld4 gather variants (fp_variant 10, 11) bind `vol` as
+        textures on this device (stt_fp_texture_ok); else they run as loads."""
+        ok = C.c_int(0)
+        self._chk(lib.stt_fp_texture_ok(self._h, _ptr(vol), C.byref(ok)))
+        return bool(ok.value)
 
     def bp_ray_scatter(self, corr, contrib, wsum, view, stream=None):
         """The ray-driven backprojection's raw accumulation: contrib += c*w and

@@ -31,9 +31,11 @@ __device__ __forceinline__ bool tile_pixel(const GeomDev &g, int &i, int &j) {
 // (the samples are added one by one in march order).
 constexpr int FP_GROUP = 4;
 
-template <int FAST, typename I, int G = FP_GROUP, bool PK = false, typename T>
-__device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__restrict__ src, const Strides &st,
-                                                 const Ray &r, int *count) {
+// `corners(k, c, v)` fetches the 8 corners of cell c, the k-th sample of a
+// group (0 for a sample on its own): loads from an array, or tld4 gathers of
+// its texture (the same values).
+template <int G = FP_GROUP, bool PK = false, typename Corners>
+__device__ __forceinline__ float fp_ray_sum_with(const GeomDev &g, const Corners &corners, const Ray &r, int *count) {
     Kahan acc{0.0f, 0.0f};
     int n = 0;
     march_groups<G>(
@@ -42,7 +44,7 @@ __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__re
             FpCell c;
             fp_cell(g, p, c);
             float v[8];
-            fp_corners<FAST, I>(src, st, c, v);
+            corners(0, c, v);
             acc.add(__fmul_rn(trilerp(v, c), g.sd));
             ++n;
         },
@@ -54,8 +56,8 @@ __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__re
 #pragma unroll
                 for (int i = 0; i < G; i += 2) {
                     fp_cell2(g, p[i], p[i + 1], c[i], c[i + 1]);
-                    fp_corners<FAST, I>(src, st, c[i], v[i]);
-                    fp_corners<FAST, I>(src, st, c[i + 1], v[i + 1]);
+                    corners(i, c[i], v[i]);
+                    corners(i + 1, c[i + 1], v[i + 1]);
                 }
                 const float2 sd2 = make_float2(g.sd, g.sd);
 #pragma unroll
@@ -68,7 +70,7 @@ __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__re
 #pragma unroll
                 for (int i = 0; i < G; ++i) {
                     fp_cell(g, p[i], c[i]);
-                    fp_corners<FAST, I>(src, st, c[i], v[i]);
+                    corners(i, c[i], v[i]);
                 }
 #pragma unroll
                 for (int i = 0; i < G; ++i) acc.add(__fmul_rn(trilerp(v[i], c[i]), g.sd));
@@ -77,6 +79,29 @@ __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__re
         });
     if (count) *count = n;
     return acc.s;
+}
+
+template <int FAST, typename I, int G = FP_GROUP, bool PK = false, typename T>
+__device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__restrict__ src, const Strides &st,
+                                                 const Ray &r, int *count) {
+    return fp_ray_sum_with<G, PK>(
+        g, [=](int, const FpCell &c, float v[8]) { fp_corners<FAST, I>(src, st, c, v); }, r, count);
+}
+
+// The ray sum through the textures of FpTex: the transposed copy's for
+// layout-1 views when there is one, as fp_ray_sum reads the arrays.
+template <int G = FP_GROUP, bool PK = false>
+__device__ __forceinline__ float fp_ray_sum_tex(const GeomDev &g, const ViewRec &v, const FpTex &tex, const Ray &r) {
+    if (tex.z && v.layout == 1) {
+        const unsigned long long t = tex.z;
+        const int row = g.nz;
+        return fp_ray_sum_with<G, PK>(
+            g, [=](int, const FpCell &c, float w[8]) { fp_corners_tex<2>(t, row, c, w); }, r, nullptr);
+    }
+    const unsigned long long t = tex.x;
+    const int row = g.nx;
+    return fp_ray_sum_with<G, PK>(
+        g, [=](int, const FpCell &c, float w[8]) { fp_corners_tex<0>(t, row, c, w); }, r, nullptr);
 }
 
 template <typename I, int G = FP_GROUP, bool PK = false, typename T>
@@ -133,14 +158,16 @@ __global__ void __launch_bounds__(128) k_fp(const GeomDev g, const ViewRec *__re
 // never a ray's arithmetic.
 // T, B: the storage of the volume and of the sinogram stack (float, or BF16
 // bits widened exactly to FP32).
+// TX: the corners come from the textures of `tex` (FP32 volumes below 2^31
+// voxels), not from vol and vol_t.
 template <typename I, int WX = 32, int NW = 4, int G = FP_GROUP, bool PK = false, typename T = float,
-          typename B = float>
+          typename B = float, bool TX = false>
 __global__ void __launch_bounds__(32 * NW) k_fp_corr(const GeomDev g, const ViewRec *__restrict__ views,
                                                      const T *__restrict__ vol, const T *__restrict__ vol_t,
                                                      const ViewSel sel, const B *__restrict__ b_stack,
                                                      float *__restrict__ raylen_state,
                                                      float *__restrict__ corr, unsigned long long corr_surf,
-                                                     int skip_staged) {
+                                                     int skip_staged, const FpTex tex) {
     int i, j;
     if (!tile_pixel_t<WX, NW>(g, i, j)) return;
     int local;
@@ -153,7 +180,10 @@ __global__ void __launch_bounds__(32 * NW) k_fp_corr(const GeomDev g, const View
     const size_t pix = i + (size_t)j * g.W;
     float L, sum = 0.0f;
     if (r.tnear < r.tfar) {
-        sum = fp_ray_sum<I, G, PK>(g, vr, vol, vol_t, r, nullptr);
+        if constexpr (TX)
+            sum = fp_ray_sum_tex<G, PK>(g, vr, tex, r);
+        else
+            sum = fp_ray_sum<I, G, PK>(g, vr, vol, vol_t, r, nullptr);
         L = r.tfar - r.tnear;
         if (raylen_state) raylen_state[pix] = L;
     } else {
@@ -343,14 +373,15 @@ dim3 transpose_grid(const GeomDev &g) { return dim3((g.nx + 63) / 64, (g.nz + 63
 // The gather ceiling of the forward projector: each ray of one view takes as
 // many samples as its clip length holds, at the projector's step from its
 // entry point, with the projector's cell, 8-corner gather and trilinear
-// interpolation (G = 4 samples' loads in flight, packed pairs when PK), and
-// none of its march control (no segment splits, no per-sample bound, a plain
-// sum).  No counterpart in the reference: a measurement of the rate the
-// gathers alone reach on a volume, the on-chip roofline of the projectors.
-template <int FAST, bool PK>
+// interpolation (G = 4 samples' loads in flight, packed pairs when PK; the
+// corners as tld4 gathers of texture `tex` when TX), and none of its march
+// control (no segment splits, no per-sample bound, a plain sum).  No
+// counterpart in the reference: a measurement of the rate the gathers alone
+// reach on a volume, the on-chip roofline of the projectors.
+template <int FAST, bool PK, bool TX = false>
 __global__ void __launch_bounds__(128) k_gather_ceiling(const GeomDev g, const ViewRec *__restrict__ views, int view,
-                                                        const float *__restrict__ src, float *__restrict__ out,
-                                                        int *__restrict__ count) {
+                                                        const float *__restrict__ src, unsigned long long tex,
+                                                        float *__restrict__ out, int *__restrict__ count) {
     int i, j;
     if (!tile_pixel(g, i, j)) return;
     Ray r;
@@ -387,7 +418,12 @@ __global__ void __launch_bounds__(128) k_gather_ceiling(const GeomDev g, const V
                 for (int s = 0; s < G; ++s) fp_cell(g, q[s], c[s]);
             }
 #pragma unroll
-            for (int s = 0; s < G; ++s) fp_corners<FAST, int>(src, st, c[s], v[s]);
+            for (int s = 0; s < G; ++s) {
+                if constexpr (TX)
+                    fp_corners_tex<FAST>(tex, FAST ? g.nz : g.nx, c[s], v[s]);
+                else
+                    fp_corners<FAST, int>(src, st, c[s], v[s]);
+            }
             if constexpr (PK) {
 #pragma unroll
                 for (int s = 0; s < G; s += 2) {
@@ -404,7 +440,10 @@ __global__ void __launch_bounds__(128) k_gather_ceiling(const GeomDev g, const V
             FpCell c;
             fp_cell(g, p, c);
             float v[8];
-            fp_corners<FAST, int>(src, st, c, v);
+            if constexpr (TX)
+                fp_corners_tex<FAST>(tex, FAST ? g.nz : g.nx, c, v);
+            else
+                fp_corners<FAST, int>(src, st, c, v);
             sum = __fadd_rn(sum, trilerp(v, c));
 #pragma unroll
             for (int a = 0; a < 3; ++a) p[a] = __fadd_rn(p[a], step[a]);
@@ -453,14 +492,72 @@ cudaError_t launch_fp(const GeomDev &g, const ViewRec *views, const float *vol, 
 
 namespace {
 
-// One launch of gather variant <WX, NW, G, PK>: a block is NW warps of WX x (32/WX) pixels.
-template <int WX, int NW, int G, bool PK = false>
+// One launch of gather variant <WX, NW, G, PK, TX>: a block is NW warps of WX x (32/WX) pixels.
+template <int WX, int NW, int G, bool PK = false, bool TX = false>
 void fp_corr_variant(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t, const ViewSel &sel,
                      const float *b_stack, float *raylen_state, float *corr, cudaStream_t s,
-                     unsigned long long corr_surf, int skip) {
+                     unsigned long long corr_surf, int skip, const FpTex &tex = FpTex{}) {
     constexpr int TH = (32 / WX) * NW;  // detector rows per block
-    k_fp_corr<int, WX, NW, G, PK><<<dim3((g.W + WX - 1) / WX, (g.H + TH - 1) / TH, 1), 32 * NW, 0, s>>>(
-        g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip);
+    k_fp_corr<int, WX, NW, G, PK, float, float, TX>
+        <<<dim3((g.W + WX - 1) / WX, (g.H + TH - 1) / TH, 1), 32 * NW, 0, s>>>(
+            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip, tex);
+}
+
+// Device limits of pitch-linear 2D textures, read once per device.
+struct TexLimits {
+    int width = 0, height = 0, pitch = 0, pitch_align = 0, base_align = 0;
+};
+
+bool tex_limits(TexLimits &l) {
+    static TexLimits cache[64];
+    static bool have[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    if (!have[dev]) {
+        TexLimits t;
+        if (cudaDeviceGetAttribute(&t.width, cudaDevAttrMaxTexture2DLinearWidth, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&t.height, cudaDevAttrMaxTexture2DLinearHeight, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&t.pitch, cudaDevAttrMaxTexture2DLinearPitch, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&t.pitch_align, cudaDevAttrTexturePitchAlignment, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&t.base_align, cudaDevAttrTextureAlignment, dev) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        cache[dev] = t;
+        have[dev] = true;
+    }
+    l = cache[dev];
+    return true;
+}
+
+bool slices_fit(const TexLimits &l, const float *p, long long width, long long rows) {
+    const long long pitch = width * (long long)sizeof(float);
+    return p && width >= 2 && rows >= 2 && width <= l.width && rows <= l.height && pitch <= l.pitch &&
+           !(l.pitch_align > 0 && pitch % l.pitch_align) && !(l.base_align > 0 && (uintptr_t)p % l.base_align);
+}
+
+// A point-sampled, clamped FP32 texture of `rows` rows of `width` texels over
+// linear memory; 0 where the limits do not admit it.
+unsigned long long slices_texture(const TexLimits &l, const float *p, long long width, long long rows) {
+    const long long pitch = width * (long long)sizeof(float);
+    if (!slices_fit(l, p, width, rows)) return 0;
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypePitch2D;
+    rd.res.pitch2D.devPtr = const_cast<float *>(p);
+    rd.res.pitch2D.desc = cudaCreateChannelDesc<float>();
+    rd.res.pitch2D.width = (size_t)width;
+    rd.res.pitch2D.height = (size_t)rows;
+    rd.res.pitch2D.pitchInBytes = (size_t)pitch;
+    cudaTextureDesc td{};
+    td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    cudaTextureObject_t t = 0;
+    if (cudaCreateTextureObject(&t, &rd, &td, nullptr) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (unsigned long long)t;
 }
 
 }  // namespace
@@ -475,15 +572,55 @@ const char *fp_variant_name(int v) {
                                              "32x4 rays per block, 8 in flight",
                                              "32x4 rays per block, 4 in flight, packed pairs",
                                              "32x4 rays per block, 8 in flight, packed pairs",
-                                             "32x8 rays per block, 4 in flight, packed pairs"};
+                                             "32x8 rays per block, 4 in flight, packed pairs",
+                                             "warps of 8x4 rays, 8x16 per block, 8 in flight, packed pairs, tld4 corners",
+                                             "32x4 rays per block, 8 in flight, packed pairs, tld4 corners"};
     return v >= 0 && v < kFpVariants ? names[v] : "?";
+}
+
+bool is_tex_fp_variant(int fp_variant) { return fp_variant == 10 || fp_variant == 11; }
+
+bool make_fp_tex(const GeomDev &g, const float *vol, const float *vol_t, FpTex &t) {
+    t = FpTex{};
+    TexLimits l;
+    if (!small_volume(g) || !tex_limits(l)) return false;
+    const unsigned long long x = slices_texture(l, vol, (long long)g.nx * g.ny, g.nz);
+    if (!x) return false;
+    unsigned long long z = 0;
+    if (vol_t && !(z = slices_texture(l, vol_t, (long long)g.nz * g.ny, g.nx))) {
+        cudaDestroyTextureObject((cudaTextureObject_t)x);
+        return false;
+    }
+    t.x = x;
+    t.z = z;
+    t.ok = 1;
+    return true;
+}
+
+bool fp_tex_fits(const GeomDev &g, const float *vol) {
+    TexLimits l;
+    if (!small_volume(g) || !tex_limits(l)) return false;
+    const float *aligned = reinterpret_cast<const float *>((uintptr_t)(l.base_align > 0 ? l.base_align : 256));
+    return slices_fit(l, vol, (long long)g.nx * g.ny, g.nz) && slices_fit(l, aligned, (long long)g.nz * g.ny, g.nx);
+}
+
+void destroy_fp_tex(FpTex &t) {
+    if (t.x) cudaDestroyTextureObject((cudaTextureObject_t)t.x);
+    if (t.z) cudaDestroyTextureObject((cudaTextureObject_t)t.z);
+    t = FpTex{};
 }
 
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
                            cudaStream_t s, unsigned long long corr_surf, const FpSlabMaps *maps, int *status,
-                           int fp_variant) {
+                           int fp_variant, const FpTex *tex) {
     const int skip = maps && maps->ok && maps->esize == 4 && (!vol_t || maps->has_z);
+    // a texture variant whose textures are missing, or do not cover vol_t,
+    // runs the load-based variant of the same shape
+    if (is_tex_fp_variant(fp_variant) && !(tex && tex->ok && (!vol_t || tex->z)))
+        fp_variant = fp_variant == 10 ? 4 : 8;
+    FpTex tx = tex ? *tex : FpTex{};
+    if (!vol_t) tx.z = 0;  // without the copy every view reads the volume, as the loads do
     if (skip) {
         cudaError_t e = launch_fp_corr_slab(g, views, *maps, vol, vol_t, sel, b_stack, raylen_state, corr, s,
                                             corr_surf, status);
@@ -491,7 +628,7 @@ cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *
     }
     if (!small_volume(g)) {
         k_fp_corr<long long><<<ray_grid(g, 1), 128, 0, s>>>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr,
-                                                            corr_surf, skip);
+                                                            corr_surf, skip, FpTex{});
         return cudaGetLastError();
     }
     switch (fp_variant) {
@@ -504,6 +641,14 @@ cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *
     case 7: fp_corr_variant<32, 4, 4, true>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
     case 8: fp_corr_variant<32, 4, 8, true>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
     case 9: fp_corr_variant<32, 8, 4, true>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
+    case 10:
+        fp_corr_variant<8, 4, 8, true, true>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf,
+                                             skip, tx);
+        break;
+    case 11:
+        fp_corr_variant<32, 4, 8, true, true>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf,
+                                              skip, tx);
+        break;
     default: fp_corr_variant<32, 4, 4>(g, views, vol, vol_t, sel, b_stack, raylen_state, corr, s, corr_surf, skip); break;
     }
     return cudaGetLastError();
@@ -568,10 +713,10 @@ cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const unsigne
     }
     if (small_volume(g))
         k_fp_corr<int, 32, 4, FP_GROUP, false, U, U><<<ray_grid(g, 1), 128, 0, s>>>(
-            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip);
+            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip, FpTex{});
     else
         k_fp_corr<long long, 32, 4, FP_GROUP, false, U, U><<<ray_grid(g, 1), 128, 0, s>>>(
-            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip);
+            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip, FpTex{});
     return cudaGetLastError();
 }
 
@@ -627,14 +772,20 @@ cudaError_t launch_fp_adjoint(const GeomDev &g, const ViewRec *views, int view0,
 
 cudaError_t launch_gather_ceiling(const GeomDev &g, const ViewRec *views, const ViewRec &host_view, int view,
                                   const float *vol, const float *vol_t, int packed, float *out, int *count,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, const FpTex *tex) {
     if (!small_volume(g)) return cudaErrorInvalidValue;
     const bool zf = vol_t && host_view.layout == 1;
     const float *src = zf ? vol_t : vol;
-    if (zf && packed) k_gather_ceiling<2, true><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, out, count);
-    else if (zf) k_gather_ceiling<2, false><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, out, count);
-    else if (packed) k_gather_ceiling<0, true><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, out, count);
-    else k_gather_ceiling<0, false><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, out, count);
+    if (tex) {  // packed pairs, tld4 corners
+        if (!tex->ok || (zf && !tex->z)) return cudaErrorInvalidValue;
+        if (zf) k_gather_ceiling<2, true, true><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, tex->z, out, count);
+        else k_gather_ceiling<0, true, true><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, tex->x, out, count);
+        return cudaGetLastError();
+    }
+    if (zf && packed) k_gather_ceiling<2, true><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, 0, out, count);
+    else if (zf) k_gather_ceiling<2, false><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, 0, out, count);
+    else if (packed) k_gather_ceiling<0, true><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, 0, out, count);
+    else k_gather_ceiling<0, false><<<ray_grid(g, 1), 128, 0, s>>>(g, views, view, src, 0, out, count);
     return cudaGetLastError();
 }
 

@@ -140,6 +140,7 @@ stt_status stt_destroy(stt_ctx *ctx) {
     cudaFree(ctx->pw);
     cudaFree(ctx->pwd);
     cudaFree(ctx->status);
+    for (auto &e : ctx->fp_tex) stt::destroy_fp_tex(e.tex);
     delete ctx;
     return STT_OK;
 }
@@ -382,8 +383,17 @@ stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, flo
     stt::FpSlabMaps maps{};  // ok = 0: every view gathers, one launch
     if (staged_mask(ctx, vol)) stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
     STT_CUDA(ctx, stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, b, raylen_state, corr, S(stream), 0, &maps,
-                                      ctx->status, ctx->tuning.fp),
+                                      ctx->status, ctx->tuning.fp, stt::ctx_fp_tex(ctx, vol, volt)),
              "k_fp_corr launch");
+    return STT_OK;
+}
+
+stt_status stt_fp_texture_ok(stt_ctx *ctx, const float *vol, int *ok) {
+    stt_status st = need_geom(ctx);
+    if (st) return st;
+    if (!vol || !ok) return fail(ctx, STT_ERR_INVALID, "null vol or ok");
+    if ((st = set_device(ctx))) return st;
+    *ok = stt::fp_tex_fits(ctx->g, vol) ? 1 : 0;
     return STT_OK;
 }
 
@@ -398,8 +408,14 @@ stt_status stt_gather_ceiling(stt_ctx *ctx, const float *vol, int view, int pack
     if ((st = set_device(ctx))) return st;
     const float *volt = nullptr;
     if ((st = transposed_if_needed(ctx, vol, view, 1, S(stream), &volt))) return st;
-    STT_CUDA(ctx, stt::launch_gather_ceiling(ctx->g, ctx->views_d, ctx->views_h[view], view, vol, volt, packed, out,
-                                             count, S(stream)),
+    const stt::FpTex *tex = nullptr;
+    if (packed & 2) {  // tld4 corners
+        tex = stt::ctx_fp_tex_any(ctx, vol, volt);
+        if (!tex || !tex->ok)
+            return fail(ctx, STT_ERR_UNSUPPORTED, "the device's texture limits do not admit this volume");
+    }
+    STT_CUDA(ctx, stt::launch_gather_ceiling(ctx->g, ctx->views_d, ctx->views_h[view], view, vol, volt, packed & 1, out,
+                                             count, S(stream), tex),
              "k_gather_ceiling launch");
     return STT_OK;
 }
@@ -510,7 +526,7 @@ static cudaError_t sweep_fp_corr(stt_ctx *ctx, const float *vol, const float *vo
     stt::FpSlabMaps maps{};  // ok = 0: every view gathers, one launch
     if (staged_mask(ctx, vol)) stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
     return stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, stack, rl, ctx->corr, s, 0, &maps, ctx->status,
-                               ctx->tuning.fp);
+                               ctx->tuning.fp, stt::ctx_fp_tex(ctx, vol, volt));
 }
 
 static cudaError_t sweep_fp_corr(stt_ctx *ctx, const unsigned short *vol, const unsigned short *volt,

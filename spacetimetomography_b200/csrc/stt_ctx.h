@@ -43,6 +43,18 @@ struct stt_ctx {
     unsigned staged_bins16 = 0x1E0u;  // the same for a BF16-stored volume (ViewRec::staged16)
     bool tuned = false;
     stt_tuning report{};
+    // Texture objects of the tld4 gather variants for the arrays the entry
+    // points were given, keyed by the arrays and the dimensions (at most
+    // kFpTexCache; past that the load-based variant of the same shape runs).
+    // Kept until stt_destroy, so a stream capture of an entry point that
+    // bound one stays valid.
+    struct FpTexEntry {
+        const float *vol, *volt;
+        int nx, ny, nz;
+        stt::FpTex tex;
+    };
+    static constexpr int kFpTexCache = 32;
+    std::vector<FpTexEntry> fp_tex;
 };
 
 namespace stt {
@@ -53,4 +65,9 @@ inline int off_axis_bin(float deg) {
 }
 // Applies ctx->staged_bins and staged_bins16 to every view (host and device tables).
 stt_status apply_staged_bins(stt_ctx *ctx);
+// The textures of the tuned gather variant for (vol, vol_t) when it is a tld4
+// variant (created on first use, cached in the context); nullptr otherwise.
+const FpTex *ctx_fp_tex(stt_ctx *ctx, const float *vol, const float *vol_t);
+// The same whatever the tuned variant (nullptr only when the cache is full).
+const FpTex *ctx_fp_tex_any(stt_ctx *ctx, const float *vol, const float *vol_t);
 }  // namespace stt

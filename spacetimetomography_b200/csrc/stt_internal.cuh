@@ -293,6 +293,29 @@ __device__ __forceinline__ void fp_corners(const T *__restrict__ src, const Stri
     }
 }
 
+// The same 8 corners through two tld4 gathers of a pitch-linear 2D texture
+// whose rows are the array's slices across its slowest axis: for the volume
+// (FAST 0) texel (x + nx*y, z); for the z-fastest copy (FAST 2) texel
+// (z + nz*y, x).  A gather at texel (u, v) returns {u, u+1} x {v, v+1} (.w =
+// (u, v), .z = (u+1, v), .x = (u, v+1), .y = (u+1, v+1)): the fast-axis pair
+// of two neighbouring slices; the second gather, one row of `row` texels on,
+// is the y+1 pair.  The cell's base is at most dims-2 on every axis, so no
+// gather leaves the array or crosses into another row of slices.
+template <int FAST>
+__device__ __forceinline__ void fp_corners_tex(unsigned long long tex, int row, const FpCell &c, float v[8]) {
+    const int u = FAST == 0 ? c.ix + row * c.iy : c.iz + row * c.iy;
+    const float fv = (float)(FAST == 0 ? c.iz : c.ix) + 1.0f;
+    const float4 a = tex2Dgather<float4>(tex, (float)u + 1.0f, fv, 0);
+    const float4 b = tex2Dgather<float4>(tex, (float)(u + row) + 1.0f, fv, 0);
+    if (FAST == 0) {  // u along x, v along z
+        v[0] = a.w, v[1] = a.z, v[4] = a.x, v[5] = a.y;
+        v[2] = b.w, v[3] = b.z, v[6] = b.x, v[7] = b.y;
+    } else {  // u along z, v along x
+        v[0] = a.w, v[4] = a.z, v[1] = a.x, v[5] = a.y;
+        v[2] = b.w, v[6] = b.z, v[3] = b.x, v[7] = b.y;
+    }
+}
+
 template <int FAST, typename I, typename T>
 __device__ __forceinline__ float fp_sample(const GeomDev &g, const T *__restrict__ src, const Strides &st,
                                            const float p[3]) {

@@ -23,8 +23,9 @@ int grid_stride_blocks(long long n, int threads);
 // Variant 0 of each is the default; all variants of a kernel give the same
 // bits (they change which thread or block computes what, never a value's
 // arithmetic).
-//   fp:   the gather forward projector k_fp_corr: detector tile and samples
-//         in flight (fp_variant_name);
+//   fp:   the gather forward projector k_fp_corr: detector tile, samples
+//         in flight and, for variants 10 and 11, corners fetched as two tld4
+//         texture gathers per sample instead of eight loads (fp_variant_name);
 //   slab: the box of the slab-staged projector (slab_variant_name);
 //   bp:   the column length of the voxel backprojection (bp_variant_name);
 //   ray:  the scatter of the ray-driven backprojection (ray_variant_name):
@@ -32,7 +33,7 @@ int grid_stride_blocks(long long n, int threads);
 //         slab (volumes below 2^31 voxels).  Its sums differ in float order
 //         only (as any two atomic runs do), not in their terms.
 // Which views the slab kernel projects is the per-view ViewRec::staged flag.
-constexpr int kFpVariants = 10, kSlabVariants = 8, kBpVariants = 3, kRayVariants = 2;
+constexpr int kFpVariants = 12, kSlabVariants = 8, kBpVariants = 3, kRayVariants = 2;
 struct Tuning {
     int fp = 0, slab = 0, bp = 0, ray = 0;
 };
@@ -74,14 +75,36 @@ cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const Fp
                                 const unsigned short *vol, const unsigned short *vol_t, const ViewSel &sel,
                                 const unsigned short *b_stack, float *raylen_state, float *corr, cudaStream_t s,
                                 unsigned long long corr_surf, int *status);
+// Texture objects of the gather variants that fetch corners with tld4: the
+// FP32 volume as a pitch-linear 2D texture whose rows are its z slices (width
+// nx*ny texels, nz rows) and its z-fastest copy likewise (rows the x slices;
+// z = 0 without a copy).  Point sampling of an FP32 texture returns stored
+// values exactly, so the samples are those of the loads they replace.
+// make_fp_tex returns false (and creates nothing) where the device's limits
+// on linear 2D textures do not admit the arrays: a row of more than the
+// maximum width or pitch, more rows than the maximum height, a base not
+// aligned to the texture alignment.  The caller owns the objects
+// (destroy_fp_tex).
+struct FpTex {
+    unsigned long long x = 0, z = 0;
+    int ok = 0;
+};
+bool is_tex_fp_variant(int fp_variant);
+bool make_fp_tex(const GeomDev &g, const float *vol, const float *vol_t, FpTex &t);
+// Whether make_fp_tex admits `vol` and a z-fastest copy at an aligned base on
+// this device (checks the limits only; creates nothing).
+bool fp_tex_fits(const GeomDev &g, const float *vol);
+void destroy_fp_tex(FpTex &t);
 // Forward projection of one view fused with the SART correction.  With usable
 // slab maps, staged views run in the slab-staged kernel and the others in the
 // gather kernel (both are launched; each leaves the other's views alone).
-// `fp_variant` selects the gather kernel's launch shape.
+// `fp_variant` selects the gather kernel's launch shape; a texture variant
+// (is_tex_fp_variant) without usable `tex` runs the load-based variant of the
+// same shape, which gives the same bits.
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *vol, const float *vol_t,
                            const ViewSel &sel, const float *b_stack, float *raylen_state, float *corr,
                            cudaStream_t s, unsigned long long corr_surf = 0, const FpSlabMaps *maps = nullptr,
-                           int *status = nullptr, int fp_variant = 0);
+                           int *status = nullptr, int fp_variant = 0, const FpTex *tex = nullptr);
 cudaError_t launch_transpose(const GeomDev &g, const float *in, float *out, cudaStream_t s);
 cudaError_t launch_fp_bf16(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
                            const unsigned short *vol_t, int view0, int nviews, float *proj, float *raylen,
@@ -124,10 +147,11 @@ cudaError_t launch_fp_adjoint(const GeomDev &g, const ViewRec *views, int view0,
                               const float *proj_bar, float *vol_bar, cudaStream_t s);
 // The gather ceiling (k_project.cu): one view's rays sampled at the
 // projector's step with its gathers and interpolation and none of its march
-// control; `host_view` is the view's record (its layout picks vol_t).
+// control; `host_view` is the view's record (its layout picks vol_t).  With
+// `tex` (made over vol and vol_t) the corners are tld4 gathers in packed pairs.
 cudaError_t launch_gather_ceiling(const GeomDev &g, const ViewRec *views, const ViewRec &host_view, int view,
                                   const float *vol, const float *vol_t, int packed, float *out, int *count,
-                                  cudaStream_t s);
+                                  cudaStream_t s, const FpTex *tex = nullptr);
 cudaError_t launch_fill_zero(float *p, long long n, cudaStream_t s);
 cudaError_t launch_dot_f64(long long n, const float *a, const float *b, double *out, cudaStream_t s);
 cudaError_t launch_scale_inv_sqrt(long long n, float *x, const double *norm2, cudaStream_t s);

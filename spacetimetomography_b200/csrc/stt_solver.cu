@@ -138,6 +138,7 @@ struct stt_solver {
     long long phase_launches[2] = {0, 0};
     std::vector<LayeredTex> corr_tex;  // batched modes: per frame, the correction as a texture
     std::vector<stt::FpSlabMaps> fpmaps;  // batched modes: per frame, TMA maps of the volume and its copy
+    std::vector<stt::FpTex> fptex;  // batched modes, FP32, a tld4 gather variant: per frame, the volume's textures
     std::string err;
 };
 
@@ -262,7 +263,7 @@ int fp_corr(stt_solver *s, int f, const float *vol, const float *volt, const stt
             float *rl, float *corr, cudaStream_t cs, unsigned long long surf, cudaError_t &e) {
     const stt::FpSlabMaps *maps = s->fpmaps.empty() ? nullptr : &s->fpmaps[f];
     e = stt::launch_fp_corr(*s->g, s->views, vol, volt, sel, stack, rl, corr, cs, surf, maps, s->status,
-                            s->ctx->tuning.fp);
+                            s->ctx->tuning.fp, s->fptex.empty() ? nullptr : &s->fptex[f]);
     return (maps && maps->ok) ? 2 : 1;  // slab-staged + gather kernels, or gather only
 }
 
@@ -534,6 +535,11 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
                                        ctx->tuning.slab);
         }
     }
+    if (cfg->mode != STT_SOLVE_PLAIN && cfg->storage == STT_DTYPE_F32 && stt::is_tex_fp_variant(ctx->tuning.fp)) {
+        s->fptex.resize(F);  // where they cannot be made, ok stays 0 and the loads run
+        for (int f = 0; f < F; ++f)
+            stt::make_fp_tex(*g, s->st.vol + f * s->n, static_cast<float *>(s->volt) + f * s->n, s->fptex[f]);
+    }
     if (cfg->mode != STT_SOLVE_PLAIN && cfg->bp_mode == 0) {
         s->corr_tex.resize(F);
         for (int f = 0; f < F; ++f)
@@ -693,6 +699,7 @@ stt_status stt_solver_destroy(stt_solver *s) {
         if (e) cudaEventDestroy(e);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     for (auto &t : s->corr_tex) free_layered(t);
+    for (auto &t : s->fptex) stt::destroy_fp_tex(t);
     cudaFree(s->warpbuf);
     cudaFree(s->corr);
     cudaFree(s->ax);

@@ -3,8 +3,9 @@
 //
 // What it picks, for one context's geometry (volume, detector, distances,
 // view list):
-//   * the gather projector's launch variant (detector tile of a block and
-//     samples in flight per ray, fp_variant_name);
+//   * the gather projector's launch variant (detector tile of a block,
+//     samples in flight per ray, corners by loads or by tld4 texture gathers,
+//     fp_variant_name);
 //   * the slab-staged projector's TMA box (slab_variant_name);
 //   * for every 5-degree class of views (the central ray's angle off the
 //     nearest of the x and z axes), which of the two projectors runs them;
@@ -56,8 +57,10 @@ struct Scratch {
     stt::ViewRec *tv = nullptr;
     cudaArray_t arr = nullptr;
     cudaTextureObject_t tex = 0;
+    stt::FpTex fptex;  // the textures of the tld4 gather variants over vol and volt
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     ~Scratch() {
+        stt::destroy_fp_tex(fptex);
         cudaFree(vol);
         cudaFree(volt);
         cudaFree(b);
@@ -115,6 +118,21 @@ stt_status apply_staged_bins(stt_ctx *ctx) {
         return STT_ERR_CUDA;
     }
     return STT_OK;
+}
+
+const FpTex *ctx_fp_tex(stt_ctx *ctx, const float *vol, const float *vol_t) {
+    return is_tex_fp_variant(ctx->tuning.fp) ? ctx_fp_tex_any(ctx, vol, vol_t) : nullptr;
+}
+
+const FpTex *ctx_fp_tex_any(stt_ctx *ctx, const float *vol, const float *vol_t) {
+    const GeomDev &g = ctx->g;
+    for (const auto &e : ctx->fp_tex)
+        if (e.vol == vol && e.volt == vol_t && e.nx == g.nx && e.ny == g.ny && e.nz == g.nz) return &e.tex;
+    if ((int)ctx->fp_tex.size() >= stt_ctx::kFpTexCache) return nullptr;
+    stt_ctx::FpTexEntry e{vol, vol_t, g.nx, g.ny, g.nz, FpTex{}};
+    make_fp_tex(g, vol, vol_t, e.tex);  // where it fails, tex.ok = 0 is cached too: the loads run
+    ctx->fp_tex.push_back(e);
+    return &ctx->fp_tex.back().tex;
 }
 
 }  // namespace stt
@@ -245,6 +263,7 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
     bool slab_ok = false;
     for (int sv = 0; sv < stt::kSlabVariants; ++sv)
         slab_ok |= maps_ok[sv] = stt::make_fp_slab_maps(g, sc.vol, sc.volt, maps[sv], sv);
+    stt::make_fp_tex(g, sc.vol, sc.volt, sc.fptex);  // where it fails, ok = 0 and the tld4 variants are skipped
     for (int b = 0; b < 9; ++b) {
         if (rep[b] < 0) continue;
         stt::ViewRec two[2] = {ctx->views_h[rep[b]], ctx->views_h[rep[b]]};
@@ -254,9 +273,13 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
             return fail(e, "view copy");
         const stt::ViewSel gather_sel{0, nullptr, 0, 0}, slab_sel{1, nullptr, 0, 1};
         for (int fv = 0; fv < stt::kFpVariants; ++fv) {
+            if (stt::is_tex_fp_variant(fv) && !sc.fptex.ok) {
+                tg[fv][b] = 3.0e38f;  // no textures on this geometry: never chosen
+                continue;
+            }
             e = time_us(sc, s, [&] {
                 return stt::launch_fp_corr(g, sc.tv, sc.vol, sc.volt, gather_sel, sc.b, sc.rl, sc.corr, s, 0, nullptr,
-                                           ctx->status, fv);
+                                           ctx->status, fv, &sc.fptex);
             }, tg[fv][b]);
             if (e) return fail(e, "gather projector");
         }
@@ -283,6 +306,7 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
     stt_tuning t{};
     double best = 1e300;
     for (int fv = 0; fv < stt::kFpVariants; ++fv) {
+        if (stt::is_tex_fp_variant(fv) && !sc.fptex.ok) continue;  // not timed: fp_us stays 0
         double tot = 0.0, w = 0.0;
         for (int b = 0; b < 9; ++b)
             if (rep[b] >= 0) tot += (double)count[b] * tg[fv][b], w += count[b];

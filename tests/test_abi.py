@@ -121,7 +121,7 @@ def test_tuning_variant_names_and_struct_layout(lib):
     layout (the host reads the tuner's report through it)."""
     from spacetimetomography_b200._lib import SolveCfg, Instance, Tuning
 
-    counts = {0: 10, 1: 8, 2: 3, 3: 2}  # gather projector, slab projector, voxel BP, ray-BP scatter
+    counts = {0: 12, 1: 8, 2: 3, 3: 2}  # gather projector, slab projector, voxel BP, ray-BP scatter
     for kernel, n in counts.items():
         names = [lib.stt_tuning_variant_name(kernel, v) for v in range(n)]
         assert all(names) and len(set(names)) == n, (kernel, names)

@@ -387,7 +387,9 @@ def test_bp_ray_scatter_slab_vs_sequential_oracle(cuda, dims, det, off):
 def test_gather_ceiling_packed_pairs_equal_scalar(cuda):
     """The gather ceiling in packed FP32x2 pairs (fp_cell2/trilerp2, the
     helpers of the packed projector variants) gives the scalar form's bits,
-    and its sums track the projector's (same rays, nearly the same samples)."""
+    so does its tld4 form (fp_corners_tex, the corner fetch of the texture
+    projector variants), and its sums track the projector's (same rays,
+    nearly the same samples)."""
     import torch
 
     scan = ob.Scan((64, 56, 72), (96, 80), off=(0.7, -1.1, 0.4))
@@ -401,6 +403,9 @@ def test_gather_ceiling_packed_pairs_equal_scalar(cuda):
         n = torch.zeros((H, W), dtype=torch.int32, device=cuda)
         ctx.gather_ceiling(vol, v, a, n, packed=True)
         ctx.gather_ceiling(vol, v, b, packed=False)
+        np.testing.assert_array_equal(_np(a), _np(b))
+        assert ctx.fp_texture_ok(vol)
+        ctx.gather_ceiling(vol, v, b, texture=True)
         np.testing.assert_array_equal(_np(a), _np(b))
         proj = torch.zeros((1, H, W), device=cuda)
         ctx.fp(vol, proj, view0=v, nviews=1)

@@ -56,7 +56,9 @@ def test_every_projector_variant_gives_the_same_bits(cuda, dims, det, off):
     views = range(len(ANGLES))
     ctx.set_tuning(0, 0, 0, staged_bins=0)  # everything through the default gather variant
     base = _corrections(ctx, vol, b, views)
-    for fv in range(1, 10):  # tiles, samples in flight, packed FP32x2 pairs
+    # the tld4 variants must really bind the volume here, not run as loads
+    assert ctx.fp_texture_ok(vol)
+    for fv in range(1, 12):  # tiles, samples in flight, packed FP32x2 pairs, tld4 corners
         ctx.set_tuning(fv, 0, 0, staged_bins=0)
         for k, (a, c) in enumerate(zip(base, _corrections(ctx, vol, b, views))):
             np.testing.assert_array_equal(a, c, err_msg=f"gather variant {fv}, output {k}")
@@ -118,7 +120,7 @@ def test_autotune_picks_a_valid_choice_and_caches_it(cuda):
     ctx = _ctx(scan, ANGLES)
     t = ctx.autotune()
     assert t["tuned"] and not t["from_cache"]
-    assert 0 <= t["fp_variant"] < 10 and 0 <= t["slab_variant"] < 8 and 0 <= t["bp_variant"] < 3
+    assert 0 <= t["fp_variant"] < 12 and 0 <= t["slab_variant"] < 8 and 0 <= t["bp_variant"] < 3
     assert 0 <= t["ray_variant"] < 2
     assert 0 <= t["staged_bins"] < 512 and 0 <= t["staged_bins_bf16"] < 512
     assert all(x > 0 for x in t["fp_us"]) and all(x > 0 for x in t["bp_us"]) and all(x > 0 for x in t["ray_us"])
