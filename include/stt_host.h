@@ -73,6 +73,8 @@ void stt_host_free(void *p);
  * STT_DTYPE_F32; use STT_SOLVE_GRAPH); `slots` (1..8) complete copies of the device state are
  * allocated on the current stt_host_set_device device, so that with 2 slots a
  * step's upload and the previous step's read-back overlap a step's compute.
+ * With cfg->autotune the launch choices are timed on this geometry once, when
+ * the first slot's solver is created (the others share the context). 
  *
  * stt_host_solver_submit: one step on the next slot (waiting first for that
  * slot's previous step if it is still pending): uploads vol (F volumes, x

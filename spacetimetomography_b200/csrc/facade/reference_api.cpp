@@ -590,6 +590,7 @@ void ST_Tomography::_ensure_device() {
     std::memcpy(cfg.roi_cut, kCut, sizeof(kCut));
     cfg.seed = m_seed;
     cfg.mode = STT_SOLVE_GRAPH;
+    cfg.autotune = 1;  // the launch choices timed on this geometry (stt_autotune) before the graph is captured
     stt_pd_state st{};
     st.vol = d->vol;
     st.xbar = d->xbar;

@@ -58,18 +58,19 @@ class HostSolver:
     """stt_host_solver: submit() enqueues one step (upload, n_iters
     iterations, read-back) on the next of `slots` device states; wait()
     completes the oldest pending step.  Keep the arrays of a step alive and
-    unread until its wait()."""
+    unread until its wait().  `autotune` (stt_solve_cfg.autotune): the
+    launch choices are timed on this geometry when the solver is created."""
 
     def __init__(self, dims, spacing, det, ds, sid, sdd, angles, n_frames, views_per_frame, pd: PdParams,
                  alpha=0.3, bp_mode=0, roi_cut=REFERENCE_CUT, seed=0, mode=SOLVE_GRAPH, slots=2, device=0,
-                 offset=(0.0, 0.0, 0.0)):
+                 offset=(0.0, 0.0, 0.0), autotune=True):
         lib = facade()
         self._ang = np.ascontiguousarray(angles, dtype=np.float64)
         g = Geometry(int(dims[0]), int(dims[1]), int(dims[2]), *map(float, spacing), int(det[0]), int(det[1]),
                      float(ds), float(sid), float(sdd), (C.c_double * 3)(*map(float, offset)), len(self._ang),
                      self._ang.ctypes.data_as(C.POINTER(C.c_double)))
         cfg = SolveCfg(n_frames, views_per_frame, bp_mode, float(alpha), pd.c(), (C.c_int * 8)(*map(int, roi_cut)),
-                       C.c_ulonglong(seed), mode, 0, 0, 0)
+                       C.c_ulonglong(seed), mode, 0, 0, 0, int(bool(autotune)))
         self._chk(lib.stt_host_set_device(int(device)))
         h = C.c_void_p()
         self._chk(lib.stt_host_solver_create(C.byref(g), C.byref(cfg), int(slots), C.byref(h)))
