@@ -978,7 +978,7 @@ def fp_probe(cid, dev, stream, tuned=False, tuning=None) -> None:
         print(json.dumps({"tuning": tune_or_set(ctx, stream, tuning)}), flush=True)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("fp_probe")
-    for v in (0, V // 8, V // 4, 3 * V // 8):  # 0, 45, 90, 135 degrees
+    for v in (0, V // 8, V // 4, 3 * V // 8):  # about 0, 45, 90, 135 degrees (0, 40, 90, 130 for 36 views)
         ctx.fp_correction(vol, b, rl, corr, v, stream=stream)
     torch.cuda.synchronize()
     if tuned:
@@ -1005,7 +1005,7 @@ def bp_ray_probe(cid, dev, stream) -> None:
     g = torch.Generator(device=dev)
     g.manual_seed(3)
     corr = torch.rand((D, D), device=dev, generator=g) - 0.5
-    for v in (0, V // 8, V // 4, 3 * V // 8):  # 0, 45, 90, 135 degrees
+    for v in (0, V // 8, V // 4, 3 * V // 8):  # about 0, 45, 90, 135 degrees (0, 40, 90, 130 for 36 views)
         for rv in (0, 1):  # both scatters: global vector atomics, the shared-memory slab box
             ctx.set_tuning(ray_variant=rv)
             ctx.bp_ray(corr, vol, 1e9, v, stream=stream)
