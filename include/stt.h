@@ -151,6 +151,10 @@ typedef struct stt_tuning {
     float ray_us[2];
     unsigned staged_bins_bf16;  /* staged_bins for a BF16-stored volume (stt_solve_cfg.storage,
                                    stt_sart_sweep_typed): its gathers and boxes move half the bytes */
+    int fp_variant_bf16;  /* the gather projector's form for a BF16-stored volume (kernel 4 of
+                             stt_tuning_variant_name): 0 loads, 1 tld4 gathers of 16-bit textures
+                             (where the device's texture limits admit the volume; else loads) */
+    float fp16_us[2];
 } stt_tuning;
 stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream);
 stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out);
@@ -160,9 +164,13 @@ stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t);
  * the volume (nx*ny texels a row, nz rows, its base aligned) and its z-fastest
  * copy; 0 when those variants run as their load-based forms for it. */
 stt_status stt_fp_texture_ok(stt_ctx *ctx, const float *vol, int *ok);
+/* The same for a volume stored as `dtype` (STT_DTYPE_BF16: 16-bit texels,
+ * the gather form fp_variant_bf16 1). */
+stt_status stt_fp_texture_ok_typed(stt_ctx *ctx, const void *vol, int dtype, int *ok);
 /* Description of variant `variant` of kernel `kernel` (0 gather projector,
  * 1 slab-staged projector, 2 voxel backprojection, 3 ray backprojection
- * scatter); NULL when out of range. */
+ * scatter, 4 gather projector of a BF16-stored volume); NULL when out of
+ * range. */
 const char *stt_tuning_variant_name(int kernel, int variant);
 
 /* ---- forward projector (TypicalRayProducer.core.h:123-268) ---------------

@@ -74,7 +74,8 @@ class Tuning(C.Structure):
     _fields_ = [("fp_variant", C.c_int), ("slab_variant", C.c_int), ("bp_variant", C.c_int),
                 ("staged_bins", C.c_uint), ("tuned", C.c_int), ("from_cache", C.c_int),
                 ("fp_us", C.c_float * 12), ("slab_us", C.c_float * 8), ("bp_us", C.c_float * 8),
-                ("ray_variant", C.c_int), ("ray_us", C.c_float * 2), ("staged_bins_bf16", C.c_uint)]
+                ("ray_variant", C.c_int), ("ray_us", C.c_float * 2), ("staged_bins_bf16", C.c_uint),
+                ("fp_variant_bf16", C.c_int), ("fp16_us", C.c_float * 2)]
 
 
 def _load() -> C.CDLL:
@@ -99,6 +100,7 @@ def _load() -> C.CDLL:
         "stt_bp_ray_scatter": [vp, vp, vp, vp, i, vp],
         "stt_gather_ceiling": [vp, vp, i, i, vp, vp, vp],
         "stt_fp_texture_ok": [vp, vp, vp],
+        "stt_fp_texture_ok_typed": [vp, vp, i, vp],
         "stt_sart_sweep_typed": [vp, vp, i, vp, vp, i, i, d, f, i, vp, vp, vp],
         "stt_bp_voxel_typed": [vp, vp, vp, i, d, f, i, vp],
         "stt_bp_ray_typed": [vp, vp, vp, i, f, i, vp],

@@ -175,6 +175,8 @@ class Context:
                 "staged_bins": t.staged_bins, "tuned": bool(t.tuned), "from_cache": bool(t.from_cache),
                 "fp_us": list(t.fp_us)[:12], "slab_us": list(t.slab_us)[:8], "bp_us": list(t.bp_us)[:3],
                 "ray_variant": t.ray_variant, "ray_us": list(t.ray_us), "staged_bins_bf16": t.staged_bins_bf16,
+                "fp_variant_bf16": t.fp_variant_bf16, "fp16_us": list(t.fp16_us),
+                "fp16": (lib.stt_tuning_variant_name(4, t.fp_variant_bf16) or b"").decode(),
                 "ray": (lib.stt_tuning_variant_name(3, t.ray_variant) or b"").decode(),
                 "fp": (lib.stt_tuning_variant_name(0, t.fp_variant) or b"").decode(),
                 "slab": (lib.stt_tuning_variant_name(1, t.slab_variant) or b"").decode(),
@@ -192,14 +194,18 @@ class Context:
         return self._tuning_dict(t)
 
     def set_tuning(self, fp_variant=0, slab_variant=0, bp_variant=0, staged_bins=0x1E0, ray_variant=None,
-                   staged_bins_bf16=None):
-        """ray_variant None keeps the context's current ray-scatter choice;
-        staged_bins_bf16 None takes staged_bins."""
+                   staged_bins_bf16=None, fp_variant_bf16=None):
+        """ray_variant and fp_variant_bf16 None keep the context's current
+        choices; staged_bins_bf16 None takes staged_bins."""
+        cur = self.get_tuning() if ray_variant is None or fp_variant_bf16 is None else None
         if ray_variant is None:
-            ray_variant = self.get_tuning()["ray_variant"]
+            ray_variant = cur["ray_variant"]
+        if fp_variant_bf16 is None:
+            fp_variant_bf16 = cur["fp_variant_bf16"]
         t = Tuning(int(fp_variant), int(slab_variant), int(bp_variant), int(staged_bins), 1, 0)
         t.ray_variant = int(ray_variant)
         t.staged_bins_bf16 = int(staged_bins if staged_bins_bf16 is None else staged_bins_bf16)
+        t.fp_variant_bf16 = int(fp_variant_bf16)
         self._chk(lib.stt_set_tuning(self._h, C.byref(t)))
 
     def fp_correction(self, vol, b, raylen_state, corr, view, stream=None):
@@ -234,10 +240,11 @@ class Context:
                                          _ptr(count) if count is not None else None, _stream(stream)))
 
     def fp_texture_ok(self, vol) -> bool:
-        """Whether the tld4 gather variants (fp_variant 10, 11) bind `vol` as
-        textures on this device (stt_fp_texture_ok); else they run as loads."""
+        """Whether the tld4 gather forms bind `vol` as textures on this device
+        (fp_variant 10, 11 for float32; fp_variant_bf16 1 for bfloat16;
+        stt_fp_texture_ok_typed); else they run as loads."""
         ok = C.c_int(0)
-        self._chk(lib.stt_fp_texture_ok(self._h, _ptr(vol), C.byref(ok)))
+        self._chk(lib.stt_fp_texture_ok_typed(self._h, _ptr(vol), _dtype_code(vol), C.byref(ok)))
         return bool(ok.value)
 
     def bp_ray_scatter(self, corr, contrib, wsum, view, stream=None):

@@ -90,18 +90,18 @@ __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__re
 
 // The ray sum through the textures of FpTex: the transposed copy's for
 // layout-1 views when there is one, as fp_ray_sum reads the arrays.
-template <int G = FP_GROUP, bool PK = false>
+template <int G = FP_GROUP, bool PK = false, typename T = float>
 __device__ __forceinline__ float fp_ray_sum_tex(const GeomDev &g, const ViewRec &v, const FpTex &tex, const Ray &r) {
     if (tex.z && v.layout == 1) {
         const unsigned long long t = tex.z;
         const int row = g.nz;
         return fp_ray_sum_with<G, PK>(
-            g, [=](int, const FpCell &c, float w[8]) { fp_corners_tex<2>(t, row, c, w); }, r, nullptr);
+            g, [=](int, const FpCell &c, float w[8]) { fp_corners_tex<2, T>(t, row, c, w); }, r, nullptr);
     }
     const unsigned long long t = tex.x;
     const int row = g.nx;
     return fp_ray_sum_with<G, PK>(
-        g, [=](int, const FpCell &c, float w[8]) { fp_corners_tex<0>(t, row, c, w); }, r, nullptr);
+        g, [=](int, const FpCell &c, float w[8]) { fp_corners_tex<0, T>(t, row, c, w); }, r, nullptr);
 }
 
 template <typename I, int G = FP_GROUP, bool PK = false, typename T>
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(32 * NW) k_fp_corr(const GeomDev g, const View
     float L, sum = 0.0f;
     if (r.tnear < r.tfar) {
         if constexpr (TX)
-            sum = fp_ray_sum_tex<G, PK>(g, vr, tex, r);
+            sum = fp_ray_sum_tex<G, PK, T>(g, vr, tex, r);
         else
             sum = fp_ray_sum<I, G, PK>(g, vr, vol, vol_t, r, nullptr);
         L = r.tfar - r.tnear;
@@ -530,21 +530,23 @@ bool tex_limits(TexLimits &l) {
     return true;
 }
 
-bool slices_fit(const TexLimits &l, const float *p, long long width, long long rows) {
-    const long long pitch = width * (long long)sizeof(float);
+bool slices_fit(const TexLimits &l, const void *p, long long width, long long rows, int esize) {
+    const long long pitch = width * (long long)esize;
     return p && width >= 2 && rows >= 2 && width <= l.width && rows <= l.height && pitch <= l.pitch &&
            !(l.pitch_align > 0 && pitch % l.pitch_align) && !(l.base_align > 0 && (uintptr_t)p % l.base_align);
 }
 
-// A point-sampled, clamped FP32 texture of `rows` rows of `width` texels over
-// linear memory; 0 where the limits do not admit it.
-unsigned long long slices_texture(const TexLimits &l, const float *p, long long width, long long rows) {
-    const long long pitch = width * (long long)sizeof(float);
-    if (!slices_fit(l, p, width, rows)) return 0;
+// A point-sampled, clamped texture of `rows` rows of `width` texels over
+// linear memory (FP32 texels, or 16-bit unsigned ones holding BF16 bits); 0
+// where the limits do not admit it.
+template <typename T>
+unsigned long long slices_texture(const TexLimits &l, const T *p, long long width, long long rows) {
+    const long long pitch = width * (long long)sizeof(T);
+    if (!slices_fit(l, p, width, rows, (int)sizeof(T))) return 0;
     cudaResourceDesc rd{};
     rd.resType = cudaResourceTypePitch2D;
-    rd.res.pitch2D.devPtr = const_cast<float *>(p);
-    rd.res.pitch2D.desc = cudaCreateChannelDesc<float>();
+    rd.res.pitch2D.devPtr = const_cast<T *>(p);
+    rd.res.pitch2D.desc = cudaCreateChannelDesc<T>();
     rd.res.pitch2D.width = (size_t)width;
     rd.res.pitch2D.height = (size_t)rows;
     rd.res.pitch2D.pitchInBytes = (size_t)pitch;
@@ -580,7 +582,15 @@ const char *fp_variant_name(int v) {
 
 bool is_tex_fp_variant(int fp_variant) { return fp_variant == 10 || fp_variant == 11; }
 
-bool make_fp_tex(const GeomDev &g, const float *vol, const float *vol_t, FpTex &t) {
+const char *fp16_variant_name(int v) {
+    static const char *names[kFp16Variants] = {"32x4 rays per block, 4 samples in flight",
+                                               "warps of 8x4 rays, 8 in flight, packed pairs, tld4 corners"};
+    return v >= 0 && v < kFp16Variants ? names[v] : "?";
+}
+
+namespace {
+template <typename T>
+bool make_fp_tex_any(const GeomDev &g, const T *vol, const T *vol_t, FpTex &t) {
     t = FpTex{};
     TexLimits l;
     if (!small_volume(g) || !tex_limits(l)) return false;
@@ -594,14 +604,25 @@ bool make_fp_tex(const GeomDev &g, const float *vol, const float *vol_t, FpTex &
     t.x = x;
     t.z = z;
     t.ok = 1;
+    t.esize = (int)sizeof(T);
     return true;
 }
+}  // namespace
 
-bool fp_tex_fits(const GeomDev &g, const float *vol) {
+bool make_fp_tex(const GeomDev &g, const float *vol, const float *vol_t, FpTex &t) {
+    return make_fp_tex_any(g, vol, vol_t, t);
+}
+
+bool make_fp_tex(const GeomDev &g, const unsigned short *vol, const unsigned short *vol_t, FpTex &t) {
+    return make_fp_tex_any(g, vol, vol_t, t);
+}
+
+bool fp_tex_fits(const GeomDev &g, const void *vol, int esize) {
     TexLimits l;
     if (!small_volume(g) || !tex_limits(l)) return false;
-    const float *aligned = reinterpret_cast<const float *>((uintptr_t)(l.base_align > 0 ? l.base_align : 256));
-    return slices_fit(l, vol, (long long)g.nx * g.ny, g.nz) && slices_fit(l, aligned, (long long)g.nz * g.ny, g.nx);
+    const void *aligned = reinterpret_cast<const void *>((uintptr_t)(l.base_align > 0 ? l.base_align : 256));
+    return slices_fit(l, vol, (long long)g.nx * g.ny, g.nz, esize) &&
+           slices_fit(l, aligned, (long long)g.nz * g.ny, g.nx, esize);
 }
 
 void destroy_fp_tex(FpTex &t) {
@@ -617,7 +638,7 @@ cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const float *
     const int skip = maps && maps->ok && maps->esize == 4 && (!vol_t || maps->has_z);
     // a texture variant whose textures are missing, or do not cover vol_t,
     // runs the load-based variant of the same shape
-    if (is_tex_fp_variant(fp_variant) && !(tex && tex->ok && (!vol_t || tex->z)))
+    if (is_tex_fp_variant(fp_variant) && !(tex && tex->ok && tex->esize == 4 && (!vol_t || tex->z)))
         fp_variant = fp_variant == 10 ? 4 : 8;
     FpTex tx = tex ? *tex : FpTex{};
     if (!vol_t) tx.z = 0;  // without the copy every view reads the volume, as the loads do
@@ -703,13 +724,21 @@ cudaError_t launch_correction(long long n, const unsigned short *b, const float 
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
                            const unsigned short *vol_t, const ViewSel &sel, const unsigned short *b_stack,
                            float *raylen_state, float *corr, cudaStream_t s, unsigned long long corr_surf,
-                           const FpSlabMaps *maps, int *status) {
+                           const FpSlabMaps *maps, int *status, int fp_variant16, const FpTex *tex) {
     typedef unsigned short U;
     const int skip = maps && maps->ok && maps->esize == 2 && (!vol_t || maps->has_z);
     if (skip) {
         cudaError_t e = launch_fp_corr_slab(g, views, *maps, vol, vol_t, sel, b_stack, raylen_state, corr, s,
                                             corr_surf, status);
         if (e != cudaSuccess) return e;
+    }
+    if (fp_variant16 == 1 && tex && tex->ok && tex->esize == 2 && (!vol_t || tex->z) && small_volume(g)) {
+        FpTex tx = *tex;
+        if (!vol_t) tx.z = 0;
+        constexpr int WX = 8, NW = 4, TH = (32 / WX) * NW;
+        k_fp_corr<int, WX, NW, 8, true, U, U, true><<<dim3((g.W + WX - 1) / WX, (g.H + TH - 1) / TH, 1), 32 * NW, 0, s>>>(
+            g, views, vol, vol_t, sel, b_stack, raylen_state, corr, corr_surf, skip, tx);
+        return cudaGetLastError();
     }
     if (small_volume(g))
         k_fp_corr<int, 32, 4, FP_GROUP, false, U, U><<<ray_grid(g, 1), 128, 0, s>>>(

@@ -388,13 +388,18 @@ stt_status stt_fp_correction(stt_ctx *ctx, const float *vol, const float *b, flo
     return STT_OK;
 }
 
-stt_status stt_fp_texture_ok(stt_ctx *ctx, const float *vol, int *ok) {
+stt_status stt_fp_texture_ok_typed(stt_ctx *ctx, const void *vol, int dtype, int *ok) {
     stt_status st = need_geom(ctx);
     if (st) return st;
     if (!vol || !ok) return fail(ctx, STT_ERR_INVALID, "null vol or ok");
+    if (dtype != STT_DTYPE_F32 && dtype != STT_DTYPE_BF16) return fail(ctx, STT_ERR_INVALID, "unknown dtype");
     if ((st = set_device(ctx))) return st;
-    *ok = stt::fp_tex_fits(ctx->g, vol) ? 1 : 0;
+    *ok = stt::fp_tex_fits(ctx->g, vol, dtype == STT_DTYPE_BF16 ? 2 : 4) ? 1 : 0;
     return STT_OK;
+}
+
+stt_status stt_fp_texture_ok(stt_ctx *ctx, const float *vol, int *ok) {
+    return stt_fp_texture_ok_typed(ctx, vol, STT_DTYPE_F32, ok);
 }
 
 stt_status stt_gather_ceiling(stt_ctx *ctx, const float *vol, int view, int packed, float *out, int *count,
@@ -533,7 +538,8 @@ static cudaError_t sweep_fp_corr(stt_ctx *ctx, const unsigned short *vol, const 
                                  const stt::ViewSel &sel, const unsigned short *stack, float *rl, cudaStream_t s) {
     stt::FpSlabMaps maps{};  // ok = 0: every view gathers, one launch
     if (staged_mask(ctx, vol)) stt::make_fp_slab_maps(ctx->g, vol, volt, maps, ctx->tuning.slab);
-    return stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, stack, rl, ctx->corr, s, 0, &maps, ctx->status);
+    return stt::launch_fp_corr(ctx->g, ctx->views_d, vol, volt, sel, stack, rl, ctx->corr, s, 0, &maps, ctx->status,
+                               ctx->tuning.fp16, stt::ctx_fp_tex(ctx, vol, volt));
 }
 
 template <typename T>

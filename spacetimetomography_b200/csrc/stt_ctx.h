@@ -49,8 +49,8 @@ struct stt_ctx {
     // Kept until stt_destroy, so a stream capture of an entry point that
     // bound one stays valid.
     struct FpTexEntry {
-        const float *vol, *volt;
-        int nx, ny, nz;
+        const void *vol, *volt;
+        int nx, ny, nz, esize;
         stt::FpTex tex;
     };
     static constexpr int kFpTexCache = 32;
@@ -70,4 +70,6 @@ stt_status apply_staged_bins(stt_ctx *ctx);
 const FpTex *ctx_fp_tex(stt_ctx *ctx, const float *vol, const float *vol_t);
 // The same whatever the tuned variant (nullptr only when the cache is full).
 const FpTex *ctx_fp_tex_any(stt_ctx *ctx, const float *vol, const float *vol_t);
+// The BF16 volume's textures when the tuned BF16 gather form is the tld4 one.
+const FpTex *ctx_fp_tex(stt_ctx *ctx, const unsigned short *vol, const unsigned short *vol_t);
 }  // namespace stt

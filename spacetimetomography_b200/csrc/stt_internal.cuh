@@ -301,12 +301,23 @@ __device__ __forceinline__ void fp_corners(const T *__restrict__ src, const Stri
 // of two neighbouring slices; the second gather, one row of `row` texels on,
 // is the y+1 pair.  The cell's base is at most dims-2 on every axis, so no
 // gather leaves the array or crosses into another row of slices.
-template <int FAST>
+// T: the texels' storage; BF16 (unsigned short bits, a 16-bit unsigned
+// texture) is widened exactly to FP32 as ld_voxel does.
+__device__ __forceinline__ float4 gather_texels(unsigned long long tex, float u, float v, const float *) {
+    return tex2Dgather<float4>(tex, u, v, 0);
+}
+__device__ __forceinline__ float4 gather_texels(unsigned long long tex, float u, float v, const unsigned short *) {
+    const ushort4 r = tex2Dgather<ushort4>(tex, u, v, 0);
+    return make_float4(__uint_as_float((unsigned)r.x << 16), __uint_as_float((unsigned)r.y << 16),
+                       __uint_as_float((unsigned)r.z << 16), __uint_as_float((unsigned)r.w << 16));
+}
+
+template <int FAST, typename T = float>
 __device__ __forceinline__ void fp_corners_tex(unsigned long long tex, int row, const FpCell &c, float v[8]) {
     const int u = FAST == 0 ? c.ix + row * c.iy : c.iz + row * c.iy;
     const float fv = (float)(FAST == 0 ? c.iz : c.ix) + 1.0f;
-    const float4 a = tex2Dgather<float4>(tex, (float)u + 1.0f, fv, 0);
-    const float4 b = tex2Dgather<float4>(tex, (float)(u + row) + 1.0f, fv, 0);
+    const float4 a = gather_texels(tex, (float)u + 1.0f, fv, (const T *)nullptr);
+    const float4 b = gather_texels(tex, (float)(u + row) + 1.0f, fv, (const T *)nullptr);
     if (FAST == 0) {  // u along x, v along z
         v[0] = a.w, v[1] = a.z, v[4] = a.x, v[5] = a.y;
         v[2] = b.w, v[3] = b.z, v[6] = b.x, v[7] = b.y;

@@ -36,6 +36,7 @@ int grid_stride_blocks(long long n, int threads);
 constexpr int kFpVariants = 12, kSlabVariants = 8, kBpVariants = 3, kRayVariants = 2;
 struct Tuning {
     int fp = 0, slab = 0, bp = 0, ray = 0;
+    int fp16 = 0;  // the BF16-stored volume's gather form (fp16_variant_name)
 };
 const char *fp_variant_name(int v);
 const char *slab_variant_name(int v);
@@ -76,10 +77,11 @@ cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const Fp
                                 const unsigned short *b_stack, float *raylen_state, float *corr, cudaStream_t s,
                                 unsigned long long corr_surf, int *status);
 // Texture objects of the gather variants that fetch corners with tld4: the
-// FP32 volume as a pitch-linear 2D texture whose rows are its z slices (width
+// volume as a pitch-linear 2D texture whose rows are its z slices (width
 // nx*ny texels, nz rows) and its z-fastest copy likewise (rows the x slices;
-// z = 0 without a copy).  Point sampling of an FP32 texture returns stored
-// values exactly, so the samples are those of the loads they replace.
+// z = 0 without a copy); FP32 texels, or for a BF16-stored volume 16-bit
+// unsigned texels holding its bits.  Point sampling returns stored values
+// exactly, so the samples are those of the loads they replace.
 // make_fp_tex returns false (and creates nothing) where the device's limits
 // on linear 2D textures do not admit the arrays: a row of more than the
 // maximum width or pitch, more rows than the maximum height, a base not
@@ -88,12 +90,15 @@ cudaError_t launch_fp_corr_slab(const GeomDev &g, const ViewRec *views, const Fp
 struct FpTex {
     unsigned long long x = 0, z = 0;
     int ok = 0;
+    int esize = 0;  // bytes per texel: 4 (FP32) or 2 (BF16)
 };
 bool is_tex_fp_variant(int fp_variant);
 bool make_fp_tex(const GeomDev &g, const float *vol, const float *vol_t, FpTex &t);
-// Whether make_fp_tex admits `vol` and a z-fastest copy at an aligned base on
-// this device (checks the limits only; creates nothing).
-bool fp_tex_fits(const GeomDev &g, const float *vol);
+bool make_fp_tex(const GeomDev &g, const unsigned short *vol, const unsigned short *vol_t, FpTex &t);
+// Whether make_fp_tex admits `vol` (esize bytes per voxel) and a z-fastest
+// copy at an aligned base on this device (checks the limits only; creates
+// nothing).
+bool fp_tex_fits(const GeomDev &g, const void *vol, int esize);
 void destroy_fp_tex(FpTex &t);
 // Forward projection of one view fused with the SART correction.  With usable
 // slab maps, staged views run in the slab-staged kernel and the others in the
@@ -123,10 +128,17 @@ cudaError_t launch_transpose_for_view(const GeomDev &g, const ViewRec *views, co
 // The fused forward projection of a BF16 volume against a BF16 sinogram:
 // with usable BF16 slab maps the staged views run in the slab kernel (BF16
 // boxes), the others in the gather kernel; without them every view gathers.
+// The gather kernel loads its corners (fp_variant16 0: 32x4 rays, 4 samples
+// in flight) or, with usable BF16 textures `tex`, gathers them with tld4
+// (fp_variant16 1: warps of 8x4 rays, 8 samples in flight in packed pairs);
+// the same bits either way.
+constexpr int kFp16Variants = 2;
+const char *fp16_variant_name(int v);
 cudaError_t launch_fp_corr(const GeomDev &g, const ViewRec *views, const unsigned short *vol,
                            const unsigned short *vol_t, const ViewSel &sel, const unsigned short *b_stack,
                            float *raylen_state, float *corr, cudaStream_t s, unsigned long long corr_surf = 0,
-                           const FpSlabMaps *maps = nullptr, int *status = nullptr);
+                           const FpSlabMaps *maps = nullptr, int *status = nullptr, int fp_variant16 = 0,
+                           const FpTex *tex = nullptr);
 cudaError_t launch_correction(long long n, const unsigned short *b, const float *ax, const float *raylen,
                               float *corr, cudaStream_t s);
 cudaError_t launch_correction(long long n, const float *b, const float *ax, const float *raylen,

@@ -138,7 +138,7 @@ struct stt_solver {
     long long phase_launches[2] = {0, 0};
     std::vector<LayeredTex> corr_tex;  // batched modes: per frame, the correction as a texture
     std::vector<stt::FpSlabMaps> fpmaps;  // batched modes: per frame, TMA maps of the volume and its copy
-    std::vector<stt::FpTex> fptex;  // batched modes, FP32, a tld4 gather variant: per frame, the volume's textures
+    std::vector<stt::FpTex> fptex;  // batched modes, a tld4 gather form: per frame, the volume's textures
     std::string err;
 };
 
@@ -271,7 +271,8 @@ int fp_corr(stt_solver *s, int f, const unsigned short *vol, const unsigned shor
             const unsigned short *stack, float *rl, float *corr, cudaStream_t cs, unsigned long long surf,
             cudaError_t &e) {
     const stt::FpSlabMaps *maps = s->fpmaps.empty() ? nullptr : &s->fpmaps[f];
-    e = stt::launch_fp_corr(*s->g, s->views, vol, volt, sel, stack, rl, corr, cs, surf, maps, s->status);
+    e = stt::launch_fp_corr(*s->g, s->views, vol, volt, sel, stack, rl, corr, cs, surf, maps, s->status,
+                            s->ctx->tuning.fp16, s->fptex.empty() ? nullptr : &s->fptex[f]);
     return (maps && maps->ok) ? 2 : 1;
 }
 
@@ -539,6 +540,12 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
         s->fptex.resize(F);  // where they cannot be made, ok stays 0 and the loads run
         for (int f = 0; f < F; ++f)
             stt::make_fp_tex(*g, s->st.vol + f * s->n, static_cast<float *>(s->volt) + f * s->n, s->fptex[f]);
+    }
+    if (cfg->mode != STT_SOLVE_PLAIN && cfg->storage == STT_DTYPE_BF16 && ctx->tuning.fp16 == 1) {
+        s->fptex.resize(F);
+        for (int f = 0; f < F; ++f)
+            stt::make_fp_tex(*g, reinterpret_cast<const unsigned short *>(s->st.vol) + f * s->n,
+                             static_cast<unsigned short *>(s->volt) + f * s->n, s->fptex[f]);
     }
     if (cfg->mode != STT_SOLVE_PLAIN && cfg->bp_mode == 0) {
         s->corr_tex.resize(F);

@@ -57,10 +57,12 @@ struct Scratch {
     stt::ViewRec *tv = nullptr;
     cudaArray_t arr = nullptr;
     cudaTextureObject_t tex = 0;
-    stt::FpTex fptex;  // the textures of the tld4 gather variants over vol and volt
+    stt::FpTex fptex;    // the textures of the tld4 gather variants over vol and volt
+    stt::FpTex fptex16;  // the same over vol16 and volt16
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     ~Scratch() {
         stt::destroy_fp_tex(fptex);
+        stt::destroy_fp_tex(fptex16);
         cudaFree(vol);
         cudaFree(volt);
         cudaFree(b);
@@ -124,15 +126,28 @@ const FpTex *ctx_fp_tex(stt_ctx *ctx, const float *vol, const float *vol_t) {
     return is_tex_fp_variant(ctx->tuning.fp) ? ctx_fp_tex_any(ctx, vol, vol_t) : nullptr;
 }
 
-const FpTex *ctx_fp_tex_any(stt_ctx *ctx, const float *vol, const float *vol_t) {
+namespace {
+template <typename T>
+const FpTex *cached_tex(stt_ctx *ctx, const T *vol, const T *vol_t) {
     const GeomDev &g = ctx->g;
+    const int es = (int)sizeof(T);
     for (const auto &e : ctx->fp_tex)
-        if (e.vol == vol && e.volt == vol_t && e.nx == g.nx && e.ny == g.ny && e.nz == g.nz) return &e.tex;
+        if (e.vol == vol && e.volt == vol_t && e.nx == g.nx && e.ny == g.ny && e.nz == g.nz && e.esize == es)
+            return &e.tex;
     if ((int)ctx->fp_tex.size() >= stt_ctx::kFpTexCache) return nullptr;
-    stt_ctx::FpTexEntry e{vol, vol_t, g.nx, g.ny, g.nz, FpTex{}};
+    stt_ctx::FpTexEntry e{vol, vol_t, g.nx, g.ny, g.nz, es, FpTex{}};
     make_fp_tex(g, vol, vol_t, e.tex);  // where it fails, tex.ok = 0 is cached too: the loads run
     ctx->fp_tex.push_back(e);
     return &ctx->fp_tex.back().tex;
+}
+}  // namespace
+
+const FpTex *ctx_fp_tex_any(stt_ctx *ctx, const float *vol, const float *vol_t) {
+    return cached_tex(ctx, vol, vol_t);
+}
+
+const FpTex *ctx_fp_tex(stt_ctx *ctx, const unsigned short *vol, const unsigned short *vol_t) {
+    return ctx->tuning.fp16 == 1 ? cached_tex(ctx, vol, vol_t) : nullptr;
 }
 
 }  // namespace stt
@@ -143,7 +158,8 @@ const char *stt_tuning_variant_name(int kernel, int variant) {
     const char *s = kernel == 0 ? stt::fp_variant_name(variant)
                     : kernel == 1 ? stt::slab_variant_name(variant)
                     : kernel == 2 ? stt::bp_variant_name(variant)
-                    : kernel == 3 ? stt::ray_variant_name(variant) : "?";
+                    : kernel == 3 ? stt::ray_variant_name(variant)
+                    : kernel == 4 ? stt::fp16_variant_name(variant) : "?";
     return s[0] == '?' ? nullptr : s;
 }
 
@@ -155,6 +171,7 @@ stt_status stt_get_tuning(const stt_ctx *ctx, stt_tuning *out) {
     out->slab_variant = ctx->tuning.slab;
     out->bp_variant = ctx->tuning.bp;
     out->ray_variant = ctx->tuning.ray;
+    out->fp_variant_bf16 = ctx->tuning.fp16;
     out->staged_bins = ctx->staged_bins;
     out->staged_bins_bf16 = ctx->staged_bins16;
     out->tuned = ctx->tuned ? 1 : 0;
@@ -167,7 +184,7 @@ stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t) {
     if (t->fp_variant < 0 || t->fp_variant >= stt::kFpVariants || t->slab_variant < 0 ||
         t->slab_variant >= stt::kSlabVariants || t->bp_variant < 0 || t->bp_variant >= stt::kBpVariants ||
         t->ray_variant < 0 || t->ray_variant >= stt::kRayVariants || (t->staged_bins >> 9) != 0 ||
-        (t->staged_bins_bf16 >> 9) != 0) {
+        (t->staged_bins_bf16 >> 9) != 0 || t->fp_variant_bf16 < 0 || t->fp_variant_bf16 >= stt::kFp16Variants) {
         ctx->err = "stt_set_tuning: a variant or staged_bins out of range";
         return STT_ERR_INVALID;
     }
@@ -180,6 +197,7 @@ stt_status stt_set_tuning(stt_ctx *ctx, const stt_tuning *t) {
     ctx->tuning.slab = t->slab_variant;
     ctx->tuning.bp = t->bp_variant;
     ctx->tuning.ray = t->ray_variant;
+    ctx->tuning.fp16 = t->fp_variant_bf16;
     ctx->staged_bins = t->staged_bins;
     ctx->staged_bins16 = t->staged_bins_bf16;
     ctx->tuned = true;
@@ -348,10 +366,12 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
     } else {
         t.staged_bins = 0x1E0u;  // irrelevant: without slab maps every view gathers
     }
-    // BF16 storage: the gather kernel against the slab kernel's BF16 box (the
-    // box just chosen) per class; a BF16 volume's gathers move half the bytes,
+    // BF16 storage: per class the gather kernel's two forms (loads, and tld4
+    // gathers of 16-bit textures where they bind) and the slab kernel's BF16
+    // box (the box just chosen); a BF16 volume's gathers move half the bytes,
     // so the faster projector can differ from the FP32 choice
     t.staged_bins_bf16 = 0x1E0u;  // irrelevant where the BF16 maps do not apply
+    t.fp_variant_bf16 = 0;
     {
         if ((e = cudaMalloc(&sc.vol16, n * sizeof(unsigned short))) ||
             (e = cudaMalloc(&sc.volt16, n * sizeof(unsigned short))) ||
@@ -360,44 +380,64 @@ stt_status stt_autotune(stt_ctx *ctx, stt_tuning *out, void *stream) {
             (e = cudaMemsetAsync(sc.volt16, 0x3F, n * sizeof(unsigned short), s)) ||
             (e = cudaMemsetAsync(sc.b16, 0, npix * sizeof(unsigned short), s)))
             return fail(e, "BF16 scratch");
+        stt::make_fp_tex(g, sc.vol16, sc.volt16, sc.fptex16);  // where it fails, ok = 0: loads only
         stt::FpSlabMaps m16;
-        if (stt::make_fp_slab_maps(g, sc.vol16, sc.volt16, m16, t.slab_variant)) {
+        const bool maps16 = stt::make_fp_slab_maps(g, sc.vol16, sc.volt16, m16, t.slab_variant);
+        float tg16[stt::kFp16Variants][9] = {}, ts16[9] = {};
+        float t_idle16 = 0.0f;
+        for (int b = 0; b < 9; ++b) {
+            if (rep[b] < 0) continue;
+            stt::ViewRec two[2] = {ctx->views_h[rep[b]], ctx->views_h[rep[b]]};
+            two[0].staged16 = 0;
+            two[1].staged16 = 1;
+            if ((e = cudaMemcpyAsync(sc.tv, two, sizeof two, cudaMemcpyHostToDevice, s)) ||
+                (e = cudaStreamSynchronize(s)))
+                return fail(e, "view copy");
+            for (int fv = 0; fv < stt::kFp16Variants; ++fv) {
+                if (fv == 1 && !sc.fptex16.ok) continue;
+                e = time_us(sc, s, [&] {
+                    return stt::launch_fp_corr(g, sc.tv, sc.vol16, sc.volt16, stt::ViewSel{0, nullptr, 0, 0}, sc.b16,
+                                               sc.rl, sc.corr, s, 0, nullptr, ctx->status, fv, &sc.fptex16);
+                }, tg16[fv][b]);
+                if (e) return fail(e, "BF16 gather projector");
+            }
+            if (!maps16) continue;
+            e = time_us(sc, s, [&] {
+                return stt::launch_fp_corr_slab(g, sc.tv, m16, sc.vol16, sc.volt16, stt::ViewSel{1, nullptr, 0, 1},
+                                                sc.b16, sc.rl, sc.corr, s, 0, ctx->status);
+            }, ts16[b]);
+            if (e) return fail(e, "BF16 slab projector");
+            if (t_idle16 == 0.0f) {
+                e = time_us(sc, s, [&] {
+                    return stt::launch_fp_corr_slab(g, sc.tv, m16, sc.vol16, sc.volt16, stt::ViewSel{0, nullptr, 0, 0},
+                                                    sc.b16, sc.rl, sc.corr, s, 0, ctx->status);
+                }, t_idle16);
+                if (e) return fail(e, "idle BF16 slab launch");
+            }
+        }
+        // the gather form with the least time over all views, then the classes
+        // the slab kernel takes from it
+        double best16 = 1e300;
+        for (int fv = 0; fv < stt::kFp16Variants; ++fv) {
+            if (fv == 1 && !sc.fptex16.ok) continue;  // not timed: fp16_us stays 0
+            double tot = 0.0, w = 0.0;
+            for (int b = 0; b < 9; ++b)
+                if (rep[b] >= 0) tot += (double)count[b] * tg16[fv][b], w += count[b];
+            t.fp16_us[fv] = (float)(tot / w);
+            if (tot < best16) best16 = tot, t.fp_variant_bf16 = fv;
+        }
+        if (maps16) {
             t.staged_bins_bf16 = 0;
             double split = 0.0, gather_all = 0.0;
-            float t_idle16 = 0.0f;
             for (int b = 0; b < 9; ++b) {
                 if (rep[b] < 0) {
                     t.staged_bins_bf16 |= 0x1E0u & (1u << b);
                     continue;
                 }
-                stt::ViewRec two[2] = {ctx->views_h[rep[b]], ctx->views_h[rep[b]]};
-                two[0].staged16 = 0;
-                two[1].staged16 = 1;
-                if ((e = cudaMemcpyAsync(sc.tv, two, sizeof two, cudaMemcpyHostToDevice, s)) ||
-                    (e = cudaStreamSynchronize(s)))
-                    return fail(e, "view copy");
-                float tg16 = 0.0f, ts16 = 0.0f;
-                e = time_us(sc, s, [&] {
-                    return stt::launch_fp_corr(g, sc.tv, sc.vol16, sc.volt16, stt::ViewSel{0, nullptr, 0, 0}, sc.b16,
-                                               sc.rl, sc.corr, s, 0, nullptr, ctx->status);
-                }, tg16);
-                if (e) return fail(e, "BF16 gather projector");
-                e = time_us(sc, s, [&] {
-                    return stt::launch_fp_corr_slab(g, sc.tv, m16, sc.vol16, sc.volt16, stt::ViewSel{1, nullptr, 0, 1},
-                                                    sc.b16, sc.rl, sc.corr, s, 0, ctx->status);
-                }, ts16);
-                if (e) return fail(e, "BF16 slab projector");
-                if (t_idle16 == 0.0f) {
-                    e = time_us(sc, s, [&] {
-                        return stt::launch_fp_corr_slab(g, sc.tv, m16, sc.vol16, sc.volt16,
-                                                        stt::ViewSel{0, nullptr, 0, 0}, sc.b16, sc.rl, sc.corr, s, 0,
-                                                        ctx->status);
-                    }, t_idle16);
-                    if (e) return fail(e, "idle BF16 slab launch");
-                }
-                if (ts16 < tg16) t.staged_bins_bf16 |= 1u << b;
-                split += (double)count[b] * (std::fmin(ts16, tg16) + t_idle16);
-                gather_all += (double)count[b] * tg16;
+                const float tg = tg16[t.fp_variant_bf16][b];
+                if (ts16[b] < tg) t.staged_bins_bf16 |= 1u << b;
+                split += (double)count[b] * (std::fmin(ts16[b], tg) + t_idle16);
+                gather_all += (double)count[b] * tg;
             }
             if (split >= gather_all) t.staged_bins_bf16 = 0;  // (as for FP32 above)
         }

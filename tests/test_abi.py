@@ -116,21 +116,22 @@ def test_flow_argument_checks_without_gpu(lib):
 
 
 def test_tuning_variant_names_and_struct_layout(lib):
-    """stt_tuning_variant_name names every variant of the four tuned kernels
+    """stt_tuning_variant_name names every variant of the five tuned kernels
     and returns NULL past them; the ctypes stt_tuning matches the header's
     layout (the host reads the tuner's report through it)."""
     from spacetimetomography_b200._lib import SolveCfg, Instance, Tuning
 
-    counts = {0: 12, 1: 8, 2: 3, 3: 2}  # gather projector, slab projector, voxel BP, ray-BP scatter
+    # gather projector, slab projector, voxel BP, ray-BP scatter, BF16 gather projector
+    counts = {0: 12, 1: 8, 2: 3, 3: 2, 4: 2}
     for kernel, n in counts.items():
         names = [lib.stt_tuning_variant_name(kernel, v) for v in range(n)]
         assert all(names) and len(set(names)) == n, (kernel, names)
         assert lib.stt_tuning_variant_name(kernel, n) is None
         assert lib.stt_tuning_variant_name(kernel, -1) is None
-    assert lib.stt_tuning_variant_name(4, 0) is None
+    assert lib.stt_tuning_variant_name(5, 0) is None
     # int fp, slab, bp; unsigned bins; int tuned, from_cache; float fp_us[12], slab_us[8], bp_us[8];
-    # int ray_variant; float ray_us[2]; unsigned staged_bins_bf16
-    assert C.sizeof(Tuning) == 6 * 4 + (12 + 8 + 8) * 4 + 4 + 2 * 4 + 4
+    # int ray_variant; float ray_us[2]; unsigned staged_bins_bf16; int fp_variant_bf16; float fp16_us[2]
+    assert C.sizeof(Tuning) == 6 * 4 + (12 + 8 + 8) * 4 + 4 + 2 * 4 + 4 + 4 + 2 * 4
     assert Tuning.ray_variant.offset == 6 * 4 + 28 * 4
     assert SolveCfg.storage.offset > SolveCfg.autotune.offset and Instance.storage.offset > Instance.autotune.offset
 

@@ -23,18 +23,23 @@ def bf16_problem(seed):
     return scan, angles, st, gmax
 
 
-def run_bf16(scan, angles, st, gmax, mode, bp_mode, iters, cuda, seed=42):
+def run_bf16(scan, angles, st, gmax, mode, bp_mode, iters, cuda, seed=42, fp16=None):
     import torch
 
     import spacetimetomography_b200 as stt
 
     ctx = stt.Context(0)
     ctx.set_geometry(scan.dims, scan.sp, scan.det, scan.ds, scan.sid, scan.sdd, angles, scan.off)
+    if fp16 is not None:
+        ctx.set_tuning(0, 0, 0, staged_bins=0x1E0, fp_variant_bf16=fp16)
     g = {}
     for k, v in st.items():
         t = torch.from_numpy(np.ascontiguousarray(v)).to(cuda)
         g[k] = t.to(torch.bfloat16) if k in PRIMAL else t  # exact: the values are BF16 already
     pd = stt.PdParams(sigma=0.1125, tau=1.0, tv_w=0.05, tp_w=0.3, bc_w=0.2, huber_factor=0.9, gmax=gmax, cut=PD_CUT)
+    if fp16:
+        # frame f starts f * N^3 * 2 bytes on, a multiple of the texture alignment here
+        assert ctx.fp_texture_ok(g["vol"]) and (N ** 3 * 2) % 512 == 0
     s = stt.Solver(ctx, g, F, V, pd, alpha=0.3, bp_mode=bp_mode, roi_cut=ROI_CUT, seed=seed, mode=mode,
                    storage="bf16")
     s.iterate(iters)
@@ -74,6 +79,19 @@ def test_bf16_modes_agree(cuda, bp_mode):
                 np.testing.assert_array_equal(res[m][k], base[k], err_msg=k)
             else:  # float atomics: a sum order can flip a BF16 rounding
                 assert ob.rel_l2(res[m][k], base[k]) < 5e-3, k
+
+
+def test_bf16_texture_gathers_leave_the_solve_unchanged(cuda):
+    """The BF16 solve with the gather projector's tld4 form (16-bit textures,
+    fp_variant_bf16 1) gives the bits of its load form, in the graph mode."""
+    import spacetimetomography_b200 as stt
+
+    scan, angles, st, gmax = bf16_problem(5)
+    a = run_bf16(scan, angles, st, gmax, stt.SOLVE_GRAPH, 0, 2, cuda, fp16=0)
+    b = run_bf16(scan, angles, st, gmax, stt.SOLVE_GRAPH, 0, 2, cuda, fp16=1)
+    for k in ("vol", "xbar", "xprev", "ytv", "ytp", "ybc"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    assert np.abs(a["vol"]).max() > 0
 
 
 @pytest.mark.parametrize("bp_mode", [0, 1])
@@ -169,13 +187,15 @@ def _bf16(t):
 # (40, 36, 44): nz is not a multiple of 8, so the BF16 sweep gathers every
 # view; (48, 40, 56): the BF16 slab maps apply and the oblique views go
 # through the slab-staged kernel's BF16 boxes
+@pytest.mark.parametrize("fp16", [0, 1])
 @pytest.mark.parametrize("dims", [(40, 36, 44), (48, 40, 56)])
 @pytest.mark.parametrize("bp_mode", [0, 1])
-def test_bf16_sart_sweep_equals_rounded_fp32_views(cuda, bp_mode, dims):
+def test_bf16_sart_sweep_equals_rounded_fp32_views(cuda, bp_mode, dims, fp16):
     """stt_sart_sweep_typed(BF16) against the FP32 sweep run one view at a time
     on the widened volume, rounded to BF16 after each view: the same bits with
-    voxel BP (the BF16 gather and slab projectors add what the FP32 ones do),
-    within a few rounding flips with ray BP (float atomics)."""
+    voxel BP (the BF16 gather projector, by loads or by tld4 gathers of 16-bit
+    textures (fp16), and the slab projector add what the FP32 ones do), within
+    a few rounding flips with ray BP (float atomics)."""
     import torch
 
     import spacetimetomography_b200 as stt
@@ -195,6 +215,9 @@ def test_bf16_sart_sweep_equals_rounded_fp32_views(cuda, bp_mode, dims):
     perm = stt.permutation(3, V)
     gmax = float(proj.max()) / 4
     a = start.clone()
+    ctx.set_tuning(0, 0, 0, staged_bins=0x1E0, fp_variant_bf16=fp16)
+    if fp16:
+        assert ctx.fp_texture_ok(a)  # the texture form really runs
     rl = torch.zeros(scan.det[::-1], device=cuda)
     ctx.sart_sweep(a, proj16, perm, 0.3, gmax, bp_mode, rl)
     b = start.float()
