@@ -1522,7 +1522,7 @@ def run_batch_only(args):
                          "cache_hits": sum(c["from_cache"] for c in choices),
                          "fp_variant_counts": np.bincount([c["fp_variant"] for c in choices], minlength=10).tolist(),
                          "slab_variant_counts": np.bincount([c["slab_variant"] for c in choices], minlength=8).tolist(),
-                         "bp_variant_counts": np.bincount([c["bp_variant"] for c in choices], minlength=3).tolist(),
+                         "bp_variant_counts": np.bincount([c["bp_variant"] for c in choices], minlength=5).tolist(),
                          "first_instances": [{k: c[k] for k in ("fp", "slab", "bp", "staged_bins")}
                                              for c in choices[:4]]}}
     print(json.dumps(line), flush=True)

@@ -123,7 +123,9 @@ stt_status stt_set_geometry(stt_ctx *ctx, const stt_geometry *g);
  *                until stt_destroy; where the device's texture limits do not
  *                admit the array, the load-based variant of the same shape runs);
  *   slab_variant the box the slab-staged projector stages with TMA;
- *   bp_variant   the column length of the voxel backprojection (solver);
+ *   bp_variant   the column length of the voxel backprojection (solver), and
+ *                whether each column's voxels are first prefetched into L2
+ *                (for volumes larger than L2);
  *   staged_bins  bit b set: views whose central ray is 5b to 5b+5 degrees off
  *                the nearest of the x and z axes (bit 8: 40 to 45) are
  *                projected by the slab-staged kernel, the others by the gather

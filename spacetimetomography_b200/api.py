@@ -173,7 +173,7 @@ class Context:
     def _tuning_dict(t: Tuning) -> dict:
         return {"fp_variant": t.fp_variant, "slab_variant": t.slab_variant, "bp_variant": t.bp_variant,
                 "staged_bins": t.staged_bins, "tuned": bool(t.tuned), "from_cache": bool(t.from_cache),
-                "fp_us": list(t.fp_us)[:12], "slab_us": list(t.slab_us)[:8], "bp_us": list(t.bp_us)[:3],
+                "fp_us": list(t.fp_us)[:12], "slab_us": list(t.slab_us)[:8], "bp_us": list(t.bp_us)[:5],
                 "ray_variant": t.ray_variant, "ray_us": list(t.ray_us), "staged_bins_bf16": t.staged_bins_bf16,
                 "fp_variant_bf16": t.fp_variant_bf16, "fp16_us": list(t.fp16_us),
                 "fp16": (lib.stt_tuning_variant_name(4, t.fp_variant_bf16) or b"").decode(),

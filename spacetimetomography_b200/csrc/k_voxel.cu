@@ -147,7 +147,14 @@ constexpr int BP_COL = 16;
 // by texture latency, so the extra warps pay (10 blocks: 104.1 ms per
 // iteration of the 10 x 256^3 solve against 106.6 ms with the compiler's
 // 52 registers and 9 blocks).
-template <int K = BP_COL, typename T = float>
+//
+// PF: before the walk, every thread asks L2 for its column's K voxels
+// (prefetch.global.L2: no register, no scoreboard).  Where the volume does not
+// fit in L2 (512^3 FP32 is 512 MiB against 126 MB), the walk's one load per
+// voxel otherwise waits for HBM with a single load in flight per thread, and
+// ten blocks of them keep too few bytes in flight to cover HBM latency.  The
+// values read, and so the bits written, are the same.
+template <int K = BP_COL, typename T = float, bool PF = false>
 __global__ void __launch_bounds__(128, 10) k_bp_voxel_cols(const GeomDev g, const ViewRec *__restrict__ views,
                                                        const ViewSel sel, T *__restrict__ vol, float alpha,
                                                        float gmax, unsigned long long tex) {
@@ -166,6 +173,10 @@ __global__ void __launch_bounds__(128, 10) k_bp_voxel_cols(const GeomDev g, cons
     const float upx = bp_pixel(g.cx, bp_cam(v, 0, fx, (float)y0, fz), ndepth, g.sdd_ds);
     if (!(upx >= 2.0f && upx < (float)(g.W - 2))) return;
     const int px = (int)upx;
+    if (PF) {
+        const T *col = vol + x + (size_t)z * g.nx * g.ny;
+        for (int y = y0; y < y1; ++y) asm volatile("prefetch.global.L2 [%0];" ::"l"(col + (size_t)y * g.nx));
+    }
     float wx[4];
     bp_weights(upx - (float)px, wx);
     float R[4][4];  // R[a][b]: column px-1+a, row pyc-1+b
@@ -380,11 +391,11 @@ cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, c
 }
 
 namespace {
-template <int K, typename T>
+template <int K, typename T, bool PF = false>
 void bp_cols(const GeomDev &g, const ViewRec *views, const ViewSel &sel, T *vol, float alpha, float gmax,
              cudaStream_t s, unsigned long long tex) {
-    k_bp_voxel_cols<K, T><<<dim3((g.nx + 127) / 128, (g.ny + K - 1) / K, g.nz), 128, 0, s>>>(g, views, sel, vol,
-                                                                                          alpha, gmax, tex);
+    k_bp_voxel_cols<K, T, PF><<<dim3((g.nx + 127) / 128, (g.ny + K - 1) / K, g.nz), 128, 0, s>>>(
+        g, views, sel, vol, alpha, gmax, tex);
 }
 
 template <typename T>
@@ -394,6 +405,8 @@ cudaError_t bp_voxel_any(const GeomDev &g, const ViewRec *views, const ViewSel &
         switch (bp_variant) {
         case 1: bp_cols<8>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
         case 2: bp_cols<32>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
+        case 3: bp_cols<16, T, true>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
+        case 4: bp_cols<32, T, true>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
         default: bp_cols<BP_COL>(g, views, sel, vol, alpha, gmax, s, corr_tex); break;
         }
     } else {
@@ -434,7 +447,8 @@ cudaError_t pd_extrapolate_any(const int *d, const int *cut, const T *vol, const
 }  // namespace
 
 const char *bp_variant_name(int v) {
-    static const char *names[kBpVariants] = {"columns of 16 voxels", "columns of 8 voxels", "columns of 32 voxels"};
+    static const char *names[kBpVariants] = {"columns of 16 voxels", "columns of 8 voxels", "columns of 32 voxels",
+                                             "columns of 16 voxels, L2 prefetch", "columns of 32 voxels, L2 prefetch"};
     return v >= 0 && v < kBpVariants ? names[v] : "?";
 }
 

@@ -27,13 +27,14 @@ int grid_stride_blocks(long long n, int threads);
 //         in flight and, for variants 10 and 11, corners fetched as two tld4
 //         texture gathers per sample instead of eight loads (fp_variant_name);
 //   slab: the box of the slab-staged projector (slab_variant_name);
-//   bp:   the column length of the voxel backprojection (bp_variant_name);
+//   bp:   the column length of the voxel backprojection, and whether each
+//         column's voxels are first prefetched into L2 (bp_variant_name);
 //   ray:  the scatter of the ray-driven backprojection (ray_variant_name):
 //         0 one global vector atomic per corner, 1 a shared-memory box per
 //         slab (volumes below 2^31 voxels).  Its sums differ in float order
 //         only (as any two atomic runs do), not in their terms.
 // Which views the slab kernel projects is the per-view ViewRec::staged flag.
-constexpr int kFpVariants = 12, kSlabVariants = 8, kBpVariants = 3, kRayVariants = 2;
+constexpr int kFpVariants = 12, kSlabVariants = 8, kBpVariants = 5, kRayVariants = 2;
 struct Tuning {
     int fp = 0, slab = 0, bp = 0, ray = 0;
     int fp16 = 0;  // the BF16-stored volume's gather form (fp16_variant_name)
