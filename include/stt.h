@@ -449,9 +449,21 @@ stt_status stt_flow_resize(stt_flow *f, const int *dim, int nc, const float *in,
  *   flow  F*3    flow[f]: motion from frame f to f+1 (planar channels)
  *   proj  F*V*H*W measured projections */
 typedef enum stt_solve_mode {
-    STT_SOLVE_PLAIN = 0,    /* per-view launches from a host loop, sync per view */
-    STT_SOLVE_STREAMS = 1,  /* batched: fused launches, one stream per frame */
-    STT_SOLVE_GRAPH = 2     /* batched, captured once into a CUDA graph and replayed */
+    STT_SOLVE_PLAIN = 0,      /* per-view launches from a host loop, sync per view */
+    STT_SOLVE_STREAMS = 1,    /* batched: fused launches, one stream per frame */
+    STT_SOLVE_GRAPH = 2,      /* batched, captured once into a CUDA graph and replayed */
+    /* Every frame's SART call (all views: transpose, projection + correction,
+     * backprojection), its ROI mask and over-relaxation in ONE persistent
+     * cooperative launch, the frames side by side on their share of the
+     * resident blocks, after the warps, duals and primals; the iteration is
+     * captured into a CUDA graph and replayed (enqueued directly where the
+     * runtime cannot capture a cooperative launch: stt_solver_stats).  Voxel-based
+     * backprojection only (bp_mode 0).  The same bits as the other batched
+     * modes; inside one launch the volume is gathered with plain loads (the
+     * texture and read-only caches are not coherent with the launch's own
+     * writes), so on volumes that the texture gathers serve well it is
+     * slower than STT_SOLVE_GRAPH. */
+    STT_SOLVE_PERSISTENT = 3
 } stt_solve_mode;
 
 typedef struct stt_solve_cfg {
@@ -512,6 +524,10 @@ stt_status stt_solver_set_iteration(stt_solver *s, unsigned long long iter, void
 /* Kernel launches per iteration and iterations run so far. */
 stt_status stt_solver_stats(const stt_solver *s, long long *launches_per_iter,
                             unsigned long long *iterations);
+/* STT_SOLVE_PERSISTENT: blocks of the persistent launch, and whether the
+ * iteration is a replayed graph (1) or enqueued directly (0; the runtime
+ * refused to capture the cooperative launch).  Zeros in the other modes. */
+stt_status stt_solver_persistent_info(const stt_solver *s, int *blocks, int *graph);
 const char *stt_solver_last_error(const stt_solver *s);
 /* See stt_poll_status. */
 stt_status stt_solver_poll_status(stt_solver *s, void *stream);

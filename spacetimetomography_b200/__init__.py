@@ -8,6 +8,7 @@ streams only); every operation is a call into libstt.
 from ._lib import STTError, lib  # noqa: F401  (loads libstt.so or raises)
 from .api import (  # noqa: F401
     SOLVE_GRAPH,
+    SOLVE_PERSISTENT,
     SOLVE_PLAIN,
     SOLVE_STREAMS,
     Batch,

@@ -116,6 +116,7 @@ def _load() -> C.CDLL:
         "stt_solver_iterate": [vp, i, vp],
         "stt_solver_iterate_phase": [vp, i, vp],
         "stt_solver_stats": [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_ulonglong)],
+        "stt_solver_persistent_info": [vp, C.POINTER(i), C.POINTER(i)],
         "stt_solver_destroy": [vp],
         "stt_solver_frame_order": [C.c_ulonglong, C.c_ulonglong, i, i, i, vp],
         "stt_fp_typed": [vp, vp, i, vp, vp, vp, i, i, vp],

@@ -453,7 +453,7 @@ class Flow:
             pass
 
 
-SOLVE_PLAIN, SOLVE_STREAMS, SOLVE_GRAPH = 0, 1, 2
+SOLVE_PLAIN, SOLVE_STREAMS, SOLVE_GRAPH, SOLVE_PERSISTENT = 0, 1, 2, 3
 
 
 def frame_order(seed: int, iteration: int, n_frames: int, frame: int, views: int) -> np.ndarray:
@@ -525,6 +525,13 @@ class Solver:
         nl, it = C.c_longlong(), C.c_ulonglong()
         check(lib.stt_solver_stats(self._h, C.byref(nl), C.byref(it)))
         return nl.value, it.value
+
+    def persistent_info(self):
+        """SOLVE_PERSISTENT: (blocks of the persistent launch, True if the
+        iteration replays a captured graph); (0, False) in the other modes."""
+        b, g = C.c_int(), C.c_int()
+        check(lib.stt_solver_persistent_info(self._h, C.byref(b), C.byref(g)))
+        return b.value, bool(g.value)
 
     def close(self):
         if getattr(self, "_h", None):

@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompil
 
 KERNEL_SOURCES = ["stt_capi.cu", "stt_solver.cu", "stt_batch.cu", "stt_noalloc.cu", "stt_flow.cu", "stt_tune.cu",
                   "k_project.cu",
-                  "k_fp_slab.cu", "k_bp_slab.cu", "k_voxel.cu", "k_warp.cu", "k_flow.cu"]
+                  "k_fp_slab.cu", "k_bp_slab.cu", "k_voxel.cu", "k_persist.cu", "k_warp.cu", "k_flow.cu"]
 # Per-file flags.  The optical-flow kernels keep the reference's float
 # rounding operation by operation, so no multiply-add contraction there.
 FILE_FLAGS = {"k_flow.cu": ["-fmad=false"]}

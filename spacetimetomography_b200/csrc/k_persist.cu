@@ -1,0 +1,240 @@
+// k_persist.cu -- the persistent sweep: every view of every frame's SART call
+// (S/ST_Tomo/ST_Tomography.cpp:616-808) -- or of every batch instance's --
+// and the ROI mask with the over-relaxation that follows it (:586-604,
+// :793-804), in ONE cooperative launch.
+//
+// The blocks of the launch are split into jobs (SweepJob: one frame or one
+// instance each, blocks in proportion to its work).  A job's blocks walk its
+// views in the frame's order; per view, three phases separated by the job's
+// own barrier:
+//   transpose  (views that gather along x) the z-fastest copy of the volume,
+//              32 x 32 tiles through shared memory;
+//   project    the forward projection with the SART correction, one thread
+//              per detector pixel, 32 x 4 pixel tiles (k_fp_corr's arithmetic:
+//              the same samples, Kahan order and epilogue);
+//   backproject the voxel-based backprojection, one thread per (x, z) column
+//              walking 16 voxels up y (bp_column, the column walk of the
+//              per-view kernel);
+// and after the last view the ROI mask and the over-relaxation.  Each phase's
+// tiles go round-robin over the job's blocks, so the block that owns a
+// pixel's sticky ray length or a voxel column is the same for every view.
+//
+// What one launch changes: no launch gaps between the ~3 V dependent steps of
+// a sweep, and all frames' (instances') sweeps side by side.  What it costs:
+// data that the launch itself writes (the volume, its copy, the correction)
+// cannot be read through the texture or read-only paths, whose caches are not
+// kept coherent within a launch, so the gathers are plain L1-cached loads
+// (after each barrier's acquire) instead of the per-view kernels' tld4
+// gathers, and every phase runs at the launch's one occupancy.
+//
+// The barrier: a block's thread 0 makes the block's writes visible
+// (__threadfence), adds one arrival to the job's counter, and polls it with
+// acquire loads until all of the job's blocks have arrived.  The launch is
+// cooperative, so every block is resident and every wait ends; the poll is
+// still bounded (about 1 s by the global timer): a wait that runs out raises
+// the job's abort word and the status word (STT_WAIT_TIMEOUT_FLAG), and every
+// block of the job leaves at its next barrier.
+#include "stt_internal.cuh"
+#include "stt_kernels.h"
+#include "stt_voxel.cuh"
+
+namespace stt {
+
+namespace {
+
+constexpr int SWEEP_THREADS = 128;
+constexpr int SWEEP_COL = 16;                              // voxels per column of the backprojection
+constexpr unsigned long long SWEEP_WAIT_NS = 1000000000ull;  // bound of one barrier wait
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// The job's barrier: true when all `target` arrivals are in (the job's blocks
+// have passed it as many times), false when the job aborted.
+__device__ __forceinline__ bool sweep_barrier(unsigned *bar, unsigned target, int *status) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        const unsigned long long t0 = global_ns();
+        int good = 1;
+        while (ld_acquire(bar) < target) {
+            if (ld_acquire(bar + 1)) {
+                good = 0;
+                break;
+            }
+            if (global_ns() - t0 > SWEEP_WAIT_NS) {
+                atomicExch(bar + 1, 1u);
+                atomicOr(status, STT_WAIT_TIMEOUT_FLAG);
+                good = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// The forward projection with the correction of pixel (i, j)
+// (k_fp_corr's body, corners by plain loads).
+template <typename I, typename T>
+__device__ __forceinline__ void sweep_fp_pixel(const GeomDev &g, const ViewRec &vr, const T *vol, const T *volt,
+                                               const T *b, float *raylen, float *corr, int i, int j) {
+    Ray r;
+    make_ray(g, vr, i, j, r);
+    const size_t pix = i + (size_t)j * g.W;
+    float L, sum = 0.0f;
+    if (r.tnear < r.tfar) {
+        if (volt && vr.layout == 1) {
+            const Strides st = zyx_strides(g);
+            sum = fp_ray_sum_with<FP_GROUP, false>(
+                g, [=](int, const FpCell &c, float v[8]) { fp_corners<2, I, T, true>(volt, st, c, v); }, r, nullptr);
+        } else {
+            const Strides st = xyz_strides(g);
+            sum = fp_ray_sum_with<FP_GROUP, false>(
+                g, [=](int, const FpCell &c, float v[8]) { fp_corners<0, I, T, true>(vol, st, c, v); }, r, nullptr);
+        }
+        L = r.tfar - r.tnear;
+        raylen[pix] = L;
+    } else {
+        L = raylen[pix];
+    }
+    corr[pix] = __fdiv_rn(__fsub_rn(ld_voxel(b + pix), sum), __fadd_rn(L, 1.0f));
+}
+
+// Seven blocks per SM: 72 registers, no spills (eight would spill); 1036
+// resident blocks on 148 SMs.
+template <typename T, typename I>
+__global__ void __launch_bounds__(SWEEP_THREADS, 7) k_sweep_persistent(const SweepJob *__restrict__ jobs, int njobs,
+                                                                    int *status) {
+    __shared__ T tile[32][33];
+    int jid = 0;
+    while (jid + 1 < njobs && (int)blockIdx.x >= jobs[jid + 1].block0) ++jid;
+    const SweepJob &J = jobs[jid];
+    const GeomDev g = J.g;
+    const int rank = (int)blockIdx.x - J.block0, nb = J.nblocks;
+    if (rank < 0 || rank >= nb) return;  // (blocks beyond the last job's range: none by construction)
+    T *vol = static_cast<T *>(J.vol);
+    T *volt = static_cast<T *>(J.volt);
+    const T *stack = static_cast<const T *>(J.stack);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const size_t nxy = (size_t)g.nx * g.ny, nzy = (size_t)g.nz * g.ny, npix = (size_t)g.W * g.H;
+    unsigned passed = 0;
+    for (int v = 0; v < J.V; ++v) {
+        const int local = __ldg(J.perm + v);
+        const ViewRec &vr = J.views[J.view_base + local];
+        if (volt && vr.layout == 1) {  // the z-fastest copy this view gathers from
+            const int tx = (g.nx + 31) / 32, tz = (g.nz + 31) / 32;
+            for (int t = rank; t < tx * tz * g.ny; t += nb) {
+                const int x0 = (t % tx) * 32, z0 = ((t / tx) % tz) * 32, y = t / (tx * tz);
+                for (int r = warp; r < 32; r += SWEEP_THREADS / 32)
+                    if (x0 + lane < g.nx && z0 + r < g.nz)
+                        tile[r][lane] = vol[(x0 + lane) + (size_t)y * g.nx + (size_t)(z0 + r) * nxy];
+                __syncthreads();
+                for (int r = warp; r < 32; r += SWEEP_THREADS / 32)
+                    if (x0 + r < g.nx && z0 + lane < g.nz)
+                        volt[(z0 + lane) + (size_t)y * g.nz + (size_t)(x0 + r) * nzy] = tile[lane][r];
+                __syncthreads();
+            }
+            if (!sweep_barrier(J.bar, ++passed * nb, status)) return;
+        }
+        {  // forward projection + correction
+            const T *b = stack + (size_t)local * npix;
+            const int tw = (g.W + 31) / 32, th = (g.H + 3) / 4;
+            for (int t = rank; t < tw * th; t += nb) {
+                const int i = (t % tw) * 32 + lane, j = (t / tw) * 4 + warp;
+                if (i < g.W && j < g.H) sweep_fp_pixel<I>(g, vr, vol, volt, b, J.raylen, J.corr, i, j);
+            }
+        }
+        if (!sweep_barrier(J.bar, ++passed * nb, status)) return;
+        {  // voxel-based backprojection
+            const int cx = (g.nx + SWEEP_THREADS - 1) / SWEEP_THREADS, cy = (g.ny + SWEEP_COL - 1) / SWEEP_COL;
+            const BpRowsLoad rows{J.corr, g.W};
+            for (int t = rank; t < cx * cy * g.nz; t += nb) {
+                const int x = (t % cx) * SWEEP_THREADS + threadIdx.x, y0 = ((t / cx) % cy) * SWEEP_COL;
+                const int z = t / (cx * cy);
+                if (x < g.nx) bp_column<SWEEP_COL, false>(g, vr, rows, vol, x, y0, z, J.alpha, J.gmax);
+            }
+        }
+        if (!sweep_barrier(J.bar, ++passed * nb, status)) return;
+    }
+    // the ROI mask and the over-relaxation
+    const int rx = (g.nx + SWEEP_THREADS - 1) / SWEEP_THREADS;
+    const T *xprev = static_cast<const T *>(J.xprev);
+    T *xbar = static_cast<T *>(J.xbar);
+    for (int t = rank; t < rx * g.ny * g.nz; t += nb) {
+        const int i = (t % rx) * SWEEP_THREADS + threadIdx.x, j = (t / rx) % g.ny, k = t / (rx * g.ny);
+        if (i < g.nx) roi_apply_at(i, j, k, g.nx, g.ny, g.nz, J.roi, J.pdcut, vol, xprev, xbar);
+    }
+}
+
+template <typename T, typename I>
+const void *sweep_kernel() {
+    return reinterpret_cast<const void *>(&k_sweep_persistent<T, I>);
+}
+
+const void *pick(bool bf16, bool wide) {
+    if (bf16) return wide ? sweep_kernel<unsigned short, long long>() : sweep_kernel<unsigned short, int>();
+    return wide ? sweep_kernel<float, long long>() : sweep_kernel<float, int>();
+}
+
+}  // namespace
+
+int sweep_max_blocks(bool bf16, bool wide) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick(bf16, wide), SWEEP_THREADS, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per_sm * sm_count();
+}
+
+void sweep_assign_blocks(SweepJob *jobs, int njobs, int nblocks) {
+    double total = 0.0;
+    for (int q = 0; q < njobs; ++q) total += jobs[q].work > 0.0 ? jobs[q].work : 1.0;
+    // every job one block, the rest in proportion to the work (largest remainders last)
+    int spare = nblocks - njobs, given = 0;
+    for (int q = 0; q < njobs; ++q) {
+        const double w = jobs[q].work > 0.0 ? jobs[q].work : 1.0;
+        const int extra = (int)((double)spare * w / total);
+        jobs[q].nblocks = 1 + extra;
+        given += jobs[q].nblocks;
+    }
+    for (int q = 0; given < nblocks; q = (q + 1) % njobs, ++given) ++jobs[q].nblocks;
+    int b0 = 0;
+    for (int q = 0; q < njobs; ++q) {
+        jobs[q].block0 = b0;
+        b0 += jobs[q].nblocks;
+    }
+}
+
+cudaError_t launch_sweep_persistent(const SweepJob *jobs_d, int njobs, int nblocks, bool bf16, bool wide,
+                                    int *status, cudaStream_t s) {
+    if (njobs < 1 || nblocks < njobs) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(SWEEP_THREADS);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {(void *)&jobs_d, (void *)&njobs, (void *)&status};
+    return cudaLaunchKernelExC(&cfg, pick(bf16, wide), args);
+}
+
+}  // namespace stt

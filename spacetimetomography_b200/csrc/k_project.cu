@@ -24,63 +24,8 @@ __device__ __forceinline__ bool tile_pixel(const GeomDev &g, int &i, int &j) {
     return i < g.W && j < g.H;
 }
 
-// The ray sum of one forward-projector ray (hit rays only), gathered from the
-// z-fastest transposed copy for layout-1 views when one is given, else from
-// the volume.  Samples go G at a time where the march allows: all their taps
-// are loaded before any is interpolated.  The sum is the same for every G
-// (the samples are added one by one in march order).
-constexpr int FP_GROUP = 4;
-
-// `corners(k, c, v)` fetches the 8 corners of cell c, the k-th sample of a
-// group (0 for a sample on its own): loads from an array, or tld4 gathers of
-// its texture (the same values).
-template <int G = FP_GROUP, bool PK = false, typename Corners>
-__device__ __forceinline__ float fp_ray_sum_with(const GeomDev &g, const Corners &corners, const Ray &r, int *count) {
-    Kahan acc{0.0f, 0.0f};
-    int n = 0;
-    march_groups<G>(
-        g, r,
-        [&](const float p[3]) {
-            FpCell c;
-            fp_cell(g, p, c);
-            float v[8];
-            corners(0, c, v);
-            acc.add(__fmul_rn(trilerp(v, c), g.sd));
-            ++n;
-        },
-        [&](const float (*p)[3]) {
-            FpCell c[G];
-            float v[G][8];
-            if constexpr (PK) {  // pairs of samples in the packed FP32x2 instructions
-                static_assert(G % 2 == 0, "samples go in packed pairs");
-#pragma unroll
-                for (int i = 0; i < G; i += 2) {
-                    fp_cell2(g, p[i], p[i + 1], c[i], c[i + 1]);
-                    corners(i, c[i], v[i]);
-                    corners(i + 1, c[i + 1], v[i + 1]);
-                }
-                const float2 sd2 = make_float2(g.sd, g.sd);
-#pragma unroll
-                for (int i = 0; i < G; i += 2) {
-                    const float2 s = __fmul2_rn(trilerp2(v[i], v[i + 1], c[i], c[i + 1]), sd2);
-                    acc.add(s.x);
-                    acc.add(s.y);
-                }
-            } else {
-#pragma unroll
-                for (int i = 0; i < G; ++i) {
-                    fp_cell(g, p[i], c[i]);
-                    corners(i, c[i], v[i]);
-                }
-#pragma unroll
-                for (int i = 0; i < G; ++i) acc.add(__fmul_rn(trilerp(v[i], c[i]), g.sd));
-            }
-            n += G;
-        });
-    if (count) *count = n;
-    return acc.s;
-}
-
+// The ray sum gathered from the z-fastest transposed copy for layout-1 views
+// when one is given, else from the volume (fp_ray_sum_with).
 template <int FAST, typename I, int G = FP_GROUP, bool PK = false, typename T>
 __device__ __forceinline__ float fp_ray_sum_from(const GeomDev &g, const T *__restrict__ src, const Strides &st,
                                                  const Ray &r, int *count) {

@@ -5,120 +5,13 @@
 // voxel along x, blocks of 128 threads, grid (ceil(nx/128), ny, nz), so every
 // warp reads and writes 128 contiguous bytes per array.  The stencil
 // neighbours (x+-1, y+-1, z+-1) come from L1/L2.
-#include <climits>
-
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
+#include "stt_voxel.cuh"
 
 namespace stt {
 
 namespace {
-
-// ROI box of the primal-dual loops (ST_Tomography.cpp:514, 565, 593).
-__device__ __forceinline__ bool roi_out(int i, int j, int k, int nx, int ny, int nz, const int *cut) {
-    return i < cut[0] || i > nx - cut[1] || j < cut[2] || j > ny - cut[3] || k < cut[4] ||
-           k > nz - cut[5];
-}
-
-// ROI mask (ST_Tomography.cpp:303-329); note the literal 7 in the y test of :324.
-__device__ __forceinline__ float roi_value(int i, int j, int k, int nx, int ny, int nz, const int *cut) {
-    float r = 1.0f;
-    if (((i < cut[6]) && (k < cut[7])) || ((i < cut[6]) && (k > (nz - cut[7])))) r = 0.0f;
-    if (((i > (nx - cut[6])) && (k < cut[7])) || ((i > (nx - cut[6])) && (k > (nz - cut[7])))) r = 0.0f;
-    if (((k < cut[6]) && (i < cut[7])) || ((k < cut[6]) && (i > (nx - cut[7])))) r = 0.0f;
-    if (((k > (nz - cut[6])) && (i < cut[7])) || ((k > (nz - cut[6])) && (i > (nx - cut[7])))) r = 0.0f;
-    if (i < cut[0] || i > nx - cut[1] || j < cut[2] || j > ny - 7 || k < cut[4] || k > nz - cut[5]) r = 0.0f;
-    return r;
-}
-
-struct Cut8 {
-    int c[8];
-};
-
-// Voxel-based backprojection (ST_Tomography.cpp:690-730): project the voxel
-// centre, Catmull-Rom 4x4 gather of the correction image (y first, then x),
-// vol += alpha*val, clamp to [0, gmax]; voxels whose footprint leaves
-// [2, W-2) x [2, H-2) are untouched.  Every product and sum is rounded on its
-// own (explicit intrinsics), so the per-voxel and the column forms below give
-// the same bits.
-
-// Camera coordinate r of voxel (fx, fy, fz): A[r]*(x, y, z) + b[r].
-__device__ __forceinline__ float bp_cam(const ViewRec &v, int r, float fx, float fy, float fz) {
-    return __fadd_rn(__fmaf_rn(v.A[3 * r + 2], fz, __fmaf_rn(v.A[3 * r + 1], fy, __fmul_rn(v.A[3 * r], fx))), v.b[r]);
-}
-
-// Detector coordinate c + cam/(-depth) * sdd/ds.
-__device__ __forceinline__ float bp_pixel(float c, float cam, float ndepth, float sdd_ds) {
-    return __fmaf_rn(__fdiv_rn(cam, ndepth), sdd_ds, c);
-}
-
-// Catmull-Rom weights of taps (-1, 0, +1, +2) at fraction d.
-__device__ __forceinline__ void bp_weights(float d, float w[4]) {
-    const float d2 = __fmul_rn(d, d), d3 = __fmul_rn(d2, d);
-    w[0] = __fmul_rn(0.5f, __fsub_rn(__fmaf_rn(2.0f, d2, -d), d3));
-    w[1] = __fadd_rn(1.0f, __fmul_rn(0.5f, __fmaf_rn(3.0f, d3, __fmul_rn(-5.0f, d2))));
-    w[2] = __fmul_rn(0.5f, __fmaf_rn(-3.0f, d3, __fmaf_rn(4.0f, d2, d)));
-    w[3] = __fmul_rn(0.5f, __fsub_rn(d3, d2));
-}
-
-// sum_a wx[a] * sum_b wy[b] * tap[a][b]; tap[a][b] is column px-1+a, row py-1+b.
-__device__ __forceinline__ float bp_sum(const float tap[4][4], const float wx[4], const float wy[4]) {
-    float val = 0.0f;
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const float s = __fmaf_rn(wy[3], tap[a][3],
-                                  __fmaf_rn(wy[2], tap[a][2], __fmaf_rn(wy[1], tap[a][1], __fmul_rn(wy[0], tap[a][0]))));
-        val = a == 0 ? __fmul_rn(wx[0], s) : __fmaf_rn(wx[a], s, val);
-    }
-    return val;
-}
-
-// T: the volume's storage (float, or BF16 bits widened to FP32 and rounded
-// back to nearest even on store).
-template <typename T>
-__device__ __forceinline__ void bp_update(T *__restrict__ vol, size_t o, float alpha, float val, float gmax) {
-    const float nv = __fmaf_rn(alpha, val, ld_stored(vol + o));
-    st_stored(vol + o, rmax(rmin(gmax, nv), 0.0f));
-}
-
-// The 4x4 footprint at (px, py): four tld4 gathers of the correction's
-// one-layer texture copy (TEX), or sixteen loads.
-template <bool TEX>
-__device__ __forceinline__ void bp_taps(const GeomDev &g, const float *__restrict__ corr, unsigned long long tex,
-                                        int px, int py, float tap[4][4]) {
-    if (TEX) {
-        const float4 g00 = gather_layer(tex, px - 1, py - 1, 0), g10 = gather_layer(tex, px + 1, py - 1, 0);
-        const float4 g01 = gather_layer(tex, px - 1, py + 1, 0), g11 = gather_layer(tex, px + 1, py + 1, 0);
-        tap[0][0] = g00.w, tap[0][1] = g00.x, tap[0][2] = g01.w, tap[0][3] = g01.x;
-        tap[1][0] = g00.z, tap[1][1] = g00.y, tap[1][2] = g01.z, tap[1][3] = g01.y;
-        tap[2][0] = g10.w, tap[2][1] = g10.x, tap[2][2] = g11.w, tap[2][3] = g11.x;
-        tap[3][0] = g10.z, tap[3][1] = g10.y, tap[3][2] = g11.z, tap[3][3] = g11.y;
-    } else {
-        const float *c0 = corr + (size_t)(py - 1) * g.W + (px - 1);
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) tap[a][b] = __ldg(c0 + a + b * g.W);
-    }
-}
-
-// One voxel, everything computed for it alone.
-template <bool TEX, typename T>
-__device__ __forceinline__ void bp_voxel_at(const GeomDev &g, const ViewRec &v, const float *__restrict__ corr,
-                                            unsigned long long tex, T *__restrict__ vol, int x, int y, int z,
-                                            float alpha, float gmax) {
-    const float fx = (float)x, fy = (float)y, fz = (float)z;
-    const float ndepth = -bp_cam(v, 2, fx, fy, fz);
-    const float upx = bp_pixel(g.cx, bp_cam(v, 0, fx, fy, fz), ndepth, g.sdd_ds);
-    const float upy = bp_pixel(g.cy, bp_cam(v, 1, fx, fy, fz), ndepth, g.sdd_ds);
-    if (!(upx >= 2.0f && upx < (float)(g.W - 2) && upy >= 2.0f && upy < (float)(g.H - 2))) return;
-    const int px = (int)upx, py = (int)upy;
-    float wx[4], wy[4], tap[4][4];
-    bp_weights(upx - (float)px, wx);
-    bp_weights(upy - (float)py, wy);
-    bp_taps<TEX>(g, corr, tex, px, py, tap);
-    bp_update(vol, x + (size_t)y * g.nx + (size_t)z * g.nx * g.ny, alpha, bp_sum(tap, wx, wy), gmax);
-}
 
 template <bool TEX, typename T>
 __global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec *__restrict__ views,
@@ -129,18 +22,16 @@ __global__ void __launch_bounds__(128) k_bp_voxel(const GeomDev g, const ViewRec
     if (x >= g.nx) return;
     int local;
     const ViewRec &v = views[sel_view(sel, local)];
-    bp_voxel_at<TEX>(g, v, corr, corr_tex, vol, x, blockIdx.y, blockIdx.z, alpha, gmax);
+    if (TEX)
+        bp_voxel_at(g, v, BpRowsTex{corr_tex}, vol, x, blockIdx.y, blockIdx.z, alpha, gmax);
+    else
+        bp_voxel_at(g, v, BpRowsLdg{corr, g.W}, vol, x, blockIdx.y, blockIdx.z, alpha, gmax);
 }
 
-// Column form, texture taps: one thread per (x, z) walks K voxels up y.  For
-// a view whose matrix has A[1] == A[7] == 0 (every rotation about y) the
-// voxel's detector column and depth do not depend on y: they are computed
-// once (the y term of their sums is an exact zero, so the values are the
-// per-voxel ones).  The detector row moves by about sdd/sid per voxel, and
-// the 4x4 window's rows are kept in registers: a step of s = 0, 1 or 2 rows
-// reuses two of them and gathers the two new ones (2 tld4 instead of 4).
-// Column length K: 16 by default; the autotuner may pick 8 or 32 (the
-// voxels' values do not depend on which thread walks them).
+// Column form, texture taps (bp_column in stt_voxel.cuh): one thread per
+// (x, z) walks K voxels up y.  Column length K: 16 by default; the autotuner
+// may pick 8 or 32 (the voxels' values do not depend on which thread walks
+// them).
 constexpr int BP_COL = 16;
 
 // Ten 128-thread blocks per SM (48 registers, no spills): the walk is bound
@@ -159,58 +50,10 @@ __global__ void __launch_bounds__(128, 10) k_bp_voxel_cols(const GeomDev g, cons
                                                        const ViewSel sel, T *__restrict__ vol, float alpha,
                                                        float gmax, unsigned long long tex) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y0 = blockIdx.y * K, z = blockIdx.z;
     if (x >= g.nx) return;
     int local;
     const ViewRec &v = views[sel_view(sel, local)];
-    const int y1 = min(y0 + K, g.ny);
-    if (!(v.A[1] == 0.0f && v.A[7] == 0.0f)) {
-        for (int y = y0; y < y1; ++y) bp_voxel_at<true>(g, v, nullptr, tex, vol, x, y, z, alpha, gmax);
-        return;
-    }
-    const float fx = (float)x, fz = (float)z;
-    const float ndepth = -bp_cam(v, 2, fx, (float)y0, fz);
-    const float upx = bp_pixel(g.cx, bp_cam(v, 0, fx, (float)y0, fz), ndepth, g.sdd_ds);
-    if (!(upx >= 2.0f && upx < (float)(g.W - 2))) return;
-    const int px = (int)upx;
-    if (PF) {
-        const T *col = vol + x + (size_t)z * g.nx * g.ny;
-        for (int y = y0; y < y1; ++y) asm volatile("prefetch.global.L2 [%0];" ::"l"(col + (size_t)y * g.nx));
-    }
-    float wx[4];
-    bp_weights(upx - (float)px, wx);
-    float R[4][4];  // R[a][b]: column px-1+a, row pyc-1+b
-    int pyc = INT_MIN / 2;
-    for (int y = y0; y < y1; ++y) {
-        const float upy = bp_pixel(g.cy, bp_cam(v, 1, fx, (float)y, fz), ndepth, g.sdd_ds);
-        if (!(upy >= 2.0f && upy < (float)(g.H - 2))) continue;
-        const int py = (int)upy;
-        float wy[4];
-        bp_weights(upy - (float)py, wy);
-        const int s = py - pyc;
-        float r0[4], r1[4];  // rows py-1, py
-        if (s >= 0 && s <= 2) {
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                r0[a] = s == 0 ? R[a][0] : (s == 1 ? R[a][1] : R[a][2]);
-                r1[a] = s == 0 ? R[a][1] : (s == 1 ? R[a][2] : R[a][3]);
-            }
-        } else {
-            const float4 gc = gather_layer(tex, px - 1, py - 1, 0), gd = gather_layer(tex, px + 1, py - 1, 0);
-            r0[0] = gc.w, r0[1] = gc.z, r0[2] = gd.w, r0[3] = gd.z;
-            r1[0] = gc.x, r1[1] = gc.y, r1[2] = gd.x, r1[3] = gd.y;
-        }
-        const float4 ga = gather_layer(tex, px - 1, py + 1, 0), gb = gather_layer(tex, px + 1, py + 1, 0);
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            R[a][0] = r0[a];
-            R[a][1] = r1[a];
-        }
-        R[0][2] = ga.w, R[1][2] = ga.z, R[2][2] = gb.w, R[3][2] = gb.z;  // row py+1
-        R[0][3] = ga.x, R[1][3] = ga.y, R[2][3] = gb.x, R[3][3] = gb.y;  // row py+2
-        pyc = py;
-        bp_update(vol, x + (size_t)y * g.nx + (size_t)z * g.nx * g.ny, alpha, bp_sum(R, wx, wy), gmax);
-    }
+    bp_column<K, PF>(g, v, BpRowsTex{tex}, vol, x, blockIdx.y * K, blockIdx.z, alpha, gmax);
 }
 
 // Dual step of one frame (ST_Tomography.cpp:504-534), fused:
@@ -303,20 +146,16 @@ __global__ void __launch_bounds__(128) k_pd_extrapolate(int nx, int ny, int nz, 
 }
 
 // End of a SART call (ST_Tomography.cpp:793-804) optionally fused with the
-// over-relaxation that follows it in the primal-dual loop (:586-604):
-// vol *= roi; if xbar: xbar = 2*vol - xprev in the ROI box.
+// over-relaxation that follows it in the primal-dual loop (:586-604)
+// (roi_apply_at).
 template <typename T>
 __global__ void __launch_bounds__(128) k_roi_apply(int nx, int ny, int nz, Cut8 cut, Cut8 pdcut,
                                                    T *__restrict__ vol,
                                                    const T *__restrict__ xprev,
                                                    T *__restrict__ xbar) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
     if (i >= nx) return;
-    const size_t p = i + (size_t)j * nx + (size_t)k * nx * ny;
-    const float v = ld_stored(vol + p) * roi_value(i, j, k, nx, ny, nz, cut.c);  // (a product by 0 or 1: exact)
-    st_stored(vol + p, v);
-    if (xbar && !roi_out(i, j, k, nx, ny, nz, pdcut.c)) st_stored(xbar + p, 2.0f * v - ld_voxel(xprev + p));
+    roi_apply_at(i, (int)blockIdx.y, (int)blockIdx.z, nx, ny, nz, cut.c, pdcut.c, vol, xprev, xbar);
 }
 
 __global__ void __launch_bounds__(128) k_roi_mask(int nx, int ny, int nz, Cut8 cut, float *__restrict__ roi) {

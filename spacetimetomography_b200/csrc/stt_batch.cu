@@ -5,10 +5,17 @@
 // one iteration of all of them is enqueued together -- or captured once into
 // one CUDA graph and replayed.  The instances share nothing, so their views
 // run concurrently and small instances fill the GPU that one alone leaves idle.
+// In the persistent form (STT_SOLVE_PERSISTENT) every instance's duals and
+// primal run on its own stream, then ONE cooperative launch runs all
+// instances' SART calls, ROI masks and over-relaxations side by side, the
+// resident blocks split between the instances in proportion to their work
+// (k_persist.cu); the iteration is captured into a graph and replayed.
 #include <string>
 #include <vector>
 
 #include "stt.h"
+#include "stt_internal.cuh"
+#include "stt_kernels.h"
 
 struct stt_batch {
     struct Inst {
@@ -29,12 +36,22 @@ struct stt_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool skip_copy = false;  // timing runs do not copy results into the callers' volumes
+    // STT_SOLVE_PERSISTENT: one sweep job per instance, their barrier words,
+    // the launch's blocks, storage and index width, the sweep's status word
+    stt::SweepJob *jobs_d = nullptr;
+    unsigned *bar = nullptr;
+    int *status = nullptr;
+    int sweep_blocks = 0;
+    bool bf16 = false, wide = false, direct = false;
     int staging_timed = 0, all_gather = 0;
     float ms_split = 0.0f, ms_gather = 0.0f;
     std::string err;
 };
 
 extern "C" stt_status stt_internal_set_error(stt_ctx *ctx, stt_status st, const char *msg);
+extern "C" stt_status stt_internal_solver_presweep(stt_solver *s, void *stream);
+extern "C" int stt_internal_solver_jobs(const stt_solver *s, void *jobs);
+extern "C" void stt_internal_solver_end_iteration(stt_solver *s);
 
 namespace {
 
@@ -67,6 +84,63 @@ stt_status enqueue_all(stt_batch *b, cudaStream_t main) {
     return STT_OK;
 }
 
+// The persistent form: every instance's steps before its SART call on its own
+// stream, then one launch for all SART calls, then the results.
+stt_status enqueue_all_persistent(stt_batch *b, cudaStream_t main) {
+    BCUDA(b, cudaEventRecord(b->fork, main), "event record");
+    for (size_t i = 0; i < b->inst.size(); ++i) {
+        stt_batch::Inst &in = b->inst[i];
+        BCUDA(b, cudaStreamWaitEvent(in.stream, b->fork, 0), "stream wait");
+        stt_status st = stt_internal_solver_presweep(in.solver, in.stream);
+        if (st) return bfail(b, st, "instance " + std::to_string(i) + ": " + stt_solver_last_error(in.solver));
+        BCUDA(b, cudaEventRecord(in.done, in.stream), "event record");
+        BCUDA(b, cudaStreamWaitEvent(main, in.done, 0), "stream wait");
+    }
+    const int n = (int)b->inst.size();
+    BCUDA(b, cudaMemsetAsync(b->bar, 0, 2 * (size_t)n * sizeof(unsigned), main), "barrier reset");
+    BCUDA(b, stt::launch_sweep_persistent(b->jobs_d, n, b->sweep_blocks, b->bf16, b->wide, b->status, main),
+          "persistent sweep");
+    for (stt_batch::Inst &in : b->inst) {
+        stt_internal_solver_end_iteration(in.solver);
+        if (!b->skip_copy)
+            BCUDA(b, cudaMemcpyAsync(in.user_vol, in.state, in.n * in.es, cudaMemcpyDeviceToDevice, main),
+                  "copy result");
+    }
+    return STT_OK;
+}
+
+// The instances' sweep jobs, the launch's blocks split between them.
+stt_status build_sweep(stt_batch *b) {
+    const int n = (int)b->inst.size();
+    std::vector<stt::SweepJob> jobs(n);
+    b->bf16 = b->inst[0].cfg.storage == STT_DTYPE_BF16;
+    b->wide = false;
+    for (int i = 0; i < n; ++i) {
+        if (stt_internal_solver_jobs(b->inst[i].solver, &jobs[i]) != 1)
+            return bfail(b, STT_ERR_INVALID, "instance " + std::to_string(i) + ": sweep job");
+        const stt::GeomDev &g = jobs[i].g;
+        b->wide |= (long long)g.nx * g.ny * g.nz >= (1LL << 31);
+    }
+    b->sweep_blocks = stt::sweep_max_blocks(b->bf16, b->wide);
+    if (b->sweep_blocks < n)
+        return bfail(b, STT_ERR_INVALID, "more instances than resident blocks of the persistent sweep (" +
+                                             std::to_string(b->sweep_blocks) + ")");
+    stt::sweep_assign_blocks(jobs.data(), n, b->sweep_blocks);
+    if (cudaMalloc(&b->bar, 2 * (size_t)n * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&b->jobs_d, n * sizeof(stt::SweepJob)) != cudaSuccess ||
+        cudaMalloc(&b->status, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return bfail(b, STT_ERR_NOMEM, "persistent sweep buffers");
+    }
+    for (int i = 0; i < n; ++i) jobs[i].bar = b->bar + 2 * i;
+    if (cudaMemcpy(b->jobs_d, jobs.data(), n * sizeof(stt::SweepJob), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(b->status, 0, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return bfail(b, STT_ERR_CUDA, "persistent sweep set-up");
+    }
+    return STT_OK;
+}
+
 // The instance's solver state from its start volume: vol (and the duplicated
 // last frame) and X_bar = the caller's volume; X_prev, the duals and the flow
 // zero.
@@ -84,7 +158,7 @@ cudaError_t init_state(stt_batch::Inst &in) {
 
 // (Re)creates the instance's one-frame solver with its context's current
 // launch choices.
-stt_status make_solver(stt_batch::Inst &in) {
+stt_status make_solver(stt_batch::Inst &in, bool persistent = false) {
     if (in.solver) {
         stt_solver_destroy(in.solver);
         in.solver = nullptr;
@@ -106,7 +180,7 @@ stt_status make_solver(stt_batch::Inst &in) {
     cfg.seed = I.seed;
     cfg.autotune = I.autotune;
     cfg.storage = I.storage;
-    cfg.mode = STT_SOLVE_STREAMS;
+    cfg.mode = persistent ? STT_SOLVE_PERSISTENT : STT_SOLVE_STREAMS;
     stt_pd_state state{};  // (BF16 storage: the primal pointers address BF16 arrays)
     state.vol = reinterpret_cast<float *>(vol);
     state.xbar = reinterpret_cast<float *>(xbar);
@@ -211,8 +285,14 @@ extern "C" {
 
 stt_status stt_batch_create(const stt_instance *instances, int n, int mode, stt_batch **out) {
     if (!instances || n < 1 || !out) return stt_internal_set_error(nullptr, STT_ERR_INVALID, "null argument or n < 1");
-    if (mode != STT_SOLVE_STREAMS && mode != STT_SOLVE_GRAPH)
-        return stt_internal_set_error(nullptr, STT_ERR_INVALID, "mode must be STT_SOLVE_STREAMS or STT_SOLVE_GRAPH");
+    if (mode != STT_SOLVE_STREAMS && mode != STT_SOLVE_GRAPH && mode != STT_SOLVE_PERSISTENT)
+        return stt_internal_set_error(nullptr, STT_ERR_INVALID,
+                                      "mode must be STT_SOLVE_STREAMS, STT_SOLVE_GRAPH or STT_SOLVE_PERSISTENT");
+    const bool persistent = mode == STT_SOLVE_PERSISTENT;
+    for (int i = 0; persistent && i < n; ++i)
+        if (instances[i].bp_mode != 0 || instances[i].storage != instances[0].storage)
+            return stt_internal_set_error(nullptr, STT_ERR_INVALID,
+                                          "STT_SOLVE_PERSISTENT: every instance voxel-based (bp_mode 0), one storage");
     *out = nullptr;
     stt_batch *b = new stt_batch;
     b->mode = mode;
@@ -246,16 +326,20 @@ stt_status stt_batch_create(const stt_instance *instances, int n, int mode, stt_
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&in.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&in.done, cudaEventDisableTiming);
         if (e != cudaSuccess) return bail(STT_ERR_CUDA, std::string("instance set-up: ") + cudaGetErrorString(e));
-        stt_status st = make_solver(in);
+        stt_status st = make_solver(in, persistent);
         if (st) return bail(st, "instance " + std::to_string(i) + ": " + stt_last_error(I.ctx));
     }
     if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
         return bail(STT_ERR_CUDA, "event create");
     bool tune = false;
     for (int i = 0; i < n; ++i) tune |= instances[i].autotune != 0;
-    if (tune) {
+    if (tune && !persistent) {  // (the persistent sweep has one projector: nothing to choose)
         const stt_status st = choose_staging(b);
         if (st) return bail(st, "batch staging choice: " + b->err);
+    }
+    if (persistent) {
+        const stt_status st = build_sweep(b);
+        if (st) return bail(st, b->err);
     }
     *out = b;
     return STT_OK;
@@ -267,6 +351,33 @@ stt_status stt_batch_iterate(stt_batch *b, int n_iters, void *stream) {
     for (int it = 0; it < n_iters; ++it) {
         if (b->mode == STT_SOLVE_STREAMS) {
             stt_status st = enqueue_all(b, cs);
+            if (st) return st;
+            continue;
+        }
+        if (b->mode == STT_SOLVE_PERSISTENT && !b->exec && !b->direct) {
+            // capture once; where the runtime refuses to capture the
+            // cooperative launch, enqueue every iteration directly
+            cudaStream_t cap;
+            BCUDA(b, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "capture stream");
+            stt_status st = STT_OK;
+            cudaGraph_t graph = nullptr;
+            if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                st = enqueue_all_persistent(b, cap);
+                if (cudaStreamEndCapture(cap, &graph) != cudaSuccess) graph = nullptr;
+            }
+            cudaGetLastError();
+            cudaStreamDestroy(cap);
+            if (!st && graph && cudaGraphInstantiate(&b->exec, graph, 0) == cudaSuccess) {
+                b->graph = graph;
+            } else {
+                if (graph) cudaGraphDestroy(graph);
+                cudaGetLastError();
+                b->exec = nullptr;
+                b->direct = true;
+            }
+        }
+        if (b->mode == STT_SOLVE_PERSISTENT && b->direct) {
+            stt_status st = enqueue_all_persistent(b, cs);
             if (st) return st;
             continue;
         }
@@ -294,6 +405,19 @@ stt_status stt_batch_iterate(stt_batch *b, int n_iters, void *stream) {
 stt_status stt_batch_poll_status(stt_batch *b, void *stream) {
     if (!b) return STT_ERR_INVALID;
     stt_status worst = STT_OK;
+    if (b->status) {  // the persistent sweep's word
+        cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+        int flag = 0;
+        BCUDA(b, cudaMemcpyAsync(&flag, b->status, sizeof(int), cudaMemcpyDeviceToHost, cs), "read status word");
+        BCUDA(b, cudaStreamSynchronize(cs), "cudaStreamSynchronize");
+        if (flag) {
+            BCUDA(b, cudaMemsetAsync(b->status, 0, sizeof(int), cs), "clear status word");
+            BCUDA(b, cudaStreamSynchronize(cs), "cudaStreamSynchronize");
+            worst = bfail(b, STT_ERR_TIMEOUT,
+                          "a barrier of the persistent sweep waited about 1 s: the sweep was abandoned and the "
+                          "iteration's results are not valid");
+        }
+    }
     for (size_t i = 0; i < b->inst.size(); ++i) {
         const stt_status st = stt_solver_poll_status(b->inst[i].solver, stream);
         if (st != STT_OK && worst == STT_OK) {
@@ -325,6 +449,9 @@ stt_status stt_batch_destroy(stt_batch *b) {
         cudaFree(in.state);
     }
     if (b->fork) cudaEventDestroy(b->fork);
+    cudaFree(b->jobs_d);
+    cudaFree(b->bar);
+    cudaFree(b->status);
     delete b;
     return STT_OK;
 }

@@ -271,25 +271,34 @@ __device__ __forceinline__ float2 trilerp2(const float va[8], const float vb[8],
     return lerp2(lerp2(a, b, fy1, fy), lerp2(d0, d1, fy1, fy), fz1, fz);
 }
 
+// One voxel of an array that the running kernel itself writes elsewhere (the
+// persistent sweep): a plain, L1-cached load, ordered after the kernel's own
+// barriers, never the read-only ld.global.nc path, which may return data
+// older than a write made earlier in the same launch.
+template <typename T>
+__device__ __forceinline__ float ld_src(const T *p, bool rw) {
+    return rw ? ld_stored(p) : ld_voxel(p);
+}
+
 // The 8 corners of a cell from a volume array: FAST is its contiguous axis
 // (0: x, the volume; 2: z, its transposed copy), whose +1 neighbour is the
 // next element.  I is the index type: int when the volume has fewer than
-// 2^31 voxels.
-template <int FAST, typename I, typename T>
-__device__ __forceinline__ void fp_corners(const T *__restrict__ src, const Strides &st, const FpCell &c, float v[8]) {
+// 2^31 voxels.  RW: the array is written by the same launch (ld_src).
+template <int FAST, typename I, typename T, bool RW = false>
+__device__ __forceinline__ void fp_corners(const T *src, const Strides &st, const FpCell &c, float v[8]) {
     const I idx = (I)c.ix * st.sx + (I)c.iy * st.sy + (I)c.iz * st.sz;
     if (FAST == 0) {  // rows along x at (y, z), (y+1, z), (y, z+1), (y+1, z+1)
         const I r00 = idx, r10 = idx + st.sy, r01 = idx + st.sz, r11 = r01 + st.sy;
-        v[0] = ld_voxel(src + r00), v[1] = ld_voxel(src + r00 + 1);
-        v[2] = ld_voxel(src + r10), v[3] = ld_voxel(src + r10 + 1);
-        v[4] = ld_voxel(src + r01), v[5] = ld_voxel(src + r01 + 1);
-        v[6] = ld_voxel(src + r11), v[7] = ld_voxel(src + r11 + 1);
+        v[0] = ld_src(src + r00, RW), v[1] = ld_src(src + r00 + 1, RW);
+        v[2] = ld_src(src + r10, RW), v[3] = ld_src(src + r10 + 1, RW);
+        v[4] = ld_src(src + r01, RW), v[5] = ld_src(src + r01 + 1, RW);
+        v[6] = ld_src(src + r11, RW), v[7] = ld_src(src + r11 + 1, RW);
     } else {  // runs along z at (x, y), (x+1, y), (x, y+1), (x+1, y+1)
         const I r00 = idx, r10 = idx + st.sx, r01 = idx + st.sy, r11 = r10 + st.sy;
-        v[0] = ld_voxel(src + r00), v[4] = ld_voxel(src + r00 + 1);
-        v[1] = ld_voxel(src + r10), v[5] = ld_voxel(src + r10 + 1);
-        v[2] = ld_voxel(src + r01), v[6] = ld_voxel(src + r01 + 1);
-        v[3] = ld_voxel(src + r11), v[7] = ld_voxel(src + r11 + 1);
+        v[0] = ld_src(src + r00, RW), v[4] = ld_src(src + r00 + 1, RW);
+        v[1] = ld_src(src + r10, RW), v[5] = ld_src(src + r10 + 1, RW);
+        v[2] = ld_src(src + r01, RW), v[6] = ld_src(src + r01 + 1, RW);
+        v[3] = ld_src(src + r11, RW), v[7] = ld_src(src + r11 + 1, RW);
     }
 }
 
@@ -591,5 +600,87 @@ __device__ __forceinline__ void cr_weights(float d, float w[4]) {
     w[2] = 0.5f * (d + 4.0f * d2 - 3.0f * d3);
     w[3] = 0.5f * (-d2 + d3);
 }
+
+// The ray sum of one forward-projector ray (hit rays only): the Kahan sum of
+// its samples times the sample distance.  Samples go G at a time where the
+// march allows: all their taps are fetched before any is interpolated.  The
+// sum is the same for every G (the samples are added one by one in march
+// order).
+constexpr int FP_GROUP = 4;
+
+// `corners(k, c, v)` fetches the 8 corners of cell c, the k-th sample of a
+// group (0 for a sample on its own): loads from an array, or tld4 gathers of
+// its texture (the same values).
+template <int G = FP_GROUP, bool PK = false, typename Corners>
+__device__ __forceinline__ float fp_ray_sum_with(const GeomDev &g, const Corners &corners, const Ray &r, int *count) {
+    Kahan acc{0.0f, 0.0f};
+    int n = 0;
+    march_groups<G>(
+        g, r,
+        [&](const float p[3]) {
+            FpCell c;
+            fp_cell(g, p, c);
+            float v[8];
+            corners(0, c, v);
+            acc.add(__fmul_rn(trilerp(v, c), g.sd));
+            ++n;
+        },
+        [&](const float (*p)[3]) {
+            FpCell c[G];
+            float v[G][8];
+            if constexpr (PK) {  // pairs of samples in the packed FP32x2 instructions
+                static_assert(G % 2 == 0, "samples go in packed pairs");
+#pragma unroll
+                for (int i = 0; i < G; i += 2) {
+                    fp_cell2(g, p[i], p[i + 1], c[i], c[i + 1]);
+                    corners(i, c[i], v[i]);
+                    corners(i + 1, c[i + 1], v[i + 1]);
+                }
+                const float2 sd2 = make_float2(g.sd, g.sd);
+#pragma unroll
+                for (int i = 0; i < G; i += 2) {
+                    const float2 s = __fmul2_rn(trilerp2(v[i], v[i + 1], c[i], c[i + 1]), sd2);
+                    acc.add(s.x);
+                    acc.add(s.y);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < G; ++i) {
+                    fp_cell(g, p[i], c[i]);
+                    corners(i, c[i], v[i]);
+                }
+#pragma unroll
+                for (int i = 0; i < G; ++i) acc.add(__fmul_rn(trilerp(v[i], c[i]), g.sd));
+            }
+            n += G;
+        });
+    if (count) *count = n;
+    return acc.s;
+}
+
+// One job of the persistent sweep (k_persist.cu): one frame's SART call (or
+// one batch instance's) -- V views in the order perm[0 .. V), each the
+// transpose (views that gather along x), the forward projection with the
+// correction and the voxel-based backprojection -- then the ROI mask with the
+// over-relaxation.  The job runs on blocks [block0, block0 + nblocks) of the
+// launch, which meet at the job's own barrier between phases.  Built on the
+// host; vol, volt, stack, xprev and xbar are arrays of the launch's storage
+// (float, or BF16 bits).
+struct SweepJob {
+    GeomDev g;
+    const ViewRec *views;  // the context's view table
+    const int *perm;       // V local view indices (device; drawn by an earlier launch)
+    int view_base, V;      // view perm[i] of the job is table entry view_base + perm[i]
+    void *vol, *volt;      // the frame's volume and its z-fastest copy
+    const void *stack;     // V projections, W*H each, in local view order
+    float *raylen, *corr;  // sticky ray lengths and the correction, W*H each
+    const void *xprev;
+    void *xbar;            // over-relaxed X_bar (null: the ROI mask only)
+    float alpha, gmax;
+    int roi[8], pdcut[8];  // ROI mask cut, primal-dual region cut
+    int block0, nblocks;
+    unsigned *bar;         // [0] arrivals, [1] abort; zeroed before every launch
+    double work;           // relative cost, for the host's split of the blocks
+};
 
 }  // namespace stt

@@ -170,6 +170,19 @@ cudaError_t launch_dot_f64(long long n, const float *a, const float *b, double *
 cudaError_t launch_scale_inv_sqrt(long long n, float *x, const double *norm2, cudaStream_t s);
 cudaError_t launch_fill_seeded(long long n, unsigned long long seed, float *x, cudaStream_t s);
 
+// The persistent sweep (k_persist.cu): the SART calls of all jobs (frames or
+// batch instances, SweepJob in stt_internal.cuh) in one cooperative launch of
+// `nblocks` blocks, jobs_d a device array sorted by block0.  bf16: the jobs'
+// storage; wide: some job's volume has 2^31 voxels or more.
+struct SweepJob;
+// Blocks of the launch that can be resident at once on the current device (0
+// on error): the most a launch may have.
+int sweep_max_blocks(bool bf16, bool wide);
+// Splits nblocks (>= njobs) over the jobs: block0/nblocks from their work.
+void sweep_assign_blocks(SweepJob *jobs, int njobs, int nblocks);
+cudaError_t launch_sweep_persistent(const SweepJob *jobs_d, int njobs, int nblocks, bool bf16, bool wide,
+                                    int *status, cudaStream_t s);
+
 // Voxel-driven backprojection; with the correction as a texture (corr_tex)
 // the column walk of bp variant `bp_variant` runs, else the per-voxel form.
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,

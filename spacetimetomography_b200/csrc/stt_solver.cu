@@ -10,12 +10,17 @@
 //                      correction;
 //   STT_SOLVE_GRAPH    the batched form captured once into a CUDA graph and
 //                      replayed (the view order is drawn on the device from a
-//                      counter, so every replay gets a fresh seeded order).
+//                      counter, so every replay gets a fresh seeded order);
+//   STT_SOLVE_PERSISTENT the duals and primals as in the batched form, then
+//                      every frame's SART call, ROI mask and over-relaxation
+//                      in one persistent cooperative launch (k_persist.cu),
+//                      captured and replayed as a graph.
 //
 // Reordering "all duals, then every frame's primal chain" is exact: frame f's
 // dual reads X_bar[f], X_bar[f+1] and flow[f] only, and X_bar[f] is rewritten
 // only by frame f's own over-relaxation (ST_Tomography.cpp:503-534 vs :598),
 // which the graph orders after the duals of frames f-1 and f.
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -139,6 +144,11 @@ struct stt_solver {
     std::vector<LayeredTex> corr_tex;  // batched modes: per frame, the correction as a texture
     std::vector<stt::FpSlabMaps> fpmaps;  // batched modes: per frame, TMA maps of the volume and its copy
     std::vector<stt::FpTex> fptex;  // batched modes, a tld4 gather form: per frame, the volume's textures
+    stt::SweepJob *jobs_d = nullptr;  // STT_SOLVE_PERSISTENT: one job per frame
+    unsigned *sweep_bar = nullptr;    // the jobs' barrier words (2 per frame)
+    int sweep_blocks = 0;
+    bool sweep_wide = false;
+    bool sweep_direct = false;        // the cooperative launch could not be captured
     std::string err;
 };
 
@@ -365,6 +375,97 @@ stt_status enqueue_batched(stt_solver *s, cudaStream_t main, long long &nl) {
     return enqueue_phase1(s, main, nl, false);
 }
 
+// STT_SOLVE_PERSISTENT, before the sweep: per frame, after the previous
+// frame's dual, the primal step; the frame chains rejoin `main` (`fork`: as in
+// enqueue_phase1).
+stt_status enqueue_primals(stt_solver *s, cudaStream_t main, long long &nl, bool fork) {
+    const int F = s->F;
+    if (fork) {
+        SCUDA(s, cudaEventRecord(s->ev_fork, main), "event record");
+        for (int f = 0; f < F; ++f) SCUDA(s, cudaStreamWaitEvent(s->streams[f], s->ev_fork, 0), "stream wait");
+    }
+    for (int f = 0; f < F; ++f) {
+        cudaStream_t cs = s->streams[f];
+        if (f > 0 && !fork) SCUDA(s, cudaStreamWaitEvent(cs, s->ev_dual[f - 1], 0), "stream wait");
+        stt_status st = bf16(s) ? enqueue_primal<unsigned short>(s, f, cs, nl) : enqueue_primal<float>(s, f, cs, nl);
+        if (st) return st;
+        SCUDA(s, cudaEventRecord(s->ev_done[f], cs), "event record");
+        SCUDA(s, cudaStreamWaitEvent(main, s->ev_done[f], 0), "stream wait");
+    }
+    return STT_OK;
+}
+
+// Every frame's SART call, ROI mask and over-relaxation: one persistent launch.
+stt_status enqueue_sweep(stt_solver *s, cudaStream_t main, long long &nl) {
+    SCUDA(s, cudaMemsetAsync(s->sweep_bar, 0, 2 * (size_t)s->F * sizeof(unsigned), main), "barrier reset");
+    SCUDA(s, stt::launch_sweep_persistent(s->jobs_d, s->F, s->sweep_blocks, bf16(s), s->sweep_wide, s->status, main),
+          "persistent sweep");
+    ++nl;
+    return STT_OK;
+}
+
+stt_status enqueue_persistent(stt_solver *s, cudaStream_t main, long long &nl) {
+    stt_status st = enqueue_phase0(s, main, nl, false);
+    if (!st) st = enqueue_primals(s, main, nl, false);
+    if (!st) st = enqueue_sweep(s, main, nl);
+    return st;
+}
+
+// The solver's frames as persistent-sweep jobs; the caller sets block0,
+// nblocks and bar.
+void fill_jobs(const stt_solver *s, stt::SweepJob *jobs) {
+    const size_t es = s->cfg.storage == STT_DTYPE_BF16 ? 2 : 4, n = s->n, npix = s->npix;
+    const int V = s->V;
+    for (int f = 0; f < s->F; ++f) {
+        stt::SweepJob &J = jobs[f];
+        J = stt::SweepJob{};
+        J.g = *s->g;
+        J.views = s->views;
+        J.perm = s->perm + (size_t)f * V;
+        J.view_base = f * V;
+        J.V = V;
+        J.vol = reinterpret_cast<unsigned char *>(s->st.vol) + (size_t)f * n * es;
+        J.volt = static_cast<unsigned char *>(s->volt) + (size_t)f * n * es;
+        J.stack = reinterpret_cast<const unsigned char *>(s->st.proj) + (size_t)f * V * npix * es;
+        J.raylen = s->raylen + (size_t)f * npix;
+        J.corr = s->corr + (size_t)f * npix;
+        J.xprev = reinterpret_cast<const unsigned char *>(s->st.xprev) + (size_t)f * n * es;
+        J.xbar = reinterpret_cast<unsigned char *>(s->st.xbar) + (size_t)f * n * es;
+        J.alpha = (float)s->cfg.alpha;
+        J.gmax = s->cfg.pd.gmax;
+        for (int q = 0; q < 8; ++q) J.roi[q] = s->cfg.roi_cut[q], J.pdcut[q] = s->cfg.pd.cut[q];
+        const int nmax = std::max(s->g->nx, std::max(s->g->ny, s->g->nz));
+        J.work = (double)V * ((double)n + (double)npix * nmax / 2.0);
+    }
+}
+
+// Captures `enqueue` into a graph: the instantiated graph, or null with the
+// failure cleared (the caller then enqueues directly).
+cudaGraphExec_t try_capture(stt_solver *s, cudaGraph_t &graph, long long &nl,
+                            stt_status (*enqueue)(stt_solver *, cudaStream_t, long long &), stt_status &st) {
+    graph = nullptr;
+    cudaStream_t cap;
+    if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        st = enqueue(s, cap, nl);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(cap, &g);
+        if (!st && ce == cudaSuccess && g && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
+            graph = g;
+        } else {
+            if (g) cudaGraphDestroy(g);
+            exec = nullptr;
+        }
+    }
+    cudaGetLastError();
+    cudaStreamDestroy(cap);
+    return exec;
+}
+
 // The per-view form: frame by frame as the reference loops, each view's
 // forward projection, correction and backprojection as separate launches,
 // and a host synchronisation after every view.
@@ -481,7 +582,8 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     if (cfg->n_frames < 1 || cfg->views_per_frame < 1 || (long long)cfg->n_frames * cfg->views_per_frame > g->n_views)
         return STT_ERR_INVALID;
     if (cfg->bp_mode != 0 && cfg->bp_mode != 1) return STT_ERR_INVALID;
-    if (cfg->mode < STT_SOLVE_PLAIN || cfg->mode > STT_SOLVE_GRAPH) return STT_ERR_INVALID;
+    if (cfg->mode < STT_SOLVE_PLAIN || cfg->mode > STT_SOLVE_PERSISTENT) return STT_ERR_INVALID;
+    if (cfg->mode == STT_SOLVE_PERSISTENT && cfg->bp_mode != 0) return STT_ERR_INVALID;  // voxel-based only
     if (cfg->storage != STT_DTYPE_F32 && cfg->storage != STT_DTYPE_BF16) return STT_ERR_INVALID;
     if (!state->vol || !state->xbar || !state->xprev || !state->ytv || !state->ytp || !state->ybc ||
         !state->flow || !state->proj)
@@ -524,7 +626,9 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     // no views staged for this storage (the tuner found one gather launch per
     // view faster than the two kernels): no maps, one launch per view
     const bool any_staged = (cfg->storage == STT_DTYPE_F32 ? ctx->staged_bins : ctx->staged_bins16) != 0;
-    if (cfg->mode != STT_SOLVE_PLAIN && any_staged) {
+    // (the persistent sweep gathers with loads: no maps, textures or texture copy of the correction)
+    const bool per_view_kernels = cfg->mode == STT_SOLVE_STREAMS || cfg->mode == STT_SOLVE_GRAPH;
+    if (per_view_kernels && any_staged) {
         s->fpmaps.resize(F);
         for (int f = 0; f < F; ++f) {  // where the maps do not apply, ok stays 0 and every view gathers
             if (cfg->storage == STT_DTYPE_F32)
@@ -536,18 +640,18 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
                                        ctx->tuning.slab);
         }
     }
-    if (cfg->mode != STT_SOLVE_PLAIN && cfg->storage == STT_DTYPE_F32 && stt::is_tex_fp_variant(ctx->tuning.fp)) {
+    if (per_view_kernels && cfg->storage == STT_DTYPE_F32 && stt::is_tex_fp_variant(ctx->tuning.fp)) {
         s->fptex.resize(F);  // where they cannot be made, ok stays 0 and the loads run
         for (int f = 0; f < F; ++f)
             stt::make_fp_tex(*g, s->st.vol + f * s->n, static_cast<float *>(s->volt) + f * s->n, s->fptex[f]);
     }
-    if (cfg->mode != STT_SOLVE_PLAIN && cfg->storage == STT_DTYPE_BF16 && ctx->tuning.fp16 == 1) {
+    if (per_view_kernels && cfg->storage == STT_DTYPE_BF16 && ctx->tuning.fp16 == 1) {
         s->fptex.resize(F);
         for (int f = 0; f < F; ++f)
             stt::make_fp_tex(*g, reinterpret_cast<const unsigned short *>(s->st.vol) + f * s->n,
                              static_cast<unsigned short *>(s->volt) + f * s->n, s->fptex[f]);
     }
-    if (cfg->mode != STT_SOLVE_PLAIN && cfg->bp_mode == 0) {
+    if (per_view_kernels && cfg->bp_mode == 0) {
         s->corr_tex.resize(F);
         for (int f = 0; f < F; ++f)
             if (make_layered(g->W, g->H, 1, s->corr_tex[f]) != cudaSuccess) {
@@ -555,6 +659,31 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
                 stt_solver_destroy(s);
                 return STT_ERR_NOMEM;
             }
+    }
+    if (cfg->mode == STT_SOLVE_PERSISTENT) {
+        s->sweep_wide = (long long)g->nx * g->ny * g->nz >= (1LL << 31);  // 64-bit gather offsets
+        s->sweep_blocks = stt::sweep_max_blocks(cfg->storage == STT_DTYPE_BF16, s->sweep_wide);
+        std::vector<stt::SweepJob> jobs(F);
+        fill_jobs(s, jobs.data());
+        if (s->sweep_blocks < F) {
+            stt_solver_destroy(s);
+            return STT_ERR_INVALID;  // fewer resident blocks than frames
+        }
+        stt::sweep_assign_blocks(jobs.data(), F, s->sweep_blocks);
+        e = alloc(s, s->sweep_bar, 2 * (size_t)F, "sweep barriers");
+        unsigned char *jd = nullptr;
+        if (!e) e = alloc(s, jd, F * sizeof(stt::SweepJob), "sweep jobs");
+        s->jobs_d = reinterpret_cast<stt::SweepJob *>(jd);
+        if (e) {
+            stt_solver_destroy(s);
+            return e;
+        }
+        for (int f = 0; f < F; ++f) jobs[f].bar = s->sweep_bar + 2 * f;
+        if (cudaMemcpy(s->jobs_d, jobs.data(), F * sizeof(stt::SweepJob), cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaGetLastError();
+            stt_solver_destroy(s);
+            return STT_ERR_CUDA;
+        }
     }
     cudaError_t ce = cudaMemset(s->raylen, 0, (size_t)F * s->npix * sizeof(float));
     if (ce == cudaSuccess) ce = cudaMemset(s->counter, 0, sizeof(unsigned long long));
@@ -594,6 +723,21 @@ stt_status stt_solver_iterate(stt_solver *s, int n_iters, void *stream) {
         } else if (s->cfg.mode == STT_SOLVE_STREAMS) {
             st = enqueue_batched(s, cs, nl);
             ++s->host_iter;
+        } else if (s->cfg.mode == STT_SOLVE_PERSISTENT) {
+            if (!s->exec && !s->sweep_direct) {
+                stt_status cst = STT_OK;
+                s->exec = try_capture(s, s->graph, nl, enqueue_persistent, cst);
+                if (s->exec) s->launches_per_iter = nl;
+                else s->sweep_direct = true, s->err.clear();
+            }
+            if (s->exec) {
+                SCUDA(s, cudaGraphLaunch(s->exec, cs), "graph launch");
+                nl = s->launches_per_iter;
+            } else {
+                nl = 0;
+                st = enqueue_persistent(s, cs, nl);
+            }
+            ++s->host_iter;
         } else {
             if (!s->exec) {
                 cudaStream_t cap;
@@ -632,6 +776,15 @@ stt_status stt_solver_iterate_phase(stt_solver *s, int phase, void *stream) {
     } else if (s->cfg.mode == STT_SOLVE_STREAMS) {
         st = phase == 0 ? enqueue_phase0(s, cs, nl, true) : enqueue_phase1(s, cs, nl, true);
         if (phase == 1) ++s->host_iter;
+    } else if (s->cfg.mode == STT_SOLVE_PERSISTENT) {
+        // (enqueued directly: a handful of launches per phase)
+        if (phase == 0) {
+            st = enqueue_phase0(s, cs, nl, true);
+        } else {
+            st = enqueue_primals(s, cs, nl, true);
+            if (!st) st = enqueue_sweep(s, cs, nl);
+            ++s->host_iter;
+        }
     } else {
         if (!s->pexec[phase]) {
             cudaStream_t cap;
@@ -674,6 +827,14 @@ stt_status stt_solver_stats(const stt_solver *s, long long *launches_per_iter, u
     return STT_OK;
 }
 
+stt_status stt_solver_persistent_info(const stt_solver *s, int *blocks, int *graph) {
+    if (!s) return STT_ERR_INVALID;
+    const bool p = s->cfg.mode == STT_SOLVE_PERSISTENT;
+    if (blocks) *blocks = p ? s->sweep_blocks : 0;
+    if (graph) *graph = p && s->exec ? 1 : 0;
+    return STT_OK;
+}
+
 stt_status stt_solver_poll_status(stt_solver *s, void *stream) {
     if (!s) return STT_ERR_INVALID;
     cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
@@ -685,7 +846,8 @@ stt_status stt_solver_poll_status(stt_solver *s, void *stream) {
     SCUDA(s, cudaStreamSynchronize(cs), "cudaStreamSynchronize");
     return sfail(s, STT_ERR_TIMEOUT,
                  "a bounded device-side wait gave up: a TMA copy into shared memory did not land within about 0.1 s "
-                 "(the results were computed from global memory instead)");
+                 "(the results were computed from global memory instead), or a barrier of the persistent sweep "
+                 "waited about 1 s (the sweep was abandoned: the iteration's results are not valid)");
 }
 
 const char *stt_solver_last_error(const stt_solver *s) { return s ? s->err.c_str() : ""; }
@@ -707,6 +869,8 @@ stt_status stt_solver_destroy(stt_solver *s) {
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     for (auto &t : s->corr_tex) free_layered(t);
     for (auto &t : s->fptex) stt::destroy_fp_tex(t);
+    cudaFree(s->jobs_d);
+    cudaFree(s->sweep_bar);
     cudaFree(s->warpbuf);
     cudaFree(s->corr);
     cudaFree(s->ax);
@@ -719,6 +883,32 @@ stt_status stt_solver_destroy(stt_solver *s) {
     delete s;
     return STT_OK;
 }
+
+// Hooks of the batch's persistent form (stt_batch.cu), for a solver created
+// with STT_SOLVE_PERSISTENT: one iteration's steps before the sweep, joined
+// into `stream`; the solver's frames as sweep jobs (block ranges and barrier
+// words are the caller's); the end of an iteration whose sweep the caller
+// launched; the status word its sweep should raise.
+stt_status stt_internal_solver_presweep(stt_solver *s, void *stream) {
+    if (!s || s->cfg.mode != STT_SOLVE_PERSISTENT) return STT_ERR_INVALID;
+    long long nl = 0;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+    stt_status st = enqueue_phase0(s, cs, nl, false);
+    if (!st) st = enqueue_primals(s, cs, nl, false);
+    return st;
+}
+
+int stt_internal_solver_jobs(const stt_solver *s, void *jobs) {
+    if (!s || !jobs) return 0;
+    fill_jobs(s, static_cast<stt::SweepJob *>(jobs));
+    return s->F;
+}
+
+void stt_internal_solver_end_iteration(stt_solver *s) {
+    if (s) ++s->host_iter;
+}
+
+int *stt_internal_solver_status(stt_solver *s) { return s ? s->status : nullptr; }
 
 stt_status stt_solver_frame_order(unsigned long long seed, unsigned long long iter, int n_frames, int frame,
                                   int views, int *perm_out) {

@@ -122,7 +122,7 @@ def test_tuning_variant_names_and_struct_layout(lib):
     from spacetimetomography_b200._lib import SolveCfg, Instance, Tuning
 
     # gather projector, slab projector, voxel BP, ray-BP scatter, BF16 gather projector
-    counts = {0: 12, 1: 8, 2: 3, 3: 2, 4: 2}
+    counts = {0: 12, 1: 8, 2: 5, 3: 2, 4: 2}
     for kernel, n in counts.items():
         names = [lib.stt_tuning_variant_name(kernel, v) for v in range(n)]
         assert all(names) and len(set(names)) == n, (kernel, names)
