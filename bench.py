@@ -1195,6 +1195,29 @@ def run_stt(args):
         plain = p0.elapsed_time(p1) / 1000.0
         sp.close()
 
+    # ---- the persistent form: every frame's SART call in one cooperative launch ----
+    persistent = None
+    if not args.no_plain and world == 1 and bp_mode == 0:
+        spp = make_solver(stt.SOLVE_PERSISTENT)
+        spp.iterate(2, stream)  # warm-up (captures the iteration's graph)
+        torch.cuda.synchronize()
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        kq = max(1, min(args.steps, 5))
+        q0.record(stream)
+        spp.iterate(kq, stream)
+        q1.record(stream)
+        torch.cuda.synchronize()
+        spp.poll_status(stream)
+        blocks, graph = spp.persistent_info()
+        t_p = q0.elapsed_time(q1) / 1000.0 / kq
+        persistent = {"s_per_iter": t_p, "gups": F * N ** 3 * V / t_p / 1e9, "graph_vs_persistent": t_p / t_iter,
+                      "blocks": blocks, "graph_captured": graph, "launches_per_iter": spp.stats()[0],
+                      "note": "STT_SOLVE_PERSISTENT: warps, duals and primals as launches, then all frames' SART "
+                              "calls, ROI masks and over-relaxations in one cooperative launch (k_sweep_persistent), "
+                              "the same bits as the graph form; its gathers are plain loads (the texture path is "
+                              "not coherent with the launch's own writes)"}
+        spp.close()
+
     # ---- end to end with host buffers ----
     # Every step uploads its inputs (volumes, flows, projections) from pinned
     # host memory and reads its result back.  On one GPU this goes through the
@@ -1295,6 +1318,7 @@ def run_stt(args):
                 "s_per_4d_pd_iter": t_iter,
                 "plain_s_per_iter": plain,
                 "batched_vs_plain": (plain / t_iter) if plain else None,
+                "persistent": persistent,
                 "roofline": {"bound": "hbm", "kernel": "k_fp_corr (forward projection + SART correction)",
                              "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                              "peak_source": peak_kind, "traffic": traffic_per_launch(args),
@@ -1457,6 +1481,23 @@ def run_batch_only(args):
     bf16_vs_f32 = math.sqrt(num / den)
     bf16_err = [float((d["vol"].float() - o["truth"]).norm() / o["truth"].norm()) for d, o in zip(inst16[:4], inst)]
     del inst16
+    # every instance's SART call in ONE persistent cooperative launch per
+    # iteration (STT_SOLVE_PERSISTENT), the same iterations from the same start
+    for d in inst:
+        d["vol"].zero_()
+    bpers = stt.Batch(inst, mode=stt.SOLVE_PERSISTENT)
+    for _ in range(args.warmup):
+        bpers.iterate(1, stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        bpers.iterate(1, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    bpers.poll_status(stream)
+    t_pers = e0.elapsed_time(e1) / 1000.0 / args.steps
+    bpers.close()
+    pers_diff = max(float((d["vol"] - r).abs().max()) for d, r in zip(inst, f32_result))
     # the instances' own tuned choices again (the batches may have set their
     # staged masks to 0), for the one-after-another forms below
     for d, c in zip(inst, choices):
@@ -1510,6 +1551,10 @@ def run_batch_only(args):
             "plain_note": "the same instances one after another in the per-view form (STT_SOLVE_PLAIN: each "
                           "view's launches from a host loop, a host synchronisation per view)",
             "rel_l2_to_phantom_first4": errs,
+            "persistent": {"ms_per_iter": 1000 * t_pers, "gups": units / t_pers / 1e9,
+                           "graph_vs_persistent": t_pers / t_batch, "max_abs_diff_to_graph_batch": pers_diff,
+                           "note": "STT_SOLVE_PERSISTENT: every instance's duals and primal on its stream, then all "
+                                   "64 SART calls in one cooperative launch (blocks split by work)"},
             "bf16_storage": {"ms_per_iter": 1000 * t_b16, "gups": units / t_b16 / 1e9,
                              "rel_l2_to_f32_storage": bf16_vs_f32, "rel_l2_to_phantom_first4": bf16_err,
                              "iterations": args.warmup + args.steps,

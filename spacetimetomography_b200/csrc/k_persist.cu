@@ -3,10 +3,16 @@
 // and the ROI mask with the over-relaxation that follows it (:586-604,
 // :793-804), in ONE cooperative launch.
 //
-// The blocks of the launch are split into jobs (SweepJob: one frame or one
-// instance each, blocks in proportion to its work).  A job's blocks walk its
-// views in the frame's order; per view, three phases separated by the job's
-// own barrier:
+// The jobs (SweepJob: one frame or one instance each) share the launch's
+// blocks in proportion to their work and run side by side; only when there
+// are more jobs than resident blocks do they run in rounds (a block moves on
+// to its job of the next round as soon as its own is done: jobs are
+// independent, so there is no barrier between rounds).  Measured on the 10
+// frames of 256^3 with 36 views each: side by side 160 ms per iteration, one
+// frame after another on every block 179 ms -- a block then has two detector
+// tiles per view, the slowest block sets each phase's time, and every barrier
+// spans all 1036 blocks.  A job's blocks walk its views in the frame's order;
+// per view, three phases separated by the job's own barrier:
 //   transpose  (views that gather along x) the z-fastest copy of the volume,
 //              32 x 32 tiles through shared memory;
 //   project    the forward projection with the SART correction, one thread
@@ -30,13 +36,17 @@
 // The barrier: a block's thread 0 makes the block's writes visible
 // (__threadfence), adds one arrival to the job's counter, and polls it with
 // acquire loads until all of the job's blocks have arrived.  The launch is
-// cooperative, so every block is resident and every wait ends; the poll is
-// still bounded (about 1 s by the global timer): a wait that runs out raises
-// the job's abort word and the status word (STT_WAIT_TIMEOUT_FLAG), and every
-// block of the job leaves at its next barrier.
+// cooperative, so every block is resident and every wait ends (a block that
+// reaches a job early waits for the job's other blocks to finish their
+// previous round's jobs); the poll is still bounded (about 5 s by the global
+// timer): a wait that runs out raises the job's abort word and the status
+// word (STT_WAIT_TIMEOUT_FLAG), and every block of the job leaves at its next
+// barrier.
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
 #include "stt_voxel.cuh"
+
+#include <algorithm>
 
 namespace stt {
 
@@ -44,7 +54,7 @@ namespace {
 
 constexpr int SWEEP_THREADS = 128;
 constexpr int SWEEP_COL = 16;                              // voxels per column of the backprojection
-constexpr unsigned long long SWEEP_WAIT_NS = 1000000000ull;  // bound of one barrier wait
+constexpr unsigned long long SWEEP_WAIT_NS = 5000000000ull;  // bound of one barrier wait
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -115,18 +125,12 @@ __device__ __forceinline__ void sweep_fp_pixel(const GeomDev &g, const ViewRec &
     corr[pix] = __fdiv_rn(__fsub_rn(ld_voxel(b + pix), sum), __fadd_rn(L, 1.0f));
 }
 
-// Seven blocks per SM: 72 registers, no spills (eight would spill); 1036
-// resident blocks on 148 SMs.
+// One job on this block (rank `rank` of the job's nblocks): false when the
+// job aborted.
 template <typename T, typename I>
-__global__ void __launch_bounds__(SWEEP_THREADS, 7) k_sweep_persistent(const SweepJob *__restrict__ jobs, int njobs,
-                                                                    int *status) {
-    __shared__ T tile[32][33];
-    int jid = 0;
-    while (jid + 1 < njobs && (int)blockIdx.x >= jobs[jid + 1].block0) ++jid;
-    const SweepJob &J = jobs[jid];
+__device__ __forceinline__ bool run_job(const SweepJob &J, int rank, T (*tile)[33], int *status) {
     const GeomDev g = J.g;
-    const int rank = (int)blockIdx.x - J.block0, nb = J.nblocks;
-    if (rank < 0 || rank >= nb) return;  // (blocks beyond the last job's range: none by construction)
+    const int nb = J.nblocks;
     T *vol = static_cast<T *>(J.vol);
     T *volt = static_cast<T *>(J.volt);
     const T *stack = static_cast<const T *>(J.stack);
@@ -149,7 +153,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 7) k_sweep_persistent(const Swe
                         volt[(z0 + lane) + (size_t)y * g.nz + (size_t)(x0 + r) * nzy] = tile[lane][r];
                 __syncthreads();
             }
-            if (!sweep_barrier(J.bar, ++passed * nb, status)) return;
+            if (!sweep_barrier(J.bar, ++passed * nb, status)) return false;
         }
         {  // forward projection + correction
             const T *b = stack + (size_t)local * npix;
@@ -159,7 +163,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 7) k_sweep_persistent(const Swe
                 if (i < g.W && j < g.H) sweep_fp_pixel<I>(g, vr, vol, volt, b, J.raylen, J.corr, i, j);
             }
         }
-        if (!sweep_barrier(J.bar, ++passed * nb, status)) return;
+        if (!sweep_barrier(J.bar, ++passed * nb, status)) return false;
         {  // voxel-based backprojection
             const int cx = (g.nx + SWEEP_THREADS - 1) / SWEEP_THREADS, cy = (g.ny + SWEEP_COL - 1) / SWEEP_COL;
             const BpRowsLoad rows{J.corr, g.W};
@@ -169,15 +173,32 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 7) k_sweep_persistent(const Swe
                 if (x < g.nx) bp_column<SWEEP_COL, false>(g, vr, rows, vol, x, y0, z, J.alpha, J.gmax);
             }
         }
-        if (!sweep_barrier(J.bar, ++passed * nb, status)) return;
+        if (!sweep_barrier(J.bar, ++passed * nb, status)) return false;
     }
-    // the ROI mask and the over-relaxation
+    // the ROI mask and the over-relaxation (the job's last step: nothing of
+    // this job reads it before the launch ends)
     const int rx = (g.nx + SWEEP_THREADS - 1) / SWEEP_THREADS;
     const T *xprev = static_cast<const T *>(J.xprev);
     T *xbar = static_cast<T *>(J.xbar);
     for (int t = rank; t < rx * g.ny * g.nz; t += nb) {
         const int i = (t % rx) * SWEEP_THREADS + threadIdx.x, j = (t / rx) % g.ny, k = t / (rx * g.ny);
         if (i < g.nx) roi_apply_at(i, j, k, g.nx, g.ny, g.nz, J.roi, J.pdcut, vol, xprev, xbar);
+    }
+    return true;
+}
+
+// Seven blocks per SM: 72 registers, no spills (eight would spill); 1036
+// resident blocks on 148 SMs.  jobs: sorted by round; a block runs, round
+// after round, the job whose block range holds it.
+template <typename T, typename I>
+__global__ void __launch_bounds__(SWEEP_THREADS, 7) k_sweep_persistent(const SweepJob *__restrict__ jobs, int njobs,
+                                                                       int *status) {
+    __shared__ T tile[32][33];
+    const int b = (int)blockIdx.x;
+    for (int q = 0; q < njobs; ++q) {
+        const SweepJob &J = jobs[q];
+        if (b < J.block0 || b >= J.block0 + J.nblocks) continue;  // another block's job of this round
+        if (!run_job<T, I>(J, b - J.block0, tile, status)) return;
     }
 }
 
@@ -202,28 +223,44 @@ int sweep_max_blocks(bool bf16, bool wide) {
     return per_sm * sm_count();
 }
 
-void sweep_assign_blocks(SweepJob *jobs, int njobs, int nblocks) {
+namespace {
+// One round's jobs [q0, q1) share all nblocks: every job one block, the rest
+// in proportion to the work.
+void split_round(SweepJob *jobs, int q0, int q1, int nblocks) {
     double total = 0.0;
-    for (int q = 0; q < njobs; ++q) total += jobs[q].work > 0.0 ? jobs[q].work : 1.0;
-    // every job one block, the rest in proportion to the work (largest remainders last)
-    int spare = nblocks - njobs, given = 0;
-    for (int q = 0; q < njobs; ++q) {
+    for (int q = q0; q < q1; ++q) total += jobs[q].work > 0.0 ? jobs[q].work : 1.0;
+    const int spare = nblocks - (q1 - q0);
+    int given = 0;
+    for (int q = q0; q < q1; ++q) {
         const double w = jobs[q].work > 0.0 ? jobs[q].work : 1.0;
-        const int extra = (int)((double)spare * w / total);
-        jobs[q].nblocks = 1 + extra;
+        jobs[q].nblocks = 1 + (int)((double)spare * w / total);
         given += jobs[q].nblocks;
     }
-    for (int q = 0; given < nblocks; q = (q + 1) % njobs, ++given) ++jobs[q].nblocks;
+    for (int q = q0; given < nblocks; q = q + 1 < q1 ? q + 1 : q0, ++given) ++jobs[q].nblocks;
     int b0 = 0;
-    for (int q = 0; q < njobs; ++q) {
+    for (int q = q0; q < q1; ++q) {
         jobs[q].block0 = b0;
         b0 += jobs[q].nblocks;
     }
 }
+}  // namespace
+
+int sweep_plan(SweepJob *jobs, int njobs, int nblocks) {
+    if (njobs < 1 || nblocks < 1) return 0;
+    // largest first, at most nblocks jobs a round
+    std::stable_sort(jobs, jobs + njobs, [](const SweepJob &a, const SweepJob &b) { return a.work > b.work; });
+    int rounds = 0;
+    for (int q0 = 0; q0 < njobs; q0 += nblocks, ++rounds) {
+        const int q1 = q0 + nblocks < njobs ? q0 + nblocks : njobs;
+        split_round(jobs, q0, q1, nblocks);
+        for (int k = q0; k < q1; ++k) jobs[k].round = rounds;
+    }
+    return rounds;
+}
 
 cudaError_t launch_sweep_persistent(const SweepJob *jobs_d, int njobs, int nblocks, bool bf16, bool wide,
                                     int *status, cudaStream_t s) {
-    if (njobs < 1 || nblocks < njobs) return cudaErrorInvalidValue;
+    if (njobs < 1 || nblocks < 1) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(nblocks);
     cfg.blockDim = dim3(SWEEP_THREADS);

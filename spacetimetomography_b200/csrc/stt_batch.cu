@@ -41,7 +41,7 @@ struct stt_batch {
     stt::SweepJob *jobs_d = nullptr;
     unsigned *bar = nullptr;
     int *status = nullptr;
-    int sweep_blocks = 0;
+    int sweep_blocks = 0, rounds = 0;
     bool bf16 = false, wide = false, direct = false;
     int staging_timed = 0, all_gather = 0;
     float ms_split = 0.0f, ms_gather = 0.0f;
@@ -122,10 +122,8 @@ stt_status build_sweep(stt_batch *b) {
         b->wide |= (long long)g.nx * g.ny * g.nz >= (1LL << 31);
     }
     b->sweep_blocks = stt::sweep_max_blocks(b->bf16, b->wide);
-    if (b->sweep_blocks < n)
-        return bfail(b, STT_ERR_INVALID, "more instances than resident blocks of the persistent sweep (" +
-                                             std::to_string(b->sweep_blocks) + ")");
-    stt::sweep_assign_blocks(jobs.data(), n, b->sweep_blocks);
+    if (b->sweep_blocks < 1) return bfail(b, STT_ERR_CUDA, "occupancy of the persistent sweep");
+    b->rounds = stt::sweep_plan(jobs.data(), n, b->sweep_blocks);
     if (cudaMalloc(&b->bar, 2 * (size_t)n * sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&b->jobs_d, n * sizeof(stt::SweepJob)) != cudaSuccess ||
         cudaMalloc(&b->status, sizeof(int)) != cudaSuccess) {

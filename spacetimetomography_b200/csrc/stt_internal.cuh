@@ -662,10 +662,12 @@ __device__ __forceinline__ float fp_ray_sum_with(const GeomDev &g, const Corners
 // one batch instance's) -- V views in the order perm[0 .. V), each the
 // transpose (views that gather along x), the forward projection with the
 // correction and the voxel-based backprojection -- then the ROI mask with the
-// over-relaxation.  The job runs on blocks [block0, block0 + nblocks) of the
-// launch, which meet at the job's own barrier between phases.  Built on the
-// host; vol, volt, stack, xprev and xbar are arrays of the launch's storage
-// (float, or BF16 bits).
+// over-relaxation.  Jobs run in rounds: in its round a job has blocks
+// [block0, block0 + nblocks) of the launch, which meet at the job's own
+// barrier between phases; a block goes on to its job of the next round when
+// its job is done (jobs are independent).  Built on the host; vol, volt,
+// stack, xprev and xbar are arrays of the launch's storage (float, or BF16
+// bits).
 struct SweepJob {
     GeomDev g;
     const ViewRec *views;  // the context's view table
@@ -678,7 +680,7 @@ struct SweepJob {
     void *xbar;            // over-relaxed X_bar (null: the ROI mask only)
     float alpha, gmax;
     int roi[8], pdcut[8];  // ROI mask cut, primal-dual region cut
-    int block0, nblocks;
+    int round, block0, nblocks;
     unsigned *bar;         // [0] arrivals, [1] abort; zeroed before every launch
     double work;           // relative cost, for the host's split of the blocks
 };

@@ -178,8 +178,11 @@ struct SweepJob;
 // Blocks of the launch that can be resident at once on the current device (0
 // on error): the most a launch may have.
 int sweep_max_blocks(bool bf16, bool wide);
-// Splits nblocks (>= njobs) over the jobs: block0/nblocks from their work.
-void sweep_assign_blocks(SweepJob *jobs, int njobs, int nblocks);
+// Orders the jobs into rounds (largest first, at most nblocks jobs a round:
+// one round unless there are more jobs than blocks) and splits the nblocks
+// over each round's jobs in proportion to their work: sets round, block0 and
+// nblocks and sorts the array by round.  Returns the number of rounds.
+int sweep_plan(SweepJob *jobs, int njobs, int nblocks);
 cudaError_t launch_sweep_persistent(const SweepJob *jobs_d, int njobs, int nblocks, bool bf16, bool wide,
                                     int *status, cudaStream_t s);
 

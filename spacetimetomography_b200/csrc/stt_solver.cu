@@ -665,11 +665,11 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
         s->sweep_blocks = stt::sweep_max_blocks(cfg->storage == STT_DTYPE_BF16, s->sweep_wide);
         std::vector<stt::SweepJob> jobs(F);
         fill_jobs(s, jobs.data());
-        if (s->sweep_blocks < F) {
+        if (s->sweep_blocks < 1) {
             stt_solver_destroy(s);
-            return STT_ERR_INVALID;  // fewer resident blocks than frames
+            return STT_ERR_CUDA;  // the occupancy query failed
         }
-        stt::sweep_assign_blocks(jobs.data(), F, s->sweep_blocks);
+        stt::sweep_plan(jobs.data(), F, s->sweep_blocks);
         e = alloc(s, s->sweep_bar, 2 * (size_t)F, "sweep barriers");
         unsigned char *jd = nullptr;
         if (!e) e = alloc(s, jd, F * sizeof(stt::SweepJob), "sweep jobs");

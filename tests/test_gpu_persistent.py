@@ -112,3 +112,43 @@ def test_persistent_mode_refuses_ray_backprojection(cuda):
     with pytest.raises(stt.STTError):
         stt.Solver(ctx, g, F, V, pd, bp_mode=1, roi_cut=ROI_CUT, mode=stt.SOLVE_PERSISTENT)
     ctx.close()
+
+
+def test_persistent_larger_frames_equal_graph(cuda):
+    """Two frames of 160 x 160 x 164 voxels (4 views each, 128 x 112
+    detector; every block runs thousands of tiles per phase): the same bits
+    as the graph solve."""
+    import math
+
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200 import phantom as ph
+
+    dims, det, Fr, Vr = (160, 160, 164), (128, 112), 2, 4
+    angles = np.arange(Fr * Vr) * (2 * math.pi / (Fr * Vr)) + 0.2
+    outs = {}
+    for mode in (stt.SOLVE_GRAPH, stt.SOLVE_PERSISTENT):
+        ctx = stt.Context(0)
+        ctx.set_geometry(dims, (1.0, 1.0, 1.0), det, 1.6, 600.0, 1000.0, angles)
+        n = dims[::-1]
+        truth = ph.ellipsoid_phantom(dims, 8, seed=7, semi=(8.0, 40.0)).to(cuda)
+        proj = torch.zeros((Fr * Vr, det[1], det[0]), device=cuda)
+        ctx.fp(truth, proj)
+        vol = (0.5 * truth).expand(Fr + 1, *n).contiguous()
+        st = dict(vol=vol, xbar=vol.clone(), xprev=torch.zeros((Fr,) + n, device=cuda),
+                  ytv=torch.zeros((Fr, 3) + n, device=cuda), ytp=torch.zeros((Fr,) + n, device=cuda),
+                  ybc=torch.zeros((Fr,) + n, device=cuda), flow=torch.zeros((Fr, 3) + n, device=cuda),
+                  proj=proj.view(Fr, Vr, det[1], det[0]).contiguous())
+        pd = stt.PdParams(tv_w=0.01, tp_w=0.1, bc_w=0.05, huber_factor=0.9, gmax=float(proj.max()) / 4,
+                          cut=(4, 4, 4, 8, 4, 4, 8, 6))
+        s = stt.Solver(ctx, st, Fr, Vr, pd, alpha=0.3, roi_cut=(4, 4, 4, 8, 4, 4, 8, 6), seed=3, mode=mode)
+        s.iterate(2)
+        torch.cuda.synchronize()
+        s.poll_status()
+        outs[mode] = {k: st[k].cpu().numpy() for k in KEYS}
+        s.close()
+        ctx.close()
+    assert np.abs(outs[stt.SOLVE_GRAPH]["vol"]).max() > 0
+    for k in KEYS:
+        np.testing.assert_array_equal(outs[stt.SOLVE_PERSISTENT][k], outs[stt.SOLVE_GRAPH][k], err_msg=k)
