@@ -212,7 +212,12 @@ stt_status stt_fp_vjp(stt_ctx *ctx, const float *proj_bar, float *vol_bar, int v
 /* ---- backprojectors ------------------------------------------------------
  * Voxel-driven (ST_Tomography.cpp:690-730): vol = clamp(vol + alpha *
  * bicubic(corr at the voxel's projection), 0, gmax); voxels projecting
- * outside [2, W-2) x [2, H-2) are left unchanged.  Deterministic. */
+ * outside [2, W-2) x [2, H-2) are left unchanged.  Deterministic.  From
+ * 2^23 voxels on, corr is first copied (on `stream`) into a texture the
+ * context owns, which the column walk of the tuned bp_variant gathers from
+ * (stt_sart_sweep writes it from the projector directly, at every size);
+ * calls of one context that overlap on different streams race on that copy.
+ * The result is the same either way. */
 stt_status stt_bp_voxel(stt_ctx *ctx, const float *corr, float *vol, double alpha, float gmax,
                         int view, void *stream);
 /* stt_bp_voxel on a volume stored as `dtype` (STT_DTYPE_BF16: each voxel is

@@ -285,6 +285,37 @@ cudaError_t pd_extrapolate_any(const int *d, const int *cut, const T *vol, const
 }
 }  // namespace
 
+cudaError_t make_corr_tex(int W, int H, CorrTex &o) {
+    o = CorrTex{};
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+    cudaError_t e = cudaMalloc3DArray(&o.arr, &cd, make_cudaExtent(W, H, 1), cudaArrayLayered | cudaArraySurfaceLoadStore);
+    if (e != cudaSuccess) return e;
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = o.arr;
+    cudaTextureDesc td{};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaTextureObject_t t = 0;
+    cudaSurfaceObject_t sf = 0;
+    if ((e = cudaCreateTextureObject(&t, &rd, &td, nullptr)) == cudaSuccess) e = cudaCreateSurfaceObject(&sf, &rd);
+    o.tex = t;
+    o.surf = sf;
+    o.W = W;
+    o.H = H;
+    if (e != cudaSuccess) free_corr_tex(o);
+    return e;
+}
+
+void free_corr_tex(CorrTex &o) {
+    if (o.surf) cudaDestroySurfaceObject((cudaSurfaceObject_t)o.surf);
+    if (o.tex) cudaDestroyTextureObject((cudaTextureObject_t)o.tex);
+    if (o.arr) cudaFreeArray(o.arr);
+    o = CorrTex{};
+}
+
 const char *bp_variant_name(int v) {
     static const char *names[kBpVariants] = {"columns of 16 voxels", "columns of 8 voxels", "columns of 32 voxels",
                                              "columns of 16 voxels, L2 prefetch", "columns of 32 voxels, L2 prefetch"};

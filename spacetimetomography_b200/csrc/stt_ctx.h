@@ -25,6 +25,10 @@ struct stt_ctx {
     size_t acc_n = 0;
     float *corr = nullptr;  // W*H correction image used by stt_sart_sweep
     size_t corr_n = 0;
+    // The correction as a texture for the column backprojection of
+    // stt_sart_sweep and stt_bp_voxel (made on first use at the geometry's
+    // W x H; tex 0 where it could not be made: the per-voxel load form runs).
+    stt::CorrTex corr_tex{};
     float *volt = nullptr;  // z-fastest copy of the volume for views gathering along x
     size_t volt_n = 0;
     unsigned short *volt16 = nullptr;  // the same for a BF16-stored volume

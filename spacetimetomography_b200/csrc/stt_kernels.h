@@ -186,6 +186,17 @@ int sweep_plan(SweepJob *jobs, int njobs, int nblocks);
 cudaError_t launch_sweep_persistent(const SweepJob *jobs_d, int njobs, int nblocks, bool bf16, bool wide,
                                     int *status, cudaStream_t s);
 
+// The correction image held as a one-layer layered CUDA array: the texture
+// object the column backprojection gathers from (tld4) and the surface object
+// the fused forward projection writes (launch_fp_corr's corr_surf).
+struct CorrTex {
+    cudaArray_t arr = nullptr;
+    unsigned long long tex = 0, surf = 0;
+    int W = 0, H = 0;
+};
+cudaError_t make_corr_tex(int W, int H, CorrTex &o);
+void free_corr_tex(CorrTex &o);
+
 // Voxel-driven backprojection; with the correction as a texture (corr_tex)
 // the column walk of bp variant `bp_variant` runs, else the per-voxel form.
 cudaError_t launch_bp_voxel(const GeomDev &g, const ViewRec *views, const ViewSel &sel, const float *corr,

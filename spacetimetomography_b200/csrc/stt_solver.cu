@@ -104,15 +104,6 @@ void host_perm(unsigned long long seed, unsigned long long iter, int frames, int
 // The context internals the solver needs (defined in stt_capi.cu).
 extern "C" stt_status stt_internal_geom(stt_ctx *ctx, const void **geom, const void **views);
 
-// An image held as a one-layer layered CUDA array, with the texture object
-// the voxel-driven backprojector gathers from and the surface object the
-// fused forward projection writes.
-struct LayeredTex {
-    cudaArray_t arr = nullptr;
-    cudaTextureObject_t tex = 0;
-    cudaSurfaceObject_t surf = 0;
-};
-
 struct stt_solver {
     stt_ctx *ctx = nullptr;
     stt_solve_cfg cfg{};
@@ -141,7 +132,7 @@ struct stt_solver {
     cudaGraphExec_t pexec[2] = {nullptr, nullptr};
     long long launches_per_iter = 0;
     long long phase_launches[2] = {0, 0};
-    std::vector<LayeredTex> corr_tex;  // batched modes: per frame, the correction as a texture
+    std::vector<stt::CorrTex> corr_tex;  // batched modes: per frame, the correction as a texture
     std::vector<stt::FpSlabMaps> fpmaps;  // batched modes: per frame, TMA maps of the volume and its copy
     std::vector<stt::FpTex> fptex;  // batched modes, a tld4 gather form: per frame, the volume's textures
     stt::SweepJob *jobs_d = nullptr;  // STT_SOLVE_PERSISTENT: one job per frame
@@ -153,31 +144,6 @@ struct stt_solver {
 };
 
 namespace {
-
-cudaError_t make_layered(int w, int h, int layers, LayeredTex &o) {
-    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
-    cudaError_t e = cudaMalloc3DArray(&o.arr, &cd, make_cudaExtent(w, h, layers),
-                                      cudaArrayLayered | cudaArraySurfaceLoadStore);
-    if (e != cudaSuccess) return e;
-    cudaResourceDesc rd{};
-    rd.resType = cudaResourceTypeArray;
-    rd.res.array.array = o.arr;
-    cudaTextureDesc td{};
-    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
-    td.filterMode = cudaFilterModePoint;
-    td.readMode = cudaReadModeElementType;
-    td.normalizedCoords = 0;
-    e = cudaCreateTextureObject(&o.tex, &rd, &td, nullptr);
-    if (e != cudaSuccess) return e;
-    return cudaCreateSurfaceObject(&o.surf, &rd);
-}
-
-void free_layered(LayeredTex &o) {
-    if (o.surf) cudaDestroySurfaceObject(o.surf);
-    if (o.tex) cudaDestroyTextureObject(o.tex);
-    if (o.arr) cudaFreeArray(o.arr);
-    o = LayeredTex{};
-}
 
 stt_status sfail(stt_solver *s, stt_status st, const std::string &m) {
     if (s) s->err = m;
@@ -654,7 +620,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
     if (per_view_kernels && cfg->bp_mode == 0) {
         s->corr_tex.resize(F);
         for (int f = 0; f < F; ++f)
-            if (make_layered(g->W, g->H, 1, s->corr_tex[f]) != cudaSuccess) {
+            if (stt::make_corr_tex(g->W, g->H, s->corr_tex[f]) != cudaSuccess) {
                 cudaGetLastError();
                 stt_solver_destroy(s);
                 return STT_ERR_NOMEM;
@@ -867,7 +833,7 @@ stt_status stt_solver_destroy(stt_solver *s) {
     for (auto e : s->ev_done)
         if (e) cudaEventDestroy(e);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
-    for (auto &t : s->corr_tex) free_layered(t);
+    for (auto &t : s->corr_tex) stt::free_corr_tex(t);
     for (auto &t : s->fptex) stt::destroy_fp_tex(t);
     cudaFree(s->jobs_d);
     cudaFree(s->sweep_bar);
