@@ -71,6 +71,12 @@ struct stt_flow {
     int *iters = nullptr;
     float *errs = nullptr;
     int n_stat = 0, stat_cap = 0;
+    // The stop flag as the host last saw it: at every residual check the flag
+    // is copied into a slot of this pinned ring behind an event, so the host
+    // can stop enqueuing a warp whose iterations stopped (enqueue_level).
+    static constexpr int kRing = 8, kLookahead = 4;
+    int *done_host = nullptr;
+    cudaEvent_t ring_ev[kRing] = {};
 
     stt_status fail(stt_status st, const std::string &m) {
         err = m;
@@ -93,6 +99,9 @@ struct stt_flow {
     }
     ~stt_flow() {
         for (void *q : allocs) cudaFree(q);
+        for (cudaEvent_t e : ring_ev)
+            if (e) cudaEventDestroy(e);
+        if (done_host) cudaFreeHost(done_host);
     }
 };
 
@@ -180,6 +189,23 @@ stt_status enqueue_level(stt_flow *f, const int *d, const float *box, const int 
     const bool runs = 1.0f > p.tol;  // err starts at 1 (optical_flow.h:305-306)
     const int last = p.max_iter + 1;
     bool any_dual = false;
+    // Once a warp's check has stopped it, the launches of its remaining
+    // iterations return at once, but each still costs its full grid (about
+    // 75 us per iteration at 256^3; with the reference's parameters the warps
+    // of a 256^3 multiscale solve stop after 400-1000 of their 3001
+    // iterations).  So after every check the stop flag is copied to pinned
+    // host memory behind an event; the host stays at most kLookahead checks
+    // ahead of the device, and when a copy that has landed shows the warp
+    // stopped, the rest of its iterations are not enqueued (they would have
+    // done nothing: the same results, and the same iteration counts, which
+    // the check recorded when it stopped).  Not while the stream is being
+    // captured: then every iteration is enqueued.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        cap = cudaStreamCaptureStatusActive;
+    }
+    const bool poll = cap == cudaStreamCaptureStatusNone;
     for (int w = 0; w < p.n_warps; ++w) {
         int *it_slot = f->iters + stat0 + w;
         float *err_slot = f->errs + stat0 + w;
@@ -188,6 +214,7 @@ stt_status enqueue_level(stt_flow *f, const int *d, const float *box, const int 
         FLOW_CUDA(f, stt::launch_flow_setup(d, roi, f->i2w, i1, V, f->u, f->tau, f->sig2, f->k4prev, s),
                   "k_flow_setup");
         if (!runs) continue;
+        int pushed = 0, seen = 0;  // checks whose flag copy was enqueued / looked at
         for (int it = 1; it <= last; ++it) {
             int flags = (it % 50 == 0 ? 1 : 0) | ((it + 1) % 50 == 0 ? 2 : 0);
             if (it == 1) flags |= any_dual ? 8 : 4;
@@ -203,6 +230,35 @@ stt_status enqueue_level(stt_flow *f, const int *d, const float *box, const int 
                 FLOW_CUDA(f, stt::launch_flow_check(f->resid, n, p.tol, it, flags & 1, it == last, f->done, it_slot,
                                                     err_slot, s),
                           "k_flow_check");
+            if (poll && (flags & 1) && it < last) {
+                // at most kLookahead checks (kLookahead * 50 iterations) ahead of the
+                // device: past that, wait for the oldest copy, so that no more than
+                // those iterations are enqueued after the warp stopped
+                if (pushed - seen >= stt_flow::kLookahead) {
+                    FLOW_CUDA(f, cudaEventSynchronize(f->ring_ev[seen % stt_flow::kRing]), "cudaEventSynchronize");
+                    if (f->done_host[seen % stt_flow::kRing]) break;
+                    ++seen;
+                }
+                const int q = pushed++ % stt_flow::kRing;
+                FLOW_CUDA(f, cudaMemcpyAsync(f->done_host + q, f->done, sizeof(int), cudaMemcpyDeviceToHost, s),
+                          "copy stop flag");
+                FLOW_CUDA(f, cudaEventRecord(f->ring_ev[q], s), "event record");
+                bool stopped = false;
+                while (seen < pushed) {
+                    const cudaError_t qe = cudaEventQuery(f->ring_ev[seen % stt_flow::kRing]);
+                    if (qe == cudaErrorNotReady) {
+                        cudaGetLastError();  // (not an error: the copy has not landed yet)
+                        break;
+                    }
+                    FLOW_CUDA(f, qe, "cudaEventQuery");
+                    if (f->done_host[seen % stt_flow::kRing]) {
+                        stopped = true;
+                        break;
+                    }
+                    ++seen;
+                }
+                if (stopped) break;
+            }
         }
         any_dual = true;
         FLOW_CUDA(f, stt::launch_flow_settle(3 * n, it_slot, f->vpp, V, s), "k_flow_settle");
@@ -295,6 +351,17 @@ stt_status stt_flow_create(int device, const int *dims, const stt_flow_params *p
     f->stat_cap = std::max(1, (int)f->lev.size() * std::max(1, p->n_warps));
     A(&f->iters, f->stat_cap);
     A(&f->errs, f->stat_cap);
+    if (st == STT_OK && cudaHostAlloc((void **)&f->done_host, stt_flow::kRing * sizeof(int), cudaHostAllocDefault) !=
+                            cudaSuccess) {
+        cudaGetLastError();
+        f->done_host = nullptr;
+        st = f->fail(STT_ERR_NOMEM, "cudaHostAlloc of the stop-flag ring failed");
+    }
+    for (int q = 0; q < stt_flow::kRing && st == STT_OK; ++q)
+        if (cudaEventCreateWithFlags(&f->ring_ev[q], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            st = f->fail(STT_ERR_CUDA, "event create");
+        }
     if (st != STT_OK) {
         std::string m = f->err;
         delete f;
