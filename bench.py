@@ -514,6 +514,25 @@ def flow_bench(args, dev, stream, rank: int) -> dict:
                         "moved_bytes_per_voxel": 212,
                         "note": "moved per iteration: primal reads y 10, u 3, tau 3, v 3 and writes v 3 (ROI); "
                                 "dual reads v 3, v_old 3, u 4, sigma2 1, y 10 and writes y 10"}}
+    # the whole multiscale solve between the same frames with the reference's
+    # parameters (tol 0.1, 3000 iterations, 3 warps, 3 scales, the ROI cut):
+    # the warps stop on their residuals
+    fm = stt.Flow(dims, stt.FlowParams(cut=cut), device=dev.index or 0)
+    ms = []
+    for _ in range(2):  # (the first is a warm-up)
+        V.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fm.multiscale(i1, i2, V, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    its, _ = fm.stats()
+    fm.close()
+    out["multiscale"] = {"s": ms[-1] / 1000.0, "iterations_per_level_and_warp": its.tolist(),
+                         "workload": f"L1Huber_OF_MultiScale3D, {N}^3, tol 0.1, lambda 1.2, Huber 1, 3000 "
+                                     "iterations, 3 warps, 3 scales (eta 0.65), ROI cut, zero start"}
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = flow_cpu_sample(i1, i2)
     return out
