@@ -38,8 +38,7 @@ __device__ __forceinline__ void scatter_global(const GeomDev &g, const float p[3
     make_taps(g, p, t);
     float w[8];
     tri_weights(t, w);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) atomicAdd(acc + tap_index(t, k), make_float2(c * w[k], w[k]));
+    scatter_corners(acc, t, c, w);
 }
 
 template <bool ZF>

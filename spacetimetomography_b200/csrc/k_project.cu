@@ -161,8 +161,7 @@ __global__ void __launch_bounds__(128) k_bp_ray_scatter(const GeomDev g,
         make_taps(g, p, t);
         float w[8];
         tri_weights(t, w);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) atomicAdd(acc + tap_index(t, k), make_float2(c * w[k], w[k]));
+        scatter_corners(acc, t, c, w);
     });
 }
 

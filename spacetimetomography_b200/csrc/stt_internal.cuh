@@ -363,6 +363,25 @@ __device__ __forceinline__ long long tap_index(const Taps &t, int k) {
     return t.base + ((k & 1) ? t.dx : 0) + ((k & 2) ? t.dy : 0) + ((k & 4) ? t.dz : 0);
 }
 
+// The ray-driven backprojection's update of one sample: (c*w_k, w_k) into the
+// interleaved accumulators of its 8 corners (x-fastest taps).  Corners 2m
+// and 2m+1 are x-neighbours; inside the volume (dx = 1) their accumulators
+// are adjacent, and where the first index is even the two are one aligned
+// 16-byte vector atomic instead of two 8-byte ones (the same terms, fewer
+// atomics at L2, whose atomic rate bounds the scatter).
+__device__ __forceinline__ void scatter_corners(float2 *acc, const Taps &t, float c, const float w[8]) {
+#pragma unroll
+    for (int m = 0; m < 8; m += 2) {
+        const long long idx = tap_index(t, m);
+        if (t.dx == 1 && !(idx & 1)) {
+            atomicAdd(reinterpret_cast<float4 *>(acc + idx), make_float4(c * w[m], w[m], c * w[m + 1], w[m + 1]));
+        } else {
+            atomicAdd(acc + idx, make_float2(c * w[m], w[m]));
+            atomicAdd(acc + idx + t.dx, make_float2(c * w[m + 1], w[m + 1]));
+        }
+    }
+}
+
 // The march of CastingRay (S/ImageFormationModel/RayCaster.core.h:42-188).  The
 // DDA over blocks of size dims splits a ray only where it crosses coordinate
 // 0.5 on an axis it travels down; each segment restarts at
