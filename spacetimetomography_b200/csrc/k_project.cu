@@ -184,8 +184,19 @@ __global__ void __launch_bounds__(128) k_fp_adjoint(const GeomDev g, const ViewR
         make_taps(g, p, t);
         float w[8];
         tri_weights(t, w);
+        // x-neighbour corners inside the volume whose first address is 8-byte
+        // aligned (the caller's vol_bar may start anywhere on 4 bytes): one
+        // vector atomic (the same terms)
 #pragma unroll
-        for (int k = 0; k < 8; ++k) atomicAdd(vol_bar + tap_index(t, k), ys * w[k]);
+        for (int m = 0; m < 8; m += 2) {
+            const long long idx = tap_index(t, m);
+            if (t.dx == 1 && !(reinterpret_cast<uintptr_t>(vol_bar + idx) & 7)) {
+                atomicAdd(reinterpret_cast<float2 *>(vol_bar + idx), make_float2(ys * w[m], ys * w[m + 1]));
+            } else {
+                atomicAdd(vol_bar + idx, ys * w[m]);
+                atomicAdd(vol_bar + idx + t.dx, ys * w[m + 1]);
+            }
+        }
     });
 }
 

@@ -366,14 +366,16 @@ __device__ __forceinline__ long long tap_index(const Taps &t, int k) {
 // The ray-driven backprojection's update of one sample: (c*w_k, w_k) into the
 // interleaved accumulators of its 8 corners (x-fastest taps).  Corners 2m
 // and 2m+1 are x-neighbours; inside the volume (dx = 1) their accumulators
-// are adjacent, and where the first index is even the two are one aligned
-// 16-byte vector atomic instead of two 8-byte ones (the same terms, fewer
-// atomics at L2, whose atomic rate bounds the scatter).
+// are adjacent, and where the first one's address is 16-byte aligned the two
+// are one vector atomic instead of two 8-byte ones (the same terms, fewer
+// atomics at L2, whose atomic rate bounds the scatter).  The test is on the
+// address, not on the index: a frame's accumulators start at acc + f * n,
+// which is only 8-byte aligned when f and n are odd.
 __device__ __forceinline__ void scatter_corners(float2 *acc, const Taps &t, float c, const float w[8]) {
 #pragma unroll
     for (int m = 0; m < 8; m += 2) {
         const long long idx = tap_index(t, m);
-        if (t.dx == 1 && !(idx & 1)) {
+        if (t.dx == 1 && !(reinterpret_cast<uintptr_t>(acc + idx) & 15)) {
             atomicAdd(reinterpret_cast<float4 *>(acc + idx), make_float4(c * w[m], w[m], c * w[m + 1], w[m + 1]));
         } else {
             atomicAdd(acc + idx, make_float2(c * w[m], w[m]));
