@@ -45,6 +45,7 @@
 #include "stt_internal.cuh"
 #include "stt_kernels.h"
 #include "stt_voxel.cuh"
+#include "warp_dev.cuh"
 
 #include <algorithm>
 
@@ -127,8 +128,10 @@ __device__ __forceinline__ void sweep_fp_pixel(const GeomDev &g, const ViewRec &
 
 // One job on this block (rank `rank` of the job's nblocks): false when the
 // job aborted.
+// passed: the job barriers this block has passed before the call.
 template <typename T, typename I>
-__device__ __forceinline__ bool run_job(const SweepJob &J, int rank, T (*tile)[33], int *status) {
+__device__ __forceinline__ bool run_job(const SweepJob &J, int rank, T (*tile)[33], int *status,
+                                       unsigned passed = 0) {
     const GeomDev g = J.g;
     const int nb = J.nblocks;
     T *vol = static_cast<T *>(J.vol);
@@ -136,9 +139,8 @@ __device__ __forceinline__ bool run_job(const SweepJob &J, int rank, T (*tile)[3
     const T *stack = static_cast<const T *>(J.stack);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const size_t nxy = (size_t)g.nx * g.ny, nzy = (size_t)g.nz * g.ny, npix = (size_t)g.W * g.H;
-    unsigned passed = 0;
     for (int v = 0; v < J.V; ++v) {
-        const int local = __ldg(J.perm + v);
+        const int local = J.perm[v];  // (a plain load: the whole-iteration launch draws perm itself)
         const ViewRec &vr = J.views[J.view_base + local];
         if (volt && vr.layout == 1) {  // the z-fastest copy this view gathers from
             const int tx = (g.nx + 31) / 32, tz = (g.nz + 31) / 32;
@@ -202,12 +204,83 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 7) k_sweep_persistent(const Swe
     }
 }
 
+// The whole primal-dual iteration of every job in one cooperative launch
+// (ST_Tomography.cpp:492-607; one round: a block per job at least).  Per job
+// (frame): its view order (from the iteration counter, which its owner job
+// advances once every job has read it); over its voxels the backward warp
+// of X_bar[f+1] along flow[f] and the dual step; a barrier of the whole grid
+// (frame f's primal step reads frame f-1's duals); over its voxels the
+// forward warp of Y_bc[f-1] along flow[f-1] and the primal step; the job's
+// barrier; then the SART call, ROI mask and over-relaxation of run_job.  The
+// warp is the gather form's trace and sample (trace_cell, sample_cell), the
+// dual and primal steps the per-voxel functions of the separate kernels
+// (pd_dual_at, pd_primal_at), the warped value passed in a register; the
+// duals the primal step reads were written in this launch, so it loads them
+// (and the warp's taps of Y_bc[f-1]) with plain loads.
+template <typename T, typename I>
+__global__ void __launch_bounds__(SWEEP_THREADS, 7) k_iter_persistent(const SweepJob *__restrict__ jobs, int njobs,
+                                                                      unsigned *gbar, int *status) {
+    __shared__ T tile[32][33];
+    const int b = (int)blockIdx.x;
+    int q = 0;
+    while (q + 1 < njobs && b >= jobs[q + 1].block0) ++q;
+    const SweepJob &J = jobs[q];
+    const int rank = b - J.block0, nb = J.nblocks;
+    const warpdev::Dim3i d{J.g.nx, J.g.ny, J.g.nz};
+    const int gx = (d.x + SWEEP_THREADS - 1) / SWEEP_THREADS;
+    const long long rows = (long long)gx * d.y * d.z;
+    const T *xbar = static_cast<const T *>(J.xbar), *xbar1 = static_cast<const T *>(J.xbar1);
+    if (rank == 0 && threadIdx.x == 0) view_order(J.seed, *J.counter, J.frames_total, J.frame_seq, J.V, J.perm);
+    for (long long t = rank; t < rows; t += nb) {  // backward warp + dual step
+        const int i = (int)(t % gx) * SWEEP_THREADS + threadIdx.x, j = (int)((t / gx) % d.y);
+        const int k = (int)(t / ((long long)gx * d.y));
+        if (i < d.x) {
+            warpdev::Cell s;
+            warpdev::trace_cell(d, J.flow, -1.0f, i, j, k, s);
+            float bw[1];
+            warpdev::sample_cell<1, false, T>(xbar1, 0, s, bw);
+            pd_dual_at(i, j, k, d.x, d.y, d.z, J.sigma, J.tv_w, J.tp_w, J.bc_w, J.hf, J.pdcut, xbar, xbar1, bw[0],
+                       J.ytv, J.ytp, J.ybc);
+        }
+    }
+    if (!sweep_barrier(gbar, gridDim.x, status)) return;
+    if (J.counter_owner && rank == 0 && threadIdx.x == 0) *J.counter += 1;
+    T *vol = static_cast<T *>(J.vol), *xprev = static_cast<T *>(J.xprev);
+    for (long long t = rank; t < rows; t += nb) {  // forward warp + primal step
+        const int i = (int)(t % gx) * SWEEP_THREADS + threadIdx.x, j = (int)((t / gx) % d.y);
+        const int k = (int)(t / ((long long)gx * d.y));
+        if (i < d.x) {
+            float fw = 0.0f;
+            if (!J.first) {
+                warpdev::Cell s;
+                warpdev::trace_cell(d, J.flow_prev, 1.0f, i, j, k, s);
+                float v[1];
+                warpdev::sample_cell<1, false, float, true>(J.ybc_prev, 0, s, v);
+                fw = v[0];
+            }
+            pd_primal_at<true>(i, j, k, d.x, d.y, d.z, J.tau, J.gmax, J.pdcut, J.first, J.ytp_prev, J.ytp, fw, J.ybc,
+                               J.ytv, vol, xprev);
+        }
+    }
+    if (!sweep_barrier(J.bar, nb, status)) return;  // (the SART call reads every voxel of the volume)
+    run_job<T, I>(J, rank, tile, status, 1);
+}
+
 template <typename T, typename I>
 const void *sweep_kernel() {
     return reinterpret_cast<const void *>(&k_sweep_persistent<T, I>);
 }
 
-const void *pick(bool bf16, bool wide) {
+template <typename T, typename I>
+const void *iter_kernel() {
+    return reinterpret_cast<const void *>(&k_iter_persistent<T, I>);
+}
+
+const void *pick(bool bf16, bool wide, bool whole = false) {
+    if (whole) {
+        if (bf16) return wide ? iter_kernel<unsigned short, long long>() : iter_kernel<unsigned short, int>();
+        return wide ? iter_kernel<float, long long>() : iter_kernel<float, int>();
+    }
     if (bf16) return wide ? sweep_kernel<unsigned short, long long>() : sweep_kernel<unsigned short, int>();
     return wide ? sweep_kernel<float, long long>() : sweep_kernel<float, int>();
 }
@@ -215,12 +288,18 @@ const void *pick(bool bf16, bool wide) {
 }  // namespace
 
 int sweep_max_blocks(bool bf16, bool wide) {
-    int per_sm = 0;
+    // (the smaller of the two kernels' resident blocks: one plan serves both)
+    int per_sm = 0, per_sm2 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, pick(bf16, wide, true), SWEEP_THREADS, 0) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick(bf16, wide), SWEEP_THREADS, 0) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
-    return per_sm * sm_count();
+    return (per_sm2 < per_sm ? per_sm2 : per_sm) * sm_count();
 }
 
 namespace {
@@ -256,6 +335,22 @@ int sweep_plan(SweepJob *jobs, int njobs, int nblocks) {
         for (int k = q0; k < q1; ++k) jobs[k].round = rounds;
     }
     return rounds;
+}
+
+cudaError_t launch_iter_persistent(const SweepJob *jobs_d, int njobs, int nblocks, bool bf16, bool wide,
+                                   unsigned *gbar, int *status, cudaStream_t s) {
+    if (njobs < 1 || nblocks < njobs) return cudaErrorInvalidValue;  // one round
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(SWEEP_THREADS);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {(void *)&jobs_d, (void *)&njobs, (void *)&gbar, (void *)&status};
+    return cudaLaunchKernelExC(&cfg, pick(bf16, wide, true), args);
 }
 
 cudaError_t launch_sweep_persistent(const SweepJob *jobs_d, int njobs, int nblocks, bool bf16, bool wide,

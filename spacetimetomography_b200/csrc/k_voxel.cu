@@ -56,11 +56,8 @@ __global__ void __launch_bounds__(128, 10) k_bp_voxel_cols(const GeomDev g, cons
     bp_column<K, PF>(g, v, BpRowsTex{tex}, vol, x, blockIdx.y * K, blockIdx.z, alpha, gmax);
 }
 
-// Dual step of one frame (ST_Tomography.cpp:504-534), fused:
-//   whole volume:     ytp += sigma*(xf1 - xf);  ybc += sigma*(bw - xf)
-//   interior & ROI:   ytv_c += sigma*(xf(p+e_c) - xf(p))*hf, clamp +-tv_w;
-//                     ytp = ytp*tp_w/(tp_w + 2 sigma);  ybc clamp +-bc_w
-// T: the storage of X_bar (the duals and the warped bw are FP32).
+// The dual and primal steps of one frame (pd_dual_at, pd_primal_at in
+// stt_voxel.cuh), one thread per voxel.
 template <typename T>
 __global__ void __launch_bounds__(128) k_pd_dual(int nx, int ny, int nz, float sigma, float tv_w,
                                                  float tp_w, float bc_w, float hf, Cut8 cut,
@@ -71,32 +68,10 @@ __global__ void __launch_bounds__(128) k_pd_dual(int nx, int ny, int nz, float s
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     if (i >= nx) return;
-    const size_t sy = nx, sz = (size_t)nx * ny, n = sz * nz;
-    const size_t p = i + j * sy + k * sz;
-    const float x0 = ld_voxel(xf + p);
-    float tp = ytp[p] + sigma * (ld_voxel(xf1 + p) - x0);
-    float bc = ybc[p] + sigma * (__ldg(bw + p) - x0);
-    const bool inner = i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < nz - 1 &&
-                       !roi_out(i, j, k, nx, ny, nz, cut.c);
-    if (inner) {
-        float y0 = ytv[p] + sigma * (ld_voxel(xf + p + 1) - x0) * hf;
-        float y1 = ytv[p + n] + sigma * (ld_voxel(xf + p + sy) - x0) * hf;
-        float y2 = ytv[p + 2 * n] + sigma * (ld_voxel(xf + p + sz) - x0) * hf;
-        ytv[p] = rmax(-tv_w, rmin(tv_w, y0));
-        ytv[p + n] = rmax(-tv_w, rmin(tv_w, y1));
-        ytv[p + 2 * n] = rmax(-tv_w, rmin(tv_w, y2));
-        tp = __fdiv_rn(tp * tp_w, tp_w + 2.0f * sigma);
-        bc = rmax(-bc_w, rmin(bc_w, bc));
-    }
-    ytp[p] = tp;
-    ybc[p] = bc;
+    const size_t p = i + (size_t)j * nx + (size_t)k * nx * ny;
+    pd_dual_at(i, j, k, nx, ny, nz, sigma, tv_w, tp_w, bc_w, hf, cut.c, xf, xf1, __ldg(bw + p), ytv, ytp, ybc);
 }
 
-// Primal step of one frame (ST_Tomography.cpp:536-578), fused: xprev = vol;
-// vol -= tau*(-ytp); vol -= tau*(-ybc) for the first frame, otherwise
-// vol -= tau*(ytp_prev - ytp); vol -= tau*(fw - ybc); then on the interior
-// ROI vol -= tau*(-div ytv) and clamp to [0, gmax].
-// T: the storage of vol and xprev (the duals and the warped fw are FP32).
 template <typename T>
 __global__ void __launch_bounds__(128) k_pd_primal(int nx, int ny, int nz, float tau, float gmax,
                                                    Cut8 cut, int first,
@@ -109,27 +84,9 @@ __global__ void __launch_bounds__(128) k_pd_primal(int nx, int ny, int nz, float
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     if (i >= nx) return;
-    const size_t sy = nx, sz = (size_t)nx * ny, n = sz * nz;
-    const size_t p = i + j * sy + k * sz;
-    float v = ld_stored(vol + p);
-    st_stored(xprev + p, v);
-    if (first) {
-        v = v - tau * (-__ldg(ytp + p));
-        v = v - tau * (-__ldg(ybc + p));
-    } else {
-        v = v - tau * (__ldg(ytp_prev + p) - __ldg(ytp + p));
-        v = v - tau * (__ldg(fw + p) - __ldg(ybc + p));
-    }
-    const bool inner = i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < nz - 1 &&
-                       !roi_out(i, j, k, nx, ny, nz, cut.c);
-    if (inner) {
-        const float *y0 = ytv, *y1 = ytv + n, *y2 = ytv + 2 * n;
-        float y = -(__ldg(y0 + p) - __ldg(y0 + p - 1) + __ldg(y1 + p) - __ldg(y1 + p - sy) +
-                    __ldg(y2 + p) - __ldg(y2 + p - sz));
-        v = v - tau * y;
-        v = rmax(rmin(gmax, v), 0.0f);
-    }
-    st_stored(vol + p, v);
+    const size_t p = i + (size_t)j * nx + (size_t)k * nx * ny;
+    pd_primal_at<false>(i, j, k, nx, ny, nz, tau, gmax, cut.c, first, ytp_prev, ytp, first ? 0.0f : __ldg(fw + p),
+                        ybc, ytv, vol, xprev);
 }
 
 // Over-relaxation (ST_Tomography.cpp:586-604): xbar = 2*vol - xprev in the ROI box.

@@ -37,31 +37,8 @@ __global__ void __launch_bounds__(WARP_BX *WARP_BY) k_warp(const Dim3i d, const 
     const int j = blockIdx.y * WARP_BY + threadIdx.y, k = blockIdx.z;
     if (i >= d.x || j >= d.y) return;
     const int n = d.x * d.y * d.z;
-    const float h = -dt;
-    // cell centre (warping.h:25-29); the velocity there is an exact node read
-    const float p[3] = {(float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f};
-    const int ci = min(max(i, 1), d.x - 2), cj = min(max(j, 1), d.y - 2), ck = min(max(k, 1), d.z - 2);
-    const int c = ci + cj * d.x + ck * d.x * d.y;
-    const float v1[3] = {__ldg(vel + c), __ldg(vel + n + c), __ldg(vel + 2 * n + c)};
-    // trace (warping.h:100-114): p2 = p + h v(p); p0 = p2 - h v(p2); q = p2 + (p - p0)/2
-    float p2[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) p2[a] = __fadd_rn(p[a], __fmul_rn(h, v1[a]));
-    const float g2[3] = {to_grid(p2[0], d.x, nullptr), to_grid(p2[1], d.y, nullptr),
-                         to_grid(p2[2], d.z, nullptr)};
-    Cell s2;
-    cell_setup(d, g2, s2);
-    float v2[3];
-    sample_cell<3>(vel, n, s2, v2);
-    float q[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float p0 = __fsub_rn(p2[a], __fmul_rn(h, v2[a]));
-        q[a] = __fadd_rn(p2[a], __fmul_rn(0.5f, __fsub_rn(p[a], p0)));
-    }
-    const float gq[3] = {to_grid(q[0], d.x, nullptr), to_grid(q[1], d.y, nullptr), to_grid(q[2], d.z, nullptr)};
     Cell s;
-    cell_setup(d, gq, s);
+    trace_cell(d, vel, dt, i, j, k, s);
     const int o = i + j * d.x + k * d.x * d.y;
     for (int ch = 0; ch < nc; ++ch) {
         float v[1];

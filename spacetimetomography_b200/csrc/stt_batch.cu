@@ -5,11 +5,13 @@
 // one iteration of all of them is enqueued together -- or captured once into
 // one CUDA graph and replayed.  The instances share nothing, so their views
 // run concurrently and small instances fill the GPU that one alone leaves idle.
-// In the persistent form (STT_SOLVE_PERSISTENT) every instance's duals and
-// primal run on its own stream, then ONE cooperative launch runs all
-// instances' SART calls, ROI masks and over-relaxations side by side, the
+// In the persistent form (STT_SOLVE_PERSISTENT) ONE cooperative launch runs
+// the whole iteration of every instance side by side -- view order, warps,
+// dual and primal steps, SART call, ROI mask and over-relaxation -- the
 // resident blocks split between the instances in proportion to their work
-// (k_persist.cu); the iteration is captured into a graph and replayed.
+// (k_iter_persistent, k_persist.cu); the iteration is captured into a graph
+// and replayed.  (More instances than resident blocks: the duals and primals
+// run as launches on the instances' streams and the SART calls in rounds.)
 #include <string>
 #include <vector>
 
@@ -87,6 +89,20 @@ stt_status enqueue_all(stt_batch *b, cudaStream_t main) {
 // The persistent form: every instance's steps before its SART call on its own
 // stream, then one launch for all SART calls, then the results.
 stt_status enqueue_all_persistent(stt_batch *b, cudaStream_t main) {
+    const int ni = (int)b->inst.size();
+    if (ni <= b->sweep_blocks) {  // the whole iteration of every instance: one launch
+        BCUDA(b, cudaMemsetAsync(b->bar, 0, (2 * (size_t)ni + 2) * sizeof(unsigned), main), "barrier reset");
+        BCUDA(b, stt::launch_iter_persistent(b->jobs_d, ni, b->sweep_blocks, b->bf16, b->wide, b->bar + 2 * ni,
+                                             b->status, main),
+              "persistent iteration");
+        for (stt_batch::Inst &in : b->inst) {
+            stt_internal_solver_end_iteration(in.solver);
+            if (!b->skip_copy)
+                BCUDA(b, cudaMemcpyAsync(in.user_vol, in.state, in.n * in.es, cudaMemcpyDeviceToDevice, main),
+                      "copy result");
+        }
+        return STT_OK;
+    }
     BCUDA(b, cudaEventRecord(b->fork, main), "event record");
     for (size_t i = 0; i < b->inst.size(); ++i) {
         stt_batch::Inst &in = b->inst[i];
@@ -124,7 +140,7 @@ stt_status build_sweep(stt_batch *b) {
     b->sweep_blocks = stt::sweep_max_blocks(b->bf16, b->wide);
     if (b->sweep_blocks < 1) return bfail(b, STT_ERR_CUDA, "occupancy of the persistent sweep");
     b->rounds = stt::sweep_plan(jobs.data(), n, b->sweep_blocks);
-    if (cudaMalloc(&b->bar, 2 * (size_t)n * sizeof(unsigned)) != cudaSuccess ||
+    if (cudaMalloc(&b->bar, (2 * (size_t)n + 2) * sizeof(unsigned)) != cudaSuccess ||  // per instance, the grid's
         cudaMalloc(&b->jobs_d, n * sizeof(stt::SweepJob)) != cudaSuccess ||
         cudaMalloc(&b->status, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();

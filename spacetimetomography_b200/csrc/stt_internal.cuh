@@ -679,6 +679,37 @@ __device__ __forceinline__ float fp_ray_sum_with(const GeomDev &g, const Corners
     return acc.s;
 }
 
+__device__ __host__ __forceinline__ unsigned long long splitmix(unsigned long long &s) {
+    unsigned long long z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Seed of frame f's view order in PD iteration `iter` (the reference reseeds
+// with time(0) in every SART call, ST_Tomography.cpp:635).  f is the frame's
+// index in the whole sequence of `frames`, so that shards of a frame-sharded
+// solve draw the orders the unsharded solve would.
+__device__ __host__ __forceinline__ unsigned long long frame_seed(unsigned long long seed,
+                                                                 unsigned long long iter, int frames,
+                                                                 int f) {
+    return seed + 0x9E3779B97F4A7C15ull * (iter * (unsigned long long)frames + (unsigned long long)f + 1ull);
+}
+
+// The view order of frame f (of a sequence of `frames`) in PD iteration
+// `iter`: Fisher-Yates with SplitMix64 (the same stream as stt_permutation).
+__device__ __host__ __forceinline__ void view_order(unsigned long long seed, unsigned long long iter, int frames,
+                                                    int f, int views, int *p) {
+    for (int i = 0; i < views; ++i) p[i] = i;
+    unsigned long long s = frame_seed(seed, iter, frames, f);
+    for (int i = views - 1; i > 0; --i) {
+        const int j = (int)(splitmix(s) % (unsigned long long)(i + 1));
+        const int t = p[i];
+        p[i] = p[j];
+        p[j] = t;
+    }
+}
+
 // One job of the persistent sweep (k_persist.cu): one frame's SART call (or
 // one batch instance's) -- V views in the order perm[0 .. V), each the
 // transpose (views that gather along x), the forward projection with the
@@ -692,18 +723,31 @@ __device__ __forceinline__ float fp_ray_sum_with(const GeomDev &g, const Corners
 struct SweepJob {
     GeomDev g;
     const ViewRec *views;  // the context's view table
-    const int *perm;       // V local view indices (device; drawn by an earlier launch)
+    int *perm;             // V local view indices (drawn by an earlier launch, or by the whole-iteration launch)
     int view_base, V;      // view perm[i] of the job is table entry view_base + perm[i]
     void *vol, *volt;      // the frame's volume and its z-fastest copy
     const void *stack;     // V projections, W*H each, in local view order
     float *raylen, *corr;  // sticky ray lengths and the correction, W*H each
-    const void *xprev;
+    void *xprev;
     void *xbar;            // over-relaxed X_bar (null: the ROI mask only)
     float alpha, gmax;
     int roi[8], pdcut[8];  // ROI mask cut, primal-dual region cut
     int round, block0, nblocks;
     unsigned *bar;         // [0] arrivals, [1] abort; zeroed before every launch
     double work;           // relative cost, for the host's split of the blocks
+    // The whole-iteration launch (k_iter_persistent) also runs, before the
+    // SART call, the frame's view order, backward warp + dual step and forward
+    // warp + primal step (ST_Tomography.cpp:492-578).
+    float sigma, tau, tv_w, tp_w, bc_w, hf;
+    int first;                         // the sequence's first frame: no f-1 terms in the primal step
+    const void *xbar1;                 // X_bar[f+1] (the job's storage)
+    const float *flow, *flow_prev;     // flow[f], flow[f-1]
+    float *ytv, *ytp, *ybc;            // the frame's duals
+    const float *ytp_prev, *ybc_prev;  // frame f-1's (written by its dual step in the same launch)
+    unsigned long long seed;           // the view order: frame frame_seq of frames_total, iteration *counter
+    unsigned long long *counter;
+    int frame_seq, frames_total;
+    int counter_owner;                 // this job advances *counter once every job has read it
 };
 
 }  // namespace stt

@@ -185,6 +185,12 @@ int sweep_max_blocks(bool bf16, bool wide);
 int sweep_plan(SweepJob *jobs, int njobs, int nblocks);
 cudaError_t launch_sweep_persistent(const SweepJob *jobs_d, int njobs, int nblocks, bool bf16, bool wide,
                                     int *status, cudaStream_t s);
+// The whole primal-dual iteration of every job (view order, warps, dual and
+// primal steps, then the SART call) in one cooperative launch; one round (at
+// most nblocks jobs); gbar: two words zeroed before the launch, like the
+// jobs' barrier words.
+cudaError_t launch_iter_persistent(const SweepJob *jobs_d, int njobs, int nblocks, bool bf16, bool wide,
+                                   unsigned *gbar, int *status, cudaStream_t s);
 
 // The correction image held as a one-layer layered CUDA array: the texture
 // object the column backprojection gathers from (tld4) and the surface object

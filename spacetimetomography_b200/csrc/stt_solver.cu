@@ -33,23 +33,6 @@
 namespace stt {
 namespace {
 
-__device__ __host__ __forceinline__ unsigned long long splitmix(unsigned long long &s) {
-    unsigned long long z = (s += 0x9E3779B97F4A7C15ull);
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
-
-// Seed of frame f's view order in PD iteration `iter` (the reference reseeds
-// with time(0) in every SART call, ST_Tomography.cpp:635).  f is the frame's
-// index in the whole sequence of `frames`, so that shards of a frame-sharded
-// solve draw the orders the unsharded solve would.
-__device__ __host__ __forceinline__ unsigned long long frame_seed(unsigned long long seed,
-                                                                 unsigned long long iter, int frames,
-                                                                 int f) {
-    return seed + 0x9E3779B97F4A7C15ull * (iter * (unsigned long long)frames + (unsigned long long)f + 1ull);
-}
-
 // One thread per local frame: Fisher-Yates with SplitMix64 (the same stream
 // as stt_permutation), then thread 0 advances the iteration counter.  Local
 // frame f is frame frame0 + f of a sequence of `total` frames.
@@ -57,17 +40,7 @@ __global__ void k_make_perm(unsigned long long seed, unsigned long long *counter
                             int views, int *perm) {
     const int f = threadIdx.x + blockIdx.x * blockDim.x;
     const unsigned long long iter = *counter;
-    if (f < frames) {
-        int *p = perm + (size_t)f * views;
-        for (int i = 0; i < views; ++i) p[i] = i;
-        unsigned long long s = frame_seed(seed, iter, total, frame0 + f);
-        for (int i = views - 1; i > 0; --i) {
-            const int j = (int)(splitmix(s) % (unsigned long long)(i + 1));
-            const int t = p[i];
-            p[i] = p[j];
-            p[j] = t;
-        }
-    }
+    if (f < frames) view_order(seed, iter, total, frame0 + f, views, perm + (size_t)f * views);
     __syncthreads();
     if (f == 0) *counter = iter + 1;
 }
@@ -89,14 +62,7 @@ cudaError_t launch_set_counter(unsigned long long *counter, unsigned long long v
 }
 
 void host_perm(unsigned long long seed, unsigned long long iter, int frames, int f, int views, int *p) {
-    for (int i = 0; i < views; ++i) p[i] = i;
-    unsigned long long s = frame_seed(seed, iter, frames, f);
-    for (int i = views - 1; i > 0; --i) {
-        const int j = (int)(splitmix(s) % (unsigned long long)(i + 1));
-        const int t = p[i];
-        p[i] = p[j];
-        p[j] = t;
-    }
+    view_order(seed, iter, frames, f, views, p);
 }
 
 }  // namespace stt
@@ -370,7 +336,19 @@ stt_status enqueue_sweep(stt_solver *s, cudaStream_t main, long long &nl) {
     return STT_OK;
 }
 
+// The whole iteration: one cooperative launch (view orders, warps, duals,
+// primals, SART calls, ROI masks, over-relaxations of every frame), or, with
+// more frames than resident blocks, the duals and primals as launches and
+// then the sweep.
 stt_status enqueue_persistent(stt_solver *s, cudaStream_t main, long long &nl) {
+    if (s->F <= s->sweep_blocks) {
+        SCUDA(s, cudaMemsetAsync(s->sweep_bar, 0, (2 * (size_t)s->F + 2) * sizeof(unsigned), main), "barrier reset");
+        SCUDA(s, stt::launch_iter_persistent(s->jobs_d, s->F, s->sweep_blocks, bf16(s), s->sweep_wide,
+                                             s->sweep_bar + 2 * s->F, s->status, main),
+              "persistent iteration");
+        ++nl;
+        return STT_OK;
+    }
     stt_status st = enqueue_phase0(s, main, nl, false);
     if (!st) st = enqueue_primals(s, main, nl, false);
     if (!st) st = enqueue_sweep(s, main, nl);
@@ -395,13 +373,31 @@ void fill_jobs(const stt_solver *s, stt::SweepJob *jobs) {
         J.stack = reinterpret_cast<const unsigned char *>(s->st.proj) + (size_t)f * V * npix * es;
         J.raylen = s->raylen + (size_t)f * npix;
         J.corr = s->corr + (size_t)f * npix;
-        J.xprev = reinterpret_cast<const unsigned char *>(s->st.xprev) + (size_t)f * n * es;
+        J.xprev = reinterpret_cast<unsigned char *>(s->st.xprev) + (size_t)f * n * es;
         J.xbar = reinterpret_cast<unsigned char *>(s->st.xbar) + (size_t)f * n * es;
         J.alpha = (float)s->cfg.alpha;
         J.gmax = s->cfg.pd.gmax;
         for (int q = 0; q < 8; ++q) J.roi[q] = s->cfg.roi_cut[q], J.pdcut[q] = s->cfg.pd.cut[q];
         const int nmax = std::max(s->g->nx, std::max(s->g->ny, s->g->nz));
         J.work = (double)V * ((double)n + (double)npix * nmax / 2.0);
+        // the whole-iteration launch: view order, warps, dual and primal steps
+        const stt_pd_params &pd = s->cfg.pd;
+        J.sigma = pd.sigma, J.tau = pd.tau, J.tv_w = pd.tv_w, J.tp_w = pd.tp_w, J.bc_w = pd.bc_w;
+        J.hf = pd.huber_factor;
+        J.first = f == 0 && !s->cfg.halo;
+        J.xbar1 = reinterpret_cast<const unsigned char *>(s->st.xbar) + (size_t)(f + 1) * n * es;
+        J.flow = s->st.flow + (size_t)f * 3 * n;
+        J.flow_prev = f > 0 ? s->st.flow + (size_t)(f - 1) * 3 * n : nullptr;
+        J.ytv = s->st.ytv + (size_t)f * 3 * n;
+        J.ytp = s->st.ytp + (size_t)f * n;
+        J.ybc = s->st.ybc + (size_t)f * n;
+        J.ytp_prev = f > 0 ? s->st.ytp + (size_t)(f - 1) * n : nullptr;
+        J.ybc_prev = f > 0 ? s->st.ybc + (size_t)(f - 1) * n : nullptr;
+        J.seed = s->cfg.seed;
+        J.counter = s->counter;
+        J.frame_seq = s->cfg.frame_offset + f;
+        J.frames_total = s->total_frames;
+        J.counter_owner = f == 0;
     }
 }
 
@@ -636,7 +632,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
             return STT_ERR_CUDA;  // the occupancy query failed
         }
         stt::sweep_plan(jobs.data(), F, s->sweep_blocks);
-        e = alloc(s, s->sweep_bar, 2 * (size_t)F, "sweep barriers");
+        e = alloc(s, s->sweep_bar, 2 * (size_t)F + 2, "sweep barriers");  // per frame, then the grid's
         unsigned char *jd = nullptr;
         if (!e) e = alloc(s, jd, F * sizeof(stt::SweepJob), "sweep jobs");
         s->jobs_d = reinterpret_cast<stt::SweepJob *>(jd);

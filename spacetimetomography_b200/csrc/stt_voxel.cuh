@@ -47,6 +47,78 @@ __device__ __forceinline__ void roi_apply_at(int i, int j, int k, int nx, int ny
     if (xbar && !roi_out(i, j, k, nx, ny, nz, pdcut)) st_stored(xbar + p, 2.0f * v - ld_voxel(xprev + p));
 }
 
+// A load of an FP32 array: through the read-only path, or (RW) a plain load
+// for an array that the running launch has written (the persistent sweep).
+template <bool RW>
+__device__ __forceinline__ float ld_f(const float *p) {
+    if constexpr (RW) return *p;
+    else return __ldg(p);
+}
+
+// Dual step of one frame at voxel (i, j, k) (ST_Tomography.cpp:504-534), fused:
+//   whole volume:     ytp += sigma*(xf1 - xf);  ybc += sigma*(bw - xf)
+//   interior & ROI:   ytv_c += sigma*(xf(p+e_c) - xf(p))*hf, clamp +-tv_w;
+//                     ytp = ytp*tp_w/(tp_w + 2 sigma);  ybc clamp +-bc_w
+// bw: the backward-warped X_bar[f+1] at the voxel.  T: the storage of X_bar
+// (the duals are FP32).
+template <typename T>
+__device__ __forceinline__ void pd_dual_at(int i, int j, int k, int nx, int ny, int nz, float sigma, float tv_w,
+                                           float tp_w, float bc_w, float hf, const int *cut, const T *xf,
+                                           const T *xf1, float bw, float *ytv, float *ytp, float *ybc) {
+    const size_t sy = nx, sz = (size_t)nx * ny, n = sz * nz;
+    const size_t p = i + j * sy + k * sz;
+    const float x0 = ld_voxel(xf + p);
+    float tp = ytp[p] + sigma * (ld_voxel(xf1 + p) - x0);
+    float bc = ybc[p] + sigma * (bw - x0);
+    const bool inner = i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < nz - 1 &&
+                       !roi_out(i, j, k, nx, ny, nz, cut);
+    if (inner) {
+        float y0 = ytv[p] + sigma * (ld_voxel(xf + p + 1) - x0) * hf;
+        float y1 = ytv[p + n] + sigma * (ld_voxel(xf + p + sy) - x0) * hf;
+        float y2 = ytv[p + 2 * n] + sigma * (ld_voxel(xf + p + sz) - x0) * hf;
+        ytv[p] = rmax(-tv_w, rmin(tv_w, y0));
+        ytv[p + n] = rmax(-tv_w, rmin(tv_w, y1));
+        ytv[p + 2 * n] = rmax(-tv_w, rmin(tv_w, y2));
+        tp = __fdiv_rn(tp * tp_w, tp_w + 2.0f * sigma);
+        bc = rmax(-bc_w, rmin(bc_w, bc));
+    }
+    ytp[p] = tp;
+    ybc[p] = bc;
+}
+
+// Primal step of one frame at voxel (i, j, k) (ST_Tomography.cpp:536-578),
+// fused: xprev = vol; vol -= tau*(-ytp); vol -= tau*(-ybc) for the first
+// frame, otherwise vol -= tau*(ytp_prev - ytp); vol -= tau*(fw - ybc); then
+// on the interior ROI vol -= tau*(-div ytv) and clamp to [0, gmax].  fw: the
+// forward-warped Y_bc[f-1] at the voxel.  T: the storage of vol and xprev
+// (the duals are FP32).  RW: the duals were written by the same launch.
+template <bool RW, typename T>
+__device__ __forceinline__ void pd_primal_at(int i, int j, int k, int nx, int ny, int nz, float tau, float gmax,
+                                             const int *cut, int first, const float *ytp_prev, const float *ytp,
+                                             float fw, const float *ybc, const float *ytv, T *vol, T *xprev) {
+    const size_t sy = nx, sz = (size_t)nx * ny, n = sz * nz;
+    const size_t p = i + j * sy + k * sz;
+    float v = ld_stored(vol + p);
+    st_stored(xprev + p, v);
+    if (first) {
+        v = v - tau * (-ld_f<RW>(ytp + p));
+        v = v - tau * (-ld_f<RW>(ybc + p));
+    } else {
+        v = v - tau * (ld_f<RW>(ytp_prev + p) - ld_f<RW>(ytp + p));
+        v = v - tau * (fw - ld_f<RW>(ybc + p));
+    }
+    const bool inner = i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < nz - 1 &&
+                       !roi_out(i, j, k, nx, ny, nz, cut);
+    if (inner) {
+        const float *y0 = ytv, *y1 = ytv + n, *y2 = ytv + 2 * n;
+        float y = -(ld_f<RW>(y0 + p) - ld_f<RW>(y0 + p - 1) + ld_f<RW>(y1 + p) - ld_f<RW>(y1 + p - sy) +
+                    ld_f<RW>(y2 + p) - ld_f<RW>(y2 + p - sz));
+        v = v - tau * y;
+        v = rmax(rmin(gmax, v), 0.0f);
+    }
+    st_stored(vol + p, v);
+}
+
 // Voxel-based backprojection (ST_Tomography.cpp:690-730): project the voxel
 // centre, Catmull-Rom 4x4 gather of the correction image (y first, then x),
 // vol += alpha*val, clamp to [0, gmax]; voxels whose footprint leaves

@@ -130,9 +130,12 @@ __device__ __forceinline__ void cell_setup(const Dim3i d, const float g[3], Cell
 // A tap: read-only global load (a BF16-stored image widened exactly), or a
 // plain load when SHARED (img then points into shared memory, which the
 // global read-only path cannot address).
-template <bool SHARED, typename T>
+// RW: a plain load of a global image that the running launch has written
+// (the persistent iteration's Y_bc).
+template <bool SHARED, typename T, bool RW = false>
 __device__ __forceinline__ float ld_tap(const T *p) {
     if constexpr (SHARED) return *p;
+    else if constexpr (RW) return ld_stored(p);
     else return ld_voxel(p);
 }
 
@@ -141,7 +144,7 @@ __device__ __forceinline__ float ld_tap(const T *p) {
 // Plane p starts at img + p * pstride.  The sums run in the order of
 // sample_clamped above (x taps, then rows, then planes), so both give the
 // same bits.
-template <int NC, bool SHARED = false, typename T = float>
+template <int NC, bool SHARED = false, typename T = float, bool RW = false>
 __device__ __forceinline__ void sample_cell(const T *__restrict__ img, int pstride, const Cell &s,
                                             float out[NC]) {
     float val[NC], mn[NC], mx[NC];
@@ -164,8 +167,9 @@ __device__ __forceinline__ void sample_cell(const T *__restrict__ img, int pstri
 #pragma unroll
             for (int p = 0; p < NC; ++p) {
                 const T *r = img + p * pstride + row;
-                const float t0 = ld_tap<SHARED>(r), t1 = ld_tap<SHARED>(r + 1), t2 = ld_tap<SHARED>(r + 2);
-                const float t3 = s.x.t3 ? ld_tap<SHARED>(r + 3) : 0.0f;
+                const float t0 = ld_tap<SHARED, T, RW>(r), t1 = ld_tap<SHARED, T, RW>(r + 1),
+                            t2 = ld_tap<SHARED, T, RW>(r + 2);
+                const float t3 = s.x.t3 ? ld_tap<SHARED, T, RW>(r + 3) : 0.0f;
                 const float xv = s.x.w[0] * t0 + s.x.w[1] * t1 + s.x.w[2] * t2 + s.x.w[3] * t3;
                 yv[p] += s.y.w[b] * xv;
                 if ((b == 1 || b == 2) && (c == 1 || c == 2)) {
@@ -179,6 +183,38 @@ __device__ __forceinline__ void sample_cell(const T *__restrict__ img, int pstri
     }
 #pragma unroll
     for (int p = 0; p < NC; ++p) out[p] = fmaxf(mn[p], fminf(val[p], mx[p]));
+}
+
+// The trace of voxel (i, j, k) through vel (warping.h:100-114) with step dt
+// (the gather form's arithmetic: the exact centre read, the Catmull-Rom
+// velocity sample at the half-traced point) and the cell of its end point.
+__device__ __forceinline__ void trace_cell(const Dim3i d, const float *__restrict__ vel, float dt, int i, int j,
+                                           int k, Cell &s) {
+    const int n = d.x * d.y * d.z;
+    const float h = -dt;
+    // cell centre (warping.h:25-29); the velocity there is an exact node read
+    const float p[3] = {(float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f};
+    const int ci = min(max(i, 1), d.x - 2), cj = min(max(j, 1), d.y - 2), ck = min(max(k, 1), d.z - 2);
+    const int c = ci + cj * d.x + ck * d.x * d.y;
+    const float v1[3] = {__ldg(vel + c), __ldg(vel + n + c), __ldg(vel + 2 * n + c)};
+    // trace (warping.h:100-114): p2 = p + h v(p); p0 = p2 - h v(p2); q = p2 + (p - p0)/2
+    float p2[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) p2[a] = __fadd_rn(p[a], __fmul_rn(h, v1[a]));
+    const float g2[3] = {to_grid(p2[0], d.x, nullptr), to_grid(p2[1], d.y, nullptr),
+                         to_grid(p2[2], d.z, nullptr)};
+    Cell s2;
+    cell_setup(d, g2, s2);
+    float v2[3];
+    sample_cell<3>(vel, n, s2, v2);
+    float q[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float p0 = __fsub_rn(p2[a], __fmul_rn(h, v2[a]));
+        q[a] = __fadd_rn(p2[a], __fmul_rn(0.5f, __fsub_rn(p[a], p0)));
+    }
+    const float gq[3] = {to_grid(q[0], d.x, nullptr), to_grid(q[1], d.y, nullptr), to_grid(q[2], d.z, nullptr)};
+    cell_setup(d, gq, s);
 }
 
 __device__ __forceinline__ void trace(const Dim3i d, const float *__restrict__ vel, size_t n, int i,
