@@ -457,17 +457,20 @@ typedef enum stt_solve_mode {
     STT_SOLVE_PLAIN = 0,      /* per-view launches from a host loop, sync per view */
     STT_SOLVE_STREAMS = 1,    /* batched: fused launches, one stream per frame */
     STT_SOLVE_GRAPH = 2,      /* batched, captured once into a CUDA graph and replayed */
-    /* Every frame's SART call (all views: transpose, projection + correction,
-     * backprojection), its ROI mask and over-relaxation in ONE persistent
-     * cooperative launch, the frames side by side on their share of the
-     * resident blocks, after the warps, duals and primals; the iteration is
-     * captured into a CUDA graph and replayed (enqueued directly where the
-     * runtime cannot capture a cooperative launch: stt_solver_stats).  Voxel-based
-     * backprojection only (bp_mode 0).  The same bits as the other batched
-     * modes; inside one launch the volume is gathered with plain loads (the
-     * texture and read-only caches are not coherent with the launch's own
-     * writes), so on volumes that the texture gathers serve well it is
-     * slower than STT_SOLVE_GRAPH. */
+    /* The whole iteration in ONE persistent cooperative launch: every
+     * frame's view order, backward warp + dual step, then (after a barrier
+     * of the grid) its forward warp + primal step, SART call (all views:
+     * transpose, projection + correction, backprojection), ROI mask and
+     * over-relaxation, the frames side by side on their share of the
+     * resident blocks; the launch is captured into a CUDA graph and
+     * replayed (enqueued directly where the runtime cannot capture a
+     * cooperative launch: stt_solver_persistent_info).  A sharded solve
+     * (halo) runs its phase 0 as launches and its phase 1's SART calls as
+     * one launch.  Voxel-based backprojection only (bp_mode 0).  The same
+     * bits as the other batched modes; inside one launch the arrays it
+     * writes are gathered with plain loads (the texture and read-only caches
+     * are not coherent with the launch's own writes), so on volumes that the
+     * texture gathers serve well it is slower than STT_SOLVE_GRAPH. */
     STT_SOLVE_PERSISTENT = 3
 } stt_solve_mode;
 
