@@ -1,7 +1,11 @@
-// k_persist.cu -- the persistent sweep: every view of every frame's SART call
-// (S/ST_Tomo/ST_Tomography.cpp:616-808) -- or of every batch instance's --
-// and the ROI mask with the over-relaxation that follows it (:586-604,
-// :793-804), in ONE cooperative launch.
+// k_persist.cu -- the persistent forms of the primal-dual iteration.
+// k_iter_persistent: the whole iteration (S/ST_Tomo/ST_Tomography.cpp:492-607)
+// of every frame -- or of every batch instance -- in ONE cooperative launch:
+// view order, warps, dual and primal steps (see the kernel), then the SART
+// call.  k_sweep_persistent: only the SART calls (every view of every
+// frame's SART call, :616-808) and the ROI mask with the over-relaxation
+// that follows them (:586-604, :793-804), for a sharded solve whose halos are
+// exchanged between the phases.  Both run the SART calls as below.
 //
 // The jobs (SweepJob: one frame or one instance each) share the launch's
 // blocks in proportion to their work and run side by side; only when there

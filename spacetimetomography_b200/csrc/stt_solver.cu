@@ -11,10 +11,11 @@
 //   STT_SOLVE_GRAPH    the batched form captured once into a CUDA graph and
 //                      replayed (the view order is drawn on the device from a
 //                      counter, so every replay gets a fresh seeded order);
-//   STT_SOLVE_PERSISTENT the duals and primals as in the batched form, then
-//                      every frame's SART call, ROI mask and over-relaxation
-//                      in one persistent cooperative launch (k_persist.cu),
-//                      captured and replayed as a graph.
+//   STT_SOLVE_PERSISTENT the whole iteration of every frame (view order,
+//                      warps, dual and primal steps, SART, ROI mask,
+//                      over-relaxation) in one persistent cooperative launch
+//                      (k_iter_persistent, k_persist.cu), captured and
+//                      replayed as a graph.
 //
 // Reordering "all duals, then every frame's primal chain" is exact: frame f's
 // dual reads X_bar[f], X_bar[f+1] and flow[f] only, and X_bar[f] is rewritten
