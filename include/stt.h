@@ -418,7 +418,12 @@ stt_status stt_flow_create(int device, const int *dims, const stt_flow_params *p
 const char *stt_flow_last_error(const stt_flow *f);
 stt_status stt_flow_destroy(stt_flow *f);
 /* L1Huber_OF_MultiScale3D: V holds the initial flow and receives the
- * finest-level flow; Y0 (10 planes, NULL = zeros) is the initial dual. */
+ * finest-level flow; Y0 (10 planes, NULL = zeros) is the initial dual.
+ * This and stt_flow_level enqueue their work on `stream`; to stop enqueuing a
+ * warp's iterations once its residual check has stopped it, they keep at most
+ * 200 of a warp's iterations queued ahead of the device and wait for it
+ * (an event of `stream`) past that.  While `stream` is being captured every
+ * iteration is enqueued and nothing waits. */
 stt_status stt_flow_multiscale(stt_flow *f, const float *I1, const float *I2, float *V, const float *Y0,
                                void *stream);
 /* L1Huber_OF on one level of size dim (HOST, each extent >= 3 and at most the
