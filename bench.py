@@ -104,6 +104,8 @@ def parse_args():
                     help="with --config: only run a few ray-driven backprojections at the workload's size")
     ap.add_argument("--iter-probe", action="store_true",
                     help="only the headline solver's warm-up and one iteration in an NVTX range (for ncu's launch list)")
+    ap.add_argument("--persistent", action="store_true",
+                    help="with --iter-probe: the persistent form (STT_SOLVE_PERSISTENT, one launch per iteration)")
     ap.add_argument("--fp64-pd-check", action="store_true",
                     help="run only the full-size FP64 check of one 4D primal-dual iteration (two frames) and print it")
     ap.add_argument("--no-configs", action="store_true",
@@ -1383,8 +1385,9 @@ def run_iter_probe(args) -> int:
     stream = torch.cuda.Stream(device=dev)
     if args.tuning is not None:
         tune_or_set(ctx, stream, args.tuning)
+    mode = stt.SOLVE_PERSISTENT if args.persistent else stt.SOLVE_GRAPH
     s = stt.Solver(ctx, st, args.frames, args.views, pd_params(gmax), alpha=0.3, bp_mode=0 if args.bp == "voxel" else 1,
-                   seed=99, mode=stt.SOLVE_GRAPH, autotune=args.tuning is None)
+                   seed=99, mode=mode, autotune=args.tuning is None and not args.persistent)
     with torch.cuda.stream(stream):
         st["xbar"].copy_(st["vol"])
     s.iterate(1, stream)
@@ -1394,7 +1397,13 @@ def run_iter_probe(args) -> int:
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
     s.poll_status(stream)
-    print(json.dumps({"launches_per_iter": s.stats()[0], "tuning": ctx.get_tuning()}), flush=True)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    s.iterate(1, stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"launches_per_iter": s.stats()[0], "s_per_iter": t0.elapsed_time(t1) / 1000.0,
+                      "persistent": s.persistent_info(), "tuning": ctx.get_tuning()}), flush=True)
     s.close()
     ctx.close()
     return 0
