@@ -103,6 +103,31 @@ __device__ __forceinline__ bool sweep_barrier(unsigned *bar, unsigned target, in
     return ok != 0;
 }
 
+// Tiles [0, ntiles) of one phase handed out by the job's ticket counter:
+// thread 0 takes the next ticket while the block works on the current tile
+// (the atomic's latency hides behind the tile), so blocks that drew cheap
+// tiles take more and no block waits at the phase's barrier for a slow
+// static share.  `base` is the counter's value at the phase's start: every
+// block's last draw overshoots by one, so a phase uses ntiles + nblocks
+// tickets and the next phase starts there.  Which block computes a tile does
+// not change its values.
+template <typename Work>
+__device__ __forceinline__ void dynamic_tiles(unsigned *ticket, unsigned base, int ntiles, Work &&work) {
+    __shared__ int next;
+    if (threadIdx.x == 0) next = (int)(atomicAdd(ticket, 1u) - base);
+    __syncthreads();
+    int t = next;
+    while (t < ntiles) {
+        __syncthreads();  // every thread has read `next`
+        unsigned drawn = 0;
+        if (threadIdx.x == 0) drawn = atomicAdd(ticket, 1u);
+        work(t);
+        if (threadIdx.x == 0) next = (int)(drawn - base);
+        __syncthreads();
+        t = next;
+    }
+}
+
 // The forward projection with the correction of pixel (i, j)
 // (k_fp_corr's body, corners by plain loads).
 template <typename I, typename T>
@@ -143,6 +168,7 @@ __device__ __forceinline__ bool run_job(const SweepJob &J, int rank, T (*tile)[3
     const T *stack = static_cast<const T *>(J.stack);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const size_t nxy = (size_t)g.nx * g.ny, nzy = (size_t)g.nz * g.ny, npix = (size_t)g.W * g.H;
+    unsigned tickets = 0;  // the job's ticket counter at the next dynamic phase's start
     for (int v = 0; v < J.V; ++v) {
         const int local = J.perm[v];  // (a plain load: the whole-iteration launch draws perm itself)
         const ViewRec &vr = J.views[J.view_base + local];
@@ -161,23 +187,25 @@ __device__ __forceinline__ bool run_job(const SweepJob &J, int rank, T (*tile)[3
             }
             if (!sweep_barrier(J.bar, ++passed * nb, status)) return false;
         }
-        {  // forward projection + correction
+        {  // forward projection + correction (tiles of uneven cost: handed out dynamically)
             const T *b = stack + (size_t)local * npix;
             const int tw = (g.W + 31) / 32, th = (g.H + 3) / 4;
-            for (int t = rank; t < tw * th; t += nb) {
+            dynamic_tiles(J.bar + 2, tickets, tw * th, [&](int t) {
                 const int i = (t % tw) * 32 + lane, j = (t / tw) * 4 + warp;
                 if (i < g.W && j < g.H) sweep_fp_pixel<I>(g, vr, vol, volt, b, J.raylen, J.corr, i, j);
-            }
+            });
+            tickets += (unsigned)(tw * th + nb);
         }
         if (!sweep_barrier(J.bar, ++passed * nb, status)) return false;
-        {  // voxel-based backprojection
+        {  // voxel-based backprojection (columns outside the view's shadow are cheap: dynamic too)
             const int cx = (g.nx + SWEEP_THREADS - 1) / SWEEP_THREADS, cy = (g.ny + SWEEP_COL - 1) / SWEEP_COL;
             const BpRowsLoad rows{J.corr, g.W};
-            for (int t = rank; t < cx * cy * g.nz; t += nb) {
+            dynamic_tiles(J.bar + 2, tickets, cx * cy * g.nz, [&](int t) {
                 const int x = (t % cx) * SWEEP_THREADS + threadIdx.x, y0 = ((t / cx) % cy) * SWEEP_COL;
                 const int z = t / (cx * cy);
                 if (x < g.nx) bp_column<SWEEP_COL, false>(g, vr, rows, vol, x, y0, z, J.alpha, J.gmax);
-            }
+            });
+            tickets += (unsigned)(cx * cy * g.nz + nb);
         }
         if (!sweep_barrier(J.bar, ++passed * nb, status)) return false;
     }

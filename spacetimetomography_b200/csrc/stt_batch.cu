@@ -91,8 +91,8 @@ stt_status enqueue_all(stt_batch *b, cudaStream_t main) {
 stt_status enqueue_all_persistent(stt_batch *b, cudaStream_t main) {
     const int ni = (int)b->inst.size();
     if (ni <= b->sweep_blocks) {  // the whole iteration of every instance: one launch
-        BCUDA(b, cudaMemsetAsync(b->bar, 0, (2 * (size_t)ni + 2) * sizeof(unsigned), main), "barrier reset");
-        BCUDA(b, stt::launch_iter_persistent(b->jobs_d, ni, b->sweep_blocks, b->bf16, b->wide, b->bar + 2 * ni,
+        BCUDA(b, cudaMemsetAsync(b->bar, 0, (4 * (size_t)ni + 2) * sizeof(unsigned), main), "barrier reset");
+        BCUDA(b, stt::launch_iter_persistent(b->jobs_d, ni, b->sweep_blocks, b->bf16, b->wide, b->bar + 4 * ni,
                                              b->status, main),
               "persistent iteration");
         for (stt_batch::Inst &in : b->inst) {
@@ -113,7 +113,7 @@ stt_status enqueue_all_persistent(stt_batch *b, cudaStream_t main) {
         BCUDA(b, cudaStreamWaitEvent(main, in.done, 0), "stream wait");
     }
     const int n = (int)b->inst.size();
-    BCUDA(b, cudaMemsetAsync(b->bar, 0, 2 * (size_t)n * sizeof(unsigned), main), "barrier reset");
+    BCUDA(b, cudaMemsetAsync(b->bar, 0, 4 * (size_t)n * sizeof(unsigned), main), "barrier reset");
     BCUDA(b, stt::launch_sweep_persistent(b->jobs_d, n, b->sweep_blocks, b->bf16, b->wide, b->status, main),
           "persistent sweep");
     for (stt_batch::Inst &in : b->inst) {
@@ -140,13 +140,13 @@ stt_status build_sweep(stt_batch *b) {
     b->sweep_blocks = stt::sweep_max_blocks(b->bf16, b->wide);
     if (b->sweep_blocks < 1) return bfail(b, STT_ERR_CUDA, "occupancy of the persistent sweep");
     b->rounds = stt::sweep_plan(jobs.data(), n, b->sweep_blocks);
-    if (cudaMalloc(&b->bar, (2 * (size_t)n + 2) * sizeof(unsigned)) != cudaSuccess ||  // per instance, the grid's
+    if (cudaMalloc(&b->bar, (4 * (size_t)n + 2) * sizeof(unsigned)) != cudaSuccess ||  // 4 per instance, the grid's
         cudaMalloc(&b->jobs_d, n * sizeof(stt::SweepJob)) != cudaSuccess ||
         cudaMalloc(&b->status, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         return bfail(b, STT_ERR_NOMEM, "persistent sweep buffers");
     }
-    for (int i = 0; i < n; ++i) jobs[i].bar = b->bar + 2 * i;
+    for (int i = 0; i < n; ++i) jobs[i].bar = b->bar + 4 * i;
     if (cudaMemcpy(b->jobs_d, jobs.data(), n * sizeof(stt::SweepJob), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(b->status, 0, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();

@@ -733,7 +733,7 @@ struct SweepJob {
     float alpha, gmax;
     int roi[8], pdcut[8];  // ROI mask cut, primal-dual region cut
     int round, block0, nblocks;
-    unsigned *bar;         // [0] arrivals, [1] abort; zeroed before every launch
+    unsigned *bar;         // [0] arrivals, [1] abort, [2] tile tickets; zeroed before every launch
     double work;           // relative cost, for the host's split of the blocks
     // The whole-iteration launch (k_iter_persistent) also runs, before the
     // SART call, the frame's view order, backward warp + dual step and forward

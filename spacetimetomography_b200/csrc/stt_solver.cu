@@ -103,7 +103,7 @@ struct stt_solver {
     std::vector<stt::FpSlabMaps> fpmaps;  // batched modes: per frame, TMA maps of the volume and its copy
     std::vector<stt::FpTex> fptex;  // batched modes, a tld4 gather form: per frame, the volume's textures
     stt::SweepJob *jobs_d = nullptr;  // STT_SOLVE_PERSISTENT: one job per frame
-    unsigned *sweep_bar = nullptr;    // the jobs' barrier words (2 per frame)
+    unsigned *sweep_bar = nullptr;    // the jobs' barrier and ticket words (4 per frame), then the grid's
     int sweep_blocks = 0;
     bool sweep_wide = false;
     bool sweep_direct = false;        // the cooperative launch could not be captured
@@ -330,7 +330,7 @@ stt_status enqueue_primals(stt_solver *s, cudaStream_t main, long long &nl, bool
 
 // Every frame's SART call, ROI mask and over-relaxation: one persistent launch.
 stt_status enqueue_sweep(stt_solver *s, cudaStream_t main, long long &nl) {
-    SCUDA(s, cudaMemsetAsync(s->sweep_bar, 0, 2 * (size_t)s->F * sizeof(unsigned), main), "barrier reset");
+    SCUDA(s, cudaMemsetAsync(s->sweep_bar, 0, 4 * (size_t)s->F * sizeof(unsigned), main), "barrier reset");
     SCUDA(s, stt::launch_sweep_persistent(s->jobs_d, s->F, s->sweep_blocks, bf16(s), s->sweep_wide, s->status, main),
           "persistent sweep");
     ++nl;
@@ -343,9 +343,9 @@ stt_status enqueue_sweep(stt_solver *s, cudaStream_t main, long long &nl) {
 // then the sweep.
 stt_status enqueue_persistent(stt_solver *s, cudaStream_t main, long long &nl) {
     if (s->F <= s->sweep_blocks) {
-        SCUDA(s, cudaMemsetAsync(s->sweep_bar, 0, (2 * (size_t)s->F + 2) * sizeof(unsigned), main), "barrier reset");
+        SCUDA(s, cudaMemsetAsync(s->sweep_bar, 0, (4 * (size_t)s->F + 2) * sizeof(unsigned), main), "barrier reset");
         SCUDA(s, stt::launch_iter_persistent(s->jobs_d, s->F, s->sweep_blocks, bf16(s), s->sweep_wide,
-                                             s->sweep_bar + 2 * s->F, s->status, main),
+                                             s->sweep_bar + 4 * s->F, s->status, main),
               "persistent iteration");
         ++nl;
         return STT_OK;
@@ -633,7 +633,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
             return STT_ERR_CUDA;  // the occupancy query failed
         }
         stt::sweep_plan(jobs.data(), F, s->sweep_blocks);
-        e = alloc(s, s->sweep_bar, 2 * (size_t)F + 2, "sweep barriers");  // per frame, then the grid's
+        e = alloc(s, s->sweep_bar, 4 * (size_t)F + 2, "sweep barriers");  // 4 per frame, then the grid's
         unsigned char *jd = nullptr;
         if (!e) e = alloc(s, jd, F * sizeof(stt::SweepJob), "sweep jobs");
         s->jobs_d = reinterpret_cast<stt::SweepJob *>(jd);
@@ -641,7 +641,7 @@ stt_status stt_solver_create(stt_ctx *ctx, const stt_solve_cfg *cfg, const stt_p
             stt_solver_destroy(s);
             return e;
         }
-        for (int f = 0; f < F; ++f) jobs[f].bar = s->sweep_bar + 2 * f;
+        for (int f = 0; f < F; ++f) jobs[f].bar = s->sweep_bar + 4 * f;
         if (cudaMemcpy(s->jobs_d, jobs.data(), F * sizeof(stt::SweepJob), cudaMemcpyHostToDevice) != cudaSuccess) {
             cudaGetLastError();
             stt_solver_destroy(s);
