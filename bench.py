@@ -1423,6 +1423,65 @@ def run_flow_only(args):
     return 0
 
 
+def batch_fp64_check(inst, dev, stream, count=2) -> dict:
+    """One primal-dual iteration of the batch's smallest instances (by voxels
+    x views) against the FP64 oracle, FP32 and BF16 storage: each instance's
+    own single-frame solve (which a batch reproduces bit for bit), from a
+    state one GPU iteration into the solve, and the oracle's reference-ordered
+    iteration (dual, primal, SART with voxel BP, ROI mask, over-relaxation)
+    from the same state (for BF16 storage: the BF16 state, the oracle
+    unrounded)."""
+    import torch
+
+    import spacetimetomography_b200 as stt
+    from spacetimetomography_b200.api import REFERENCE_CUT
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_bind as ob
+
+    order = sorted(range(len(inst)), key=lambda k: inst[k]["geom"][0] ** 3 * inst[k]["proj"].shape[0])[:count]
+    out = []
+    for k in order:
+        d = inst[k]
+        n, det, ds, sid, sdd, ang = d["geom"]
+        V = d["proj"].shape[0]
+        pd = d["pd"]
+        row = {"instance": k, "volume": n, "detector": det, "views": V}
+        for storage in ("f32", "bf16"):
+            dt = torch.bfloat16 if storage == "bf16" else torch.float32
+            z = lambda *s_: torch.zeros(s_, device=dev)  # noqa: E731
+            v0 = (0.8 * d["truth"]).to(dt)
+            st = dict(vol=torch.stack([v0, v0]), xbar=torch.stack([v0, v0]), xprev=z(1, n, n, n).to(dt),
+                      ytv=z(1, 3, n, n, n), ytp=z(1, n, n, n), ybc=z(1, n, n, n), flow=z(1, 3, n, n, n),
+                      proj=d["proj"].to(dt).unsqueeze(0).contiguous())
+            s1 = stt.Solver(d["ctx"], st, 1, V, pd, alpha=0.3, roi_cut=REFERENCE_CUT, seed=5, mode=stt.SOLVE_GRAPH,
+                            storage=storage)
+            s1.iterate(1, stream)  # into the solve: non-zero duals
+            torch.cuda.synchronize()
+            s1.close()
+            start = {kk: vv.detach().float().cpu().numpy().copy() for kk, vv in st.items()}
+            s2 = stt.Solver(d["ctx"], st, 1, V, pd, alpha=0.3, roi_cut=REFERENCE_CUT, seed=11, mode=stt.SOLVE_GRAPH,
+                            storage=storage)
+            s2.iterate(1, stream)
+            torch.cuda.synchronize()
+            s2.poll_status(stream)
+            s2.close()
+            gpu = st["vol"][0].float().cpu().numpy()
+            pp = [pd.sigma, pd.tau, pd.tv_w, pd.tp_w, pd.bc_w, pd.huber_factor, pd.gmax]
+            scan = ob.Scan(n, (det, det), sid=sid, sdd=sdd, ds=ds)
+            with c_stdout_to_stderr():
+                ref = ob.pd_iteration(scan, ang, start, 1, V, pp, tuple(pd.cut), REFERENCE_CUT, 0.3, 0,
+                                      [stt.frame_order(11, 0, 1, 0, V)], [np.zeros((det, det), np.float64)],
+                                      fp64=True)
+            row[f"{storage}_vol_rel_l2_vs_fp64"] = ob.rel_l2(gpu, ref["vol"][0])
+            del st
+        out.append(row)
+    return {"instances": out,
+            "sample": "one PD iteration of each of the batch's two smallest instances (voxels x views) at its own "
+                      "size, from one GPU iteration into the solve; relative L2 of the GPU volume against the FP64 "
+                      "oracle (BF16 storage: the GPU's BF16 result against the unrounded FP64 iteration)"}
+
+
 def run_batch_only(args):
     """Config 4: independent single-frame TV + SART solves of uneven size
     (cubes 64^3-192^3, detectors 128^2-384^2, 60-240 views, sid 500-700 mm,
@@ -1455,7 +1514,7 @@ def run_batch_only(args):
         pd = stt.PdParams(tv_w=0.01, tp_w=0.0, bc_w=0.0, huber_factor=float(1 / (1 + 0.1125)),
                           gmax=float(proj.max().item() / 4))
         inst.append(dict(ctx=ctx, vol=torch.zeros_like(truth), proj=proj, bp_mode=0, alpha=0.3, pd=pd, seed=k,
-                         truth=truth))
+                         truth=truth, geom=(n, det, ds, sid, sdd, ang)))
         units += n ** 3 * V
     stream = torch.cuda.Stream(device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1569,6 +1628,7 @@ def run_batch_only(args):
     for sv in plain:
         sv.close()
     errs = [float((d["vol"] - d["truth"]).norm() / d["truth"].norm()) for d in inst[:4]]
+    fp64 = batch_fp64_check(inst, dev, stream)
     line = {"metric": "projector GUPS over one batched iteration of independent instances", "value": units / t_batch / 1e9,
             "unit": "GUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_batch,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic",
@@ -1579,6 +1639,7 @@ def run_batch_only(args):
             "plain_note": "the same instances one after another in the per-view form (STT_SOLVE_PLAIN: each "
                           "view's launches from a host loop, a host synchronisation per view)",
             "rel_l2_to_phantom_first4": errs,
+            "fp64_check": fp64,
             "persistent": {"ms_per_iter": 1000 * t_pers, "gups": units / t_pers / 1e9,
                            "graph_vs_persistent": t_pers / t_batch, "max_abs_diff_to_graph_batch": pers_diff,
                            "note": "STT_SOLVE_PERSISTENT: every instance's duals and primal on its stream, then all "
