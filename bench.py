@@ -110,6 +110,8 @@ def parse_args():
                     help="run only the full-size FP64 check of one 4D primal-dual iteration (two frames) and print it")
     ap.add_argument("--no-configs", action="store_true",
                     help="default run: skip the single-frame workloads' sub-lines")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="default run: skip the batched-instances leg (config 4; --batch-only runs it alone)")
     ap.add_argument("--fp-probe", action="store_true",
                     help="with --config: only project a few views with the fused forward projector "
                          "(a small command for ncu captures at that size)")
@@ -1311,6 +1313,11 @@ def run_stt(args):
 
     # the single-frame workloads, one sub-line each (rank 0, one GPU)
     configs = None
+    # config 4 (the batch of 64 uneven instances), a few iterations each form
+    batch = None
+    if not args.no_batch and world == 1:
+        with c_stdout_to_stderr():
+            batch = batch_leg(args, min(args.steps, 3), min(args.warmup, 2))
     if not args.no_configs and world == 1:
         configs = {}
         for cid in sorted(CONFIG_SPECS):
@@ -1359,7 +1366,8 @@ def run_stt(args):
                 "fp64_check": None if cpu is None else cpu.get("fp64_check"),
                 "fp64_pd_iteration": None if cpu is None else cpu.get("fp64_pd_iteration"),
                 "flow": flow,
-                "configs": configs}
+                "configs": configs,
+                "batch": batch}
         print(json.dumps(line), flush=True)
     solver.close()
     ctx.close()
@@ -1483,10 +1491,16 @@ def batch_fp64_check(inst, dev, stream, count=2) -> dict:
 
 
 def run_batch_only(args):
+    print(json.dumps(batch_leg(args, args.steps, args.warmup)), flush=True)
+    return 0
+
+
+def batch_leg(args, steps, warmup) -> dict:
     """Config 4: independent single-frame TV + SART solves of uneven size
     (cubes 64^3-192^3, detectors 128^2-384^2, 60-240 views, sid 500-700 mm,
     sdd 900-1100 mm, seeded), one batched graph iteration against the same
-    instances solved one after another on one stream."""
+    instances solved one after another on one stream; `steps` timed
+    iterations after `warmup`."""
     import torch
 
     import spacetimetomography_b200 as stt
@@ -1526,16 +1540,16 @@ def run_batch_only(args):
             d["vol"].zero_()
         b = stt.Batch(inst, mode=stt.SOLVE_GRAPH)
         staging["f32"] = b.staging()
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             b.iterate(1, stream)
         torch.cuda.synchronize()
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             b.iterate(1, stream)
         e1.record(stream)
         torch.cuda.synchronize()
         b.close()
-        return e0.elapsed_time(e1) / 1000.0 / args.steps
+        return e0.elapsed_time(e1) / 1000.0 / steps
 
     t_default = batched_time()  # the default launch choices
     t0 = time.perf_counter()
@@ -1553,15 +1567,15 @@ def run_batch_only(args):
         d.pop("truth")
     b16 = stt.Batch(inst16, mode=stt.SOLVE_GRAPH)
     staging["bf16"] = b16.staging()
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         b16.iterate(1, stream)
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         b16.iterate(1, stream)
     e1.record(stream)
     torch.cuda.synchronize()
-    t_b16 = e0.elapsed_time(e1) / 1000.0 / args.steps
+    t_b16 = e0.elapsed_time(e1) / 1000.0 / steps
     b16.close()
     num = sum(float((d["vol"].float() - r).norm() ** 2) for d, r in zip(inst16, f32_result))
     den = sum(float(r.norm() ** 2) for r in f32_result)
@@ -1573,16 +1587,16 @@ def run_batch_only(args):
     for d in inst:
         d["vol"].zero_()
     bpers = stt.Batch(inst, mode=stt.SOLVE_PERSISTENT)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         bpers.iterate(1, stream)
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         bpers.iterate(1, stream)
     e1.record(stream)
     torch.cuda.synchronize()
     bpers.poll_status(stream)
-    t_pers = e0.elapsed_time(e1) / 1000.0 / args.steps
+    t_pers = e0.elapsed_time(e1) / 1000.0 / steps
     bpers.close()
     pers_diff = max(float((d["vol"] - r).abs().max()) for d, r in zip(inst, f32_result))
     # the instances' own tuned choices again (the batches may have set their
@@ -1630,7 +1644,7 @@ def run_batch_only(args):
     errs = [float((d["vol"] - d["truth"]).norm() / d["truth"].norm()) for d in inst[:4]]
     fp64 = batch_fp64_check(inst, dev, stream)
     line = {"metric": "projector GUPS over one batched iteration of independent instances", "value": units / t_batch / 1e9,
-            "unit": "GUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_batch,
+            "unit": "GUPS", "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": 1000 * t_batch,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{args.batch_instances} single-frame TV + SART instances, cubes 64^3-192^3, "
                                    "detectors 128^2-384^2, 60-240 views, voxel-based BP"},
@@ -1646,7 +1660,7 @@ def run_batch_only(args):
                                    "64 SART calls in one cooperative launch (blocks split by work)"},
             "bf16_storage": {"ms_per_iter": 1000 * t_b16, "gups": units / t_b16 / 1e9,
                              "rel_l2_to_f32_storage": bf16_vs_f32, "rel_l2_to_phantom_first4": bf16_err,
-                             "iterations": args.warmup + args.steps,
+                             "iterations": warmup + steps,
                              "note": "volumes and sinograms stored in BF16, FP32 arithmetic; compared with the "
                                      "FP32-storage batch after the same iterations from the same start"},
             "autotune": {"batched_ms_per_iter_default_choices": 1000 * t_default,
@@ -1659,10 +1673,9 @@ def run_batch_only(args):
                          "bp_variant_counts": np.bincount([c["bp_variant"] for c in choices], minlength=5).tolist(),
                          "first_instances": [{k: c[k] for k in ("fp", "slab", "bp", "staged_bins")}
                                              for c in choices[:4]]}}
-    print(json.dumps(line), flush=True)
     for sv, _ in solvers:
         sv.close()
-    return 0
+    return line
 
 
 def main():
