@@ -428,7 +428,7 @@ stt_status stt_batch_poll_status(stt_batch *b, void *stream) {
             BCUDA(b, cudaMemsetAsync(b->status, 0, sizeof(int), cs), "clear status word");
             BCUDA(b, cudaStreamSynchronize(cs), "cudaStreamSynchronize");
             worst = bfail(b, STT_ERR_TIMEOUT,
-                          "a barrier of the persistent sweep waited about 1 s: the sweep was abandoned and the "
+                          "a barrier of the persistent iteration waited about 5 s: it was abandoned and the "
                           "iteration's results are not valid");
         }
     }

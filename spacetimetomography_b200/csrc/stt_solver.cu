@@ -810,7 +810,7 @@ stt_status stt_solver_poll_status(stt_solver *s, void *stream) {
     return sfail(s, STT_ERR_TIMEOUT,
                  "a bounded device-side wait gave up: a TMA copy into shared memory did not land within about 0.1 s "
                  "(the results were computed from global memory instead), or a barrier of the persistent sweep "
-                 "waited about 1 s (the sweep was abandoned: the iteration's results are not valid)");
+                 "waited about 5 s (it was abandoned: the iteration's results are not valid)");
 }
 
 const char *stt_solver_last_error(const stt_solver *s) { return s ? s->err.c_str() : ""; }
