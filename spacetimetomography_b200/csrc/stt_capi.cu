@@ -560,6 +560,9 @@ stt_status stt_bp_ray_scatter(stt_ctx *ctx, const float *corr, float *contrib, f
 // per-voxel load form runs (the same bits).
 static void ensure_corr_tex(stt_ctx *ctx) {
     if (ctx->corr_tex.tex && ctx->corr_tex.W == ctx->g.W && ctx->corr_tex.H == ctx->g.H) return;
+    // another detector size: launches enqueued earlier (on any stream) may still
+    // gather from the old texture, so the device drains before it is destroyed
+    if (ctx->corr_tex.tex && cudaDeviceSynchronize() != cudaSuccess) cudaGetLastError();
     stt::free_corr_tex(ctx->corr_tex);
     if (stt::make_corr_tex(ctx->g.W, ctx->g.H, ctx->corr_tex) != cudaSuccess) cudaGetLastError();
 }
