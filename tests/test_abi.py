@@ -142,3 +142,17 @@ def test_typed_entry_points_reject_bad_dtypes_without_gpu(lib):
     assert lib.stt_sart_sweep_typed(None, None, 7, None, None, 0, 0, 0.3, 1.0, 0, None, None, None) != 0
     assert lib.stt_bp_voxel_typed(None, None, None, 7, 0.3, 1.0, 0, None) != 0
     assert lib.stt_bp_ray_typed(None, None, None, 7, 1.0, 0, None) != 0
+
+
+def test_solver_modes_and_persistent_info_without_gpu(lib):
+    """The solver modes of stt_solve_mode as the Python side numbers them, and
+    the persistent form's report refusing a null solver (no device touched)."""
+    import spacetimetomography_b200 as stt
+
+    text = (ROOT / "include" / "stt.h").read_text()
+    for name, value in (("PLAIN", stt.SOLVE_PLAIN), ("STREAMS", stt.SOLVE_STREAMS), ("GRAPH", stt.SOLVE_GRAPH),
+                        ("PERSISTENT", stt.SOLVE_PERSISTENT)):
+        assert re.search(rf"STT_SOLVE_{name}\s*=\s*{value}\b", text), name
+    b, g = C.c_int(7), C.c_int(7)
+    assert lib.stt_solver_persistent_info(None, C.byref(b), C.byref(g)) == 1  # STT_ERR_INVALID
+    assert lib.stt_solver_stats(None, None, None) == 1
